@@ -1,0 +1,154 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+``liborc.so`` is the C++ restatement of the reference's RRTM LW/SW column radiation in this directory
+(``rrtm_lw.hpp``, ``rrtm_sw.hpp``, ``rrtm_mcica.hpp``).  ``solve(cols, precision="double")`` returns the
+same outputs as the product's C-ABI (in float64).  ``reference_solve`` runs the reference's own kernels
+compiled for the host (``_ref/libref_rrtm.so``, built by ``build_ref.sh`` where the reference tree is
+available) through the same interface.
+
+Only the tests, the smoke check and the benchmark's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liborc.so"
+REF_LIB = HERE / "_ref" / "libref_rrtm.so"
+TABLES = HERE.parent / "woof_nam_b200" / "data" / "rrtm_tables.npz"
+
+_F = ctypes.POINTER(ctypes.c_float)
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_U = ctypes.POINTER(ctypes.c_uint)
+
+
+def build(force: bool = False) -> Path:
+    """Compile liborc.so with the Makefile beside this file (no GPU needed)."""
+    if force or not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime
+                                        for p in HERE.glob("rrtm_*.?pp")):
+        subprocess.run(["make", "-C", str(HERE), "liborc.so"], check=True)
+    return LIB
+
+
+def _load(path: Path):
+    lib = ctypes.CDLL(str(path))
+    lib.orc_add_table.argtypes = [ctypes.c_char_p, _D, ctypes.c_long]
+    lib.orc_add_itable.argtypes = [ctypes.c_char_p, _I, ctypes.c_long]
+    lib.orc_solve.restype = ctypes.c_int
+    tabs = np.load(TABLES)
+    lib.orc_clear_tables()
+    for name in tabs.files:
+        a = tabs[name]
+        if a.dtype.kind == "i":
+            b = np.ascontiguousarray(a, dtype=np.int32).ravel()
+            lib.orc_add_itable(name.encode(), b.ctypes.data_as(_I), b.size)
+        else:
+            b = np.ascontiguousarray(a, dtype=np.float64).ravel()
+            lib.orc_add_table(name.encode(), b.ctypes.data_as(_D), b.size)
+    return lib
+
+
+_LIBS: dict = {}
+
+
+def lib(which: str = "port"):
+    if which not in _LIBS:
+        if which == "port":
+            _LIBS[which] = _load(build())
+        else:
+            if not REF_LIB.exists():
+                raise FileNotFoundError(f"{REF_LIB} is not built (oracle/build_ref.sh needs the reference tree)")
+            _LIBS[which] = _load(REF_LIB)
+    return _LIBS[which]
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def solve(cols, precision: str = "double", iswmode: int = 2, window_cols: int = 0, sw_chunk: int = 32768,
+          route: int = 0, iovrlw: int = 1, iovrsw: int = 1, lw_seed0: int = 140, sw_seed0: int = 1,
+          cpathfac: float = 1.5, nthreads: int = 0, which: str = "port", want_profiles: bool = False,
+          icseed=None, faerlw=None, faersw=None) -> dict:
+    """Run the oracle on a ``woof_nam_b200.columns.Columns`` request; returns float64 outputs."""
+    L = lib(which)
+    nlay, ncol = cols.nlay, cols.ncol
+    cfg = np.array([iswmode, int(cols.diagnostic_clouds), window_cols, sw_chunk, route, iovrlw, iovrsw,
+                    lw_seed0, sw_seed0], dtype=np.int32)
+    out = {
+        "htlw": np.zeros((nlay, ncol)), "htsw": np.zeros((nlay, ncol)),
+        "topflw": np.zeros((2, ncol)), "sfcflw": np.zeros((4, ncol)),
+        "topfsw": np.zeros((3, ncol)), "sfcfsw": np.zeros((4, ncol)), "fdncmp": np.zeros((6, ncol)),
+    }
+    if want_profiles:
+        out["lwflx"] = np.zeros((4, nlay + 1, ncol))
+        out["swflx"] = np.zeros((4, nlay + 1, ncol))
+    if route == 1:
+        out["lw_mask"] = np.zeros((5, nlay, ncol), dtype=np.uint32)
+        out["sw_mask"] = np.zeros((4, nlay, ncol), dtype=np.uint32)
+    keep = [_f(getattr(cols, f)) for f in cols.FIELDS]
+    fa = _f(faerlw) if faerlw is not None else None
+    fs = _f(faersw) if faersw is not None else None
+    seeds = np.ascontiguousarray(icseed, dtype=np.int32) if icseed is not None else None
+
+    def p(a, t):
+        return a.ctypes.data_as(t) if a is not None else None
+
+    rc = L.orc_solve(
+        ctypes.c_int(0 if precision == "float" else 1), p(cfg, _I), ctypes.c_double(cpathfac),
+        ctypes.c_int(nlay), ctypes.c_int(ncol),
+        *[p(a, _F) for a in keep[:8]], p(fa, _F), p(fs, _F), *[p(a, _F) for a in keep[8:]],
+        p(seeds, _I), ctypes.c_double(cols.solcon),
+        p(out["htlw"], _D), p(out["htsw"], _D), p(out["topflw"], _D), p(out["sfcflw"], _D),
+        p(out["topfsw"], _D), p(out["sfcfsw"], _D), p(out["fdncmp"], _D),
+        p(out.get("lwflx"), _D), p(out.get("swflx"), _D), p(out.get("lw_mask"), _U), p(out.get("sw_mask"), _U),
+        ctypes.c_int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"oracle solve failed ({rc})")
+    return out
+
+
+def reference_solve(cols, **kw) -> dict:
+    """The reference's own kernels compiled for the host, driven in the reference's call order (float32)."""
+    kw = dict(kw)
+    kw.pop("precision", None)
+    return solve(cols, precision="float", which="ref", **kw)
+
+
+def host_threads() -> int:
+    return len(os.sched_getaffinity(0))
+
+
+def set_debug(sw_tau_scale: float = 1.0, which: str = "port") -> None:
+    """Test hook: scale the SW gas optical depths before the two-stream solver (1.0 = off)."""
+    lib(which).orc_set_debug(ctypes.c_double(sw_tau_scale))
+
+
+def sw_stages(cols, which: str = "port", iswmode: int = 2) -> dict:
+    """SW stage outputs (float statements) of the request's day columns, layers surface first."""
+    L = lib(which)
+    nlay, ncol = cols.nlay, cols.ncol
+    nday = int((cols.coszen >= np.float32(1e-4)).sum())
+    out = {"taug": np.zeros((nday, nlay, 112), np.float32), "taur": np.zeros((nday, nlay, 112), np.float32),
+           "sfluxzen": np.zeros((nday, 112), np.float32), "taucw": np.zeros((nday, 14, nlay), np.float32),
+           "ssacw": np.zeros((nday, 14, nlay), np.float32), "asycw": np.zeros((nday, 14, nlay), np.float32),
+           "cldfrc": np.zeros((nday, nlay), np.float32), "zcf": np.zeros((nday, 2), np.float32),
+           "laytrop": np.zeros(nday, np.int32)}
+    cfg = np.array([iswmode, int(cols.diagnostic_clouds)], dtype=np.int32)
+    keep = {f: _f(getattr(cols, f)) for f in cols.FIELDS}
+    rc = L.orc_sw_stages(cfg.ctypes.data_as(_I), ctypes.c_int(nlay), ctypes.c_int(ncol),
+                         *[keep[f].ctypes.data_as(_F) for f in ("plyr", "plvl", "tlyr", "tlvl", "qlyr", "olyr",
+                                                              "gasvmr", "clouds", "sfcalb", "coszen")],
+                         ctypes.c_double(cols.solcon),
+                         *[out[k].ctypes.data_as(_F) for k in ("taug", "taur", "sfluxzen", "taucw", "ssacw",
+                                                              "asycw", "cldfrc", "zcf")],
+                         out["laytrop"].ctypes.data_as(_I))
+    if rc != 0:
+        raise RuntimeError("sw_stages failed")
+    return out

@@ -1,0 +1,333 @@
+// rrtm_oracle.cpp -- C entry points of the CPU oracle (test infrastructure only).
+//
+// Drives the LW and SW column restatements (rrtm_lw.hpp, rrtm_sw.hpp) over a request in the reference's
+// call order: grrad cloud-path factor and lwrad (phys_rrtm_grrad_lw.cu:58-80, lw_core.seam), swrad on the
+// day columns (coszen >= 1e-4, phys_rrtm_grrad_sw.cu:69) with the day list split into windows and chunks
+// for the MINVAL(laytrop) groups (physics/rrtm/sw_seam.py:23-37, phys_rrtm_sw_swrad.py:340-386).
+// Precision 0 runs every statement in float, precision 1 in double.  OpenMP over columns.
+#include <cstdio>
+#include <limits>
+#include "rrtm_lw.hpp"
+#include "rrtm_sw.hpp"
+#include "rrtm_mcica.hpp"
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace orc {
+// Test hook: factor applied to the SW gas optical depths before the two-stream solver (orc_set_debug).
+double g_sw_tau_scale = 1.0;
+
+TableStore& tables()
+{
+    static TableStore s;
+    return s;
+}
+
+template <class R>
+static void run_lw(const Config& cfg, const Inputs& in, const Outputs& out)
+{
+    const int nlay = in.nlay, ncol = in.ncol, nlp1 = nlay + 1;
+    const LwTables<R> tb;
+    const R heatfac = (R)CON_G * (R)1.0e-2f / (R)CON_CP;
+    const R fluxfac = std::is_same<R, float>::value ? (R)((double)(float)(2.0 * std::asin(1.0)) * 2.0e4)
+                                                    : (R)(2.0 * std::asin(1.0) * 2.0e4);
+    const int ilwcliq = cfg.diagnostic ? 0 : 1;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int col = 0; col < ncol; ++col) {
+        std::vector<float> cl(9 * (size_t)nlay);
+        for (int n = 0; n < 9; ++n)
+            for (int k = 0; k < nlay; ++k) cl[n * nlay + k] = in.clouds[((size_t)n * nlay + k) * ncol + col];
+        if (ilwcliq > 0) {   // grrad_lw_pre: clouds(.,.,2) and (.,.,4) scaled by the cloud-path factor
+            for (int k = 0; k < nlay; ++k) {
+                cl[1 * nlay + k] = cl[1 * nlay + k] * (float)cfg.cpathfac;
+                cl[3 * nlay + k] = cl[3 * nlay + k] * (float)cfg.cpathfac;
+            }
+        }
+        LwColumn<R> c(nlay);
+        lw_prep(c, in, col, cl.data(), ilwcliq);
+        lw_cldprop(c, cl.data(), ilwcliq);
+        lw_setcoef(c);
+        lw_taumol(c);
+        if (cfg.route == 1) {
+            lw_mcica<R>(c, cl.data(), ilwcliq, cfg, in, col, out.lw_mask);
+            lw_rtrnmc(c, tb, heatfac, fluxfac);
+        } else {
+            lw_rtrnmr(c, tb, heatfac, fluxfac);
+        }
+        for (int k0 = 0; k0 < nlay; ++k0) out.htlw[(size_t)(nlay - 1 - k0) * ncol + col] = (double)c.htr[k0];
+        out.topflw[0 * (size_t)ncol + col] = (double)c.totuflux[nlay];
+        out.topflw[1 * (size_t)ncol + col] = (double)c.totuclfl[nlay];
+        out.sfcflw[0 * (size_t)ncol + col] = (double)c.totuflux[0];
+        out.sfcflw[1 * (size_t)ncol + col] = (double)c.totuclfl[0];
+        out.sfcflw[2 * (size_t)ncol + col] = (double)c.totdflux[0];
+        out.sfcflw[3 * (size_t)ncol + col] = (double)c.totdclfl[0];
+        if (out.lwflx) {
+            for (int k = 0; k <= nlay; ++k) {
+                const size_t lev = (size_t)(nlay - k);
+                out.lwflx[(0 * (size_t)nlp1 + lev) * ncol + col] = (double)c.totuflux[k];
+                out.lwflx[(1 * (size_t)nlp1 + lev) * ncol + col] = (double)c.totdflux[k];
+                out.lwflx[(2 * (size_t)nlp1 + lev) * ncol + col] = (double)c.totuclfl[k];
+                out.lwflx[(3 * (size_t)nlp1 + lev) * ncol + col] = (double)c.totdclfl[k];
+            }
+        }
+    }
+}
+
+// Day list, windows and chunks of the SW MINVAL(laytrop) groups.  kmin8[d] is the minimum laytrop over
+// the day column's group of 8 consecutive day columns of its chunk; kminw[d] over the whole chunk.
+static void sw_groups(const std::vector<int>& day, const std::vector<int>& lt, const Config& cfg, int ncol,
+                      std::vector<int>& kmin8, std::vector<int>& kminw)
+{
+    const int nday = (int)day.size();
+    kmin8.assign(nday, 0);
+    kminw.assign(nday, 0);
+    const int wcols = cfg.window_cols > 0 ? cfg.window_cols : ncol;
+    int d = 0;
+    while (d < nday) {
+        const int win = day[d] / wcols;
+        int e = d;
+        while (e < nday && day[e] / wcols == win) ++e;           // [d, e): this window's day columns
+        for (int c0 = d; c0 < e; c0 += cfg.sw_chunk) {
+            const int c1 = std::min(e, c0 + cfg.sw_chunk);
+            int mw = std::numeric_limits<int>::max();
+            for (int i = c0; i < c1; ++i) mw = std::min(mw, lt[i]);
+            for (int g0 = c0; g0 < c1; g0 += 8) {
+                const int g1 = std::min(c1, g0 + 8);
+                int m8 = std::numeric_limits<int>::max();
+                for (int i = g0; i < g1; ++i) m8 = std::min(m8, lt[i]);
+                for (int i = g0; i < g1; ++i) kmin8[i] = m8;
+            }
+            for (int i = c0; i < c1; ++i) kminw[i] = mw;
+        }
+        d = e;
+    }
+}
+
+template <class R>
+static void run_sw(const Config& cfg, const Inputs& in, const Outputs& out)
+{
+    const int nlay = in.nlay, ncol = in.ncol, nlp1 = nlay + 1;
+    const int iswcliq = cfg.diagnostic ? 0 : 1;
+    const SwExpTable<R> tb;
+    const R heatfac = std::is_same<R, float>::value ? (R)(float)(9.80665 * 1.0e-2 / 1.0046e3)
+                                                    : (R)(9.80665 * 1.0e-2 / 1.0046e3);
+    for (int i = 0; i < nlay * ncol; ++i) out.htsw[i] = 0;
+    for (int i = 0; i < 3 * ncol; ++i) out.topfsw[i] = 0;
+    for (int i = 0; i < 4 * ncol; ++i) out.sfcfsw[i] = 0;
+    if (out.fdncmp)
+        for (int i = 0; i < 6 * ncol; ++i) out.fdncmp[i] = 0;
+    if (out.swflx)
+        for (size_t i = 0; i < (size_t)4 * nlp1 * ncol; ++i) out.swflx[i] = 0;
+    std::vector<int> day;
+    for (int col = 0; col < ncol; ++col)
+        if (in.coszen[col] >= 1.0e-4f) day.push_back(col);
+    const int nday = (int)day.size();
+    std::vector<int> lt(nday);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int d = 0; d < nday; ++d) {
+        SwColumn<R> c(nlay);
+        sw_prep(c, in, day[d], iswcliq);
+        sw_setcoef(c);
+        lt[d] = c.laytrop;
+    }
+    std::vector<int> kmin8, kminw;
+    sw_groups(day, lt, cfg, ncol, kmin8, kminw);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int d = 0; d < nday; ++d) {
+        const int col = day[d];
+        SwColumn<R> c(nlay);
+        sw_prep(c, in, col, iswcliq);
+        sw_cldprop(c, iswcliq);
+        sw_setcoef(c);
+        sw_taumol(c, kmin8[d], kminw[d]);
+        if (g_sw_tau_scale != 1.0)
+            for (auto& v : c.taug) v = v * (R)g_sw_tau_scale;
+        if (cfg.route == 1) {
+            sw_mcica<R>(c, cfg, in, col, out.sw_mask);
+            sw_spcvrtm(c, tb, cfg.iswmode);
+        } else {
+            sw_spcvrtc(c, tb, cfg.iswmode);
+        }
+        // swrad_post: band sums of the level fluxes, heating rates, TOA and surface fluxes
+        std::vector<R> flxuc(nlp1), flxdc(nlp1), fnet(nlp1);
+        for (int k = 0; k < nlp1; ++k) {
+            R su = 0, sd = 0;
+            for (int ib = 0; ib < 14; ++ib) {
+                su = su + c.fxupc[(size_t)ib * nlp1 + k];
+                sd = sd + c.fxdnc[(size_t)ib * nlp1 + k];
+            }
+            flxuc[k] = su; flxdc[k] = sd;
+            fnet[k] = flxdc[k] - flxuc[k];
+        }
+        for (int k = 1; k < nlp1; ++k) {
+            const R rf = heatfac / c.delp[k - 1];
+            const R h = (fnet[k] - fnet[k - 1]) * rf;
+            out.htsw[(size_t)(nlp1 - 1 - k) * ncol + col] = (double)h;
+        }
+        out.topfsw[0 * (size_t)ncol + col] = (double)c.ftoauc;
+        out.topfsw[1 * (size_t)ncol + col] = (double)c.ftoadc;
+        out.topfsw[2 * (size_t)ncol + col] = (double)c.ftoau0;
+        out.sfcfsw[0 * (size_t)ncol + col] = (double)c.fsfcuc;
+        out.sfcfsw[1 * (size_t)ncol + col] = (double)c.fsfcdc;
+        out.sfcfsw[2 * (size_t)ncol + col] = (double)c.fsfcu0;
+        out.sfcfsw[3 * (size_t)ncol + col] = (double)c.fsfcd0;
+        if (out.fdncmp) {
+            out.fdncmp[0 * (size_t)ncol + col] = (double)c.suvbf0;
+            out.fdncmp[1 * (size_t)ncol + col] = (double)c.suvbfc;
+            out.fdncmp[2 * (size_t)ncol + col] = (double)c.sfbmc[0];
+            out.fdncmp[3 * (size_t)ncol + col] = (double)c.sfdfc[0];
+            out.fdncmp[4 * (size_t)ncol + col] = (double)c.sfbmc[1];
+            out.fdncmp[5 * (size_t)ncol + col] = (double)c.sfdfc[1];
+        }
+        if (out.swflx) {
+            for (int k = 0; k < nlp1; ++k) {
+                R su0 = 0, sd0 = 0;
+                for (int ib = 0; ib < 14; ++ib) {
+                    su0 = su0 + c.fxup0[(size_t)ib * nlp1 + k];
+                    sd0 = sd0 + c.fxdn0[(size_t)ib * nlp1 + k];
+                }
+                const size_t lev = (size_t)(nlp1 - 1 - k);
+                out.swflx[(0 * (size_t)nlp1 + lev) * ncol + col] = (double)flxuc[k];
+                out.swflx[(1 * (size_t)nlp1 + lev) * ncol + col] = (double)flxdc[k];
+                out.swflx[(2 * (size_t)nlp1 + lev) * ncol + col] = (double)su0;
+                out.swflx[(3 * (size_t)nlp1 + lev) * ncol + col] = (double)sd0;
+            }
+        }
+    }
+}
+}  // namespace orc
+
+extern "C" {
+
+int orc_set_debug(double sw_tau_scale)
+{
+    orc::g_sw_tau_scale = sw_tau_scale;
+    return 0;
+}
+
+// SW stage outputs (float statements) of the request's day columns; same layout as the reference
+// driver's orc_sw_stages (oracle/ref_driver.cpp): one window, one chunk.
+int orc_sw_stages(const int* cfg_i, int nlay, int ncol, const float* plyr, const float* plvl, const float* tlyr,
+                  const float* tlvl, const float* qlyr, const float* olyr, const float* gasvmr, const float* clouds,
+                  const float* sfcalb, const float* coszen, double solcon, float* taug, float* taur, float* sfluxzen,
+                  float* taucw, float* ssacw, float* asycw, float* cldfrc, float* zcf, int* laytrop)
+{
+    try {
+        using namespace orc;
+        Config cfg;
+        cfg.iswmode = cfg_i[0];
+        cfg.diagnostic = cfg_i[1];
+        cfg.sw_chunk = 1 << 30;
+        Inputs in{plyr, plvl, tlyr, tlvl, qlyr, olyr, gasvmr, clouds, nullptr, nullptr, nullptr, nullptr,
+                  sfcalb, coszen, nullptr, solcon, nlay, ncol};
+        const int iswcliq = cfg.diagnostic ? 0 : 1;
+        std::vector<int> day;
+        for (int col = 0; col < ncol; ++col)
+            if (coszen[col] >= 1.0e-4f) day.push_back(col);
+        const int nday = (int)day.size();
+        std::vector<int> lt(nday);
+        for (int d = 0; d < nday; ++d) {
+            SwColumn<float> c(nlay);
+            sw_prep(c, in, day[d], iswcliq);
+            sw_setcoef(c);
+            lt[d] = c.laytrop;
+        }
+        std::vector<int> kmin8, kminw;
+        sw_groups(day, lt, cfg, ncol, kmin8, kminw);
+        for (int d = 0; d < nday; ++d) {
+            SwColumn<float> c(nlay);
+            sw_prep(c, in, day[d], iswcliq);
+            sw_cldprop(c, iswcliq);
+            sw_setcoef(c);
+            sw_taumol(c, kmin8[d], kminw[d]);
+            for (int k = 0; k < nlay; ++k)
+                for (int g = 0; g < 112; ++g) {
+                    taug[((size_t)d * nlay + k) * 112 + g] = c.TG(g, k);
+                    taur[((size_t)d * nlay + k) * 112 + g] = c.TR(g, k);
+                }
+            for (int g = 0; g < 112; ++g) sfluxzen[(size_t)d * 112 + g] = c.sfluxzen[g];
+            for (int ib = 0; ib < 14; ++ib)
+                for (int k = 0; k < nlay; ++k) {
+                    const size_t o = ((size_t)d * 14 + ib) * nlay + k;
+                    taucw[o] = c.taucw[(size_t)ib * nlay + k];
+                    ssacw[o] = c.ssacw[(size_t)ib * nlay + k];
+                    asycw[o] = c.asycw[(size_t)ib * nlay + k];
+                }
+            for (int k = 0; k < nlay; ++k) cldfrc[(size_t)d * nlay + k] = c.cldfrc[k];
+            zcf[2 * d] = c.zcf0;
+            zcf[2 * d + 1] = c.zcf1;
+            laytrop[d] = c.laytrop;
+        }
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
+int orc_clear_tables(void)
+{
+    orc::tables().t.clear();
+    orc::tables().ti.clear();
+    return 0;
+}
+
+int orc_add_table(const char* name, const double* data, long n)
+{
+    orc::tables().t[name] = std::vector<double>(data, data + n);
+    return 0;
+}
+
+int orc_add_itable(const char* name, const int* data, long n)
+{
+    orc::tables().ti[name] = std::vector<int>(data, data + n);
+    return 0;
+}
+
+// Solve a request.  precision: 0 float, 1 double.  cfg_i: iswmode, diagnostic, window_cols, sw_chunk,
+// route, iovrlw, iovrsw, lw_seed0, sw_seed0.  Outputs are double arrays (see rrtm_common.hpp Outputs);
+// fdncmp, lwflx, swflx and the masks may be null.
+int orc_solve(int precision, const int* cfg_i, double cpathfac, int nlay, int ncol, const float* plyr,
+              const float* plvl, const float* tlyr, const float* tlvl, const float* qlyr, const float* olyr,
+              const float* gasvmr, const float* clouds, const float* faerlw, const float* faersw,
+              const float* sfcemis, const float* tsfg, const float* sfcalb, const float* coszen,
+              const int* icseed, double solcon, double* htlw, double* htsw, double* topflw, double* sfcflw,
+              double* topfsw, double* sfcfsw, double* fdncmp, double* lwflx, double* swflx,
+              unsigned int* lw_mask, unsigned int* sw_mask, int nthreads)
+{
+    try {
+#ifdef _OPENMP
+        if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+        (void)nthreads;
+#endif
+        orc::Config cfg;
+        cfg.iswmode = cfg_i[0];
+        cfg.diagnostic = cfg_i[1];
+        cfg.window_cols = cfg_i[2];
+        cfg.sw_chunk = cfg_i[3] > 0 ? cfg_i[3] : 32768;
+        cfg.route = cfg_i[4];
+        cfg.iovrlw = cfg_i[5];
+        cfg.iovrsw = cfg_i[6];
+        cfg.lw_seed0 = cfg_i[7];
+        cfg.sw_seed0 = cfg_i[8];
+        cfg.cpathfac = cpathfac;
+        orc::Inputs in{plyr, plvl, tlyr, tlvl, qlyr, olyr, gasvmr, clouds, faerlw, faersw, sfcemis, tsfg,
+                       sfcalb, coszen, icseed, solcon, nlay, ncol};
+        orc::Outputs out{htlw, htsw, topflw, sfcflw, topfsw, sfcfsw, fdncmp, lwflx, swflx, lw_mask, sw_mask};
+        if (precision == 0) {
+            orc::run_lw<float>(cfg, in, out);
+            orc::run_sw<float>(cfg, in, out);
+        } else {
+            orc::run_lw<double>(cfg, in, out);
+            orc::run_sw<double>(cfg, in, out);
+        }
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
+}  // extern "C"
