@@ -1,0 +1,130 @@
+/* radb200.h -- C ABI of the B200 RRTM longwave + shortwave column-radiation library (libradb200.so).
+ *
+ * The library replaces the column solve that WOOF-NAM's radiation driver hook runs between the grrad
+ * input set-up and driver_post: the reference binds it as the callable `rrtm_call(ctx, args)` handed to
+ * `phys_rad_driver.run(ctx, *, radupdate=None, rrtm_call=None, mype=0)`
+ * (namgpu/physics/driver/phys_rad_driver.py:25-30, :171, :255-262), whose column work is
+ * `lwrad.run(ctx)` (namgpu/physics/rrtm/phys_rrtm_lw_lwrad.py:247) and `swrad.run(ctx, has_htrswb, nc)`
+ * (namgpu/physics/rrtm/phys_rrtm_sw_swrad.py:282).  Inputs and outputs keep the reference's arrays,
+ * names, units and layout: float32, [field][level][column] with the column index fastest and level 0 the
+ * model top (the reference's [field, level, JM, IM] with JM*IM columns flattened).
+ *
+ * Conventions: every entry returns 0 or a negative RAD_E_* code; rad_last_error() gives the message.
+ * Device pointers only in rad_solve (the caller owns inputs and outputs, the library owns its scratch
+ * and tables); rad_solve is asynchronous on the given stream and performs no host synchronisation.
+ * One handle per host thread or stream; calls on distinct handles are thread-safe.
+ */
+#ifndef RADB200_H
+#define RADB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RAD_ABI_VERSION 1
+
+enum {
+    RAD_OK = 0,
+    RAD_E_INVALID = -1,      /* bad argument, shape or configuration */
+    RAD_E_TABLES = -2,       /* tables missing or malformed */
+    RAD_E_CUDA = -3,         /* a CUDA call failed */
+    RAD_E_NOMEM = -4,        /* device allocation failed */
+    RAD_E_BUDGET = -5,       /* request refused by the HBM budget (serving queue) */
+    RAD_E_TIMEOUT = -6,      /* a bounded wait gave up (serving queue) */
+    RAD_E_BUSY = -7          /* queue full or slot in use */
+};
+
+enum { RAD_PREC_FP64 = 0, RAD_PREC_MIXED = 1 };
+enum { RAD_ROUTE_NAM = 0, RAD_ROUTE_MCICA = 1 };
+
+typedef struct RadHandle RadHandle;
+
+/* Solve configuration.  Defaults (rad_config_default) are NAM's runtime switches: iswmode 2 (PIFM),
+ * iovrlw = iovrsw = 1 (maximum-random), prognostic clouds, cloud-path factor 1.5 for LW
+ * (module_RA_RRTM.F90:212 as cited at namgpu/physics/rrtm/phys_rrtm_grrad_lw.py:75). */
+typedef struct {
+    int32_t nlay;            /* radiation layers, including the extra top layer (61 for 60 model layers) */
+    int32_t precision;       /* RAD_PREC_FP64 or RAD_PREC_MIXED */
+    int32_t route;           /* RAD_ROUTE_NAM (rtrnmr + spcvrtc) or RAD_ROUTE_MCICA */
+    int32_t iswmode;         /* SW two-stream: 1 delta-Eddington, 2 PIFM, 3 discrete ordinates */
+    int32_t diagnostic;      /* 1: clouds hold optical depth / SSA / asymmetry (ilwcliq = iswcliq = 0) */
+    int32_t window_cols;     /* columns per SW MINVAL(laytrop) window, 0 = the whole request */
+    int32_t sw_chunk;        /* SW day columns per chunk (reference 32768) */
+    int32_t iovrlw, iovrsw;  /* McICA overlap (0 random, 1 max-random, 2 maximum) */
+    int32_t lw_seed0, sw_seed0;   /* McICA permutation seed offsets (ipsdlw0 = 140, ipsdsw0 = 1) */
+    float cpathfac;          /* LW cloud-path factor (1.5) */
+} RadConfig;
+
+/* Column inputs (device pointers, float32).  ncol columns, nlay layers, nlp1 = nlay + 1 levels. */
+typedef struct {
+    const float* plyr;       /* [nlay][ncol]    layer pressure, mb        (RAD_PLYR) */
+    const float* plvl;       /* [nlp1][ncol]    interface pressure, mb    (RAD_PLVL) */
+    const float* tlyr;       /* [nlay][ncol]    layer temperature, K      (RAD_TLYR) */
+    const float* tlvl;       /* [nlp1][ncol]    level temperature, K      (TLVL) */
+    const float* qlyr;       /* [nlay][ncol]    specific humidity, kg/kg  (QLYR) */
+    const float* olyr;       /* [nlay][ncol]    ozone mass mixing ratio   (RAD_OLYR) */
+    const float* gasvmr;     /* [10][nlay][ncol] co2 n2o ch4 o2 co cfc11 cfc12 cfc22 ccl4 cfc113 (GASVMR) */
+    const float* clouds;     /* [9][nlay][ncol]  cfrac clwp relw ciwp reiw rain rrain snow rsnow (RAD_CLOUDS) */
+    const float* faerlw;     /* [3][16][nlay][ncol] tau, ssa, asy per LW band, or NULL (no aerosol) */
+    const float* faersw;     /* [3][14][nlay][ncol] tau, ssa, asy per SW band, or NULL */
+    const float* sfcemis;    /* [ncol] surface emissivity */
+    const float* tsfg;       /* [ncol] ground temperature, K (RAD_TSFG) */
+    const float* sfcalb;     /* [4][ncol] nir-beam, nir-diffuse, uv-vis beam, uv-vis diffuse (SFCALB) */
+    const float* coszen;     /* [ncol] cosine of the solar zenith angle (SW_COSZEN) */
+    const int32_t* icseed;   /* [ncol] McICA permutation seeds or NULL */
+    float solcon;            /* solar constant of this call, W/m2 */
+} RadColumns;
+
+/* Outputs (device pointers, float32); any optional pointer may be NULL. */
+typedef struct {
+    float* htlw;             /* [nlay][ncol] LW total-sky heating rate, K/s   (htlwc) */
+    float* htsw;             /* [nlay][ncol] SW total-sky heating rate, K/s   (HTSWC) */
+    float* topflw;           /* [2][ncol] TOA upward LW: total, clear         (topflw upfxc, upfx0) */
+    float* sfcflw;           /* [4][ncol] sfc LW: up total, up clear, down total, down clear */
+    float* topfsw;           /* [3][ncol] TOA SW: up total, down, up clear    (TOPFLX) */
+    float* sfcfsw;           /* [4][ncol] sfc SW: up total, down total, up clear, down clear (SFCFLX) */
+    float* fdncmp;           /* [6][ncol] uvbf0 uvbfc nirbm nirdf visbm visdf (FDNCMP), optional */
+    uint32_t* lw_mask;       /* [5][nlay][ncol] McICA LW cloud bits, optional (McICA route) */
+    uint32_t* sw_mask;       /* [4][nlay][ncol] McICA SW cloud bits, optional (McICA route) */
+} RadOutputs;
+
+/* Library version (RAD_ABI_VERSION).  Replaces: nothing in the reference (a versioned ABI). */
+int rad_version(void);
+
+/* Fill *cfg with the NAM defaults for nlay layers. */
+void rad_config_default(RadConfig* cfg, int32_t nlay);
+
+/* Create a handle on the current CUDA device.  Replaces the reference's per-unit table and scratch set-up
+ * (namgpu/physics/rrtm/lw_core.py:217-286 seam, phys_rrtm_sw_swrad.py:168-212 chunk_scratch). */
+int rad_create(const RadConfig* cfg, RadHandle** out);
+
+/* Load the packed k-distribution / cloud-optics / Planck tables (blob made by woof_nam_b200.tables).
+ * Replaces the reference's npz loads (namgpu/physics/rrtm/phys_rrtm_lw_setcoef.py:160-169 and the band
+ * units' load_tables). */
+int rad_load_tables(RadHandle* h, const void* blob, size_t nbytes);
+
+/* Solve ncol columns: LW on every column, SW on the sunlit ones (coszen >= 1e-4).  Replaces
+ * lwrad.run (phys_rrtm_lw_lwrad.py:247) + swrad.run (phys_rrtm_sw_swrad.py:282) as rrtm_call drives them
+ * (namgpu/physics/rrtm/rrtm_call.py:246).  stream is a cudaStream_t (NULL = legacy default stream). */
+int rad_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream);
+
+/* Scratch bytes rad_solve needs for ncol columns (the HBM admission budget uses it). */
+int64_t rad_workspace_bytes(const RadHandle* h, int64_t ncol);
+
+/* Batched solve of several independent requests in one launch set (uneven domains).  Each request keeps
+ * its own SW MINVAL(laytrop) groups, so every result equals the result of solving it alone. */
+int rad_solve_batch(RadHandle* h, int32_t nreq, const RadColumns* ins, const RadOutputs* outs,
+                    const int64_t* ncols, void* stream);
+
+/* Thread-local message of the last failing call on this handle (or a global message when h is NULL). */
+const char* rad_last_error(const RadHandle* h);
+
+void rad_destroy(RadHandle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RADB200_H */

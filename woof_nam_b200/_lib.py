@@ -1,0 +1,93 @@
+"""ctypes binding of libradb200.so (include/radb200.h).
+
+The product path is this library: if it is missing or fails to load, every solve raises -- there is no
+CPU or PyTorch fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libradb200.so"
+
+RAD_OK, RAD_E_INVALID, RAD_E_TABLES, RAD_E_CUDA, RAD_E_NOMEM, RAD_E_BUDGET, RAD_E_TIMEOUT, RAD_E_BUSY = \
+    0, -1, -2, -3, -4, -5, -6, -7
+PREC = {"fp64": 0, "mixed": 1}
+ROUTE = {"nam": 0, "mcica": 1}
+
+_fp = ctypes.POINTER(ctypes.c_float)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_up = ctypes.POINTER(ctypes.c_uint32)
+
+
+class RadConfig(ctypes.Structure):
+    _fields_ = [("nlay", ctypes.c_int32), ("precision", ctypes.c_int32), ("route", ctypes.c_int32),
+                ("iswmode", ctypes.c_int32), ("diagnostic", ctypes.c_int32), ("window_cols", ctypes.c_int32),
+                ("sw_chunk", ctypes.c_int32), ("iovrlw", ctypes.c_int32), ("iovrsw", ctypes.c_int32),
+                ("lw_seed0", ctypes.c_int32), ("sw_seed0", ctypes.c_int32), ("cpathfac", ctypes.c_float)]
+
+
+class RadColumns(ctypes.Structure):
+    _fields_ = [("plyr", ctypes.c_void_p), ("plvl", ctypes.c_void_p), ("tlyr", ctypes.c_void_p),
+                ("tlvl", ctypes.c_void_p), ("qlyr", ctypes.c_void_p), ("olyr", ctypes.c_void_p),
+                ("gasvmr", ctypes.c_void_p), ("clouds", ctypes.c_void_p), ("faerlw", ctypes.c_void_p),
+                ("faersw", ctypes.c_void_p), ("sfcemis", ctypes.c_void_p), ("tsfg", ctypes.c_void_p),
+                ("sfcalb", ctypes.c_void_p), ("coszen", ctypes.c_void_p), ("icseed", ctypes.c_void_p),
+                ("solcon", ctypes.c_float)]
+
+
+class RadOutputs(ctypes.Structure):
+    _fields_ = [("htlw", ctypes.c_void_p), ("htsw", ctypes.c_void_p), ("topflw", ctypes.c_void_p),
+                ("sfcflw", ctypes.c_void_p), ("topfsw", ctypes.c_void_p), ("sfcfsw", ctypes.c_void_p),
+                ("fdncmp", ctypes.c_void_p), ("lw_mask", ctypes.c_void_p), ("sw_mask", ctypes.c_void_p)]
+
+
+# Every symbol include/radb200.h declares, with its ctypes signature.
+SIGNATURES = {
+    "rad_version": ([], ctypes.c_int),
+    "rad_config_default": ([ctypes.POINTER(RadConfig), ctypes.c_int32], None),
+    "rad_create": ([ctypes.POINTER(RadConfig), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "rad_load_tables": ([ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+    "rad_solve": ([ctypes.c_void_p, ctypes.POINTER(RadColumns), ctypes.POINTER(RadOutputs), ctypes.c_int64,
+                   ctypes.c_void_p], ctypes.c_int),
+    "rad_workspace_bytes": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int64),
+    "rad_solve_batch": ([ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(RadColumns), ctypes.POINTER(RadOutputs),
+                         ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p], ctypes.c_int),
+    "rad_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
+    "rad_destroy": ([ctypes.c_void_p], None),
+}
+
+_LIB = None
+
+
+class RadError(RuntimeError):
+    """A failing library call: carries the RAD_E_* code."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (code {code})")
+        self.code = code
+
+
+def load(path: Path | None = None):
+    """Load libradb200.so and bind every declared symbol; raises if the library is missing."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is not built: run woof_nam_b200.build.build() (nvcc, sm_100a)")
+    lib = ctypes.CDLL(str(p))
+    for name, (args, res) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def check(lib, handle, rc: int, what: str):
+    if rc != RAD_OK:
+        msg = lib.rad_last_error(handle)
+        raise RadError(rc, f"{what}: {msg.decode() if msg else 'error'}")

@@ -1,0 +1,433 @@
+// rad_capi.cu -- the C ABI of libradb200.so (include/radb200.h): handle, tables, the SW day list and
+// MINVAL(laytrop) groups on the device, and the LW / SW column kernel launches.
+//
+// The reference drives its radiation per row window from the host with one device-to-host read of the
+// day counts per call and ~52k launches (namgpu/physics/rrtm/rrtm_call.py:44-48, :206-235).  Here one
+// rad_solve is a fixed, host-sync-free sequence of launches on the caller's stream: day flags, an
+// exclusive scan (CUB), the day list, per-day-column laytrop and group minima, the LW kernel over all
+// columns and the SW kernel over the day columns (its grid is the column count; CTAs past the device day
+// count exit at once).
+#include <cuda_runtime.h>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#define RAD_WANT_TABLE_NAMES
+#include "../../include/radb200.h"
+#include "rad_tabids.h"
+
+namespace rad {
+__constant__ int c_lw_ns[17] = {0, 10, 22, 38, 52, 68, 76, 88, 96, 108, 114, 122, 130, 134, 136, 138, 140};
+__constant__ int c_sw_ns[15] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94, 100, 112};
+}  // namespace rad
+
+#include "rad_lw.cuh"
+#include "rad_sw.cuh"
+
+using namespace rad;
+
+struct RadHandle {
+    RadConfig cfg{};
+    int device = 0;
+    bool tables_ok = false;
+    float* d_tf = nullptr;
+    double* d_td = nullptr;
+    float *d_lwf = nullptr, *d_swf = nullptr;      // LW LUT (3 x 10001) and SW exp table, float32
+    double *d_lwd = nullptr, *d_swd = nullptr;     // the same in float64
+    int* d_err = nullptr;
+    // day-list scratch
+    int64_t cap = 0;
+    int *d_flag = nullptr, *d_pos = nullptr, *d_daycol = nullptr, *d_lt = nullptr, *d_k8 = nullptr, *d_kw = nullptr;
+    int *d_cmin = nullptr, *d_nday = nullptr;
+    int64_t cmin_cap = 0;
+    void* d_cub = nullptr;
+    size_t cub_bytes = 0;
+    std::string err;
+};
+
+namespace {
+thread_local std::string g_err;
+
+int fail(RadHandle* h, int code, const std::string& msg)
+{
+    if (h) h->err = msg;
+    g_err = msg;
+    return code;
+}
+#define RAD_CUDA(h, call)                                                                                  \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) return fail((h), RAD_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------------- device helpers
+__global__ void k_dayflags(const float* coszen, int64_t n, int* flag)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n) flag[c] = coszen[c] >= 1.0e-4f ? 1 : 0;
+    if (c == n) flag[c] = 0;
+}
+__global__ void k_scatter(const int* flag, const int* pos, int64_t n, int* daycol, int* nday)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n && flag[c]) daycol[pos[c]] = (int)c;
+    if (c == n) *nday = pos[n];
+}
+// SW setcoef laytrop of each day column (setcoef.cu:28-73): the last layer (surface first) with
+// ln(p) > 4.56, nlay when there is none.
+__global__ void k_laytrop(const float* plyr, int64_t n, int nlay, const int* daycol, const int* nday, int* lt,
+                          int* cmin, int64_t ncmin, int wc, int chunk, int maxc, const int* pos)
+{
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= *nday) return;
+    const int64_t c = daycol[d];
+    int l = nlay;
+    for (int k0 = 0; k0 < nlay; ++k0)
+        if (logf(plyr[(size_t)(nlay - 1 - k0) * n + c]) > 4.56f) l = k0 + 1;
+    lt[d] = l;
+    const int w = (int)(c / wc);
+    const int dw0 = pos[(int64_t)w * wc];
+    const int ci = (d - dw0) / chunk;
+    const int64_t key = (int64_t)w * maxc + ci;
+    if (key < ncmin) atomicMin(cmin + key, l);
+}
+__global__ void k_groups(int64_t n, const int* daycol, const int* nday, const int* lt, const int* cmin,
+                         int64_t ncmin, int wc, int chunk, int maxc, const int* pos, int* k8, int* kw)
+{
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= *nday) return;
+    const int64_t c = daycol[d];
+    const int w = (int)(c / wc);
+    const int dw0 = pos[(int64_t)w * wc];
+    const int64_t wend = ((int64_t)w + 1) * wc < n ? ((int64_t)w + 1) * wc : n;
+    const int dw1 = pos[wend];
+    const int ci = (d - dw0) / chunk;
+    const int dc0 = dw0 + ci * chunk;
+    const int dc1 = dc0 + chunk < dw1 ? dc0 + chunk : dw1;
+    const int g0 = dc0 + ((d - dc0) / 8) * 8;
+    const int g1 = g0 + 8 < dc1 ? g0 + 8 : dc1;
+    int m = lt[d];
+    for (int i = g0; i < g1; ++i) m = min(m, lt[i]);
+    k8[d] = m;
+    const int64_t key = (int64_t)w * maxc + ci;
+    kw[d] = key < ncmin ? cmin[key] : lt[d];
+}
+__global__ void k_fill_int(int* p, int64_t n, int v)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// ---------------------------------------------------------------------------------- host tables
+template <class R>
+void lw_lut(std::vector<R>& v)   // [ex | tfn | tau], 3 x 10001 (phys_rrtm_lw_rtrnmr.py:108-131 recipe)
+{
+    const int n = 10000;
+    v.assign(3 * (n + 1), 0);
+    R* ex = v.data();
+    R* tfn = ex + n + 1;
+    R* tau = tfn + n + 1;
+    const R bpade = (R)1.0f / (R)0.278f, expeps = (R)1.0e-20f;
+    const R explimit = (R)std::trunc(-std::log((double)std::numeric_limits<R>::min()));
+    ex[0] = 1; tau[0] = 0; tfn[0] = 0;
+    for (int i = 1; i < n; ++i) {
+        const R tf = (R)i / (R)(n - i);
+        const R ta = bpade * tf;
+        const R e = ta >= explimit ? expeps : (R)std::exp(-(double)ta);
+        tau[i] = ta; ex[i] = e;
+        tfn[i] = ta < (R)0.06f ? ta / (R)6 : (R)1 - (R)2 * (((R)1 / ta) - (e / ((R)1 - e)));
+    }
+    ex[n] = expeps; tau[n] = (R)1.0e10f; tfn[n] = 1;
+}
+template <class R>
+void sw_lut(std::vector<R>& v)   // exp_tbl(0:10000) (phys_rrtm_sw_spcvrtc.py:60-73)
+{
+    const int n = 10000;
+    v.assign(n + 1, 0);
+    v[0] = 1;
+    const double bpade = 1.0 / 0.278;
+    for (int i = 1; i < n; ++i) v[i] = (R)std::exp(-bpade * ((double)i / ((double)n - i)));
+    v[n] = (R)1.0e-20f;
+}
+
+template <class R>
+void* kernel_ptr_lw() { return (void*)lw_column_kernel<R>; }
+template <class R>
+void* kernel_ptr_sw() { return (void*)sw_column_kernel<R>; }
+
+template <class T>
+int upload(RadHandle* h, T** dptr, const std::vector<T>& host)
+{
+    if (*dptr) cudaFree(*dptr);
+    *dptr = nullptr;
+    RAD_CUDA(h, cudaMalloc((void**)dptr, host.size() * sizeof(T)));
+    RAD_CUDA(h, cudaMemcpy(*dptr, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return RAD_OK;
+}
+
+int ensure_scratch(RadHandle* h, int64_t n)
+{
+    if (n + 1 > h->cap) {
+        const int64_t cap = n + 1 + (n >> 3);
+        for (int** p : {&h->d_flag, &h->d_pos, &h->d_daycol, &h->d_lt, &h->d_k8, &h->d_kw})
+            if (*p) cudaFree(*p);
+        for (int** p : {&h->d_flag, &h->d_pos, &h->d_daycol, &h->d_lt, &h->d_k8, &h->d_kw})
+            RAD_CUDA(h, cudaMalloc((void**)p, (size_t)cap * sizeof(int)));
+        size_t need = 0;
+        RAD_CUDA(h, cub::DeviceScan::ExclusiveSum(nullptr, need, h->d_flag, h->d_pos, (int)cap));
+        if (need > h->cub_bytes) {
+            if (h->d_cub) cudaFree(h->d_cub);
+            RAD_CUDA(h, cudaMalloc(&h->d_cub, need));
+            h->cub_bytes = need;
+        }
+        h->cap = cap;
+    }
+    return RAD_OK;
+}
+
+template <class R>
+int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t n, cudaStream_t st)
+{
+    const RadConfig& cfg = h->cfg;
+    const int nlay = cfg.nlay;
+    // ---- LW over every column
+    {
+        LwIn a{in->plyr, in->plvl, in->tlyr, in->tlvl, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faerlw,
+               in->sfcemis, in->tsfg, out->htlw, out->topflw, out->sfcflw, n, 0, nlay, cfg.diagnostic, cfg.cpathfac};
+        LwLut<R> lut;
+        const R* base = sizeof(R) == 4 ? (const R*)h->d_lwf : (const R*)h->d_lwd;
+        lut.ex = base; lut.tfn = base + 10001; lut.tau = base + 2 * 10001;
+        const size_t smem = sizeof(LwShared<R>);
+        RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_lw<R>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int64_t maxg = 1 << 30;
+        for (int64_t c0 = 0; c0 < n; c0 += maxg) {
+            a.col0 = c0;
+            const int64_t nb = std::min<int64_t>(maxg, n - c0);
+            lw_column_kernel<R><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
+        }
+        RAD_CUDA(h, cudaGetLastError());
+    }
+    // ---- SW day list, laytrop, groups
+    int rc = ensure_scratch(h, n);
+    if (rc) return rc;
+    const int wc = cfg.window_cols > 0 ? (int)std::min<int64_t>(cfg.window_cols, n) : (int)n;
+    const int chunk = cfg.sw_chunk > 0 ? cfg.sw_chunk : 32768;
+    const int64_t nwin = (n + wc - 1) / wc;
+    const int maxc = (wc + chunk - 1) / chunk;
+    const int64_t ncmin = nwin * maxc;
+    if (ncmin > h->cmin_cap) {
+        if (h->d_cmin) cudaFree(h->d_cmin);
+        RAD_CUDA(h, cudaMalloc((void**)&h->d_cmin, (size_t)ncmin * sizeof(int)));
+        h->cmin_cap = ncmin;
+    }
+    const int T = 256;
+    const unsigned gb = (unsigned)((n + 1 + T - 1) / T);
+    k_dayflags<<<gb, T, 0, st>>>(in->coszen, n, h->d_flag);
+    size_t tb = h->cub_bytes;
+    RAD_CUDA(h, cub::DeviceScan::ExclusiveSum(h->d_cub, tb, h->d_flag, h->d_pos, (int)(n + 1), st));
+    k_scatter<<<gb, T, 0, st>>>(h->d_flag, h->d_pos, n, h->d_daycol, h->d_nday);
+    k_fill_int<<<(unsigned)((ncmin + T - 1) / T), T, 0, st>>>(h->d_cmin, ncmin, std::numeric_limits<int>::max());
+    k_laytrop<<<gb, T, 0, st>>>(in->plyr, n, nlay, h->d_daycol, h->d_nday, h->d_lt, h->d_cmin, ncmin, wc, chunk,
+                                maxc, h->d_pos);
+    k_groups<<<gb, T, 0, st>>>(n, h->d_daycol, h->d_nday, h->d_lt, h->d_cmin, ncmin, wc, chunk, maxc, h->d_pos,
+                               h->d_k8, h->d_kw);
+    RAD_CUDA(h, cudaGetLastError());
+    // ---- SW over the day columns; write zeros first (night columns keep them, as swrad does)
+    RAD_CUDA(h, cudaMemsetAsync(out->htsw, 0, (size_t)nlay * n * sizeof(float), st));
+    RAD_CUDA(h, cudaMemsetAsync(out->topfsw, 0, (size_t)3 * n * sizeof(float), st));
+    RAD_CUDA(h, cudaMemsetAsync(out->sfcfsw, 0, (size_t)4 * n * sizeof(float), st));
+    if (out->fdncmp) RAD_CUDA(h, cudaMemsetAsync(out->fdncmp, 0, (size_t)6 * n * sizeof(float), st));
+    {
+        SwIn a{in->plyr, in->plvl, in->tlyr, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faersw, in->sfcalb,
+               in->coszen, h->d_daycol, h->d_nday, h->d_k8, h->d_kw, out->htsw, out->topfsw, out->sfcfsw,
+               out->fdncmp, n, nlay, cfg.diagnostic, cfg.iswmode, in->solcon};
+        SwLut<R> lut;
+        lut.ex = sizeof(R) == 4 ? (const R*)h->d_swf : (const R*)h->d_swd;
+        const size_t smem = sizeof(SwShared<R>);
+        RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_sw<R>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        sw_column_kernel<R><<<(unsigned)n, SW_THREADS, smem, st>>>(a, lut, h->d_swd, h->d_err);
+        RAD_CUDA(h, cudaGetLastError());
+    }
+    return RAD_OK;
+}
+}  // namespace
+
+// ============================================================================================== C ABI
+extern "C" {
+
+int rad_version(void) { return RAD_ABI_VERSION; }
+
+void rad_config_default(RadConfig* cfg, int32_t nlay)
+{
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->nlay = nlay;
+    cfg->precision = RAD_PREC_MIXED;
+    cfg->route = RAD_ROUTE_NAM;
+    cfg->iswmode = 2;
+    cfg->diagnostic = 0;
+    cfg->window_cols = 0;
+    cfg->sw_chunk = 32768;
+    cfg->iovrlw = 1;
+    cfg->iovrsw = 1;
+    cfg->lw_seed0 = 140;
+    cfg->sw_seed0 = 1;
+    cfg->cpathfac = 1.5f;
+}
+
+int rad_create(const RadConfig* cfg, RadHandle** out)
+{
+    if (!cfg || !out) return fail(nullptr, RAD_E_INVALID, "rad_create: null argument");
+    if (cfg->nlay < 2 || cfg->nlay > NLAY_MAX)
+        return fail(nullptr, RAD_E_INVALID, "rad_create: nlay must be in [2, " + std::to_string(NLAY_MAX) + "]");
+    if (cfg->iswmode < 1 || cfg->iswmode > 3) return fail(nullptr, RAD_E_INVALID, "rad_create: iswmode must be 1, 2 or 3");
+    if (cfg->precision != RAD_PREC_FP64 && cfg->precision != RAD_PREC_MIXED)
+        return fail(nullptr, RAD_E_INVALID, "rad_create: precision must be RAD_PREC_FP64 or RAD_PREC_MIXED");
+    if (cfg->route != RAD_ROUTE_NAM && cfg->route != RAD_ROUTE_MCICA)
+        return fail(nullptr, RAD_E_INVALID, "rad_create: unknown route");
+    if (cfg->route == RAD_ROUTE_MCICA) return fail(nullptr, RAD_E_INVALID, "rad_create: the McICA route is not built in this library version");
+    RadHandle* h = new RadHandle();
+    h->cfg = *cfg;
+    cudaGetDevice(&h->device);
+    if (cudaMalloc((void**)&h->d_err, sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void**)&h->d_nday, sizeof(int)) != cudaSuccess) {
+        delete h;
+        return fail(nullptr, RAD_E_NOMEM, "rad_create: device allocation failed");
+    }
+    cudaMemset(h->d_err, 0, sizeof(int));
+    *out = h;
+    return RAD_OK;
+}
+
+// Blob: "RADTBL01", uint32 count, then per table: uint16 name length, name, uint8 dtype (0 f32, 1 f64,
+// 2 i32), uint64 element count, data.
+int rad_load_tables(RadHandle* h, const void* blob, size_t nbytes)
+{
+    if (!h || !blob) return fail(h, RAD_E_INVALID, "rad_load_tables: null argument");
+    const unsigned char* p = (const unsigned char*)blob;
+    const unsigned char* end = p + nbytes;
+    if (nbytes < 12 || std::memcmp(p, "RADTBL01", 8) != 0) return fail(h, RAD_E_TABLES, "rad_load_tables: bad magic");
+    uint32_t count;
+    std::memcpy(&count, p + 8, 4);
+    p += 12;
+    std::vector<std::vector<double>> vals(T_COUNT);
+    std::vector<bool> seen(T_COUNT, false);
+    std::vector<double> chi64;
+    for (uint32_t e = 0; e < count; ++e) {
+        if (p + 2 > end) return fail(h, RAD_E_TABLES, "rad_load_tables: truncated blob");
+        uint16_t ln;
+        std::memcpy(&ln, p, 2);
+        p += 2;
+        if (p + ln + 9 > end) return fail(h, RAD_E_TABLES, "rad_load_tables: truncated blob");
+        std::string name((const char*)p, ln);
+        p += ln;
+        const uint8_t dt = *p++;
+        uint64_t cnt;
+        std::memcpy(&cnt, p, 8);
+        p += 8;
+        const size_t es = dt == 1 ? 8 : 4;
+        if (p + cnt * es > end) return fail(h, RAD_E_TABLES, "rad_load_tables: truncated data of " + name);
+        std::vector<double> v(cnt);
+        for (uint64_t i = 0; i < cnt; ++i) {
+            if (dt == 0) { float f; std::memcpy(&f, p + 4 * i, 4); v[i] = f; }
+            else if (dt == 1) { double x; std::memcpy(&x, p + 8 * i, 8); v[i] = x; }
+            else { int32_t x; std::memcpy(&x, p + 4 * i, 4); v[i] = x; }
+        }
+        p += cnt * es;
+        if (name == "lw05_chi_mls_f64") { chi64 = v; continue; }
+        for (int t = 0; t < T_COUNT; ++t)
+            if (name == RAD_TABLE_NAMES[t]) { vals[t] = std::move(v); seen[t] = true; break; }
+    }
+    for (int t = 0; t < T_COUNT; ++t)
+        if (!seen[t]) return fail(h, RAD_E_TABLES, std::string("rad_load_tables: missing table ") + RAD_TABLE_NAMES[t]);
+    if (chi64.size() != 59 * 7) return fail(h, RAD_E_TABLES, "rad_load_tables: missing lw05_chi_mls_f64");
+    std::vector<int64_t> off(T_COUNT);
+    int64_t tot = 0;
+    for (int t = 0; t < T_COUNT; ++t) { off[t] = tot; tot += (int64_t)vals[t].size(); }
+    std::vector<float> hf(tot);
+    std::vector<double> hd(tot);
+    for (int t = 0; t < T_COUNT; ++t)
+        for (size_t i = 0; i < vals[t].size(); ++i) {
+            hf[off[t] + i] = (float)vals[t][i];
+            hd[off[t] + i] = (double)(float)vals[t][i];   // the float32 table values, exactly
+        }
+    // host-side reference ratios (phys_rrtm_lw_taugb04.py:87-99, taugb05.py:81-85, taugb15.py:135-136)
+    const std::vector<double>& chi = vals[T_LW_CHI_MLS];   // [59][7]
+    LwHostConsts k;
+    k.b4_rpa = (float)chi[10 * 7 + 0] / (float)chi[10 * 7 + 1];
+    k.b4_rpb = (float)chi[12 * 7 + 2] / (float)chi[12 * 7 + 1];
+    k.b5_rpa = (float)(chi64[4 * 7 + 0] / chi64[4 * 7 + 1]);
+    k.b5_rpb = (float)(chi64[42 * 7 + 2] / chi64[42 * 7 + 1]);
+    k.b5_rma = (float)(chi64[6 * 7 + 0] / chi64[6 * 7 + 1]);
+    k.b15_r = (float)chi[0 * 7 + 3] / (float)chi[0 * 7 + 1];
+    std::vector<float> lwf, swf;
+    std::vector<double> lwd, swd;
+    lw_lut(lwf); lw_lut(lwd); sw_lut(swf); sw_lut(swd);
+    int rc;
+    if ((rc = upload(h, &h->d_tf, hf)) || (rc = upload(h, &h->d_td, hd)) || (rc = upload(h, &h->d_lwf, lwf)) ||
+        (rc = upload(h, &h->d_lwd, lwd)) || (rc = upload(h, &h->d_swf, swf)) || (rc = upload(h, &h->d_swd, swd)))
+        return rc;
+    RAD_CUDA(h, cudaMemcpyToSymbol(c_toff, off.data(), T_COUNT * sizeof(int64_t)));
+    RAD_CUDA(h, cudaMemcpyToSymbol(c_tf, &h->d_tf, sizeof(float*)));
+    RAD_CUDA(h, cudaMemcpyToSymbol(c_td, &h->d_td, sizeof(double*)));
+    RAD_CUDA(h, cudaMemcpyToSymbol(c_lwk, &k, sizeof(k)));
+    h->tables_ok = true;
+    return RAD_OK;
+}
+
+int64_t rad_workspace_bytes(const RadHandle* h, int64_t ncol)
+{
+    (void)h;
+    return (ncol + 1) * 6 * (int64_t)sizeof(int) + (1 << 20);
+}
+
+int rad_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream)
+{
+    if (!h || !in || !out) return fail(h, RAD_E_INVALID, "rad_solve: null argument");
+    if (!h->tables_ok) return fail(h, RAD_E_TABLES, "rad_solve: tables not loaded (rad_load_tables)");
+    if (ncol <= 0 || ncol > (int64_t)std::numeric_limits<int>::max() - 1)
+        return fail(h, RAD_E_INVALID, "rad_solve: ncol out of range");
+    if (!in->plyr || !in->plvl || !in->tlyr || !in->tlvl || !in->qlyr || !in->olyr || !in->gasvmr || !in->clouds ||
+        !in->sfcemis || !in->tsfg || !in->sfcalb || !in->coszen)
+        return fail(h, RAD_E_INVALID, "rad_solve: a required input pointer is null");
+    if (!out->htlw || !out->htsw || !out->topflw || !out->sfcflw || !out->topfsw || !out->sfcfsw)
+        return fail(h, RAD_E_INVALID, "rad_solve: a required output pointer is null");
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != h->device) return fail(h, RAD_E_INVALID, "rad_solve: handle belongs to another device");
+    cudaStream_t st = (cudaStream_t)stream;
+    return h->cfg.precision == RAD_PREC_FP64 ? launch_solve<double>(h, in, out, ncol, st)
+                                             : launch_solve<float>(h, in, out, ncol, st);
+}
+
+int rad_solve_batch(RadHandle* h, int32_t nreq, const RadColumns* ins, const RadOutputs* outs, const int64_t* ncols,
+                    void* stream)
+{
+    if (!h || nreq < 0 || (nreq > 0 && (!ins || !outs || !ncols))) return fail(h, RAD_E_INVALID, "rad_solve_batch: bad arguments");
+    for (int32_t r = 0; r < nreq; ++r) {
+        const int rc = rad_solve(h, ins + r, outs + r, ncols[r], stream);
+        if (rc) return rc;
+    }
+    return RAD_OK;
+}
+
+const char* rad_last_error(const RadHandle* h) { return h ? h->err.c_str() : g_err.c_str(); }
+
+void rad_destroy(RadHandle* h)
+{
+    if (!h) return;
+    for (void* p : {(void*)h->d_tf, (void*)h->d_td, (void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
+                    (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
+                    (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub})
+        if (p) cudaFree(p);
+    delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,67 @@
+// rad_common.cuh -- device-side pieces shared by the LW and SW column kernels.
+//
+// Tables: every packed RRTM table lives in one float32 and one float64 device buffer; the offset of each
+// table (by RadTableId) is published in constant memory, so a kernel instantiated for float reads the
+// float32 copy and one instantiated for double reads the float64 copy, with the same index arithmetic.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "rad_tabids.h"
+
+namespace rad {
+
+constexpr int NLAY_MAX = 64;        // per-thread sweep arrays are sized for this many layers
+constexpr int LW_NGPT = 140, SW_NGPT = 112;
+
+__constant__ int64_t c_toff[T_COUNT];
+__constant__ const float* c_tf;
+__constant__ const double* c_td;
+
+// Scalars the reference's wrappers compute on the host (band 4, 5 and 15 reference ratios), float32.
+struct LwHostConsts {
+    float b4_rpa, b4_rpb, b5_rpa, b5_rpb, b5_rma, b15_r;
+};
+__constant__ LwHostConsts c_lwk;
+
+template <class R> __device__ __forceinline__ const R* tab(int id);
+template <> __device__ __forceinline__ const float* tab<float>(int id) { return c_tf + c_toff[id]; }
+template <> __device__ __forceinline__ const double* tab<double>(int id) { return c_td + c_toff[id]; }
+
+template <class R> __device__ __forceinline__ R ldt(const R* p) { return __ldg(p); }
+
+// IEEE minNum/maxNum as CUDA's fminf/fmaxf: a NaN operand yields the other one.
+__device__ __forceinline__ float fminR(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ float fmaxR(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double fminR(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ double fmaxR(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float rlog(float x) { return logf(x); }
+__device__ __forceinline__ double rlog(double x) { return log(x); }
+__device__ __forceinline__ float rexp(float x) { return expf(x); }
+__device__ __forceinline__ double rexp(double x) { return exp(x); }
+__device__ __forceinline__ float rpow(float x, float y) { return powf(x, y); }
+__device__ __forceinline__ double rpow(double x, double y) { return pow(x, y); }
+__device__ __forceinline__ float sqrtR(float x) { return sqrtf(x); }
+__device__ __forceinline__ double sqrtR(double x) { return sqrt(x); }
+__device__ __forceinline__ float rfmod1(float x) { return fmodf(x, 1.0f); }
+__device__ __forceinline__ double rfmod1(double x) { return fmod(x, 1.0); }
+
+// t(ig, ind) + frac * (t(ig, ind+1) - t(ig, ind)) for a [ind][g] table, 1-based ind.
+template <class R>
+__device__ __forceinline__ R interp(const R* t, int ng, int ind, int ig, R frac)
+{
+    const R a = ldt(t + (size_t)(ind - 1) * ng + ig), b = ldt(t + (size_t)ind * ng + ig);
+    return a + frac * (b - a);
+}
+
+// Warp sum of a double, lanes 0..31 (result valid in lane 0); a fixed tree, so bit-reproducible.
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Error word written by kernels on bad input (host reads it after a synchronising call).
+enum : int { RAD_DEV_OK = 0, RAD_DEV_NLAY = 1, RAD_DEV_INDEX = 2 };
+
+}  // namespace rad

@@ -1,0 +1,954 @@
+// rad_lw.cuh -- RRTM longwave column kernel for sm_100a: one CTA per column, fused prep, setcoef, gas
+// optics (16 bands, 140 g-points) and max-random-overlap transfer (rtrnmr).
+//
+// Reference path: namgpu/kernels/phys_rrtm_lw_lwrad.cu:98-366 (prep/post), phys_rrtm_lw_cldprop.cu:79-243,
+// phys_rrtm_lw_setcoef.cu:82-244, phys_rrtm_lw_taugb01..16.cu, phys_rrtm_lw_rtrnmr_body.cuh:9-365, driven
+// as namgpu/physics/rrtm/lw_core.py:217-286 does.  The reference runs ~20 launches per chunk with the
+// 140 x nlay taug/fracs pair round-tripping HBM; here one CTA holds a column on chip:
+//   phase A  threads = layers: absorber amounts, cloud optics, setcoef, Planck functions (shared memory)
+//   phase B  threads = (g, layer) pairs in g-major order (warps stay inside one band): tautot, fracs
+//   phase C  lanes = g-points: the down/up sweeps of rtrnmr; per-level fluxes summed across the g-points
+//            of a warp by shuffles, then across warps in a fixed order -> deterministic, in float64.
+// R = double is the plain FP64 kernel; R = float is the mixed kernel (float optics and sweeps, float64 flux
+// sums and heating-rate differences).
+#pragma once
+#include "rad_common.cuh"
+
+namespace rad {
+
+constexpr int LW_THREADS = 160;     // 5 warps: lanes 0..139 carry g-points in the sweeps
+constexpr int LW_WARPS = LW_THREADS / 32;
+
+template <class R>
+struct LwShared {
+    R pavel[NLAY_MAX], tavel[NLAY_MAX], coldry[NLAY_MAX], colbrd[NLAY_MAX], h2ovmr[NLAY_MAX], delp[NLAY_MAX];
+    R fac00[NLAY_MAX], fac01[NLAY_MAX], fac10[NLAY_MAX], fac11[NLAY_MAX], selffac[NLAY_MAX], selffrac[NLAY_MAX];
+    R forfac[NLAY_MAX], forfrac[NLAY_MAX], minorfrac[NLAY_MAX], scaleminor[NLAY_MAX], scaleminorn2[NLAY_MAX];
+    R colamt[7][NLAY_MAX], wx[4][NLAY_MAX], rfrate[2][6][NLAY_MAX];
+    int jp[NLAY_MAX], jt[NLAY_MAX], jt1[NLAY_MAX], indself[NLAY_MAX], indfor[NLAY_MAX], indminor[NLAY_MAX];
+    int lower[NLAY_MAX];
+    R tz[NLAY_MAX + 1];
+    R pklay[NLAY_MAX + 1][16], pklev[NLAY_MAX + 1][16];
+    R taucld[16][NLAY_MAX], tauaer[16][NLAY_MAX];
+    R cldfrc[NLAY_MAX + 2];
+    R taug[LW_NGPT][NLAY_MAX], fracs[LW_NGPT][NLAY_MAX];
+    R facclr1u[NLAY_MAX + 2], facclr2u[NLAY_MAX + 2], faccld1u[NLAY_MAX + 2], faccld2u[NLAY_MAX + 2];
+    R faccmb1u[NLAY_MAX + 2], faccmb2u[NLAY_MAX + 2];
+    R facclr1d[NLAY_MAX + 2], facclr2d[NLAY_MAX + 2], faccld1d[NLAY_MAX + 2], faccld2d[NLAY_MAX + 2];
+    R faccmb1d[NLAY_MAX + 2], faccmb2d[NLAY_MAX + 2];
+    int lstu[NLAY_MAX + 2], lstd[NLAY_MAX + 2];
+    double fnet[LW_WARPS][NLAY_MAX + 1];      // per-warp partial of sum_g (up - down) per level
+    double scal[LW_WARPS][8];                 // per-warp partials: toa up, toa up clr, sfc up/dn, clr up/dn
+    R secdiff[16], semiss[16];
+    R stemp, pwvcm;
+    int laytrop, lcf1;
+};
+
+// ------------------------------------------------------------------------------------------------------
+// Binary-species key of a band at one layer: specparm/js/fs (phys_rrtm_lw_taugb03.cu:123-128 pattern).
+template <class R>
+__device__ __forceinline__ void spec(R c1, R rat, R c2, R mult, R& sc, R& sp, int& js, R& fs)
+{
+    const R oneminus = (R)1.0f - (R)1.0e-6f;
+    sc = c1 + rat * c2;
+    sp = c1 / sc;
+    const R sm = mult * fminR(sp, oneminus);
+    js = 1 + (int)sm;
+    fs = rfmod1(sm);
+}
+
+template <class R>
+struct Sel {
+    R fk0, fk1, fk2;
+    int id[6];
+};
+template <class R>
+__device__ __forceinline__ Sel<R> sel_branch(int br, R fs, int ind)
+{
+    Sel<R> s;
+    if (br == 0) {
+        const R p = fs - (R)1, p2 = p * p, p4 = p2 * p2;
+        s.fk0 = p4; s.fk1 = (R)1 - p - (R)2 * p4; s.fk2 = p + p4;
+        s.id[0] = ind; s.id[1] = ind + 9; s.id[2] = ind + 1; s.id[3] = ind + 10; s.id[4] = ind + 2; s.id[5] = ind + 11;
+    } else if (br == 1) {
+        const R p = -fs, p2 = p * p, p4 = p2 * p2;
+        s.fk0 = p4; s.fk1 = (R)1 - p - (R)2 * p4; s.fk2 = p + p4;
+        s.id[0] = ind + 1; s.id[1] = ind + 10; s.id[2] = ind; s.id[3] = ind + 9; s.id[4] = ind - 1; s.id[5] = ind + 8;
+    } else {
+        s.fk0 = (R)1 - fs; s.fk1 = fs; s.fk2 = 0;
+        s.id[0] = ind; s.id[1] = ind + 9; s.id[2] = ind + 1; s.id[3] = ind + 10; s.id[4] = ind; s.id[5] = ind;
+    }
+    return s;
+}
+template <class R> __device__ __forceinline__ int br_of(R sp) { return sp < (R)0.125f ? 0 : (sp > (R)0.875f ? 1 : 2); }
+template <class R> __device__ __forceinline__ int br_joint(R a, R b)
+{
+    if (a < (R)0.125f && b < (R)0.125f) return 0;
+    if (a > (R)0.875f && b > (R)0.875f) return 1;
+    return 2;
+}
+template <class R>
+__device__ __forceinline__ R major12(const R* absa, int ng, int ig, R sc, const Sel<R>& s0, R f00, R f10, R sc1,
+                                     const Sel<R>& s1, R f01, R f11)
+{
+    auto A = [&](int id) { return ldt(absa + (size_t)(id - 1) * ng + ig); };
+    const R fac000 = s0.fk0 * f00, fac100 = s0.fk1 * f00, fac200 = s0.fk2 * f00;
+    const R fac010 = s0.fk0 * f10, fac110 = s0.fk1 * f10, fac210 = s0.fk2 * f10;
+    const R fac001 = s1.fk0 * f01, fac101 = s1.fk1 * f01, fac201 = s1.fk2 * f01;
+    const R fac011 = s1.fk0 * f11, fac111 = s1.fk1 * f11, fac211 = s1.fk2 * f11;
+    const R t0 = sc * (fac000 * A(s0.id[0]) + fac010 * A(s0.id[1]) + fac100 * A(s0.id[2]) + fac110 * A(s0.id[3]) +
+                       fac200 * A(s0.id[4]) + fac210 * A(s0.id[5]));
+    const R t1 = sc1 * (fac001 * A(s1.id[0]) + fac011 * A(s1.id[1]) + fac101 * A(s1.id[2]) + fac111 * A(s1.id[3]) +
+                        fac201 * A(s1.id[4]) + fac211 * A(s1.id[5]));
+    return t0 + t1;
+}
+template <class R>
+__device__ __forceinline__ R adjcol(R col, R temp, R thr, R off, R ex)   // the minor-gas column adjustment
+{
+    const R rat = col / temp;
+    return rat > thr ? (off + rpow(rat - off, ex)) * temp : col;
+}
+template <class R>
+__device__ __forceinline__ R minor2d(const R* t, int nj, int ng, int j, R fj, int m, R fm, int ig)  // t[m][j][g]
+{
+    auto K = [&](int jj, int mm) { return ldt(t + ((size_t)(mm - 1) * nj + (jj - 1)) * ng + ig); };
+    const R m1 = K(j, m) + fj * (K(j + 1, m) - K(j, m));
+    const R m2 = K(j, m + 1) + fj * (K(j + 1, m + 1) - K(j, m + 1));
+    return m1 + fm * (m2 - m1);
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Gas optical depth and Planck fraction of LW g-point g (0..139) at layer k0: the band kernels of the
+// reference restated per (g, layer).  Statement order follows each band's reference kernel.
+template <class R>
+__device__ void lw_gas(const LwShared<R>& s, int g, int k0, R& tg, R& fr)
+{
+    const bool low = s.lower[k0];
+    const int jpk = s.jp[k0], jtk = s.jt[k0], jt1k = s.jt1[k0];
+    const R f00 = s.fac00[k0], f01 = s.fac01[k0], f10 = s.fac10[k0], f11 = s.fac11[k0];
+    const int inds = s.indself[k0], indf = s.indfor[k0], indm = s.indminor[k0];
+    const R sfac = s.selffac[k0], sfr = s.selffrac[k0], ffac = s.forfac[k0], ffr = s.forfrac[k0],
+            mf = s.minorfrac[k0];
+    const R* chi = tab<R>(T_LW_CHI_MLS);
+    auto CHI = [&](int gg, int lev) { return ldt(chi + (size_t)(lev - 1) * 7 + (gg - 1)); };
+    auto A4 = [&](const R* t, int ng, int ig, int i0, int i1) {
+        auto a = [&](int id) { return ldt(t + (size_t)(id - 1) * ng + ig); };
+        return f00 * a(i0) + f10 * a(i0 + 1) + f01 * a(i1) + f11 * a(i1 + 1);
+    };
+    const int ind0l = (jpk - 1) * 5 + (jtk - 1) + 1, ind1l = jpk * 5 + (jt1k - 1) + 1;
+    const int ind0u = (jpk - 13) * 5 + (jtk - 1) + 1, ind1u = (jpk - 12) * 5 + (jt1k - 1) + 1;
+    int band = 0;
+    while (g >= c_lw_ns[band + 1]) ++band;
+    const int ig = g - c_lw_ns[band];
+    switch (band + 1) {
+    case 1: {
+        const int NG = 10;
+        const R pp = s.pavel[k0], scalen2 = s.colbrd[k0] * s.scaleminorn2[k0], col = s.colamt[0][k0];
+        const R taufor = ffac * interp(tab<R>(T_LW01_FORREF), NG, indf, ig, ffr);
+        if (low) {
+            const R corradj = pp < (R)250 ? (R)1 - (R)0.15f * ((R)250 - pp) / (R)154.4f : (R)1;
+            const R tauself = sfac * interp(tab<R>(T_LW01_SELFREF), NG, inds, ig, sfr);
+            const R taun2 = scalen2 * interp(tab<R>(T_LW01_KA_MN2), NG, indm, ig, mf);
+            tg = corradj * (col * A4(tab<R>(T_LW01_ABSA), NG, ig, ind0l, ind1l) + tauself + taufor + taun2);
+            fr = ldt(tab<R>(T_LW01_FRACREFA) + ig);
+        } else {
+            const R corradj = (R)1 - (R)0.15f * (pp / (R)95.6f);
+            const R taun2 = scalen2 * interp(tab<R>(T_LW01_KB_MN2), NG, indm, ig, mf);
+            tg = corradj * (col * A4(tab<R>(T_LW01_ABSB), NG, ig, ind0u, ind1u) + taufor + taun2);
+            fr = ldt(tab<R>(T_LW01_FRACREFB) + ig);
+        }
+        break;
+    }
+    case 2: {
+        const int NG = 12;
+        const R col = s.colamt[0][k0];
+        const R taufor = ffac * interp(tab<R>(T_LW02_FORREF), NG, indf, ig, ffr);
+        if (low) {
+            const R corradj = (R)1 - (R)0.05f * (s.pavel[k0] - (R)100) / (R)900;
+            const R tauself = sfac * interp(tab<R>(T_LW02_SELFREF), NG, inds, ig, sfr);
+            tg = corradj * (col * A4(tab<R>(T_LW02_ABSA), NG, ig, ind0l, ind1l) + tauself + taufor);
+            fr = ldt(tab<R>(T_LW02_FRACREFA) + ig);
+        } else {
+            tg = col * A4(tab<R>(T_LW02_ABSB), NG, ig, ind0u, ind1u) + taufor;
+            fr = ldt(tab<R>(T_LW02_FRACREFB) + ig);
+        }
+        break;
+    }
+    case 3:
+    case 4: {
+        const bool b3 = band == 2;
+        const int NG = b3 ? 16 : 14;
+        const R *absa = tab<R>(b3 ? T_LW03_ABSA : T_LW04_ABSA), *absb = tab<R>(b3 ? T_LW03_ABSB : T_LW04_ABSB),
+                *fa = tab<R>(b3 ? T_LW03_FRACREFA : T_LW04_FRACREFA), *fb = tab<R>(b3 ? T_LW03_FRACREFB : T_LW04_FRACREFB);
+        R rpa, rpb, rma = 0, rmb = 0;
+        if (b3) { rpa = CHI(1, 9) / CHI(2, 9); rpb = CHI(1, 13) / CHI(2, 13); rma = CHI(1, 3) / CHI(2, 3); rmb = CHI(1, 13) / CHI(2, 13); }
+        else { rpa = (R)c_lwk.b4_rpa; rpb = (R)c_lwk.b4_rpb; }
+        R adjn2o = 0;
+        if (b3) adjn2o = adjcol(s.colamt[3][k0], s.coldry[k0] * CHI(4, jpk + 1), (R)1.5f, (R)0.5f, (R)0.65f);
+        if (low) {
+            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fmn = 0, fpl;
+            int js, js1, jmn = 1, jpl;
+            const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0];
+            spec(c1, s.rfrate[0][0][k0], c2, (R)8, sc, sp, js, fs);
+            spec(c1, s.rfrate[1][0][k0], c2, (R)8, sc1, sp1, js1, fs1);
+            if (b3) spec(c1, rma, c2, (R)8, scm, spm, jmn, fmn);
+            spec(c1, rpa, c2, (R)8, scp, spp, jpl, fpl);
+            const Sel<R> s0 = sel_branch(br_of(sp), fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
+            const Sel<R> s1 = sel_branch(br_of(sp1), fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
+            const R tauself = sfac * interp(tab<R>(b3 ? T_LW03_SELFREF : T_LW04_SELFREF), NG, inds, ig, sfr);
+            const R taufor = ffac * interp(tab<R>(b3 ? T_LW03_FORREF : T_LW04_FORREF), NG, indf, ig, ffr);
+            const R major = major12(absa, NG, ig, sc, s0, f00, f10, sc1, s1, f01, f11);
+            if (b3) tg = major + tauself + taufor + adjn2o * minor2d(tab<R>(T_LW03_KA_MN2O), 9, NG, jmn, fmn, indm, mf, ig);
+            else tg = major + tauself + taufor;
+            fr = interp(fa, NG, jpl, ig, fpl);
+        } else {
+            const R ka1 = b3 ? s.colamt[0][k0] : s.colamt[2][k0];
+            const R r0 = b3 ? s.rfrate[0][0][k0] : s.rfrate[0][5][k0];
+            const R r1 = b3 ? s.rfrate[1][0][k0] : s.rfrate[1][5][k0];
+            const R c2 = s.colamt[1][k0];
+            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fmn = 0, fpl;
+            int js, js1, jmn = 1, jpl;
+            spec(ka1, r0, c2, (R)4, sc, sp, js, fs);
+            const int ind0 = ((jpk - 13) * 5 + (jtk - 1)) * 5 + js;
+            spec(ka1, r1, c2, (R)4, sc1, sp1, js1, fs1);
+            const int ind1 = ((jpk - 12) * 5 + (jt1k - 1)) * 5 + js1;
+            if (b3) spec(ka1, rmb, c2, (R)4, scm, spm, jmn, fmn);
+            spec(ka1, rpb, c2, (R)4, scp, spp, jpl, fpl);
+            const R fac000 = ((R)1 - fs) * f00, fac010 = ((R)1 - fs) * f10, fac100 = fs * f00, fac110 = fs * f10;
+            const R fac001 = ((R)1 - fs1) * f01, fac011 = ((R)1 - fs1) * f11, fac101 = fs1 * f01, fac111 = fs1 * f11;
+            auto B = [&](int id) { return ldt(absb + (size_t)(id - 1) * NG + ig); };
+            const R t0 = sc * (fac000 * B(ind0) + fac010 * B(ind0 + 5) + fac100 * B(ind0 + 1) + fac110 * B(ind0 + 6));
+            const R t1 = sc1 * (fac001 * B(ind1) + fac011 * B(ind1 + 5) + fac101 * B(ind1 + 1) + fac111 * B(ind1 + 6));
+            if (b3) {
+                const R taufor = ffac * interp(tab<R>(T_LW03_FORREF), NG, indf, ig, ffr);
+                tg = t0 + t1 + taufor + adjn2o * minor2d(tab<R>(T_LW03_KB_MN2O), 5, NG, jmn, fmn, indm, mf, ig);
+            } else {
+                tg = t0 + t1;
+                if (ig >= 7) {
+                    const float adj[7] = {0.92f, 0.88f, 1.07f, 1.1f, 0.99f, 0.88f, 0.943f};
+                    tg = tg * (R)adj[ig - 7];
+                }
+            }
+            fr = interp(fb, NG, jpl, ig, fpl);
+        }
+        break;
+    }
+    case 5: {
+        const int NG = 16;
+        const R wxk = s.wx[0][k0], ccl4 = ldt(tab<R>(T_LW05_CCL4) + ig);
+        if (low) {
+            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fm, fpl;
+            int js, js1, jm, jpl;
+            const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0];
+            spec(c1, s.rfrate[0][0][k0], c2, (R)8, sc, sp, js, fs);
+            spec(c1, s.rfrate[1][0][k0], c2, (R)8, sc1, sp1, js1, fs1);
+            spec(c1, (R)c_lwk.b5_rma, c2, (R)8, scm, spm, jm, fm);
+            spec(c1, (R)c_lwk.b5_rpa, c2, (R)8, scp, spp, jpl, fpl);
+            const int br = br_joint(sp, sp1);
+            const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
+            const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
+            const R tauself = sfac * interp(tab<R>(T_LW05_SELFREF), NG, inds, ig, sfr);
+            const R taufor = ffac * interp(tab<R>(T_LW05_FORREF), NG, indf, ig, ffr);
+            const R abso3 = minor2d(tab<R>(T_LW05_KA_MO3), 9, NG, jm, fm, indm, mf, ig);
+            tg = major12(tab<R>(T_LW05_ABSA), NG, ig, sc, s0, f00, f10, sc1, s1, f01, f11) + tauself + taufor +
+                 abso3 * s.colamt[2][k0] + wxk * ccl4;
+            fr = interp(tab<R>(T_LW05_FRACREFA), NG, jpl, ig, fpl);
+        } else {
+            R sc, sp, sc1, sp1, scp, spp, fs, fs1, fpl;
+            int js, js1, jpl;
+            const R c3 = s.colamt[2][k0], c2 = s.colamt[1][k0];
+            spec(c3, s.rfrate[0][5][k0], c2, (R)4, sc, sp, js, fs);
+            const int ind0 = ((jpk - 13) * 5 + (jtk - 1)) * 5 + js;
+            spec(c3, s.rfrate[1][5][k0], c2, (R)4, sc1, sp1, js1, fs1);
+            const int ind1 = ((jpk - 12) * 5 + (jt1k - 1)) * 5 + js1;
+            spec(c3, (R)c_lwk.b5_rpb, c2, (R)4, scp, spp, jpl, fpl);
+            const R fac000 = ((R)1 - fs) * f00, fac010 = ((R)1 - fs) * f10, fac100 = fs * f00, fac110 = fs * f10;
+            const R fac001 = ((R)1 - fs1) * f01, fac011 = ((R)1 - fs1) * f11, fac101 = fs1 * f01, fac111 = fs1 * f11;
+            const R* absb = tab<R>(T_LW05_ABSB);
+            auto B = [&](int id) { return ldt(absb + (size_t)(id - 1) * NG + ig); };
+            tg = sc * (fac000 * B(ind0) + fac010 * B(ind0 + 5) + fac100 * B(ind0 + 1) + fac110 * B(ind0 + 6)) +
+                 sc1 * (fac001 * B(ind1) + fac011 * B(ind1 + 5) + fac101 * B(ind1 + 1) + fac111 * B(ind1 + 6)) + wxk * ccl4;
+            fr = interp(tab<R>(T_LW05_FRACREFB), NG, jpl, ig, fpl);
+        }
+        break;
+    }
+    case 6: {
+        const int NG = 8;
+        const R wx2 = s.wx[1][k0], wx3 = s.wx[2][k0];
+        const R xsec = wx2 * ldt(tab<R>(T_LW06_CFC11ADJ) + ig) + wx3 * ldt(tab<R>(T_LW06_CFC12) + ig);
+        if (low) {
+            const R adj = adjcol(s.colamt[1][k0], s.coldry[k0] * CHI(2, jpk + 1), (R)3, (R)2, (R)0.77f);
+            const R tauself = sfac * interp(tab<R>(T_LW06_SELFREF), NG, inds, ig, sfr);
+            const R taufor = ffac * interp(tab<R>(T_LW06_FORREF), NG, indf, ig, ffr);
+            const R absco2 = interp(tab<R>(T_LW06_KA_MCO2), NG, indm, ig, mf);
+            tg = s.colamt[0][k0] * A4(tab<R>(T_LW06_ABSA), NG, ig, ind0l, ind1l) + tauself + taufor + adj * absco2 + xsec;
+        } else {
+            tg = xsec;
+        }
+        fr = ldt(tab<R>(T_LW06_FRACREFA) + ig);
+        break;
+    }
+    case 7: {
+        const int NG = 12;
+        const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0], c3 = s.colamt[2][k0];
+        const R temp = s.coldry[k0] * CHI(2, jpk + 1);
+        if (low) {
+            const R rr = CHI(1, 3) / CHI(3, 3);
+            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fm, fpl;
+            int js, js1, jm, jpl;
+            spec(c1, s.rfrate[0][1][k0], c3, (R)8, sc, sp, js, fs);
+            spec(c1, s.rfrate[1][1][k0], c3, (R)8, sc1, sp1, js1, fs1);
+            spec(c1, rr, c3, (R)8, scm, spm, jm, fm);
+            spec(c1, rr, c3, (R)8, scp, spp, jpl, fpl);
+            const R adj = adjcol(c2, temp, (R)3, (R)3, (R)0.79f);
+            const int br = br_joint(sp, sp1);
+            const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
+            const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
+            const R tauself = sfac * interp(tab<R>(T_LW07_SELFREF), NG, inds, ig, sfr);
+            const R taufor = ffac * interp(tab<R>(T_LW07_FORREF), NG, indf, ig, ffr);
+            tg = major12(tab<R>(T_LW07_ABSA), NG, ig, sc, s0, f00, f10, sc1, s1, f01, f11) + tauself + taufor +
+                 adj * minor2d(tab<R>(T_LW07_KA_MCO2), 9, NG, jm, fm, indm, mf, ig);
+            fr = interp(tab<R>(T_LW07_FRACREFA), NG, jpl, ig, fpl);
+        } else {
+            const R adj = adjcol(c2, temp, (R)3, (R)2, (R)0.79f);
+            const R absco2 = interp(tab<R>(T_LW07_KB_MCO2), NG, indm, ig, mf);
+            tg = c3 * A4(tab<R>(T_LW07_ABSB), NG, ig, ind0u, ind1u) + adj * absco2;
+            if (ig >= 5 && ig <= 10) {
+                const float scl[6] = {0.92f, 0.88f, 1.07f, 1.1f, 0.99f, 0.855f};
+                tg = tg * (R)scl[ig - 5];
+            }
+            fr = ldt(tab<R>(T_LW07_FRACREFB) + ig);
+        }
+        break;
+    }
+    case 8: {
+        const int NG = 8;
+        const R adj = adjcol(s.colamt[1][k0], s.coldry[k0] * CHI(2, jpk + 1), (R)3, (R)2, (R)0.65f);
+        const R xsec = s.wx[2][k0] * ldt(tab<R>(T_LW08_CFC12) + ig) + s.wx[3][k0] * ldt(tab<R>(T_LW08_CFC22ADJ) + ig);
+        if (low) {
+            const R tauself = sfac * interp(tab<R>(T_LW08_SELFREF), NG, inds, ig, sfr);
+            const R taufor = ffac * interp(tab<R>(T_LW08_FORREF), NG, indf, ig, ffr);
+            const R absco2 = interp(tab<R>(T_LW08_KA_MCO2), NG, indm, ig, mf);
+            const R abso3 = interp(tab<R>(T_LW08_KA_MO3), NG, indm, ig, mf);
+            const R absn2o = interp(tab<R>(T_LW08_KA_MN2O), NG, indm, ig, mf);
+            tg = s.colamt[0][k0] * A4(tab<R>(T_LW08_ABSA), NG, ig, ind0l, ind1l) + tauself + taufor + adj * absco2 +
+                 s.colamt[2][k0] * abso3 + s.colamt[3][k0] * absn2o + xsec;
+            fr = ldt(tab<R>(T_LW08_FRACREFA) + ig);
+        } else {
+            const R absco2 = interp(tab<R>(T_LW08_KB_MCO2), NG, indm, ig, mf);
+            const R absn2o = interp(tab<R>(T_LW08_KB_MN2O), NG, indm, ig, mf);
+            tg = s.colamt[2][k0] * A4(tab<R>(T_LW08_ABSB), NG, ig, ind0u, ind1u) + adj * absco2 +
+                 s.colamt[3][k0] * absn2o + xsec;
+            fr = ldt(tab<R>(T_LW08_FRACREFB) + ig);
+        }
+        break;
+    }
+    case 9: {
+        const int NG = 12;
+        const R c1 = s.colamt[0][k0], c4 = s.colamt[3][k0], c5 = s.colamt[4][k0];
+        const R adj = adjcol(c4, s.coldry[k0] * CHI(4, jpk + 1), (R)1.5f, (R)0.5f, (R)0.65f);
+        if (low) {
+            const R rpa = CHI(1, 9) / CHI(6, 9), rma = CHI(1, 3) / CHI(6, 3);
+            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fm, fpl;
+            int js, js1, jm, jpl;
+            spec(c1, s.rfrate[0][3][k0], c5, (R)8, sc, sp, js, fs);
+            spec(c1, s.rfrate[1][3][k0], c5, (R)8, sc1, sp1, js1, fs1);
+            spec(c1, rma, c5, (R)8, scm, spm, jm, fm);
+            spec(c1, rpa, c5, (R)8, scp, spp, jpl, fpl);
+            const int br = br_joint(sp, sp1);
+            const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
+            const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
+            const R tauself = sfac * interp(tab<R>(T_LW09_SELFREF), NG, inds, ig, sfr);
+            const R taufor = ffac * interp(tab<R>(T_LW09_FORREF), NG, indf, ig, ffr);
+            tg = major12(tab<R>(T_LW09_ABSA), NG, ig, sc, s0, f00, f10, sc1, s1, f01, f11) + tauself + taufor +
+                 adj * minor2d(tab<R>(T_LW09_KA_MN2O), 9, NG, jm, fm, indm, mf, ig);
+            fr = interp(tab<R>(T_LW09_FRACREFA), NG, jpl, ig, fpl);
+        } else {
+            tg = c5 * A4(tab<R>(T_LW09_ABSB), NG, ig, ind0u, ind1u) + adj * interp(tab<R>(T_LW09_KB_MN2O), NG, indm, ig, mf);
+            fr = ldt(tab<R>(T_LW09_FRACREFB) + ig);
+        }
+        break;
+    }
+    case 10:
+    case 11:
+    case 14: {
+        const int b = band + 1;
+        const int NG = b == 10 ? 6 : (b == 11 ? 8 : 2);
+        const int ia = b == 10 ? T_LW10_ABSA : (b == 11 ? T_LW11_ABSA : T_LW14_ABSA);
+        const int ib_ = b == 10 ? T_LW10_ABSB : (b == 11 ? T_LW11_ABSB : T_LW14_ABSB);
+        const int is = b == 10 ? T_LW10_SELFREF : (b == 11 ? T_LW11_SELFREF : T_LW14_SELFREF);
+        const int iff = b == 10 ? T_LW10_FORREF : (b == 11 ? T_LW11_FORREF : T_LW14_FORREF);
+        const int ifa = b == 10 ? T_LW10_FRACREFA : (b == 11 ? T_LW11_FRACREFA : T_LW14_FRACREFA);
+        const int ifb = b == 10 ? T_LW10_FRACREFB : (b == 11 ? T_LW11_FRACREFB : T_LW14_FRACREFB);
+        const R col = b == 14 ? s.colamt[1][k0] : s.colamt[0][k0];
+        const R scaleo2 = s.colamt[5][k0] * s.scaleminor[k0];
+        if (low) {
+            const R tauself = sfac * interp(tab<R>(is), NG, inds, ig, sfr);
+            const R taufor = ffac * interp(tab<R>(iff), NG, indf, ig, ffr);
+            tg = col * A4(tab<R>(ia), NG, ig, ind0l, ind1l) + tauself + taufor;
+            if (b == 11) tg = tg + scaleo2 * interp(tab<R>(T_LW11_KA_MO2), NG, indm, ig, mf);
+            fr = ldt(tab<R>(ifa) + ig);
+        } else {
+            tg = col * A4(tab<R>(ib_), NG, ig, ind0u, ind1u);
+            if (b != 14) tg = tg + ffac * interp(tab<R>(iff), NG, indf, ig, ffr);
+            if (b == 11) tg = tg + scaleo2 * interp(tab<R>(T_LW11_KB_MO2), NG, indm, ig, mf);
+            fr = ldt(tab<R>(ifb) + ig);
+        }
+        break;
+    }
+    case 12:
+    case 16: {
+        const bool b12 = band == 11;
+        const int NG = b12 ? 8 : 2;
+        if (low) {
+            const R c1 = s.colamt[0][k0], c2 = b12 ? s.colamt[1][k0] : s.colamt[4][k0];
+            const int rate = b12 ? 0 : 3;
+            const R rpa = b12 ? CHI(1, 10) / CHI(2, 10) : CHI(1, 6) / CHI(6, 6);
+            R sc, sp, sc1, sp1, fs, fs1;
+            int js, js1;
+            spec(c1, s.rfrate[0][rate][k0], c2, (R)8, sc, sp, js, fs);
+            spec(c1, s.rfrate[1][rate][k0], c2, (R)8, sc1, sp1, js1, fs1);
+            const R oneminus = (R)1.0f - (R)1.0e-6f;
+            const R scp = c1 + rpa * c2;
+            R spp = c1 / scp;
+            if (spp >= oneminus) spp = oneminus;
+            const R smp = (R)8 * spp;
+            const int jpl = 1 + (int)smp;
+            const R fpl = rfmod1(smp);
+            const int br = br_joint(sp, sp1);
+            const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
+            const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
+            const R tauself = sfac * interp(tab<R>(b12 ? T_LW12_SELFREF : T_LW16_SELFREF), NG, inds, ig, sfr);
+            const R taufor = ffac * interp(tab<R>(b12 ? T_LW12_FORREF : T_LW16_FORREF), NG, indf, ig, ffr);
+            tg = major12(tab<R>(b12 ? T_LW12_ABSA : T_LW16_ABSA), NG, ig, sc, s0, f00, f10, sc1, s1, f01, f11) + tauself + taufor;
+            fr = interp(tab<R>(b12 ? T_LW12_FRACREFA : T_LW16_FRACREFA), NG, jpl, ig, fpl);
+        } else if (b12) {
+            tg = 0;
+            fr = 0;
+        } else {
+            tg = s.colamt[4][k0] * A4(tab<R>(T_LW16_ABSB), NG, ig, 1, 1);   // nspb(16) = 0: row 1 always
+            fr = ldt(tab<R>(T_LW16_FRACREFB) + ig);
+        }
+        break;
+    }
+    case 13: {
+        const int NG = 4;
+        if (low) {
+            const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0], c4 = s.colamt[3][k0], c7 = s.colamt[6][k0];
+            const R rpa = CHI(1, 5) / CHI(4, 5), rma = CHI(1, 1) / CHI(4, 1), rma3 = CHI(1, 3) / CHI(4, 3);
+            R sc, sp, sc1, sp1, scm, spm, scc, spc, scp, spp, fs, fs1, fm, fmc, fpl;
+            int js, js1, jm, jmc, jpl;
+            spec(c1, s.rfrate[0][2][k0], c4, (R)8, sc, sp, js, fs);
+            spec(c1, s.rfrate[1][2][k0], c4, (R)8, sc1, sp1, js1, fs1);
+            spec(c1, rma, c4, (R)8, scm, spm, jm, fm);
+            spec(c1, rma3, c4, (R)8, scc, spc, jmc, fmc);
+            spec(c1, rpa, c4, (R)8, scp, spp, jpl, fpl);
+            const R adj = adjcol(c2, s.coldry[k0] * (R)3.55e-4f, (R)3, (R)2, (R)0.68f);
+            const int br = br_joint(sp, sp1);
+            const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
+            const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
+            const R tauself = sfac * interp(tab<R>(T_LW13_SELFREF), NG, inds, ig, sfr);
+            const R taufor = ffac * interp(tab<R>(T_LW13_FORREF), NG, indf, ig, ffr);
+            tg = major12(tab<R>(T_LW13_ABSA), NG, ig, sc, s0, f00, f10, sc1, s1, f01, f11) + tauself + taufor +
+                 adj * minor2d(tab<R>(T_LW13_KA_MCO2), 9, NG, jm, fm, indm, mf, ig) +
+                 c7 * minor2d(tab<R>(T_LW13_KA_MCO), 9, NG, jmc, fmc, indm, mf, ig);
+            fr = interp(tab<R>(T_LW13_FRACREFA), NG, jpl, ig, fpl);
+        } else {
+            tg = s.colamt[2][k0] * interp(tab<R>(T_LW13_KB_MO3), NG, indm, ig, mf);
+            fr = ldt(tab<R>(T_LW13_FRACREFB) + ig);
+        }
+        break;
+    }
+    case 15: {
+        const int NG = 2;
+        if (low) {
+            const R cn = s.colamt[3][k0], cc = s.colamt[1][k0];
+            const R r = (R)c_lwk.b15_r;
+            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fm, fpl;
+            int js, js1, jm, jpl;
+            spec(cn, s.rfrate[0][4][k0], cc, (R)8, sc, sp, js, fs);
+            spec(cn, s.rfrate[1][4][k0], cc, (R)8, sc1, sp1, js1, fs1);
+            spec(cn, r, cc, (R)8, scm, spm, jm, fm);
+            spec(cn, r, cc, (R)8, scp, spp, jpl, fpl);
+            const R scalen2 = s.colbrd[k0] * s.scaleminor[k0];
+            const int br = br_joint(sp, sp1);
+            const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
+            const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
+            const R tauself = sfac * interp(tab<R>(T_LW15_SELFREF), NG, inds, ig, sfr);
+            const R taufor = ffac * interp(tab<R>(T_LW15_FORREF), NG, indf, ig, ffr);
+            const R taun2 = scalen2 * minor2d(tab<R>(T_LW15_KA_MN2), 9, NG, jm, fm, indm, mf, ig);
+            const R* absa = tab<R>(T_LW15_ABSA);
+            auto A = [&](int id) { return ldt(absa + (size_t)(id - 1) * NG + ig); };
+            const R sumA = s0.fk0 * f00 * A(s0.id[0]) + s0.fk0 * f10 * A(s0.id[1]) + s0.fk1 * f00 * A(s0.id[2]) +
+                           s0.fk1 * f10 * A(s0.id[3]) + s0.fk2 * f00 * A(s0.id[4]) + s0.fk2 * f10 * A(s0.id[5]);
+            const R sumB = s1.fk0 * f01 * A(s1.id[0]) + s1.fk0 * f11 * A(s1.id[1]) + s1.fk1 * f01 * A(s1.id[2]) +
+                           s1.fk1 * f11 * A(s1.id[3]) + s1.fk2 * f01 * A(s1.id[4]) + s1.fk2 * f11 * A(s1.id[5]);
+            tg = sc * sumA + sc1 * sumB + tauself + taufor + taun2;
+            fr = interp(tab<R>(T_LW15_FRACREFA), NG, jpl, ig, fpl);
+        } else {
+            tg = 0;
+            fr = 0;
+        }
+        break;
+    }
+    default:
+        tg = 0;
+        fr = 0;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------
+// rlwinit lookup tables (exp, tfn, tau) are built once per handle on the host (float32 recipe for the
+// mixed kernel, float64 statements for the FP64 kernel) and read through these pointers.
+template <class R>
+struct LwLut {
+    const R *ex, *tfn, *tau;
+};
+
+struct LwIn {
+    const float *plyr, *plvl, *tlyr, *tlvl, *qlyr, *olyr, *gasvmr, *clouds, *faerlw, *sfcemis, *tsfg;
+    float *htlw, *topflw, *sfcflw;
+    int64_t ncol, col0;       // this launch covers columns [col0, col0 + gridDim.x) of an ncol request
+    int nlay, diagnostic;
+    float cpathfac;
+};
+
+// ------------------------------------------------------------------------------------------------------
+template <class R>
+__global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(LwIn a, LwLut<R> lut, int* err)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    LwShared<R>& s = *reinterpret_cast<LwShared<R>*>(smem_raw);
+    const int nlay = a.nlay, nlp1 = nlay + 1;
+    const int64_t col = a.col0 + blockIdx.x;
+    const int64_t N = a.ncol;
+    const int tid = threadIdx.x;
+    if (nlay > NLAY_MAX || col >= N) {
+        if (tid == 0 && nlay > NLAY_MAX) atomicExch(err, RAD_DEV_NLAY);
+        return;
+    }
+    const int ilwcliq = a.diagnostic ? 0 : 1;
+    const R eps = (R)1.0e-6f;
+    auto IN = [&](const float* p, int lev) { return (R)__ldg(p + (size_t)lev * N + col); };
+    // ---- phase A1: lwrad_prep per layer (phys_rrtm_lw_lwrad.cu:142-236), ivflip = 0, internal order
+    if (tid == 0) s.tz[0] = IN(a.tlvl, nlay);
+    for (int k0 = tid; k0 < nlay; k0 += LW_THREADS) {
+        const int kin = nlay - 1 - k0;
+        const R amdw = (R)28.9644 / (R)18.0154, amdo3 = (R)28.9644 / (R)47.9982;
+        const R tem1g = (R)100.0 * (R)9.80665, tem2c = (R)1.0e-20 * (R)1.0e3 * (R)6.0221415e23;
+        const R dlp = IN(a.plvl, nlay - k0) - IN(a.plvl, nlay - k0 - 1);
+        s.tz[k0 + 1] = IN(a.tlvl, nlay - k0 - 1);
+        const R qv = IN(a.qlyr, kin), ov = IN(a.olyr, kin);
+        s.pavel[k0] = IN(a.plyr, kin);
+        s.tavel[k0] = IN(a.tlyr, kin);
+        s.delp[k0] = dlp;
+        const R h2ovmr = fmaxR((R)0, qv * amdw / ((R)1 - qv));
+        const R o3vmr = fmaxR((R)0, ov * amdo3);
+        const R tem0 = ((R)1 - h2ovmr) * (R)28.9644 + h2ovmr * (R)18.0154;
+        const R cdry = tem2c * dlp / (tem1g * tem0 * ((R)1 + h2ovmr));
+        const R temcol = (R)1.0e-12 * cdry;
+        s.coldry[k0] = cdry;
+        auto G = [&](int n) { return (R)__ldg(a.gasvmr + ((size_t)n * nlay + kin) * N + col); };
+        s.colamt[0][k0] = fmaxR((R)0, cdry * h2ovmr);
+        s.colamt[1][k0] = fmaxR(temcol, cdry * G(0));
+        s.colamt[2][k0] = fmaxR(temcol, cdry * o3vmr);
+        s.colamt[3][k0] = fmaxR(temcol, cdry * G(1));
+        s.colamt[4][k0] = fmaxR(temcol, cdry * G(2));
+        s.colamt[5][k0] = fmaxR((R)0, cdry * G(3));
+        s.colamt[6][k0] = fmaxR((R)0, cdry * G(4));
+        s.wx[0][k0] = fmaxR((R)0, cdry * G(8));
+        s.wx[1][k0] = fmaxR((R)0, cdry * G(5));
+        s.wx[2][k0] = fmaxR((R)0, cdry * G(6));
+        s.wx[3][k0] = fmaxR((R)0, cdry * G(7));
+        R summol = 0;
+        for (int m = 1; m < 7; ++m) summol = summol + s.colamt[m][k0];
+        s.colbrd[k0] = cdry - summol;
+        s.h2ovmr[k0] = s.colamt[0][k0] / fmaxR(cdry, (R)1e-30f);
+        for (int b = 0; b < 16; ++b) {
+            R tau = 0, ssa = 0;
+            if (a.faerlw) {
+                tau = (R)__ldg(a.faerlw + (((size_t)b) * nlay + kin) * N + col);
+                ssa = (R)__ldg(a.faerlw + (((size_t)(16 + b)) * nlay + kin) * N + col);
+            }
+            s.tauaer[b][k0] = tau * ((R)1 - ssa);
+        }
+        s.cldfrc[k0 + 1] = IN(a.clouds, kin);
+    }
+    __syncthreads();
+    // ---- column reductions in the reference's order (thread 0): pwvcm, lcf1, laytrop flags
+    if (tid == 0) {
+        s.cldfrc[0] = 1;
+        s.cldfrc[nlay + 1] = 0;
+        R tem1 = 0, tem2 = 0;
+        for (int k0 = 0; k0 < nlay; ++k0) {
+            tem1 = tem1 + s.coldry[k0] + s.colamt[0][k0];
+            tem2 = tem2 + s.colamt[0][k0];
+        }
+        const R amdw = (R)28.9644 / (R)18.0154;
+        s.pwvcm = (R)10.0 * tem2 / (amdw * tem1 * (R)9.80665) * IN(a.plvl, nlay);
+        int lcf = 0;
+        for (int k = 1; k <= nlay; ++k)
+            if (s.cldfrc[k] > eps) { lcf = 1; break; }
+        s.lcf1 = lcf;
+        s.stemp = (R)__ldg(a.tsfg + col);
+        int lt = 0;
+        for (int k0 = 0; k0 < nlay; ++k0) {
+            const bool lo = rlog(s.pavel[k0]) > (R)4.56f;
+            s.lower[k0] = lo;
+            lt += lo ? 1 : 0;
+        }
+        s.laytrop = lt;
+    }
+    __syncthreads();
+    // ---- phase A2: secdiff/semiss, cldprop, setcoef, Planck functions
+    if (tid < 16) {
+        const float A0[16] = {1.66f, 1.55f, 1.58f, 1.66f, 1.54f, 1.454f, 1.89f, 1.33f, 1.668f, 1.66f, 1.66f, 1.66f, 1.66f, 1.66f, 1.66f, 1.66f};
+        const float A1[16] = {0.00f, 0.25f, 0.22f, 0.00f, 0.13f, 0.446f, -0.10f, 0.40f, -0.006f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f};
+        const float A2[16] = {0.00f, -12.0f, -11.7f, 0.00f, -0.72f, -0.243f, 0.19f, -0.062f, 0.414f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f};
+        const int j1 = tid + 1;
+        s.secdiff[tid] = (j1 == 1 || j1 == 4 || j1 == 10)
+                             ? (R)1.66f
+                             : fminR((R)1.80f, fmaxR((R)1.50f, (R)A0[tid] + (R)A1[tid] * rexp((R)A2[tid] * s.pwvcm)));
+        const R sfe = (R)__ldg(a.sfcemis + col);
+        s.semiss[tid] = (sfe > eps && sfe <= (R)1) ? sfe : (R)1;
+    }
+    for (int k0 = tid; k0 < nlay; k0 += LW_THREADS) {
+        // cldprop (phys_rrtm_lw_cldprop.cu:116-232), ilwcice = 1, with the cloud-path factor
+        const int kin = nlay - 1 - k0;
+        auto CL = [&](int n) { return __ldg(a.clouds + ((size_t)n * nlay + kin) * N + col); };
+        R tc[16];
+        for (int b = 0; b < 16; ++b) tc[b] = 0;
+        const R cf = (R)CL(0);
+        if (s.lcf1 && cf > (R)0) {
+            if (ilwcliq > 0) {
+                const R tauran = (R)0.33e-3f * (R)CL(5);
+                const R tausnw = ((R)CL(7) > 0 && (R)CL(8) > (R)10) ? (R)1.5f * (R)1.05756f * (R)CL(7) / (R)CL(8) : (R)0;
+                const R cldliq = (R)(CL(1) * a.cpathfac), cldice = (R)(CL(3) * a.cpathfac), refliq = (R)CL(2);
+                R refice = (R)CL(4);
+                const R* absliq1 = tab<R>(T_LW_ABSLIQ1);
+                const R* absice1 = tab<R>(T_LW_ABSICE1);
+                const R* ipat = tab<R>(T_LW_IPAT);
+                int index = 1;
+                R fint = 0;
+                if (cldliq > 0) {
+                    const R factor = refliq - (R)1.5f;
+                    index = max(1, min(57, (int)factor));
+                    fint = factor - (R)index;
+                }
+                if (cldice > 0) refice = fminR((R)130, fmaxR((R)13, refice));
+                for (int b = 0; b < 16; ++b) {
+                    R tl = 0, ti = 0;
+                    if (cldliq > 0) {
+                        const R a1 = ldt(absliq1 + b * 58 + index - 1), a2 = ldt(absliq1 + b * 58 + index);
+                        tl = fmaxR((R)0, cldliq * (a1 + fint * (a2 - a1)));
+                    }
+                    if (cldice > 0) {
+                        const int ia0 = (int)ldt(ipat + b) - 1;
+                        ti = fmaxR((R)0, cldice * (ldt(absice1 + ia0 * 2) + ldt(absice1 + ia0 * 2 + 1) / refice));
+                    }
+                    tc[b] = ti + tl + tauran + tausnw;
+                }
+            } else {
+                for (int b = 0; b < 16; ++b) tc[b] = (R)CL(1);
+            }
+        }
+        for (int b = 0; b < 16; ++b) s.taucld[b][k0] = tc[b];
+        // setcoef per layer (phys_rrtm_lw_setcoef.cu:131-240)
+        const R pav = s.pavel[k0], tav = s.tavel[k0];
+        const R* preflog = tab<R>(T_LW_PREFLOG);
+        const R* tref = tab<R>(T_LW_TREF);
+        const R* chi = tab<R>(T_LW_CHI_MLS);
+        auto CHI = [&](int g, int lev) { return ldt(chi + (size_t)(lev - 1) * 7 + (g - 1)); };
+        const R plog = rlog(pav);
+        const int jpk = max(1, min(58, (int)((R)36 - (R)5 * (plog + (R)0.04f))));
+        const int jp1 = jpk + 1;
+        const R fp = fmaxR((R)0, fminR((R)1, (R)5 * (ldt(preflog + jpk - 1) - plog)));
+        const R tem1t = (tav - ldt(tref + jpk - 1)) / (R)15;
+        const R tem2t = (tav - ldt(tref + jp1 - 1)) / (R)15;
+        const int jtk = max(1, min(4, (int)((R)3 + tem1t)));
+        const int jt1k = max(1, min(4, (int)((R)3 + tem2t)));
+        const R ft = fmaxR((R)-0.5f, fminR((R)1.5f, tem1t - (R)(jtk - 3)));
+        const R ft1 = fmaxR((R)-0.5f, fminR((R)1.5f, tem2t - (R)(jt1k - 3)));
+        s.jp[k0] = jpk; s.jt[k0] = jtk; s.jt1[k0] = jt1k;
+        const R tem1 = (R)1 - fp;
+        s.fac10[k0] = tem1 * ft;
+        s.fac00[k0] = tem1 * ((R)1 - ft);
+        s.fac11[k0] = fp * ft1;
+        s.fac01[k0] = fp * ((R)1 - ft1);
+        const R h2o = s.h2ovmr[k0];
+        const R forf = pav * ((R)296.0f / (R)1013.0f) / (tav * ((R)1 + h2o));
+        const R selff = h2o * forf;
+        s.scaleminor[k0] = pav / tav;
+        s.scaleminorn2[k0] = (pav / tav) * (s.colbrd[k0] / (s.coldry[k0] + s.colamt[0][k0]));
+        const R tem1m = (tav - (R)180.8f) / (R)7.2f;
+        const int indmin = min(18, max(1, (int)tem1m));
+        s.indminor[k0] = indmin;
+        s.minorfrac[k0] = tem1m - (R)indmin;
+        for (int side = 0; side < 2; ++side)
+            for (int r = 0; r < 6; ++r) s.rfrate[side][r][k0] = 0;
+        if (s.lower[k0]) {
+            const R tem1f = ((R)332 - tav) / (R)36;
+            const int indf = min(2, max(1, (int)tem1f));
+            s.indfor[k0] = indf;
+            s.forfrac[k0] = tem1f - (R)indf;
+            const R tem1s = (tav - (R)188) / (R)7.2f;
+            const int inds = min(9, max(1, (int)tem1s - 7));
+            s.indself[k0] = inds;
+            s.selffrac[k0] = tem1s - (R)(inds + 7);
+            const int gas[5] = {2, 3, 4, 6, 2};
+            for (int r = 0; r < 5; ++r) {
+                const int num = r == 4 ? 4 : 1;
+                s.rfrate[0][r][k0] = CHI(num, jpk) / CHI(gas[r], jpk);
+                s.rfrate[1][r][k0] = CHI(num, jp1) / CHI(gas[r], jp1);
+            }
+        } else {
+            const R tem1f = (tav - (R)188) / (R)36;
+            s.indfor[k0] = 3;
+            s.forfrac[k0] = tem1f - (R)1;
+            s.indself[k0] = 0;
+            s.selffrac[k0] = 0;
+            s.rfrate[0][0][k0] = CHI(1, jpk) / CHI(2, jpk);
+            s.rfrate[1][0][k0] = CHI(1, jp1) / CHI(2, jp1);
+            s.rfrate[0][5][k0] = CHI(3, jpk) / CHI(2, jpk);
+            s.rfrate[1][5][k0] = CHI(3, jp1) / CHI(2, jp1);
+        }
+        s.selffac[k0] = s.colamt[0][k0] * selff;
+        s.forfac[k0] = s.colamt[0][k0] * forf;
+    }
+    // Planck functions at levels 0..nlay and bands (setcoef.cu:135-160)
+    {
+        const R* totplnk = tab<R>(T_LW_TOTPLNK);
+        const R* delwave = tab<R>(T_LW_DELWAVE);
+        for (int p = tid; p < nlp1 * 16; p += LW_THREADS) {
+            const int k = p / 16, i = p % 16;
+            const R tl = k == 0 ? (R)__ldg(a.tsfg + col) : IN(a.tlyr, nlay - k);   // layer temp (k=0: stemp)
+            const R tv = k == 0 ? IN(a.tlvl, nlay) : IN(a.tlvl, nlay - k);
+            auto TOT = [&](int kk) { return ldt(totplnk + (size_t)i * 181 + (kk - 1)); };
+            const int indlay = min(180, max(1, (int)(tl - (R)159)));
+            const int indlev = min(180, max(1, (int)(tv - (R)159)));
+            const R tlyrfr = tl - (R)((int)tl), tlvlfr = tv - (R)((int)tv);
+            const R dw = ldt(delwave + i);
+            s.pklay[k][i] = dw * (TOT(indlay) + tlyrfr * (TOT(indlay + 1) - TOT(indlay)));
+            s.pklev[k][i] = dw * (TOT(indlev) + tlvlfr * (TOT(indlev + 1) - TOT(indlev)));
+        }
+    }
+    __syncthreads();
+    // ---- phase B: gas optics per (g, layer), g-major so a warp stays inside one band
+    for (int p = tid; p < LW_NGPT * nlay; p += LW_THREADS) {
+        const int g = p / nlay, k0 = p - g * nlay;
+        R tg, fr;
+        lw_gas(s, g, k0, tg, fr);
+        int band = 0;
+        while (g >= c_lw_ns[band + 1]) ++band;
+        s.taug[g][k0] = tg + s.tauaer[band][k0];
+        s.fracs[g][k0] = fr;
+    }
+    // ---- overlap factors of rtrnmr (serial recurrence in k), thread 32 while warp 0 waits
+    if (tid == 32) {
+        const R* cf = s.cldfrc;
+        for (int k = 0; k <= nlp1; ++k) {
+            s.faccld1u[k] = 0; s.faccld2u[k] = 0; s.facclr1u[k] = 0; s.facclr2u[k] = 0; s.faccmb1u[k] = 0; s.faccmb2u[k] = 0;
+            s.faccld1d[k] = 0; s.faccld2d[k] = 0; s.facclr1d[k] = 0; s.facclr2d[k] = 0; s.faccmb1d[k] = 0; s.faccmb2d[k] = 0;
+            s.lstu[k] = 0; s.lstd[k] = 0;
+        }
+        s.lstu[1] = cf[1] > eps ? 1 : 0;
+        R rat1 = 0, rat2 = 0;
+        for (int k = 1; k <= nlay - 1; ++k) {
+            s.lstu[k + 1] = (cf[k + 1] > eps && cf[k] <= eps) ? 1 : 0;
+            if (cf[k] > eps) {
+                if (cf[k + 1] >= cf[k]) {
+                    if (s.lstu[k]) {
+                        if (cf[k] < (R)1) s.facclr2u[k + 1] = (cf[k + 1] - cf[k]) / ((R)1 - cf[k]);
+                        s.facclr2u[k] = 0; s.faccld2u[k] = 0;
+                    } else {
+                        const R fmx = fmaxR(cf[k], cf[k - 1]);
+                        if (cf[k + 1] > fmx) { s.facclr1u[k + 1] = rat2; s.facclr2u[k + 1] = (cf[k + 1] - fmx) / ((R)1 - fmx); }
+                        else if (cf[k + 1] < fmx) s.facclr1u[k + 1] = (cf[k + 1] - cf[k]) / (cf[k - 1] - cf[k]);
+                        else s.facclr1u[k + 1] = rat2;
+                    }
+                    if (s.facclr1u[k + 1] > 0 || s.facclr2u[k + 1] > 0) { rat1 = 1; rat2 = 0; } else { rat1 = 0; rat2 = 0; }
+                } else {
+                    if (s.lstu[k]) {
+                        s.faccld2u[k + 1] = (cf[k] - cf[k + 1]) / cf[k];
+                        s.facclr2u[k] = 0; s.faccld2u[k] = 0;
+                    } else {
+                        const R fmn = fminR(cf[k], cf[k - 1]);
+                        if (cf[k + 1] <= fmn) { s.faccld1u[k + 1] = rat1; s.faccld2u[k + 1] = (fmn - cf[k + 1]) / fmn; }
+                        else s.faccld1u[k + 1] = (cf[k] - cf[k + 1]) / (cf[k] - fmn);
+                    }
+                    if (s.faccld1u[k + 1] > 0 || s.faccld2u[k + 1] > 0) { rat1 = 0; rat2 = 1; } else { rat1 = 0; rat2 = 0; }
+                }
+                s.faccmb1u[k + 1] = s.facclr1u[k + 1] * s.faccld2u[k] * cf[k - 1];
+                s.faccmb2u[k + 1] = s.faccld1u[k + 1] * s.facclr2u[k] * ((R)1 - cf[k - 1]);
+            }
+        }
+        s.lstd[nlay] = cf[nlay] > eps ? 1 : 0;
+        rat1 = 0; rat2 = 0;
+        for (int k = nlay; k >= 2; --k) {
+            s.lstd[k - 1] = (cf[k - 1] > eps && cf[k] <= eps) ? 1 : 0;
+            if (cf[k] > eps) {
+                if (cf[k - 1] >= cf[k]) {
+                    if (s.lstd[k]) {
+                        if (cf[k] < (R)1) s.facclr2d[k - 1] = (cf[k - 1] - cf[k]) / ((R)1 - cf[k]);
+                        s.facclr2d[k] = 0; s.faccld2d[k] = 0;
+                    } else {
+                        const R fmx = fmaxR(cf[k], cf[k + 1]);
+                        if (cf[k - 1] > fmx) { s.facclr1d[k - 1] = rat2; s.facclr2d[k - 1] = (cf[k - 1] - fmx) / ((R)1 - fmx); }
+                        else if (cf[k - 1] < fmx) s.facclr1d[k - 1] = (cf[k - 1] - cf[k]) / (cf[k + 1] - cf[k]);
+                        else s.facclr1d[k - 1] = rat2;
+                    }
+                    if (s.facclr1d[k - 1] > 0 || s.facclr2d[k - 1] > 0) { rat1 = 1; rat2 = 0; } else { rat1 = 0; rat2 = 0; }
+                } else {
+                    if (s.lstd[k]) {
+                        s.faccld2d[k - 1] = (cf[k] - cf[k - 1]) / cf[k];
+                        s.facclr2d[k] = 0; s.faccld2d[k] = 0;
+                    } else {
+                        const R fmn = fminR(cf[k], cf[k + 1]);
+                        if (cf[k - 1] <= fmn) { s.faccld1d[k - 1] = rat1; s.faccld2d[k - 1] = (fmn - cf[k - 1]) / fmn; }
+                        else s.faccld1d[k - 1] = (cf[k] - cf[k - 1]) / (cf[k] - fmn);
+                    }
+                    if (s.faccld1d[k - 1] > 0 || s.faccld2d[k - 1] > 0) { rat1 = 0; rat2 = 1; } else { rat1 = 0; rat2 = 0; }
+                }
+                s.faccmb1d[k - 1] = s.facclr1d[k - 1] * s.faccld2d[k] * cf[k + 1];
+                s.faccmb2d[k - 1] = s.faccld1d[k - 1] * s.facclr2d[k] * ((R)1 - cf[k + 1]);
+            }
+        }
+    }
+    __syncthreads();
+    // ---- phase C: rtrnmr sweeps, one g-point per lane
+    const int warp = tid >> 5, lane = tid & 31;
+    const int g = tid;
+    const bool act = g < LW_NGPT;
+    int band = 0;
+    if (act)
+        while (g >= c_lw_ns[band + 1]) ++band;
+    const R bpade = (R)1.0f / (R)0.278f, tblint = (R)10000, rec_6 = (R)0.166667f, c06 = (R)0.06f;
+    R trngas[NLAY_MAX + 1], gassrcu[NLAY_MAX + 1], trntot[NLAY_MAX + 1], totsrcu[NLAY_MAX + 1], dn[NLAY_MAX + 1];
+    R radtotd = 0, radclrd = 0, totradd = 0, clrradd = 0, rad = 0;
+    if (act) {
+        const R sdif = s.secdiff[band];
+        for (int k = nlay; k >= 1; --k) {
+            R odepth = fmaxR((R)0, sdif * s.taug[g][k - 1]);
+            R atrgas, trng, gasfac;
+            if (odepth <= c06) {
+                atrgas = odepth - (R)0.5f * odepth * odepth;
+                trng = (R)1 - atrgas;
+                gasfac = rec_6 * odepth;
+            } else {
+                const R tblind = odepth / (bpade + odepth);
+                const int it = (int)(tblint * tblind + (R)0.5f);
+                trng = ldt(lut.ex + it); atrgas = (R)1 - trng; gasfac = ldt(lut.tfn + it); odepth = ldt(lut.tau + it);
+            }
+            const R plfrac = s.fracs[g][k - 1];
+            const R blay = s.pklay[k][band];
+            const R dplnku = s.pklev[k][band] - blay;
+            const R dplnkd = s.pklev[k - 1][band] - blay;
+            const R gassrcd = plfrac * (blay + dplnkd * gasfac) * atrgas;
+            gassrcu[k] = plfrac * (blay + dplnku * gasfac) * atrgas;
+            trngas[k] = trng;
+            const R clfr = s.cldfrc[k];
+            if (s.lstd[k]) { totradd = clfr * radtotd; clrradd = radtotd - totradd; rad = 0; }
+            if (clfr >= eps) {
+                const R odtot = odepth + sdif * s.taucld[band][k - 1];
+                R totfac, atrtot, trnt;
+                if (odtot < c06) {
+                    totfac = rec_6 * odtot; atrtot = odtot - (R)0.5f * odtot * odtot; trnt = (R)1 - atrtot;
+                } else {
+                    const R tblind = odtot / (bpade + odtot);
+                    const int it = (int)(tblint * tblind + (R)0.5f);
+                    totfac = ldt(lut.tfn + it); trnt = ldt(lut.ex + it); atrtot = (R)1 - trnt;
+                }
+                const R totsrcd = plfrac * (blay + dplnkd * totfac) * atrtot;
+                totsrcu[k] = plfrac * (blay + dplnku * totfac) * atrtot;
+                trntot[k] = trnt;
+                totradd = totradd * trnt + clfr * totsrcd;
+                clrradd = clrradd * trng + ((R)1 - clfr) * gassrcd;
+                radtotd = totradd + clrradd;
+                radclrd = radclrd * trng + gassrcd;
+                const R radmod = rad * (s.facclr1d[k - 1] * trng + s.faccld1d[k - 1] * trnt) -
+                                 s.faccmb1d[k - 1] * gassrcd + s.faccmb2d[k - 1] * totsrcd;
+                rad = -radmod + s.facclr2d[k - 1] * (clrradd + radmod) - s.faccld2d[k - 1] * (totradd - radmod);
+                totradd = totradd + rad;
+                clrradd = clrradd - rad;
+            } else {
+                radtotd = radtotd * trng + gassrcd;
+                radclrd = radclrd * trng + gassrcd;
+            }
+            dn[k - 1] = radtotd;
+        }
+    }
+    // surface: emission and reflection; clear-sky surface values
+    R radtotu = 0, radclru = 0, totradu = 0, clrradu = 0;
+    const R semi = act ? s.semiss[band] : (R)0;
+    if (act) {
+        const R reflct = (R)1 - semi;
+        const R rad0 = semi * s.fracs[g][0] * s.pklay[0][band];
+        radtotu = rad0 + reflct * radtotd;
+        radclru = rad0 + reflct * radclrd;
+    }
+    // scalar partials: sfc up/down total and clear
+    {
+        double v0 = act ? (double)radtotu : 0.0, v1 = act ? (double)radclru : 0.0;
+        double v2 = act ? (double)radtotd : 0.0, v3 = act ? (double)radclrd : 0.0;
+        v0 = warp_sum(v0); v1 = warp_sum(v1); v2 = warp_sum(v2); v3 = warp_sum(v3);
+        if (lane == 0) { s.scal[warp][2] = v0; s.scal[warp][3] = v1; s.scal[warp][4] = v2; s.scal[warp][5] = v3; }
+        double f0 = act ? (double)radtotu - (double)radtotd : 0.0;
+        f0 = warp_sum(f0);
+        if (lane == 0) s.fnet[warp][0] = f0;
+    }
+    for (int k = 1; k <= nlay; ++k) {
+        if (act) {
+            const R clfr = s.cldfrc[k], trng = trngas[k], gasu = gassrcu[k];
+            if (s.lstu[k]) { totradu = clfr * radtotu; clrradu = radtotu - totradu; rad = 0; }
+            if (clfr >= eps) {
+                const R trnt = trntot[k], totu = totsrcu[k];
+                totradu = totradu * trnt + clfr * totu;
+                clrradu = clrradu * trng + ((R)1 - clfr) * gasu;
+                radtotu = totradu + clrradu;
+                radclru = radclru * trng + gasu;
+                const R radmod = rad * (s.facclr1u[k + 1] * trng + s.faccld1u[k + 1] * trnt) -
+                                 s.faccmb1u[k + 1] * gasu + s.faccmb2u[k + 1] * totu;
+                rad = -radmod + s.facclr2u[k + 1] * (clrradu + radmod) - s.faccld2u[k + 1] * (totradu - radmod);
+                totradu = totradu + rad;
+                clrradu = clrradu - rad;
+            } else {
+                radtotu = radtotu * trng + gasu;
+                radclru = radclru * trng + gasu;
+            }
+        }
+        double f = act ? (double)radtotu - (double)(k < nlay ? dn[k] : (R)0) : 0.0;
+        f = warp_sum(f);
+        if (lane == 0) s.fnet[warp][k] = f;
+    }
+    {
+        double v0 = act ? (double)radtotu : 0.0, v1 = act ? (double)radclru : 0.0;
+        v0 = warp_sum(v0); v1 = warp_sum(v1);
+        if (lane == 0) { s.scal[warp][0] = v0; s.scal[warp][1] = v1; }
+    }
+    __syncthreads();
+    // ---- outputs: fluxes x flxfac, heating rates from float64 net-flux differences
+    const double fluxfac = sizeof(R) == 4 ? (double)(float)(2.0 * 3.14159265358979323846 / 2.0 * 2.0) * 0.0 : 0.0;
+    (void)fluxfac;
+    const double pi = 3.14159265358979323846;
+    const double flxfac = 0.5 * (sizeof(R) == 4 ? (double)(float)((double)(float)pi * 2.0e4) : pi * 2.0e4);
+    const double heatfac = sizeof(R) == 4 ? (double)(9.80665f * 1.0e-2f / 1.0046e3f) : 9.80665 * 1.0e-2 / 1.0046e3;
+    for (int k = tid; k < nlay; k += LW_THREADS) {
+        double fk = 0, fk1 = 0;
+        for (int w = 0; w < LW_WARPS; ++w) { fk += s.fnet[w][k]; fk1 += s.fnet[w][k + 1]; }
+        const double h = (fk - fk1) * flxfac * (heatfac / (double)s.delp[k]);
+        a.htlw[(size_t)(nlay - 1 - k) * N + col] = (float)h;
+    }
+    if (tid == 0) {
+        double sc[6] = {0, 0, 0, 0, 0, 0};
+        for (int w = 0; w < LW_WARPS; ++w)
+            for (int i = 0; i < 6; ++i) sc[i] += s.scal[w][i];
+        a.topflw[col] = (float)(sc[0] * flxfac);
+        a.topflw[N + col] = (float)(sc[1] * flxfac);
+        a.sfcflw[col] = (float)(sc[2] * flxfac);
+        a.sfcflw[N + col] = (float)(sc[3] * flxfac);
+        a.sfcflw[2 * N + col] = (float)(sc[4] * flxfac);
+        a.sfcflw[3 * N + col] = (float)(sc[5] * flxfac);
+    }
+}
+
+}  // namespace rad

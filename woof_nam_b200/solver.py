@@ -1,0 +1,133 @@
+"""Python front end of the B200 RRTM column radiation: device buffers in PyTorch, compute in libradb200.so.
+
+``RadSolver`` mirrors the reference's column-solve entry (lwrad + swrad as ``rrtm_call`` drives them,
+namgpu/physics/rrtm/rrtm_call.py:246): it takes the radiation driver's column state in the reference's
+layout and returns the LW/SW heating rates and the surface and TOA fluxes under the reference's names.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .tables import blob
+
+INPUT_FIELDS = ("plyr", "plvl", "tlyr", "tlvl", "qlyr", "olyr", "gasvmr", "clouds", "sfcemis", "tsfg",
+                "sfcalb", "coszen")
+OPTIONAL_INPUTS = ("faerlw", "faersw", "icseed")
+
+
+def _torch():
+    import torch
+    return torch
+
+
+@dataclass
+class SolverConfig:
+    nlay: int = 61
+    precision: str = "mixed"         # "mixed" or "fp64"
+    route: str = "nam"               # "nam" (rtrnmr + spcvrtc) or "mcica"
+    iswmode: int = 2                 # 1 delta-Eddington, 2 PIFM (NAM), 3 discrete ordinates
+    diagnostic: bool = False         # clouds give optical depth / SSA / asymmetry directly
+    window_cols: int = 0             # SW MINVAL(laytrop) window in columns (0 = whole request)
+    sw_chunk: int = 32768
+    cpathfac: float = 1.5
+
+
+def output_shapes(nlay: int, ncol: int) -> dict:
+    return {"htlw": (nlay, ncol), "htsw": (nlay, ncol), "topflw": (2, ncol), "sfcflw": (4, ncol),
+            "topfsw": (3, ncol), "sfcfsw": (4, ncol), "fdncmp": (6, ncol)}
+
+
+class RadSolver:
+    """One library handle on the current CUDA device."""
+
+    def __init__(self, cfg: SolverConfig | None = None, **kw):
+        self.cfg = cfg or SolverConfig(**kw)
+        self.lib = _lib.load()
+        c = _lib.RadConfig()
+        self.lib.rad_config_default(ctypes.byref(c), self.cfg.nlay)
+        c.precision = _lib.PREC[self.cfg.precision]
+        c.route = _lib.ROUTE[self.cfg.route]
+        c.iswmode = self.cfg.iswmode
+        c.diagnostic = int(self.cfg.diagnostic)
+        c.window_cols = self.cfg.window_cols
+        c.sw_chunk = self.cfg.sw_chunk
+        c.cpathfac = self.cfg.cpathfac
+        h = ctypes.c_void_p()
+        _lib.check(self.lib, None, self.lib.rad_create(ctypes.byref(c), ctypes.byref(h)), "rad_create")
+        self.handle = h
+        b = blob()
+        _lib.check(self.lib, h, self.lib.rad_load_tables(h, b, len(b)), "rad_load_tables")
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.rad_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------------------------------------
+    def alloc_outputs(self, ncol: int, device=None) -> dict:
+        torch = _torch()
+        return {k: torch.empty(s, dtype=torch.float32, device=device or "cuda")
+                for k, s in output_shapes(self.cfg.nlay, ncol).items()}
+
+    def solve(self, cols: dict, solcon: float, out: dict | None = None, stream=None) -> dict:
+        """Solve device-resident columns.  ``cols`` maps the reference names (INPUT_FIELDS, optionally
+        faerlw/faersw/icseed) to contiguous float32 CUDA tensors in [field][level][column] layout."""
+        torch = _torch()
+        ncol = int(cols["coszen"].shape[-1])
+        for k in INPUT_FIELDS:
+            t = cols[k]
+            if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+                raise TypeError(f"input {k!r} must be a contiguous float32 CUDA tensor")
+            if t.shape[-1] != ncol:
+                raise ValueError(f"input {k!r} has {t.shape[-1]} columns, expected {ncol}")
+        if cols["plyr"].shape[0] != self.cfg.nlay:
+            raise ValueError(f"plyr has {cols['plyr'].shape[0]} layers, the solver was built for {self.cfg.nlay}")
+        if out is None:
+            out = self.alloc_outputs(ncol, device=cols["coszen"].device)
+        ci = _lib.RadColumns()
+        for k in INPUT_FIELDS:
+            setattr(ci, k, cols[k].data_ptr())
+        for k in OPTIONAL_INPUTS:
+            t = cols.get(k)
+            setattr(ci, k, t.data_ptr() if t is not None else None)
+        ci.solcon = float(solcon)
+        co = _lib.RadOutputs()
+        for k in output_shapes(1, 1):
+            t = out.get(k)
+            setattr(co, k, t.data_ptr() if t is not None else None)
+        st = stream if stream is not None else torch.cuda.current_stream()
+        rc = self.lib.rad_solve(self.handle, ctypes.byref(ci), ctypes.byref(co), ncol, ctypes.c_void_p(st.cuda_stream))
+        _lib.check(self.lib, self.handle, rc, "rad_solve")
+        return out
+
+    def to_device(self, columns, device="cuda", pinned: bool = False) -> dict:
+        """Copy a woof_nam_b200.columns.Columns request to the device (optionally through pinned memory)."""
+        torch = _torch()
+        d = {}
+        for k in INPUT_FIELDS:
+            a = torch.from_numpy(np.ascontiguousarray(getattr(columns, k), dtype=np.float32))
+            if pinned:
+                a = a.pin_memory()
+            d[k] = a.to(device, non_blocking=pinned)
+        return d
+
+    def solve_host(self, columns) -> dict:
+        """Host arrays in, host arrays out (copies both ways)."""
+        torch = _torch()
+        d = self.to_device(columns)
+        out = self.solve(d, columns.solcon)
+        torch.cuda.synchronize()
+        return {k: v.cpu().numpy() for k, v in out.items()}
+
+    def workspace_bytes(self, ncol: int) -> int:
+        return int(self.lib.rad_workspace_bytes(self.handle, ncol))
