@@ -1,0 +1,327 @@
+"""Benchmark of the RRTM LW+SW column radiation: columns/s on the 12 km NAM parent grid (954 x 835 columns,
+60 model layers = 61 radiation layers), mixed-precision CUDA path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one LW+SW solve of the whole domain (796,590 columns) with inputs resident in HBM.  Under
+torchrun (N > 1) every rank solves its own ensemble member of the same size (weak scaling; columns are
+independent, so there is no data-path collective); the time is the max over ranks.  Rank 0 prints one
+JSON line.  The reference arm (--impl reference) times the reference's own RRTM kernels compiled for the
+host CPU (oracle/_ref) on a bounded sample of the same workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "c2_parent_954x835"
+METRIC = "LW+SW columns/s at 60 levels"
+UNIT = "columns/s"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC = ROOT / "profiles" / "traffic.json"
+B200_SMS, FP32_LANES_PER_SM = 148, 128
+CPU_SAMPLE = 8192
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 kernel leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
+    ap.add_argument("--ncol", type=int, default=None,
+                    help="solve this many columns of the workload's generator instead of the full domain "
+                         "(small cases for profiling)")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        return json.loads(PEAKS.read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def fp32_peak_tflops(pk):
+    """FP32 FMA pipe: 148 SMs x 128 lanes x 2 FLOP x the measured max SM clock."""
+    mhz = float(pk.get("sm_max_mhz", 1965.0))
+    return B200_SMS * FP32_LANES_PER_SM * 2 * mhz * 1e6 / 1e12, mhz
+
+
+# ---------------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap,pci.bus_id")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        self.bus = (bus_id or "").lower()
+        self.rows, self.proc, self.th = [], None, None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return self
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self.th:
+                self.th.join(timeout=5)
+        rows = [r for r in self.rows if len(r) >= 8]
+        mine = [r for r in rows if self.bus and self.bus.endswith(r[7].lower()[-12:])] or rows
+        if not mine:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[0]) for r in mine if r[0].replace(".", "").isdigit()]
+        reasons = sorted({self.REASONS[i] for r in mine for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(mine[0][1]) if mine[0][1].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(mine)}
+
+
+# ---------------------------------------------------------------------------------------------------
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return ws, int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle
+    from woof_nam_b200.columns import workload
+    which = "ref" if oracle.REF_LIB.exists() else "port"
+    cols = workload(args.workload, ncol=args.cpu_sample)
+    nth = oracle.host_threads()
+    for _ in range(max(args.warmup, 0)):
+        oracle.solve(cols, precision="float", which=which, nthreads=nth)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.solve(cols, precision="float", which=which, nthreads=nth)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = cols.ncol / dt
+    sample = (f"{cols.ncol} columns of the {args.workload} generator per step (FP32 reference kernels, "
+              f"LW on every column, SW on the {int((cols.coszen >= 1e-4).sum())} sunlit ones)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "columns_per_step": cols.ncol, "layers": cols.nlay},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nth, "kind": "reference" if which == "ref" else "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def cpu_baseline(cols, n_sample):
+    from oracle import oracle
+    which = "ref" if oracle.REF_LIB.exists() else "port"
+    sub = cols.slice(0, min(n_sample, cols.ncol))
+    nth = oracle.host_threads()
+    oracle.solve(sub.slice(0, 256), precision="float", which=which, nthreads=nth)
+    t0 = time.perf_counter()
+    oracle.solve(sub, precision="float", which=which, nthreads=nth)
+    dt = time.perf_counter() - t0
+    return {"value": sub.ncol / dt, "unit": UNIT, "cores": nth, "kind": "reference" if which == "ref" else "port",
+            "sample": f"first {sub.ncol} columns of the timed workload, one solve, FP32 "
+                      f"{'reference kernels compiled for the host' if which == 'ref' else 'oracle restatement'}, "
+                      f"{dt:.1f} s"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    from oracle import oracle
+    from woof_nam_b200.columns import WORKLOADS, workload, make_columns
+    from woof_nam_b200.solver import RadSolver, output_shapes, INPUT_FIELDS
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n, seed, stress = WORKLOADS[args.workload]
+    n = args.ncol or n
+    # weak scaling: rank r solves ensemble member r (same generator, seed offset by the rank)
+    cols = make_columns(n, seed + 7919 * rank, stress)
+    nday = int((cols.coszen >= np.float32(1e-4)).sum())
+    mixed = RadSolver(precision="mixed", diagnostic=stress)
+    d = mixed.to_device(cols, device=dev)
+    out = mixed.alloc_outputs(n, device=dev)
+    in_bytes = sum(d[k].numel() * 4 for k in INPUT_FIELDS)
+    out_bytes = sum(v.numel() * 4 for v in out.values())
+    stream = torch.cuda.current_stream()
+
+    def timed(solver, steps, warmup, profile=False, sampler=None):
+        for _ in range(warmup):
+            solver.solve(d, cols.solcon, out)
+        torch.cuda.synchronize()
+        barrier()
+        if profile:
+            solver.profile(True)
+        launches0 = solver.profile_read()["launches"]
+        if sampler:
+            sampler.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            solver.solve(d, cols.solcon, out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clocks = sampler.stop() if sampler else None
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps)
+        prof = solver.profile_read()
+        if profile:
+            solver.profile(False)
+        return ms, prof, prof["launches"] - launches0, clocks
+
+    bus = None
+    try:
+        p = torch.cuda.get_device_properties(dev)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+    except Exception:
+        pass
+    ms, prof, launches, clocks = timed(mixed, args.steps, args.warmup, profile=True, sampler=ClockSampler(bus))
+    value = ws * n / (ms * 1e-3)
+
+    # plain FP64 single-domain kernel (the reference statements in FP64): the x8 denominator
+    fp64 = None
+    if not args.no_fp64:
+        s64 = RadSolver(precision="fp64", diagnostic=stress)
+        ms64, _, _, _ = timed(s64, max(1, min(args.steps, 3)), max(args.warmup, 1))
+        fp64 = {"value": ws * n / (ms64 * 1e-3), "ms_per_step": ms64, "unit": UNIT}
+        del s64
+
+    # end to end through the public API with host buffers: pinned host inputs -> device, solve, -> host
+    hin = {k: v.cpu().pin_memory() for k, v in d.items()}
+    hout = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for k, v in out.items()}
+
+    def e2e_step():
+        for k in INPUT_FIELDS:
+            d[k].copy_(hin[k], non_blocking=True)
+        mixed.solve(d, cols.solcon, out)
+        for k, v in out.items():
+            hout[k].copy_(v, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+
+    # roofline of the dominant kernel (FP32 pipe; algorithmic FLOPs from the oracle's operation-count table)
+    pk = peaks()
+    peak_tf, mhz = fp32_peak_tflops(pk)
+    ops = oracle.opcount(cols.slice(0, 1024))
+    lw_ms, sw_ms = prof["lw_ms"] / max(prof["solves"], 1), prof["sw_ms"] / max(prof["solves"], 1)
+    lw_tf = ops["lw_flops_per_col"] * n / (lw_ms * 1e-3) / 1e12
+    sw_tf = ops["sw_flops_per_daycol"] * nday / (sw_ms * 1e-3) / 1e12
+    dom = "sw_column_kernel" if sw_ms >= lw_ms else "lw_column_kernel"
+    achieved = sw_tf if dom == "sw_column_kernel" else lw_tf
+    traffic = None
+    try:
+        tr = json.loads(TRAFFIC.read_text())
+        per = tr[dom]["dram_bytes_per_unit"]
+        traffic = per * (nday if dom == "sw_column_kernel" else n)
+    except (OSError, ValueError, KeyError):
+        pass
+    hbm_peak = float(pk.get("hbm_gbs", 6650.0))
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline(cols, args.cpu_sample)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: 12 km NAM parent grid 954x835 columns x 61 radiation "
+                                   f"layers (60 model layers), seed {seed}" + (" + rank offset" if ws > 1 else ""),
+                       "columns": n, "day_columns": nday, "layers": cols.nlay,
+                       "input_bytes": in_bytes, "output_bytes": out_bytes,
+                       "l2": f"inputs ({in_bytes / 1e9:.1f} GB) larger than L2 (126 MB); no flush",
+                       "parallelism": f"replicas x{ws} (one ensemble member per GPU)"},
+            "roofline": {"bound": "fp32", "kernel": dom, "achieved": achieved, "peak": peak_tf,
+                         "unit": "TFLOP/s", "frac": achieved / peak_tf, "traffic": traffic,
+                         "peak_source": f"nominal FP32 pipe 148 SM x 128 lanes x 2 at the measured sm_max "
+                                        f"{mhz:.0f} MHz (MEASURED_PEAKS.json holds no FP32 figure)",
+                         "flops_per_unit": ops["sw_flops_per_daycol"] if dom == "sw_column_kernel"
+                         else ops["lw_flops_per_col"],
+                         "unit_of_work": "sunlit column" if dom == "sw_column_kernel" else "column",
+                         "kernel_ms": {"lw_column_kernel": lw_ms, "sw_prep": prof["prep_ms"] / max(prof["solves"], 1),
+                                       "sw_column_kernel": sw_ms},
+                         "lw_tflops": lw_tf, "sw_tflops": sw_tf,
+                         "hbm": {"achieved": (in_bytes + out_bytes) / (ms * 1e-3) / 1e9, "peak": hbm_peak,
+                                 "unit": "GB/s", "frac": (in_bytes + out_bytes) / (ms * 1e-3) / 1e9 / hbm_peak}},
+            "plain_fp64": fp64,
+            "cpu_baseline": cpu,
+            "e2e": {"value": ws * n / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": in_bytes,
+                    "d2h_bytes_per_step": out_bytes, "ms_per_step": ms_e2e},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -119,6 +119,22 @@ int64_t rad_workspace_bytes(const RadHandle* h, int64_t ncol);
 int rad_solve_batch(RadHandle* h, int32_t nreq, const RadColumns* ins, const RadOutputs* outs,
                     const int64_t* ncols, void* stream);
 
+/* Device-time accounting of the library's own kernels (instrumentation; no counterpart in the reference,
+ * which has none).  While enabled, rad_solve records CUDA events on its stream around the LW kernel, the
+ * SW day-list kernels and the SW kernel; rad_profile_read waits for the last recorded event and returns
+ * the sums since the last enable.  `launches` counts every kernel the handle launched since rad_create. */
+typedef struct {
+    int64_t launches;        /* kernels launched by this handle since rad_create (profiling on or off) */
+    int64_t solves;          /* rad_solve calls profiled */
+    int64_t columns;         /* columns of the profiled solves */
+    double lw_ms;            /* device time of the LW column kernel */
+    double prep_ms;          /* device time of the SW day list and group kernels */
+    double sw_ms;            /* device time of the SW column kernel */
+} RadProfile;
+
+int rad_profile_enable(RadHandle* h, int on);
+int rad_profile_read(RadHandle* h, RadProfile* p);
+
 /* Thread-local message of the last failing call on this handle (or a global message when h is NULL). */
 const char* rad_last_error(const RadHandle* h);
 

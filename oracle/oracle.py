@@ -19,6 +19,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liborc.so"
+OPCOUNT_LIB = HERE / "libopcount.so"
 REF_LIB = HERE / "_ref" / "libref_rrtm.so"
 TABLES = HERE.parent / "woof_nam_b200" / "data" / "rrtm_tables.npz"
 
@@ -29,10 +30,11 @@ _U = ctypes.POINTER(ctypes.c_uint)
 
 
 def build(force: bool = False) -> Path:
-    """Compile liborc.so with the Makefile beside this file (no GPU needed)."""
-    if force or not LIB.exists() or any(p.stat().st_mtime > LIB.stat().st_mtime
-                                        for p in HERE.glob("rrtm_*.?pp")):
-        subprocess.run(["make", "-C", str(HERE), "liborc.so"], check=True)
+    """Compile liborc.so and libopcount.so with the Makefile beside this file (no GPU needed)."""
+    srcs = list(HERE.glob("rrtm_*.?pp")) + list(HERE.glob("opcount.hpp"))
+    if force or not all(p.exists() for p in (LIB, OPCOUNT_LIB)) or any(
+            p.stat().st_mtime > min(LIB.stat().st_mtime, OPCOUNT_LIB.stat().st_mtime) for p in srcs):
+        subprocess.run(["make", "-C", str(HERE), "all"], check=True)
     return LIB
 
 
@@ -40,7 +42,8 @@ def _load(path: Path):
     lib = ctypes.CDLL(str(path))
     lib.orc_add_table.argtypes = [ctypes.c_char_p, _D, ctypes.c_long]
     lib.orc_add_itable.argtypes = [ctypes.c_char_p, _I, ctypes.c_long]
-    lib.orc_solve.restype = ctypes.c_int
+    if hasattr(lib, "orc_solve"):
+        lib.orc_solve.restype = ctypes.c_int
     tabs = np.load(TABLES)
     lib.orc_clear_tables()
     for name in tabs.files:
@@ -61,6 +64,9 @@ def lib(which: str = "port"):
     if which not in _LIBS:
         if which == "port":
             _LIBS[which] = _load(build())
+        elif which == "opcount":
+            build()
+            _LIBS[which] = _load(OPCOUNT_LIB)
         else:
             if not REF_LIB.exists():
                 raise FileNotFoundError(f"{REF_LIB} is not built (oracle/build_ref.sh needs the reference tree)")
@@ -152,3 +158,32 @@ def sw_stages(cols, which: str = "port", iswmode: int = 2) -> dict:
     if rc != 0:
         raise RuntimeError("sw_stages failed")
     return out
+
+
+OPCOUNT_STAGES = ("lw_prep", "lw_cldprop", "lw_setcoef", "lw_taumol", "lw_rtrnmr",
+                  "sw_prep", "sw_cldprop", "sw_setcoef", "sw_taumol", "sw_spcvrtc", "swrad_post")
+
+
+def opcount(cols, iswmode: int = 2, cpathfac: float = 1.5) -> dict:
+    """Operation-count table of the reference statements over the request (see opcount.hpp for the rule).
+
+    Returns per-stage sums of (add, mul, div, func, other) and, per column, the LW FLOPs, the SW FLOPs
+    per day column and the request-average FLOPs per column (LW + SW x day fraction)."""
+    L = lib("opcount")
+    counts = np.zeros((11, 5))
+    nday = ctypes.c_int(0)
+    keep = {f: _f(getattr(cols, f)) for f in cols.FIELDS}
+    rc = L.orc_opcount(ctypes.c_int(int(cols.diagnostic_clouds)), ctypes.c_int(iswmode), ctypes.c_double(cpathfac),
+                       ctypes.c_int(cols.nlay), ctypes.c_int(cols.ncol),
+                       *[keep[f].ctypes.data_as(_F) for f in cols.FIELDS], ctypes.c_double(cols.solcon),
+                       counts.ctypes.data_as(_D), ctypes.byref(nday))
+    if rc != 0:
+        raise RuntimeError("opcount failed")
+    n, nd = cols.ncol, nday.value
+    flops = counts[:, :4].sum(axis=1)
+    lw = flops[:5].sum() / n
+    sw = flops[5:].sum() / max(nd, 1)
+    return {"stages": {s: dict(zip(("add", "mul", "div", "func", "other"), counts[i].tolist()))
+                       for i, s in enumerate(OPCOUNT_STAGES)},
+            "ncol": n, "nday": nd, "lw_flops_per_col": lw, "sw_flops_per_daycol": sw,
+            "flops_per_col": lw + sw * nd / n}

@@ -64,6 +64,13 @@ inline int imax(int a, int b) { return a > b ? a : b; }
 // Fortran mod(a, 1.0) for a >= 0.
 template <class R> inline R fmod1(R a) { return std::fmod(a, R(1)); }
 
+// Elementary functions of the arithmetic type (the operation counter overloads them for its type).
+template <class R> inline R mexp(R a) { return std::exp(a); }
+template <class R> inline R mlog(R a) { return std::log(a); }
+template <class R> inline R msqrt(R a) { return std::sqrt(a); }
+template <class R> inline R mfabs(R a) { return std::fabs(a); }
+template <class R> inline R mpow(R a, R b) { return std::pow(a, b); }
+
 // Solve configuration (the reference's NAM runtime switches unless stated).
 struct Config {
     int iswmode = 2;          // SW two-stream: 1 delta-Eddington, 2 PIFM (NAM), 3 discrete ordinates

@@ -140,7 +140,7 @@ void lw_prep(LwColumn<R>& c, const Inputs& in, int col, const float* clouds9, in
     for (int b = 0; b < 16; ++b) {
         const int j1 = b + 1;
         if (j1 == 1 || j1 == 4 || j1 == 10) c.secdiff[b] = (R)1.66f;
-        else c.secdiff[b] = fminR((R)1.80f, fmaxR((R)1.50f, (R)A0[b] + (R)A1[b] * std::exp((R)A2[b] * pwv)));
+        else c.secdiff[b] = fminR((R)1.80f, fmaxR((R)1.50f, (R)A0[b] + (R)A1[b] * mexp((R)A2[b] * pwv)));
     }
     int lcf = 0;
     for (int k = 1; k <= nlay; ++k)
@@ -248,7 +248,7 @@ void lw_setcoef(LwColumn<R>& c)
             c.pklay[k * 16 + i - 1] = (R)delwave[i - 1] * (TOT(indlay, i) + tlyrfr * (TOT(indlay + 1, i) - TOT(indlay, i)));
             c.pklev[k * 16 + i - 1] = (R)delwave[i - 1] * (TOT(indlev, i) + tlvlfr * (TOT(indlev + 1, i) - TOT(indlev, i)));
         }
-        const R plog = std::log(pav);
+        const R plog = mlog(pav);
         const int jpk = imax(1, imin(58, (int)((R)36 - (R)5 * (plog + (R)0.04f))));
         const int jp1 = jpk + 1;
         const R fp = fmaxR((R)0, fminR((R)1, (R)5 * ((R)preflog[jpk - 1] - plog)));
@@ -496,7 +496,7 @@ void lw_taumol(LwColumn<R>& c)
                 if (band == 3) {
                     const R pn = c.coldry[k0] * CHI(4, jpk + 1);
                     const R ratn2o = c.CA(3, k0) / pn;
-                    if (ratn2o > (R)1.5f) adjcoln2o = ((R)0.5f + std::pow(ratn2o - (R)0.5f, (R)0.65f)) * pn;
+                    if (ratn2o > (R)1.5f) adjcoln2o = ((R)0.5f + mpow(ratn2o - (R)0.5f, (R)0.65f)) * pn;
                     else adjcoln2o = c.CA(3, k0);
                 }
                 const Sel<R> s0 = sel_branch(branch_of(sp), fs, ind0);
@@ -537,7 +537,7 @@ void lw_taumol(LwColumn<R>& c)
                 if (band == 3) {
                     const R pn = c.coldry[k0] * CHI(4, jpk + 1);
                     const R ratn2o = c.CA(3, k0) / pn;
-                    if (ratn2o > (R)1.5f) adjcoln2o = ((R)0.5f + std::pow(ratn2o - (R)0.5f, (R)0.65f)) * pn;
+                    if (ratn2o > (R)1.5f) adjcoln2o = ((R)0.5f + mpow(ratn2o - (R)0.5f, (R)0.65f)) * pn;
                     else adjcoln2o = c.CA(3, k0);
                 }
                 const R fac000 = ((R)1 - fs) * f00, fac010 = ((R)1 - fs) * f10, fac100 = fs * f00, fac110 = fs * f10;
@@ -640,7 +640,7 @@ void lw_taumol(LwColumn<R>& c)
                 const int ind0 = (jpk - 1) * 5 + (c.jt[k0] - 1) + 1, ind1 = jpk * 5 + (c.jt1[k0] - 1) + 1;
                 const R temp = c.coldry[k0] * CHI(2, jpk + 1);
                 const R ratco2 = c.CA(1, k0) / temp;
-                const R adj = ratco2 > (R)3 ? ((R)2 + std::pow(ratco2 - (R)2, (R)0.77f)) * temp : c.CA(1, k0);
+                const R adj = ratco2 > (R)3 ? ((R)2 + mpow(ratco2 - (R)2, (R)0.77f)) * temp : c.CA(1, k0);
                 for (int ig = 0; ig < NG; ++ig) {
                     const R tauself = c.selffac[k0] * interp(selfref, NG, c.indself[k0], ig, c.selffrac[k0]);
                     const R taufor = c.forfac[k0] * interp(forref, NG, c.indfor[k0], ig, c.forfrac[k0]);
@@ -681,7 +681,7 @@ void lw_taumol(LwColumn<R>& c)
                 const int ind1 = (jpk * 5 + (jt1k - 1)) * 9 + js1;
                 spec(c1, rma, c3, (R)8, scm, spm, jm, fm);
                 spec(c1, rpa, c3, (R)8, scp, spp, jpl, fpl);
-                const R adj = ratco2 > (R)3 ? ((R)3 + std::pow(ratco2 - (R)3, (R)0.79f)) * temp : c2;
+                const R adj = ratco2 > (R)3 ? ((R)3 + mpow(ratco2 - (R)3, (R)0.79f)) * temp : c2;
                 const int br = branch_joint(sp, sp1);
                 const Sel<R> s0 = sel_branch(br, fs, ind0), s1 = sel_branch(br, fs1, ind1);
                 const int indm = c.indminor[k0];
@@ -697,7 +697,7 @@ void lw_taumol(LwColumn<R>& c)
                     c.FR(NS + ig, k0) = interp(fa, NG, jpl, ig, fpl);
                 }
             } else {
-                const R adj = ratco2 > (R)3 ? ((R)2 + std::pow(ratco2 - (R)2, (R)0.79f)) * temp : c2;
+                const R adj = ratco2 > (R)3 ? ((R)2 + mpow(ratco2 - (R)2, (R)0.79f)) * temp : c2;
                 const int ind0 = (jpk - 13) * 5 + (jtk - 1) + 1, ind1 = (jpk - 12) * 5 + (jt1k - 1) + 1;
                 static const float scl[12] = {1, 1, 1, 1, 1, 0.92f, 0.88f, 1.07f, 1.1f, 0.99f, 0.855f, 1};
                 for (int ig = 0; ig < NG; ++ig) {
@@ -723,7 +723,7 @@ void lw_taumol(LwColumn<R>& c)
             const int jpk = c.jp[k0], jtk = c.jt[k0], jt1k = c.jt1[k0];
             const R temp = c.coldry[k0] * CHI(2, jpk + 1);
             const R ratco2 = c.CA(1, k0) / temp;
-            const R adj = ratco2 > (R)3 ? ((R)2 + std::pow(ratco2 - (R)2, (R)0.65f)) * temp : c.CA(1, k0);
+            const R adj = ratco2 > (R)3 ? ((R)2 + mpow(ratco2 - (R)2, (R)0.65f)) * temp : c.CA(1, k0);
             const R f00 = c.fac00[k0], f01 = c.fac01[k0], f10 = c.fac10[k0], f11 = c.fac11[k0];
             const R w3 = c.WX(2, k0), w4 = c.WX(3, k0);
             if (k0 < lt) {
@@ -768,7 +768,7 @@ void lw_taumol(LwColumn<R>& c)
             const R f00 = c.fac00[k0], f01 = c.fac01[k0], f10 = c.fac10[k0], f11 = c.fac11[k0];
             const R temp = c.coldry[k0] * CHI(4, jpk + 1);
             const R ratn2o = c4 / temp;
-            const R adj = ratn2o > (R)1.5f ? ((R)0.5f + std::pow(ratn2o - (R)0.5f, (R)0.65f)) * temp : c4;
+            const R adj = ratn2o > (R)1.5f ? ((R)0.5f + mpow(ratn2o - (R)0.5f, (R)0.65f)) * temp : c4;
             if (k0 < lt) {
                 R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fm, fpl;
                 int js, js1, jm, jpl;
@@ -921,7 +921,7 @@ void lw_taumol(LwColumn<R>& c)
                 spec(c1, rpa, c4, (R)8, scp, spp, jpl, fpl);
                 const R temp = c.coldry[k0] * (R)3.55e-4f;
                 const R ratco2 = c2 / temp;
-                const R adj = ratco2 > (R)3 ? ((R)2 + std::pow(ratco2 - (R)2, (R)0.68f)) * temp : c2;
+                const R adj = ratco2 > (R)3 ? ((R)2 + mpow(ratco2 - (R)2, (R)0.68f)) * temp : c2;
                 const int br = branch_joint(sp, sp1);
                 const Sel<R> s0 = sel_branch(br, fs, ind0), s1 = sel_branch(br, fs1, ind1);
                 const R f00 = c.fac00[k0], f01 = c.fac01[k0], f10 = c.fac10[k0], f11 = c.fac11[k0];

@@ -237,7 +237,7 @@ void sw_setcoef(SwColumn<R>& c)
         const R pav = c.pavel[k0], tav = c.tavel[k0], h2o = c.h2ovmr[k0];
         const R forf = pav * stpfac / (tav * ((R)1 + h2o));
         c.forfac[k0] = forf;
-        const R plog = std::log(pav);
+        const R plog = mlog(pav);
         const int jpk = imax(1, imin(58, (int)((R)36 - (R)5 * (plog + (R)0.04f))));
         const int jp1 = jpk + 1;
         const R fp = (R)5 * ((R)preflog[jpk - 1] - plog);
@@ -717,10 +717,10 @@ inline void sw_layer_rt(R ztau1, R zssaw, R zssa1, R g1, R g2, R g3, R g4, R cz,
         td = fmaxR((R)0, fminR((R)1, (R)1 - rd));
     } else {
         const R za1 = g1 * g4 + g2 * g3, za2 = g1 * g3 + g2 * g4;
-        const R zrk = std::sqrt((g1 - g2) * (g1 + g2));
+        const R zrk = msqrt((g1 - g2) * (g1 + g2));
         const R zrk2 = (R)2 * zrk, zrp = zrk * cz, zrp1 = (R)1 + zrp, zrm1 = (R)1 - zrp;
         R zrpp = (R)1 - zrp * zrp;
-        if (std::fabs(zrpp) < eps1) zrpp = zrpp < 0 ? -eps1 : eps1;
+        if (mfabs(zrpp) < eps1) zrpp = zrpp < 0 ? -eps1 : eps1;
         const R zrkg1 = zrk + g1, zrkg3 = zrk * g3, zrkg4 = zrk * g4;
         const R zr1 = zrm1 * (za2 + zrkg3), zr2 = zrp1 * (za2 - zrkg3), zr3 = zrk2 * (g3 - za2 * cz);
         const R zr4 = zrpp * zrkg1, zr5 = zrpp * (zrk - g1);

@@ -1,0 +1,153 @@
+"""Parity of the CUDA path (through the C-ABI) against the float64 oracle.
+
+  fp64 kernel   the reference statements in float64: agrees with the oracle to float32 output rounding
+  mixed kernel  float bulk, float64 where float loses the result: within 0.05 W/m^2 and 0.01 K/day
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import assert_within, golden_columns, max_errors
+from oracle import oracle
+from woof_nam_b200.columns import make_columns
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(**kw):
+    from woof_nam_b200.solver import RadSolver
+    return RadSolver(**kw)
+
+
+@pytest.fixture(scope="module")
+def plain():
+    cols = make_columns(1024, 1001)
+    return cols, oracle.solve(cols, precision="double")
+
+
+@pytest.fixture(scope="module")
+def stress():
+    cols = make_columns(1024, 5005, stress=True)
+    return cols, oracle.solve(cols, precision="double")
+
+
+def test_fp64_matches_oracle(plain):
+    cols, ref = plain
+    out = _solver(precision="fp64").solve_host(cols)
+    assert_within(out, ref, flux_tol=2e-3, heat_tol=2e-4, what="fp64 kernel")
+
+
+def test_mixed_within_tolerance(plain):
+    cols, ref = plain
+    out = _solver(precision="mixed").solve_host(cols)
+    assert_within(out, ref, what="mixed kernel, plain request")
+
+
+def test_mixed_stress_within_tolerance(stress):
+    cols, ref = stress
+    out = _solver(precision="mixed", diagnostic=True).solve_host(cols)
+    assert_within(out, ref, what="mixed kernel, precision-stress request")
+
+
+def test_fp64_stress_matches_oracle(stress):
+    cols, ref = stress
+    out = _solver(precision="fp64", diagnostic=True).solve_host(cols)
+    assert_within(out, ref, flux_tol=2e-3, heat_tol=2e-3, what="fp64 kernel, stress")
+
+
+@pytest.mark.parametrize("iswmode", [1, 3])
+def test_other_two_stream_modes(iswmode):
+    cols = make_columns(256, 77)
+    ref = oracle.solve(cols, precision="double", iswmode=iswmode)
+    out = _solver(precision="fp64", iswmode=iswmode).solve_host(cols)
+    assert_within(out, ref, flux_tol=2e-3, heat_tol=1e-3, what=f"fp64 iswmode {iswmode}")
+    out = _solver(precision="mixed", iswmode=iswmode).solve_host(cols)
+    assert_within(out, ref, what=f"mixed iswmode {iswmode}")
+
+
+def test_windows_and_chunks():
+    """MINVAL(laytrop) windows of 96 columns and SW chunks of 40 day columns, as the oracle runs them."""
+    cols = make_columns(600, 11)
+    ref = oracle.solve(cols, precision="double", window_cols=96, sw_chunk=40)
+    out = _solver(precision="fp64", window_cols=96, sw_chunk=40).solve_host(cols)
+    assert_within(out, ref, flux_tol=2e-3, heat_tol=2e-4, what="windows")
+
+
+def test_golden_reference_lw(golden):
+    """Against the reference's own float kernels (golden vectors): LW within the tolerances."""
+    for case in ("plain", "stress"):
+        cols = golden_columns(golden, case)
+        out = _solver(precision="mixed", diagnostic=cols.diagnostic_clouds).solve_host(cols)
+        ref = {k: golden[f"{case}_lw_{k}"].astype(np.float64) for k in ("htlw", "topflw", "sfcflw")}
+        assert_within(out, ref, what=f"LW vs reference float kernels ({case})")
+
+
+def test_night_only_and_empty():
+    cols = make_columns(64, 3)
+    cols.coszen[:] = -0.5
+    s = _solver(precision="mixed")
+    out = s.solve_host(cols)
+    for k in ("htsw", "topfsw", "sfcfsw", "fdncmp"):
+        assert (out[k] == 0).all(), k
+    ref = oracle.solve(cols, precision="double")
+    assert_within(out, ref, what="night-only")
+    empty = cols.slice(0, 0)
+    out = s.solve_host(empty)
+    assert out["htlw"].shape == (61, 0)
+
+
+def test_alone_equals_in_batch():
+    """Groups are request-local: a request gives the same bits alone and inside a batch call."""
+    import torch
+    s = _solver(precision="mixed")
+    reqs = [make_columns(n, 100 + n) for n in (37, 300, 129)]
+    alone = [s.solve_host(c) for c in reqs]
+    batch = s.solve_batch([s.to_device(c) for c in reqs], [c.solcon for c in reqs])
+    torch.cuda.synchronize()
+    for a, b in zip(alone, batch):
+        for k in a:
+            assert np.array_equal(a[k], b[k].cpu().numpy()), k
+
+
+def test_errors_are_loud():
+    import torch
+    from woof_nam_b200._lib import RadError
+    s = _solver(precision="mixed")
+    cols = make_columns(8, 1)
+    d = s.to_device(cols)
+    with pytest.raises(TypeError):
+        s.solve({**d, "plyr": d["plyr"].cpu()}, cols.solcon)
+    with pytest.raises(ValueError):
+        s.solve({**d, "tsfg": d["tsfg"][:4].contiguous()}, cols.solcon)
+    bad = _solver(precision="mixed", nlay=40)
+    with pytest.raises(ValueError):
+        bad.solve(d, cols.solcon)
+    torch.cuda.synchronize()
+    assert isinstance(RadError(-1, "x"), RuntimeError)
+
+
+def test_error_report(plain):
+    """Per-output error of both kernels against the oracle (printed for the record)."""
+    cols, ref = plain
+    for prec in ("fp64", "mixed"):
+        e = max_errors(_solver(precision=prec).solve_host(cols), ref)
+        print(prec, {k: f"{v:.2e}" for k, v in e.items()})
+
+
+def test_handle_lifetime():
+    """A handle keeps working when other handles are created and destroyed (the k-tables are shared per
+    device and outlive every handle)."""
+    import gc
+    s = _solver(precision="mixed")
+    cols = make_columns(128, 5)
+    a = s.solve_host(cols)
+    for prec in ("fp64", "mixed"):
+        t = _solver(precision=prec)
+        t.solve_host(cols)
+        t.close()
+        del t
+        gc.collect()
+    b = s.solve_host(cols)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k

@@ -1,0 +1,108 @@
+"""The oracle against the reference: the float statements of the C++ restatement reproduce the golden
+vectors of the reference's own kernels bit for bit, and the float64 restatement stays within the
+tolerances of the float reference where the reference is finite."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import golden_columns, max_errors
+from oracle import oracle
+
+CASES = ("plain", "stress")
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_lw_bit_exact(golden, case):
+    cols = golden_columns(golden, case)
+    r = oracle.solve(cols, precision="float")
+    for k in ("htlw", "topflw", "sfcflw"):
+        assert np.array_equal(r[k].astype(np.float32), golden[f"{case}_lw_{k}"], equal_nan=True), k
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_sw_full_depth_bit_exact(golden, case):
+    """At full optical depth the reference's float layer solver returns NaN on sunlit columns
+    (exp-table underflow makes its 1/exp(-k tau) overflow); the restatement reproduces that pattern."""
+    cols = golden_columns(golden, case)
+    r = oracle.solve(cols, precision="float")
+    for k in ("htsw", "topfsw", "sfcfsw", "fdncmp"):
+        assert np.array_equal(r[k].astype(np.float32), golden[f"{case}_sw_{k}"], equal_nan=True), k
+    day = cols.coszen >= np.float32(1e-4)
+    assert np.isnan(golden[f"{case}_sw_htsw"][:, day]).any()
+    assert not np.isnan(golden[f"{case}_sw_htsw"][:, ~day]).any()
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_sw_scaled_bit_exact(golden, case):
+    cols = golden_columns(golden, case)
+    oracle.set_debug(1.0e-3)
+    try:
+        r = oracle.solve(cols, precision="float")
+    finally:
+        oracle.set_debug(1.0)
+    for k in ("htsw", "topfsw", "sfcfsw", "fdncmp"):
+        assert np.array_equal(r[k].astype(np.float32), golden[f"{case}_swq_{k}"]), k
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_sw_stages_bit_exact(golden, case):
+    cols = golden_columns(golden, case)
+    st = oracle.sw_stages(cols)
+    n = golden[f"{case}_st_laytrop"].shape[0]
+    for k in ("taug", "taur", "sfluxzen", "taucw", "ssacw", "asycw", "cldfrc", "zcf", "laytrop"):
+        assert np.array_equal(st[k][:n], golden[f"{case}_st_{k}"]), k
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fp64_lw_close_to_reference(golden, case):
+    """The float64 restatement differs from the float reference by rounding only."""
+    cols = golden_columns(golden, case)
+    r = oracle.solve(cols, precision="double")
+    ref = {k: golden[f"{case}_lw_{k}"].astype(np.float64) for k in ("htlw", "topflw", "sfcflw")}
+    e = max_errors(r, ref)
+    assert e["htlw"] < 0.01 and e["topflw"] < 0.05 and e["sfcflw"] < 0.05, e
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_fp64_sw_scaled_follows_reference(golden, case):
+    """The float64 restatement follows the reference statement by statement: the median difference is
+    rounding.  The tails are the reference's own float losses (near-conservative cancellation and the
+    k*mu0 = 1 resonance in its layer solver): on the plain request up to ~0.7 K/day and ~2 W/m^2, on the
+    precision-stress request hundreds of K/day -- the float reference cannot meet the 0.01 K/day /
+    0.05 W/m^2 tolerances there, which is what the mixed-precision design of the CUDA path addresses."""
+    cols = golden_columns(golden, case)
+    oracle.set_debug(1.0e-3)
+    try:
+        r = oracle.solve(cols, precision="double")
+    finally:
+        oracle.set_debug(1.0)
+    for k in ("htsw", "topfsw", "sfcfsw", "fdncmp"):
+        e = np.abs(r[k] - golden[f"{case}_swq_{k}"]) * (86400.0 if k == "htsw" else 1.0)
+        assert np.percentile(e, 50) < (0.01 if k == "htsw" else 0.05), (k, np.percentile(e, 50))
+        assert np.isfinite(e).all()
+    if case == "stress":
+        assert np.max(np.abs(r["htsw"] - golden["stress_swq_htsw"])) * 86400.0 > 0.01
+
+
+def test_fp64_sw_finite_and_night_zero(golden):
+    cols = golden_columns(golden, "plain")
+    r = oracle.solve(cols, precision="double")
+    day = cols.coszen >= np.float32(1e-4)
+    for k in ("htsw", "topfsw", "sfcfsw", "fdncmp"):
+        assert np.isfinite(r[k]).all(), k
+        assert (r[k][:, ~day] == 0).all(), k
+    # energy: what enters at the top and is not reflected is absorbed in the column or at the surface
+    top_in = r["topfsw"][1]
+    assert (top_in[day] > 0).all()
+
+
+def test_windows_change_only_group_minima():
+    """SW MINVAL(laytrop) windows: a request solved as one window or as windows of 8 columns differs
+    only through bands 19/23/25/28 (group minima); LW is untouched."""
+    from woof_nam_b200.columns import make_columns
+    cols = make_columns(64, 7)
+    a = oracle.solve(cols, precision="double")
+    b = oracle.solve(cols, precision="double", window_cols=16)
+    assert np.array_equal(a["htlw"], b["htlw"])
+    assert np.isfinite(b["htsw"]).all()

@@ -43,6 +43,11 @@ class RadOutputs(ctypes.Structure):
                 ("fdncmp", ctypes.c_void_p), ("lw_mask", ctypes.c_void_p), ("sw_mask", ctypes.c_void_p)]
 
 
+class RadProfile(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_int64), ("solves", ctypes.c_int64), ("columns", ctypes.c_int64),
+                ("lw_ms", ctypes.c_double), ("prep_ms", ctypes.c_double), ("sw_ms", ctypes.c_double)]
+
+
 # Every symbol include/radb200.h declares, with its ctypes signature.
 SIGNATURES = {
     "rad_version": ([], ctypes.c_int),
@@ -54,6 +59,8 @@ SIGNATURES = {
     "rad_workspace_bytes": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int64),
     "rad_solve_batch": ([ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(RadColumns), ctypes.POINTER(RadOutputs),
                          ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p], ctypes.c_int),
+    "rad_profile_enable": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
+    "rad_profile_read": ([ctypes.c_void_p, ctypes.POINTER(RadProfile)], ctypes.c_int),
     "rad_last_error": ([ctypes.c_void_p], ctypes.c_char_p),
     "rad_destroy": ([ctypes.c_void_p], None),
 }

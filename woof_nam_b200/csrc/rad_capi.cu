@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -38,8 +39,6 @@ struct RadHandle {
     RadConfig cfg{};
     int device = 0;
     bool tables_ok = false;
-    float* d_tf = nullptr;
-    double* d_td = nullptr;
     float *d_lwf = nullptr, *d_swf = nullptr;      // LW LUT (3 x 10001) and SW exp table, float32
     double *d_lwd = nullptr, *d_swd = nullptr;     // the same in float64
     int* d_err = nullptr;
@@ -51,10 +50,27 @@ struct RadHandle {
     void* d_cub = nullptr;
     size_t cub_bytes = 0;
     std::string err;
+    // kernel accounting
+    int64_t launches = 0;
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev;      // 4 events per profiled solve: before LW, after LW, after prep, after SW
+    size_t ev_used = 0;
+    int64_t prof_solves = 0, prof_columns = 0;
 };
 
 namespace {
 thread_local std::string g_err;
+
+// Per-device k-table store shared by every handle of the process (see rad_load_tables).
+struct DeviceTables {
+    float* tf = nullptr;
+    double* td = nullptr;
+    std::vector<int64_t> off;
+    std::vector<float> hf;
+    LwHostConsts k{};
+};
+std::mutex g_tab_mu;
+std::map<int, DeviceTables> g_tabs;
 
 int fail(RadHandle* h, int code, const std::string& msg)
 {
@@ -193,11 +209,33 @@ int ensure_scratch(RadHandle* h, int64_t n)
     return RAD_OK;
 }
 
+// Record the next profiling event on st (no-op while profiling is off).
+int mark(RadHandle* h, cudaStream_t st, size_t base, int i)
+{
+    if (!h->profiling) return RAD_OK;
+    RAD_CUDA(h, cudaEventRecord(h->ev[base + i], st));
+    return RAD_OK;
+}
+
 template <class R>
 int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t n, cudaStream_t st)
 {
     const RadConfig& cfg = h->cfg;
     const int nlay = cfg.nlay;
+    size_t eb = 0;
+    if (h->profiling) {
+        eb = h->ev_used;
+        while (h->ev.size() < eb + 4) {
+            cudaEvent_t e;
+            RAD_CUDA(h, cudaEventCreate(&e));
+            h->ev.push_back(e);
+        }
+        h->ev_used += 4;
+        h->prof_solves += 1;
+        h->prof_columns += n;
+    }
+    int mrc = mark(h, st, eb, 0);
+    if (mrc) return mrc;
     // ---- LW over every column
     {
         LwIn a{in->plyr, in->plvl, in->tlyr, in->tlvl, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faerlw,
@@ -212,9 +250,11 @@ int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int6
             a.col0 = c0;
             const int64_t nb = std::min<int64_t>(maxg, n - c0);
             lw_column_kernel<R><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
+            h->launches += 1;
         }
         RAD_CUDA(h, cudaGetLastError());
     }
+    if ((mrc = mark(h, st, eb, 1))) return mrc;
     // ---- SW day list, laytrop, groups
     int rc = ensure_scratch(h, n);
     if (rc) return rc;
@@ -239,6 +279,7 @@ int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int6
                                 maxc, h->d_pos);
     k_groups<<<gb, T, 0, st>>>(n, h->d_daycol, h->d_nday, h->d_lt, h->d_cmin, ncmin, wc, chunk, maxc, h->d_pos,
                                h->d_k8, h->d_kw);
+    h->launches += 7;   // day flags, scan (2 kernels), scatter, fill, laytrop, groups
     RAD_CUDA(h, cudaGetLastError());
     // ---- SW over the day columns; write zeros first (night columns keep them, as swrad does)
     RAD_CUDA(h, cudaMemsetAsync(out->htsw, 0, (size_t)nlay * n * sizeof(float), st));
@@ -253,10 +294,12 @@ int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int6
         lut.ex = sizeof(R) == 4 ? (const R*)h->d_swf : (const R*)h->d_swd;
         const size_t smem = sizeof(SwShared<R>);
         RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_sw<R>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if ((mrc = mark(h, st, eb, 2))) return mrc;
         sw_column_kernel<R><<<(unsigned)n, SW_THREADS, smem, st>>>(a, lut, h->d_swd, h->d_err);
+        h->launches += 1;
         RAD_CUDA(h, cudaGetLastError());
     }
-    return RAD_OK;
+    return mark(h, st, eb, 3);
 }
 }  // namespace
 
@@ -371,13 +414,37 @@ int rad_load_tables(RadHandle* h, const void* blob, size_t nbytes)
     std::vector<double> lwd, swd;
     lw_lut(lwf); lw_lut(lwd); sw_lut(swf); sw_lut(swd);
     int rc;
-    if ((rc = upload(h, &h->d_tf, hf)) || (rc = upload(h, &h->d_td, hd)) || (rc = upload(h, &h->d_lwf, lwf)) ||
-        (rc = upload(h, &h->d_lwd, lwd)) || (rc = upload(h, &h->d_swf, swf)) || (rc = upload(h, &h->d_swd, swd)))
+    if ((rc = upload(h, &h->d_lwf, lwf)) || (rc = upload(h, &h->d_lwd, lwd)) || (rc = upload(h, &h->d_swf, swf)) ||
+        (rc = upload(h, &h->d_swd, swd)))
         return rc;
-    RAD_CUDA(h, cudaMemcpyToSymbol(c_toff, off.data(), T_COUNT * sizeof(int64_t)));
-    RAD_CUDA(h, cudaMemcpyToSymbol(c_tf, &h->d_tf, sizeof(float*)));
-    RAD_CUDA(h, cudaMemcpyToSymbol(c_td, &h->d_td, sizeof(double*)));
-    RAD_CUDA(h, cudaMemcpyToSymbol(c_lwk, &k, sizeof(k)));
+    // The k-tables are read through __constant__ pointers, which are per device, not per handle: the
+    // first load on a device uploads them and sets the constants; they stay until the process exits and
+    // every later handle on that device shares them.  A later blob with different content is refused, so a
+    // handle can never leave another handle's kernels reading freed or different tables.
+    std::lock_guard<std::mutex> lock(g_tab_mu);
+    DeviceTables& dt = g_tabs[h->device];
+    if (dt.tf) {
+        if (dt.off != off || dt.hf != hf || std::memcmp(&dt.k, &k, sizeof(k)) != 0)
+            return fail(h, RAD_E_TABLES, "rad_load_tables: tables with different content are already loaded on this "
+                                         "device (one table set per device and process)");
+    } else {
+        float* tf = nullptr;
+        double* td = nullptr;
+        if ((rc = upload(h, &tf, hf)) || (rc = upload(h, &td, hd))) {
+            if (tf) cudaFree(tf);
+            return rc;
+        }
+        RAD_CUDA(h, cudaMemcpyToSymbol(c_toff, off.data(), T_COUNT * sizeof(int64_t)));
+        RAD_CUDA(h, cudaMemcpyToSymbol(c_tf, &tf, sizeof(float*)));
+        RAD_CUDA(h, cudaMemcpyToSymbol(c_td, &td, sizeof(double*)));
+        RAD_CUDA(h, cudaMemcpyToSymbol(c_lwk, &k, sizeof(k)));
+        RAD_CUDA(h, cudaDeviceSynchronize());
+        dt.tf = tf;
+        dt.td = td;
+        dt.off = off;
+        dt.hf = std::move(hf);
+        dt.k = k;
+    }
     h->tables_ok = true;
     return RAD_OK;
 }
@@ -392,8 +459,9 @@ int rad_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t
 {
     if (!h || !in || !out) return fail(h, RAD_E_INVALID, "rad_solve: null argument");
     if (!h->tables_ok) return fail(h, RAD_E_TABLES, "rad_solve: tables not loaded (rad_load_tables)");
-    if (ncol <= 0 || ncol > (int64_t)std::numeric_limits<int>::max() - 1)
+    if (ncol < 0 || ncol > (int64_t)std::numeric_limits<int>::max() - 1)
         return fail(h, RAD_E_INVALID, "rad_solve: ncol out of range");
+    if (ncol == 0) return RAD_OK;
     if (!in->plyr || !in->plvl || !in->tlyr || !in->tlvl || !in->qlyr || !in->olyr || !in->gasvmr || !in->clouds ||
         !in->sfcemis || !in->tsfg || !in->sfcalb || !in->coszen)
         return fail(h, RAD_E_INVALID, "rad_solve: a required input pointer is null");
@@ -418,12 +486,40 @@ int rad_solve_batch(RadHandle* h, int32_t nreq, const RadColumns* ins, const Rad
     return RAD_OK;
 }
 
+int rad_profile_enable(RadHandle* h, int on)
+{
+    if (!h) return fail(h, RAD_E_INVALID, "rad_profile_enable: null handle");
+    h->profiling = on != 0;
+    h->ev_used = 0;
+    h->prof_solves = h->prof_columns = 0;
+    return RAD_OK;
+}
+
+int rad_profile_read(RadHandle* h, RadProfile* p)
+{
+    if (!h || !p) return fail(h, RAD_E_INVALID, "rad_profile_read: null argument");
+    *p = RadProfile{};
+    p->launches = h->launches;
+    p->solves = h->prof_solves;
+    p->columns = h->prof_columns;
+    if (h->ev_used) RAD_CUDA(h, cudaEventSynchronize(h->ev[h->ev_used - 1]));
+    for (size_t b = 0; b + 4 <= h->ev_used; b += 4) {
+        float t[3];
+        for (int i = 0; i < 3; ++i) RAD_CUDA(h, cudaEventElapsedTime(&t[i], h->ev[b + i], h->ev[b + i + 1]));
+        p->lw_ms += t[0];
+        p->prep_ms += t[1];
+        p->sw_ms += t[2];
+    }
+    return RAD_OK;
+}
+
 const char* rad_last_error(const RadHandle* h) { return h ? h->err.c_str() : g_err.c_str(); }
 
 void rad_destroy(RadHandle* h)
 {
     if (!h) return;
-    for (void* p : {(void*)h->d_tf, (void*)h->d_td, (void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
+    for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+    for (void* p : {(void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
                     (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
                     (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub})
         if (p) cudaFree(p);

@@ -79,9 +79,7 @@ class RadSolver:
         return {k: torch.empty(s, dtype=torch.float32, device=device or "cuda")
                 for k, s in output_shapes(self.cfg.nlay, ncol).items()}
 
-    def solve(self, cols: dict, solcon: float, out: dict | None = None, stream=None) -> dict:
-        """Solve device-resident columns.  ``cols`` maps the reference names (INPUT_FIELDS, optionally
-        faerlw/faersw/icseed) to contiguous float32 CUDA tensors in [field][level][column] layout."""
+    def _abi_args(self, cols: dict, solcon: float, out: dict | None):
         torch = _torch()
         ncol = int(cols["coszen"].shape[-1])
         for k in INPUT_FIELDS:
@@ -105,10 +103,31 @@ class RadSolver:
         for k in output_shapes(1, 1):
             t = out.get(k)
             setattr(co, k, t.data_ptr() if t is not None else None)
+        return ci, co, ncol, out
+
+    def solve(self, cols: dict, solcon: float, out: dict | None = None, stream=None) -> dict:
+        """Solve device-resident columns.  ``cols`` maps the reference names (INPUT_FIELDS, optionally
+        faerlw/faersw/icseed) to contiguous float32 CUDA tensors in [field][level][column] layout."""
+        torch = _torch()
+        ci, co, ncol, out = self._abi_args(cols, solcon, out)
         st = stream if stream is not None else torch.cuda.current_stream()
         rc = self.lib.rad_solve(self.handle, ctypes.byref(ci), ctypes.byref(co), ncol, ctypes.c_void_p(st.cuda_stream))
         _lib.check(self.lib, self.handle, rc, "rad_solve")
         return out
+
+    def solve_batch(self, requests: list, solcons: list, outs: list | None = None, stream=None) -> list:
+        """Several independent requests in one call (rad_solve_batch); each keeps its own SW groups."""
+        torch = _torch()
+        n = len(requests)
+        outs = outs or [None] * n
+        args = [self._abi_args(c, s, o) for c, s, o in zip(requests, solcons, outs)]
+        ins = (_lib.RadColumns * max(n, 1))(*[a[0] for a in args])
+        ous = (_lib.RadOutputs * max(n, 1))(*[a[1] for a in args])
+        ncols = (ctypes.c_int64 * max(n, 1))(*[a[2] for a in args])
+        st = stream if stream is not None else torch.cuda.current_stream()
+        rc = self.lib.rad_solve_batch(self.handle, n, ins, ous, ncols, ctypes.c_void_p(st.cuda_stream))
+        _lib.check(self.lib, self.handle, rc, "rad_solve_batch")
+        return [a[3] for a in args]
 
     def to_device(self, columns, device="cuda", pinned: bool = False) -> dict:
         """Copy a woof_nam_b200.columns.Columns request to the device (optionally through pinned memory)."""
@@ -128,6 +147,16 @@ class RadSolver:
         out = self.solve(d, columns.solcon)
         torch.cuda.synchronize()
         return {k: v.cpu().numpy() for k, v in out.items()}
+
+    def profile(self, on: bool = True) -> None:
+        """Start (or stop) device-time accounting of the library's kernels on this handle."""
+        _lib.check(self.lib, self.handle, self.lib.rad_profile_enable(self.handle, int(on)), "rad_profile_enable")
+
+    def profile_read(self) -> dict:
+        """Kernel launches since creation and device ms of the LW / SW-prep / SW kernels since profile()."""
+        p = _lib.RadProfile()
+        _lib.check(self.lib, self.handle, self.lib.rad_profile_read(self.handle, ctypes.byref(p)), "rad_profile_read")
+        return {k: getattr(p, k) for k, _ in p._fields_}
 
     def workspace_bytes(self, ncol: int) -> int:
         return int(self.lib.rad_workspace_bytes(self.handle, ncol))
