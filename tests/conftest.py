@@ -38,14 +38,22 @@ def golden_columns(z, case: str):
 
 
 def max_errors(out: dict, ref: dict) -> dict:
-    """Largest absolute error per output: heating rates in K/day, fluxes in W/m^2."""
+    """Largest absolute error per output: heating rates in K/day, fluxes in W/m^2.  A value that is not
+    finite where the reference is finite (or the other way round) counts as an infinite error."""
     e = {}
-    for k in HEAT_KEYS:
+    for k in HEAT_KEYS + FLUX_KEYS:
         if k in out and k in ref:
-            e[k] = float(np.max(np.abs(np.asarray(out[k], np.float64) - ref[k])) * 86400.0)
-    for k in FLUX_KEYS:
-        if k in out and k in ref:
-            e[k] = float(np.max(np.abs(np.asarray(out[k], np.float64) - ref[k])))
+            o = np.asarray(out[k], np.float64)
+            r = np.asarray(ref[k], np.float64)
+            if o.size == 0:
+                e[k] = 0.0
+                continue
+            if not np.array_equal(np.isfinite(o), np.isfinite(r)):
+                e[k] = float("inf")
+                continue
+            m = np.isfinite(r)
+            d = np.abs(o[m] - r[m])
+            e[k] = float(d.max() if d.size else 0.0) * (86400.0 if k in HEAT_KEYS else 1.0)
     return e
 
 

@@ -32,6 +32,8 @@ __constant__ int c_sw_ns[15] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94
 
 #include "rad_lw.cuh"
 #include "rad_sw.cuh"
+#include "rad_sw2.cuh"
+#include "rad_lw2.cuh"
 
 using namespace rad;
 
@@ -107,7 +109,7 @@ __global__ void k_laytrop(const float* plyr, int64_t n, int nlay, const int* day
     const int64_t c = daycol[d];
     int l = nlay;
     for (int k0 = 0; k0 < nlay; ++k0)
-        if (logf(plyr[(size_t)(nlay - 1 - k0) * n + c]) > 4.56f) l = k0 + 1;
+        if (log((double)plyr[(size_t)(nlay - 1 - k0) * n + c]) > (double)4.56f) l = k0 + 1;
     lt[d] = l;
     const int w = (int)(c / wc);
     const int dw0 = pos[(int64_t)w * wc];
@@ -174,8 +176,10 @@ void sw_lut(std::vector<R>& v)   // exp_tbl(0:10000) (phys_rrtm_sw_spcvrtc.py:60
     v[n] = (R)1.0e-20f;
 }
 
+// The plain FP64 precision runs the first-design kernels (lw_column_kernel / sw_column_kernel<double>);
+// the mixed precision runs the production kernels (lw2_column_kernel<float> / sw2_column_kernel).
 template <class R>
-void* kernel_ptr_lw() { return (void*)lw_column_kernel<R>; }
+void* kernel_ptr_lw() { return sizeof(R) == 4 ? (void*)lw2_column_kernel<float> : (void*)lw_column_kernel<double>; }
 template <class R>
 void* kernel_ptr_sw() { return (void*)sw_column_kernel<R>; }
 
@@ -249,7 +253,10 @@ int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int6
         for (int64_t c0 = 0; c0 < n; c0 += maxg) {
             a.col0 = c0;
             const int64_t nb = std::min<int64_t>(maxg, n - c0);
-            lw_column_kernel<R><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
+            if (sizeof(R) == 4)
+                lw2_column_kernel<R><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
+            else
+                lw_column_kernel<R><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
             h->launches += 1;
         }
         RAD_CUDA(h, cudaGetLastError());
@@ -290,12 +297,18 @@ int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int6
         SwIn a{in->plyr, in->plvl, in->tlyr, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faersw, in->sfcalb,
                in->coszen, h->d_daycol, h->d_nday, h->d_k8, h->d_kw, out->htsw, out->topfsw, out->sfcfsw,
                out->fdncmp, n, nlay, cfg.diagnostic, cfg.iswmode, in->solcon};
-        SwLut<R> lut;
-        lut.ex = sizeof(R) == 4 ? (const R*)h->d_swf : (const R*)h->d_swd;
-        const size_t smem = sizeof(SwShared<R>);
-        RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_sw<R>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         if ((mrc = mark(h, st, eb, 2))) return mrc;
-        sw_column_kernel<R><<<(unsigned)n, SW_THREADS, smem, st>>>(a, lut, h->d_swd, h->d_err);
+        if (sizeof(R) == 4) {
+            const size_t smem = sw2_smem_bytes(in->faersw != nullptr);
+            RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            sw2_column_kernel<<<(unsigned)n, SW2_THREADS, smem, st>>>(a, h->d_swf, h->d_swd, h->d_err);
+        } else {
+            SwLut<R> lut;
+            lut.ex = (const R*)h->d_swd;
+            const size_t smem = sizeof(SwShared<R>);
+            RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_sw<R>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            sw_column_kernel<R><<<(unsigned)n, SW_THREADS, smem, st>>>(a, lut, h->d_swd, h->d_err);
+        }
         h->launches += 1;
         RAD_CUDA(h, cudaGetLastError());
     }

@@ -38,6 +38,7 @@ struct LwShared {
     R faccmb1d[NLAY_MAX + 2], faccmb2d[NLAY_MAX + 2];
     int lstu[NLAY_MAX + 2], lstd[NLAY_MAX + 2];
     double fnet[LW_WARPS][NLAY_MAX + 1];      // per-warp partial of sum_g (up - down) per level
+    double fnet2[LW_WARPS][NLAY_MAX + 1];     // second per-warp level partial (the downward sums of lw2)
     double scal[LW_WARPS][8];                 // per-warp partials: toa up, toa up clr, sfc up/dn, clr up/dn
     R secdiff[16], semiss[16];
     R stemp, pwvcm;
@@ -514,25 +515,21 @@ struct LwIn {
 };
 
 // ------------------------------------------------------------------------------------------------------
-template <class R>
-__global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(LwIn a, LwLut<R> lut, int* err)
+// Phases A and B of the LW column (everything before the sweeps), shared by the column kernels:
+// absorber amounts, cloud optics, setcoef, Planck functions, gas optics per (g, layer) and the
+// max-random overlap factors of rtrnmr, all in shared memory.  NT threads, tid = threadIdx.x.
+template <class R, int NT>
+__device__ void lw_setup(LwShared<R>& s, const LwIn& a, int64_t col, int tid)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    LwShared<R>& s = *reinterpret_cast<LwShared<R>*>(smem_raw);
     const int nlay = a.nlay, nlp1 = nlay + 1;
-    const int64_t col = a.col0 + blockIdx.x;
     const int64_t N = a.ncol;
-    const int tid = threadIdx.x;
-    if (nlay > NLAY_MAX || col >= N) {
-        if (tid == 0 && nlay > NLAY_MAX) atomicExch(err, RAD_DEV_NLAY);
-        return;
-    }
+    (void)nlp1;
     const int ilwcliq = a.diagnostic ? 0 : 1;
     const R eps = (R)1.0e-6f;
     auto IN = [&](const float* p, int lev) { return (R)__ldg(p + (size_t)lev * N + col); };
     // ---- phase A1: lwrad_prep per layer (phys_rrtm_lw_lwrad.cu:142-236), ivflip = 0, internal order
     if (tid == 0) s.tz[0] = IN(a.tlvl, nlay);
-    for (int k0 = tid; k0 < nlay; k0 += LW_THREADS) {
+    for (int k0 = tid; k0 < nlay; k0 += NT) {
         const int kin = nlay - 1 - k0;
         const R amdw = (R)28.9644 / (R)18.0154, amdo3 = (R)28.9644 / (R)47.9982;
         const R tem1g = (R)100.0 * (R)9.80665, tem2c = (R)1.0e-20 * (R)1.0e3 * (R)6.0221415e23;
@@ -612,7 +609,7 @@ __global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(LwIn a, LwLut<R> 
         const R sfe = (R)__ldg(a.sfcemis + col);
         s.semiss[tid] = (sfe > eps && sfe <= (R)1) ? sfe : (R)1;
     }
-    for (int k0 = tid; k0 < nlay; k0 += LW_THREADS) {
+    for (int k0 = tid; k0 < nlay; k0 += NT) {
         // cldprop (phys_rrtm_lw_cldprop.cu:116-232), ilwcice = 1, with the cloud-path factor
         const int kin = nlay - 1 - k0;
         auto CL = [&](int n) { return __ldg(a.clouds + ((size_t)n * nlay + kin) * N + col); };
@@ -719,7 +716,7 @@ __global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(LwIn a, LwLut<R> 
     {
         const R* totplnk = tab<R>(T_LW_TOTPLNK);
         const R* delwave = tab<R>(T_LW_DELWAVE);
-        for (int p = tid; p < nlp1 * 16; p += LW_THREADS) {
+        for (int p = tid; p < nlp1 * 16; p += NT) {
             const int k = p / 16, i = p % 16;
             const R tl = k == 0 ? (R)__ldg(a.tsfg + col) : IN(a.tlyr, nlay - k);   // layer temp (k=0: stemp)
             const R tv = k == 0 ? IN(a.tlvl, nlay) : IN(a.tlvl, nlay - k);
@@ -734,7 +731,7 @@ __global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(LwIn a, LwLut<R> 
     }
     __syncthreads();
     // ---- phase B: gas optics per (g, layer), g-major so a warp stays inside one band
-    for (int p = tid; p < LW_NGPT * nlay; p += LW_THREADS) {
+    for (int p = tid; p < LW_NGPT * nlay; p += NT) {
         const int g = p / nlay, k0 = p - g * nlay;
         R tg, fr;
         lw_gas(s, g, k0, tg, fr);
@@ -815,6 +812,23 @@ __global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(LwIn a, LwLut<R> 
         }
     }
     __syncthreads();
+}
+
+template <class R>
+__global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(LwIn a, LwLut<R> lut, int* err)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    LwShared<R>& s = *reinterpret_cast<LwShared<R>*>(smem_raw);
+    const int nlay = a.nlay;
+    const int64_t col = a.col0 + blockIdx.x;
+    const int64_t N = a.ncol;
+    const int tid = threadIdx.x;
+    if (nlay > NLAY_MAX || col >= N) {
+        if (tid == 0 && nlay > NLAY_MAX) atomicExch(err, RAD_DEV_NLAY);
+        return;
+    }
+    lw_setup<R, LW_THREADS>(s, a, col, tid);
+    const R eps = (R)1.0e-6f;
     // ---- phase C: rtrnmr sweeps, one g-point per lane
     const int warp = tid >> 5, lane = tid & 31;
     const int g = tid;

@@ -60,11 +60,15 @@ struct SwLut {
     const R* ex;             // exp_tbl(0:10000) of rswinit
 };
 
+// Key-species counts of the lower / upper atmosphere k-tables per SW band (taumol16..29: nspa, nspb).
+__constant__ int c_sw_nspa[14] = {9, 9, 9, 9, 1, 9, 9, 1, 9, 1, 0, 1, 9, 1};
+__constant__ int c_sw_nspb[14] = {1, 5, 1, 1, 1, 5, 1, 0, 1, 0, 0, 1, 5, 1};
+
 // ------------------------------------------------------------------------------------------------------
 // Gas and Rayleigh optical depths of SW g-point g (0..111) at layer k0 (phys_rrtm_sw_taumol16..29.cu with
 // the reference's handling of the layer k = laytrop).
-template <class R>
-__device__ void sw_gas(const SwShared<R>& s, int g, int k0, R& tg, R& tr)
+template <class R, class S>
+__device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr)
 {
     const int k = k0 + 1, lt = s.laytrop;
     const int jpk = s.jp[k0], jtk = s.jt[k0], jt1k = s.jt1[k0];
@@ -79,11 +83,9 @@ __device__ void sw_gas(const SwShared<R>& s, int g, int k0, R& tg, R& tr)
     while (g >= c_sw_ns[b + 1]) ++b;
     const int ig = g - c_sw_ns[b], jb = b + 16;
     auto idx = [&](int jbb, int& id0, int& id1) {
-        const int nspa[14] = {9, 9, 9, 9, 1, 9, 9, 1, 9, 1, 0, 1, 9, 1};
-        const int nspb[14] = {1, 5, 1, 1, 1, 5, 1, 0, 1, 0, 0, 1, 5, 1};
         const int bb = jbb - 16;
-        if (k <= lt) { id0 = ((jpk - 1) * 5 + (jtk - 1)) * nspa[bb]; id1 = (jpk * 5 + (jt1k - 1)) * nspa[bb]; }
-        else { id0 = ((jpk - 13) * 5 + (jtk - 1)) * nspb[bb]; id1 = ((jpk - 12) * 5 + (jt1k - 1)) * nspb[bb]; }
+        if (k <= lt) { id0 = ((jpk - 1) * 5 + (jtk - 1)) * c_sw_nspa[bb]; id1 = (jpk * 5 + (jt1k - 1)) * c_sw_nspa[bb]; }
+        else { id0 = ((jpk - 13) * 5 + (jtk - 1)) * c_sw_nspb[bb]; id1 = ((jpk - 12) * 5 + (jt1k - 1)) * c_sw_nspb[bb]; }
     };
     auto sum8 = [&](const R* A, int ng, int msa, int id0, int id1, int js, R fs, int o1, int o2) {
         const R fs1 = (R)1 - fs;
@@ -304,10 +306,10 @@ __device__ void sw_gas(const SwShared<R>& s, int g, int k0, R& tg, R& tr)
         const int i1 = low ? jpk * 5 + (jt1k - 1) : (jpk - 12) * 5 + (jt1k - 1);
         if (low) {
             const int indsp = min(inds + 1, 10), indfp = min(indf + 1, 4);
-            const R* S = tab<R>(T_SW29_SELFREF);
-            const R* F = tab<R>(T_SW29_FORREF);
-            auto Sv = [&](int i) { return ldt(S + (size_t)(i - 1) * NG + ig); };
-            auto Fv = [&](int i) { return ldt(F + (size_t)(i - 1) * NG + ig); };
+            const R* Sref = tab<R>(T_SW29_SELFREF);
+            const R* Fref = tab<R>(T_SW29_FORREF);
+            auto Sv = [&](int i) { return ldt(Sref + (size_t)(i - 1) * NG + ig); };
+            auto Fv = [&](int i) { return ldt(Fref + (size_t)(i - 1) * NG + ig); };
             tg = c1 * ((sum4(tab<R>(T_SW29_ABSA), NG, 65, i0, i1)) + sfac * (Sv(inds) + sfrac * (Sv(indsp) - Sv(inds))) +
                        ffac * (Fv(indf) + ffrac * (Fv(indfp) - Fv(indf)))) + c2 * ldt(tab<R>(T_SW29_ABSCO2) + ig);
         } else {
@@ -315,6 +317,49 @@ __device__ void sw_gas(const SwShared<R>& s, int g, int k0, R& tg, R& tr)
         }
         break;
     }
+    }
+}
+
+// Solar source of band b (taumol.cu:59-120): sfluxzen of the band's g-points from the reference solar
+// source at the layer the band's interpolation uses.
+template <class R, class S>
+__device__ void sw_sfluxzen(S& s, int b, int nlay)
+{
+    const int jb = b + 16, lt = s.laytrop;
+    const int ibd = (int)ldt(tab<R>(T_SW_IBX) + b), njb = c_sw_ns[b + 1] - c_sw_ns[b], ns = c_sw_ns[b];
+    const int lr = (int)ldt(tab<R>(T_SW_LAYREFFR) + b);
+    const R* sf01 = tab<R>(T_SW_SFLUXREF01);
+    if (jb == 16 || jb == 20 || jb == 23 || jb == 25 || jb == 26 || jb == 29 || jb == 27) {
+        const R scl = jb == 27 ? ldt(tab<R>(T_SW_SCALEKUR)) : (R)1;
+        for (int j = 0; j < njb; ++j) {
+            const R v = ldt(sf01 + (ibd - 1) * 16 + j);
+            s.sfluxzen[ns + j] = jb == 27 ? scl * v : v;
+        }
+    } else {
+        int ks;
+        const bool two = (jb == 17 || jb == 28);
+        if (two) {
+            ks = nlay;
+            for (int k = lt; k <= nlay - 1; ++k)
+                if (s.jp[k - 1] < lr && s.jp[k] >= lr) { ks = k + 1; break; }
+        } else {
+            ks = lt;
+            for (int k = 1; k <= lt - 1; ++k)
+                if (s.jp[k - 1] < lr && s.jp[k] >= lr) { ks = k + 1; break; }
+        }
+        const int ix1 = (int)ldt(tab<R>(T_SW_IX1) + b), ix2 = (int)ldt(tab<R>(T_SW_IX2) + b);
+        const R colm1 = s.colamt[ix1 - 1][ks - 1], colm2 = s.colamt[ix2 - 1][ks - 1];
+        const R sc = colm1 + ldt(tab<R>(T_SW_STRRAT) + b) * colm2;
+        const R sm = ldt(tab<R>(T_SW_SPECWT) + b) * fminR((R)0.999999f, colm1 / sc);
+        const int jsi = (int)sm;
+        const int js = 1 + jsi;
+        const R fs = sm - (R)jsi;
+        const R* sf = tab<R>(two ? T_SW_SFLUXREF02 : T_SW_SFLUXREF03);
+        const int base = ((ibd - 1) * (two ? 5 : 9)) * 16;
+        for (int j = 0; j < njb; ++j) {
+            const R x0 = ldt(sf + base + (js - 1) * 16 + j), x1 = ldt(sf + base + js * 16 + j);
+            s.sfluxzen[ns + j] = x0 + fs * (x1 - x0);
+        }
     }
 }
 
@@ -660,44 +705,7 @@ __global__ void __launch_bounds__(SW_THREADS) sw_column_kernel(SwIn a, SwLut<R> 
         s.taucw[ib][k0] = tcw; s.ssacw[ib][k0] = scw; s.asycw[ib][k0] = acw;
         if (ib == 0) s.cldfrc[k0] = s.zcf1 > 0 ? s.cfrac[k0] / s.zcf1 : (R)0;
     }
-    if (tid < 14) {   // sfluxzen of band tid (taumol.cu:59-120)
-        const int b = tid, jb = b + 16, lt = s.laytrop;
-        const int ibd = (int)ldt(tab<R>(T_SW_IBX) + b), njb = c_sw_ns[b + 1] - c_sw_ns[b], ns = c_sw_ns[b];
-        const int lr = (int)ldt(tab<R>(T_SW_LAYREFFR) + b);
-        const R* sf01 = tab<R>(T_SW_SFLUXREF01);
-        if (jb == 16 || jb == 20 || jb == 23 || jb == 25 || jb == 26 || jb == 29 || jb == 27) {
-            const R scl = jb == 27 ? ldt(tab<R>(T_SW_SCALEKUR)) : (R)1;
-            for (int j = 0; j < njb; ++j) {
-                const R v = ldt(sf01 + (ibd - 1) * 16 + j);
-                s.sfluxzen[ns + j] = jb == 27 ? scl * v : v;
-            }
-        } else {
-            int ks;
-            const bool two = (jb == 17 || jb == 28);
-            if (two) {
-                ks = nlay;
-                for (int k = lt; k <= nlay - 1; ++k)
-                    if (s.jp[k - 1] < lr && s.jp[k] >= lr) { ks = k + 1; break; }
-            } else {
-                ks = lt;
-                for (int k = 1; k <= lt - 1; ++k)
-                    if (s.jp[k - 1] < lr && s.jp[k] >= lr) { ks = k + 1; break; }
-            }
-            const int ix1 = (int)ldt(tab<R>(T_SW_IX1) + b), ix2 = (int)ldt(tab<R>(T_SW_IX2) + b);
-            const R colm1 = s.colamt[ix1 - 1][ks - 1], colm2 = s.colamt[ix2 - 1][ks - 1];
-            const R sc = colm1 + ldt(tab<R>(T_SW_STRRAT) + b) * colm2;
-            const R sm = ldt(tab<R>(T_SW_SPECWT) + b) * fminR((R)0.999999f, colm1 / sc);
-            const int jsi = (int)sm;
-            const int js = 1 + jsi;
-            const R fs = sm - (R)jsi;
-            const R* sf = tab<R>(two ? T_SW_SFLUXREF02 : T_SW_SFLUXREF03);
-            const int base = ((ibd - 1) * (two ? 5 : 9)) * 16;
-            for (int j = 0; j < njb; ++j) {
-                const R x0 = ldt(sf + base + (js - 1) * 16 + j), x1 = ldt(sf + base + js * 16 + j);
-                s.sfluxzen[ns + j] = x0 + fs * (x1 - x0);
-            }
-        }
-    }
+    if (tid < 14) sw_sfluxzen<R>(s, tid, nlay);
     __syncthreads();
     // ---- phase B: gas and Rayleigh optical depths per (g, layer), g-major
     for (int p = tid; p < SW_NGPT * nlay; p += SW_THREADS) {

@@ -1,0 +1,681 @@
+// rad_sw2.cuh -- the production SW column kernel for sm_100a (mixed precision).
+//
+// Same column physics as rad_sw.cuh (swrad prep, cldprop, setcoef, taumol16..29, spcvrtc + swflux,
+// namgpu/kernels/phys_rrtm_sw_*.cu), organised for throughput:
+//
+//  * 256 threads per sunlit column.  Phase A: threads = layers / (band, layer) pairs / bands build the
+//    layer coefficients, cloud optics and solar source in shared memory.  Phase B: threads = (g, layer)
+//    pairs in g-major order compute the gas and Rayleigh optical depths once (a warp stays inside one
+//    band, so the band switch does not diverge).  Phase C: warps 0-3 run the clear pass and warps 4-7 the
+//    cloudy pass of spcvrtc, one g-point per lane (28/28/30/26 lanes per warp, the Rayleigh-dominated
+//    bands 23-26 grouped in one warp).
+//  * No per-thread layer arrays.  The adding method needs the upward reflectances of every level while
+//    it walks down; the upward sweep keeps only one checkpoint per segment of SEG layers (shared memory),
+//    and the downward sweep recomputes each segment's layer R/T into registers before walking through it.
+//  * Level fluxes are summed over the g-points of a warp in float64 (shuffles) and over warps in a fixed
+//    order: results are bit-reproducible and do not depend on what else runs on the GPU.
+//
+// Precision (mixed):
+//  * The layer R/T (sw2_rt) is an algebraically equal rearrangement of the reference's statements that
+//    float evaluates accurately: co-albedo carried from the optics (no 1 - ssa cancellation), the
+//    complements 1 - exp(-x) carried next to exp(-x), and exp(-k tau) multiplied through instead of
+//    divided (the reference's float form overflows and returns NaN once k tau > ~88).  Near-conservative
+//    and thin layers need no float64.
+//  * Within 1 % of the two-stream resonance k mu0 = 1 the reference's formula divides two small
+//    quantities, clamps 1 - (k mu0)^2 at 1e-8 and compares exp-table entries of two nearly equal depths;
+//    there the layer's optical properties are recomputed from the column inputs in float64 (prep,
+//    setcoef, gas, aerosol and cloud optics) and the reference's statements are evaluated in float64, so
+//    the result follows the reference's own arithmetic (about 0.4 % of the layer evaluations).
+//  * Flux sums over g-points and bands and the heating-rate flux differences are float64.
+#pragma once
+#include "rad_sw.cuh"
+
+namespace rad {
+
+constexpr int SW2_WARPS = 8, SW2_THREADS = 256;
+#ifndef RAD_SW2_SEG
+#define RAD_SW2_SEG 4
+#endif
+constexpr int SW2_SEG = RAD_SW2_SEG;                              // layers per checkpoint segment
+constexpr int SW2_NSEG = (NLAY_MAX + SW2_SEG - 1) / SW2_SEG;
+constexpr float SW2_RESONANCE = 1.0e-2f;                          // exact recompute where |1-(k mu0)^2| < this
+
+// Rain and snow optical coefficients per SW band (phys_rrtm_sw_cldprop.cu): b0r, c0r, b0s, b1s, c0s.
+__constant__ float c_sw_rain_snow[5][14] = {
+    {0.466f, 0.437f, 0.416f, 0.391f, 0.374f, 0.352f, 0.183f, 0.048f, 0.012f, 0.000f, 0.000f, 0.000f, 0.000f, 0.496f},
+    {0.975f, 0.965f, 0.960f, 0.955f, 0.952f, 0.950f, 0.944f, 0.894f, 0.884f, 0.883f, 0.883f, 0.883f, 0.883f, 0.980f},
+    {0.460f, 0.460f, 0.460f, 0.460f, 0.460f, 0.460f, 0.460f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.460f},
+    {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 1.62e-5f, 1.62e-5f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {0.970f, 0.970f, 0.970f, 0.970f, 0.970f, 0.970f, 0.970f, 0.970f, 0.970f, 0.700f, 0.700f, 0.700f, 0.700f, 0.970f}};
+
+template <class T>
+struct One {   // a scalar read through the array syntax of the shared-memory layer arrays
+    T v;
+    __device__ __forceinline__ T operator[](int) const { return v; }
+};
+
+// One layer after swrad_prep + setcoef (swrad.cu:166-240, setcoef.cu:17-97).
+template <class R>
+struct SwCoef {
+    R fac00, fac01, fac10, fac11, selffac, selffrac, forfac, forfrac, colmol;
+    R colamt[6];
+    int jp, jt, jt1, indself, indfor;
+    bool low;   // ln(p) > 4.56, decided in float64 for every precision
+};
+
+template <class R>
+__device__ void sw2_layer_coef(const SwIn& a, int64_t col, int k0, SwCoef<R>& c)
+{
+    const int nlay = a.nlay;
+    const int64_t N = a.ncol;
+    const int kk0 = nlay - 1 - k0;
+    auto IN = [&](const float* p, int lev) { return (R)__ldg(p + (size_t)lev * N + col); };
+    const R amdw = (R)28.9644f / (R)18.0154f, amdo3 = (R)28.9644f / (R)47.9982f;
+    const R tem1 = (R)100.0f * (R)9.80665f, tem2 = (R)1.0e-20f * (R)1.0e3f * (R)6.0221415e23f;
+    const float pin = __ldg(a.plyr + (size_t)kk0 * N + col);
+    const R pav = (R)pin, tav = IN(a.tlyr, kk0);
+    const R dl = IN(a.plvl, kk0 + 1) - IN(a.plvl, kk0);
+    const R qv = IN(a.qlyr, kk0), ov = IN(a.olyr, kk0);
+    const R h2o = fmaxR((R)0, qv * amdw / ((R)1 - qv));
+    const R o3 = fmaxR((R)0, ov * amdo3);
+    const R tem0 = ((R)1 - h2o) * (R)28.9644f + h2o * (R)18.0154f;
+    const R cd = tem2 * dl / (tem1 * tem0 * ((R)1 + h2o));
+    const R tc = (R)1.0e-12f * cd;
+    auto G = [&](int n) { return (R)__ldg(a.gasvmr + ((size_t)n * nlay + kk0) * N + col); };
+    c.colamt[0] = fmaxR((R)0, cd * h2o);
+    c.colamt[1] = fmaxR(tc, cd * G(0));
+    c.colamt[2] = fmaxR((R)0, cd * o3);
+    c.colmol = cd + c.colamt[0];
+    c.colamt[3] = fmaxR(tc, cd * G(1));
+    c.colamt[4] = fmaxR(tc, cd * G(2));
+    c.colamt[5] = fmaxR(tc, cd * G(3));
+    const R forf = pav * ((R)296.0f / (R)1013.0f) / (tav * ((R)1 + h2o));
+    c.forfac = forf;
+    const R plog = rlog(pav);
+    const int jpk = max(1, min(58, (int)((R)36 - (R)5 * (plog + (R)0.04f))));
+    const int jp1 = jpk + 1;
+    const R* preflog = tab<R>(T_SW_PREFLOG);
+    const R* tref = tab<R>(T_SW_TREF);
+    const R fp = (R)5 * (ldt(preflog + jpk - 1) - plog);
+    const R t1 = (tav - ldt(tref + jpk - 1)) / (R)15, t2 = (tav - ldt(tref + jp1 - 1)) / (R)15;
+    const int jtk = max(1, min(4, (int)((R)3 + t1))), jt1k = max(1, min(4, (int)((R)3 + t2)));
+    const R ft = t1 - (R)(jtk - 3), ft1 = t2 - (R)(jt1k - 3);
+    c.jp = jpk; c.jt = jtk; c.jt1 = jt1k;
+    const R fp1 = (R)1 - fp;
+    c.fac10 = fp1 * ft;
+    c.fac00 = fp1 * ((R)1 - ft);
+    c.fac11 = fp * ft1;
+    c.fac01 = fp * ((R)1 - ft1);
+    c.low = log((double)pin) > (double)4.56f;
+    if (c.low) {
+        const R tem1f = ((R)332 - tav) / (R)36;
+        const int indf = min(2, max(1, (int)tem1f));
+        c.indfor = indf;
+        c.forfrac = tem1f - (R)indf;
+        const R tem2s = (tav - (R)188) / (R)7.2f;
+        const int inds = min(9, max(1, (int)tem2s - 7));
+        c.indself = inds;
+        c.selffrac = tem2s - (R)(inds + 7);
+        c.selffac = h2o * forf;
+    } else {
+        const R tem1f = (tav - (R)188) / (R)36;
+        c.indfor = 3;
+        c.forfrac = tem1f - (R)1;
+        c.indself = 0;
+        c.selffrac = 0;
+        c.selffac = 0;
+    }
+}
+
+// Cloud optics of band ib in layer k0 (phys_rrtm_sw_cldprop.cu: iswcliq = 1 with the liquid table,
+// iswcice = 3, rain and snow; iswcliq = 0: optical depth, SSA and asymmetry given directly).  Besides the
+// reference's tau, tau*ssa and tau*ssa*g it returns the absorption optical depth tau*(1-ssa) formed from
+// the co-albedos of the tables (no 1 - ssa cancellation).
+template <class R>
+__device__ void sw2_cloud(const SwIn& a, int64_t col, int k0, int ib, R cf, R& tcw, R& scw, R& acw, R& tabs)
+{
+    const int nlay = a.nlay;
+    const int64_t N = a.ncol;
+    const int kk0 = nlay - 1 - k0;
+    auto CLD = [&](int n) { return (R)__ldg(a.clouds + ((size_t)n * nlay + kk0) * N + col); };
+    const R ftiny = (R)1.0e-12f;
+    tcw = 0; scw = 1; acw = 0; tabs = 0;
+    if (!(cf > ftiny)) return;
+    if (!a.diagnostic) {
+        const float* b0r = c_sw_rain_snow[0];
+        const float* c0r = c_sw_rain_snow[1];
+        const float* b0s = c_sw_rain_snow[2];
+        const float* b1s = c_sw_rain_snow[3];
+        const float* c0s = c_sw_rain_snow[4];
+        const R cldran = CLD(5), cldsnw = CLD(7), refsnw = CLD(8);
+        const R dgesnw = (R)1.0315f * refsnw;
+        const R tauran = cldran * (R)3.07e-3f;
+        const R tausnw = (cldsnw > 0 && refsnw > (R)10) ? cldsnw * (R)1.09087f * ((R)0 + (R)1.5f / dgesnw) : (R)0;
+        const R ssaran = tauran * ((R)1 - (R)b0r[ib]);
+        const R wsnw = (R)b0s[ib] + (R)b1s[ib] * dgesnw;
+        const R ssasnw = tausnw * ((R)1 - wsnw);
+        const R asyran = ssaran * (R)c0r[ib], asysnw = ssasnw * (R)c0s[ib];
+        const R cldliq = CLD(1), refliq = CLD(2), cldice = CLD(3), refice = CLD(4);
+        R tl = 0, sl = 0, al = 0, ti = 0, si = 0, ai = 0, bl = 0, bi = 0;
+        // interpolated SSA and its co-albedo (1 - v0) - f (v1 - v0), both clamped to [0, 1]
+        auto ssa_w = [&](const R* t, int i, R f, R& ssa, R& w) {
+            const R v0 = ldt(t + i - 1), v1 = ldt(t + i), dv = v1 - v0;
+            ssa = fmaxR((R)0, fminR((R)1, v0 + f * dv));
+            w = fmaxR((R)0, fminR((R)1, ((R)1 - v0) - f * dv));
+        };
+        if (!(cldliq <= 0)) {
+            const R factor = refliq - (R)1.5f;
+            const int index = max(1, min(57, (int)factor));
+            const R fint = factor - (R)index;
+            const R *e = tab<R>(T_SW_EXTLIQ1) + ib * 58, *sv = tab<R>(T_SW_SSALIQ1) + ib * 58, *av = tab<R>(T_SW_ASYLIQ1) + ib * 58;
+            const R ext = fmaxR((R)0, ldt(e + index - 1) + fint * (ldt(e + index) - ldt(e + index - 1)));
+            R ssa, w;
+            ssa_w(sv, index, fint, ssa, w);
+            const R asy = fmaxR((R)0, fminR((R)1, ldt(av + index - 1) + fint * (ldt(av + index) - ldt(av + index - 1))));
+            tl = cldliq * ext; sl = tl * ssa; al = sl * asy; bl = tl * w;
+        }
+        if (!(cldice <= 0)) {
+            const R dge = fmaxR((R)5, fminR((R)140, (R)1.0315f * refice));
+            const R factor = (dge - (R)2) / (R)3;
+            const int index = max(1, min(45, (int)factor));
+            const R fint = factor - (R)index;
+            const R *e = tab<R>(T_SW_EXTICE3) + ib * 46, *sv = tab<R>(T_SW_SSAICE3) + ib * 46, *av = tab<R>(T_SW_ASYICE3) + ib * 46;
+            const R ext = fmaxR((R)0, ldt(e + index - 1) + fint * (ldt(e + index) - ldt(e + index - 1)));
+            R ssa, w;
+            ssa_w(sv, index, fint, ssa, w);
+            const R asy = fmaxR((R)0, fminR((R)1, ldt(av + index - 1) + fint * (ldt(av + index) - ldt(av + index - 1))));
+            ti = cldice * ext; si = ti * ssa; ai = si * asy; bi = ti * w;
+        }
+        tcw = tl + ti + tauran + tausnw;
+        scw = sl + si + ssaran + ssasnw;
+        acw = al + ai + asyran + asysnw;
+        tabs = bl + bi + tauran * (R)b0r[ib] + tausnw * wsnw;
+    } else {
+        const R t = CLD(1), w = CLD(2);
+        tcw = t;
+        scw = t * w;
+        acw = scw * CLD(3);
+        tabs = t * ((R)1 - w);
+    }
+}
+
+// Layer coefficients of one layer in float64, read with the shared-memory array syntax by sw_gas.
+struct SwOne {
+    One<double> fac00, fac01, fac10, fac11, selffac, selffrac, forfac, forfrac, colmol;
+    One<double> colamt[6];
+    One<int> jp, jt, jt1, indself, indfor;
+    int laytrop, kmin8, kminw;
+};
+
+// ------------------------------------------------------------------------------------------------------
+// exp(-zb) as sw_expm evaluates it, together with its complement 1 - exp(-zb) formed without cancellation
+// (below 0.06 the reference's expansion 1 - zb + zb^2/2, whose complement is zb - zb^2/2).
+template <class T>
+__device__ __forceinline__ T sw2_expm_c(T zb, const T* ex, T& em)
+{
+    if (zb <= (T)0.06f) {
+        em = zb - (T)0.5f * zb * zb;
+        return (T)1 - zb + (T)0.5f * zb * zb;
+    }
+    const T e = sw_expm(zb, ex, false);
+    em = (T)1 - e;
+    return e;
+}
+
+// Layer R/T (spcvrtc.cu:112-173) from (tau, absorption tau, scattering tau, scattering tau x g), equal to
+// the reference's statements in exact arithmetic and accurate in float:
+//  * co-albedo w = tau_abs / tau, so g1 - g2 = 2 w / (1 - zssaw g^2) (PIFM; sqrt(3) w / ... for the
+//    discrete-ordinates mode) and g1 - k = g2^2 / (g1 + k) carry no cancellation;
+//  * with e1 = exp(-k tau1), e2 = exp(-tau1 / mu0) and their complements m1 = 1 - e1, m2 = 1 - e2, the
+//    reference's ze1r45 * e1 = (1 - (k mu0)^2) B with B = k (1 + e1^2) + g1 (1 - e1^2), and its
+//    numerators become  rb: (1-e1^2)(a2 - k g3 k mu0) + k (g3 - a2 mu0)(m1^2 + 2 e1 m2)
+//                       tb: e2 + [k (g4 + a1 mu0)(2 e1 m2 - e2 m1^2) - e2 (1-e1^2)(a1 + k g4 k mu0)] / ...
+//    so thin and near-conservative layers (k tau1 -> 0) keep their accuracy;  rd = g2 (1-e1^2) / B,
+//    td = 2 k e1 / B;
+//  * finite for any optical depth (the reference's float form overflows 1/exp(-k tau) beyond ~88).
+// zrpp_raw returns 1 - (k mu0)^2 before the reference's 1e-8 clamp.
+template <class T>
+__device__ __forceinline__ void sw2_rt(T ztau0, T tabs, T zssa0, T zasy0, int mode, T cz, T snt, const T* ex,
+                                       T& rb, T& rd, T& tb, T& td, T& ztau1, T& zrpp_raw)
+{
+    const T ftiny = (T)1.0e-12f, eps1 = (T)1.0e-8f;
+    const T cwmin = (T)(1.0 - ((double)1.0f - (double)1.0e-6f));   // 1 - min(oneminus, ssa) bound of FP64
+    const T cw = fmaxR(cwmin, tabs / ztau0);
+    const T zssaw = (T)1 - cw;
+    const T zasyw = zasy0 / fmaxR(ftiny, zssa0);
+    const T za2s = zssaw * (zasyw * zasyw);
+    const T om = (T)1 - za2s;
+    ztau1 = om * ztau0;
+    const T zssa1 = (zssaw - za2s) / om, cw1 = cw / om;
+    const T zasy1 = zasyw / ((T)1 + zasyw), zasy3 = (T)0.75f * zasy1;
+    T g1, g2, g3, gm, gp;
+    if (mode == 2) {
+        g1 = (T)2 - zssa1 * ((T)1.25f + zasy3);
+        g2 = (T)0.75f * zssa1 * ((T)1 - zasy1);
+        g3 = (T)0.5f - zasy3 * cz;
+        gm = (T)2 * cw1;
+        gp = (T)2 - zssa1 * ((T)0.5f + (T)1.5f * zasy1);
+    } else if (mode == 1) {
+        g1 = (T)1.75f - zssa1 * ((T)1 + zasy3);
+        g2 = (T)-0.25f - zssa1 * ((T)1 - zasy3);
+        g3 = (T)0.5f - zasy3 * cz;
+        gm = g1 - g2;
+        gp = g1 + g2;
+    } else {
+        const T zsr3 = (T)1.7320508f;
+        g1 = zsr3 * ((T)2 - zssa1 * ((T)1 + zasy1)) * (T)0.5f;
+        g2 = zsr3 * zssa1 * ((T)1 - zasy1) * (T)0.5f;
+        g3 = ((T)1 - zsr3 * zasy1 * cz) * (T)0.5f;
+        gm = zsr3 * cw1;
+        gp = zsr3 * ((T)1 - zssa1 * zasy1);
+    }
+    const T g4 = (T)1 - g3;
+    const T zrk = sqrtR(gm * gp);
+    const T zrp = zrk * cz;
+    T zrpp = ((T)1 - zrp) * ((T)1 + zrp);
+    zrpp_raw = zrpp;
+    if (fabs(zrpp) < eps1) zrpp = zrpp < 0 ? -eps1 : eps1;
+    const T za1 = g1 * g4 + g2 * g3, za2 = g1 * g3 + g2 * g4;
+    T em1, em2;
+    const T e1 = sw2_expm_c(fminR(zrk * ztau1, (T)500), ex, em1);
+    const T e2 = sw2_expm_c(fminR(ztau1 * snt, (T)500), ex, em2);
+    const T e11 = e1 * e1, em11 = em1 * ((T)2 - em1);
+    const T B = zrk * ((T)1 + e11) + g1 * em11;
+    const T D = zrpp * B;                                        // (reference ze1r45) * exp(-k tau)
+    if (D >= -eps1 * e1 && D <= eps1 * e1) {
+        rb = eps1;
+        tb = e2;
+    } else {
+        const T q = zssa1 / D;
+        const T nr = em11 * (za2 - zrk * g3 * zrp) + zrk * (g3 - za2 * cz) * (em1 * em1 + (T)2 * e1 * em2);
+        const T nt = zrk * (g4 + za1 * cz) * ((T)2 * e1 * em2 - e2 * em1 * em1) - e2 * em11 * (za1 + zrk * g4 * zrp);
+        rb = fmaxR((T)0, fminR((T)1, nr * q));
+        tb = fmaxR((T)0, fminR((T)1, e2 + nt * q));
+    }
+    rd = fmaxR((T)0, fminR((T)1, g2 * em11 / B));
+    td = fmaxR((T)0, fminR((T)1, (T)2 * zrk * e1 / B));
+}
+
+// ------------------------------------------------------------------------------------------------------
+// Shared memory of one sunlit column.
+struct SwSh2 {
+    float fac00[NLAY_MAX], fac01[NLAY_MAX], fac10[NLAY_MAX], fac11[NLAY_MAX];
+    float selffac[NLAY_MAX], selffrac[NLAY_MAX], forfac[NLAY_MAX], forfrac[NLAY_MAX], colmol[NLAY_MAX];
+    float colamt[6][NLAY_MAX];
+    int jp[NLAY_MAX], jt[NLAY_MAX], jt1[NLAY_MAX], indself[NLAY_MAX], indfor[NLAY_MAX];
+    float cfrac[NLAY_MAX], cldfrc[NLAY_MAX];
+    float taucw[14][NLAY_MAX], ssacw[14][NLAY_MAX], asycw[14][NLAY_MAX], tabsc[14][NLAY_MAX];
+    float taug[SW_NGPT][NLAY_MAX], taur[SW_NGPT][NLAY_MAX];
+    float sfluxzen[SW_NGPT];
+    double rdelp[NLAY_MAX];                    // heatfac / delp, float64
+    double fn[SW2_WARPS][NLAY_MAX + 2];        // per-warp level sums of zsolar * (down - up)
+    double sc[SW2_WARPS][10];                  // per-warp scalar sums
+    float cosz, sntz, ssolar, albbm[2], albdf[2], zcf0, zcf1;
+    int laytrop, kmin8, kminw;
+    unsigned char low[NLAY_MAX];
+};
+// Dynamic tail: the aerosol block (present only with aerosol inputs) and the segment checkpoints.
+struct SwAer {
+    float tau[14][NLAY_MAX], tasa[14][NLAY_MAX], tay[14][NLAY_MAX], tabs[14][NLAY_MAX];
+};
+__host__ __device__ constexpr size_t sw2_ckpt_bytes() { return (size_t)(SW2_NSEG - 1) * 2 * SW2_THREADS * sizeof(float); }
+__host__ __device__ constexpr size_t sw2_smem_bytes(bool aer)
+{
+    return sizeof(SwSh2) + (aer ? sizeof(SwAer) : 0) + sw2_ckpt_bytes();
+}
+
+struct SwLayerRT {
+    float rb, rd, tb, td, e3, e4;
+};
+
+// Everything the float64 recompute of a layer needs besides the layer index and g-point.
+struct SwExactCtx {
+    const SwIn* a;
+    int64_t col;
+    int laytrop, kmin8, kminw, mode;
+    double cz, snt;
+    const double* exd;
+};
+
+// The layer's clear (cloud = false) or cloud-mixture optical properties recomputed from the column
+// inputs in float64, then the reference's R/T statements in float64 (spcvrtc.cu:112-173 via sw_rt).
+__device__ __noinline__ void sw2_exact(const SwExactCtx& x, int k0, int g, int ib, bool cloud, double& rb,
+                                       double& rd, double& tb, double& td, double& e3, double& e4)
+{
+    const SwIn& a = *x.a;
+    SwCoef<double> c;
+    sw2_layer_coef<double>(a, x.col, k0, c);
+    SwOne L;
+    L.fac00.v = c.fac00; L.fac01.v = c.fac01; L.fac10.v = c.fac10; L.fac11.v = c.fac11;
+    L.selffac.v = c.selffac; L.selffrac.v = c.selffrac; L.forfac.v = c.forfac; L.forfrac.v = c.forfrac;
+    L.colmol.v = c.colmol;
+    for (int m = 0; m < 6; ++m) L.colamt[m].v = c.colamt[m];
+    L.jp.v = c.jp; L.jt.v = c.jt; L.jt1.v = c.jt1; L.indself.v = c.indself; L.indfor.v = c.indfor;
+    L.laytrop = x.laytrop; L.kmin8 = x.kmin8; L.kminw = x.kminw;
+    double tg, tr;
+    sw_gas<double>(L, g, k0, tg, tr);
+    double ta = 0, sa = 0, ya = 0;
+    const int64_t N = a.ncol;
+    const int kk0 = a.nlay - 1 - k0;
+    if (a.faersw) {
+        ta = (double)__ldg(a.faersw + (((size_t)ib) * a.nlay + kk0) * N + x.col);
+        sa = (double)__ldg(a.faersw + (((size_t)(14 + ib)) * a.nlay + kk0) * N + x.col);
+        ya = (double)__ldg(a.faersw + (((size_t)(28 + ib)) * a.nlay + kk0) * N + x.col);
+    }
+    double t0 = fmax((double)1.0e-12f, tr + tg + ta), s0 = tr + ta * sa, y0 = ya * sa * ta;
+    if (cloud) {
+        const double cf = (double)__ldg(a.clouds + (size_t)kk0 * N + x.col);
+        double tc, sc, ac, tb_;
+        sw2_cloud<double>(a, x.col, k0, ib, cf, tc, sc, ac, tb_);
+        t0 = t0 + tc; s0 = s0 + sc; y0 = y0 + ac;
+    }
+    const double oneminus = (double)1.0f - (double)1.0e-6f, ftiny = (double)1.0e-12f;
+    const double zssaw = fmin(oneminus, s0 / t0);
+    const double zasyw = y0 / fmax(ftiny, s0);
+    const double za1s = zasyw * zasyw, za2s = zssaw * za1s;
+    const double ztau1 = (1.0 - za2s) * t0;
+    const double zssa1 = (zssaw - za2s) / (1.0 - za2s);
+    const double zasy1 = zasyw / (1.0 + zasyw), zasy3 = 0.75 * zasy1;
+    double g1, g2, g3;
+    sw_gam<double>(x.mode, zssa1, zasy1, zasy3, x.cz, g1, g2, g3);
+    sw_rt<double, false>(ztau1, zssaw, zssa1, g1, g2, g3, 1.0 - g3, x.cz, x.snt, x.exd, rb, rd, tb, td);
+    e3 = sw_expm(ztau1 * x.snt, x.exd, true);
+    e4 = sw_expm(t0 * x.snt, x.exd, true);
+}
+
+// One optical-property set of a layer -> R/T and direct transmissions: float, or the exact float64
+// recompute near the resonance.
+__device__ __forceinline__ void sw2_rt_mixed(float t0, float tabs, float s0, float y0, float cz, float snt,
+                                             const float* ex, const SwExactCtx& x, int k0, int g, int ib,
+                                             bool cloud, float& rb, float& rd, float& tb, float& td, float& e3,
+                                             float& e4)
+{
+    float zrpp, t1;
+    sw2_rt<float>(t0, tabs, s0, y0, x.mode, cz, snt, ex, rb, rd, tb, td, t1, zrpp);
+    e3 = sw_expm(t1 * snt, ex, true);
+    e4 = sw_expm(t0 * snt, ex, true);
+    if (fabsf(zrpp) < SW2_RESONANCE) {
+        double a, b, c, d, f3, f4;
+        sw2_exact(x, k0, g, ib, cloud, a, b, c, d, f3, f4);
+        rb = (float)a; rd = (float)b; tb = (float)c; td = (float)d; e3 = (float)f3; e4 = (float)f4;
+    }
+}
+
+// R/T of layer k0 for g-point g in the clear (cloudy_pass = false) or cloudy pass of spcvrtc
+// (spcvrtc.cu:330-460: the cloudy pass blends the clear and cloud-mixture R/T by the layer cloud fraction).
+__device__ __noinline__ SwLayerRT sw2_layer(const SwSh2& s, const SwAer* aer, const SwExactCtx& x, int k0, int g,
+                                               int ib, bool cloudy_pass, float cz, float snt, const float* ex)
+{
+    SwLayerRT L;
+    if (k0 >= x.a->nlay) {   // padding above the model top: a transparent, non-reflecting layer
+        L.rb = 0; L.rd = 0; L.tb = 1; L.td = 1; L.e3 = 1; L.e4 = 1;
+        return L;
+    }
+    const float tr = s.taur[g][k0], tg = s.taug[g][k0];
+    float ta = 0, tasa = 0, tay = 0, taab = 0;
+    if (aer) { ta = aer->tau[ib][k0]; tasa = aer->tasa[ib][k0]; tay = aer->tay[ib][k0]; taab = aer->tabs[ib][k0]; }
+    const float ct0 = fmaxf(1.0e-12f, tr + tg + ta), cs0 = tr + tasa, cy0 = tay, cab = tg + taab;
+    sw2_rt_mixed(ct0, cab, cs0, cy0, cz, snt, ex, x, k0, g, ib, false, L.rb, L.rd, L.tb, L.td, L.e3, L.e4);
+    if (cloudy_pass) {
+        const float zc1 = s.cldfrc[k0];
+        if (zc1 > 1.0e-12f) {
+            const float ot0 = ct0 + s.taucw[ib][k0], os0 = cs0 + s.ssacw[ib][k0], oy0 = cy0 + s.asycw[ib][k0];
+            const float oab = cab + s.tabsc[ib][k0];
+            float rb2, rd2, tb2, td2, e32, e42;
+            sw2_rt_mixed(ot0, oab, os0, oy0, cz, snt, ex, x, k0, g, ib, true, rb2, rd2, tb2, td2, e32, e42);
+            const float zc0 = 1.0f - zc1;
+            L.rb = zc0 * L.rb + zc1 * rb2;
+            L.rd = zc0 * L.rd + zc1 * rd2;
+            L.tb = zc0 * L.tb + zc1 * tb2;
+            L.td = zc0 * L.td + zc1 * td2;
+            L.e3 = zc0 * L.e3 + zc1 * e32;
+            L.e4 = zc0 * L.e4 + zc1 * e42;
+        }
+    }
+    return L;
+}
+
+// ------------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(SW2_THREADS, 2)
+sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SwSh2& s = *reinterpret_cast<SwSh2*>(smem_raw);
+    SwAer* aer = a.faersw ? reinterpret_cast<SwAer*>(smem_raw + sizeof(SwSh2)) : nullptr;
+    float* ckpt = reinterpret_cast<float*>(smem_raw + sizeof(SwSh2) + (a.faersw ? sizeof(SwAer) : 0));
+    const int nlay = a.nlay, nlp1 = nlay + 1;
+    const int d = blockIdx.x;
+    if (d >= *a.nday) return;
+    if (nlay > NLAY_MAX) {
+        if (threadIdx.x == 0) atomicExch(err, RAD_DEV_NLAY);
+        return;
+    }
+    const int64_t N = a.ncol;
+    const int64_t col = a.daycol[d];
+    const int tid = threadIdx.x;
+    const double heatfac = 9.80665 * 1.0e-2 / 1.0046e3;
+    // ---- phase A1: layer coefficients (threads = layers), aerosol, heating factors
+    for (int k0 = tid; k0 < nlay; k0 += SW2_THREADS) {
+        SwCoef<float> c;
+        sw2_layer_coef<float>(a, col, k0, c);
+        s.fac00[k0] = c.fac00; s.fac01[k0] = c.fac01; s.fac10[k0] = c.fac10; s.fac11[k0] = c.fac11;
+        s.selffac[k0] = c.selffac; s.selffrac[k0] = c.selffrac; s.forfac[k0] = c.forfac; s.forfrac[k0] = c.forfrac;
+        s.colmol[k0] = c.colmol;
+        for (int m = 0; m < 6; ++m) s.colamt[m][k0] = c.colamt[m];
+        s.jp[k0] = c.jp; s.jt[k0] = c.jt; s.jt1[k0] = c.jt1; s.indself[k0] = c.indself; s.indfor[k0] = c.indfor;
+        s.low[k0] = c.low ? 1 : 0;
+        const int kk0 = nlay - 1 - k0;
+        s.cfrac[k0] = __ldg(a.clouds + (size_t)kk0 * N + col);
+        const double dl = (double)__ldg(a.plvl + (size_t)(kk0 + 1) * N + col) - (double)__ldg(a.plvl + (size_t)kk0 * N + col);
+        s.rdelp[k0] = heatfac / dl;
+        if (aer) {
+            for (int ib = 0; ib < 14; ++ib) {
+                const float ta = __ldg(a.faersw + (((size_t)ib) * nlay + kk0) * N + col);
+                const float sa = __ldg(a.faersw + (((size_t)(14 + ib)) * nlay + kk0) * N + col);
+                const float ya = __ldg(a.faersw + (((size_t)(28 + ib)) * nlay + kk0) * N + col);
+                aer->tau[ib][k0] = ta;
+                aer->tasa[ib][k0] = ta * sa;
+                aer->tay[ib][k0] = ya * sa * ta;
+                aer->tabs[ib][k0] = ta * (1.0f - sa);
+            }
+        }
+    }
+    __syncthreads();
+    // ---- column scalars (thread 0): sun, albedo, overlap fractions (swrad.cu:242-279), laytrop
+    if (tid == 0) {
+        const float cz = __ldg(a.coszen + col);
+        s.cosz = cz;
+        s.sntz = 1.0f / cz;
+        s.ssolar = (a.solcon / 1368.22f) * cz;
+        s.albbm[0] = __ldg(a.sfcalb + col);
+        s.albdf[0] = __ldg(a.sfcalb + N + col);
+        s.albbm[1] = __ldg(a.sfcalb + 2 * N + col);
+        s.albdf[1] = __ldg(a.sfcalb + 3 * N + col);
+        const float ftiny = 1.0e-12f, oneminus = 1.0f - 1.0e-6f;
+        float z0 = 1, z1 = 1;
+        for (int k0 = 0; k0 < nlay; ++k0) {
+            const float cf = s.cfrac[k0];
+            if (cf > ftiny) z1 = fminf(z1, 1.0f - cf);
+            else if (z1 < 1.0f) { z0 = z0 * z1; z1 = 1; }
+        }
+        z0 = z0 * z1;
+        if (z0 <= ftiny) z0 = 0;
+        if (z0 > oneminus) z0 = 1;
+        s.zcf0 = z0;
+        s.zcf1 = 1.0f - z0;
+        int lt = nlay;
+        for (int k0 = 0; k0 < nlay; ++k0)
+            if (s.low[k0]) lt = k0 + 1;
+        s.laytrop = lt;
+        s.kmin8 = a.kmin8[d];
+        s.kminw = a.kminw[d];
+    }
+    __syncthreads();
+    // ---- phase A2: cloud optics per (band, layer); solar source per band
+    for (int p = tid; p < 14 * nlay; p += SW2_THREADS) {
+        const int ib = p / nlay, k0 = p - ib * nlay;
+        float tcw = 0, scw = 0, acw = 0, tab_ = 0;
+        if (s.zcf1 > 0) sw2_cloud<float>(a, col, k0, ib, s.cfrac[k0], tcw, scw, acw, tab_);
+        s.taucw[ib][k0] = tcw; s.ssacw[ib][k0] = scw; s.asycw[ib][k0] = acw; s.tabsc[ib][k0] = tab_;
+        if (ib == 0) s.cldfrc[k0] = s.zcf1 > 0 ? s.cfrac[k0] / s.zcf1 : 0.0f;
+    }
+    if (tid < 14) sw_sfluxzen<float>(s, tid, nlay);
+    __syncthreads();
+    // ---- phase B: gas and Rayleigh optical depths per (g, layer), g-major
+    for (int p = tid; p < SW_NGPT * nlay; p += SW2_THREADS) {
+        const int g = p / nlay, k0 = p - g * nlay;
+        float tg, tr;
+        sw_gas<float>(s, g, k0, tg, tr);
+        s.taug[g][k0] = tg;
+        s.taur[g][k0] = tr;
+    }
+    __syncthreads();
+    // ---- phase C: the two passes of spcvrtc, one g-point per lane
+    const int warp = tid >> 5, lane = tid & 31;
+    const int pass = warp >> 2, wq = warp & 3;
+    const int gb = wq == 0 ? 0 : (wq == 1 ? 28 : (wq == 2 ? 56 : 86));
+    const int ge = wq == 0 ? 28 : (wq == 1 ? 56 : (wq == 2 ? 86 : SW_NGPT));
+    const bool act = gb + lane < ge;
+    const int g = act ? gb + lane : ge - 1;
+    int ib0 = 0;
+    while (g >= c_sw_ns[ib0 + 1]) ++ib0;
+    const int ibd = ib0 == 8 ? 0 : ((ib0 >= 9 && ib0 <= 12) ? 2 : 1);   // idxsfc
+    const float cz = s.cosz, snt = s.sntz;
+    const bool cloudy = s.zcf1 > 1.0e-6f;
+    const float zsolar = act ? s.ssolar * s.sfluxzen[g] : 0.0f;
+    const float ab = ibd ? s.albbm[ibd - 1] : 0.5f * (s.albbm[0] + s.albbm[1]);
+    const float ad = ibd ? s.albdf[ibd - 1] : 0.5f * (s.albdf[0] + s.albdf[1]);
+    SwExactCtx x{&a, col, s.laytrop, s.kmin8, s.kminw, a.iswmode, (double)__ldg(a.coszen + col),
+                 1.0 / (double)__ldg(a.coszen + col), exd};
+    float toa_up = 0, sfc_up = 0, sfc_dn = 0, sfc_dir = 0;
+    const int nseg = (nlay + SW2_SEG - 1) / SW2_SEG;
+    if (pass == 0 || cloudy) {
+        const bool cp = pass == 1;
+        // upward sweep: reflectances of the atmosphere below each level (swflux.cu, zrupb/zrupd)
+        float ub = ab, ud = ad;
+        for (int sg = 0; sg < nseg; ++sg) {
+            if (sg > 0) {
+                ckpt[((sg - 1) * 2 + 0) * SW2_THREADS + tid] = ub;
+                ckpt[((sg - 1) * 2 + 1) * SW2_THREADS + tid] = ud;
+            }
+#pragma unroll 2
+            for (int j = 0; j < SW2_SEG; ++j) {
+                const SwLayerRT L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cp, cz, snt, ex);
+                const float den = 1.0f / (1.0f - ud * L.rd);
+                ub = L.rb + (L.td * ((L.tb - L.e3) * ud + L.e3 * ub)) * den;
+                ud = L.rd + L.td * L.td * ud * den;
+            }
+        }
+        // downward sweep, segment by segment from the top
+        float tdn = 1, rdn = 0, tdb = 1, tdb0 = 1;
+        for (int sg = nseg - 1; sg >= 0; --sg) {
+            float zub[SW2_SEG + 1], zud[SW2_SEG + 1];
+            float rb[SW2_SEG], rd[SW2_SEG], tb[SW2_SEG], td[SW2_SEG], e3[SW2_SEG];
+            float e4p = 1;
+            zub[0] = sg ? ckpt[((sg - 1) * 2 + 0) * SW2_THREADS + tid] : ab;
+            zud[0] = sg ? ckpt[((sg - 1) * 2 + 1) * SW2_THREADS + tid] : ad;
+#pragma unroll
+            for (int j = 0; j < SW2_SEG; ++j) {
+                const SwLayerRT L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cp, cz, snt, ex);
+                rb[j] = L.rb; rd[j] = L.rd; tb[j] = L.tb; td[j] = L.td; e3[j] = L.e3;
+                e4p = e4p * L.e4;
+                const float den = 1.0f / (1.0f - zud[j] * L.rd);
+                zub[j + 1] = L.rb + (L.td * ((L.tb - L.e3) * zud[j] + L.e3 * zub[j])) * den;
+                zud[j + 1] = L.rd + L.td * L.td * zud[j] * den;
+            }
+#pragma unroll
+            for (int j = SW2_SEG - 1; j >= 0; --j) {
+                const int lev = sg * SW2_SEG + j + 2;        // level above layer j (1 = surface)
+                if (lev <= nlp1) {
+                    const float den = 1.0f / (1.0f - rdn * zud[j + 1]);
+                    const float fu = (tdb * zub[j + 1] + (tdn - tdb) * zud[j + 1]) * den;
+                    const float fd = tdb + (tdn - tdb + tdb * zub[j + 1] * rdn) * den;
+                    double v = act ? (double)zsolar * ((double)fd - (double)fu) : 0.0;
+                    v = warp_sum(v);
+                    if (lane == 0) s.fn[warp][lev - 1] = v;
+                    if (lev == nlp1) toa_up = fu;
+                }
+                const float den = 1.0f / (1.0f - rd[j] * rdn);
+                const float tdn1 = tdb * tb[j] + (td[j] * ((tdn - tdb) + tdb * rb[j] * rdn)) * den;
+                rdn = rd[j] + td[j] * td[j] * rdn * den;
+                tdn = tdn1;
+                tdb = e3[j] * tdb;
+            }
+            tdb0 = tdb0 * e4p;
+        }
+        // surface level
+        {
+            const float den = 1.0f / (1.0f - rdn * ad);
+            const float fu = (tdb * ab + (tdn - tdb) * ad) * den;
+            const float fd = tdb + (tdn - tdb + tdb * ab * rdn) * den;
+            double v = act ? (double)zsolar * ((double)fd - (double)fu) : 0.0;
+            v = warp_sum(v);
+            if (lane == 0) s.fn[warp][0] = v;
+            sfc_up = fu;
+            sfc_dn = fd;
+            sfc_dir = tdb0;
+        }
+    } else {
+        for (int k = lane; k <= nlay; k += 32) s.fn[warp][k] = 0;
+    }
+    {
+        // per-lane scalars (zero for idle lanes and for the cloudy warps of a clear column)
+        double scv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (act && (pass == 0 || cloudy)) {
+            const double zs = (double)zsolar;
+            scv[0] = zs * (double)toa_up;
+            scv[1] = zs * (double)sfc_up;
+            scv[2] = zs * (double)sfc_dn;
+            scv[3] = ib0 == 11 ? zs * (double)sfc_dn : 0.0;
+            const double zb1 = (double)(zsolar * sfc_dir), zb2 = (double)(zsolar * (sfc_dn - sfc_dir));
+            if (ibd == 1) { scv[4] = zb1; scv[5] = zb2; }
+            else if (ibd == 2) { scv[6] = zb1; scv[7] = zb2; }
+            else { scv[4] = 0.5 * zb1; scv[5] = 0.5 * zb2; scv[6] = 0.5 * zb1; scv[7] = 0.5 * zb2; }
+            scv[8] = zs;
+        }
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const double v = warp_sum(scv[i]);
+            if (lane == 0) s.sc[warp][i] = v;
+        }
+    }
+    __syncthreads();
+    // ---- column end (spcvrtc.cu:493-545) and swrad_post (swrad.cu:365-403), float64
+    const double c1d = (double)s.zcf1, c0d = (double)s.zcf0;
+    auto tot = [&](double clr, double cld) { return cloudy ? c1d * cld + c0d * clr : clr; };
+    for (int k = tid; k < nlay; k += SW2_THREADS) {
+        double a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+        for (int w = 0; w < 4; ++w) {
+            a0 += s.fn[w][k]; a1 += s.fn[w][k + 1];
+            b0 += s.fn[4 + w][k]; b1 += s.fn[4 + w][k + 1];
+        }
+        const double fk = tot(a0, b0), fk1 = tot(a1, b1);
+        a.htsw[(size_t)(nlay - 1 - k) * N + col] = (float)((fk1 - fk) * s.rdelp[k]);
+    }
+    if (tid == 0) {
+        double c[9], t[9];
+        for (int i = 0; i < 9; ++i) {
+            c[i] = 0; t[i] = 0;
+            for (int w = 0; w < 4; ++w) { c[i] += s.sc[w][i]; t[i] += s.sc[4 + w][i]; }
+        }
+        // slots: 0 toa up, 1 sfc up, 2 sfc dn, 3 uv-b, 4 nir beam, 5 nir diffuse, 6 vis beam, 7 vis diffuse,
+        // 8 toa down
+        a.topfsw[col] = (float)tot(c[0], t[0]);
+        a.topfsw[N + col] = (float)c[8];
+        a.topfsw[2 * N + col] = (float)c[0];
+        a.sfcfsw[col] = (float)tot(c[1], t[1]);
+        a.sfcfsw[N + col] = (float)tot(c[2], t[2]);
+        a.sfcfsw[2 * N + col] = (float)c[1];
+        a.sfcfsw[3 * N + col] = (float)c[2];
+        if (a.fdncmp) {
+            a.fdncmp[col] = (float)c[3];
+            a.fdncmp[N + col] = (float)tot(c[3], t[3]);
+            a.fdncmp[2 * N + col] = (float)tot(c[4], t[4]);
+            a.fdncmp[3 * N + col] = (float)tot(c[5], t[5]);
+            a.fdncmp[4 * N + col] = (float)tot(c[6], t[6]);
+            a.fdncmp[5 * N + col] = (float)tot(c[7], t[7]);
+        }
+    }
+}
+
+}  // namespace rad
