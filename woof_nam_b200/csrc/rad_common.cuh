@@ -61,6 +61,29 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+// Visit every (g-point, layer) pair of a column with the CTA's warps such that each warp works on one band
+// at a time: lane l of a task of band b takes g-point ns[b] + l % ng and layer k0 + l / ng (ng = the band's
+// g-point count, 32 / ng layers per task).  Neighbouring lanes then read neighbouring g entries of the
+// band's [..][g] k-tables (coalesced) and take the same band branch.  f(g, k0) runs once per pair.
+template <class F>
+__device__ __forceinline__ void for_each_band_pair(const int* ns, int nbands, int nlay, int warp, int nwarps, int lane,
+                                                   F f)
+{
+    int b = 0, t0 = 0;   // band of the current task and the index of its first task
+    int ng = ns[1] - ns[0], kpw = 32 / ng, nt = (nlay + kpw - 1) / kpw;
+    for (int t = warp;; t += nwarps) {
+        while (b < nbands && t >= t0 + nt) {
+            t0 += nt;
+            ++b;
+            if (b < nbands) { ng = ns[b + 1] - ns[b]; kpw = 32 / ng; nt = (nlay + kpw - 1) / kpw; }
+        }
+        if (b >= nbands) break;
+        const int kk = lane / ng, jg = lane - kk * ng;
+        const int k0 = (t - t0) * kpw + kk;
+        if (kk < kpw && k0 < nlay) f(ns[b] + jg, k0);
+    }
+}
+
 // Error word written by kernels on bad input (host reads it after a synchronising call).
 enum : int { RAD_DEV_OK = 0, RAD_DEV_NLAY = 1, RAD_DEV_INDEX = 2 };
 

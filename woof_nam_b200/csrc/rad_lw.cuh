@@ -730,16 +730,15 @@ __device__ void lw_setup(LwShared<R>& s, const LwIn& a, int64_t col, int tid)
         }
     }
     __syncthreads();
-    // ---- phase B: gas optics per (g, layer), g-major so a warp stays inside one band
-    for (int p = tid; p < LW_NGPT * nlay; p += NT) {
-        const int g = p / nlay, k0 = p - g * nlay;
+    // ---- phase B: gas optics per (g, layer), band by band (one band per warp task, coalesced table reads)
+    for_each_band_pair(c_lw_ns, 16, nlay, tid >> 5, NT / 32, tid & 31, [&](int g, int k0) {
         R tg, fr;
         lw_gas(s, g, k0, tg, fr);
         int band = 0;
         while (g >= c_lw_ns[band + 1]) ++band;
         s.taug[g][k0] = tg + s.tauaer[band][k0];
         s.fracs[g][k0] = fr;
-    }
+    });
     // ---- overlap factors of rtrnmr (serial recurrence in k), thread 32 while warp 0 waits
     if (tid == 32) {
         const R* cf = s.cldfrc;

@@ -39,6 +39,7 @@ constexpr int SW2_WARPS = 8, SW2_THREADS = 256;
 constexpr int SW2_SEG = RAD_SW2_SEG;                              // layers per checkpoint segment
 constexpr int SW2_NSEG = (NLAY_MAX + SW2_SEG - 1) / SW2_SEG;
 constexpr float SW2_RESONANCE = 1.0e-2f;                          // exact recompute where |1-(k mu0)^2| < this
+constexpr int SW2_QCAP = 192;                                     // queued exact recomputes per column
 
 // Rain and snow optical coefficients per SW band (phys_rrtm_sw_cldprop.cu): b0r, c0r, b0s, b1s, c0s.
 __constant__ float c_sw_rain_snow[5][14] = {
@@ -223,7 +224,7 @@ __device__ __forceinline__ T sw2_expm_c(T zb, const T* ex, T& em)
 }
 
 // Layer R/T (spcvrtc.cu:112-173) from (tau, absorption tau, scattering tau, scattering tau x g), equal to
-// the reference's statements in exact arithmetic and accurate in float:
+// the reference's statements in exact arithmetic and accurate in float (sw2_prologue + sw2_rt_tail):
 //  * co-albedo w = tau_abs / tau, so g1 - g2 = 2 w / (1 - zssaw g^2) (PIFM; sqrt(3) w / ... for the
 //    discrete-ordinates mode) and g1 - k = g2^2 / (g1 + k) carry no cancellation;
 //  * with e1 = exp(-k tau1), e2 = exp(-tau1 / mu0) and their complements m1 = 1 - e1, m2 = 1 - e2, the
@@ -233,52 +234,65 @@ __device__ __forceinline__ T sw2_expm_c(T zb, const T* ex, T& em)
 //    so thin and near-conservative layers (k tau1 -> 0) keep their accuracy;  rd = g2 (1-e1^2) / B,
 //    td = 2 k e1 / B;
 //  * finite for any optical depth (the reference's float form overflows 1/exp(-k tau) beyond ~88).
-// zrpp_raw returns 1 - (k mu0)^2 before the reference's 1e-8 clamp.
 template <class T>
-__device__ __forceinline__ void sw2_rt(T ztau0, T tabs, T zssa0, T zasy0, int mode, T cz, T snt, const T* ex,
-                                       T& rb, T& rd, T& tb, T& td, T& ztau1, T& zrpp_raw)
+struct SwPro {   // the part of the layer R/T before the exponentials
+    T ztau1, zssa1, g1, g2, g3, g4, zrk, zrp, zrpp;
+};
+
+template <class T>
+__device__ __forceinline__ SwPro<T> sw2_prologue(T ztau0, T tabs, T zssa0, T zasy0, int mode, T cz)
 {
-    const T ftiny = (T)1.0e-12f, eps1 = (T)1.0e-8f;
+    SwPro<T> p;
+    const T ftiny = (T)1.0e-12f;
     const T cwmin = (T)(1.0 - ((double)1.0f - (double)1.0e-6f));   // 1 - min(oneminus, ssa) bound of FP64
     const T cw = fmaxR(cwmin, tabs / ztau0);
     const T zssaw = (T)1 - cw;
     const T zasyw = zasy0 / fmaxR(ftiny, zssa0);
     const T za2s = zssaw * (zasyw * zasyw);
     const T om = (T)1 - za2s;
-    ztau1 = om * ztau0;
-    const T zssa1 = (zssaw - za2s) / om, cw1 = cw / om;
+    p.ztau1 = om * ztau0;
+    p.zssa1 = (zssaw - za2s) / om;
+    const T cw1 = cw / om;
     const T zasy1 = zasyw / ((T)1 + zasyw), zasy3 = (T)0.75f * zasy1;
-    T g1, g2, g3, gm, gp;
+    T gm, gp;
     if (mode == 2) {
-        g1 = (T)2 - zssa1 * ((T)1.25f + zasy3);
-        g2 = (T)0.75f * zssa1 * ((T)1 - zasy1);
-        g3 = (T)0.5f - zasy3 * cz;
+        p.g1 = (T)2 - p.zssa1 * ((T)1.25f + zasy3);
+        p.g2 = (T)0.75f * p.zssa1 * ((T)1 - zasy1);
+        p.g3 = (T)0.5f - zasy3 * cz;
         gm = (T)2 * cw1;
-        gp = (T)2 - zssa1 * ((T)0.5f + (T)1.5f * zasy1);
+        gp = (T)2 - p.zssa1 * ((T)0.5f + (T)1.5f * zasy1);
     } else if (mode == 1) {
-        g1 = (T)1.75f - zssa1 * ((T)1 + zasy3);
-        g2 = (T)-0.25f - zssa1 * ((T)1 - zasy3);
-        g3 = (T)0.5f - zasy3 * cz;
-        gm = g1 - g2;
-        gp = g1 + g2;
+        p.g1 = (T)1.75f - p.zssa1 * ((T)1 + zasy3);
+        p.g2 = (T)-0.25f - p.zssa1 * ((T)1 - zasy3);
+        p.g3 = (T)0.5f - zasy3 * cz;
+        gm = p.g1 - p.g2;
+        gp = p.g1 + p.g2;
     } else {
         const T zsr3 = (T)1.7320508f;
-        g1 = zsr3 * ((T)2 - zssa1 * ((T)1 + zasy1)) * (T)0.5f;
-        g2 = zsr3 * zssa1 * ((T)1 - zasy1) * (T)0.5f;
-        g3 = ((T)1 - zsr3 * zasy1 * cz) * (T)0.5f;
+        p.g1 = zsr3 * ((T)2 - p.zssa1 * ((T)1 + zasy1)) * (T)0.5f;
+        p.g2 = zsr3 * p.zssa1 * ((T)1 - zasy1) * (T)0.5f;
+        p.g3 = ((T)1 - zsr3 * zasy1 * cz) * (T)0.5f;
         gm = zsr3 * cw1;
-        gp = zsr3 * ((T)1 - zssa1 * zasy1);
+        gp = zsr3 * ((T)1 - p.zssa1 * zasy1);
     }
-    const T g4 = (T)1 - g3;
-    const T zrk = sqrtR(gm * gp);
-    const T zrp = zrk * cz;
-    T zrpp = ((T)1 - zrp) * ((T)1 + zrp);
-    zrpp_raw = zrpp;
-    if (fabs(zrpp) < eps1) zrpp = zrpp < 0 ? -eps1 : eps1;
+    p.g4 = (T)1 - p.g3;
+    p.zrk = sqrtR(gm * gp);
+    p.zrp = p.zrk * cz;
+    p.zrpp = ((T)1 - p.zrp) * ((T)1 + p.zrp);
+    return p;
+}
+
+// R/T from the prologue (1 - (k mu0)^2 clamped at 1e-8 as the reference does).
+template <class T>
+__device__ __forceinline__ void sw2_rt_tail(const SwPro<T>& p, T cz, T snt, const T* ex, T& rb, T& rd, T& tb, T& td)
+{
+    const T eps1 = (T)1.0e-8f;
+    const T zrpp = fabs(p.zrpp) < eps1 ? (p.zrpp < 0 ? -eps1 : eps1) : p.zrpp;
+    const T g1 = p.g1, g2 = p.g2, g3 = p.g3, g4 = p.g4, zrk = p.zrk, zrp = p.zrp;
     const T za1 = g1 * g4 + g2 * g3, za2 = g1 * g3 + g2 * g4;
     T em1, em2;
-    const T e1 = sw2_expm_c(fminR(zrk * ztau1, (T)500), ex, em1);
-    const T e2 = sw2_expm_c(fminR(ztau1 * snt, (T)500), ex, em2);
+    const T e1 = sw2_expm_c(fminR(zrk * p.ztau1, (T)500), ex, em1);
+    const T e2 = sw2_expm_c(fminR(p.ztau1 * snt, (T)500), ex, em2);
     const T e11 = e1 * e1, em11 = em1 * ((T)2 - em1);
     const T B = zrk * ((T)1 + e11) + g1 * em11;
     const T D = zrpp * B;                                        // (reference ze1r45) * exp(-k tau)
@@ -286,7 +300,7 @@ __device__ __forceinline__ void sw2_rt(T ztau0, T tabs, T zssa0, T zasy0, int mo
         rb = eps1;
         tb = e2;
     } else {
-        const T q = zssa1 / D;
+        const T q = p.zssa1 / D;
         const T nr = em11 * (za2 - zrk * g3 * zrp) + zrk * (g3 - za2 * cz) * (em1 * em1 + (T)2 * e1 * em2);
         const T nt = zrk * (g4 + za1 * cz) * ((T)2 * e1 * em2 - e2 * em1 * em1) - e2 * em11 * (za1 + zrk * g4 * zrp);
         rb = fmaxR((T)0, fminR((T)1, nr * q));
@@ -313,6 +327,9 @@ struct SwSh2 {
     float cosz, sntz, ssolar, albbm[2], albdf[2], zcf0, zcf1;
     int laytrop, kmin8, kminw;
     unsigned char low[NLAY_MAX];
+    int nexact;                                // layer evaluations queued for the float64 recompute
+    int qkey[SW2_QCAP];                        // thread | layer << 8 | cloud << 15
+    float qval[SW2_QCAP][6];                   // their rb, rd, tb, td, e3, e4
 };
 // Dynamic tail: the aerosol block (present only with aerosol inputs) and the segment checkpoints.
 struct SwAer {
@@ -383,22 +400,33 @@ __device__ __noinline__ void sw2_exact(const SwExactCtx& x, int k0, int g, int i
     e4 = sw_expm(t0 * x.snt, x.exd, true);
 }
 
-// One optical-property set of a layer -> R/T and direct transmissions: float, or the exact float64
-// recompute near the resonance.
-__device__ __forceinline__ void sw2_rt_mixed(float t0, float tabs, float s0, float y0, float cz, float snt,
-                                             const float* ex, const SwExactCtx& x, int k0, int g, int ib,
+__device__ __forceinline__ int sw2_qkey(int tid, int k0, bool cloud) { return tid | (k0 << 8) | ((int)cloud << 15); }
+
+// One optical-property set of a layer -> R/T and direct transmissions: float, or near the resonance the
+// float64 recompute -- taken from the column's queue, where the pre-pass put it, or done here.
+__device__ __forceinline__ void sw2_rt_mixed(const SwSh2& s, float t0, float tabs, float s0, float y0, float cz,
+                                             float snt, const float* ex, const SwExactCtx& x, int k0, int g, int ib,
                                              bool cloud, float& rb, float& rd, float& tb, float& td, float& e3,
                                              float& e4)
 {
-    float zrpp, t1;
-    sw2_rt<float>(t0, tabs, s0, y0, x.mode, cz, snt, ex, rb, rd, tb, td, t1, zrpp);
-    e3 = sw_expm(t1 * snt, ex, true);
-    e4 = sw_expm(t0 * snt, ex, true);
-    if (fabsf(zrpp) < SW2_RESONANCE) {
+    const SwPro<float> p = sw2_prologue<float>(t0, tabs, s0, y0, x.mode, cz);
+    if (fabsf(p.zrpp) < SW2_RESONANCE) {
+        const int key = sw2_qkey(threadIdx.x, k0, cloud);
+        const int nq = min(s.nexact, SW2_QCAP);
+        for (int i = 0; i < nq; ++i)
+            if (s.qkey[i] == key) {
+                rb = s.qval[i][0]; rd = s.qval[i][1]; tb = s.qval[i][2]; td = s.qval[i][3];
+                e3 = s.qval[i][4]; e4 = s.qval[i][5];
+                return;
+            }
         double a, b, c, d, f3, f4;
         sw2_exact(x, k0, g, ib, cloud, a, b, c, d, f3, f4);
         rb = (float)a; rd = (float)b; tb = (float)c; td = (float)d; e3 = (float)f3; e4 = (float)f4;
+        return;
     }
+    sw2_rt_tail<float>(p, cz, snt, ex, rb, rd, tb, td);
+    e3 = sw_expm(p.ztau1 * snt, ex, true);
+    e4 = sw_expm(t0 * snt, ex, true);
 }
 
 // R/T of layer k0 for g-point g in the clear (cloudy_pass = false) or cloudy pass of spcvrtc
@@ -415,14 +443,14 @@ __device__ __noinline__ SwLayerRT sw2_layer(const SwSh2& s, const SwAer* aer, co
     float ta = 0, tasa = 0, tay = 0, taab = 0;
     if (aer) { ta = aer->tau[ib][k0]; tasa = aer->tasa[ib][k0]; tay = aer->tay[ib][k0]; taab = aer->tabs[ib][k0]; }
     const float ct0 = fmaxf(1.0e-12f, tr + tg + ta), cs0 = tr + tasa, cy0 = tay, cab = tg + taab;
-    sw2_rt_mixed(ct0, cab, cs0, cy0, cz, snt, ex, x, k0, g, ib, false, L.rb, L.rd, L.tb, L.td, L.e3, L.e4);
+    sw2_rt_mixed(s, ct0, cab, cs0, cy0, cz, snt, ex, x, k0, g, ib, false, L.rb, L.rd, L.tb, L.td, L.e3, L.e4);
     if (cloudy_pass) {
         const float zc1 = s.cldfrc[k0];
         if (zc1 > 1.0e-12f) {
             const float ot0 = ct0 + s.taucw[ib][k0], os0 = cs0 + s.ssacw[ib][k0], oy0 = cy0 + s.asycw[ib][k0];
             const float oab = cab + s.tabsc[ib][k0];
             float rb2, rd2, tb2, td2, e32, e42;
-            sw2_rt_mixed(ot0, oab, os0, oy0, cz, snt, ex, x, k0, g, ib, true, rb2, rd2, tb2, td2, e32, e42);
+            sw2_rt_mixed(s, ot0, oab, os0, oy0, cz, snt, ex, x, k0, g, ib, true, rb2, rd2, tb2, td2, e32, e42);
             const float zc0 = 1.0f - zc1;
             L.rb = zc0 * L.rb + zc1 * rb2;
             L.rd = zc0 * L.rd + zc1 * rd2;
@@ -435,8 +463,20 @@ __device__ __noinline__ SwLayerRT sw2_layer(const SwSh2& s, const SwAer* aer, co
     return L;
 }
 
+// Phase-C thread -> g-point: warps 0-3 the clear pass, 4-7 the cloudy pass; in each pass the four warps take
+// g-points 0-27, 28-55, 56-85 (the Rayleigh-dominated bands 23-26) and 86-111.  Idle lanes mirror the
+// warp's last g-point (act = false).
+__device__ __forceinline__ int sw2_lane_g(int t, bool& act)
+{
+    const int wq = (t >> 5) & 3, lane = t & 31;
+    const int gb = wq == 0 ? 0 : (wq == 1 ? 28 : (wq == 2 ? 56 : 86));
+    const int ge = wq == 0 ? 28 : (wq == 1 ? 56 : (wq == 2 ? 86 : SW_NGPT));
+    act = gb + lane < ge;
+    return act ? gb + lane : ge - 1;
+}
+
 // ------------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(SW2_THREADS, 2)
+__global__ void __launch_bounds__(SW2_THREADS, 1)
 sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -509,6 +549,7 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
         s.laytrop = lt;
         s.kmin8 = a.kmin8[d];
         s.kminw = a.kminw[d];
+        s.nexact = 0;
     }
     __syncthreads();
     // ---- phase A2: cloud optics per (band, layer); solar source per band
@@ -521,22 +562,19 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
     }
     if (tid < 14) sw_sfluxzen<float>(s, tid, nlay);
     __syncthreads();
-    // ---- phase B: gas and Rayleigh optical depths per (g, layer), g-major
-    for (int p = tid; p < SW_NGPT * nlay; p += SW2_THREADS) {
-        const int g = p / nlay, k0 = p - g * nlay;
+    // ---- phase B: gas and Rayleigh optical depths per (g, layer), band by band
+    for_each_band_pair(c_sw_ns, 14, nlay, tid >> 5, SW2_WARPS, tid & 31, [&](int g, int k0) {
         float tg, tr;
         sw_gas<float>(s, g, k0, tg, tr);
         s.taug[g][k0] = tg;
         s.taur[g][k0] = tr;
-    }
+    });
     __syncthreads();
     // ---- phase C: the two passes of spcvrtc, one g-point per lane
     const int warp = tid >> 5, lane = tid & 31;
-    const int pass = warp >> 2, wq = warp & 3;
-    const int gb = wq == 0 ? 0 : (wq == 1 ? 28 : (wq == 2 ? 56 : 86));
-    const int ge = wq == 0 ? 28 : (wq == 1 ? 56 : (wq == 2 ? 86 : SW_NGPT));
-    const bool act = gb + lane < ge;
-    const int g = act ? gb + lane : ge - 1;
+    const int pass = warp >> 2;
+    bool act;
+    const int g = sw2_lane_g(tid, act);
     int ib0 = 0;
     while (g >= c_sw_ns[ib0 + 1]) ++ib0;
     const int ibd = ib0 == 8 ? 0 : ((ib0 >= 9 && ib0 <= 12) ? 2 : 1);   // idxsfc
@@ -547,6 +585,42 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
     const float ad = ibd ? s.albdf[ibd - 1] : 0.5f * (s.albdf[0] + s.albdf[1]);
     SwExactCtx x{&a, col, s.laytrop, s.kmin8, s.kminw, a.iswmode, (double)__ldg(a.coszen + col),
                  1.0 / (double)__ldg(a.coszen + col), exd};
+    // ---- phase C0: layer evaluations near the two-stream resonance (|1 - (k mu0)^2| < SW2_RESONANCE) are
+    // queued and recomputed in float64 by all threads of the column, instead of by one lane of a warp
+    // while the other lanes wait; the sweeps below read them back from the queue.
+    if (act && (pass == 0 || cloudy)) {
+        for (int k0 = 0; k0 < nlay; ++k0) {
+            const float tr = s.taur[g][k0], tg = s.taug[g][k0];
+            float ta = 0, tasa = 0, tay = 0, taab = 0;
+            if (aer) { ta = aer->tau[ib0][k0]; tasa = aer->tasa[ib0][k0]; tay = aer->tay[ib0][k0]; taab = aer->tabs[ib0][k0]; }
+            const float ct0 = fmaxf(1.0e-12f, tr + tg + ta), cs0 = tr + tasa, cy0 = tay, cab = tg + taab;
+            if (fabsf(sw2_prologue<float>(ct0, cab, cs0, cy0, x.mode, cz).zrpp) < SW2_RESONANCE) {
+                const int i = atomicAdd(&s.nexact, 1);
+                if (i < SW2_QCAP) s.qkey[i] = sw2_qkey(tid, k0, false);
+            }
+            if (pass == 1 && s.cldfrc[k0] > 1.0e-12f) {
+                const float ot0 = ct0 + s.taucw[ib0][k0], os0 = cs0 + s.ssacw[ib0][k0], oy0 = cy0 + s.asycw[ib0][k0];
+                const float oab = cab + s.tabsc[ib0][k0];
+                if (fabsf(sw2_prologue<float>(ot0, oab, os0, oy0, x.mode, cz).zrpp) < SW2_RESONANCE) {
+                    const int i = atomicAdd(&s.nexact, 1);
+                    if (i < SW2_QCAP) s.qkey[i] = sw2_qkey(tid, k0, true);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < min(s.nexact, SW2_QCAP); i += SW2_THREADS) {
+        const int key = s.qkey[i];
+        const int t = key & 255, k0 = (key >> 8) & 127;
+        bool act_t;
+        const int gt = sw2_lane_g(t, act_t);
+        int ibt = 0;
+        while (gt >= c_sw_ns[ibt + 1]) ++ibt;
+        double v[6];
+        sw2_exact(x, k0, gt, ibt, (key >> 15) != 0, v[0], v[1], v[2], v[3], v[4], v[5]);
+        for (int j = 0; j < 6; ++j) s.qval[i][j] = (float)v[j];
+    }
+    __syncthreads();
     float toa_up = 0, sfc_up = 0, sfc_dn = 0, sfc_dir = 0;
     const int nseg = (nlay + SW2_SEG - 1) / SW2_SEG;
     if (pass == 0 || cloudy) {
