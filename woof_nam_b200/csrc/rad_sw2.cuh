@@ -32,7 +32,7 @@
 
 namespace rad {
 
-constexpr int SW2_WARPS = 8, SW2_THREADS = 256;
+constexpr int SW2_WARPS = 4, SW2_THREADS = 128;
 #ifndef RAD_SW2_SEG
 #define RAD_SW2_SEG 4
 #endif
@@ -311,6 +311,33 @@ __device__ __forceinline__ void sw2_rt_tail(const SwPro<T>& p, T cz, T snt, cons
 }
 
 // ------------------------------------------------------------------------------------------------------
+// Rayleigh optical depth per unit colmol of g-point g, as each taumol band forms taur = colmol * coefficient
+// (phys_rrtm_sw_taumol16..29.cu); band 24 below laytrop interpolates in the species ratio instead (its
+// depths are kept per layer).
+__device__ __forceinline__ float sw2_rayl_coef(int g)
+{
+    int b = 0;
+    while (g >= c_sw_ns[b + 1]) ++b;
+    const int ig = g - c_sw_ns[b];
+    switch (b + 16) {
+    case 16: return ldt(tab<float>(T_SW16_RAYL));
+    case 17: return 6.86e-10f;
+    case 18: return ldt(tab<float>(T_SW18_RAYL));
+    case 19: return 2.29e-09f;
+    case 20: return ldt(tab<float>(T_SW20_RAYL));
+    case 21: return 9.41e-09f;
+    case 22: return 1.54e-08f;
+    case 23: return ldt(tab<float>(T_SW23_RAYL) + ig);
+    case 24: return ldt(tab<float>(T_SW24_RAYLB) + ig);
+    case 25: return ldt(tab<float>(T_SW25_RAYL) + ig);
+    case 26: return ldt(tab<float>(T_SW26_RAYL) + ig);
+    case 27: return ldt(tab<float>(T_SW27_RAYL) + ig);
+    case 28: return ldt(tab<float>(T_SW28_RAYL));
+    default: return 9.30e-11f;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------
 // Shared memory of one sunlit column.
 struct SwSh2 {
     float fac00[NLAY_MAX], fac01[NLAY_MAX], fac10[NLAY_MAX], fac11[NLAY_MAX];
@@ -319,11 +346,13 @@ struct SwSh2 {
     int jp[NLAY_MAX], jt[NLAY_MAX], jt1[NLAY_MAX], indself[NLAY_MAX], indfor[NLAY_MAX];
     float cfrac[NLAY_MAX], cldfrc[NLAY_MAX];
     float taucw[14][NLAY_MAX], ssacw[14][NLAY_MAX], asycw[14][NLAY_MAX], tabsc[14][NLAY_MAX];
-    float taug[SW_NGPT][NLAY_MAX], taur[SW_NGPT][NLAY_MAX];
+    float taug[SW_NGPT][NLAY_MAX];
+    float raylc[SW_NGPT];                      // Rayleigh optical depth per unit colmol (band 24: upper atmosphere)
+    float taur24[8][NLAY_MAX];                 // band 24 Rayleigh optical depth below laytrop
     float sfluxzen[SW_NGPT];
     double rdelp[NLAY_MAX];                    // heatfac / delp, float64
-    double fn[SW2_WARPS][NLAY_MAX + 2];        // per-warp level sums of zsolar * (down - up)
-    double sc[SW2_WARPS][10];                  // per-warp scalar sums
+    double fn[SW2_WARPS][NLAY_MAX + 2];        // per-warp level sums of zsolar * (down - up), passes combined
+    double sc[SW2_WARPS][18];                  // per-warp scalar sums, clear (0..8) and cloudy (9..17)
     float cosz, sntz, ssolar, albbm[2], albdf[2], zcf0, zcf1;
     int laytrop, kmin8, kminw;
     unsigned char low[NLAY_MAX];
@@ -335,15 +364,11 @@ struct SwSh2 {
 struct SwAer {
     float tau[14][NLAY_MAX], tasa[14][NLAY_MAX], tay[14][NLAY_MAX], tabs[14][NLAY_MAX];
 };
-__host__ __device__ constexpr size_t sw2_ckpt_bytes() { return (size_t)(SW2_NSEG - 1) * 2 * SW2_THREADS * sizeof(float); }
+__host__ __device__ constexpr size_t sw2_ckpt_bytes() { return (size_t)(SW2_NSEG - 1) * 4 * SW2_THREADS * sizeof(float); }
 __host__ __device__ constexpr size_t sw2_smem_bytes(bool aer)
 {
     return sizeof(SwSh2) + (aer ? sizeof(SwAer) : 0) + sw2_ckpt_bytes();
 }
-
-struct SwLayerRT {
-    float rb, rd, tb, td, e3, e4;
-};
 
 // Everything the float64 recompute of a layer needs besides the layer index and g-point.
 struct SwExactCtx {
@@ -429,22 +454,39 @@ __device__ __forceinline__ void sw2_rt_mixed(const SwSh2& s, float t0, float tab
     e4 = sw_expm(t0 * snt, ex, true);
 }
 
-// R/T of layer k0 for g-point g in the clear (cloudy_pass = false) or cloudy pass of spcvrtc
-// (spcvrtc.cu:330-460: the cloudy pass blends the clear and cloud-mixture R/T by the layer cloud fraction).
-__device__ __noinline__ SwLayerRT sw2_layer(const SwSh2& s, const SwAer* aer, const SwExactCtx& x, int k0, int g,
-                                               int ib, bool cloudy_pass, float cz, float snt, const float* ex)
+struct SwLayerRT {
+    float rb, rd, tb, td, e3, e4;
+};
+
+__device__ __forceinline__ float sw2_taur(const SwSh2& s, int g, int k0)
 {
-    SwLayerRT L;
+    return (g >= 66 && g < 74 && k0 < s.laytrop) ? s.taur24[g - 66][k0] : s.colmol[k0] * s.raylc[g];
+}
+
+// R/T of layer k0 for g-point g in the clear pass (c) and, for a cloudy column, the cloudy pass (o) of
+// spcvrtc (spcvrtc.cu:330-460: the cloudy pass blends the clear and the cloud-mixture R/T by the layer's
+// cloud fraction).  The clear R/T is computed once and serves both passes.
+struct SwLayerRT2 {
+    SwLayerRT c, o;
+};
+__device__ __noinline__ SwLayerRT2 sw2_layer(const SwSh2& s, const SwAer* aer, const SwExactCtx& x, int k0, int g,
+                                             int ib, bool cloudy, float cz, float snt, const float* ex)
+{
+    SwLayerRT2 r;
+    SwLayerRT& c = r.c;
+    SwLayerRT& o = r.o;
     if (k0 >= x.a->nlay) {   // padding above the model top: a transparent, non-reflecting layer
-        L.rb = 0; L.rd = 0; L.tb = 1; L.td = 1; L.e3 = 1; L.e4 = 1;
-        return L;
+        c.rb = 0; c.rd = 0; c.tb = 1; c.td = 1; c.e3 = 1; c.e4 = 1;
+        o = c;
+        return r;
     }
-    const float tr = s.taur[g][k0], tg = s.taug[g][k0];
+    const float tr = sw2_taur(s, g, k0), tg = s.taug[g][k0];
     float ta = 0, tasa = 0, tay = 0, taab = 0;
     if (aer) { ta = aer->tau[ib][k0]; tasa = aer->tasa[ib][k0]; tay = aer->tay[ib][k0]; taab = aer->tabs[ib][k0]; }
     const float ct0 = fmaxf(1.0e-12f, tr + tg + ta), cs0 = tr + tasa, cy0 = tay, cab = tg + taab;
-    sw2_rt_mixed(s, ct0, cab, cs0, cy0, cz, snt, ex, x, k0, g, ib, false, L.rb, L.rd, L.tb, L.td, L.e3, L.e4);
-    if (cloudy_pass) {
+    sw2_rt_mixed(s, ct0, cab, cs0, cy0, cz, snt, ex, x, k0, g, ib, false, c.rb, c.rd, c.tb, c.td, c.e3, c.e4);
+    o = c;
+    if (cloudy) {
         const float zc1 = s.cldfrc[k0];
         if (zc1 > 1.0e-12f) {
             const float ot0 = ct0 + s.taucw[ib][k0], os0 = cs0 + s.ssacw[ib][k0], oy0 = cy0 + s.asycw[ib][k0];
@@ -452,20 +494,45 @@ __device__ __noinline__ SwLayerRT sw2_layer(const SwSh2& s, const SwAer* aer, co
             float rb2, rd2, tb2, td2, e32, e42;
             sw2_rt_mixed(s, ot0, oab, os0, oy0, cz, snt, ex, x, k0, g, ib, true, rb2, rd2, tb2, td2, e32, e42);
             const float zc0 = 1.0f - zc1;
-            L.rb = zc0 * L.rb + zc1 * rb2;
-            L.rd = zc0 * L.rd + zc1 * rd2;
-            L.tb = zc0 * L.tb + zc1 * tb2;
-            L.td = zc0 * L.td + zc1 * td2;
-            L.e3 = zc0 * L.e3 + zc1 * e32;
-            L.e4 = zc0 * L.e4 + zc1 * e42;
+            o.rb = zc0 * c.rb + zc1 * rb2;
+            o.rd = zc0 * c.rd + zc1 * rd2;
+            o.tb = zc0 * c.tb + zc1 * tb2;
+            o.td = zc0 * c.td + zc1 * td2;
+            o.e3 = zc0 * c.e3 + zc1 * e32;
+            o.e4 = zc0 * c.e4 + zc1 * e42;
         }
     }
-    return L;
+    return r;
 }
 
-// Phase-C thread -> g-point: warps 0-3 the clear pass, 4-7 the cloudy pass; in each pass the four warps take
-// g-points 0-27, 28-55, 56-85 (the Rayleigh-dominated bands 23-26) and 86-111.  Idle lanes mirror the
-// warp's last g-point (act = false).
+// One step of the upward (bottom-up) adding recursion through layer L (swflux.cu, zrupb / zrupd).
+__device__ __forceinline__ void sw2_up(const SwLayerRT& L, float& ub, float& ud)
+{
+    const float den = 1.0f / (1.0f - ud * L.rd);
+    const float ub1 = L.rb + (L.td * ((L.tb - L.e3) * ud + L.e3 * ub)) * den;
+    ud = L.rd + L.td * L.td * ud * den;
+    ub = ub1;
+}
+// Level fluxes from the upward (ub, ud) and downward (tdn, rdn, tdb) states (swflux.cu, zfu / zfd).
+__device__ __forceinline__ void sw2_flux(float ub, float ud, float tdn, float rdn, float tdb, float& fu, float& fd)
+{
+    const float den = 1.0f / (1.0f - rdn * ud);
+    fu = (tdb * ub + (tdn - tdb) * ud) * den;
+    fd = tdb + (tdn - tdb + tdb * ub * rdn) * den;
+}
+// One step of the downward recursion through layer L (swflux.cu, ztdn / zrdnd / ztdbt).
+__device__ __forceinline__ void sw2_down(const SwLayerRT& L, float& tdn, float& rdn, float& tdb)
+{
+    const float den = 1.0f / (1.0f - L.rd * rdn);
+    const float tdn1 = tdb * L.tb + (L.td * ((tdn - tdb) + tdb * L.rb * rdn)) * den;
+    rdn = L.rd + L.td * L.td * rdn * den;
+    tdn = tdn1;
+    tdb = L.e3 * tdb;
+}
+
+// Phase-C thread -> g-point: the four warps take g-points 0-27, 28-55, 56-85 (the Rayleigh-dominated bands
+// 23-26) and 86-111, one per lane; each lane runs both passes of its g-point.  Idle lanes mirror the warp's
+// last g-point (act = false).
 __device__ __forceinline__ int sw2_lane_g(int t, bool& act)
 {
     const int wq = (t >> 5) & 3, lane = t & 31;
@@ -476,7 +543,7 @@ __device__ __forceinline__ int sw2_lane_g(int t, bool& act)
 }
 
 // ------------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(SW2_THREADS, 1)
+__global__ void __launch_bounds__(SW2_THREADS, 2)
 sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -561,18 +628,18 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
         if (ib == 0) s.cldfrc[k0] = s.zcf1 > 0 ? s.cfrac[k0] / s.zcf1 : 0.0f;
     }
     if (tid < 14) sw_sfluxzen<float>(s, tid, nlay);
+    for (int g = tid; g < SW_NGPT; g += SW2_THREADS) s.raylc[g] = sw2_rayl_coef(g);
     __syncthreads();
     // ---- phase B: gas and Rayleigh optical depths per (g, layer), band by band
     for_each_band_pair(c_sw_ns, 14, nlay, tid >> 5, SW2_WARPS, tid & 31, [&](int g, int k0) {
         float tg, tr;
         sw_gas<float>(s, g, k0, tg, tr);
         s.taug[g][k0] = tg;
-        s.taur[g][k0] = tr;
+        if (g >= 66 && g < 74 && k0 < s.laytrop) s.taur24[g - 66][k0] = tr;
     });
     __syncthreads();
-    // ---- phase C: the two passes of spcvrtc, one g-point per lane
+    // ---- phase C: spcvrtc, one g-point per lane, both passes
     const int warp = tid >> 5, lane = tid & 31;
-    const int pass = warp >> 2;
     bool act;
     const int g = sw2_lane_g(tid, act);
     int ib0 = 0;
@@ -587,10 +654,10 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
                  1.0 / (double)__ldg(a.coszen + col), exd};
     // ---- phase C0: layer evaluations near the two-stream resonance (|1 - (k mu0)^2| < SW2_RESONANCE) are
     // queued and recomputed in float64 by all threads of the column, instead of by one lane of a warp
-    // while the other lanes wait; the sweeps below read them back from the queue.
-    if (act && (pass == 0 || cloudy)) {
+    // while the other lanes wait; the sweeps read them back from the queue.
+    if (act) {
         for (int k0 = 0; k0 < nlay; ++k0) {
-            const float tr = s.taur[g][k0], tg = s.taug[g][k0];
+            const float tr = sw2_taur(s, g, k0), tg = s.taug[g][k0];
             float ta = 0, tasa = 0, tay = 0, taab = 0;
             if (aer) { ta = aer->tau[ib0][k0]; tasa = aer->tasa[ib0][k0]; tay = aer->tay[ib0][k0]; taab = aer->tabs[ib0][k0]; }
             const float ct0 = fmaxf(1.0e-12f, tr + tg + ta), cs0 = tr + tasa, cy0 = tay, cab = tg + taab;
@@ -598,7 +665,7 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
                 const int i = atomicAdd(&s.nexact, 1);
                 if (i < SW2_QCAP) s.qkey[i] = sw2_qkey(tid, k0, false);
             }
-            if (pass == 1 && s.cldfrc[k0] > 1.0e-12f) {
+            if (cloudy && s.cldfrc[k0] > 1.0e-12f) {
                 const float ot0 = ct0 + s.taucw[ib0][k0], os0 = cs0 + s.ssacw[ib0][k0], oy0 = cy0 + s.asycw[ib0][k0];
                 const float oab = cab + s.tabsc[ib0][k0];
                 if (fabsf(sw2_prologue<float>(ot0, oab, os0, oy0, x.mode, cz).zrpp) < SW2_RESONANCE) {
@@ -621,119 +688,121 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
         for (int j = 0; j < 6; ++j) s.qval[i][j] = (float)v[j];
     }
     __syncthreads();
-    float toa_up = 0, sfc_up = 0, sfc_dn = 0, sfc_dir = 0;
     const int nseg = (nlay + SW2_SEG - 1) / SW2_SEG;
-    if (pass == 0 || cloudy) {
-        const bool cp = pass == 1;
-        // upward sweep: reflectances of the atmosphere below each level (swflux.cu, zrupb/zrupd)
-        float ub = ab, ud = ad;
-        for (int sg = 0; sg < nseg; ++sg) {
-            if (sg > 0) {
-                ckpt[((sg - 1) * 2 + 0) * SW2_THREADS + tid] = ub;
-                ckpt[((sg - 1) * 2 + 1) * SW2_THREADS + tid] = ud;
-            }
-#pragma unroll 2
-            for (int j = 0; j < SW2_SEG; ++j) {
-                const SwLayerRT L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cp, cz, snt, ex);
-                const float den = 1.0f / (1.0f - ud * L.rd);
-                ub = L.rb + (L.td * ((L.tb - L.e3) * ud + L.e3 * ub)) * den;
-                ud = L.rd + L.td * L.td * ud * den;
-            }
+    float* ck = ckpt + tid;
+    auto CK = [&](int sg, int q) -> float& { return ck[((sg - 1) * 4 + q) * SW2_THREADS]; };
+    // upward sweep: reflectances of the atmosphere below each level, clear (c) and cloudy (o) passes
+    float ubc = ab, udc = ad, ubo = ab, udo = ad;
+    for (int sg = 0; sg < nseg; ++sg) {
+        if (sg > 0) { CK(sg, 0) = ubc; CK(sg, 1) = udc; CK(sg, 2) = ubo; CK(sg, 3) = udo; }
+        for (int j = 0; j < SW2_SEG; ++j) {
+            const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, cz, snt, ex);
+            sw2_up(L.c, ubc, udc);
+            if (cloudy) sw2_up(L.o, ubo, udo);
         }
-        // downward sweep, segment by segment from the top
-        float tdn = 1, rdn = 0, tdb = 1, tdb0 = 1;
-        for (int sg = nseg - 1; sg >= 0; --sg) {
-            float zub[SW2_SEG + 1], zud[SW2_SEG + 1];
-            float rb[SW2_SEG], rd[SW2_SEG], tb[SW2_SEG], td[SW2_SEG], e3[SW2_SEG];
-            float e4p = 1;
-            zub[0] = sg ? ckpt[((sg - 1) * 2 + 0) * SW2_THREADS + tid] : ab;
-            zud[0] = sg ? ckpt[((sg - 1) * 2 + 1) * SW2_THREADS + tid] : ad;
-#pragma unroll
-            for (int j = 0; j < SW2_SEG; ++j) {
-                const SwLayerRT L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cp, cz, snt, ex);
-                rb[j] = L.rb; rd[j] = L.rd; tb[j] = L.tb; td[j] = L.td; e3[j] = L.e3;
-                e4p = e4p * L.e4;
-                const float den = 1.0f / (1.0f - zud[j] * L.rd);
-                zub[j + 1] = L.rb + (L.td * ((L.tb - L.e3) * zud[j] + L.e3 * zub[j])) * den;
-                zud[j + 1] = L.rd + L.td * L.td * zud[j] * den;
-            }
-#pragma unroll
-            for (int j = SW2_SEG - 1; j >= 0; --j) {
-                const int lev = sg * SW2_SEG + j + 2;        // level above layer j (1 = surface)
-                if (lev <= nlp1) {
-                    const float den = 1.0f / (1.0f - rdn * zud[j + 1]);
-                    const float fu = (tdb * zub[j + 1] + (tdn - tdb) * zud[j + 1]) * den;
-                    const float fd = tdb + (tdn - tdb + tdb * zub[j + 1] * rdn) * den;
-                    double v = act ? (double)zsolar * ((double)fd - (double)fu) : 0.0;
-                    v = warp_sum(v);
-                    if (lane == 0) s.fn[warp][lev - 1] = v;
-                    if (lev == nlp1) toa_up = fu;
-                }
-                const float den = 1.0f / (1.0f - rd[j] * rdn);
-                const float tdn1 = tdb * tb[j] + (td[j] * ((tdn - tdb) + tdb * rb[j] * rdn)) * den;
-                rdn = rd[j] + td[j] * td[j] * rdn * den;
-                tdn = tdn1;
-                tdb = e3[j] * tdb;
-            }
-            tdb0 = tdb0 * e4p;
-        }
-        // surface level
-        {
-            const float den = 1.0f / (1.0f - rdn * ad);
-            const float fu = (tdb * ab + (tdn - tdb) * ad) * den;
-            const float fd = tdb + (tdn - tdb + tdb * ab * rdn) * den;
-            double v = act ? (double)zsolar * ((double)fd - (double)fu) : 0.0;
-            v = warp_sum(v);
-            if (lane == 0) s.fn[warp][0] = v;
-            sfc_up = fu;
-            sfc_dn = fd;
-            sfc_dir = tdb0;
-        }
-    } else {
-        for (int k = lane; k <= nlay; k += 32) s.fn[warp][k] = 0;
     }
-    {
-        // per-lane scalars (zero for idle lanes and for the cloudy warps of a clear column)
-        double scv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        if (act && (pass == 0 || cloudy)) {
-            const double zs = (double)zsolar;
-            scv[0] = zs * (double)toa_up;
-            scv[1] = zs * (double)sfc_up;
-            scv[2] = zs * (double)sfc_dn;
-            scv[3] = ib0 == 11 ? zs * (double)sfc_dn : 0.0;
-            const double zb1 = (double)(zsolar * sfc_dir), zb2 = (double)(zsolar * (sfc_dn - sfc_dir));
-            if (ibd == 1) { scv[4] = zb1; scv[5] = zb2; }
-            else if (ibd == 2) { scv[6] = zb1; scv[7] = zb2; }
-            else { scv[4] = 0.5 * zb1; scv[5] = 0.5 * zb2; scv[6] = 0.5 * zb1; scv[7] = 0.5 * zb2; }
-            scv[8] = zs;
+    // downward sweep, segment by segment from the top: recompute the segment's R/T and upward states into
+    // registers from its checkpoint, then walk down through it
+    const double w0 = cloudy ? (double)s.zcf0 : 1.0, w1 = cloudy ? (double)s.zcf1 : 0.0;
+    float tdnc = 1, rdnc = 0, tdbc = 1, tdbc0 = 1, tdno = 1, rdno = 0, tdbo = 1, tdbo0 = 1;
+    float toa_c = 0, toa_o = 0;
+    for (int sg = nseg - 1; sg >= 0; --sg) {
+        SwLayerRT Lc[SW2_SEG], Lo[SW2_SEG];
+        float zubc[SW2_SEG + 1], zudc[SW2_SEG + 1], zubo[SW2_SEG + 1], zudo[SW2_SEG + 1];
+        zubc[0] = sg ? CK(sg, 0) : ab;
+        zudc[0] = sg ? CK(sg, 1) : ad;
+        zubo[0] = sg ? CK(sg, 2) : ab;
+        zudo[0] = sg ? CK(sg, 3) : ad;
+        float e4c = 1, e4o = 1;
+#pragma unroll
+        for (int j = 0; j < SW2_SEG; ++j) {
+            const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, cz, snt, ex);
+            Lc[j] = L.c;
+            Lo[j] = L.o;
+            zubc[j + 1] = zubc[j]; zudc[j + 1] = zudc[j];
+            sw2_up(Lc[j], zubc[j + 1], zudc[j + 1]);
+            e4c = e4c * Lc[j].e4;
+            if (cloudy) {
+                zubo[j + 1] = zubo[j]; zudo[j + 1] = zudo[j];
+                sw2_up(Lo[j], zubo[j + 1], zudo[j + 1]);
+                e4o = e4o * Lo[j].e4;
+            }
         }
 #pragma unroll
-        for (int i = 0; i < 9; ++i) {
-            const double v = warp_sum(scv[i]);
-            if (lane == 0) s.sc[warp][i] = v;
+        for (int j = SW2_SEG - 1; j >= 0; --j) {
+            const int lev = sg * SW2_SEG + j + 2;        // level above layer j (1 = surface)
+            if (lev <= nlp1) {
+                float fu, fd;
+                sw2_flux(zubc[j + 1], zudc[j + 1], tdnc, rdnc, tdbc, fu, fd);
+                double net = w0 * ((double)fd - (double)fu);
+                if (lev == nlp1) toa_c = fu;
+                if (cloudy) {
+                    float fuo, fdo;
+                    sw2_flux(zubo[j + 1], zudo[j + 1], tdno, rdno, tdbo, fuo, fdo);
+                    net += w1 * ((double)fdo - (double)fuo);
+                    if (lev == nlp1) toa_o = fuo;
+                }
+                const double v = warp_sum(act ? (double)zsolar * net : 0.0);
+                if (lane == 0) s.fn[warp][lev - 1] = v;
+            }
+            sw2_down(Lc[j], tdnc, rdnc, tdbc);
+            if (cloudy) sw2_down(Lo[j], tdno, rdno, tdbo);
         }
+        tdbc0 = tdbc0 * e4c;
+        tdbo0 = tdbo0 * e4o;
+    }
+    // surface level, and the per-lane scalars (zero for idle lanes)
+    double scv[18];
+#pragma unroll
+    for (int i = 0; i < 18; ++i) scv[i] = 0;
+    {
+        float fu, fd, fuo = 0, fdo = 0;
+        sw2_flux(ab, ad, tdnc, rdnc, tdbc, fu, fd);
+        double net = w0 * ((double)fd - (double)fu);
+        if (cloudy) {
+            sw2_flux(ab, ad, tdno, rdno, tdbo, fuo, fdo);
+            net += w1 * ((double)fdo - (double)fuo);
+        }
+        const double v = warp_sum(act ? (double)zsolar * net : 0.0);
+        if (lane == 0) s.fn[warp][0] = v;
+        if (act) {
+            const double zs = (double)zsolar;
+            // slots: 0 toa up, 1 sfc up, 2 sfc dn, 3 uv-b, 4 nir beam, 5 nir diffuse, 6 vis beam, 7 vis diffuse, 8 toa down
+            auto fill = [&](double* o, float tu, float su, float sd, float sdir) {
+                o[0] = zs * (double)tu;
+                o[1] = zs * (double)su;
+                o[2] = zs * (double)sd;
+                o[3] = ib0 == 11 ? zs * (double)sd : 0.0;
+                const double zb1 = (double)(zsolar * sdir), zb2 = (double)(zsolar * (sd - sdir));
+                if (ibd == 1) { o[4] = zb1; o[5] = zb2; }
+                else if (ibd == 2) { o[6] = zb1; o[7] = zb2; }
+                else { o[4] = 0.5 * zb1; o[5] = 0.5 * zb2; o[6] = 0.5 * zb1; o[7] = 0.5 * zb2; }
+                o[8] = zs;
+            };
+            fill(scv, toa_c, fu, fd, tdbc0);
+            if (cloudy) fill(scv + 9, toa_o, fuo, fdo, tdbo0);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 18; ++i) {
+        const double v = warp_sum(scv[i]);
+        if (lane == 0) s.sc[warp][i] = v;
     }
     __syncthreads();
     // ---- column end (spcvrtc.cu:493-545) and swrad_post (swrad.cu:365-403), float64
     const double c1d = (double)s.zcf1, c0d = (double)s.zcf0;
     auto tot = [&](double clr, double cld) { return cloudy ? c1d * cld + c0d * clr : clr; };
     for (int k = tid; k < nlay; k += SW2_THREADS) {
-        double a0 = 0, a1 = 0, b0 = 0, b1 = 0;
-        for (int w = 0; w < 4; ++w) {
-            a0 += s.fn[w][k]; a1 += s.fn[w][k + 1];
-            b0 += s.fn[4 + w][k]; b1 += s.fn[4 + w][k + 1];
-        }
-        const double fk = tot(a0, b0), fk1 = tot(a1, b1);
-        a.htsw[(size_t)(nlay - 1 - k) * N + col] = (float)((fk1 - fk) * s.rdelp[k]);
+        double f0 = 0, f1 = 0;
+        for (int w = 0; w < SW2_WARPS; ++w) { f0 += s.fn[w][k]; f1 += s.fn[w][k + 1]; }
+        a.htsw[(size_t)(nlay - 1 - k) * N + col] = (float)((f1 - f0) * s.rdelp[k]);
     }
     if (tid == 0) {
         double c[9], t[9];
         for (int i = 0; i < 9; ++i) {
             c[i] = 0; t[i] = 0;
-            for (int w = 0; w < 4; ++w) { c[i] += s.sc[w][i]; t[i] += s.sc[4 + w][i]; }
+            for (int w = 0; w < SW2_WARPS; ++w) { c[i] += s.sc[w][i]; t[i] += s.sc[w][9 + i]; }
         }
-        // slots: 0 toa up, 1 sfc up, 2 sfc dn, 3 uv-b, 4 nir beam, 5 nir diffuse, 6 vis beam, 7 vis diffuse,
-        // 8 toa down
         a.topfsw[col] = (float)tot(c[0], t[0]);
         a.topfsw[N + col] = (float)c[8];
         a.topfsw[2 * N + col] = (float)c[0];
