@@ -74,7 +74,8 @@ typedef struct {
     const float* tsfg;       /* [ncol] ground temperature, K (RAD_TSFG) */
     const float* sfcalb;     /* [4][ncol] nir-beam, nir-diffuse, uv-vis beam, uv-vis diffuse (SFCALB) */
     const float* coszen;     /* [ncol] cosine of the solar zenith angle (SW_COSZEN) */
-    const int32_t* icseed;   /* [ncol] McICA permutation seeds or NULL */
+    const int32_t* icseed;   /* [2][ncol] McICA seeds, LW row then SW row (icsdlw, icsdsw), or NULL for
+                                seed0 + column + 1 (isubcl 1, radlw/radsw_main_nmmb.f) */
     float solcon;            /* solar constant of this call, W/m2 */
 } RadColumns;
 
@@ -87,8 +88,9 @@ typedef struct {
     float* topfsw;           /* [3][ncol] TOA SW: up total, down, up clear    (TOPFLX) */
     float* sfcfsw;           /* [4][ncol] sfc SW: up total, down total, up clear, down clear (SFCFLX) */
     float* fdncmp;           /* [6][ncol] uvbf0 uvbfc nirbm nirdf visbm visdf (FDNCMP), optional */
-    uint32_t* lw_mask;       /* [5][nlay][ncol] McICA LW cloud bits, optional (McICA route) */
-    uint32_t* sw_mask;       /* [4][nlay][ncol] McICA SW cloud bits, optional (McICA route) */
+    uint32_t* lw_mask;       /* [5][nlay][ncol] McICA LW sub-column cloud words, optional (McICA route):
+                                bit g & 31 of word g >> 5 for g-point g, layers surface first (lcloudy) */
+    uint32_t* sw_mask;       /* [4][nlay][ncol] McICA SW sub-column cloud words, optional, same packing */
 } RadOutputs;
 
 /* Library version (RAD_ABI_VERSION).  Replaces: nothing in the reference (a versioned ABI). */

@@ -187,3 +187,22 @@ def opcount(cols, iswmode: int = 2, cpathfac: float = 1.5) -> dict:
                        for i, s in enumerate(OPCOUNT_STAGES)},
             "ncol": n, "nday": nd, "lw_flops_per_col": lw, "sw_flops_per_daycol": sw,
             "flops_per_col": lw + sw * nd / n}
+
+
+def mcica_masks(cols, which: str = "port", iovrlw: int = 1, iovrsw: int = 1, lw_seed0: int = 140,
+                sw_seed0: int = 1, icseed=None) -> dict:
+    """McICA sub-column masks of a request: lw uint32 [5][nlay][ncol], sw uint32 [4][nlay][ncol], layers
+    surface first (bit g & 31 of word g >> 5).  icseed: optional int32 [2][ncol] (LW row, SW row)."""
+    L = lib(which)
+    nlay, ncol = cols.nlay, cols.ncol
+    cfg = np.array([2, 0, 0, 32768, 1, iovrlw, iovrsw, lw_seed0, sw_seed0], dtype=np.int32)
+    lw = np.zeros((5, nlay, ncol), dtype=np.uint32)
+    sw = np.zeros((4, nlay, ncol), dtype=np.uint32)
+    cl = _f(cols.clouds)
+    seeds = np.ascontiguousarray(icseed, dtype=np.int32) if icseed is not None else None
+    rc = L.orc_mcica_masks(cfg.ctypes.data_as(_I), ctypes.c_int(nlay), ctypes.c_int(ncol), cl.ctypes.data_as(_F),
+                           seeds.ctypes.data_as(_I) if seeds is not None else None,
+                           lw.ctypes.data_as(_U), sw.ctypes.data_as(_U))
+    if rc != 0:
+        raise RuntimeError("mcica_masks failed")
+    return {"lw": lw, "sw": sw}

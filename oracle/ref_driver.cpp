@@ -83,6 +83,14 @@ namespace r_b16 {
 namespace r_rtrnmr {
 #include "phys_rrtm_lw_rtrnmr.cu"
 }
+namespace r_lwmc {
+#include "phys_rrtm_lw_mcica_subcol.cu"
+}
+#undef MCICA_NGPTLW
+#undef MCICA_NWORD
+namespace r_swmc {
+#include "phys_rrtm_sw_mcica_subcol.cu"
+}
 namespace r_swrad {
 #include "phys_rrtm_sw_swrad.cu"
 }
@@ -974,6 +982,39 @@ void run_sw(const Req& q, double* htsw, double* topfsw, double* sfcfsw, double* 
 }  // namespace drv
 
 extern "C" {
+
+// McICA sub-column masks of a request from the reference's generator kernels: LW words [5][nlay][ncol]
+// from the LW cloud fraction (cldprop: the input cloud fraction, zero for a column with no layer above
+// 1e-6), SW words [4][nlay][ncol] from the input cloud fraction (the kernel applies the 1e-12 step);
+// layers surface first.  Seeds: icseed [2][ncol] (LW row, SW row) or seed0 + column + 1.
+int orc_mcica_masks(const int* cfg_i, int nlay, int ncol, const float* clouds, const int* icseed,
+                    unsigned int* lw_out, unsigned int* sw_out)
+{
+    const int iovrlw = cfg_i[5], iovrsw = cfg_i[6], lw_seed0 = cfg_i[7], sw_seed0 = cfg_i[8];
+    std::vector<float> cf((size_t)nlay * ncol), cfl((size_t)nlay * ncol, 0.0f);
+    std::vector<int> slw(ncol), ssw(ncol);
+    for (int c = 0; c < ncol; ++c) {
+        bool any = false;
+        for (int k0 = 0; k0 < nlay; ++k0) {
+            const float x = clouds[(size_t)(nlay - 1 - k0) * ncol + c];
+            cf[(size_t)k0 * ncol + c] = x;
+            any = any || x > 1.0e-6f;
+        }
+        if (any)
+            for (int k0 = 0; k0 < nlay; ++k0) cfl[(size_t)k0 * ncol + c] = cf[(size_t)k0 * ncol + c];
+        slw[c] = icseed ? icseed[c] : lw_seed0 + c + 1;
+        ssw[c] = icseed ? icseed[(size_t)ncol + c] : sw_seed0 + c + 1;
+    }
+    if (lw_out)
+        drv::launch(drv::cdiv(ncol, 128), 1, 1, 128, [&] {
+            r_lwmc::phys_rrtm_lw_mcica_subcol(cfl.data(), slw.data(), lw_out, nlay, 1, ncol, iovrlw);
+        });
+    if (sw_out)
+        drv::launch(drv::cdiv(ncol, 128), 1, 1, 128, [&] {
+            r_swmc::phys_rrtm_sw_mcica_subcol(cf.data(), ssw.data(), sw_out, nlay, 1, ncol, iovrsw);
+        });
+    return 0;
+}
 
 int orc_set_debug(double sw_tau_scale)
 {

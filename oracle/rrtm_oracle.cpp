@@ -119,6 +119,15 @@ static void run_sw(const Config& cfg, const Inputs& in, const Outputs& out)
         for (int i = 0; i < 6 * ncol; ++i) out.fdncmp[i] = 0;
     if (out.swflx)
         for (size_t i = 0; i < (size_t)4 * nlp1 * ncol; ++i) out.swflx[i] = 0;
+    if (cfg.route == 1 && out.sw_mask) {   // the SW generator runs over every column, as the reference's does
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int col = 0; col < ncol; ++col) {
+            std::vector<uint32_t> w;
+            sw_mcica_words(cfg, in, col, w);
+            for (int ww = 0; ww < 4; ++ww)
+                for (int k0 = 0; k0 < nlay; ++k0) out.sw_mask[((size_t)ww * nlay + k0) * ncol + col] = w[(size_t)ww * nlay + k0];
+        }
+    }
     std::vector<int> day;
     for (int col = 0; col < ncol; ++col)
         if (in.coszen[col] >= 1.0e-4f) day.push_back(col);
@@ -262,6 +271,44 @@ int orc_sw_stages(const int* cfg_i, int nlay, int ncol, const float* plyr, const
     } catch (const std::exception& e) {
         std::fprintf(stderr, "oracle: %s\n", e.what());
         return -1;
+    }
+    return 0;
+}
+
+// McICA sub-column masks of a request (the restatement of the generators; same layout and seeds as the
+// reference driver's orc_mcica_masks).
+int orc_mcica_masks(const int* cfg_i, int nlay, int ncol, const float* clouds, const int* icseed,
+                    unsigned int* lw_out, unsigned int* sw_out)
+{
+    using namespace orc;
+    Config cfg;
+    cfg.iovrlw = cfg_i[5];
+    cfg.iovrsw = cfg_i[6];
+    cfg.lw_seed0 = cfg_i[7];
+    cfg.sw_seed0 = cfg_i[8];
+    Inputs in{};
+    in.clouds = clouds;
+    in.icseed = icseed;
+    in.nlay = nlay;
+    in.ncol = ncol;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int c = 0; c < ncol; ++c) {
+        std::vector<uint32_t> w;
+        if (lw_out) {
+            std::vector<float> cf(nlay, 0.0f);
+            bool any = false;
+            for (int k0 = 0; k0 < nlay; ++k0) any = any || clouds[(size_t)(nlay - 1 - k0) * ncol + c] > 1.0e-6f;
+            if (any)
+                for (int k0 = 0; k0 < nlay; ++k0) cf[k0] = clouds[(size_t)(nlay - 1 - k0) * ncol + c];
+            mcica_bits(cf, nlay, 140, cfg.iovrlw, icseed ? icseed[c] : cfg.lw_seed0 + c + 1, w);
+            for (int ww = 0; ww < 5; ++ww)
+                for (int k0 = 0; k0 < nlay; ++k0) lw_out[((size_t)ww * nlay + k0) * ncol + c] = w[(size_t)ww * nlay + k0];
+        }
+        if (sw_out) {
+            sw_mcica_words(cfg, in, c, w);
+            for (int ww = 0; ww < 4; ++ww)
+                for (int k0 = 0; k0 < nlay; ++k0) sw_out[((size_t)ww * nlay + k0) * ncol + c] = w[(size_t)ww * nlay + k0];
+        }
     }
     return 0;
 }

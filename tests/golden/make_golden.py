@@ -13,6 +13,8 @@ vectors are committed:
     swq_*           SW outputs with every gas optical depth scaled by 1e-3 before the two-stream solver
                     (finite everywhere; pins the solver arithmetic)
     st_*            SW stage outputs (taug, taur, sfluxzen, cloud optics, laytrop) of the first 6 day columns
+    mc{0,1,2}_*     McICA sub-column cloud words of the reference's LW / SW generators, overlap 0, 1, 2
+    mcseed, mcs_*   the same for explicit seeds (overlap 1)
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -58,6 +60,15 @@ def main():
         st = oracle.sw_stages(cols, which="ref")
         for k, v in st.items():
             blob[f"{case}_st_{k}"] = v[:NSTAGE]
+        for iovr in (0, 1, 2):
+            m = oracle.mcica_masks(cols, which="ref", iovrlw=iovr, iovrsw=iovr)
+            blob[f"{case}_mc{iovr}_lw"] = m["lw"]
+            blob[f"{case}_mc{iovr}_sw"] = m["sw"]
+        seeds = np.random.default_rng(seed).integers(-2**31, 2**31 - 1, size=(2, ncol)).astype(np.int32)
+        m = oracle.mcica_masks(cols, which="ref", icseed=seeds)
+        blob[f"{case}_mcseed"] = seeds
+        blob[f"{case}_mcs_lw"] = m["lw"]
+        blob[f"{case}_mcs_sw"] = m["sw"]
     np.savez_compressed(OUT, **blob)
     print(f"wrote {OUT} ({OUT.stat().st_size / 1e3:.0f} kB)")
 

@@ -106,3 +106,17 @@ def test_windows_change_only_group_minima():
     b = oracle.solve(cols, precision="double", window_cols=16)
     assert np.array_equal(a["htlw"], b["htlw"])
     assert np.isfinite(b["htsw"]).all()
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_mcica_masks_bit_exact(golden, case):
+    """McICA sub-column words of the restated generators equal the reference kernels' (MT19937 stream,
+    overlap 0/1/2, default and explicit seeds)."""
+    cols = golden_columns(golden, case)
+    for iovr in (0, 1, 2):
+        m = oracle.mcica_masks(cols, iovrlw=iovr, iovrsw=iovr)
+        assert np.array_equal(m["lw"], golden[f"{case}_mc{iovr}_lw"]), iovr
+        assert np.array_equal(m["sw"], golden[f"{case}_mc{iovr}_sw"]), iovr
+    m = oracle.mcica_masks(cols, icseed=golden[f"{case}_mcseed"])
+    assert np.array_equal(m["lw"], golden[f"{case}_mcs_lw"])
+    assert np.array_equal(m["sw"], golden[f"{case}_mcs_sw"])

@@ -34,6 +34,7 @@ __constant__ int c_sw_ns[15] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94
 #include "rad_sw.cuh"
 #include "rad_sw2.cuh"
 #include "rad_lw2.cuh"
+#include "rad_mcica.cuh"
 
 using namespace rad;
 
@@ -49,6 +50,8 @@ struct RadHandle {
     int *d_flag = nullptr, *d_pos = nullptr, *d_daycol = nullptr, *d_lt = nullptr, *d_k8 = nullptr, *d_kw = nullptr;
     int *d_cmin = nullptr, *d_nday = nullptr;
     int64_t cmin_cap = 0;
+    uint32_t *d_lwm = nullptr, *d_swm = nullptr;   // McICA sub-column words when the caller passes no mask
+    int64_t mask_cap = 0;                          // columns x layers the mask scratch holds
     void* d_cub = nullptr;
     size_t cub_bytes = 0;
     std::string err;
@@ -179,7 +182,7 @@ void sw_lut(std::vector<R>& v)   // exp_tbl(0:10000) (phys_rrtm_sw_spcvrtc.py:60
 // The plain FP64 precision runs the first-design kernels (lw_column_kernel / sw_column_kernel<double>);
 // the mixed precision runs the production kernels (lw2_column_kernel<float> / sw2_column_kernel).
 template <class R>
-void* kernel_ptr_lw() { return sizeof(R) == 4 ? (void*)lw2_column_kernel<float> : (void*)lw_column_kernel<double>; }
+void* kernel_ptr_lw(bool mc) { return sizeof(R) == 4 ? (mc ? (void*)lw2_column_kernel<float, true> : (void*)lw2_column_kernel<float, false>) : (void*)lw_column_kernel<double>; }
 template <class R>
 void* kernel_ptr_sw() { return (void*)sw_column_kernel<R>; }
 
@@ -213,6 +216,38 @@ int ensure_scratch(RadHandle* h, int64_t n)
     return RAD_OK;
 }
 
+// McICA: LW and SW sub-column words of every column, into the caller's mask outputs when given, else into
+// the handle's scratch.  Seeds: icseed [2][ncol] (LW row, SW row) or seed0 + column + 1.
+int mcica_masks(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t n, cudaStream_t st,
+                const uint32_t** lwm, const uint32_t** swm)
+{
+    const RadConfig& cfg = h->cfg;
+    const int nlay = cfg.nlay;
+    uint32_t* lw = out->lw_mask;
+    uint32_t* sw = out->sw_mask;
+    if (!lw || !sw) {
+        if (n * nlay > h->mask_cap) {
+            if (h->d_lwm) cudaFree(h->d_lwm);
+            if (h->d_swm) cudaFree(h->d_swm);
+            h->d_lwm = h->d_swm = nullptr;
+            h->mask_cap = 0;
+            RAD_CUDA(h, cudaMalloc((void**)&h->d_lwm, (size_t)5 * nlay * n * sizeof(uint32_t)));
+            RAD_CUDA(h, cudaMalloc((void**)&h->d_swm, (size_t)4 * nlay * n * sizeof(uint32_t)));
+            h->mask_cap = n * nlay;
+        }
+        if (!lw) lw = h->d_lwm;
+        if (!sw) sw = h->d_swm;
+    }
+    const unsigned grid = (unsigned)((n + MC_WARPS - 1) / MC_WARPS);
+    k_mcica<140><<<grid, MC_WARPS * 32, 0, st>>>(in->clouds, n, nlay, in->icseed, 0, cfg.lw_seed0, cfg.iovrlw, 1, lw);
+    k_mcica<112><<<grid, MC_WARPS * 32, 0, st>>>(in->clouds, n, nlay, in->icseed, 1, cfg.sw_seed0, cfg.iovrsw, 0, sw);
+    h->launches += 2;
+    RAD_CUDA(h, cudaGetLastError());
+    *lwm = lw;
+    *swm = sw;
+    return RAD_OK;
+}
+
 // Record the next profiling event on st (no-op while profiling is off).
 int mark(RadHandle* h, cudaStream_t st, size_t base, int i)
 {
@@ -240,21 +275,30 @@ int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int6
     }
     int mrc = mark(h, st, eb, 0);
     if (mrc) return mrc;
+    // ---- McICA route: sub-column cloud words of every column (LW and SW generators)
+    const uint32_t *lwm = nullptr, *swm = nullptr;
+    if (cfg.route == RAD_ROUTE_MCICA) {
+        const int mrc2 = mcica_masks(h, in, out, n, st, &lwm, &swm);
+        if (mrc2) return mrc2;
+    }
     // ---- LW over every column
     {
         LwIn a{in->plyr, in->plvl, in->tlyr, in->tlvl, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faerlw,
-               in->sfcemis, in->tsfg, out->htlw, out->topflw, out->sfcflw, n, 0, nlay, cfg.diagnostic, cfg.cpathfac};
+               in->sfcemis, in->tsfg, out->htlw, out->topflw, out->sfcflw, n, 0, nlay, cfg.diagnostic, cfg.cpathfac,
+               lwm};
         LwLut<R> lut;
         const R* base = sizeof(R) == 4 ? (const R*)h->d_lwf : (const R*)h->d_lwd;
         lut.ex = base; lut.tfn = base + 10001; lut.tau = base + 2 * 10001;
         const size_t smem = sizeof(LwShared<R>);
-        RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_lw<R>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_lw<R>(lwm != nullptr), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const int64_t maxg = 1 << 30;
         for (int64_t c0 = 0; c0 < n; c0 += maxg) {
             a.col0 = c0;
             const int64_t nb = std::min<int64_t>(maxg, n - c0);
-            if (sizeof(R) == 4)
-                lw2_column_kernel<R><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
+            if (sizeof(R) == 4 && lwm)
+                lw2_column_kernel<R, true><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
+            else if (sizeof(R) == 4)
+                lw2_column_kernel<R, false><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
             else
                 lw_column_kernel<R><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
             h->launches += 1;
@@ -296,7 +340,7 @@ int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int6
     {
         SwIn a{in->plyr, in->plvl, in->tlyr, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faersw, in->sfcalb,
                in->coszen, h->d_daycol, h->d_nday, h->d_k8, h->d_kw, out->htsw, out->topfsw, out->sfcfsw,
-               out->fdncmp, n, nlay, cfg.diagnostic, cfg.iswmode, in->solcon};
+               out->fdncmp, n, nlay, cfg.diagnostic, cfg.iswmode, in->solcon, swm};
         if ((mrc = mark(h, st, eb, 2))) return mrc;
         if (sizeof(R) == 4) {
             const size_t smem = sw2_smem_bytes(in->faersw != nullptr);
@@ -348,7 +392,10 @@ int rad_create(const RadConfig* cfg, RadHandle** out)
         return fail(nullptr, RAD_E_INVALID, "rad_create: precision must be RAD_PREC_FP64 or RAD_PREC_MIXED");
     if (cfg->route != RAD_ROUTE_NAM && cfg->route != RAD_ROUTE_MCICA)
         return fail(nullptr, RAD_E_INVALID, "rad_create: unknown route");
-    if (cfg->route == RAD_ROUTE_MCICA) return fail(nullptr, RAD_E_INVALID, "rad_create: the McICA route is not built in this library version");
+    if (cfg->route == RAD_ROUTE_MCICA && cfg->precision != RAD_PREC_MIXED)
+        return fail(nullptr, RAD_E_INVALID, "rad_create: the McICA route runs in the mixed precision");
+    if (cfg->route == RAD_ROUTE_MCICA && (cfg->iovrlw < 0 || cfg->iovrlw > 2 || cfg->iovrsw < 0 || cfg->iovrsw > 2))
+        return fail(nullptr, RAD_E_INVALID, "rad_create: iovrlw and iovrsw must be 0, 1 or 2");
     RadHandle* h = new RadHandle();
     h->cfg = *cfg;
     cudaGetDevice(&h->device);
@@ -451,6 +498,10 @@ int rad_load_tables(RadHandle* h, const void* blob, size_t nbytes)
         RAD_CUDA(h, cudaMemcpyToSymbol(c_tf, &tf, sizeof(float*)));
         RAD_CUDA(h, cudaMemcpyToSymbol(c_td, &td, sizeof(double*)));
         RAD_CUDA(h, cudaMemcpyToSymbol(c_lwk, &k, sizeof(k)));
+        uint32_t pw[624];
+        pw[0] = 1u;
+        for (int i = 1; i < 624; ++i) pw[i] = 69069u * pw[i - 1];
+        RAD_CUDA(h, cudaMemcpyToSymbol(c_mt_pow, pw, sizeof(pw)));
         RAD_CUDA(h, cudaDeviceSynchronize());
         dt.tf = tf;
         dt.td = td;
@@ -534,7 +585,8 @@ void rad_destroy(RadHandle* h)
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     for (void* p : {(void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
                     (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
-                    (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub})
+                    (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub, (void*)h->d_lwm,
+                    (void*)h->d_swm})
         if (p) cudaFree(p);
     delete h;
 }

@@ -39,6 +39,7 @@ struct LwShared {
     int lstu[NLAY_MAX + 2], lstd[NLAY_MAX + 2];
     double fnet[LW_WARPS][NLAY_MAX + 1];      // per-warp partial of sum_g (up - down) per level
     double fnet2[LW_WARPS][NLAY_MAX + 1];     // second per-warp level partial (the downward sums of lw2)
+    uint32_t mcw[5][NLAY_MAX];                // McICA route: the column's sub-column cloud words
     double scal[LW_WARPS][8];                 // per-warp partials: toa up, toa up clr, sfc up/dn, clr up/dn
     R secdiff[16], semiss[16];
     R stemp, pwvcm;
@@ -512,6 +513,7 @@ struct LwIn {
     int64_t ncol, col0;       // this launch covers columns [col0, col0 + gridDim.x) of an ncol request
     int nlay, diagnostic;
     float cpathfac;
+    const uint32_t* mask;     // McICA route: sub-column cloud words [5][nlay][ncol] (null: NAM route)
 };
 
 // ------------------------------------------------------------------------------------------------------

@@ -62,7 +62,10 @@ __device__ __forceinline__ LwTerms<R> lw2_terms(const LwShared<R>& s, const LwLu
     return t;
 }
 
-template <class R>
+// MC = false: the NAM route (rtrnmr, maximum-random overlap of the layer cloud fractions).
+// MC = true: the McICA route (rtrnmc, phys_rrtm_lw_rtrnmc.cu:85-310): a layer is cloudy for g-point g
+// when its sub-column bit is set, with effective clear fraction 1 - (1 - exp(-odcld)).
+template <class R, bool MC>
 __global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(LwIn a, LwLut<R> lut, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -75,6 +78,9 @@ __global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(LwIn a, LwLut
         if (tid == 0 && nlay > NLAY_MAX) atomicExch(err, RAD_DEV_NLAY);
         return;
     }
+    if (MC)
+        for (int i = tid; i < 5 * nlay; i += LW_THREADS)
+            s.mcw[i / nlay][i % nlay] = __ldg(a.mask + ((size_t)(i / nlay) * nlay + (i % nlay)) * N + col);
     lw_setup<R, LW_THREADS>(s, a, col, tid);
     const R eps = (R)1.0e-6f;
     const int warp = tid >> 5, lane = tid & 31;
@@ -86,6 +92,20 @@ __global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(LwIn a, LwLut
     // ---- downward sweep (top to surface): per level, the warp's sum of the total-sky radiance
     R radtotd = 0, radclrd = 0, totradd = 0, clrradd = 0, rad = 0;
     for (int k = nlay; k >= 1; --k) {
+        if (MC) {
+            const bool cl = (s.mcw[g >> 5][k - 1] >> (g & 31)) & 1u;
+            const LwTerms<R> t = lw2_terms(s, lut, g, band, k, sdif, cl);
+            if (cl) {
+                const R efclrfr = (R)1 - ((R)1 - rexp(-(sdif * s.taucld[band][k - 1])));
+                radtotd = radtotd * t.trng * efclrfr + t.gassrcd + (t.totsrcd - t.gassrcd);
+            } else {
+                radtotd = radtotd * t.trng + t.gassrcd;
+            }
+            radclrd = radclrd * t.trng + t.gassrcd;
+            const double v = warp_sum(act ? (double)radtotd : 0.0);
+            if (lane == 0) s.fnet2[warp][k - 1] = v;
+            continue;
+        }
         const R clfr = s.cldfrc[k];
         const bool cl = clfr >= eps;
         const LwTerms<R> t = lw2_terms(s, lut, g, band, k, sdif, cl);
@@ -125,6 +145,20 @@ __global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(LwIn a, LwLut
     R totradu = 0, clrradu = 0;
     rad = 0;
     for (int k = 1; k <= nlay; ++k) {
+        if (MC) {
+            const bool cl = (s.mcw[g >> 5][k - 1] >> (g & 31)) & 1u;
+            const LwTerms<R> t = lw2_terms(s, lut, g, band, k, sdif, cl);
+            if (cl) {
+                const R efclrfr = (R)1 - ((R)1 - rexp(-(sdif * s.taucld[band][k - 1])));
+                radtotu = radtotu * t.trng * efclrfr + t.gassrcu + (t.totsrcu - t.gassrcu);
+            } else {
+                radtotu = radtotu * t.trng + t.gassrcu;
+            }
+            radclru = radclru * t.trng + t.gassrcu;
+            const double v = warp_sum(act ? (double)radtotu : 0.0);
+            if (lane == 0) s.fnet[warp][k] = v;
+            continue;
+        }
         const R clfr = s.cldfrc[k];
         const bool cl = clfr >= eps;
         const LwTerms<R> t = lw2_terms(s, lut, g, band, k, sdif, cl);

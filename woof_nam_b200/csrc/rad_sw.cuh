@@ -53,6 +53,7 @@ struct SwIn {
     int64_t ncol;
     int nlay, diagnostic, iswmode;
     float solcon;
+    const uint32_t* mask;     // McICA route: sub-column cloud words [4][nlay][ncol] (null: NAM route)
 };
 
 template <class R>

@@ -356,6 +356,7 @@ struct SwSh2 {
     float cosz, sntz, ssolar, albbm[2], albdf[2], zcf0, zcf1;
     int laytrop, kmin8, kminw;
     unsigned char low[NLAY_MAX];
+    uint32_t mcw[4][NLAY_MAX];                 // McICA route: the column's sub-column cloud words
     int nexact;                                // layer evaluations queued for the float64 recompute
     int qkey[SW2_QCAP];                        // thread | layer << 8 | cloud << 15
     float qval[SW2_QCAP][6];                   // their rb, rd, tb, td, e3, e4
@@ -465,12 +466,18 @@ __device__ __forceinline__ float sw2_taur(const SwSh2& s, int g, int k0)
 
 // R/T of layer k0 for g-point g in the clear pass (c) and, for a cloudy column, the cloudy pass (o) of
 // spcvrtc (spcvrtc.cu:330-460: the cloudy pass blends the clear and the cloud-mixture R/T by the layer's
-// cloud fraction).  The clear R/T is computed once and serves both passes.
+// cloud fraction).  The clear R/T is computed once and serves both passes.  McICA route (mc): the second
+// pass takes the cloud-mixture R/T unblended in the cloudy layers whose sub-column bit is set.
 struct SwLayerRT2 {
     SwLayerRT c, o;
 };
+__device__ __forceinline__ bool sw2_cloud_layer(const SwSh2& s, bool mc, int g, int k0)
+{
+    return s.cldfrc[k0] > 1.0e-12f && (!mc || ((s.mcw[g >> 5][k0] >> (g & 31)) & 1u));
+}
+
 __device__ __noinline__ SwLayerRT2 sw2_layer(const SwSh2& s, const SwAer* aer, const SwExactCtx& x, int k0, int g,
-                                             int ib, bool cloudy, float cz, float snt, const float* ex)
+                                             int ib, bool cloudy, bool mc, float cz, float snt, const float* ex)
 {
     SwLayerRT2 r;
     SwLayerRT& c = r.c;
@@ -486,13 +493,17 @@ __device__ __noinline__ SwLayerRT2 sw2_layer(const SwSh2& s, const SwAer* aer, c
     const float ct0 = fmaxf(1.0e-12f, tr + tg + ta), cs0 = tr + tasa, cy0 = tay, cab = tg + taab;
     sw2_rt_mixed(s, ct0, cab, cs0, cy0, cz, snt, ex, x, k0, g, ib, false, c.rb, c.rd, c.tb, c.td, c.e3, c.e4);
     o = c;
-    if (cloudy) {
-        const float zc1 = s.cldfrc[k0];
-        if (zc1 > 1.0e-12f) {
+    if (cloudy && sw2_cloud_layer(s, mc, g, k0)) {
+        {
+            const float zc1 = mc ? 1.0f : s.cldfrc[k0];
             const float ot0 = ct0 + s.taucw[ib][k0], os0 = cs0 + s.ssacw[ib][k0], oy0 = cy0 + s.asycw[ib][k0];
             const float oab = cab + s.tabsc[ib][k0];
             float rb2, rd2, tb2, td2, e32, e42;
             sw2_rt_mixed(s, ot0, oab, os0, oy0, cz, snt, ex, x, k0, g, ib, true, rb2, rd2, tb2, td2, e32, e42);
+            if (mc) {
+                o.rb = rb2; o.rd = rd2; o.tb = tb2; o.td = td2; o.e3 = e32; o.e4 = e42;
+                return r;
+            }
             const float zc0 = 1.0f - zc1;
             o.rb = zc0 * c.rb + zc1 * rb2;
             o.rd = zc0 * c.rd + zc1 * rd2;
@@ -618,6 +629,9 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
         s.kminw = a.kminw[d];
         s.nexact = 0;
     }
+    if (a.mask)
+        for (int i = tid; i < 4 * nlay; i += SW2_THREADS)
+            s.mcw[i / nlay][i % nlay] = __ldg(a.mask + ((size_t)(i / nlay) * nlay + (i % nlay)) * N + col);
     __syncthreads();
     // ---- phase A2: cloud optics per (band, layer); solar source per band
     for (int p = tid; p < 14 * nlay; p += SW2_THREADS) {
@@ -646,7 +660,8 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
     while (g >= c_sw_ns[ib0 + 1]) ++ib0;
     const int ibd = ib0 == 8 ? 0 : ((ib0 >= 9 && ib0 <= 12) ? 2 : 1);   // idxsfc
     const float cz = s.cosz, snt = s.sntz;
-    const bool cloudy = s.zcf1 > 1.0e-6f;
+    const bool mc = a.mask != nullptr;
+    const bool cloudy = mc ? s.zcf1 > 0.0f : s.zcf1 > 1.0e-6f;
     const float zsolar = act ? s.ssolar * s.sfluxzen[g] : 0.0f;
     const float ab = ibd ? s.albbm[ibd - 1] : 0.5f * (s.albbm[0] + s.albbm[1]);
     const float ad = ibd ? s.albdf[ibd - 1] : 0.5f * (s.albdf[0] + s.albdf[1]);
@@ -665,7 +680,7 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
                 const int i = atomicAdd(&s.nexact, 1);
                 if (i < SW2_QCAP) s.qkey[i] = sw2_qkey(tid, k0, false);
             }
-            if (cloudy && s.cldfrc[k0] > 1.0e-12f) {
+            if (cloudy && sw2_cloud_layer(s, mc, g, k0)) {
                 const float ot0 = ct0 + s.taucw[ib0][k0], os0 = cs0 + s.ssacw[ib0][k0], oy0 = cy0 + s.asycw[ib0][k0];
                 const float oab = cab + s.tabsc[ib0][k0];
                 if (fabsf(sw2_prologue<float>(ot0, oab, os0, oy0, x.mode, cz).zrpp) < SW2_RESONANCE) {
@@ -696,14 +711,14 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
     for (int sg = 0; sg < nseg; ++sg) {
         if (sg > 0) { CK(sg, 0) = ubc; CK(sg, 1) = udc; CK(sg, 2) = ubo; CK(sg, 3) = udo; }
         for (int j = 0; j < SW2_SEG; ++j) {
-            const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, cz, snt, ex);
+            const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, mc, cz, snt, ex);
             sw2_up(L.c, ubc, udc);
             if (cloudy) sw2_up(L.o, ubo, udo);
         }
     }
     // downward sweep, segment by segment from the top: recompute the segment's R/T and upward states into
     // registers from its checkpoint, then walk down through it
-    const double w0 = cloudy ? (double)s.zcf0 : 1.0, w1 = cloudy ? (double)s.zcf1 : 0.0;
+    const double w0 = cloudy ? (mc ? 0.0 : (double)s.zcf0) : 1.0, w1 = cloudy ? (mc ? 1.0 : (double)s.zcf1) : 0.0;
     float tdnc = 1, rdnc = 0, tdbc = 1, tdbc0 = 1, tdno = 1, rdno = 0, tdbo = 1, tdbo0 = 1;
     float toa_c = 0, toa_o = 0;
     for (int sg = nseg - 1; sg >= 0; --sg) {
@@ -716,7 +731,7 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
         float e4c = 1, e4o = 1;
 #pragma unroll
         for (int j = 0; j < SW2_SEG; ++j) {
-            const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, cz, snt, ex);
+            const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, mc, cz, snt, ex);
             Lc[j] = L.c;
             Lo[j] = L.o;
             zubc[j + 1] = zubc[j]; zudc[j + 1] = zudc[j];
@@ -790,8 +805,7 @@ sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
     }
     __syncthreads();
     // ---- column end (spcvrtc.cu:493-545) and swrad_post (swrad.cu:365-403), float64
-    const double c1d = (double)s.zcf1, c0d = (double)s.zcf0;
-    auto tot = [&](double clr, double cld) { return cloudy ? c1d * cld + c0d * clr : clr; };
+    auto tot = [&](double clr, double cld) { return cloudy ? w1 * cld + w0 * clr : clr; };
     for (int k = tid; k < nlay; k += SW2_THREADS) {
         double f0 = 0, f1 = 0;
         for (int w = 0; w < SW2_WARPS; ++w) { f0 += s.fn[w][k]; f1 += s.fn[w][k + 1]; }

@@ -34,11 +34,24 @@ class SolverConfig:
     window_cols: int = 0             # SW MINVAL(laytrop) window in columns (0 = whole request)
     sw_chunk: int = 32768
     cpathfac: float = 1.5
+    iovrlw: int = 1                  # McICA overlap: 0 random, 1 maximum-random, 2 maximum
+    iovrsw: int = 1
+    lw_seed0: int = 140              # McICA seed offsets (ipsdlw0, ipsdsw0)
+    sw_seed0: int = 1
 
 
-def output_shapes(nlay: int, ncol: int) -> dict:
-    return {"htlw": (nlay, ncol), "htsw": (nlay, ncol), "topflw": (2, ncol), "sfcflw": (4, ncol),
-            "topfsw": (3, ncol), "sfcfsw": (4, ncol), "fdncmp": (6, ncol)}
+def output_shapes(nlay: int, ncol: int, route: str = "nam") -> dict:
+    """Output arrays of a solve; the McICA route adds the sub-column cloud words (int32 storage of the
+    uint32 words, [word][layer][column], layers surface first, bit g & 31 of word g >> 5)."""
+    d = {"htlw": (nlay, ncol), "htsw": (nlay, ncol), "topflw": (2, ncol), "sfcflw": (4, ncol),
+         "topfsw": (3, ncol), "sfcfsw": (4, ncol), "fdncmp": (6, ncol)}
+    if route == "mcica":
+        d["lw_mask"] = (5, nlay, ncol)
+        d["sw_mask"] = (4, nlay, ncol)
+    return d
+
+
+MASK_KEYS = ("lw_mask", "sw_mask")
 
 
 class RadSolver:
@@ -56,6 +69,8 @@ class RadSolver:
         c.window_cols = self.cfg.window_cols
         c.sw_chunk = self.cfg.sw_chunk
         c.cpathfac = self.cfg.cpathfac
+        c.iovrlw, c.iovrsw = self.cfg.iovrlw, self.cfg.iovrsw
+        c.lw_seed0, c.sw_seed0 = self.cfg.lw_seed0, self.cfg.sw_seed0
         h = ctypes.c_void_p()
         _lib.check(self.lib, None, self.lib.rad_create(ctypes.byref(c), ctypes.byref(h)), "rad_create")
         self.handle = h
@@ -76,8 +91,8 @@ class RadSolver:
     # ---------------------------------------------------------------------------------------------
     def alloc_outputs(self, ncol: int, device=None) -> dict:
         torch = _torch()
-        return {k: torch.empty(s, dtype=torch.float32, device=device or "cuda")
-                for k, s in output_shapes(self.cfg.nlay, ncol).items()}
+        return {k: torch.empty(s, dtype=torch.int32 if k in MASK_KEYS else torch.float32, device=device or "cuda")
+                for k, s in output_shapes(self.cfg.nlay, ncol, self.cfg.route).items()}
 
     def _abi_args(self, cols: dict, solcon: float, out: dict | None):
         torch = _torch()
@@ -97,10 +112,14 @@ class RadSolver:
             setattr(ci, k, cols[k].data_ptr())
         for k in OPTIONAL_INPUTS:
             t = cols.get(k)
+            if t is not None:
+                want = torch.int32 if k == "icseed" else torch.float32
+                if not (t.is_cuda and t.dtype == want and t.is_contiguous()):
+                    raise TypeError(f"input {k!r} must be a contiguous {want} CUDA tensor")
             setattr(ci, k, t.data_ptr() if t is not None else None)
         ci.solcon = float(solcon)
         co = _lib.RadOutputs()
-        for k in output_shapes(1, 1):
+        for k in output_shapes(1, 1, "mcica"):
             t = out.get(k)
             setattr(co, k, t.data_ptr() if t is not None else None)
         return ci, co, ncol, out
@@ -129,8 +148,9 @@ class RadSolver:
         _lib.check(self.lib, self.handle, rc, "rad_solve_batch")
         return [a[3] for a in args]
 
-    def to_device(self, columns, device="cuda", pinned: bool = False) -> dict:
-        """Copy a woof_nam_b200.columns.Columns request to the device (optionally through pinned memory)."""
+    def to_device(self, columns, device="cuda", pinned: bool = False, icseed=None) -> dict:
+        """Copy a woof_nam_b200.columns.Columns request to the device (optionally through pinned memory).
+        icseed: optional McICA seeds, int32 [2][ncol] (LW row, SW row)."""
         torch = _torch()
         d = {}
         for k in INPUT_FIELDS:
@@ -138,15 +158,21 @@ class RadSolver:
             if pinned:
                 a = a.pin_memory()
             d[k] = a.to(device, non_blocking=pinned)
+        if icseed is not None:
+            d["icseed"] = torch.from_numpy(np.ascontiguousarray(icseed, dtype=np.int32)).to(device)
         return d
 
-    def solve_host(self, columns) -> dict:
+    def solve_host(self, columns, icseed=None) -> dict:
         """Host arrays in, host arrays out (copies both ways)."""
         torch = _torch()
-        d = self.to_device(columns)
+        d = self.to_device(columns, icseed=icseed)
         out = self.solve(d, columns.solcon)
         torch.cuda.synchronize()
-        return {k: v.cpu().numpy() for k, v in out.items()}
+        r = {k: v.cpu().numpy() for k, v in out.items()}
+        for k in MASK_KEYS:
+            if k in r:
+                r[k] = r[k].view(np.uint32)
+        return r
 
     def profile(self, on: bool = True) -> None:
         """Start (or stop) device-time accounting of the library's kernels on this handle."""
