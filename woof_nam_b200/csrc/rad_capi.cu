@@ -90,10 +90,25 @@ int fail(RadHandle* h, int code, const std::string& msg)
     } while (0)
 
 // ---------------------------------------------------------------------------------- device helpers
-__global__ void k_dayflags(const float* coszen, int64_t n, int* flag)
+// The SW day list of a launch's requests (their columns concatenated; phys_rrtm_grrad_sw.cu:69,80 per
+// request) and, per day column, laytrop and the MINVAL(laytrop) minima of its 8-column group and of its
+// chunk (sw_seam.py:23-37, rrtm_sw_kmin_windows.cu).  Windows and chunks restart with every request.
+struct DayReq {
+    const float* coszen;
+    const float* plyr;
+    int64_t ncol;
+    int wc, maxc;          // window columns, chunks per window
+    int64_t cmin_off;      // first chunk-minimum slot of the request
+};
+using DayBatch = ReqBatch<DayReq>;
+
+__global__ void k_dayflags(const __grid_constant__ DayBatch b, int64_t n, int* flag)
 {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < n) flag[c] = coszen[c] >= 1.0e-4f ? 1 : 0;
+    if (c < n) {
+        const int r = b.find(c);
+        flag[c] = b.req[r].coszen[c - b.off[r]] >= 1.0e-4f ? 1 : 0;
+    }
     if (c == n) flag[c] = 0;
 }
 __global__ void k_scatter(const int* flag, const int* pos, int64_t n, int* daycol, int* nday)
@@ -104,32 +119,37 @@ __global__ void k_scatter(const int* flag, const int* pos, int64_t n, int* dayco
 }
 // SW setcoef laytrop of each day column (setcoef.cu:28-73): the last layer (surface first) with
 // ln(p) > 4.56, nlay when there is none.
-__global__ void k_laytrop(const float* plyr, int64_t n, int nlay, const int* daycol, const int* nday, int* lt,
-                          int* cmin, int64_t ncmin, int wc, int chunk, int maxc, const int* pos)
+__global__ void k_laytrop(const __grid_constant__ DayBatch b, int nlay, const int* daycol, const int* nday, int* lt,
+                          int* cmin, int chunk, const int* pos)
 {
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= *nday) return;
-    const int64_t c = daycol[d];
+    const int64_t g = daycol[d];
+    const int r = b.find(g);
+    const DayReq& q = b.req[r];
+    const int64_t c = g - b.off[r];
     int l = nlay;
     for (int k0 = 0; k0 < nlay; ++k0)
-        if (log((double)plyr[(size_t)(nlay - 1 - k0) * n + c]) > (double)4.56f) l = k0 + 1;
+        if (log((double)q.plyr[(size_t)(nlay - 1 - k0) * q.ncol + c]) > (double)4.56f) l = k0 + 1;
     lt[d] = l;
-    const int w = (int)(c / wc);
-    const int dw0 = pos[(int64_t)w * wc];
+    const int w = (int)(c / q.wc);
+    const int dw0 = pos[b.off[r] + (int64_t)w * q.wc];
     const int ci = (d - dw0) / chunk;
-    const int64_t key = (int64_t)w * maxc + ci;
-    if (key < ncmin) atomicMin(cmin + key, l);
+    atomicMin(cmin + q.cmin_off + (int64_t)w * q.maxc + ci, l);
 }
-__global__ void k_groups(int64_t n, const int* daycol, const int* nday, const int* lt, const int* cmin,
-                         int64_t ncmin, int wc, int chunk, int maxc, const int* pos, int* k8, int* kw)
+__global__ void k_groups(const __grid_constant__ DayBatch b, const int* daycol, const int* nday, const int* lt,
+                         const int* cmin, int chunk, const int* pos, int* k8, int* kw)
 {
     const int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= *nday) return;
-    const int64_t c = daycol[d];
-    const int w = (int)(c / wc);
-    const int dw0 = pos[(int64_t)w * wc];
-    const int64_t wend = ((int64_t)w + 1) * wc < n ? ((int64_t)w + 1) * wc : n;
-    const int dw1 = pos[wend];
+    const int64_t g = daycol[d];
+    const int r = b.find(g);
+    const DayReq& q = b.req[r];
+    const int64_t c = g - b.off[r];
+    const int w = (int)(c / q.wc);
+    const int dw0 = pos[b.off[r] + (int64_t)w * q.wc];
+    const int64_t wend = ((int64_t)w + 1) * q.wc < q.ncol ? ((int64_t)w + 1) * q.wc : q.ncol;
+    const int dw1 = pos[b.off[r] + wend];
     const int ci = (d - dw0) / chunk;
     const int dc0 = dw0 + ci * chunk;
     const int dc1 = dc0 + chunk < dw1 ? dc0 + chunk : dw1;
@@ -138,8 +158,7 @@ __global__ void k_groups(int64_t n, const int* daycol, const int* nday, const in
     int m = lt[d];
     for (int i = g0; i < g1; ++i) m = min(m, lt[i]);
     k8[d] = m;
-    const int64_t key = (int64_t)w * maxc + ci;
-    kw[d] = key < ncmin ? cmin[key] : lt[d];
+    kw[d] = cmin[q.cmin_off + (int64_t)w * q.maxc + ci];
 }
 __global__ void k_fill_int(int* p, int64_t n, int v)
 {
@@ -216,28 +235,19 @@ int ensure_scratch(RadHandle* h, int64_t n)
     return RAD_OK;
 }
 
-// McICA: LW and SW sub-column words of every column, into the caller's mask outputs when given, else into
-// the handle's scratch.  Seeds: icseed [2][ncol] (LW row, SW row) or seed0 + column + 1.
-int mcica_masks(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t n, cudaStream_t st,
-                const uint32_t** lwm, const uint32_t** swm)
+// McICA: LW and SW sub-column words of every column of request r, into the caller's mask outputs when
+// given, else into the handle's scratch at the request's column offset (scratch holds the launch's columns).
+// Seeds: icseed [2][ncol] (LW row, SW row) or seed0 + column + 1.
+int mcica_masks(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t n, int64_t scratch_off,
+                cudaStream_t st, const uint32_t** lwm, const uint32_t** swm)
 {
     const RadConfig& cfg = h->cfg;
     const int nlay = cfg.nlay;
     uint32_t* lw = out->lw_mask;
     uint32_t* sw = out->sw_mask;
-    if (!lw || !sw) {
-        if (n * nlay > h->mask_cap) {
-            if (h->d_lwm) cudaFree(h->d_lwm);
-            if (h->d_swm) cudaFree(h->d_swm);
-            h->d_lwm = h->d_swm = nullptr;
-            h->mask_cap = 0;
-            RAD_CUDA(h, cudaMalloc((void**)&h->d_lwm, (size_t)5 * nlay * n * sizeof(uint32_t)));
-            RAD_CUDA(h, cudaMalloc((void**)&h->d_swm, (size_t)4 * nlay * n * sizeof(uint32_t)));
-            h->mask_cap = n * nlay;
-        }
-        if (!lw) lw = h->d_lwm;
-        if (!sw) sw = h->d_swm;
-    }
+    // scratch layout per request: [5][nlay][n] LW words then [4][nlay][n] SW words, at 9 nlay offset
+    if (!lw) lw = h->d_lwm + (size_t)9 * nlay * scratch_off;
+    if (!sw) sw = (out->lw_mask ? h->d_lwm + (size_t)9 * nlay * scratch_off : lw + (size_t)5 * nlay * n);
     const unsigned grid = (unsigned)((n + MC_WARPS - 1) / MC_WARPS);
     k_mcica<140><<<grid, MC_WARPS * 32, 0, st>>>(in->clouds, n, nlay, in->icseed, 0, cfg.lw_seed0, cfg.iovrlw, 1, lw);
     k_mcica<112><<<grid, MC_WARPS * 32, 0, st>>>(in->clouds, n, nlay, in->icseed, 1, cfg.sw_seed0, cfg.iovrsw, 0, sw);
@@ -256,11 +266,62 @@ int mark(RadHandle* h, cudaStream_t st, size_t base, int i)
     return RAD_OK;
 }
 
+// Scratch for a launch of ntot columns: day list arrays, CUB temp, chunk minima, McICA words.
+int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
+{
+    int rc = ensure_scratch(h, ntot);
+    if (rc) return rc;
+    if (ncmin > h->cmin_cap) {
+        if (h->d_cmin) cudaFree(h->d_cmin);
+        h->d_cmin = nullptr;
+        h->cmin_cap = 0;
+        RAD_CUDA(h, cudaMalloc((void**)&h->d_cmin, (size_t)ncmin * sizeof(int)));
+        h->cmin_cap = ncmin;
+    }
+    if (h->cfg.route == RAD_ROUTE_MCICA && ntot * h->cfg.nlay > h->mask_cap) {
+        if (h->d_lwm) cudaFree(h->d_lwm);
+        h->d_lwm = nullptr;
+        h->mask_cap = 0;
+        RAD_CUDA(h, cudaMalloc((void**)&h->d_lwm, (size_t)9 * h->cfg.nlay * ntot * sizeof(uint32_t)));
+        h->mask_cap = ntot * h->cfg.nlay;
+    }
+    return RAD_OK;
+}
+
+// One launch set for up to RAD_MAXREQ requests: the McICA generators (McICA route), one LW launch over all
+// the requests' columns, the day list and group minima of all of them, one SW launch over all their sunlit
+// columns.  No host synchronisation.
 template <class R>
-int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t n, cudaStream_t st)
+int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs* outs, const int64_t* ncols,
+                 cudaStream_t st)
 {
     const RadConfig& cfg = h->cfg;
     const int nlay = cfg.nlay;
+    const int chunk = cfg.sw_chunk > 0 ? cfg.sw_chunk : 32768;
+    int64_t ntot = 0, ncmin = 0;
+    bool any_aer = false;
+    DayBatch db{};
+    db.nreq = nreq;
+    for (int r = 0; r < nreq; ++r) {
+        const int64_t n = ncols[r];
+        DayReq& q = db.req[r];
+        q.coszen = ins[r].coszen;
+        q.plyr = ins[r].plyr;
+        q.ncol = n;
+        q.wc = cfg.window_cols > 0 ? (int)std::min<int64_t>(cfg.window_cols, std::max<int64_t>(n, 1)) : (int)std::max<int64_t>(n, 1);
+        q.maxc = (q.wc + chunk - 1) / chunk;
+        q.cmin_off = ncmin;
+        ncmin += ((n + q.wc - 1) / q.wc) * q.maxc;
+        db.off[r] = ntot;
+        ntot += n;
+        any_aer = any_aer || ins[r].faersw != nullptr;
+    }
+    db.off[nreq] = ntot;
+    if (ntot == 0) return RAD_OK;
+    if (ntot > (int64_t)std::numeric_limits<int>::max() - 1)
+        return fail(h, RAD_E_INVALID, "rad_solve: more than 2^31 - 2 columns in one launch");
+    int rc = ensure_launch_scratch(h, ntot, std::max<int64_t>(ncmin, 1));
+    if (rc) return rc;
     size_t eb = 0;
     if (h->profiling) {
         eb = h->ev_used;
@@ -271,87 +332,89 @@ int launch_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int6
         }
         h->ev_used += 4;
         h->prof_solves += 1;
-        h->prof_columns += n;
+        h->prof_columns += ntot;
     }
     int mrc = mark(h, st, eb, 0);
     if (mrc) return mrc;
     // ---- McICA route: sub-column cloud words of every column (LW and SW generators)
-    const uint32_t *lwm = nullptr, *swm = nullptr;
-    if (cfg.route == RAD_ROUTE_MCICA) {
-        const int mrc2 = mcica_masks(h, in, out, n, st, &lwm, &swm);
-        if (mrc2) return mrc2;
-    }
+    const uint32_t* lwm[RAD_MAXREQ] = {};
+    const uint32_t* swm[RAD_MAXREQ] = {};
+    if (cfg.route == RAD_ROUTE_MCICA)
+        for (int r = 0; r < nreq; ++r)
+            if (ncols[r] > 0 && (rc = mcica_masks(h, ins + r, outs + r, ncols[r], db.off[r], st, &lwm[r], &swm[r])))
+                return rc;
     // ---- LW over every column
     {
-        LwIn a{in->plyr, in->plvl, in->tlyr, in->tlvl, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faerlw,
-               in->sfcemis, in->tsfg, out->htlw, out->topflw, out->sfcflw, n, 0, nlay, cfg.diagnostic, cfg.cpathfac,
-               lwm};
+        LwBatch bt{};
+        bt.nreq = nreq;
+        for (int r = 0; r <= nreq; ++r) bt.off[r] = db.off[r];
+        for (int r = 0; r < nreq; ++r) {
+            const RadColumns* in = ins + r;
+            const RadOutputs* out = outs + r;
+            bt.req[r] = LwIn{in->plyr, in->plvl, in->tlyr, in->tlvl, in->qlyr, in->olyr, in->gasvmr, in->clouds,
+                             in->faerlw, in->sfcemis, in->tsfg, out->htlw, out->topflw, out->sfcflw, ncols[r], nlay,
+                             cfg.diagnostic, cfg.cpathfac, lwm[r]};
+        }
         LwLut<R> lut;
         const R* base = sizeof(R) == 4 ? (const R*)h->d_lwf : (const R*)h->d_lwd;
         lut.ex = base; lut.tfn = base + 10001; lut.tau = base + 2 * 10001;
+        const bool mc = cfg.route == RAD_ROUTE_MCICA;
         const size_t smem = sizeof(LwShared<R>);
-        RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_lw<R>(lwm != nullptr), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        const int64_t maxg = 1 << 30;
-        for (int64_t c0 = 0; c0 < n; c0 += maxg) {
-            a.col0 = c0;
-            const int64_t nb = std::min<int64_t>(maxg, n - c0);
-            if (sizeof(R) == 4 && lwm)
-                lw2_column_kernel<R, true><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
-            else if (sizeof(R) == 4)
-                lw2_column_kernel<R, false><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
-            else
-                lw_column_kernel<R><<<(unsigned)nb, LW_THREADS, smem, st>>>(a, lut, h->d_err);
-            h->launches += 1;
-        }
+        RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_lw<R>(mc), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (sizeof(R) == 4 && mc)
+            lw2_column_kernel<R, true><<<(unsigned)ntot, LW_THREADS, smem, st>>>(bt, lut, h->d_err);
+        else if (sizeof(R) == 4)
+            lw2_column_kernel<R, false><<<(unsigned)ntot, LW_THREADS, smem, st>>>(bt, lut, h->d_err);
+        else
+            lw_column_kernel<R><<<(unsigned)ntot, LW_THREADS, smem, st>>>(bt, lut, h->d_err);
+        h->launches += 1;
         RAD_CUDA(h, cudaGetLastError());
     }
     if ((mrc = mark(h, st, eb, 1))) return mrc;
     // ---- SW day list, laytrop, groups
-    int rc = ensure_scratch(h, n);
-    if (rc) return rc;
-    const int wc = cfg.window_cols > 0 ? (int)std::min<int64_t>(cfg.window_cols, n) : (int)n;
-    const int chunk = cfg.sw_chunk > 0 ? cfg.sw_chunk : 32768;
-    const int64_t nwin = (n + wc - 1) / wc;
-    const int maxc = (wc + chunk - 1) / chunk;
-    const int64_t ncmin = nwin * maxc;
-    if (ncmin > h->cmin_cap) {
-        if (h->d_cmin) cudaFree(h->d_cmin);
-        RAD_CUDA(h, cudaMalloc((void**)&h->d_cmin, (size_t)ncmin * sizeof(int)));
-        h->cmin_cap = ncmin;
-    }
     const int T = 256;
-    const unsigned gb = (unsigned)((n + 1 + T - 1) / T);
-    k_dayflags<<<gb, T, 0, st>>>(in->coszen, n, h->d_flag);
+    const unsigned gb = (unsigned)((ntot + 1 + T - 1) / T);
+    k_dayflags<<<gb, T, 0, st>>>(db, ntot, h->d_flag);
     size_t tb = h->cub_bytes;
-    RAD_CUDA(h, cub::DeviceScan::ExclusiveSum(h->d_cub, tb, h->d_flag, h->d_pos, (int)(n + 1), st));
-    k_scatter<<<gb, T, 0, st>>>(h->d_flag, h->d_pos, n, h->d_daycol, h->d_nday);
+    RAD_CUDA(h, cub::DeviceScan::ExclusiveSum(h->d_cub, tb, h->d_flag, h->d_pos, (int)(ntot + 1), st));
+    k_scatter<<<gb, T, 0, st>>>(h->d_flag, h->d_pos, ntot, h->d_daycol, h->d_nday);
     k_fill_int<<<(unsigned)((ncmin + T - 1) / T), T, 0, st>>>(h->d_cmin, ncmin, std::numeric_limits<int>::max());
-    k_laytrop<<<gb, T, 0, st>>>(in->plyr, n, nlay, h->d_daycol, h->d_nday, h->d_lt, h->d_cmin, ncmin, wc, chunk,
-                                maxc, h->d_pos);
-    k_groups<<<gb, T, 0, st>>>(n, h->d_daycol, h->d_nday, h->d_lt, h->d_cmin, ncmin, wc, chunk, maxc, h->d_pos,
-                               h->d_k8, h->d_kw);
+    k_laytrop<<<gb, T, 0, st>>>(db, nlay, h->d_daycol, h->d_nday, h->d_lt, h->d_cmin, chunk, h->d_pos);
+    k_groups<<<gb, T, 0, st>>>(db, h->d_daycol, h->d_nday, h->d_lt, h->d_cmin, chunk, h->d_pos, h->d_k8, h->d_kw);
     h->launches += 7;   // day flags, scan (2 kernels), scatter, fill, laytrop, groups
     RAD_CUDA(h, cudaGetLastError());
-    // ---- SW over the day columns; write zeros first (night columns keep them, as swrad does)
-    RAD_CUDA(h, cudaMemsetAsync(out->htsw, 0, (size_t)nlay * n * sizeof(float), st));
-    RAD_CUDA(h, cudaMemsetAsync(out->topfsw, 0, (size_t)3 * n * sizeof(float), st));
-    RAD_CUDA(h, cudaMemsetAsync(out->sfcfsw, 0, (size_t)4 * n * sizeof(float), st));
-    if (out->fdncmp) RAD_CUDA(h, cudaMemsetAsync(out->fdncmp, 0, (size_t)6 * n * sizeof(float), st));
+    // ---- SW over the day columns; zeros first (night columns keep them, as swrad does)
+    for (int r = 0; r < nreq; ++r) {
+        const int64_t n = ncols[r];
+        if (!n) continue;
+        const RadOutputs* out = outs + r;
+        RAD_CUDA(h, cudaMemsetAsync(out->htsw, 0, (size_t)nlay * n * sizeof(float), st));
+        RAD_CUDA(h, cudaMemsetAsync(out->topfsw, 0, (size_t)3 * n * sizeof(float), st));
+        RAD_CUDA(h, cudaMemsetAsync(out->sfcfsw, 0, (size_t)4 * n * sizeof(float), st));
+        if (out->fdncmp) RAD_CUDA(h, cudaMemsetAsync(out->fdncmp, 0, (size_t)6 * n * sizeof(float), st));
+    }
     {
-        SwIn a{in->plyr, in->plvl, in->tlyr, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faersw, in->sfcalb,
-               in->coszen, h->d_daycol, h->d_nday, h->d_k8, h->d_kw, out->htsw, out->topfsw, out->sfcfsw,
-               out->fdncmp, n, nlay, cfg.diagnostic, cfg.iswmode, in->solcon, swm};
+        SwBatch bt{};
+        bt.nreq = nreq;
+        for (int r = 0; r <= nreq; ++r) bt.off[r] = db.off[r];
+        for (int r = 0; r < nreq; ++r) {
+            const RadColumns* in = ins + r;
+            const RadOutputs* out = outs + r;
+            bt.req[r] = SwIn{in->plyr, in->plvl, in->tlyr, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faersw,
+                             in->sfcalb, in->coszen, h->d_daycol, h->d_nday, h->d_k8, h->d_kw, out->htsw, out->topfsw,
+                             out->sfcfsw, out->fdncmp, ncols[r], nlay, cfg.diagnostic, cfg.iswmode, in->solcon, swm[r]};
+        }
         if ((mrc = mark(h, st, eb, 2))) return mrc;
         if (sizeof(R) == 4) {
-            const size_t smem = sw2_smem_bytes(in->faersw != nullptr);
+            const size_t smem = sw2_smem_bytes(any_aer);
             RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sw2_column_kernel<<<(unsigned)n, SW2_THREADS, smem, st>>>(a, h->d_swf, h->d_swd, h->d_err);
+            sw2_column_kernel<<<(unsigned)ntot, SW2_THREADS, smem, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, h->d_err);
         } else {
             SwLut<R> lut;
             lut.ex = (const R*)h->d_swd;
             const size_t smem = sizeof(SwShared<R>);
             RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_sw<R>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sw_column_kernel<R><<<(unsigned)n, SW_THREADS, smem, st>>>(a, lut, h->d_swd, h->d_err);
+            sw_column_kernel<R><<<(unsigned)ntot, SW_THREADS, smem, st>>>(bt, lut, h->d_swd, h->d_err);
         }
         h->launches += 1;
         RAD_CUDA(h, cudaGetLastError());
@@ -519,35 +582,55 @@ int64_t rad_workspace_bytes(const RadHandle* h, int64_t ncol)
     return (ncol + 1) * 6 * (int64_t)sizeof(int) + (1 << 20);
 }
 
-int rad_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream)
+// Argument checks of one request.
+static int check_request(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, const char* what)
 {
-    if (!h || !in || !out) return fail(h, RAD_E_INVALID, "rad_solve: null argument");
-    if (!h->tables_ok) return fail(h, RAD_E_TABLES, "rad_solve: tables not loaded (rad_load_tables)");
+    if (!in || !out) return fail(h, RAD_E_INVALID, std::string(what) + ": null argument");
     if (ncol < 0 || ncol > (int64_t)std::numeric_limits<int>::max() - 1)
-        return fail(h, RAD_E_INVALID, "rad_solve: ncol out of range");
+        return fail(h, RAD_E_INVALID, std::string(what) + ": ncol out of range");
     if (ncol == 0) return RAD_OK;
     if (!in->plyr || !in->plvl || !in->tlyr || !in->tlvl || !in->qlyr || !in->olyr || !in->gasvmr || !in->clouds ||
         !in->sfcemis || !in->tsfg || !in->sfcalb || !in->coszen)
-        return fail(h, RAD_E_INVALID, "rad_solve: a required input pointer is null");
+        return fail(h, RAD_E_INVALID, std::string(what) + ": a required input pointer is null");
     if (!out->htlw || !out->htsw || !out->topflw || !out->sfcflw || !out->topfsw || !out->sfcfsw)
-        return fail(h, RAD_E_INVALID, "rad_solve: a required output pointer is null");
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev != h->device) return fail(h, RAD_E_INVALID, "rad_solve: handle belongs to another device");
-    cudaStream_t st = (cudaStream_t)stream;
-    return h->cfg.precision == RAD_PREC_FP64 ? launch_solve<double>(h, in, out, ncol, st)
-                                             : launch_solve<float>(h, in, out, ncol, st);
+        return fail(h, RAD_E_INVALID, std::string(what) + ": a required output pointer is null");
+    return RAD_OK;
 }
 
 int rad_solve_batch(RadHandle* h, int32_t nreq, const RadColumns* ins, const RadOutputs* outs, const int64_t* ncols,
                     void* stream)
 {
-    if (!h || nreq < 0 || (nreq > 0 && (!ins || !outs || !ncols))) return fail(h, RAD_E_INVALID, "rad_solve_batch: bad arguments");
+    if (!h) return fail(h, RAD_E_INVALID, "rad_solve_batch: null handle");
+    if (nreq < 0 || (nreq > 0 && (!ins || !outs || !ncols))) return fail(h, RAD_E_INVALID, "rad_solve_batch: bad arguments");
+    if (!h->tables_ok) return fail(h, RAD_E_TABLES, "rad_solve: tables not loaded (rad_load_tables)");
     for (int32_t r = 0; r < nreq; ++r) {
-        const int rc = rad_solve(h, ins + r, outs + r, ncols[r], stream);
+        const int rc = check_request(h, ins + r, outs + r, ncols[r], "rad_solve");
         if (rc) return rc;
     }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != h->device) return fail(h, RAD_E_INVALID, "rad_solve: handle belongs to another device");
+    cudaStream_t st = (cudaStream_t)stream;
+    int32_t r0 = 0;
+    while (r0 < nreq) {
+        // one launch set per group of at most RAD_MAXREQ requests and 2^31 - 2 columns
+        int32_t r1 = r0;
+        int64_t cols = 0;
+        while (r1 < nreq && r1 - r0 < RAD_MAXREQ && (r1 == r0 || cols + ncols[r1] <= (int64_t)std::numeric_limits<int>::max() - 1))
+            cols += ncols[r1++];
+        const int rc = h->cfg.precision == RAD_PREC_FP64
+                           ? launch_batch<double>(h, r1 - r0, ins + r0, outs + r0, ncols + r0, st)
+                           : launch_batch<float>(h, r1 - r0, ins + r0, outs + r0, ncols + r0, st);
+        if (rc) return rc;
+        r0 = r1;
+    }
     return RAD_OK;
+}
+
+int rad_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream)
+{
+    if (!h || !in || !out) return fail(h, RAD_E_INVALID, "rad_solve: null argument");
+    return rad_solve_batch(h, 1, in, out, &ncol, stream);
 }
 
 int rad_profile_enable(RadHandle* h, int on)

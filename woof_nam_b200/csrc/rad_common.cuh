@@ -84,6 +84,26 @@ __device__ __forceinline__ void for_each_band_pair(const int* ns, int nbands, in
     }
 }
 
+// The requests of one launch (passed by value as a kernel parameter): request r covers columns
+// [off[r], off[r+1]) of the launch's concatenated column space.  A CTA finds its request by bisection.
+constexpr int RAD_MAXREQ = 32;
+template <class In>
+struct ReqBatch {
+    int nreq;
+    int64_t off[RAD_MAXREQ + 1];
+    In req[RAD_MAXREQ];
+    __device__ __forceinline__ int find(int64_t g) const
+    {
+        int lo = 0, hi = nreq - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (off[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        return lo;
+    }
+};
+
 // Error word written by kernels on bad input (host reads it after a synchronising call).
 enum : int { RAD_DEV_OK = 0, RAD_DEV_NLAY = 1, RAD_DEV_INDEX = 2 };
 

@@ -510,7 +510,7 @@ struct LwLut {
 struct LwIn {
     const float *plyr, *plvl, *tlyr, *tlvl, *qlyr, *olyr, *gasvmr, *clouds, *faerlw, *sfcemis, *tsfg;
     float *htlw, *topflw, *sfcflw;
-    int64_t ncol, col0;       // this launch covers columns [col0, col0 + gridDim.x) of an ncol request
+    int64_t ncol;             // columns of the request
     int nlay, diagnostic;
     float cpathfac;
     const uint32_t* mask;     // McICA route: sub-column cloud words [5][nlay][ncol] (null: NAM route)
@@ -815,13 +815,17 @@ __device__ void lw_setup(LwShared<R>& s, const LwIn& a, int64_t col, int tid)
     __syncthreads();
 }
 
+using LwBatch = ReqBatch<LwIn>;
+
 template <class R>
-__global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(LwIn a, LwLut<R> lut, int* err)
+__global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(const __grid_constant__ LwBatch bt, LwLut<R> lut, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LwShared<R>& s = *reinterpret_cast<LwShared<R>*>(smem_raw);
+    const int rq = bt.find((int64_t)blockIdx.x);
+    const LwIn& a = bt.req[rq];
     const int nlay = a.nlay;
-    const int64_t col = a.col0 + blockIdx.x;
+    const int64_t col = (int64_t)blockIdx.x - bt.off[rq];
     const int64_t N = a.ncol;
     const int tid = threadIdx.x;
     if (nlay > NLAY_MAX || col >= N) {

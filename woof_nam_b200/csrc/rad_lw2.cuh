@@ -66,12 +66,14 @@ __device__ __forceinline__ LwTerms<R> lw2_terms(const LwShared<R>& s, const LwLu
 // MC = true: the McICA route (rtrnmc, phys_rrtm_lw_rtrnmc.cu:85-310): a layer is cloudy for g-point g
 // when its sub-column bit is set, with effective clear fraction 1 - (1 - exp(-odcld)).
 template <class R, bool MC>
-__global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(LwIn a, LwLut<R> lut, int* err)
+__global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(const __grid_constant__ LwBatch bt, LwLut<R> lut, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LwShared<R>& s = *reinterpret_cast<LwShared<R>*>(smem_raw);
+    const int rq = bt.find((int64_t)blockIdx.x);
+    const LwIn& a = bt.req[rq];
     const int nlay = a.nlay;
-    const int64_t col = a.col0 + blockIdx.x;
+    const int64_t col = (int64_t)blockIdx.x - bt.off[rq];
     const int64_t N = a.ncol;
     const int tid = threadIdx.x;
     if (nlay > NLAY_MAX || col >= N) {

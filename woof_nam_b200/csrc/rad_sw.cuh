@@ -45,7 +45,7 @@ struct SwShared {
 
 struct SwIn {
     const float *plyr, *plvl, *tlyr, *qlyr, *olyr, *gasvmr, *clouds, *faersw, *sfcalb, *coszen;
-    const int* daycol;        // [nday] request-local column of each day index
+    const int* daycol;        // [nday] column of each day index in the launch's concatenated column space
     const int* nday;          // device count of day columns
     const int* kmin8;         // [nday] MINVAL(laytrop) of the column's 8-day-column group
     const int* kminw;         // [nday] MINVAL(laytrop) of the column's chunk
@@ -525,20 +525,26 @@ __device__ __forceinline__ void sw_swflux(const R* zrefb, const R* zrefd, const 
 }
 
 // ------------------------------------------------------------------------------------------------------
+using SwBatch = ReqBatch<SwIn>;
+
 template <class R>
-__global__ void __launch_bounds__(SW_THREADS) sw_column_kernel(SwIn a, SwLut<R> lut, const double* exd, int* err)
+__global__ void __launch_bounds__(SW_THREADS) sw_column_kernel(const __grid_constant__ SwBatch bt, SwLut<R> lut,
+                                                               const double* exd, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SwShared<R>& s = *reinterpret_cast<SwShared<R>*>(smem_raw);
-    const int nlay = a.nlay, nlp1 = nlay + 1;
     const int d = blockIdx.x;
-    if (d >= *a.nday) return;
+    if (d >= *bt.req[0].nday) return;
+    const int64_t gcol = bt.req[0].daycol[d];
+    const int rq = bt.find(gcol);
+    const SwIn& a = bt.req[rq];
+    const int nlay = a.nlay, nlp1 = nlay + 1;
     if (nlay > NLAY_MAX) {
         if (threadIdx.x == 0) atomicExch(err, RAD_DEV_NLAY);
         return;
     }
     const int64_t N = a.ncol;
-    const int64_t col = a.daycol[d];
+    const int64_t col = gcol - bt.off[rq];
     const int tid = threadIdx.x;
     const int iswcliq = a.diagnostic ? 0 : 1;
     auto IN = [&](const float* p, int lev) { return (R)__ldg(p + (size_t)lev * N + col); };

@@ -555,21 +555,25 @@ __device__ __forceinline__ int sw2_lane_g(int t, bool& act)
 
 // ------------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(SW2_THREADS, 2)
-sw2_column_kernel(SwIn a, const float* ex, const double* exd, int* err)
+sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, const double* exd, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SwSh2& s = *reinterpret_cast<SwSh2*>(smem_raw);
-    SwAer* aer = a.faersw ? reinterpret_cast<SwAer*>(smem_raw + sizeof(SwSh2)) : nullptr;
-    float* ckpt = reinterpret_cast<float*>(smem_raw + sizeof(SwSh2) + (a.faersw ? sizeof(SwAer) : 0));
-    const int nlay = a.nlay, nlp1 = nlay + 1;
     const int d = blockIdx.x;
-    if (d >= *a.nday) return;
+    if (d >= *bt.req[0].nday) return;
+    const int64_t gcol = bt.req[0].daycol[d];
+    const int rq = bt.find(gcol);
+    const SwIn& a = bt.req[rq];
+    // the aerosol block is reserved when any request of the launch has aerosol; used when this one does
+    SwAer* aer = a.faersw ? reinterpret_cast<SwAer*>(smem_raw + sizeof(SwSh2)) : nullptr;
+    float* ckpt = reinterpret_cast<float*>(smem_raw + sizeof(SwSh2) + (any_aer ? sizeof(SwAer) : 0));
+    const int nlay = a.nlay, nlp1 = nlay + 1;
     if (nlay > NLAY_MAX) {
         if (threadIdx.x == 0) atomicExch(err, RAD_DEV_NLAY);
         return;
     }
     const int64_t N = a.ncol;
-    const int64_t col = a.daycol[d];
+    const int64_t col = gcol - bt.off[rq];
     const int tid = threadIdx.x;
     const double heatfac = 9.80665 * 1.0e-2 / 1.0046e3;
     // ---- phase A1: layer coefficients (threads = layers), aerosol, heating factors
