@@ -121,6 +121,17 @@ int64_t rad_workspace_bytes(const RadHandle* h, int64_t ncol);
 int rad_solve_batch(RadHandle* h, int32_t nreq, const RadColumns* ins, const RadOutputs* outs,
                     const int64_t* ncols, void* stream);
 
+/* A batched solve captured once into a CUDA graph and replayed (no counterpart in the reference, which
+ * launches ~52k kernels per radiation call).  The graph binds the requests' buffers and solcon at capture
+ * time: refill the input buffers in place between launches; re-capture when a pointer, a column count or
+ * solcon changes.  rad_graph_create allocates the handle's scratch for the batch before capturing, so the
+ * replay allocates nothing.  A graph belongs to its handle and must be destroyed before it. */
+typedef struct RadGraph RadGraph;
+int rad_graph_create(RadHandle* h, int32_t nreq, const RadColumns* ins, const RadOutputs* outs,
+                     const int64_t* ncols, RadGraph** out);
+int rad_graph_launch(RadGraph* g, void* stream);
+void rad_graph_destroy(RadGraph* g);
+
 /* Device-time accounting of the library's own kernels (instrumentation; no counterpart in the reference,
  * which has none).  While enabled, rad_solve records CUDA events on its stream around the LW kernel, the
  * SW day-list kernels and the SW kernel; rad_profile_read waits for the last recorded event and returns

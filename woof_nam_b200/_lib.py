@@ -59,6 +59,10 @@ SIGNATURES = {
     "rad_workspace_bytes": ([ctypes.c_void_p, ctypes.c_int64], ctypes.c_int64),
     "rad_solve_batch": ([ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(RadColumns), ctypes.POINTER(RadOutputs),
                          ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p], ctypes.c_int),
+    "rad_graph_create": ([ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(RadColumns), ctypes.POINTER(RadOutputs),
+                          ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "rad_graph_launch": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rad_graph_destroy": ([ctypes.c_void_p], None),
     "rad_profile_enable": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rad_profile_read": ([ctypes.c_void_p, ctypes.POINTER(RadProfile)], ctypes.c_int),
     "rad_last_error": ([ctypes.c_void_p], ctypes.c_char_p),

@@ -627,6 +627,74 @@ int rad_solve_batch(RadHandle* h, int32_t nreq, const RadColumns* ins, const Rad
     return RAD_OK;
 }
 
+struct RadGraph {
+    RadHandle* h = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0;    // kernels one replay runs
+};
+
+int rad_graph_create(RadHandle* h, int32_t nreq, const RadColumns* ins, const RadOutputs* outs, const int64_t* ncols,
+                     RadGraph** out)
+{
+    if (!h || !out) return fail(h, RAD_E_INVALID, "rad_graph_create: null argument");
+    *out = nullptr;
+    // a first, uncaptured pass validates the arguments and grows the scratch to this batch
+    cudaStream_t st;
+    RAD_CUDA(h, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const bool prof = h->profiling;
+    h->profiling = false;
+    const int64_t l0 = h->launches;
+    int rc = rad_solve_batch(h, nreq, ins, outs, ncols, st);
+    const int64_t per = h->launches - l0;
+    if (rc == RAD_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = fail(h, RAD_E_CUDA, "rad_graph_create: warm-up solve failed");
+    RadGraph* g = nullptr;
+    if (rc == RAD_OK) {
+        g = new RadGraph();
+        g->h = h;
+        g->launches = per;
+        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            rc = rad_solve_batch(h, nreq, ins, outs, ncols, st);
+            const cudaError_t e2 = cudaStreamEndCapture(st, &g->graph);
+            if (rc == RAD_OK && e2 != cudaSuccess) rc = fail(h, RAD_E_CUDA, std::string("rad_graph_create: capture: ") + cudaGetErrorString(e2));
+        } else {
+            rc = fail(h, RAD_E_CUDA, std::string("rad_graph_create: begin capture: ") + cudaGetErrorString(e));
+        }
+        if (rc == RAD_OK && cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess)
+            rc = fail(h, RAD_E_CUDA, "rad_graph_create: instantiate failed");
+        h->launches = l0 + per;
+    }
+    h->profiling = prof;
+    cudaStreamDestroy(st);
+    if (rc != RAD_OK) {
+        if (g) {
+            if (g->exec) cudaGraphExecDestroy(g->exec);
+            if (g->graph) cudaGraphDestroy(g->graph);
+            delete g;
+        }
+        return rc;
+    }
+    *out = g;
+    return RAD_OK;
+}
+
+int rad_graph_launch(RadGraph* g, void* stream)
+{
+    if (!g) return fail(nullptr, RAD_E_INVALID, "rad_graph_launch: null graph");
+    RAD_CUDA(g->h, cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    g->h->launches += g->launches;
+    return RAD_OK;
+}
+
+void rad_graph_destroy(RadGraph* g)
+{
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+}
+
 int rad_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream)
 {
     if (!h || !in || !out) return fail(h, RAD_E_INVALID, "rad_solve: null argument");

@@ -174,6 +174,20 @@ class RadSolver:
                 r[k] = r[k].view(np.uint32)
         return r
 
+    def capture(self, requests: list, solcons: list, outs: list | None = None) -> "SolveGraph":
+        """Capture a batched solve of device-resident requests into a CUDA graph (rad_graph_create).  The
+        graph keeps the tensors' addresses: refill the inputs in place and replay with SolveGraph.launch()."""
+        n = len(requests)
+        outs = outs or [None] * n
+        args = [self._abi_args(c, s, o) for c, s, o in zip(requests, solcons, outs)]
+        ins = (_lib.RadColumns * max(n, 1))(*[a[0] for a in args])
+        ous = (_lib.RadOutputs * max(n, 1))(*[a[1] for a in args])
+        ncols = (ctypes.c_int64 * max(n, 1))(*[a[2] for a in args])
+        g = ctypes.c_void_p()
+        _lib.check(self.lib, self.handle, self.lib.rad_graph_create(self.handle, n, ins, ous, ncols, ctypes.byref(g)),
+                   "rad_graph_create")
+        return SolveGraph(self, g, requests, [a[3] for a in args])
+
     def profile(self, on: bool = True) -> None:
         """Start (or stop) device-time accounting of the library's kernels on this handle."""
         _lib.check(self.lib, self.handle, self.lib.rad_profile_enable(self.handle, int(on)), "rad_profile_enable")
@@ -186,3 +200,28 @@ class RadSolver:
 
     def workspace_bytes(self, ncol: int) -> int:
         return int(self.lib.rad_workspace_bytes(self.handle, ncol))
+
+
+class SolveGraph:
+    """A captured batched solve; holds references to its tensors so their memory outlives the graph."""
+
+    def __init__(self, solver: RadSolver, g, requests, outs):
+        self.solver, self.g, self.requests, self.outs = solver, g, requests, outs
+
+    def launch(self, stream=None) -> list:
+        torch = _torch()
+        st = stream if stream is not None else torch.cuda.current_stream()
+        _lib.check(self.solver.lib, self.solver.handle, self.solver.lib.rad_graph_launch(self.g, ctypes.c_void_p(st.cuda_stream)),
+                   "rad_graph_launch")
+        return self.outs
+
+    def close(self):
+        if getattr(self, "g", None):
+            self.solver.lib.rad_graph_destroy(self.g)
+            self.g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
