@@ -39,6 +39,7 @@ enum {
 
 enum { RAD_PREC_FP64 = 0, RAD_PREC_MIXED = 1 };
 enum { RAD_ROUTE_NAM = 0, RAD_ROUTE_MCICA = 1 };
+enum { RAD_PART_LW = 1, RAD_PART_SW = 2 };   /* RadConfig.parts bits */
 
 typedef struct RadHandle RadHandle;
 
@@ -56,6 +57,10 @@ typedef struct {
     int32_t iovrlw, iovrsw;  /* McICA overlap (0 random, 1 max-random, 2 maximum) */
     int32_t lw_seed0, sw_seed0;   /* McICA permutation seed offsets (ipsdlw0 = 140, ipsdsw0 = 1) */
     float cpathfac;          /* LW cloud-path factor (1.5) */
+    int32_t parts;           /* RAD_PART_LW | RAD_PART_SW (default both): which solves rad_solve runs, for
+                                steps where only one of lslwr / lsswr holds (module_RA_RRTM.F90:842-846 as
+                                cited at namgpu/physics/rrtm/rrtm_call.py:37); the other part's inputs and
+                                outputs may then be NULL */
 } RadConfig;
 
 /* Column inputs (device pointers, float32).  ncol columns, nlay layers, nlp1 = nlay + 1 levels. */

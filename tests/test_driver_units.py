@@ -1,0 +1,136 @@
+"""The reference-facing units (woof_nam_b200.lwrad / swrad / driver.column_solve) on a state laid out as
+the reference's: inputs by the reference's names in [field, level, JM, IM], outputs written back by name.
+They equal the solver called directly."""
+from __future__ import annotations
+
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+from woof_nam_b200 import driver
+from woof_nam_b200.columns import make_columns
+
+JM, IM = 7, 50
+
+
+class State:
+    """The reference's State surface the units use: fields by name, st[name], st.add(name, shape)."""
+
+    def __init__(self):
+        self.fields = {}
+
+    def __getitem__(self, k):
+        return self.fields[k]
+
+    def __setitem__(self, k, v):
+        self.fields[k] = v
+
+    def add(self, name, shape):
+        import torch
+        t = self.fields.get(name)
+        if t is None or tuple(t.shape) != tuple(shape):
+            t = torch.zeros(shape, dtype=torch.float32, device="cuda")
+            self.fields[name] = t
+        return t
+
+
+def _ctx(cols, device="cuda", cloud_scale=None):
+    import torch
+    st = State()
+    names = {"plyr": ("RAD_PLYR",), "plvl": ("RAD_PLVL",), "tlyr": ("RAD_TLYR",), "tlvl": ("TLVL",),
+             "qlyr": ("QLYR", "RAD_QLYR"), "olyr": ("RAD_OLYR",), "gasvmr": ("GASVMR",),
+             "clouds": ("RAD_CLOUDS",), "tsfg": ("RAD_TSFG",), "sfcemis": ("sfcemis",),
+             "coszen": ("SW_COSZEN",), "sfcalb": ("SFCALB",)}
+    for k, aliases in names.items():
+        a = np.ascontiguousarray(getattr(cols, k), dtype=np.float32)
+        t = torch.from_numpy(a.reshape(*a.shape[:-1], JM, IM).copy()).to(device)
+        if k == "clouds" and cloud_scale is not None:
+            t[1] *= cloud_scale       # cloud liquid path (Fortran index 2)
+            t[3] *= cloud_scale       # cloud ice path (Fortran index 4)
+        for n in aliases:
+            st[n] = t
+    grid = SimpleNamespace(jm=JM, im=IM, lm=cols.nlay - 1)
+    cfg = SimpleNamespace(solcon=cols.solcon, lfdncmp=True)
+    return SimpleNamespace(st=st, grid=grid, tables={}, cfg=cfg, stream=None)
+
+
+def test_missing_input_named_with_producer():
+    ctx = SimpleNamespace(st=State(), grid=SimpleNamespace(jm=JM, im=IM, lm=60), tables={}, cfg=None, stream=None)
+    with pytest.raises(KeyError, match="RAD_PLYR.*phys-rrtm-grrad-setup"):
+        driver.lwrad_run(ctx)
+    with pytest.raises(KeyError, match="RAD_PLYR.*phys-rrtm-grrad-setup"):
+        driver.swrad_run(ctx)
+
+
+def test_unsupported_sw_outputs_refused():
+    ctx = SimpleNamespace(st=State(), grid=SimpleNamespace(jm=JM, im=IM, lm=60), tables={},
+                          cfg=SimpleNamespace(lhsw0=True), stream=None)
+    with pytest.raises(NotImplementedError):
+        driver.swrad_run(ctx)
+    with pytest.raises(NotImplementedError):
+        driver.swrad_run(SimpleNamespace(st=State(), grid=None, tables={}, cfg=None, stream=None), has_htrswb=True)
+
+
+@pytest.mark.gpu
+def test_units_equal_solver():
+    import torch
+    from woof_nam_b200.solver import RadSolver
+    cols = make_columns(JM * IM, 77)
+    s = RadSolver(precision="mixed")
+    ref = s.solve(s.to_device(cols), cols.solcon)
+    torch.cuda.synchronize()
+    r = {k: v.cpu().numpy() for k, v in ref.items()}
+
+    # one launch set for both parts
+    ctx = _ctx(cols)
+    o = driver.column_solve(ctx)
+    torch.cuda.synchronize()
+    st = ctx.st
+    assert np.array_equal(st["htlwc"].cpu().numpy().reshape(cols.nlay, -1), r["htlw"])
+    assert np.array_equal(st["HTSWC"].cpu().numpy().reshape(cols.nlay, -1), r["htsw"])
+    assert np.array_equal(st["TOPFLX"].cpu().numpy().reshape(3, -1), r["topfsw"])
+    assert np.array_equal(st["SFCFLX"].cpu().numpy().reshape(4, -1), r["sfcfsw"])
+    for i, n in enumerate(driver.LW_FLUXES):
+        want = r["topflw"][i] if i < 2 else r["sfcflw"][i - 2]
+        assert np.array_equal(o[n].cpu().numpy().reshape(-1), want), n
+
+    # the SW unit alone
+    ctx = _ctx(cols)
+    o = driver.swrad_run(ctx)
+    torch.cuda.synchronize()
+    assert np.array_equal(o["HTSWC"].cpu().numpy().reshape(cols.nlay, -1), r["htsw"])
+    assert np.array_equal(o["FDNCMP"].cpu().numpy().reshape(6, -1), r["fdncmp"])
+    assert "htlwc" not in ctx.st.fields
+
+    # the LW unit alone, on clouds grrad-lw has already scaled by 1.5: equal up to the rounding of where
+    # the scaling happens, far inside 0.01 K/day and 0.05 W/m^2
+    ctx = _ctx(cols, cloud_scale=np.float32(1.5))
+    o = driver.lwrad_run(ctx)
+    torch.cuda.synchronize()
+    ht = o["hlwc"].cpu().numpy().reshape(cols.nlay, -1).astype(np.float64)
+    assert np.max(np.abs(ht - r["htlw"])) * 86400.0 < 1e-3
+    for i, n in enumerate(driver.LW_FLUXES):
+        want = r["topflw"][i] if i < 2 else r["sfcflw"][i - 2]
+        assert np.max(np.abs(o[n].cpu().numpy().reshape(-1) - want)) < 5e-3, n
+    assert "HTSWC" not in ctx.st.fields
+
+
+@pytest.mark.gpu
+def test_lw_only_and_sw_only_steps():
+    """column_solve on a step where only lslwr (or only lsswr) holds runs that part alone."""
+    import torch
+    cols = make_columns(JM * IM, 78)
+    ctx = _ctx(cols)
+    driver.column_solve(ctx, lslwr=True, lsswr=False)
+    torch.cuda.synchronize()
+    assert "htlwc" in ctx.st.fields and "HTSWC" not in ctx.st.fields
+    ctx2 = _ctx(cols)
+    driver.column_solve(ctx2, lslwr=False, lsswr=True)
+    torch.cuda.synchronize()
+    assert "HTSWC" in ctx2.st.fields and "htlwc" not in ctx2.st.fields
+    ctx3 = _ctx(cols)
+    driver.column_solve(ctx3)
+    torch.cuda.synchronize()
+    assert torch.equal(ctx.st["htlwc"], ctx3.st["htlwc"])
+    assert torch.equal(ctx2.st["HTSWC"], ctx3.st["HTSWC"])

@@ -15,6 +15,7 @@ RAD_OK, RAD_E_INVALID, RAD_E_TABLES, RAD_E_CUDA, RAD_E_NOMEM, RAD_E_BUDGET, RAD_
     0, -1, -2, -3, -4, -5, -6, -7
 PREC = {"fp64": 0, "mixed": 1}
 ROUTE = {"nam": 0, "mcica": 1}
+PARTS = {"lw": 1, "sw": 2, "both": 3}
 
 _fp = ctypes.POINTER(ctypes.c_float)
 _ip = ctypes.POINTER(ctypes.c_int32)
@@ -25,7 +26,8 @@ class RadConfig(ctypes.Structure):
     _fields_ = [("nlay", ctypes.c_int32), ("precision", ctypes.c_int32), ("route", ctypes.c_int32),
                 ("iswmode", ctypes.c_int32), ("diagnostic", ctypes.c_int32), ("window_cols", ctypes.c_int32),
                 ("sw_chunk", ctypes.c_int32), ("iovrlw", ctypes.c_int32), ("iovrsw", ctypes.c_int32),
-                ("lw_seed0", ctypes.c_int32), ("sw_seed0", ctypes.c_int32), ("cpathfac", ctypes.c_float)]
+                ("lw_seed0", ctypes.c_int32), ("sw_seed0", ctypes.c_int32), ("cpathfac", ctypes.c_float),
+                ("parts", ctypes.c_int32)]
 
 
 class RadColumns(ctypes.Structure):

@@ -291,9 +291,17 @@ int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
 // One launch set for up to RAD_MAXREQ requests: the McICA generators (McICA route), one LW launch over all
 // the requests' columns, the day list and group minima of all of them, one SW launch over all their sunlit
 // columns.  No host synchronisation.
+// Day-list scratch of one launch: the handle's growing buffers, or a fixed region the caller supplies.
+struct LaunchScratch {
+    int *flag, *pos, *daycol, *lt, *k8, *kw, *cmin, *nday;
+    void* cub;
+    size_t cub_bytes;
+    int64_t max_cols, max_cmin;   // capacity of a fixed region (unused for the handle's buffers)
+};
+
 template <class R>
 int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs* outs, const int64_t* ncols,
-                 cudaStream_t st)
+                 cudaStream_t st, const LaunchScratch* fixed = nullptr)
 {
     const RadConfig& cfg = h->cfg;
     const int nlay = cfg.nlay;
@@ -320,10 +328,19 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
     if (ntot == 0) return RAD_OK;
     if (ntot > (int64_t)std::numeric_limits<int>::max() - 1)
         return fail(h, RAD_E_INVALID, "rad_solve: more than 2^31 - 2 columns in one launch");
-    int rc = ensure_launch_scratch(h, ntot, std::max<int64_t>(ncmin, 1));
-    if (rc) return rc;
+    int rc = RAD_OK;
+    LaunchScratch sc;
+    if (fixed) {
+        if (ntot > fixed->max_cols || ncmin > fixed->max_cmin)
+            return fail(h, RAD_E_INVALID, "rad_solve: request larger than the fixed scratch region");
+        sc = *fixed;
+    } else {
+        if ((rc = ensure_launch_scratch(h, ntot, std::max<int64_t>(ncmin, 1)))) return rc;
+        sc = LaunchScratch{h->d_flag, h->d_pos, h->d_daycol, h->d_lt, h->d_k8, h->d_kw, h->d_cmin, h->d_nday,
+                           h->d_cub, h->cub_bytes, 0, 0};
+    }
     size_t eb = 0;
-    if (h->profiling) {
+    if (h->profiling && !fixed) {
         eb = h->ev_used;
         while (h->ev.size() < eb + 4) {
             cudaEvent_t e;
@@ -334,7 +351,9 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
         h->prof_solves += 1;
         h->prof_columns += ntot;
     }
-    int mrc = mark(h, st, eb, 0);
+    const bool prof = h->profiling && !fixed;
+    auto mark_if = [&](int i) { return prof ? mark(h, st, eb, i) : RAD_OK; };
+    int mrc = mark_if(0);
     if (mrc) return mrc;
     // ---- McICA route: sub-column cloud words of every column (LW and SW generators)
     const uint32_t* lwm[RAD_MAXREQ] = {};
@@ -343,8 +362,9 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
         for (int r = 0; r < nreq; ++r)
             if (ncols[r] > 0 && (rc = mcica_masks(h, ins + r, outs + r, ncols[r], db.off[r], st, &lwm[r], &swm[r])))
                 return rc;
+    const bool do_lw = cfg.parts & RAD_PART_LW, do_sw = cfg.parts & RAD_PART_SW;
     // ---- LW over every column
-    {
+    if (do_lw) {
         LwBatch bt{};
         bt.nreq = nreq;
         for (int r = 0; r <= nreq; ++r) bt.off[r] = db.off[r];
@@ -370,17 +390,21 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
         h->launches += 1;
         RAD_CUDA(h, cudaGetLastError());
     }
-    if ((mrc = mark(h, st, eb, 1))) return mrc;
+    if ((mrc = mark_if(1))) return mrc;
+    if (!do_sw) {
+        if ((mrc = mark_if(2))) return mrc;
+        return mark_if(3);
+    }
     // ---- SW day list, laytrop, groups
     const int T = 256;
     const unsigned gb = (unsigned)((ntot + 1 + T - 1) / T);
-    k_dayflags<<<gb, T, 0, st>>>(db, ntot, h->d_flag);
-    size_t tb = h->cub_bytes;
-    RAD_CUDA(h, cub::DeviceScan::ExclusiveSum(h->d_cub, tb, h->d_flag, h->d_pos, (int)(ntot + 1), st));
-    k_scatter<<<gb, T, 0, st>>>(h->d_flag, h->d_pos, ntot, h->d_daycol, h->d_nday);
-    k_fill_int<<<(unsigned)((ncmin + T - 1) / T), T, 0, st>>>(h->d_cmin, ncmin, std::numeric_limits<int>::max());
-    k_laytrop<<<gb, T, 0, st>>>(db, nlay, h->d_daycol, h->d_nday, h->d_lt, h->d_cmin, chunk, h->d_pos);
-    k_groups<<<gb, T, 0, st>>>(db, h->d_daycol, h->d_nday, h->d_lt, h->d_cmin, chunk, h->d_pos, h->d_k8, h->d_kw);
+    k_dayflags<<<gb, T, 0, st>>>(db, ntot, sc.flag);
+    size_t tb = sc.cub_bytes;
+    RAD_CUDA(h, cub::DeviceScan::ExclusiveSum(sc.cub, tb, sc.flag, sc.pos, (int)(ntot + 1), st));
+    k_scatter<<<gb, T, 0, st>>>(sc.flag, sc.pos, ntot, sc.daycol, sc.nday);
+    k_fill_int<<<(unsigned)((ncmin + T - 1) / T), T, 0, st>>>(sc.cmin, ncmin, std::numeric_limits<int>::max());
+    k_laytrop<<<gb, T, 0, st>>>(db, nlay, sc.daycol, sc.nday, sc.lt, sc.cmin, chunk, sc.pos);
+    k_groups<<<gb, T, 0, st>>>(db, sc.daycol, sc.nday, sc.lt, sc.cmin, chunk, sc.pos, sc.k8, sc.kw);
     h->launches += 7;   // day flags, scan (2 kernels), scatter, fill, laytrop, groups
     RAD_CUDA(h, cudaGetLastError());
     // ---- SW over the day columns; zeros first (night columns keep them, as swrad does)
@@ -401,10 +425,10 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
             const RadColumns* in = ins + r;
             const RadOutputs* out = outs + r;
             bt.req[r] = SwIn{in->plyr, in->plvl, in->tlyr, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faersw,
-                             in->sfcalb, in->coszen, h->d_daycol, h->d_nday, h->d_k8, h->d_kw, out->htsw, out->topfsw,
+                             in->sfcalb, in->coszen, sc.daycol, sc.nday, sc.k8, sc.kw, out->htsw, out->topfsw,
                              out->sfcfsw, out->fdncmp, ncols[r], nlay, cfg.diagnostic, cfg.iswmode, in->solcon, swm[r]};
         }
-        if ((mrc = mark(h, st, eb, 2))) return mrc;
+        if ((mrc = mark_if(2))) return mrc;
         if (sizeof(R) == 4) {
             const size_t smem = sw2_smem_bytes(any_aer);
             RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -419,7 +443,7 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
         h->launches += 1;
         RAD_CUDA(h, cudaGetLastError());
     }
-    return mark(h, st, eb, 3);
+    return mark_if(3);
 }
 }  // namespace
 
@@ -443,6 +467,7 @@ void rad_config_default(RadConfig* cfg, int32_t nlay)
     cfg->lw_seed0 = 140;
     cfg->sw_seed0 = 1;
     cfg->cpathfac = 1.5f;
+    cfg->parts = RAD_PART_LW | RAD_PART_SW;
 }
 
 int rad_create(const RadConfig* cfg, RadHandle** out)
@@ -451,6 +476,7 @@ int rad_create(const RadConfig* cfg, RadHandle** out)
     if (cfg->nlay < 2 || cfg->nlay > NLAY_MAX)
         return fail(nullptr, RAD_E_INVALID, "rad_create: nlay must be in [2, " + std::to_string(NLAY_MAX) + "]");
     if (cfg->iswmode < 1 || cfg->iswmode > 3) return fail(nullptr, RAD_E_INVALID, "rad_create: iswmode must be 1, 2 or 3");
+    if (cfg->parts < 1 || cfg->parts > 3) return fail(nullptr, RAD_E_INVALID, "rad_create: parts must be RAD_PART_LW, RAD_PART_SW or both");
     if (cfg->precision != RAD_PREC_FP64 && cfg->precision != RAD_PREC_MIXED)
         return fail(nullptr, RAD_E_INVALID, "rad_create: precision must be RAD_PREC_FP64 or RAD_PREC_MIXED");
     if (cfg->route != RAD_ROUTE_NAM && cfg->route != RAD_ROUTE_MCICA)
@@ -589,10 +615,11 @@ static int check_request(RadHandle* h, const RadColumns* in, const RadOutputs* o
     if (ncol < 0 || ncol > (int64_t)std::numeric_limits<int>::max() - 1)
         return fail(h, RAD_E_INVALID, std::string(what) + ": ncol out of range");
     if (ncol == 0) return RAD_OK;
-    if (!in->plyr || !in->plvl || !in->tlyr || !in->tlvl || !in->qlyr || !in->olyr || !in->gasvmr || !in->clouds ||
-        !in->sfcemis || !in->tsfg || !in->sfcalb || !in->coszen)
+    const bool lw = h->cfg.parts & RAD_PART_LW, sw = h->cfg.parts & RAD_PART_SW;
+    if (!in->plyr || !in->plvl || !in->tlyr || !in->qlyr || !in->olyr || !in->gasvmr || !in->clouds ||
+        (lw && (!in->tlvl || !in->sfcemis || !in->tsfg)) || (sw && (!in->sfcalb || !in->coszen)))
         return fail(h, RAD_E_INVALID, std::string(what) + ": a required input pointer is null");
-    if (!out->htlw || !out->htsw || !out->topflw || !out->sfcflw || !out->topfsw || !out->sfcfsw)
+    if ((lw && (!out->htlw || !out->topflw || !out->sfcflw)) || (sw && (!out->htsw || !out->topfsw || !out->sfcfsw)))
         return fail(h, RAD_E_INVALID, std::string(what) + ": a required output pointer is null");
     return RAD_OK;
 }

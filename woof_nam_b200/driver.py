@@ -1,0 +1,270 @@
+"""The reference's radiation units bound to this library.
+
+WOOF-NAM's radiation chain (namgpu/physics/rrtm/rrtm_call.py:246-365) runs, per chunk of rows, the grrad
+front end, then phys-rrtm-grrad-sw, which calls the SW column unit ``phys_rrtm_sw_swrad.run(ctx,
+has_htrswb)`` (phys_rrtm_grrad_sw.py:129,155), and phys-rrtm-grrad-lw, which scales the cloud paths by 1.5,
+calls the LW column unit ``phys_rrtm_lw_lwrad.run(ctx)`` (phys_rrtm_grrad_lw.py:79) and restores them.
+Both grrad units import the column unit by the module name held in ``SWRAD_MODULE`` / ``LWRAD_MODULE`` at
+call time, so the units of this module drop in by name:
+
+    phys_rrtm_grrad_sw.SWRAD_MODULE = "woof_nam_b200.swrad"
+    phys_rrtm_grrad_lw.LWRAD_MODULE = "woof_nam_b200.lwrad"
+
+or, for a whole radiation call, ``rrtm_call(ctx, args)`` below as the hook of
+``phys_rad_driver.run(ctx, rrtm_call=...)`` (phys_rad_driver.py:171,255-262).
+
+The units keep the reference's contract: inputs read from ``ctx.st`` by the reference's names, outputs
+written to ``ctx.st`` under the reference's names through ``st.add``, all work on ``ctx.stream``, no host
+synchronisation, a missing input refused by name with its producer.  Arrays may be CuPy or PyTorch CUDA
+arrays (zero-copy through ``__cuda_array_interface__``), float32, C-contiguous, [field, level, JM, IM].
+"""
+from __future__ import annotations
+
+import contextlib
+
+from .solver import RadSolver, SolverConfig
+
+# lwrad inputs: the unit's name, then the producer's state name (phys_rrtm_lw_lwrad.py:241-244), producer unit
+LW_INPUTS = {
+    "plyr": ("RAD_PLYR", "phys-rrtm-grrad-setup"), "plvl": ("RAD_PLVL", "phys-rrtm-grrad-setup"),
+    "tlyr": ("RAD_TLYR", "phys-rrtm-grrad-setup"), "tlvl": ("TLVL", "phys-rrtm-grrad-gases"),
+    "qlyr": ("QLYR", "phys-rrtm-grrad-gases"), "olyr": ("RAD_OLYR", "phys-rrtm-getozn"),
+    "gasvmr": ("GASVMR", "phys-rrtm-getgases"), "clouds": ("RAD_CLOUDS", "phys-rrtm-grrad-clouds"),
+    "tsfg": ("RAD_TSFG", "phys-rrtm-grrad-gases"), "sfcemis": ("sfcemis", "phys-rrtm-setemis"),
+}
+# swrad inputs (phys_rrtm_sw_swrad.py:104-116)
+SW_INPUTS = {
+    "plyr": ("RAD_PLYR", "phys-rrtm-grrad-setup"), "plvl": ("RAD_PLVL", "phys-rrtm-grrad-setup"),
+    "tlyr": ("RAD_TLYR", "phys-rrtm-grrad-setup"), "qlyr": ("RAD_QLYR", "phys-rrtm-grrad-gases"),
+    "olyr": ("RAD_OLYR", "phys-rrtm-getozn"), "gasvmr": ("GASVMR", "phys-rrtm-getgases"),
+    "clouds": ("RAD_CLOUDS", "phys-rrtm-grrad-clouds"), "coszen": ("SW_COSZEN", "phys-rrtm-grrad-sw"),
+    "sfcalb": ("SFCALB", "phys-rrtm-setalb"),
+}
+LW_FLUXES = ("topflw_upfxc", "topflw_upfx0", "sfcflw_upfxc", "sfcflw_upfx0", "sfcflw_dnfxc", "sfcflw_dnfx0")
+SOLCON_DEFAULT = 1368.22
+_KEY = "woof_nam_b200:solver"
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _fields(st) -> dict:
+    return st.fields if hasattr(st, "fields") else st
+
+
+def _get(st, unit: str, name: str, alias: str, producer: str):
+    f = _fields(st)
+    for k in (name, alias):
+        if k in f:
+            return f[k]
+    raise KeyError(f"{unit}: input {name!r} ({alias}) is missing; its producer is {producer}")
+
+
+def _as_tensor(x, name: str, unit: str):
+    torch = _torch()
+    t = x if isinstance(x, torch.Tensor) else torch.as_tensor(x, device="cuda")
+    if not t.is_cuda or t.dtype != torch.float32:
+        raise TypeError(f"{unit}: {name} must be a float32 CUDA array, got {t.dtype} on {t.device}")
+    if not t.is_contiguous():
+        raise ValueError(f"{unit}: {name} must be C-contiguous")
+    return t
+
+
+def _columns(st, unit: str, table: dict, jm: int, im: int, extra: dict) -> dict:
+    cols = {}
+    for k, (alias, producer) in table.items():
+        t = _as_tensor(_get(st, unit, k, alias, producer), k, unit)
+        if tuple(t.shape[-2:]) != (jm, im):
+            raise ValueError(f"{unit}: {k} has trailing shape {tuple(t.shape[-2:])}, expected ({jm}, {im})")
+        cols[k] = t.reshape(*t.shape[:-2], jm * im)
+    for k, x in extra.items():
+        if x is not None:
+            t = _as_tensor(x, k, unit)
+            cols[k] = t.reshape(*t.shape[:-2], jm * im)
+    return cols
+
+
+def _add(st, name: str, shape: tuple):
+    """A float32 output array in the state: st.add(name, shape) when the state allocates (the reference's
+    State), else a new zeroed CUDA tensor stored under name."""
+    torch = _torch()
+    if hasattr(st, "add"):
+        return st.add(name, shape)
+    t = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    st[name] = t
+    return t
+
+
+def _stream(ctx):
+    torch = _torch()
+    s = getattr(ctx, "stream", None)
+    if s is None:
+        return torch.cuda.current_stream()
+    if isinstance(s, torch.cuda.Stream):
+        return s
+    return torch.cuda.ExternalStream(int(getattr(s, "ptr", 0)))
+
+
+def _solver(ctx, parts: str, cpathfac: float, nlay: int) -> RadSolver:
+    """One handle per (parts, cloud-path factor, layers), kept in ctx.tables (tables are shared per device)."""
+    tabs = getattr(ctx, "tables", None)
+    cache = tabs.setdefault(_KEY, {}) if tabs is not None else {}
+    key = (parts, cpathfac, nlay)
+    s = cache.get(key)
+    if s is None:
+        cfg = getattr(ctx, "cfg", None)
+        s = RadSolver(SolverConfig(nlay=nlay, parts=parts, cpathfac=cpathfac,
+                                   precision=getattr(cfg, "rad_precision", "mixed")))
+        cache[key] = s
+    return s
+
+
+def _solcon(ctx) -> float:
+    """solcon of this call: rrtm_call's record, else ctx.cfg.solcon, else NMMB's 1368.22
+    (phys_rrtm_sw_swrad.py:297-304)."""
+    tabs = getattr(ctx, "tables", None) or {}
+    flags = tabs.get("rrtm_call_flags")
+    if flags is not None and flags.get("solcon") is not None:
+        return float(flags["solcon"])
+    return float(getattr(getattr(ctx, "cfg", None), "solcon", SOLCON_DEFAULT))
+
+
+def _faer(ctx, st, table_key: str, names: tuple):
+    tabs = getattr(ctx, "tables", None) or {}
+    if table_key in tabs:
+        return tabs[table_key]
+    f = _fields(st)
+    for k in names:
+        if k in f:
+            return f[k]
+    return None
+
+
+def lwrad_run(ctx) -> dict:
+    """Drop-in for phys_rrtm_lw_lwrad.run(ctx) (phys_rrtm_lw_lwrad.py:247-290): LW over every column of
+    ctx.grid.  The clouds arrive already scaled by grrad-lw's cloud-path factor, so this unit applies none.
+    Writes htlwc [LMK, JM, IM] and the six topflw_* / sfcflw_* [JM, IM] arrays; returns them as lwrad.run
+    does (keys of LW_FLUXES and "hlwc")."""
+    unit = "phys-rrtm-lw-lwrad"
+    st = ctx.st
+    g = ctx.grid
+    jm, im, nlay = int(g.jm), int(g.im), int(g.lm) + 1
+    cols = _columns(st, unit, LW_INPUTS, jm, im,
+                    {"faerlw": _faer(ctx, st, "rrtm_faerlw", ("faerlw", "RAD_FAERLW"))})
+    s = _solver(ctx, "lw", 1.0, nlay)
+    stream = _stream(ctx)
+    torch = _torch()
+    with torch.cuda.stream(stream):
+        hl = _as_tensor(_add(st, "htlwc", (nlay, jm, im)), "htlwc", unit)
+        out = s.alloc_outputs(jm * im)
+        out["htlw"] = hl.reshape(nlay, jm * im)     # solved in place into the state's htlwc
+        s.solve(cols, _solcon(ctx), out, stream=stream)
+        o = {}
+        for i, n in enumerate(LW_FLUXES):
+            dst = _as_tensor(_add(st, n, (jm, im)), n, unit)
+            src = out["topflw"][i] if i < 2 else out["sfcflw"][i - 2]
+            dst.view(-1).copy_(src)
+            o[n] = dst
+    o["hlwc"] = hl
+    o["hlw0"] = o["hlwb"] = o["flxprf"] = None
+    return o
+
+
+def swrad_run(ctx, has_htrswb: bool = False, nc: int = 0) -> dict:
+    """Drop-in for phys_rrtm_sw_swrad.run(ctx, has_htrswb, nc) (phys_rrtm_sw_swrad.py:282-386): SW over
+    the sunlit columns (SW_COSZEN >= 1e-4, the grrad-sw day predicate), zeros elsewhere.  Writes HTSWC
+    [LMK, JM, IM], TOPFLX [3, JM, IM], SFCFLX [4, JM, IM] and, with ctx.cfg.lfdncmp, FDNCMP [6, JM, IM].
+    The day list is built on the device inside the solve; nc (the reference's chunk size) has no effect
+    on the result and is accepted for the signature.  Spectral band heating (has_htrswb), clear-sky
+    heating (lhsw0) and flux profiles (lflxprf) are not produced: asking for them raises."""
+    unit = "phys-rrtm-sw-swrad"
+    del nc
+    cfg = getattr(ctx, "cfg", None)
+    if has_htrswb or getattr(cfg, "lhsw0", False) or getattr(cfg, "lflxprf", False):
+        raise NotImplementedError(f"{unit}: HTSWB / HSW0 / FLXPRF outputs are not produced by this library")
+    st = ctx.st
+    g = ctx.grid
+    jm, im, nlay = int(g.jm), int(g.im), int(g.lm) + 1
+    cols = _columns(st, unit, SW_INPUTS, jm, im,
+                    {"faersw": _faer(ctx, st, "rrtm_faersw", ("faersw", "RAD_FAERSW"))})
+    s = _solver(ctx, "sw", 1.0, nlay)
+    stream = _stream(ctx)
+    torch = _torch()
+    n = jm * im
+    with torch.cuda.stream(stream):
+        out = {}
+        o = {"HTSWC": _as_tensor(_add(st, "HTSWC", (nlay, jm, im)), "HTSWC", unit),
+             "TOPFLX": _as_tensor(_add(st, "TOPFLX", (3, jm, im)), "TOPFLX", unit),
+             "SFCFLX": _as_tensor(_add(st, "SFCFLX", (4, jm, im)), "SFCFLX", unit)}
+        out["htsw"] = o["HTSWC"].reshape(nlay, n)
+        out["topfsw"] = o["TOPFLX"].reshape(3, n)
+        out["sfcfsw"] = o["SFCFLX"].reshape(4, n)
+        if getattr(cfg, "lfdncmp", False):
+            o["FDNCMP"] = _as_tensor(_add(st, "FDNCMP", (6, jm, im)), "FDNCMP", unit)
+            out["fdncmp"] = o["FDNCMP"].reshape(6, n)
+        s.solve(cols, _solcon(ctx), out, stream=stream)
+    return o
+
+
+def column_solve(ctx, *, lslwr: bool = True, lsswr: bool = True) -> dict:
+    """LW and SW of one radiation call in one launch set, for a chain that calls it in place of grrad-sw's
+    swrad and grrad-lw's (scale clouds, lwrad, restore) block: the clouds are read unscaled and the LW
+    kernel applies NAM's cloud-path factor 1.5 itself.  Writes the outputs of both units."""
+    unit = "woof-nam-b200-column-solve"
+    parts = "both" if (lslwr and lsswr) else "lw" if lslwr else "sw" if lsswr else None
+    if parts is None:
+        return {}
+    st = ctx.st
+    g = ctx.grid
+    jm, im, nlay = int(g.jm), int(g.im), int(g.lm) + 1
+    n = jm * im
+    table = dict(LW_INPUTS) if lslwr else {}
+    if lsswr:
+        table.update(SW_INPUTS)
+        if lslwr:
+            table["qlyr"] = LW_INPUTS["qlyr"]
+    extra = {"faerlw": _faer(ctx, st, "rrtm_faerlw", ("faerlw", "RAD_FAERLW")) if lslwr else None,
+             "faersw": _faer(ctx, st, "rrtm_faersw", ("faersw", "RAD_FAERSW")) if lsswr else None}
+    cols = _columns(st, unit, table, jm, im, extra)
+    s = _solver(ctx, parts, 1.5, nlay)
+    stream = _stream(ctx)
+    torch = _torch()
+    o = {}
+    with torch.cuda.stream(stream):
+        out = {k: v for k, v in s.alloc_outputs(n).items() if k in ("topflw", "sfcflw")}
+        if lslwr:
+            o["htlwc"] = _as_tensor(_add(st, "htlwc", (nlay, jm, im)), "htlwc", unit)
+            out["htlw"] = o["htlwc"].reshape(nlay, n)
+        if lsswr:
+            for k, (name, rows) in {"htsw": ("HTSWC", nlay), "topfsw": ("TOPFLX", 3), "sfcfsw": ("SFCFLX", 4)}.items():
+                o[name] = _as_tensor(_add(st, name, (rows, jm, im)), name, unit)
+                out[k] = o[name].reshape(rows, n)
+        s.solve(cols, _solcon(ctx), out, stream=stream)
+        if lslwr:
+            for i, name in enumerate(LW_FLUXES):
+                o[name] = _as_tensor(_add(st, name, (jm, im)), name, unit)
+                o[name].view(-1).copy_(out["topflw"][i] if i < 2 else out["sfcflw"][i - 2])
+    return o
+
+
+@contextlib.contextmanager
+def bound_units():
+    """Bind the reference's grrad units to this library's column units for the duration of the block."""
+    from namgpu.physics.rrtm import phys_rrtm_grrad_lw as glw
+    from namgpu.physics.rrtm import phys_rrtm_grrad_sw as gsw
+    old = (glw.LWRAD_MODULE, gsw.SWRAD_MODULE)
+    glw.LWRAD_MODULE, gsw.SWRAD_MODULE = "woof_nam_b200.lwrad", "woof_nam_b200.swrad"
+    try:
+        yield
+    finally:
+        glw.LWRAD_MODULE, gsw.SWRAD_MODULE = old
+
+
+def rrtm_call(ctx, args: dict) -> None:
+    """The rrtm_call hook of phys_rad_driver.run (phys_rad_driver.py:255-262): the reference's radiation
+    chain (namgpu.physics.rrtm.rrtm_call.run) with its LW and SW column units bound to this library."""
+    from namgpu.physics.rrtm import rrtm_call as chain
+    with bound_units():
+        chain.run(ctx, args)

@@ -16,6 +16,10 @@ from .tables import blob
 
 INPUT_FIELDS = ("plyr", "plvl", "tlyr", "tlvl", "qlyr", "olyr", "gasvmr", "clouds", "sfcemis", "tsfg",
                 "sfcalb", "coszen")
+# inputs each solve reads (lwrad / swrad argument lists, phys_rrtm_lw_lwrad.py:36-46, phys_rrtm_sw_swrad.py:34-43)
+PART_FIELDS = {"lw": ("plyr", "plvl", "tlyr", "tlvl", "qlyr", "olyr", "gasvmr", "clouds", "sfcemis", "tsfg"),
+               "sw": ("plyr", "plvl", "tlyr", "qlyr", "olyr", "gasvmr", "clouds", "sfcalb", "coszen"),
+               "both": INPUT_FIELDS}
 OPTIONAL_INPUTS = ("faerlw", "faersw", "icseed")
 
 
@@ -38,6 +42,7 @@ class SolverConfig:
     iovrsw: int = 1
     lw_seed0: int = 140              # McICA seed offsets (ipsdlw0, ipsdsw0)
     sw_seed0: int = 1
+    parts: str = "both"              # "lw", "sw" or "both": which solves run (lslwr / lsswr steps)
 
 
 def output_shapes(nlay: int, ncol: int, route: str = "nam") -> dict:
@@ -69,6 +74,7 @@ class RadSolver:
         c.window_cols = self.cfg.window_cols
         c.sw_chunk = self.cfg.sw_chunk
         c.cpathfac = self.cfg.cpathfac
+        c.parts = _lib.PARTS[self.cfg.parts]
         c.iovrlw, c.iovrsw = self.cfg.iovrlw, self.cfg.iovrsw
         c.lw_seed0, c.sw_seed0 = self.cfg.lw_seed0, self.cfg.sw_seed0
         h = ctypes.c_void_p()
@@ -90,15 +96,20 @@ class RadSolver:
 
     # ---------------------------------------------------------------------------------------------
     def alloc_outputs(self, ncol: int, device=None) -> dict:
+        """Output tensors of a solve of ncol columns (those of the configured parts only)."""
         torch = _torch()
+        skip = {"lw": ("htsw", "topfsw", "sfcfsw", "fdncmp"), "sw": ("htlw", "topflw", "sfcflw"),
+                "both": ()}[self.cfg.parts]
         return {k: torch.empty(s, dtype=torch.int32 if k in MASK_KEYS else torch.float32, device=device or "cuda")
-                for k, s in output_shapes(self.cfg.nlay, ncol, self.cfg.route).items()}
+                for k, s in output_shapes(self.cfg.nlay, ncol, self.cfg.route).items() if k not in skip}
 
     def _abi_args(self, cols: dict, solcon: float, out: dict | None):
         torch = _torch()
-        ncol = int(cols["coszen"].shape[-1])
-        for k in INPUT_FIELDS:
-            t = cols[k]
+        ncol = int(cols["plyr"].shape[-1])
+        for k in PART_FIELDS[self.cfg.parts]:
+            t = cols.get(k)
+            if t is None:
+                raise KeyError(f"input {k!r} is missing")
             if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
                 raise TypeError(f"input {k!r} must be a contiguous float32 CUDA tensor")
             if t.shape[-1] != ncol:
@@ -106,10 +117,11 @@ class RadSolver:
         if cols["plyr"].shape[0] != self.cfg.nlay:
             raise ValueError(f"plyr has {cols['plyr'].shape[0]} layers, the solver was built for {self.cfg.nlay}")
         if out is None:
-            out = self.alloc_outputs(ncol, device=cols["coszen"].device)
+            out = self.alloc_outputs(ncol, device=cols["plyr"].device)
         ci = _lib.RadColumns()
         for k in INPUT_FIELDS:
-            setattr(ci, k, cols[k].data_ptr())
+            t = cols.get(k)
+            setattr(ci, k, t.data_ptr() if t is not None else None)
         for k in OPTIONAL_INPUTS:
             t = cols.get(k)
             if t is not None:
