@@ -137,6 +137,20 @@ int rad_graph_create(RadHandle* h, int32_t nreq, const RadColumns* ins, const Ra
 int rad_graph_launch(RadGraph* g, void* stream);
 void rad_graph_destroy(RadGraph* g);
 
+/* Solve without reaching any allocator (no counterpart in the reference).  rad_solve grows the handle's
+ * day-list scratch with cudaMalloc / cudaFree when a request is larger than any before it; cudaFree waits
+ * for the whole device, and a host model that has handed its memory to its own pool, or keeps a fixed HBM
+ * budget, may not want the library to allocate in the middle of a time step at all.  This entry runs the
+ * same kernels with that scratch in a fixed device array of the library (about 2 MB), so it takes at most
+ * RAD_NOALLOC_MAX_COLS columns (larger requests fail with RAD_E_INVALID) and, on the McICA route, needs the
+ * caller's lw_mask and sw_mask buffers.  The first call on a device resolves the array's address (a
+ * runtime query, no allocation); make that first call before any stream capture.  Every call on every
+ * handle of the process shares the one array: calls whose work may overlap on the device (other streams,
+ * other host threads) race on it, so issue them on one stream or one after another.  Profiling events are
+ * not recorded by this entry.  Results equal rad_solve's. */
+#define RAD_NOALLOC_MAX_COLS 65536
+int rad_solve_noalloc(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream);
+
 /* Device-time accounting of the library's own kernels (instrumentation; no counterpart in the reference,
  * which has none).  While enabled, rad_solve records CUDA events on its stream around the LW kernel, the
  * SW day-list kernels and the SW kernel; rad_profile_read waits for the last recorded event and returns

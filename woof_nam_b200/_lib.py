@@ -65,6 +65,8 @@ SIGNATURES = {
                           ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "rad_graph_launch": ([ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "rad_graph_destroy": ([ctypes.c_void_p], None),
+    "rad_solve_noalloc": ([ctypes.c_void_p, ctypes.POINTER(RadColumns), ctypes.POINTER(RadOutputs), ctypes.c_int64,
+                           ctypes.c_void_p], ctypes.c_int),
     "rad_profile_enable": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rad_profile_read": ([ctypes.c_void_p, ctypes.POINTER(RadProfile)], ctypes.c_int),
     "rad_last_error": ([ctypes.c_void_p], ctypes.c_char_p),

@@ -291,7 +291,7 @@ int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
 // One launch set for up to RAD_MAXREQ requests: the McICA generators (McICA route), one LW launch over all
 // the requests' columns, the day list and group minima of all of them, one SW launch over all their sunlit
 // columns.  No host synchronisation.
-// Day-list scratch of one launch: the handle's growing buffers, or a fixed region the caller supplies.
+// Day-list scratch of one launch: the handle's growing buffers, or a fixed region (rad_solve_noalloc).
 struct LaunchScratch {
     int *flag, *pos, *daycol, *lt, *k8, *kw, *cmin, *nday;
     void* cub;
@@ -332,7 +332,7 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
     LaunchScratch sc;
     if (fixed) {
         if (ntot > fixed->max_cols || ncmin > fixed->max_cmin)
-            return fail(h, RAD_E_INVALID, "rad_solve: request larger than the fixed scratch region");
+            return fail(h, RAD_E_INVALID, "rad_solve_noalloc: request larger than the fixed scratch region");
         sc = *fixed;
     } else {
         if ((rc = ensure_launch_scratch(h, ntot, std::max<int64_t>(ncmin, 1)))) return rc;
@@ -726,6 +726,81 @@ int rad_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t
 {
     if (!h || !in || !out) return fail(h, RAD_E_INVALID, "rad_solve: null argument");
     return rad_solve_batch(h, 1, in, out, &ncol, stream);
+}
+
+// ---------------------------------------------------------------------------- fixed-scratch solve
+// rad_solve_noalloc: the day-list scratch of a solve lives in this file-scope device array instead of the
+// handle's growing buffers, so the call reaches no allocator.  Layout in 32-bit words, each part 256-byte
+// aligned: flag, pos, daycol, lt, k8, kw ([NA_W] each), cmin ([2 NA_W]), nday ([64]), CUB scan temp.
+// Nothing in it has to start at zero: every word a solve reads is written earlier in the same solve.
+namespace {
+constexpr int64_t NA_W = ((RAD_NOALLOC_MAX_COLS + 1 + 63) / 64) * 64;
+constexpr int64_t NA_CUB_WORDS = 16384;   // 64 KiB for the device-wide scan
+constexpr int64_t NA_WORDS = 8 * NA_W + 64 + NA_CUB_WORDS;
+__device__ __align__(256) uint32_t g_noalloc_scratch[NA_WORDS];
+
+struct NoallocSlot {
+    bool ready = false;
+    LaunchScratch sc{};
+};
+std::mutex g_na_mu;
+NoallocSlot g_na[64];   // per device ordinal
+
+// Resolve the array's address on the current device (once per device) and check the scan's temp size.
+int noalloc_scratch(RadHandle* h, int dev, LaunchScratch* out)
+{
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    if (dev < 0 || dev >= 64) return fail(h, RAD_E_INVALID, "rad_solve_noalloc: device ordinal above 63");
+    NoallocSlot& s = g_na[dev];
+    if (!s.ready) {
+        uint32_t* base = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void**)&base, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return fail(h, RAD_E_CUDA, std::string("rad_solve_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        size_t need = 0;
+        RAD_CUDA(h, cub::DeviceScan::ExclusiveSum(nullptr, need, (int*)nullptr, (int*)nullptr, (int)(RAD_NOALLOC_MAX_COLS + 1)));
+        if (need > (size_t)NA_CUB_WORDS * 4)
+            return fail(h, RAD_E_INVALID, "rad_solve_noalloc: the scan needs more temp space than the fixed region holds");
+        int* w = (int*)base;
+        LaunchScratch& c = s.sc;
+        c.flag = w;
+        c.pos = w + NA_W;
+        c.daycol = w + 2 * NA_W;
+        c.lt = w + 3 * NA_W;
+        c.k8 = w + 4 * NA_W;
+        c.kw = w + 5 * NA_W;
+        c.cmin = w + 6 * NA_W;
+        c.nday = w + 8 * NA_W;
+        c.cub = (void*)(w + 8 * NA_W + 64);
+        c.cub_bytes = (size_t)NA_CUB_WORDS * 4;
+        c.max_cols = RAD_NOALLOC_MAX_COLS;
+        c.max_cmin = 2 * NA_W;
+        s.ready = true;
+    }
+    *out = s.sc;
+    return RAD_OK;
+}
+}  // namespace
+
+int rad_solve_noalloc(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream)
+{
+    if (!h || !in || !out) return fail(h, RAD_E_INVALID, "rad_solve_noalloc: null argument");
+    if (!h->tables_ok) return fail(h, RAD_E_TABLES, "rad_solve_noalloc: tables not loaded (rad_load_tables)");
+    int rc = check_request(h, in, out, ncol, "rad_solve_noalloc");
+    if (rc) return rc;
+    if (ncol > RAD_NOALLOC_MAX_COLS)
+        return fail(h, RAD_E_INVALID, "rad_solve_noalloc: ncol above RAD_NOALLOC_MAX_COLS (65536); use rad_solve");
+    if (h->cfg.route == RAD_ROUTE_MCICA && (!out->lw_mask || !out->sw_mask))
+        return fail(h, RAD_E_INVALID, "rad_solve_noalloc: the McICA route needs the caller's lw_mask and sw_mask buffers");
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != h->device) return fail(h, RAD_E_INVALID, "rad_solve_noalloc: handle belongs to another device");
+    if (ncol == 0) return RAD_OK;
+    LaunchScratch sc;
+    if ((rc = noalloc_scratch(h, dev, &sc))) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    return h->cfg.precision == RAD_PREC_FP64 ? launch_batch<double>(h, 1, in, out, &ncol, st, &sc)
+                                             : launch_batch<float>(h, 1, in, out, &ncol, st, &sc);
 }
 
 int rad_profile_enable(RadHandle* h, int on)
