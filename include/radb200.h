@@ -151,6 +151,42 @@ void rad_graph_destroy(RadGraph* g);
 #define RAD_NOALLOC_MAX_COLS 65536
 int rad_solve_noalloc(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream);
 
+/* The radiation call's post step (rrtm_post_outputs, namgpu/kernels/phys_rrtm_driver_post.cu:71-145, the
+ * ICWP /= -1 path of module_RA_RRTM.F90:1142-1240): heating rates and fluxes into the model's radiation
+ * state, the radiation-step cloud diagnostics, SIGT4 on LW steps.  All arrays [level or component][ncol],
+ * float32 unless noted, device pointers.  hlw / swh hold lm + kd levels: kd = 1 reads the solve's
+ * [nlay = lm + 1] htlw / htsw directly (the extra top layer skipped, as grrad's htrlw / htrsw copies do),
+ * kd = 0 reads [lm] arrays (htrlw / HTRSW, the reference kernel's interface).  cloud_block = 0 skips the
+ * cloud diagnostics (then cldcov ... ncfrcv may be NULL). */
+typedef struct {
+    const float* hlw;            /* [lm + kd][ncol] LW heating, K/s (htrlw, or the solve's htlw with kd 1) */
+    const float* swh;            /* [lm + kd][ncol] SW heating, K/s (HTRSW, or the solve's htsw with kd 1) */
+    const float* coszdg_v;       /* [ncol] GRRAD_COSZDG_V */
+    const float* coszen_v;       /* [ncol] GRRAD_COSZEN_V */
+    const float* sfcflw_dnfxc;   /* [ncol] sfc LW down, total sky (row 2 of the solve's sfcflw) */
+    const float* topflw_upfxc;   /* [ncol] TOA LW up, total sky (row 0 of topflw) */
+    const float* sfcfsw_upfxc;   /* [ncol] SFCFSW row 0 */
+    const float* sfcfsw_dnfxc;   /* [ncol] SFCFSW row 1 */
+    const float* sfcfsw_dnfx0;   /* [ncol] SFCFSW row 3 */
+    const float* topfsw_upfxc;   /* [ncol] TOPFSW row 0 */
+    float* cldcov;               /* [lm][ncol] cldcov, zeroed in place on columns with max CW < 1e-8 */
+    float* cldsa;                /* [5][ncol] cldsa, zeroed in place on the same columns */
+    const float* cw;             /* [lm][ncol] total condensate CW */
+    const float* t;              /* [lm][ncol] temperature T (level lm - 1 used) */
+    const int32_t* cu_cloud;     /* [ncol] CU_cloud flag */
+} RadPostIn;
+
+typedef struct {
+    float *rlwtt, *rswtt, *cldfra, *csmid;                       /* [lm][ncol] */
+    float *rlwin, *rswin, *rswinc, *rswout, *rlwtoa, *rswtoa;    /* [ncol] */
+    float *czmean, *sigt4, *coszdg;                              /* [ncol] */
+    float *cfracl, *cfracm, *cfrach, *acfrst, *acfrcv;           /* [ncol]; acfrst / acfrcv accumulate */
+    int32_t *ncfrst, *ncfrcv;                                    /* [ncol]; counters, incremented */
+} RadPostOut;
+
+int rad_post_outputs(RadHandle* h, const RadPostIn* in, const RadPostOut* out, int64_t ncol, int32_t lm,
+                     int32_t kd, int32_t cloud_block, int32_t lw_step, void* stream);
+
 /* Device-time accounting of the library's own kernels (instrumentation; no counterpart in the reference,
  * which has none).  While enabled, rad_solve records CUDA events on its stream around the LW kernel, the
  * SW day-list kernels and the SW kernel; rad_profile_read waits for the last recorded event and returns

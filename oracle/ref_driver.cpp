@@ -91,6 +91,9 @@ namespace r_lwmc {
 namespace r_swmc {
 #include "phys_rrtm_sw_mcica_subcol.cu"
 }
+namespace r_post {
+#include "phys_rrtm_driver_post.cu"
+}
 namespace r_swrad {
 #include "phys_rrtm_sw_swrad.cu"
 }
@@ -1083,6 +1086,28 @@ int orc_solve(int precision, const int* cfg_i, double cpathfac, int nlay, int nc
         std::fprintf(stderr, "reference driver: %s\n", e.what());
         return -1;
     }
+    return 0;
+}
+
+// The radiation call's post step from the reference kernel rrtm_post_outputs (phys_rrtm_driver_post.cu:71-145),
+// columns flattened (IM = ncol, JM = 1), so every [l, JM, IM] array is [l][ncol].  lssav is 1 (the
+// reference refuses anything else).
+int ref_post_outputs(int ncol, int lm, int icwp, int lw_step, const float* hlw, const float* swh,
+                     const float* coszdg_v, const float* coszen_v, const float* sfcflw_dnfxc,
+                     const float* sfcfsw_dnfxc, const float* sfcfsw_upfxc, const float* sfcfsw_dnfx0,
+                     const float* topflw_upfxc, const float* topfsw_upfxc, float* cldcov, float* cldsa,
+                     const float* cw, const float* t, const int* cu_cloud, float* rlwtt, float* rswtt,
+                     float* cldfra, float* csmid, float* rlwin, float* rswin, float* rswinc, float* rswout,
+                     float* rlwtoa, float* rswtoa, float* czmean, float* sigt4, float* coszdg, float* cfracl,
+                     float* cfracm, float* cfrach, float* acfrst, float* acfrcv, int* ncfrst, int* ncfrcv)
+{
+    drv::launch(drv::cdiv(ncol, 128), 1, 1, 128, [&] {
+        r_post::rrtm_post_outputs(ncol, 1, lm, icwp, 1, lw_step, hlw, swh, coszdg_v, coszen_v, sfcflw_dnfxc,
+                                  sfcfsw_dnfxc, sfcfsw_upfxc, sfcfsw_dnfx0, topflw_upfxc, topfsw_upfxc, cldcov,
+                                  cldsa, cw, t, cu_cloud, rlwtt, rswtt, cldfra, csmid, rlwin, rswin, rswinc,
+                                  rswout, rlwtoa, rswtoa, czmean, sigt4, coszdg, cfracl, cfracm, cfrach, acfrst,
+                                  acfrcv, ncfrst, ncfrcv);
+    });
     return 0;
 }
 }

@@ -134,3 +134,39 @@ def test_lw_only_and_sw_only_steps():
     torch.cuda.synchronize()
     assert torch.equal(ctx.st["htlwc"], ctx3.st["htlwc"])
     assert torch.equal(ctx2.st["HTSWC"], ctx3.st["HTSWC"])
+
+
+@pytest.mark.gpu
+def test_driver_post_equals_oracle():
+    """driver_post_run on a state under the reference's names gives the oracle's post step."""
+    import torch
+    from oracle import post
+    lm, jm, im = 60, 4, 33
+    n = jm * im
+    inp, state = post.make_case(n, lm, 9)
+    ref = post.post_outputs(inp, state, lm, lw_step=True)
+    st = State()
+    t = lambda a, *shape: torch.from_numpy(np.ascontiguousarray(a).reshape(*shape)).cuda()  # noqa: E731
+    st["htrlw"], st["HTRSW"] = t(inp["hlw"], lm, jm, im), t(inp["swh"], lm, jm, im)
+    st["cldcov"], st["cldsa"] = t(inp["cldcov"], lm, jm, im), t(inp["cldsa"], 5, jm, im)
+    st["GRRAD_COSZDG_V"], st["GRRAD_COSZEN_V"] = t(inp["coszdg_v"], jm, im), t(inp["coszen_v"], jm, im)
+    st["sfcflw_dnfxc"], st["topflw_upfxc"] = t(inp["sfcflw_dnfxc"], jm, im), t(inp["topflw_upfxc"], jm, im)
+    sfc = np.stack([inp["sfcfsw_upfxc"], inp["sfcfsw_dnfxc"], np.zeros(n, np.float32), inp["sfcfsw_dnfx0"]])
+    top = np.stack([inp["topfsw_upfxc"], np.zeros(n, np.float32), np.zeros(n, np.float32)])
+    st["SFCFSW"], st["TOPFSW"] = t(sfc, 4, jm, im), t(top, 3, jm, im)
+    st["CW"], st["T"] = t(inp["cw"], lm, jm, im), t(inp["t"], lm, jm, im)
+    for k in ("RLWTT", "RSWTT", "CLDFRA"):
+        st[k] = torch.zeros((lm, jm, im), dtype=torch.float32, device="cuda")
+    for k in driver.POST_OUTPUTS_2D:
+        low = k.lower()
+        st[k] = t(state[low], jm, im) if low in state else torch.zeros((jm, im), dtype=torch.float32, device="cuda")
+    ctx = SimpleNamespace(st=st, grid=SimpleNamespace(jm=jm, im=im, lm=lm), cfg=SimpleNamespace(nradl=48),
+                          tables={"rrtm_driver_call": {"CU_CLOUD": t(inp["cu_cloud"], jm, im)}}, stream=None,
+                          ntimestep=96)
+    driver.driver_post_run(ctx)
+    torch.cuda.synchronize()
+    for k in ("rlwtt", "rswtt", "cldfra", "csmid", "coszdg"):
+        assert np.array_equal(st[k.upper()].cpu().numpy().reshape(ref[k].shape), ref[k]), k
+    for k in driver.POST_OUTPUTS_2D:
+        assert np.array_equal(st[k].cpu().numpy().reshape(-1), ref[k.lower()]), k
+    assert np.array_equal(st["cldcov"].cpu().numpy().reshape(lm, n), ref["cldcov"])

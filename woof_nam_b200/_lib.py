@@ -50,6 +50,20 @@ class RadProfile(ctypes.Structure):
                 ("lw_ms", ctypes.c_double), ("prep_ms", ctypes.c_double), ("sw_ms", ctypes.c_double)]
 
 
+POST_IN_FIELDS = ("hlw", "swh", "coszdg_v", "coszen_v", "sfcflw_dnfxc", "topflw_upfxc", "sfcfsw_upfxc",
+                  "sfcfsw_dnfxc", "sfcfsw_dnfx0", "topfsw_upfxc", "cldcov", "cldsa", "cw", "t", "cu_cloud")
+POST_OUT_FIELDS = ("rlwtt", "rswtt", "cldfra", "csmid", "rlwin", "rswin", "rswinc", "rswout", "rlwtoa", "rswtoa",
+                   "czmean", "sigt4", "coszdg", "cfracl", "cfracm", "cfrach", "acfrst", "acfrcv", "ncfrst", "ncfrcv")
+
+
+class RadPostIn(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in POST_IN_FIELDS]
+
+
+class RadPostOut(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in POST_OUT_FIELDS]
+
+
 # Every symbol include/radb200.h declares, with its ctypes signature.
 SIGNATURES = {
     "rad_version": ([], ctypes.c_int),
@@ -67,6 +81,8 @@ SIGNATURES = {
     "rad_graph_destroy": ([ctypes.c_void_p], None),
     "rad_solve_noalloc": ([ctypes.c_void_p, ctypes.POINTER(RadColumns), ctypes.POINTER(RadOutputs), ctypes.c_int64,
                            ctypes.c_void_p], ctypes.c_int),
+    "rad_post_outputs": ([ctypes.c_void_p, ctypes.POINTER(RadPostIn), ctypes.POINTER(RadPostOut), ctypes.c_int64,
+                          ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p], ctypes.c_int),
     "rad_profile_enable": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rad_profile_read": ([ctypes.c_void_p, ctypes.POINTER(RadProfile)], ctypes.c_int),
     "rad_last_error": ([ctypes.c_void_p], ctypes.c_char_p),

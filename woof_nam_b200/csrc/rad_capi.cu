@@ -35,6 +35,7 @@ __constant__ int c_sw_ns[15] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94
 #include "rad_sw2.cuh"
 #include "rad_lw2.cuh"
 #include "rad_mcica.cuh"
+#include "rad_post.cuh"
 
 using namespace rad;
 
@@ -801,6 +802,35 @@ int rad_solve_noalloc(RadHandle* h, const RadColumns* in, const RadOutputs* out,
     cudaStream_t st = (cudaStream_t)stream;
     return h->cfg.precision == RAD_PREC_FP64 ? launch_batch<double>(h, 1, in, out, &ncol, st, &sc)
                                              : launch_batch<float>(h, 1, in, out, &ncol, st, &sc);
+}
+
+int rad_post_outputs(RadHandle* h, const RadPostIn* in, const RadPostOut* out, int64_t ncol, int32_t lm,
+                     int32_t kd, int32_t cloud_block, int32_t lw_step, void* stream)
+{
+    if (!h || !in || !out) return fail(h, RAD_E_INVALID, "rad_post_outputs: null argument");
+    if (ncol < 0 || lm < 1 || kd < 0 || kd > 1) return fail(h, RAD_E_INVALID, "rad_post_outputs: ncol, lm or kd out of range");
+    if (ncol == 0) return RAD_OK;
+    if (!in->hlw || !in->swh || !in->coszdg_v || !in->coszen_v || !in->sfcflw_dnfxc || !in->topflw_upfxc ||
+        !in->sfcfsw_upfxc || !in->sfcfsw_dnfxc || !in->sfcfsw_dnfx0 || !in->topfsw_upfxc || !out->rlwtt ||
+        !out->rswtt || !out->rlwin || !out->rswin || !out->rswinc || !out->rswout || !out->rlwtoa || !out->rswtoa ||
+        !out->czmean || !out->coszdg)
+        return fail(h, RAD_E_INVALID, "rad_post_outputs: a required pointer is null");
+    if (cloud_block && (!in->cldcov || !in->cldsa || !in->cw || !in->cu_cloud || !out->cldfra || !out->csmid ||
+                        !out->cfracl || !out->cfracm || !out->cfrach || !out->acfrst || !out->acfrcv ||
+                        !out->ncfrst || !out->ncfrcv))
+        return fail(h, RAD_E_INVALID, "rad_post_outputs: a cloud-diagnostic pointer is null");
+    if (lw_step && (!in->t || !out->sigt4)) return fail(h, RAD_E_INVALID, "rad_post_outputs: T / SIGT4 null on an LW step");
+    PostArgs a{in->hlw, in->swh, in->coszdg_v, in->coszen_v, in->sfcflw_dnfxc, in->topflw_upfxc, in->sfcfsw_upfxc,
+               in->sfcfsw_dnfxc, in->sfcfsw_dnfx0, in->topfsw_upfxc, in->cldcov, in->cldsa, in->cw, in->t,
+               in->cu_cloud, out->rlwtt, out->rswtt, out->cldfra, out->csmid, out->rlwin, out->rswin, out->rswinc,
+               out->rswout, out->rlwtoa, out->rswtoa, out->czmean, out->sigt4, out->coszdg, out->cfracl, out->cfracm,
+               out->cfrach, out->acfrst, out->acfrcv, out->ncfrst, out->ncfrcv, ncol, lm, kd, cloud_block ? 1 : 0,
+               lw_step ? 1 : 0};
+    const unsigned grid = (unsigned)((ncol + 255) / 256);
+    k_post_outputs<<<grid, 256, 0, (cudaStream_t)stream>>>(a);
+    h->launches += 1;
+    RAD_CUDA(h, cudaGetLastError());
+    return RAD_OK;
 }
 
 int rad_profile_enable(RadHandle* h, int on)

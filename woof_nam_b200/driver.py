@@ -249,6 +249,72 @@ def column_solve(ctx, *, lslwr: bool = True, lsswr: bool = True) -> dict:
     return o
 
 
+POST_OUTPUTS_2D = ("RLWIN", "RSWIN", "RSWINC", "RSWOUT", "RLWTOA", "RSWTOA", "CZMEAN", "SIGT4", "CFRACL",
+                   "CFRACM", "CFRACH", "ACFRST", "ACFRCV", "NCFRST", "NCFRCV")
+
+
+def driver_post_run(ctx, *, icwp: int = 1, ntimestep: int | None = None, lssav: bool = True,
+                    cncld: bool = True) -> None:
+    """Drop-in for phys_rrtm_driver_post.run (phys_rrtm_driver_post.py:121-202) on NAM's ICWP /= -1 path:
+    one rad_post_outputs launch reads the grrad outputs by the reference's names (htrlw, HTRSW, cldcov,
+    cldsa, GRRAD_COSZDG_V, GRRAD_COSZEN_V, sfcflw_dnfxc, topflw_upfxc, SFCFSW, TOPFSW,
+    ctx.tables["rrtm_driver_call"]["CU_CLOUD"]) and the state (CW, T), and writes RLWTT, RSWTT, CLDFRA,
+    CSMID, the surface / TOA fields, the cloud fractions and accumulators, COSZDG and, on LW steps
+    (NTIMESTEP mod NRADL == 0), SIGT4.  lssav false and the ICWP == -1 (old NAM/GFDL) cloud block are
+    refused."""
+    unit = "phys-rrtm-driver-post"
+    del cncld                 # read only by the ICWP == -1 block
+    if not lssav:
+        raise NotImplementedError(f"{unit}: lssav=False makes the Fortran STOP; not run")
+    if icwp == -1:
+        raise NotImplementedError(f"{unit}: the ICWP == -1 (old NAM/GFDL) cloud block is not built")
+    torch = _torch()
+    st, g = ctx.st, ctx.grid
+    jm, im, lm = int(g.jm), int(g.im), int(g.lm)
+    n = jm * im
+    nts = int(ctx.ntimestep if ntimestep is None else ntimestep)
+    lw_step = nts % int(getattr(ctx.cfg, "nradl", 48)) == 0
+    f = _fields(st)
+
+    def need(name, owner):
+        if name not in f:
+            raise KeyError(f"{unit}: ctx.st['{name}'] is missing (written by {owner}, which has not run)")
+        return _as_tensor(f[name], name, unit) if name not in ("NCFRST", "NCFRCV") else f[name]
+
+    lw_post = "phys-rrtm-grrad-lw (post_heat / post_flux)"
+    sfcfsw = need("SFCFSW", "phys-rrtm-grrad-sw").reshape(4, n)
+    topfsw = need("TOPFSW", "phys-rrtm-grrad-sw").reshape(3, n)
+    cu = (getattr(ctx, "tables", None) or {}).get("rrtm_driver_call", {}).get("CU_CLOUD")
+    if cu is None:
+        raise KeyError(f"{unit}: ctx.tables['rrtm_driver_call']['CU_CLOUD'] is missing (written by "
+                       "phys-rrtm-driver-call, which has not run)")
+    cu = torch.as_tensor(cu, device="cuda")
+    if cu.dtype != torch.int32:
+        raise TypeError(f"{unit}: CU_CLOUD must be int32, got {cu.dtype}")
+    inp = {"hlw": need("htrlw", lw_post).reshape(lm, n), "swh": need("HTRSW", "phys-rrtm-grrad-sw").reshape(lm, n),
+           "coszdg_v": need("GRRAD_COSZDG_V", "phys-rrtm-coszmn").reshape(n),
+           "coszen_v": need("GRRAD_COSZEN_V", "phys-rrtm-coszmn").reshape(n),
+           "sfcflw_dnfxc": need("sfcflw_dnfxc", "phys-rrtm-lw-lwrad").reshape(n),
+           "topflw_upfxc": need("topflw_upfxc", "phys-rrtm-lw-lwrad").reshape(n),
+           "sfcfsw_upfxc": sfcfsw[0], "sfcfsw_dnfxc": sfcfsw[1], "sfcfsw_dnfx0": sfcfsw[3], "topfsw_upfxc": topfsw[0],
+           "cldcov": need("cldcov", lw_post).reshape(lm, n), "cldsa": need("cldsa", lw_post).reshape(5, n),
+           "cw": need("CW", "the state").reshape(lm, n), "t": need("T", "the state").reshape(lm, n),
+           "cu_cloud": cu.reshape(n)}
+    out = {"rlwtt": need("RLWTT", "the state").reshape(lm, n), "rswtt": need("RSWTT", "the state").reshape(lm, n),
+           "cldfra": need("CLDFRA", "the state").reshape(lm, n),
+           "csmid": _as_tensor(_add(st, "CSMID", (lm, jm, im)), "CSMID", unit).reshape(lm, n),
+           "coszdg": _as_tensor(_add(st, "COSZDG", (jm, im)), "COSZDG", unit).reshape(n)}
+    for k in POST_OUTPUTS_2D:
+        t = need(k, "the state")
+        if k in ("NCFRST", "NCFRCV"):
+            t = torch.as_tensor(t, device="cuda")
+            if t.dtype != torch.int32:
+                raise TypeError(f"{unit}: {k} must be int32, got {t.dtype}")
+        out[k.lower()] = t.reshape(n)
+    s = _solver(ctx, "both", 1.5, lm + 1)
+    s.post_outputs(inp, out, lm, kd=0, cloud_block=True, lw_step=lw_step, stream=_stream(ctx))
+
+
 @contextlib.contextmanager
 def bound_units():
     """Bind the reference's grrad units to this library's column units for the duration of the block."""

@@ -200,6 +200,31 @@ class RadSolver:
                    "rad_graph_create")
         return SolveGraph(self, g, requests, [a[3] for a in args])
 
+    def post_outputs(self, inp: dict, out: dict, lm: int, kd: int = 1, cloud_block: bool = True,
+                     lw_step: bool = True, stream=None) -> dict:
+        """The radiation call's post step (rad_post_outputs; rrtm_post_outputs of the reference,
+        phys_rrtm_driver_post.cu:71-145): inp / out map the lower-case names of RadPostIn / RadPostOut to
+        contiguous CUDA tensors ([level or component][ncol]; cu_cloud, ncfrst, ncfrcv int32).  With kd = 1,
+        hlw / swh are the solve's [nlay] htlw / htsw."""
+        torch = _torch()
+        n = int(inp["coszen_v"].shape[-1])
+        pi, po = _lib.RadPostIn(), _lib.RadPostOut()
+        for k in _lib.POST_IN_FIELDS:
+            t = inp.get(k)
+            if t is not None and not (t.is_cuda and t.is_contiguous() and t.shape[-1] == n):
+                raise TypeError(f"post input {k!r} must be a contiguous CUDA tensor with {n} columns")
+            setattr(pi, k, t.data_ptr() if t is not None else None)
+        for k in _lib.POST_OUT_FIELDS:
+            t = out.get(k)
+            if t is not None and not (t.is_cuda and t.is_contiguous() and t.shape[-1] == n):
+                raise TypeError(f"post output {k!r} must be a contiguous CUDA tensor with {n} columns")
+            setattr(po, k, t.data_ptr() if t is not None else None)
+        st = stream if stream is not None else torch.cuda.current_stream()
+        rc = self.lib.rad_post_outputs(self.handle, ctypes.byref(pi), ctypes.byref(po), n, lm, kd, int(cloud_block),
+                                       int(lw_step), ctypes.c_void_p(st.cuda_stream))
+        _lib.check(self.lib, self.handle, rc, "rad_post_outputs")
+        return out
+
     def profile(self, on: bool = True) -> None:
         """Start (or stop) device-time accounting of the library's kernels on this handle."""
         _lib.check(self.lib, self.handle, self.lib.rad_profile_enable(self.handle, int(on)), "rad_profile_enable")
