@@ -61,6 +61,9 @@ typedef struct {
                                 steps where only one of lslwr / lsswr holds (module_RA_RRTM.F90:842-846 as
                                 cited at namgpu/physics/rrtm/rrtm_call.py:37); the other part's inputs and
                                 outputs may then be NULL */
+    int32_t lw_chunk;        /* mixed precision: columns per LW chunk of the two-kernel LW (gas optics through
+                                ~95 KB per column of scratch, then the sweeps); 0 = 32768; negative = the
+                                single-kernel LW (gas optics in shared memory, no scratch) */
 } RadConfig;
 
 /* Column inputs (device pointers, float32).  ncol columns, nlay layers, nlp1 = nlay + 1 levels. */
@@ -147,7 +150,8 @@ void rad_graph_destroy(RadGraph* g);
  * runtime query, no allocation); make that first call before any stream capture.  Every call on every
  * handle of the process shares the one array: calls whose work may overlap on the device (other streams,
  * other host threads) race on it, so issue them on one stream or one after another.  Profiling events are
- * not recorded by this entry.  Results equal rad_solve's. */
+ * not recorded by this entry.  The LW runs in its single-kernel form (no scratch), so results equal
+ * rad_solve's on a handle configured with lw_chunk < 0. */
 #define RAD_NOALLOC_MAX_COLS 65536
 int rad_solve_noalloc(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream);
 

@@ -34,6 +34,7 @@ __constant__ int c_sw_ns[15] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94
 #include "rad_sw.cuh"
 #include "rad_sw2.cuh"
 #include "rad_lw2.cuh"
+#include "rad_lw3.cuh"
 #include "rad_mcica.cuh"
 #include "rad_post.cuh"
 
@@ -55,6 +56,8 @@ struct RadHandle {
     int64_t mask_cap = 0;                          // columns x layers the mask scratch holds
     void* d_cub = nullptr;
     size_t cub_bytes = 0;
+    float* d_lw3 = nullptr;                        // two-kernel LW: gas optics and sweep inputs of one chunk
+    int64_t lw3_cap = 0;                           // columns d_lw3 holds
     std::string err;
     // kernel accounting
     int64_t launches = 0;
@@ -267,6 +270,13 @@ int mark(RadHandle* h, cudaStream_t st, size_t base, int i)
     return RAD_OK;
 }
 
+// Columns per chunk of the two-kernel LW (mixed precision), 0 when the single-kernel LW runs.
+int64_t lw3_chunk(const RadConfig& cfg)
+{
+    if (cfg.precision != RAD_PREC_MIXED || cfg.lw_chunk < 0) return 0;
+    return cfg.lw_chunk > 0 ? cfg.lw_chunk : 32768;
+}
+
 // Scratch for a launch of ntot columns: day list arrays, CUB temp, chunk minima, McICA words.
 int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
 {
@@ -278,6 +288,17 @@ int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
         h->cmin_cap = 0;
         RAD_CUDA(h, cudaMalloc((void**)&h->d_cmin, (size_t)ncmin * sizeof(int)));
         h->cmin_cap = ncmin;
+    }
+    const int64_t lwc = lw3_chunk(h->cfg);
+    if (lwc > 0 && (h->cfg.parts & RAD_PART_LW)) {
+        const int64_t need = std::min(lwc, ntot);
+        if (need > h->lw3_cap) {
+            if (h->d_lw3) cudaFree(h->d_lw3);
+            h->d_lw3 = nullptr;
+            h->lw3_cap = 0;
+            RAD_CUDA(h, cudaMalloc((void**)&h->d_lw3, (size_t)need * lw3_block_floats(h->cfg.nlay) * sizeof(float)));
+            h->lw3_cap = need;
+        }
     }
     if (h->cfg.route == RAD_ROUTE_MCICA && ntot * h->cfg.nlay > h->mask_cap) {
         if (h->d_lwm) cudaFree(h->d_lwm);
@@ -380,6 +401,25 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
         const R* base = sizeof(R) == 4 ? (const R*)h->d_lwf : (const R*)h->d_lwd;
         lut.ex = base; lut.tfn = base + 10001; lut.tau = base + 2 * 10001;
         const bool mc = cfg.route == RAD_ROUTE_MCICA;
+        const int64_t lwc = fixed ? 0 : lw3_chunk(cfg);
+        if (sizeof(R) == 4 && lwc > 0) {
+            // two kernels per chunk: gas optics into the scratch, then one warp per column sweeps
+            LwLut<float> fl;
+            fl.ex = h->d_lwf; fl.tfn = h->d_lwf + 10001; fl.tau = h->d_lwf + 2 * 10001;
+            const size_t smem1 = sizeof(LwSetup<float>);
+            RAD_CUDA(h, cudaFuncSetAttribute((void*)lw3_optics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
+            for (int64_t c0 = 0; c0 < ntot; c0 += lwc) {
+                const int64_t nc = std::min(lwc, ntot - c0);
+                lw3_optics_kernel<<<(unsigned)nc, LW_THREADS, smem1, st>>>(bt, c0, h->d_lw3, h->d_err);
+                const unsigned g2 = (unsigned)((nc + LW3_SWEEP_WARPS - 1) / LW3_SWEEP_WARPS);
+                if (mc)
+                    lw3_sweep_kernel<true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                else
+                    lw3_sweep_kernel<false><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                h->launches += 2;
+            }
+            RAD_CUDA(h, cudaGetLastError());
+        } else {
         const size_t smem = sizeof(LwShared<R>);
         RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_lw<R>(mc), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         if (sizeof(R) == 4 && mc)
@@ -390,6 +430,7 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
             lw_column_kernel<R><<<(unsigned)ntot, LW_THREADS, smem, st>>>(bt, lut, h->d_err);
         h->launches += 1;
         RAD_CUDA(h, cudaGetLastError());
+        }
     }
     if ((mrc = mark_if(1))) return mrc;
     if (!do_sw) {
@@ -469,6 +510,7 @@ void rad_config_default(RadConfig* cfg, int32_t nlay)
     cfg->sw_seed0 = 1;
     cfg->cpathfac = 1.5f;
     cfg->parts = RAD_PART_LW | RAD_PART_SW;
+    cfg->lw_chunk = 0;
 }
 
 int rad_create(const RadConfig* cfg, RadHandle** out)
@@ -605,8 +647,14 @@ int rad_load_tables(RadHandle* h, const void* blob, size_t nbytes)
 
 int64_t rad_workspace_bytes(const RadHandle* h, int64_t ncol)
 {
-    (void)h;
-    return (ncol + 1) * 6 * (int64_t)sizeof(int) + (1 << 20);
+    int64_t b = (ncol + 1) * 6 * (int64_t)sizeof(int) + (1 << 20);
+    if (h) {
+        const int64_t lwc = lw3_chunk(h->cfg);
+        if (lwc > 0 && (h->cfg.parts & RAD_PART_LW))
+            b += std::min(lwc, ncol) * lw3_block_floats(h->cfg.nlay) * (int64_t)sizeof(float);
+        if (h->cfg.route == RAD_ROUTE_MCICA) b += 9 * (int64_t)h->cfg.nlay * ncol * (int64_t)sizeof(uint32_t);
+    }
+    return b;
 }
 
 // Argument checks of one request.
@@ -869,7 +917,7 @@ void rad_destroy(RadHandle* h)
     for (void* p : {(void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
                     (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
                     (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub, (void*)h->d_lwm,
-                    (void*)h->d_swm})
+                    (void*)h->d_swm, (void*)h->d_lw3})
         if (p) cudaFree(p);
     delete h;
 }

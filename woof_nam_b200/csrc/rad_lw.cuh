@@ -20,7 +20,7 @@ constexpr int LW_THREADS = 160;     // 5 warps: lanes 0..139 carry g-points in t
 constexpr int LW_WARPS = LW_THREADS / 32;
 
 template <class R>
-struct LwShared {
+struct LwSetup {
     R pavel[NLAY_MAX], tavel[NLAY_MAX], coldry[NLAY_MAX], colbrd[NLAY_MAX], h2ovmr[NLAY_MAX], delp[NLAY_MAX];
     R fac00[NLAY_MAX], fac01[NLAY_MAX], fac10[NLAY_MAX], fac11[NLAY_MAX], selffac[NLAY_MAX], selffrac[NLAY_MAX];
     R forfac[NLAY_MAX], forfrac[NLAY_MAX], minorfrac[NLAY_MAX], scaleminor[NLAY_MAX], scaleminorn2[NLAY_MAX];
@@ -31,19 +31,24 @@ struct LwShared {
     R pklay[NLAY_MAX + 1][16], pklev[NLAY_MAX + 1][16];
     R taucld[16][NLAY_MAX], tauaer[16][NLAY_MAX];
     R cldfrc[NLAY_MAX + 2];
-    R taug[LW_NGPT][NLAY_MAX], fracs[LW_NGPT][NLAY_MAX];
     R facclr1u[NLAY_MAX + 2], facclr2u[NLAY_MAX + 2], faccld1u[NLAY_MAX + 2], faccld2u[NLAY_MAX + 2];
     R faccmb1u[NLAY_MAX + 2], faccmb2u[NLAY_MAX + 2];
     R facclr1d[NLAY_MAX + 2], facclr2d[NLAY_MAX + 2], faccld1d[NLAY_MAX + 2], faccld2d[NLAY_MAX + 2];
     R faccmb1d[NLAY_MAX + 2], faccmb2d[NLAY_MAX + 2];
     int lstu[NLAY_MAX + 2], lstd[NLAY_MAX + 2];
+    R secdiff[16], semiss[16];
+    R stemp, pwvcm;
+    int laytrop, lcf1;
+};
+
+// The single-kernel layout: set-up data plus the column's gas optics and the sweeps' partial sums.
+template <class R>
+struct LwShared : LwSetup<R> {
+    R taug[LW_NGPT][NLAY_MAX], fracs[LW_NGPT][NLAY_MAX];
     double fnet[LW_WARPS][NLAY_MAX + 1];      // per-warp partial of sum_g (up - down) per level
     double fnet2[LW_WARPS][NLAY_MAX + 1];     // second per-warp level partial (the downward sums of lw2)
     uint32_t mcw[5][NLAY_MAX];                // McICA route: the column's sub-column cloud words
     double scal[LW_WARPS][8];                 // per-warp partials: toa up, toa up clr, sfc up/dn, clr up/dn
-    R secdiff[16], semiss[16];
-    R stemp, pwvcm;
-    int laytrop, lcf1;
 };
 
 // ------------------------------------------------------------------------------------------------------
@@ -123,7 +128,7 @@ __device__ __forceinline__ R minor2d(const R* t, int nj, int ng, int j, R fj, in
 // Gas optical depth and Planck fraction of LW g-point g (0..139) at layer k0: the band kernels of the
 // reference restated per (g, layer).  Statement order follows each band's reference kernel.
 template <class R>
-__device__ void lw_gas(const LwShared<R>& s, int g, int k0, R& tg, R& fr)
+__device__ void lw_gas(const LwSetup<R>& s, int g, int k0, R& tg, R& fr)
 {
     const bool low = s.lower[k0];
     const int jpk = s.jp[k0], jtk = s.jt[k0], jt1k = s.jt1[k0];
@@ -520,8 +525,8 @@ struct LwIn {
 // Phases A and B of the LW column (everything before the sweeps), shared by the column kernels:
 // absorber amounts, cloud optics, setcoef, Planck functions, gas optics per (g, layer) and the
 // max-random overlap factors of rtrnmr, all in shared memory.  NT threads, tid = threadIdx.x.
-template <class R, int NT>
-__device__ void lw_setup(LwShared<R>& s, const LwIn& a, int64_t col, int tid)
+template <class R, int NT, class Sink>
+__device__ void lw_setup_core(LwSetup<R>& s, const LwIn& a, int64_t col, int tid, Sink sink)
 {
     const int nlay = a.nlay, nlp1 = nlay + 1;
     const int64_t N = a.ncol;
@@ -738,8 +743,7 @@ __device__ void lw_setup(LwShared<R>& s, const LwIn& a, int64_t col, int tid)
         lw_gas(s, g, k0, tg, fr);
         int band = 0;
         while (g >= c_lw_ns[band + 1]) ++band;
-        s.taug[g][k0] = tg + s.tauaer[band][k0];
-        s.fracs[g][k0] = fr;
+        sink(g, k0, tg + s.tauaer[band][k0], fr);
     });
     // ---- overlap factors of rtrnmr (serial recurrence in k), thread 32 while warp 0 waits
     if (tid == 32) {
@@ -813,6 +817,16 @@ __device__ void lw_setup(LwShared<R>& s, const LwIn& a, int64_t col, int tid)
         }
     }
     __syncthreads();
+}
+
+// lw_setup_core with the gas optics stored in the single-kernel shared layout.
+template <class R, int NT>
+__device__ __forceinline__ void lw_setup(LwShared<R>& s, const LwIn& a, int64_t col, int tid)
+{
+    lw_setup_core<R, NT>(s, a, col, tid, [&](int g, int k0, R tg, R fr) {
+        s.taug[g][k0] = tg;
+        s.fracs[g][k0] = fr;
+    });
 }
 
 using LwBatch = ReqBatch<LwIn>;
