@@ -64,14 +64,18 @@ __device__ __forceinline__ double warp_sum(double v)
 // Visit every (g-point, layer) pair of a column with the CTA's warps such that each warp works on one band
 // at a time: lane l of a task of band b takes g-point ns[b] + l % ng and layer k0 + l / ng (ng = the band's
 // g-point count, 32 / ng layers per task).  Neighbouring lanes then read neighbouring g entries of the
-// band's [..][g] k-tables (coalesced) and take the same band branch.  f(g, k0) runs once per pair.
+// band's [..][g] k-tables (coalesced) and take the same band branch.  Tasks are handed out in order from
+// the shared counter *next (zero before the first call of the CTA), so a warp that arrives late (after
+// other work) takes fewer tasks.  f(g, k0, b) runs once per pair.
 template <class F>
-__device__ __forceinline__ void for_each_band_pair(const int* ns, int nbands, int nlay, int warp, int nwarps, int lane,
-                                                   F f)
+__device__ __forceinline__ void for_each_band_pair(const int* ns, int nbands, int nlay, int* next, int lane, F f)
 {
     int b = 0, t0 = 0;   // band of the current task and the index of its first task
     int ng = ns[1] - ns[0], kpw = 32 / ng, nt = (nlay + kpw - 1) / kpw;
-    for (int t = warp;; t += nwarps) {
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(next, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
         while (b < nbands && t >= t0 + nt) {
             t0 += nt;
             ++b;
@@ -80,7 +84,7 @@ __device__ __forceinline__ void for_each_band_pair(const int* ns, int nbands, in
         if (b >= nbands) break;
         const int kk = lane / ng, jg = lane - kk * ng;
         const int k0 = (t - t0) * kpw + kk;
-        if (kk < kpw && k0 < nlay) f(ns[b] + jg, k0);
+        if (kk < kpw && k0 < nlay) f(ns[b] + jg, k0, b);
     }
 }
 

@@ -39,6 +39,7 @@ struct LwSetup {
     R secdiff[16], semiss[16];
     R stemp, pwvcm;
     int laytrop, lcf1;
+    int task_next;            // phase B task counter (for_each_band_pair)
 };
 
 // The single-kernel layout: set-up data plus the column's gas optics and the sweeps' partial sums.
@@ -128,7 +129,7 @@ __device__ __forceinline__ R minor2d(const R* t, int nj, int ng, int j, R fj, in
 // Gas optical depth and Planck fraction of LW g-point g (0..139) at layer k0: the band kernels of the
 // reference restated per (g, layer).  Statement order follows each band's reference kernel.
 template <class R>
-__device__ void lw_gas(const LwSetup<R>& s, int g, int k0, R& tg, R& fr)
+__device__ void lw_gas(const LwSetup<R>& s, int g, int k0, R& tg, R& fr, int band_of_g = -1)
 {
     const bool low = s.lower[k0];
     const int jpk = s.jp[k0], jtk = s.jt[k0], jt1k = s.jt1[k0];
@@ -144,8 +145,11 @@ __device__ void lw_gas(const LwSetup<R>& s, int g, int k0, R& tg, R& fr)
     };
     const int ind0l = (jpk - 1) * 5 + (jtk - 1) + 1, ind1l = jpk * 5 + (jt1k - 1) + 1;
     const int ind0u = (jpk - 13) * 5 + (jtk - 1) + 1, ind1u = (jpk - 12) * 5 + (jt1k - 1) + 1;
-    int band = 0;
-    while (g >= c_lw_ns[band + 1]) ++band;
+    int band = band_of_g;
+    if (band < 0) {
+        band = 0;
+        while (g >= c_lw_ns[band + 1]) ++band;
+    }
     const int ig = g - c_lw_ns[band];
     switch (band + 1) {
     case 1: {
@@ -521,6 +525,83 @@ struct LwIn {
     const uint32_t* mask;     // McICA route: sub-column cloud words [5][nlay][ncol] (null: NAM route)
 };
 
+// Maximum-random overlap factors of rtrnmr (phys_rrtm_lw_rtrnmr_body.cuh:51-172): a serial recurrence in k
+// over the layer cloud fractions, run by one thread.
+template <class R>
+__device__ void lw_overlap(LwSetup<R>& s, int nlay)
+{
+    const R eps = (R)1.0e-6f;
+    const int nlp1 = nlay + 1;
+    const R* cf = s.cldfrc;
+    for (int k = 0; k <= nlp1; ++k) {
+        s.faccld1u[k] = 0; s.faccld2u[k] = 0; s.facclr1u[k] = 0; s.facclr2u[k] = 0; s.faccmb1u[k] = 0; s.faccmb2u[k] = 0;
+        s.faccld1d[k] = 0; s.faccld2d[k] = 0; s.facclr1d[k] = 0; s.facclr2d[k] = 0; s.faccmb1d[k] = 0; s.faccmb2d[k] = 0;
+        s.lstu[k] = 0; s.lstd[k] = 0;
+    }
+    s.lstu[1] = cf[1] > eps ? 1 : 0;
+    R rat1 = 0, rat2 = 0;
+    for (int k = 1; k <= nlay - 1; ++k) {
+        s.lstu[k + 1] = (cf[k + 1] > eps && cf[k] <= eps) ? 1 : 0;
+        if (cf[k] > eps) {
+            if (cf[k + 1] >= cf[k]) {
+                if (s.lstu[k]) {
+                    if (cf[k] < (R)1) s.facclr2u[k + 1] = (cf[k + 1] - cf[k]) / ((R)1 - cf[k]);
+                    s.facclr2u[k] = 0; s.faccld2u[k] = 0;
+                } else {
+                    const R fmx = fmaxR(cf[k], cf[k - 1]);
+                    if (cf[k + 1] > fmx) { s.facclr1u[k + 1] = rat2; s.facclr2u[k + 1] = (cf[k + 1] - fmx) / ((R)1 - fmx); }
+                    else if (cf[k + 1] < fmx) s.facclr1u[k + 1] = (cf[k + 1] - cf[k]) / (cf[k - 1] - cf[k]);
+                    else s.facclr1u[k + 1] = rat2;
+                }
+                if (s.facclr1u[k + 1] > 0 || s.facclr2u[k + 1] > 0) { rat1 = 1; rat2 = 0; } else { rat1 = 0; rat2 = 0; }
+            } else {
+                if (s.lstu[k]) {
+                    s.faccld2u[k + 1] = (cf[k] - cf[k + 1]) / cf[k];
+                    s.facclr2u[k] = 0; s.faccld2u[k] = 0;
+                } else {
+                    const R fmn = fminR(cf[k], cf[k - 1]);
+                    if (cf[k + 1] <= fmn) { s.faccld1u[k + 1] = rat1; s.faccld2u[k + 1] = (fmn - cf[k + 1]) / fmn; }
+                    else s.faccld1u[k + 1] = (cf[k] - cf[k + 1]) / (cf[k] - fmn);
+                }
+                if (s.faccld1u[k + 1] > 0 || s.faccld2u[k + 1] > 0) { rat1 = 0; rat2 = 1; } else { rat1 = 0; rat2 = 0; }
+            }
+            s.faccmb1u[k + 1] = s.facclr1u[k + 1] * s.faccld2u[k] * cf[k - 1];
+            s.faccmb2u[k + 1] = s.faccld1u[k + 1] * s.facclr2u[k] * ((R)1 - cf[k - 1]);
+        }
+    }
+    s.lstd[nlay] = cf[nlay] > eps ? 1 : 0;
+    rat1 = 0; rat2 = 0;
+    for (int k = nlay; k >= 2; --k) {
+        s.lstd[k - 1] = (cf[k - 1] > eps && cf[k] <= eps) ? 1 : 0;
+        if (cf[k] > eps) {
+            if (cf[k - 1] >= cf[k]) {
+                if (s.lstd[k]) {
+                    if (cf[k] < (R)1) s.facclr2d[k - 1] = (cf[k - 1] - cf[k]) / ((R)1 - cf[k]);
+                    s.facclr2d[k] = 0; s.faccld2d[k] = 0;
+                } else {
+                    const R fmx = fmaxR(cf[k], cf[k + 1]);
+                    if (cf[k - 1] > fmx) { s.facclr1d[k - 1] = rat2; s.facclr2d[k - 1] = (cf[k - 1] - fmx) / ((R)1 - fmx); }
+                    else if (cf[k - 1] < fmx) s.facclr1d[k - 1] = (cf[k - 1] - cf[k]) / (cf[k + 1] - cf[k]);
+                    else s.facclr1d[k - 1] = rat2;
+                }
+                if (s.facclr1d[k - 1] > 0 || s.facclr2d[k - 1] > 0) { rat1 = 1; rat2 = 0; } else { rat1 = 0; rat2 = 0; }
+            } else {
+                if (s.lstd[k]) {
+                    s.faccld2d[k - 1] = (cf[k] - cf[k - 1]) / cf[k];
+                    s.facclr2d[k] = 0; s.faccld2d[k] = 0;
+                } else {
+                    const R fmn = fminR(cf[k], cf[k + 1]);
+                    if (cf[k - 1] <= fmn) { s.faccld1d[k - 1] = rat1; s.faccld2d[k - 1] = (fmn - cf[k - 1]) / fmn; }
+                    else s.faccld1d[k - 1] = (cf[k] - cf[k - 1]) / (cf[k] - fmn);
+                }
+                if (s.faccld1d[k - 1] > 0 || s.faccld2d[k - 1] > 0) { rat1 = 0; rat2 = 1; } else { rat1 = 0; rat2 = 0; }
+            }
+            s.faccmb1d[k - 1] = s.facclr1d[k - 1] * s.faccld2d[k] * cf[k + 1];
+            s.faccmb2d[k - 1] = s.faccld1d[k - 1] * s.facclr2d[k] * ((R)1 - cf[k + 1]);
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------------------------
 // Phases A and B of the LW column (everything before the sweeps), shared by the column kernels:
 // absorber amounts, cloud optics, setcoef, Planck functions, gas optics per (g, layer) and the
@@ -546,6 +627,7 @@ __device__ void lw_setup_core(LwSetup<R>& s, const LwIn& a, int64_t col, int tid
         s.pavel[k0] = IN(a.plyr, kin);
         s.tavel[k0] = IN(a.tlyr, kin);
         s.delp[k0] = dlp;
+        s.lower[k0] = rlog(s.pavel[k0]) > (R)4.56f;
         const R h2ovmr = fmaxR((R)0, qv * amdw / ((R)1 - qv));
         const R o3vmr = fmaxR((R)0, ov * amdo3);
         const R tem0 = ((R)1 - h2ovmr) * (R)28.9644 + h2ovmr * (R)18.0154;
@@ -596,12 +678,9 @@ __device__ void lw_setup_core(LwSetup<R>& s, const LwIn& a, int64_t col, int tid
         s.lcf1 = lcf;
         s.stemp = (R)__ldg(a.tsfg + col);
         int lt = 0;
-        for (int k0 = 0; k0 < nlay; ++k0) {
-            const bool lo = rlog(s.pavel[k0]) > (R)4.56f;
-            s.lower[k0] = lo;
-            lt += lo ? 1 : 0;
-        }
+        for (int k0 = 0; k0 < nlay; ++k0) lt += s.lower[k0] ? 1 : 0;
         s.laytrop = lt;
+        s.task_next = 0;
     }
     __syncthreads();
     // ---- phase A2: secdiff/semiss, cldprop, setcoef, Planck functions
@@ -737,85 +816,18 @@ __device__ void lw_setup_core(LwSetup<R>& s, const LwIn& a, int64_t col, int tid
         }
     }
     __syncthreads();
-    // ---- phase B: gas optics per (g, layer), band by band (one band per warp task, coalesced table reads)
-    for_each_band_pair(c_lw_ns, 16, nlay, tid >> 5, NT / 32, tid & 31, [&](int g, int k0) {
+    // ---- phase B: gas optics per (g, layer), band by band; the last warp first computes the overlap
+    // factors of rtrnmr (a serial recurrence in k, one lane) and then joins the task queue
+    const int warp = tid >> 5, lane = tid & 31;
+    if (warp == NT / 32 - 1) {
+        if (lane == 0) lw_overlap(s, nlay);
+        __syncwarp();
+    }
+    for_each_band_pair(c_lw_ns, 16, nlay, &s.task_next, lane, [&](int g, int k0, int band) {
         R tg, fr;
-        lw_gas(s, g, k0, tg, fr);
-        int band = 0;
-        while (g >= c_lw_ns[band + 1]) ++band;
+        lw_gas(s, g, k0, tg, fr, band);
         sink(g, k0, tg + s.tauaer[band][k0], fr);
     });
-    // ---- overlap factors of rtrnmr (serial recurrence in k), thread 32 while warp 0 waits
-    if (tid == 32) {
-        const R* cf = s.cldfrc;
-        for (int k = 0; k <= nlp1; ++k) {
-            s.faccld1u[k] = 0; s.faccld2u[k] = 0; s.facclr1u[k] = 0; s.facclr2u[k] = 0; s.faccmb1u[k] = 0; s.faccmb2u[k] = 0;
-            s.faccld1d[k] = 0; s.faccld2d[k] = 0; s.facclr1d[k] = 0; s.facclr2d[k] = 0; s.faccmb1d[k] = 0; s.faccmb2d[k] = 0;
-            s.lstu[k] = 0; s.lstd[k] = 0;
-        }
-        s.lstu[1] = cf[1] > eps ? 1 : 0;
-        R rat1 = 0, rat2 = 0;
-        for (int k = 1; k <= nlay - 1; ++k) {
-            s.lstu[k + 1] = (cf[k + 1] > eps && cf[k] <= eps) ? 1 : 0;
-            if (cf[k] > eps) {
-                if (cf[k + 1] >= cf[k]) {
-                    if (s.lstu[k]) {
-                        if (cf[k] < (R)1) s.facclr2u[k + 1] = (cf[k + 1] - cf[k]) / ((R)1 - cf[k]);
-                        s.facclr2u[k] = 0; s.faccld2u[k] = 0;
-                    } else {
-                        const R fmx = fmaxR(cf[k], cf[k - 1]);
-                        if (cf[k + 1] > fmx) { s.facclr1u[k + 1] = rat2; s.facclr2u[k + 1] = (cf[k + 1] - fmx) / ((R)1 - fmx); }
-                        else if (cf[k + 1] < fmx) s.facclr1u[k + 1] = (cf[k + 1] - cf[k]) / (cf[k - 1] - cf[k]);
-                        else s.facclr1u[k + 1] = rat2;
-                    }
-                    if (s.facclr1u[k + 1] > 0 || s.facclr2u[k + 1] > 0) { rat1 = 1; rat2 = 0; } else { rat1 = 0; rat2 = 0; }
-                } else {
-                    if (s.lstu[k]) {
-                        s.faccld2u[k + 1] = (cf[k] - cf[k + 1]) / cf[k];
-                        s.facclr2u[k] = 0; s.faccld2u[k] = 0;
-                    } else {
-                        const R fmn = fminR(cf[k], cf[k - 1]);
-                        if (cf[k + 1] <= fmn) { s.faccld1u[k + 1] = rat1; s.faccld2u[k + 1] = (fmn - cf[k + 1]) / fmn; }
-                        else s.faccld1u[k + 1] = (cf[k] - cf[k + 1]) / (cf[k] - fmn);
-                    }
-                    if (s.faccld1u[k + 1] > 0 || s.faccld2u[k + 1] > 0) { rat1 = 0; rat2 = 1; } else { rat1 = 0; rat2 = 0; }
-                }
-                s.faccmb1u[k + 1] = s.facclr1u[k + 1] * s.faccld2u[k] * cf[k - 1];
-                s.faccmb2u[k + 1] = s.faccld1u[k + 1] * s.facclr2u[k] * ((R)1 - cf[k - 1]);
-            }
-        }
-        s.lstd[nlay] = cf[nlay] > eps ? 1 : 0;
-        rat1 = 0; rat2 = 0;
-        for (int k = nlay; k >= 2; --k) {
-            s.lstd[k - 1] = (cf[k - 1] > eps && cf[k] <= eps) ? 1 : 0;
-            if (cf[k] > eps) {
-                if (cf[k - 1] >= cf[k]) {
-                    if (s.lstd[k]) {
-                        if (cf[k] < (R)1) s.facclr2d[k - 1] = (cf[k - 1] - cf[k]) / ((R)1 - cf[k]);
-                        s.facclr2d[k] = 0; s.faccld2d[k] = 0;
-                    } else {
-                        const R fmx = fmaxR(cf[k], cf[k + 1]);
-                        if (cf[k - 1] > fmx) { s.facclr1d[k - 1] = rat2; s.facclr2d[k - 1] = (cf[k - 1] - fmx) / ((R)1 - fmx); }
-                        else if (cf[k - 1] < fmx) s.facclr1d[k - 1] = (cf[k - 1] - cf[k]) / (cf[k + 1] - cf[k]);
-                        else s.facclr1d[k - 1] = rat2;
-                    }
-                    if (s.facclr1d[k - 1] > 0 || s.facclr2d[k - 1] > 0) { rat1 = 1; rat2 = 0; } else { rat1 = 0; rat2 = 0; }
-                } else {
-                    if (s.lstd[k]) {
-                        s.faccld2d[k - 1] = (cf[k] - cf[k - 1]) / cf[k];
-                        s.facclr2d[k] = 0; s.faccld2d[k] = 0;
-                    } else {
-                        const R fmn = fminR(cf[k], cf[k + 1]);
-                        if (cf[k - 1] <= fmn) { s.faccld1d[k - 1] = rat1; s.faccld2d[k - 1] = (fmn - cf[k - 1]) / fmn; }
-                        else s.faccld1d[k - 1] = (cf[k] - cf[k - 1]) / (cf[k] - fmn);
-                    }
-                    if (s.faccld1d[k - 1] > 0 || s.faccld2d[k - 1] > 0) { rat1 = 0; rat2 = 1; } else { rat1 = 0; rat2 = 0; }
-                }
-                s.faccmb1d[k - 1] = s.facclr1d[k - 1] * s.faccld2d[k] * cf[k + 1];
-                s.faccmb2d[k - 1] = s.faccld1d[k - 1] * s.facclr2d[k] * ((R)1 - cf[k + 1]);
-            }
-        }
-    }
     __syncthreads();
 }
 

@@ -69,7 +69,7 @@ __constant__ int c_sw_nspb[14] = {1, 5, 1, 1, 1, 5, 1, 0, 1, 0, 0, 1, 5, 1};
 // Gas and Rayleigh optical depths of SW g-point g (0..111) at layer k0 (phys_rrtm_sw_taumol16..29.cu with
 // the reference's handling of the layer k = laytrop).
 template <class R, class S>
-__device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr)
+__device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr, int band_of_g = -1)
 {
     const int k = k0 + 1, lt = s.laytrop;
     const int jpk = s.jp[k0], jtk = s.jt[k0], jt1k = s.jt1[k0];
@@ -80,8 +80,11 @@ __device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr)
     const int inds = s.indself[k0], indf = s.indfor[k0];
     const R sfac = s.selffac[k0], sfrac = s.selffrac[k0], ffac = s.forfac[k0], ffrac = s.forfrac[k0];
     const R oneminus = (R)1.0f - (R)1.0e-6f, swom = (R)0.999999f;
-    int b = 0;
-    while (g >= c_sw_ns[b + 1]) ++b;
+    int b = band_of_g;
+    if (b < 0) {
+        b = 0;
+        while (g >= c_sw_ns[b + 1]) ++b;
+    }
     const int ig = g - c_sw_ns[b], jb = b + 16;
     auto idx = [&](int jbb, int& id0, int& id1) {
         const int bb = jbb - 16;

@@ -358,6 +358,7 @@ struct SwSh2 {
     unsigned char low[NLAY_MAX];
     uint32_t mcw[4][NLAY_MAX];                 // McICA route: the column's sub-column cloud words
     int nexact;                                // layer evaluations queued for the float64 recompute
+    int task_next;                             // phase B task counter (for_each_band_pair)
     int qkey[SW2_QCAP];                        // thread | layer << 8 | cloud << 15
     float qval[SW2_QCAP][6];                   // their rb, rd, tb, td, e3, e4
 };
@@ -632,6 +633,7 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
         s.kmin8 = a.kmin8[d];
         s.kminw = a.kminw[d];
         s.nexact = 0;
+        s.task_next = 0;
     }
     if (a.mask)
         for (int i = tid; i < 4 * nlay; i += SW2_THREADS)
@@ -649,9 +651,9 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
     for (int g = tid; g < SW_NGPT; g += SW2_THREADS) s.raylc[g] = sw2_rayl_coef(g);
     __syncthreads();
     // ---- phase B: gas and Rayleigh optical depths per (g, layer), band by band
-    for_each_band_pair(c_sw_ns, 14, nlay, tid >> 5, SW2_WARPS, tid & 31, [&](int g, int k0) {
+    for_each_band_pair(c_sw_ns, 14, nlay, &s.task_next, tid & 31, [&](int g, int k0, int b) {
         float tg, tr;
-        sw_gas<float>(s, g, k0, tg, tr);
+        sw_gas<float>(s, g, k0, tg, tr, b);
         s.taug[g][k0] = tg;
         if (g >= 66 && g < 74 && k0 < s.laytrop) s.taur24[g - 66][k0] = tr;
     });
