@@ -32,7 +32,7 @@ UNIT = "columns/s"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC = ROOT / "profiles" / "traffic.json"
 B200_SMS, FP32_LANES_PER_SM = 148, 128
-CPU_SAMPLE = 8192
+CPU_SAMPLE = 16384
 
 
 def parse():
