@@ -274,8 +274,8 @@ def main():
     lw_ms, sw_ms = prof["lw_ms"] / max(prof["solves"], 1), prof["sw_ms"] / max(prof["solves"], 1)
     lw_tf = ops["lw_flops_per_col"] * n / (lw_ms * 1e-3) / 1e12
     sw_tf = ops["sw_flops_per_daycol"] * nday / (sw_ms * 1e-3) / 1e12
-    # the mixed precision runs the production kernels lw2_column_kernel / sw2_column_kernel
-    lw_name, sw_name = "lw2_column_kernel", "sw2_column_kernel"
+    # the mixed precision runs the two-kernel LW (gas optics, then sweeps, per chunk) and sw2_column_kernel
+    lw_name, sw_name = "lw3_optics_kernel+lw3_sweep_kernel", "sw2_column_kernel"
     dom = sw_name if sw_ms >= lw_ms else lw_name
     achieved = sw_tf if dom == sw_name else lw_tf
     traffic = None

@@ -128,8 +128,8 @@ __device__ __forceinline__ R minor2d(const R* t, int nj, int ng, int j, R fj, in
 // ------------------------------------------------------------------------------------------------------
 // Gas optical depth and Planck fraction of LW g-point g (0..139) at layer k0: the band kernels of the
 // reference restated per (g, layer).  Statement order follows each band's reference kernel.
-template <class R>
-__device__ void lw_gas(const LwSetup<R>& s, int g, int k0, R& tg, R& fr, int band_of_g = -1)
+template <class R, class S>
+__device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = -1)
 {
     const bool low = s.lower[k0];
     const int jpk = s.jp[k0], jtk = s.jt[k0], jt1k = s.jt1[k0];
@@ -525,6 +525,218 @@ struct LwIn {
     const uint32_t* mask;     // McICA route: sub-column cloud words [5][nlay][ncol] (null: NAM route)
 };
 
+// ------------------------------------------------------------------------------------------------------
+// Per-layer pieces of the LW set-up, written through the layer-array names of the target: the CTA's shared
+// layout, or one layer's float64 copy (Slot members) for the thin-layer recompute of the two-kernel LW.
+
+// Dry-air column (molecules / cm^2) and water vapour mixing ratio of layer k0 (phys_rrtm_lw_lwrad.cu:170-180).
+template <class R>
+__device__ __forceinline__ R lw_coldry(const LwIn& a, int64_t col, int k0, R& h2ovmr)
+{
+    const int nlay = a.nlay;
+    const int64_t N = a.ncol;
+    const int kin = nlay - 1 - k0;
+    auto IN = [&](const float* p, int lev) { return (R)__ldg(p + (size_t)lev * N + col); };
+    const R amdw = (R)28.9644 / (R)18.0154;
+    const R tem1g = (R)100.0 * (R)9.80665, tem2c = (R)1.0e-20 * (R)1.0e3 * (R)6.0221415e23;
+    const R dlp = IN(a.plvl, nlay - k0) - IN(a.plvl, nlay - k0 - 1);
+    const R qv = IN(a.qlyr, kin);
+    h2ovmr = fmaxR((R)0, qv * amdw / ((R)1 - qv));
+    const R tem0 = ((R)1 - h2ovmr) * (R)28.9644 + h2ovmr * (R)18.0154;
+    return tem2c * dlp / (tem1g * tem0 * ((R)1 + h2ovmr));
+}
+
+// lwrad_prep of layer k0 (internal order, surface first; phys_rrtm_lw_lwrad.cu:142-236), ivflip = 0.
+template <class R, class S>
+__device__ __forceinline__ void lw_prep_layer(S& s, const LwIn& a, int64_t col, int k0)
+{
+    const int nlay = a.nlay;
+    const int64_t N = a.ncol;
+    const int kin = nlay - 1 - k0;
+    auto IN = [&](const float* p, int lev) { return (R)__ldg(p + (size_t)lev * N + col); };
+    const R amdo3 = (R)28.9644 / (R)47.9982;
+    const R dlp = IN(a.plvl, nlay - k0) - IN(a.plvl, nlay - k0 - 1);
+    const R ov = IN(a.olyr, kin);
+    s.pavel[k0] = IN(a.plyr, kin);
+    s.tavel[k0] = IN(a.tlyr, kin);
+    s.delp[k0] = dlp;
+    s.lower[k0] = rlog(s.pavel[k0]) > (R)4.56f;
+    R h2ovmr;
+    const R cdry = lw_coldry<R>(a, col, k0, h2ovmr);
+    const R o3vmr = fmaxR((R)0, ov * amdo3);
+    const R temcol = (R)1.0e-12 * cdry;
+    s.coldry[k0] = cdry;
+    auto G = [&](int n) { return (R)__ldg(a.gasvmr + ((size_t)n * nlay + kin) * N + col); };
+    s.colamt[0][k0] = fmaxR((R)0, cdry * h2ovmr);
+    s.colamt[1][k0] = fmaxR(temcol, cdry * G(0));
+    s.colamt[2][k0] = fmaxR(temcol, cdry * o3vmr);
+    s.colamt[3][k0] = fmaxR(temcol, cdry * G(1));
+    s.colamt[4][k0] = fmaxR(temcol, cdry * G(2));
+    s.colamt[5][k0] = fmaxR((R)0, cdry * G(3));
+    s.colamt[6][k0] = fmaxR((R)0, cdry * G(4));
+    s.wx[0][k0] = fmaxR((R)0, cdry * G(8));
+    s.wx[1][k0] = fmaxR((R)0, cdry * G(5));
+    s.wx[2][k0] = fmaxR((R)0, cdry * G(6));
+    s.wx[3][k0] = fmaxR((R)0, cdry * G(7));
+    R summol = 0;
+    for (int m = 1; m < 7; ++m) summol = summol + s.colamt[m][k0];
+    s.colbrd[k0] = cdry - summol;
+    s.h2ovmr[k0] = s.colamt[0][k0] / fmaxR(cdry, (R)1e-30f);
+    for (int b = 0; b < 16; ++b) {
+        R tau = 0, ssa = 0;
+        if (a.faerlw) {
+            tau = (R)__ldg(a.faerlw + (((size_t)b) * nlay + kin) * N + col);
+            ssa = (R)__ldg(a.faerlw + (((size_t)(16 + b)) * nlay + kin) * N + col);
+        }
+        s.tauaer[b][k0] = tau * ((R)1 - ssa);
+    }
+}
+
+// cldprop of layer k0 (phys_rrtm_lw_cldprop.cu:116-232), ilwcice = 1, with the cloud-path factor.
+template <class R, class S>
+__device__ __forceinline__ void lw_cldprop_layer(S& s, const LwIn& a, int64_t col, int k0, int lcf1, int ilwcliq)
+{
+    const int nlay = a.nlay;
+    const int64_t N = a.ncol;
+    const int kin = nlay - 1 - k0;
+    auto CL = [&](int n) { return __ldg(a.clouds + ((size_t)n * nlay + kin) * N + col); };
+    R tc[16];
+    for (int b = 0; b < 16; ++b) tc[b] = 0;
+    const R cf = (R)CL(0);
+    if (lcf1 && cf > (R)0) {
+        if (ilwcliq > 0) {
+            const R tauran = (R)0.33e-3f * (R)CL(5);
+            const R tausnw = ((R)CL(7) > 0 && (R)CL(8) > (R)10) ? (R)1.5f * (R)1.05756f * (R)CL(7) / (R)CL(8) : (R)0;
+            const R cldliq = (R)(CL(1) * a.cpathfac), cldice = (R)(CL(3) * a.cpathfac), refliq = (R)CL(2);
+            R refice = (R)CL(4);
+            const R* absliq1 = tab<R>(T_LW_ABSLIQ1);
+            const R* absice1 = tab<R>(T_LW_ABSICE1);
+            const R* ipat = tab<R>(T_LW_IPAT);
+            int index = 1;
+            R fint = 0;
+            if (cldliq > 0) {
+                const R factor = refliq - (R)1.5f;
+                index = max(1, min(57, (int)factor));
+                fint = factor - (R)index;
+            }
+            if (cldice > 0) refice = fminR((R)130, fmaxR((R)13, refice));
+            for (int b = 0; b < 16; ++b) {
+                R tl = 0, ti = 0;
+                if (cldliq > 0) {
+                    const R a1 = ldt(absliq1 + b * 58 + index - 1), a2 = ldt(absliq1 + b * 58 + index);
+                    tl = fmaxR((R)0, cldliq * (a1 + fint * (a2 - a1)));
+                }
+                if (cldice > 0) {
+                    const int ia0 = (int)ldt(ipat + b) - 1;
+                    ti = fmaxR((R)0, cldice * (ldt(absice1 + ia0 * 2) + ldt(absice1 + ia0 * 2 + 1) / refice));
+                }
+                tc[b] = ti + tl + tauran + tausnw;
+            }
+        } else {
+            for (int b = 0; b < 16; ++b) tc[b] = (R)CL(1);
+        }
+    }
+    for (int b = 0; b < 16; ++b) s.taucld[b][k0] = tc[b];
+}
+
+// setcoef of layer k0 (phys_rrtm_lw_setcoef.cu:131-240).
+template <class R, class S>
+__device__ __forceinline__ void lw_setcoef_layer(S& s, int k0)
+{
+    const R pav = s.pavel[k0], tav = s.tavel[k0];
+    const R* preflog = tab<R>(T_LW_PREFLOG);
+    const R* tref = tab<R>(T_LW_TREF);
+    const R* chi = tab<R>(T_LW_CHI_MLS);
+    auto CHI = [&](int g, int lev) { return ldt(chi + (size_t)(lev - 1) * 7 + (g - 1)); };
+    const R plog = rlog(pav);
+    const int jpk = max(1, min(58, (int)((R)36 - (R)5 * (plog + (R)0.04f))));
+    const int jp1 = jpk + 1;
+    const R fp = fmaxR((R)0, fminR((R)1, (R)5 * (ldt(preflog + jpk - 1) - plog)));
+    const R tem1t = (tav - ldt(tref + jpk - 1)) / (R)15;
+    const R tem2t = (tav - ldt(tref + jp1 - 1)) / (R)15;
+    const int jtk = max(1, min(4, (int)((R)3 + tem1t)));
+    const int jt1k = max(1, min(4, (int)((R)3 + tem2t)));
+    const R ft = fmaxR((R)-0.5f, fminR((R)1.5f, tem1t - (R)(jtk - 3)));
+    const R ft1 = fmaxR((R)-0.5f, fminR((R)1.5f, tem2t - (R)(jt1k - 3)));
+    s.jp[k0] = jpk; s.jt[k0] = jtk; s.jt1[k0] = jt1k;
+    const R tem1 = (R)1 - fp;
+    s.fac10[k0] = tem1 * ft;
+    s.fac00[k0] = tem1 * ((R)1 - ft);
+    s.fac11[k0] = fp * ft1;
+    s.fac01[k0] = fp * ((R)1 - ft1);
+    const R h2o = s.h2ovmr[k0];
+    const R forf = pav * ((R)296.0f / (R)1013.0f) / (tav * ((R)1 + h2o));
+    const R selff = h2o * forf;
+    s.scaleminor[k0] = pav / tav;
+    s.scaleminorn2[k0] = (pav / tav) * (s.colbrd[k0] / (s.coldry[k0] + s.colamt[0][k0]));
+    const R tem1m = (tav - (R)180.8f) / (R)7.2f;
+    const int indmin = min(18, max(1, (int)tem1m));
+    s.indminor[k0] = indmin;
+    s.minorfrac[k0] = tem1m - (R)indmin;
+    for (int side = 0; side < 2; ++side)
+        for (int r = 0; r < 6; ++r) s.rfrate[side][r][k0] = 0;
+    if (s.lower[k0]) {
+        const R tem1f = ((R)332 - tav) / (R)36;
+        const int indf = min(2, max(1, (int)tem1f));
+        s.indfor[k0] = indf;
+        s.forfrac[k0] = tem1f - (R)indf;
+        const R tem1s = (tav - (R)188) / (R)7.2f;
+        const int inds = min(9, max(1, (int)tem1s - 7));
+        s.indself[k0] = inds;
+        s.selffrac[k0] = tem1s - (R)(inds + 7);
+        const int gas[5] = {2, 3, 4, 6, 2};
+        for (int r = 0; r < 5; ++r) {
+            const int num = r == 4 ? 4 : 1;
+            s.rfrate[0][r][k0] = CHI(num, jpk) / CHI(gas[r], jpk);
+            s.rfrate[1][r][k0] = CHI(num, jp1) / CHI(gas[r], jp1);
+        }
+    } else {
+        const R tem1f = (tav - (R)188) / (R)36;
+        s.indfor[k0] = 3;
+        s.forfrac[k0] = tem1f - (R)1;
+        s.indself[k0] = 0;
+        s.selffrac[k0] = 0;
+        s.rfrate[0][0][k0] = CHI(1, jpk) / CHI(2, jpk);
+        s.rfrate[1][0][k0] = CHI(1, jp1) / CHI(2, jp1);
+        s.rfrate[0][5][k0] = CHI(3, jpk) / CHI(2, jpk);
+        s.rfrate[1][5][k0] = CHI(3, jp1) / CHI(2, jp1);
+    }
+    s.selffac[k0] = s.colamt[0][k0] * selff;
+    s.forfac[k0] = s.colamt[0][k0] * forf;
+}
+
+// Planck functions of band i at level / layer k (k = 0: the surface; phys_rrtm_lw_setcoef.cu:135-160).
+template <class R>
+__device__ __forceinline__ void lw_planck(const LwIn& a, int64_t col, int k, int i, R& lay, R& lev)
+{
+    const int nlay = a.nlay;
+    const int64_t N = a.ncol;
+    auto IN = [&](const float* p, int l) { return (R)__ldg(p + (size_t)l * N + col); };
+    const R* totplnk = tab<R>(T_LW_TOTPLNK);
+    const R* delwave = tab<R>(T_LW_DELWAVE);
+    const R tl = k == 0 ? (R)__ldg(a.tsfg + col) : IN(a.tlyr, nlay - k);   // layer temp (k=0: stemp)
+    const R tv = k == 0 ? IN(a.tlvl, nlay) : IN(a.tlvl, nlay - k);
+    auto TOT = [&](int kk) { return ldt(totplnk + (size_t)i * 181 + (kk - 1)); };
+    const int indlay = min(180, max(1, (int)(tl - (R)159)));
+    const int indlev = min(180, max(1, (int)(tv - (R)159)));
+    const R tlyrfr = tl - (R)((int)tl), tlvlfr = tv - (R)((int)tv);
+    const R dw = ldt(delwave + i);
+    lay = dw * (TOT(indlay) + tlyrfr * (TOT(indlay + 1) - TOT(indlay)));
+    lev = dw * (TOT(indlev) + tlvlfr * (TOT(indlev + 1) - TOT(indlev)));
+}
+
+// Diffusivity secant of band b from the column precipitable water (phys_rrtm_lw_lwrad.cu:262-270).
+template <class R>
+__device__ __forceinline__ R lw_secdiff(int b, R pwvcm)
+{
+    const float A0[16] = {1.66f, 1.55f, 1.58f, 1.66f, 1.54f, 1.454f, 1.89f, 1.33f, 1.668f, 1.66f, 1.66f, 1.66f, 1.66f, 1.66f, 1.66f, 1.66f};
+    const float A1[16] = {0.00f, 0.25f, 0.22f, 0.00f, 0.13f, 0.446f, -0.10f, 0.40f, -0.006f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f};
+    const float A2[16] = {0.00f, -12.0f, -11.7f, 0.00f, -0.72f, -0.243f, 0.19f, -0.062f, 0.414f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f};
+    const int j1 = b + 1;
+    return (j1 == 1 || j1 == 4 || j1 == 10) ? (R)1.66f
+                                             : fminR((R)1.80f, fmaxR((R)1.50f, (R)A0[b] + (R)A1[b] * rexp((R)A2[b] * pwvcm)));
+}
+
 // Maximum-random overlap factors of rtrnmr (phys_rrtm_lw_rtrnmr_body.cuh:51-172): a serial recurrence in k
 // over the layer cloud fractions, run by one thread.
 template <class R>
@@ -619,45 +831,8 @@ __device__ void lw_setup_core(LwSetup<R>& s, const LwIn& a, int64_t col, int tid
     if (tid == 0) s.tz[0] = IN(a.tlvl, nlay);
     for (int k0 = tid; k0 < nlay; k0 += NT) {
         const int kin = nlay - 1 - k0;
-        const R amdw = (R)28.9644 / (R)18.0154, amdo3 = (R)28.9644 / (R)47.9982;
-        const R tem1g = (R)100.0 * (R)9.80665, tem2c = (R)1.0e-20 * (R)1.0e3 * (R)6.0221415e23;
-        const R dlp = IN(a.plvl, nlay - k0) - IN(a.plvl, nlay - k0 - 1);
         s.tz[k0 + 1] = IN(a.tlvl, nlay - k0 - 1);
-        const R qv = IN(a.qlyr, kin), ov = IN(a.olyr, kin);
-        s.pavel[k0] = IN(a.plyr, kin);
-        s.tavel[k0] = IN(a.tlyr, kin);
-        s.delp[k0] = dlp;
-        s.lower[k0] = rlog(s.pavel[k0]) > (R)4.56f;
-        const R h2ovmr = fmaxR((R)0, qv * amdw / ((R)1 - qv));
-        const R o3vmr = fmaxR((R)0, ov * amdo3);
-        const R tem0 = ((R)1 - h2ovmr) * (R)28.9644 + h2ovmr * (R)18.0154;
-        const R cdry = tem2c * dlp / (tem1g * tem0 * ((R)1 + h2ovmr));
-        const R temcol = (R)1.0e-12 * cdry;
-        s.coldry[k0] = cdry;
-        auto G = [&](int n) { return (R)__ldg(a.gasvmr + ((size_t)n * nlay + kin) * N + col); };
-        s.colamt[0][k0] = fmaxR((R)0, cdry * h2ovmr);
-        s.colamt[1][k0] = fmaxR(temcol, cdry * G(0));
-        s.colamt[2][k0] = fmaxR(temcol, cdry * o3vmr);
-        s.colamt[3][k0] = fmaxR(temcol, cdry * G(1));
-        s.colamt[4][k0] = fmaxR(temcol, cdry * G(2));
-        s.colamt[5][k0] = fmaxR((R)0, cdry * G(3));
-        s.colamt[6][k0] = fmaxR((R)0, cdry * G(4));
-        s.wx[0][k0] = fmaxR((R)0, cdry * G(8));
-        s.wx[1][k0] = fmaxR((R)0, cdry * G(5));
-        s.wx[2][k0] = fmaxR((R)0, cdry * G(6));
-        s.wx[3][k0] = fmaxR((R)0, cdry * G(7));
-        R summol = 0;
-        for (int m = 1; m < 7; ++m) summol = summol + s.colamt[m][k0];
-        s.colbrd[k0] = cdry - summol;
-        s.h2ovmr[k0] = s.colamt[0][k0] / fmaxR(cdry, (R)1e-30f);
-        for (int b = 0; b < 16; ++b) {
-            R tau = 0, ssa = 0;
-            if (a.faerlw) {
-                tau = (R)__ldg(a.faerlw + (((size_t)b) * nlay + kin) * N + col);
-                ssa = (R)__ldg(a.faerlw + (((size_t)(16 + b)) * nlay + kin) * N + col);
-            }
-            s.tauaer[b][k0] = tau * ((R)1 - ssa);
-        }
+        lw_prep_layer<R>(s, a, col, k0);
         s.cldfrc[k0 + 1] = IN(a.clouds, kin);
     }
     __syncthreads();
@@ -685,134 +860,19 @@ __device__ void lw_setup_core(LwSetup<R>& s, const LwIn& a, int64_t col, int tid
     __syncthreads();
     // ---- phase A2: secdiff/semiss, cldprop, setcoef, Planck functions
     if (tid < 16) {
-        const float A0[16] = {1.66f, 1.55f, 1.58f, 1.66f, 1.54f, 1.454f, 1.89f, 1.33f, 1.668f, 1.66f, 1.66f, 1.66f, 1.66f, 1.66f, 1.66f, 1.66f};
-        const float A1[16] = {0.00f, 0.25f, 0.22f, 0.00f, 0.13f, 0.446f, -0.10f, 0.40f, -0.006f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f};
-        const float A2[16] = {0.00f, -12.0f, -11.7f, 0.00f, -0.72f, -0.243f, 0.19f, -0.062f, 0.414f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f, 0.00f};
-        const int j1 = tid + 1;
-        s.secdiff[tid] = (j1 == 1 || j1 == 4 || j1 == 10)
-                             ? (R)1.66f
-                             : fminR((R)1.80f, fmaxR((R)1.50f, (R)A0[tid] + (R)A1[tid] * rexp((R)A2[tid] * s.pwvcm)));
+        s.secdiff[tid] = lw_secdiff<R>(tid, s.pwvcm);
         const R sfe = (R)__ldg(a.sfcemis + col);
         s.semiss[tid] = (sfe > eps && sfe <= (R)1) ? sfe : (R)1;
     }
     for (int k0 = tid; k0 < nlay; k0 += NT) {
-        // cldprop (phys_rrtm_lw_cldprop.cu:116-232), ilwcice = 1, with the cloud-path factor
-        const int kin = nlay - 1 - k0;
-        auto CL = [&](int n) { return __ldg(a.clouds + ((size_t)n * nlay + kin) * N + col); };
-        R tc[16];
-        for (int b = 0; b < 16; ++b) tc[b] = 0;
-        const R cf = (R)CL(0);
-        if (s.lcf1 && cf > (R)0) {
-            if (ilwcliq > 0) {
-                const R tauran = (R)0.33e-3f * (R)CL(5);
-                const R tausnw = ((R)CL(7) > 0 && (R)CL(8) > (R)10) ? (R)1.5f * (R)1.05756f * (R)CL(7) / (R)CL(8) : (R)0;
-                const R cldliq = (R)(CL(1) * a.cpathfac), cldice = (R)(CL(3) * a.cpathfac), refliq = (R)CL(2);
-                R refice = (R)CL(4);
-                const R* absliq1 = tab<R>(T_LW_ABSLIQ1);
-                const R* absice1 = tab<R>(T_LW_ABSICE1);
-                const R* ipat = tab<R>(T_LW_IPAT);
-                int index = 1;
-                R fint = 0;
-                if (cldliq > 0) {
-                    const R factor = refliq - (R)1.5f;
-                    index = max(1, min(57, (int)factor));
-                    fint = factor - (R)index;
-                }
-                if (cldice > 0) refice = fminR((R)130, fmaxR((R)13, refice));
-                for (int b = 0; b < 16; ++b) {
-                    R tl = 0, ti = 0;
-                    if (cldliq > 0) {
-                        const R a1 = ldt(absliq1 + b * 58 + index - 1), a2 = ldt(absliq1 + b * 58 + index);
-                        tl = fmaxR((R)0, cldliq * (a1 + fint * (a2 - a1)));
-                    }
-                    if (cldice > 0) {
-                        const int ia0 = (int)ldt(ipat + b) - 1;
-                        ti = fmaxR((R)0, cldice * (ldt(absice1 + ia0 * 2) + ldt(absice1 + ia0 * 2 + 1) / refice));
-                    }
-                    tc[b] = ti + tl + tauran + tausnw;
-                }
-            } else {
-                for (int b = 0; b < 16; ++b) tc[b] = (R)CL(1);
-            }
-        }
-        for (int b = 0; b < 16; ++b) s.taucld[b][k0] = tc[b];
-        // setcoef per layer (phys_rrtm_lw_setcoef.cu:131-240)
-        const R pav = s.pavel[k0], tav = s.tavel[k0];
-        const R* preflog = tab<R>(T_LW_PREFLOG);
-        const R* tref = tab<R>(T_LW_TREF);
-        const R* chi = tab<R>(T_LW_CHI_MLS);
-        auto CHI = [&](int g, int lev) { return ldt(chi + (size_t)(lev - 1) * 7 + (g - 1)); };
-        const R plog = rlog(pav);
-        const int jpk = max(1, min(58, (int)((R)36 - (R)5 * (plog + (R)0.04f))));
-        const int jp1 = jpk + 1;
-        const R fp = fmaxR((R)0, fminR((R)1, (R)5 * (ldt(preflog + jpk - 1) - plog)));
-        const R tem1t = (tav - ldt(tref + jpk - 1)) / (R)15;
-        const R tem2t = (tav - ldt(tref + jp1 - 1)) / (R)15;
-        const int jtk = max(1, min(4, (int)((R)3 + tem1t)));
-        const int jt1k = max(1, min(4, (int)((R)3 + tem2t)));
-        const R ft = fmaxR((R)-0.5f, fminR((R)1.5f, tem1t - (R)(jtk - 3)));
-        const R ft1 = fmaxR((R)-0.5f, fminR((R)1.5f, tem2t - (R)(jt1k - 3)));
-        s.jp[k0] = jpk; s.jt[k0] = jtk; s.jt1[k0] = jt1k;
-        const R tem1 = (R)1 - fp;
-        s.fac10[k0] = tem1 * ft;
-        s.fac00[k0] = tem1 * ((R)1 - ft);
-        s.fac11[k0] = fp * ft1;
-        s.fac01[k0] = fp * ((R)1 - ft1);
-        const R h2o = s.h2ovmr[k0];
-        const R forf = pav * ((R)296.0f / (R)1013.0f) / (tav * ((R)1 + h2o));
-        const R selff = h2o * forf;
-        s.scaleminor[k0] = pav / tav;
-        s.scaleminorn2[k0] = (pav / tav) * (s.colbrd[k0] / (s.coldry[k0] + s.colamt[0][k0]));
-        const R tem1m = (tav - (R)180.8f) / (R)7.2f;
-        const int indmin = min(18, max(1, (int)tem1m));
-        s.indminor[k0] = indmin;
-        s.minorfrac[k0] = tem1m - (R)indmin;
-        for (int side = 0; side < 2; ++side)
-            for (int r = 0; r < 6; ++r) s.rfrate[side][r][k0] = 0;
-        if (s.lower[k0]) {
-            const R tem1f = ((R)332 - tav) / (R)36;
-            const int indf = min(2, max(1, (int)tem1f));
-            s.indfor[k0] = indf;
-            s.forfrac[k0] = tem1f - (R)indf;
-            const R tem1s = (tav - (R)188) / (R)7.2f;
-            const int inds = min(9, max(1, (int)tem1s - 7));
-            s.indself[k0] = inds;
-            s.selffrac[k0] = tem1s - (R)(inds + 7);
-            const int gas[5] = {2, 3, 4, 6, 2};
-            for (int r = 0; r < 5; ++r) {
-                const int num = r == 4 ? 4 : 1;
-                s.rfrate[0][r][k0] = CHI(num, jpk) / CHI(gas[r], jpk);
-                s.rfrate[1][r][k0] = CHI(num, jp1) / CHI(gas[r], jp1);
-            }
-        } else {
-            const R tem1f = (tav - (R)188) / (R)36;
-            s.indfor[k0] = 3;
-            s.forfrac[k0] = tem1f - (R)1;
-            s.indself[k0] = 0;
-            s.selffrac[k0] = 0;
-            s.rfrate[0][0][k0] = CHI(1, jpk) / CHI(2, jpk);
-            s.rfrate[1][0][k0] = CHI(1, jp1) / CHI(2, jp1);
-            s.rfrate[0][5][k0] = CHI(3, jpk) / CHI(2, jpk);
-            s.rfrate[1][5][k0] = CHI(3, jp1) / CHI(2, jp1);
-        }
-        s.selffac[k0] = s.colamt[0][k0] * selff;
-        s.forfac[k0] = s.colamt[0][k0] * forf;
+        lw_cldprop_layer<R>(s, a, col, k0, s.lcf1, ilwcliq);
+        lw_setcoef_layer<R>(s, k0);
     }
     // Planck functions at levels 0..nlay and bands (setcoef.cu:135-160)
     {
-        const R* totplnk = tab<R>(T_LW_TOTPLNK);
-        const R* delwave = tab<R>(T_LW_DELWAVE);
         for (int p = tid; p < nlp1 * 16; p += NT) {
             const int k = p / 16, i = p % 16;
-            const R tl = k == 0 ? (R)__ldg(a.tsfg + col) : IN(a.tlyr, nlay - k);   // layer temp (k=0: stemp)
-            const R tv = k == 0 ? IN(a.tlvl, nlay) : IN(a.tlvl, nlay - k);
-            auto TOT = [&](int kk) { return ldt(totplnk + (size_t)i * 181 + (kk - 1)); };
-            const int indlay = min(180, max(1, (int)(tl - (R)159)));
-            const int indlev = min(180, max(1, (int)(tv - (R)159)));
-            const R tlyrfr = tl - (R)((int)tl), tlvlfr = tv - (R)((int)tv);
-            const R dw = ldt(delwave + i);
-            s.pklay[k][i] = dw * (TOT(indlay) + tlyrfr * (TOT(indlay + 1) - TOT(indlay)));
-            s.pklev[k][i] = dw * (TOT(indlev) + tlvlfr * (TOT(indlev + 1) - TOT(indlev)));
+            lw_planck<R>(a, col, k, i, s.pklay[k][i], s.pklev[k][i]);
         }
     }
     __syncthreads();

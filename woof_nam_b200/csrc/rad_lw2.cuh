@@ -20,6 +20,8 @@ constexpr int LW2_LANES = 28;   // g-points per warp
 template <class R>
 struct LwTerms {
     R trng, gassrcd, gassrcu, trnt, totsrcd, totsrcu;
+    R atrg;        // gas absorptance 1 - trng as computed (directly from the depth for thin layers)
+    R atrt;        // cloudy: total absorptance 1 - trnt, likewise
 };
 
 template <class R>
@@ -45,7 +47,8 @@ __device__ __forceinline__ LwTerms<R> lw2_terms(const LwShared<R>& s, const LwLu
     const R dplnkd = s.pklev[k - 1][band] - blay;
     t.gassrcd = plfrac * (blay + dplnkd * gasfac) * atrgas;
     t.gassrcu = plfrac * (blay + dplnku * gasfac) * atrgas;
-    t.trnt = 1; t.totsrcd = 0; t.totsrcu = 0;
+    t.atrg = atrgas;
+    t.trnt = 1; t.totsrcd = 0; t.totsrcu = 0; t.atrt = 0;
     if (cloudy) {
         const R odtot = odepth + sdif * s.taucld[band][k - 1];
         R totfac, atrtot;
@@ -58,6 +61,7 @@ __device__ __forceinline__ LwTerms<R> lw2_terms(const LwShared<R>& s, const LwLu
         }
         t.totsrcd = plfrac * (blay + dplnkd * totfac) * atrtot;
         t.totsrcu = plfrac * (blay + dplnku * totfac) * atrtot;
+        t.atrt = atrtot;
     }
     return t;
 }

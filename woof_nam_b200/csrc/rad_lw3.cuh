@@ -1,4 +1,4 @@
-// rad_lw3.cuh -- the LW column solve as two kernels over chunks of columns (mixed precision, sm_100a).
+// rad_lw3.cuh -- the LW column solve as kernels over chunks of columns (mixed precision, sm_100a).
 //
 // The single-kernel LW (rad_lw2.cuh) holds a column's gas optics (taug, fracs: 140 g x 61 layers x 2 floats,
 // 68 KB) in shared memory, so two CTAs fit an SM and the latency-bound table gathers and sweep recurrences
@@ -8,16 +8,24 @@
 //                      cldprop, setcoef, Planck functions, taugb01..16, the max-random overlap factors of
 //                      rtrnmr), with taug / fracs written straight to the chunk's scratch and the sweep inputs
 //                      copied after them.  Shared memory is the set-up data only (~32 KB).
-//   lw3_sweep_kernel   one warp per column: lane l carries g-points l, l + 32, ..., l + 128 (five
-//                      independent recurrences interleaved per lane), reading each layer's optical depths as
-//                      coalesced 128-byte rows; per level the lane sums its g-points in float64 and one warp
-//                      reduction gives the column's radiance sum.
+//   lw3_thin_kernel    one CTA per column, for layers thinner than LW3_THIN hPa only (most columns have none
+//                      and exit at once): that layer's absorber amounts, setcoef, cloud optics, Planck values
+//                      and gas optics again in float64, with the column's precipitable water and diffusivity
+//                      secants in float64.  A float optical depth puts some g-points of such a layer on the
+//                      neighbouring entry of the 10,001-entry transmittance table; in a 0.1 hPa cloudy layer
+//                      cooling at thousands of K/day that alone is ~1e-5 of the heating rate.
+//   lw3_sweep_kernel   one warp per column: lane l carries g-points l, l + 32, ..., l + 128 (five independent
+//                      recurrences interleaved per lane), reading each layer's optical depths as coalesced
+//                      128-byte rows.  Per layer each g-point's radiance CHANGE across the layer is formed
+//                      directly (source minus radiance x absorptance) and summed over g-points in float64; the
+//                      heating rates come from those changes, not from differences of ~300 W/m^2 level
+//                      fluxes.  Thin layers take this step in float64 from the float64 optics.
 //
 // Scratch block of one column (floats, 128-byte aligned): taug [nlay][160], fracs [nlay][160] (g-points
 // 140..159 unused), then one 80-word record per layer k = 1..nlay holding everything the sweeps read at that
-// layer (so a layer step touches one contiguous record), and a head record (k = 0) for the surface.  The
-// arithmetic of every term and recurrence is that of rad_lw2.cuh (rtrnmr, phys_rrtm_lw_rtrnmr_body.cuh:
-// 130-330; rtrnmc, phys_rrtm_lw_rtrnmc.cu:85-310); only the order of the float64 level sums differs.
+// layer (so a layer step touches one contiguous record) and a head record (k = 0) for the surface, then the
+// float64 thin-layer area.  The arithmetic of every term and recurrence is that of rad_lw2.cuh (rtrnmr,
+// phys_rrtm_lw_rtrnmr_body.cuh:130-330; rtrnmc, phys_rrtm_lw_rtrnmc.cu:85-310).
 #pragma once
 #include "rad_lw2.cuh"
 
@@ -37,14 +45,37 @@ constexpr int R_LSTU = 65;      // int lstu[k]
 constexpr int R_LSTD = 66;      // int lstd[k]
 constexpr int R_FACD = 67;      // [6] downward factors at k - 1: clr1 cld1 cmb1 cmb2 clr2 cld2
 constexpr int R_FACU = 73;      // [6] upward factors at k + 1, same order
+constexpr int R_THIN = 79;      // int: slot of the layer in the float64 thin-layer area, or -1
 // head record (k = 0)
 constexpr int H_PKLAY0 = 0;     // [16] pklay[0] (surface)
 constexpr int H_SECDIFF = 16;   // [16]
 constexpr int H_SEMISS = 32;    // [16]
+constexpr int H_NTHIN = 48;     // int: number of thin layers (the thin kernel's first read)
 
+// float64 thin-layer area: secdiff [16], then LW3_NTHIN slots of LW3_TSLOT doubles
+constexpr float LW3_THIN = 1.0f;   // hPa: layers thinner than this get the float64 step
+constexpr int LW3_NTHIN = 2;       // at most this many per column (the top-most ones)
+constexpr int LW3_TSLOT = 352;
+constexpr int T_TAUG = 1, T_FRACS = 141, T_PKLAY = 281, T_PKUP = 297, T_PKDN = 313, T_TAUCLD = 329;
+constexpr int LW3_THIN_FLOATS = 2 * (16 + LW3_NTHIN * LW3_TSLOT);
+
+__host__ __device__ constexpr int64_t lw3_rec_floats(int nlay) { return ((((int64_t)nlay + 1) * LW3_REC + 31) / 32) * 32; }
 __host__ __device__ constexpr int64_t lw3_block_floats(int nlay)
 {
-    return (int64_t)2 * nlay * LW3_GSTRIDE + ((((int64_t)nlay + 1) * LW3_REC + 31) / 32) * 32;
+    return (int64_t)2 * nlay * LW3_GSTRIDE + lw3_rec_floats(nlay) + LW3_THIN_FLOATS;
+}
+
+// The thin layers of a column (float layer thicknesses, top first); the optics and thin kernels agree on it.
+__device__ __forceinline__ int lw3_thin_layers(const LwIn& a, int64_t col, int* k0s)
+{
+    const int nlay = a.nlay;
+    const int64_t N = a.ncol;
+    int n = 0;
+    for (int k0 = nlay - 1; k0 >= 0 && n < LW3_NTHIN; --k0) {
+        const float dlp = __ldg(a.plvl + (size_t)(nlay - k0) * N + col) - __ldg(a.plvl + (size_t)(nlay - k0 - 1) * N + col);
+        if (dlp < LW3_THIN) k0s[n++] = k0;
+    }
+    return n;
 }
 
 __global__ void __launch_bounds__(LW_THREADS, 3) lw3_optics_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
@@ -70,6 +101,9 @@ __global__ void __launch_bounds__(LW_THREADS, 3) lw3_optics_kernel(const __grid_
         fro[k0 * LW3_GSTRIDE + g] = fr;
     });
     float* aux = blk + (size_t)2 * nlay * LW3_GSTRIDE;
+    int thin[LW3_NTHIN], nthin = 0;                  // lw3_thin_layers, from the same float thicknesses
+    for (int k0 = nlay - 1; k0 >= 0 && nthin < LW3_NTHIN; --k0)
+        if (s.delp[k0] < LW3_THIN) thin[nthin++] = k0;
     for (int i = tid; i < nlay * 64; i += LW_THREADS) {
         const int k = 1 + (i >> 6), w = i & 63, b = w & 15;
         float* r = aux + (size_t)k * LW3_REC;
@@ -85,51 +119,190 @@ __global__ void __launch_bounds__(LW_THREADS, 3) lw3_optics_kernel(const __grid_
         const float fu[6] = {s.facclr1u[k + 1], s.faccld1u[k + 1], s.faccmb1u[k + 1], s.faccmb2u[k + 1],
                              s.facclr2u[k + 1], s.faccld2u[k + 1]};
         for (int f = 0; f < 6; ++f) { r[R_FACD + f] = fd[f]; r[R_FACU + f] = fu[f]; }
-        r[LW3_REC - 1] = 0.0f;
+        int slot = -1;
+        for (int i = 0; i < nthin; ++i)
+            if (thin[i] == k - 1) slot = i;
+        r[R_THIN] = __int_as_float(slot);
     }
     if (tid < 16) {
         aux[H_PKLAY0 + tid] = s.pklay[0][tid];
         aux[H_SECDIFF + tid] = s.secdiff[tid];
         aux[H_SEMISS + tid] = s.semiss[tid];
     }
+    if (tid == 0) aux[H_NTHIN] = __int_as_float(nthin);
 }
 
-// Layer k (1-based, surface first) terms of one g-point from the chunk scratch (lw2_terms arithmetic).
-__device__ __forceinline__ LwTerms<float> lw3_terms(const LwLut<float>& lut, float taug, float plfrac, float blay,
-                                                    float plev_u, float plev_d, float taucld, float sdif, bool cloudy)
+// One layer of the LW set-up in float64, read and written through the shared-layout names (lw_gas,
+// lw_prep_layer, lw_setcoef_layer, lw_cldprop_layer take it like the CTA's shared arrays).
+struct LwOneLayer {
+    Slot<double> pavel, tavel, delp, coldry, colbrd, h2ovmr;
+    Slot<double> fac00, fac01, fac10, fac11, selffac, selffrac, forfac, forfrac, minorfrac, scaleminor, scaleminorn2;
+    Slot<int> lower, jp, jt, jt1, indself, indfor, indminor;
+    Slot<double> colamt[7], wx[4], rfrate[2][6], tauaer[16], taucld[16];
+};
+
+__global__ void __launch_bounds__(LW_THREADS) lw3_thin_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
+                                                              float* __restrict__ scr)
 {
-    const float bpade = 1.0f / 0.278f, tblint = 10000.0f, rec_6 = 0.166667f, c06 = 0.06f;
-    LwTerms<float> t;
-    float odepth = fmaxf(0.0f, sdif * taug);
-    float atrgas, gasfac;
+    __shared__ LwOneLayer L;
+    __shared__ double pwv;
+    __shared__ int lcf1;
+    const int64_t gc = c0 + blockIdx.x;
+    const int rq = bt.find(gc);
+    const LwIn& a = bt.req[rq];
+    const int nlay = a.nlay;
+    const int64_t col = gc - bt.off[rq];
+    const int64_t N = a.ncol;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (nlay > NLAY_MAX || col >= N) return;
+    const float* aux = scr + (int64_t)blockIdx.x * lw3_block_floats(nlay) + (size_t)2 * nlay * LW3_GSTRIDE;
+    if (__float_as_int(__ldg(aux + H_NTHIN)) == 0) return;   // the optics kernel's count: most columns stop here
+    int thin[LW3_NTHIN];
+    const int nthin = lw3_thin_layers(a, col, thin);
+    double* th = reinterpret_cast<double*>(const_cast<float*>(aux) + lw3_rec_floats(nlay));
+    // precipitable water (lwrad.cu:245-260) and the cloud flag lcf1, in float64 from the inputs
+    if (warp == 0) {
+        double t1 = 0, t2 = 0;
+        int cl = 0;
+        for (int k0 = lane; k0 < nlay; k0 += 32) {
+            double h;
+            const double cd = lw_coldry<double>(a, col, k0, h);
+            const double c0w = fmax(0.0, cd * h);
+            t1 += cd + c0w;
+            t2 += c0w;
+            cl |= (double)__ldg(a.clouds + (size_t)(nlay - 1 - k0) * N + col) > (double)1.0e-6f;
+        }
+        t1 = warp_sum(t1);
+        t2 = warp_sum(t2);
+        cl = __any_sync(0xffffffffu, cl);
+        if (lane == 0) {
+            const double amdw = (double)28.9644 / (double)18.0154;
+            pwv = (double)10.0 * t2 / (amdw * t1 * (double)9.80665) * (double)__ldg(a.plvl + (size_t)nlay * N + col);
+            lcf1 = cl;
+        }
+    }
+    __syncthreads();
+    if (tid < 16) th[tid] = lw_secdiff<double>(tid, pwv);
+    const int ilwcliq = a.diagnostic ? 0 : 1;
+    for (int i = 0; i < nthin; ++i) {
+        const int k0 = thin[i];
+        if (tid == 0) {
+            lw_prep_layer<double>(L, a, col, k0);
+            lw_setcoef_layer<double>(L, k0);
+            lw_cldprop_layer<double>(L, a, col, k0, lcf1, ilwcliq);
+        }
+        __syncthreads();
+        double* o = th + 16 + i * LW3_TSLOT;
+        if (tid < LW_NGPT) {
+            int b = 0;
+            while (tid >= c_lw_ns[b + 1]) ++b;
+            double tg, fr;
+            lw_gas(L, tid, k0, tg, fr, b);
+            o[T_TAUG + tid] = tg + L.tauaer[b][k0];
+            o[T_FRACS + tid] = fr;
+        } else if (tid < LW_NGPT + 16) {
+            const int b = tid - LW_NGPT;
+            double lay, lev, lay0, lev0;
+            lw_planck<double>(a, col, k0 + 1, b, lay, lev);
+            lw_planck<double>(a, col, k0, b, lay0, lev0);
+            o[T_PKLAY + b] = lay;
+            o[T_PKUP + b] = lev;
+            o[T_PKDN + b] = lev0;
+            o[T_TAUCLD + b] = L.taucld[b][k0];
+        }
+        __syncthreads();
+    }
+}
+
+// Layer k (1-based, surface first) terms of one g-point (lw2_terms arithmetic), in float or float64.
+template <class R>
+__device__ __forceinline__ LwTerms<R> lw3_terms(const LwLut<R>& lut, R taug, R plfrac, R blay, R plev_u, R plev_d,
+                                                R taucld, R sdif, bool cloudy)
+{
+    const R bpade = (R)1.0f / (R)0.278f, tblint = (R)10000, rec_6 = (R)0.166667f, c06 = (R)0.06f;
+    LwTerms<R> t;
+    R odepth = fmaxR((R)0, sdif * taug);
+    R atrgas, gasfac;
     if (odepth <= c06) {
-        atrgas = odepth - 0.5f * odepth * odepth;
-        t.trng = 1.0f - atrgas;
+        atrgas = odepth - (R)0.5f * odepth * odepth;
+        t.trng = (R)1 - atrgas;
         gasfac = rec_6 * odepth;
     } else {
-        const float tblind = odepth / (bpade + odepth);
-        const int it = (int)(tblint * tblind + 0.5f);
-        t.trng = ldt(lut.ex + it); atrgas = 1.0f - t.trng; gasfac = ldt(lut.tfn + it); odepth = ldt(lut.tau + it);
+        const R tblind = odepth / (bpade + odepth);
+        const int it = (int)(tblint * tblind + (R)0.5f);
+        t.trng = ldt(lut.ex + it); atrgas = (R)1 - t.trng; gasfac = ldt(lut.tfn + it); odepth = ldt(lut.tau + it);
     }
-    const float dplnku = plev_u - blay;
-    const float dplnkd = plev_d - blay;
+    const R dplnku = plev_u - blay;
+    const R dplnkd = plev_d - blay;
     t.gassrcd = plfrac * (blay + dplnkd * gasfac) * atrgas;
     t.gassrcu = plfrac * (blay + dplnku * gasfac) * atrgas;
-    t.trnt = 1; t.totsrcd = 0; t.totsrcu = 0;
+    t.atrg = atrgas;
+    t.trnt = 1; t.totsrcd = 0; t.totsrcu = 0; t.atrt = 0;
     if (cloudy) {
-        const float odtot = odepth + sdif * taucld;
-        float totfac, atrtot;
+        const R odtot = odepth + sdif * taucld;
+        R totfac, atrtot;
         if (odtot < c06) {
-            totfac = rec_6 * odtot; atrtot = odtot - 0.5f * odtot * odtot; t.trnt = 1.0f - atrtot;
+            totfac = rec_6 * odtot; atrtot = odtot - (R)0.5f * odtot * odtot; t.trnt = (R)1 - atrtot;
         } else {
-            const float tblind = odtot / (bpade + odtot);
-            const int it = (int)(tblint * tblind + 0.5f);
-            totfac = ldt(lut.tfn + it); t.trnt = ldt(lut.ex + it); atrtot = 1.0f - t.trnt;
+            const R tblind = odtot / (bpade + odtot);
+            const int it = (int)(tblint * tblind + (R)0.5f);
+            totfac = ldt(lut.tfn + it); t.trnt = ldt(lut.ex + it); atrtot = (R)1 - t.trnt;
         }
         t.totsrcd = plfrac * (blay + dplnkd * totfac) * atrtot;
         t.totsrcu = plfrac * (blay + dplnku * totfac) * atrtot;
+        t.atrt = atrtot;
     }
     return t;
+}
+
+// One layer of one g-point's sweep in arithmetic R on the float state (radtot, radclr and, on the NAM
+// route, totrad / clrrad / rad of the max-random overlap): the recurrences of rtrnmr / rtrnmc.  Returns the
+// total-sky radiance change across the layer formed directly -- source - radiance x absorptance, per
+// overlap part -- so it keeps its relative precision however small it is beside the radiance.
+// f = the layer's six overlap factors (clr1 cld1 cmb1 cmb2 clr2 cld2), x = sdif x cloud optical depth.
+template <class R, bool MC>
+__device__ __forceinline__ R lw3_step(float& rtot, float& rclr, float& trad, float& crad, float& radv,
+                                      const LwTerms<R>& t, bool down, bool cl, bool lst, R clfr, const float* f, R x)
+{
+    const R src = down ? t.gassrcd : t.gassrcu, tsrc = down ? t.totsrcd : t.totsrcu;
+    const R prev = (R)rtot;
+    R inc;
+    if (MC) {
+        if (cl) {
+            const R efclrfr = (R)1 - ((R)1 - rexp(-x));
+            const R S = src + (tsrc - src);
+            rtot = (float)(prev * t.trng * efclrfr + S);
+            const R cabs = -expm1(-x);             // 1 - efclrfr without the cancellation
+            inc = S - prev * (t.atrg + cabs - t.atrg * cabs);
+        } else {
+            rtot = (float)(prev * t.trng + src);
+            inc = src - prev * t.atrg;
+        }
+        rclr = (float)((R)rclr * t.trng + src);
+        return inc;
+    }
+    R tt = trad, cc = crad, r = radv;
+    if (lst) { tt = clfr * prev; cc = prev - tt; r = 0; }
+    if (cl) {
+        const R tp = tt, cp = cc;
+        tt = tt * t.trnt + clfr * tsrc;
+        cc = cc * t.trng + ((R)1 - clfr) * src;
+        rtot = (float)(tt + cc);
+        rclr = (float)((R)rclr * t.trng + src);
+        const R radmod = r * ((R)f[0] * t.trng + (R)f[1] * t.trnt) - (R)f[2] * src + (R)f[3] * tsrc;
+        r = -radmod + (R)f[4] * (cc + radmod) - (R)f[5] * (tt - radmod);
+        tt = tt + r;
+        cc = cc - r;
+        inc = (clfr * tsrc + ((R)1 - clfr) * src) - (tp * t.atrt + cp * t.atrg);
+    } else {
+        rtot = (float)(prev * t.trng + src);
+        rclr = (float)((R)rclr * t.trng + src);
+        inc = src - prev * t.atrg;
+    }
+    trad = (float)tt;
+    crad = (float)cc;
+    radv = (float)r;
+    return inc;
 }
 
 // L1 prefetch of one 128-byte line (PTX prefetch.global.L1): the sweeps fetch the next layer's rows and
@@ -149,9 +322,9 @@ __device__ __forceinline__ void lw3_prefetch_layer(const float* tg, const float*
 }
 
 template <bool MC>
-__global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
+__global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32, 4) lw3_sweep_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
                                                                          int64_t nc, const float* __restrict__ scr,
-                                                                         LwLut<float> lut)
+                                                                         LwLut<float> lut, LwLut<double> lutd)
 {
     __shared__ double fup[LW3_SWEEP_WARPS][NLAY_MAX + 1], fdn[LW3_SWEEP_WARPS][NLAY_MAX + 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -168,6 +341,7 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
     const float* tg = blk;
     const float* fr = blk + (size_t)nlay * LW3_GSTRIDE;
     const float* aux = blk + (size_t)2 * nlay * LW3_GSTRIDE;
+    const double* thin = reinterpret_cast<const double*>(aux + lw3_rec_floats(nlay));
     lw3_prefetch_layer(tg, fr, aux, nlay, lane);
     const float eps = 1.0e-6f;
     int gi[LW3_SLOTS], band[LW3_SLOTS];
@@ -186,59 +360,58 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
     auto mask_bit = [&](int j, int k) {   // McICA: word j holds g-points 32 j .. 32 j + 31
         return ((__ldg(a.mask + ((size_t)j * nlay + (k - 1)) * N + col) >> lane) & 1u) != 0;
     };
-    // ---- downward sweep
-    float radtotd[LW3_SLOTS], radclrd[LW3_SLOTS], totradd[LW3_SLOTS], clrradd[LW3_SLOTS], rad[LW3_SLOTS];
-#pragma unroll
-    for (int j = 0; j < LW3_SLOTS; ++j) { radtotd[j] = 0; radclrd[j] = 0; totradd[j] = 0; clrradd[j] = 0; rad[j] = 0; }
-    for (int k = nlay; k >= 1; --k) {
-        if (k > 1) lw3_prefetch_layer(tg, fr, aux, k - 1, lane);
+    float radtot[LW3_SLOTS], radclr[LW3_SLOTS], trad[LW3_SLOTS], crad[LW3_SLOTS], rad[LW3_SLOTS];
+    // One layer of the sweep for the warp's g-points; returns the warp's float64 sum of the radiance changes.
+    auto layer = [&](int k, bool down) -> double {
         const float* tgr = tg + (size_t)(k - 1) * LW3_GSTRIDE;
         const float* frr = fr + (size_t)(k - 1) * LW3_GSTRIDE;
         const float* r = aux + (size_t)k * LW3_REC;
         const float clfr = __ldg(r + R_CLDFRC);
-        const bool lst = __float_as_int(__ldg(r + R_LSTD)) != 0;
-        const float c1 = __ldg(r + R_FACD), d1 = __ldg(r + R_FACD + 1), m1 = __ldg(r + R_FACD + 2),
-                    m2 = __ldg(r + R_FACD + 3), c2 = __ldg(r + R_FACD + 4), d2 = __ldg(r + R_FACD + 5);
-        double sum = 0.0;
+        const bool lst = __float_as_int(__ldg(r + (down ? R_LSTD : R_LSTU))) != 0;
+        const int th = __float_as_int(__ldg(r + R_THIN));
+        float f[6];
 #pragma unroll
-        for (int j = 0; j < LW3_SLOTS; ++j) {
-            const int g = gi[j], b = band[j];
-            const bool cl = MC ? mask_bit(j, k) : clfr >= eps;
-            const float tcb = __ldg(r + R_TAUCLD + b);
-            const LwTerms<float> t = lw3_terms(lut, __ldg(tgr + g), __ldg(frr + g), __ldg(r + R_PKLAY + b),
-                                               __ldg(r + R_PKLEVU + b), __ldg(r + R_PKLEVD + b), tcb, sdif[j], cl);
-            if (MC) {
-                if (cl) {
-                    const float efclrfr = 1.0f - (1.0f - rexp(-(sdif[j] * tcb)));
-                    radtotd[j] = radtotd[j] * t.trng * efclrfr + t.gassrcd + (t.totsrcd - t.gassrcd);
-                } else {
-                    radtotd[j] = radtotd[j] * t.trng + t.gassrcd;
-                }
-                radclrd[j] = radclrd[j] * t.trng + t.gassrcd;
-            } else {
-                if (lst) { totradd[j] = clfr * radtotd[j]; clrradd[j] = radtotd[j] - totradd[j]; rad[j] = 0; }
-                if (cl) {
-                    totradd[j] = totradd[j] * t.trnt + clfr * t.totsrcd;
-                    clrradd[j] = clrradd[j] * t.trng + (1.0f - clfr) * t.gassrcd;
-                    radtotd[j] = totradd[j] + clrradd[j];
-                    radclrd[j] = radclrd[j] * t.trng + t.gassrcd;
-                    const float radmod = rad[j] * (c1 * t.trng + d1 * t.trnt) - m1 * t.gassrcd + m2 * t.totsrcd;
-                    rad[j] = -radmod + c2 * (clrradd[j] + radmod) - d2 * (totradd[j] - radmod);
-                    totradd[j] = totradd[j] + rad[j];
-                    clrradd[j] = clrradd[j] - rad[j];
-                } else {
-                    radtotd[j] = radtotd[j] * t.trng + t.gassrcd;
-                    radclrd[j] = radclrd[j] * t.trng + t.gassrcd;
-                }
+        for (int i = 0; i < 6; ++i) f[i] = __ldg(r + (down ? R_FACD : R_FACU) + i);
+        double sum = 0.0;
+        if (th < 0) {
+#pragma unroll
+            for (int j = 0; j < LW3_SLOTS; ++j) {
+                const int g = gi[j], b = band[j];
+                const bool cl = MC ? mask_bit(j, k) : clfr >= eps;
+                const float tcb = __ldg(r + R_TAUCLD + b);
+                const LwTerms<float> t = lw3_terms<float>(lut, __ldg(tgr + g), __ldg(frr + g), __ldg(r + R_PKLAY + b),
+                                                          __ldg(r + R_PKLEVU + b), __ldg(r + R_PKLEVD + b), tcb,
+                                                          sdif[j], cl);
+                const float inc = lw3_step<float, MC>(radtot[j], radclr[j], trad[j], crad[j], rad[j], t, down, cl, lst,
+                                                      clfr, f, sdif[j] * tcb);
+                if (val[j]) sum += (double)inc;
             }
-            if (val[j]) sum += (double)radtotd[j];
+        } else {
+            const double* o = thin + 16 + th * LW3_TSLOT;
+#pragma unroll
+            for (int j = 0; j < LW3_SLOTS; ++j) {
+                const int g = gi[j], b = band[j];
+                const bool cl = MC ? mask_bit(j, k) : clfr >= eps;
+                const double sd = thin[b], tcb = o[T_TAUCLD + b];
+                const LwTerms<double> t = lw3_terms<double>(lutd, o[T_TAUG + g], o[T_FRACS + g], o[T_PKLAY + b],
+                                                            o[T_PKUP + b], o[T_PKDN + b], tcb, sd, cl);
+                const double inc = lw3_step<double, MC>(radtot[j], radclr[j], trad[j], crad[j], rad[j], t, down, cl,
+                                                        lst, (double)clfr, f, sd * tcb);
+                if (val[j]) sum += inc;
+            }
         }
-        sum = warp_sum(sum);
-        if (lane == 0) fdn[warp][k - 1] = sum;
+        return warp_sum(sum);
+    };
+    // ---- downward sweep
+#pragma unroll
+    for (int j = 0; j < LW3_SLOTS; ++j) { radtot[j] = 0; radclr[j] = 0; trad[j] = 0; crad[j] = 0; rad[j] = 0; }
+    for (int k = nlay; k >= 1; --k) {
+        if (k > 1) lw3_prefetch_layer(tg, fr, aux, k - 1, lane);
+        const double v = layer(k, true);
+        if (lane == 0) fdn[warp][k - 1] = v;          // D(k-1) - D(k), summed over g
     }
     // ---- surface: emission and reflection
     lw3_prefetch_layer(tg, fr, aux, 1, lane);
-    float radtotu[LW3_SLOTS], radclru[LW3_SLOTS];
     double s_tu = 0, s_cu = 0, s_td = 0, s_cd = 0;
 #pragma unroll
     for (int j = 0; j < LW3_SLOTS; ++j) {
@@ -246,82 +419,39 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
         const float semi = __ldg(aux + H_SEMISS + b);
         const float reflct = 1.0f - semi;
         const float rad0 = semi * __ldg(fr + gi[j]) * __ldg(aux + H_PKLAY0 + b);
-        radtotu[j] = rad0 + reflct * radtotd[j];
-        radclru[j] = rad0 + reflct * radclrd[j];
+        const float rtd = radtot[j], rcd = radclr[j];
+        radtot[j] = rad0 + reflct * rtd;
+        radclr[j] = rad0 + reflct * rcd;
         if (val[j]) {
-            s_tu += (double)radtotu[j]; s_cu += (double)radclru[j];
-            s_td += (double)radtotd[j]; s_cd += (double)radclrd[j];
+            s_tu += (double)radtot[j]; s_cu += (double)radclr[j];
+            s_td += (double)rtd; s_cd += (double)rcd;
         }
+        trad[j] = 0; crad[j] = 0; rad[j] = 0;
     }
     s_tu = warp_sum(s_tu); s_cu = warp_sum(s_cu); s_td = warp_sum(s_td); s_cd = warp_sum(s_cd);
-    if (lane == 0) fup[warp][0] = s_tu;
     // ---- upward sweep
-    float totradu[LW3_SLOTS], clrradu[LW3_SLOTS];
-#pragma unroll
-    for (int j = 0; j < LW3_SLOTS; ++j) { totradu[j] = 0; clrradu[j] = 0; rad[j] = 0; }
     for (int k = 1; k <= nlay; ++k) {
         if (k < nlay) lw3_prefetch_layer(tg, fr, aux, k + 1, lane);
-        const float* tgr = tg + (size_t)(k - 1) * LW3_GSTRIDE;
-        const float* frr = fr + (size_t)(k - 1) * LW3_GSTRIDE;
-        const float* r = aux + (size_t)k * LW3_REC;
-        const float clfr = __ldg(r + R_CLDFRC);
-        const bool lst = __float_as_int(__ldg(r + R_LSTU)) != 0;
-        const float c1 = __ldg(r + R_FACU), d1 = __ldg(r + R_FACU + 1), m1 = __ldg(r + R_FACU + 2),
-                    m2 = __ldg(r + R_FACU + 3), c2 = __ldg(r + R_FACU + 4), d2 = __ldg(r + R_FACU + 5);
-        double sum = 0.0;
-#pragma unroll
-        for (int j = 0; j < LW3_SLOTS; ++j) {
-            const int g = gi[j], b = band[j];
-            const bool cl = MC ? mask_bit(j, k) : clfr >= eps;
-            const float tcb = __ldg(r + R_TAUCLD + b);
-            const LwTerms<float> t = lw3_terms(lut, __ldg(tgr + g), __ldg(frr + g), __ldg(r + R_PKLAY + b),
-                                               __ldg(r + R_PKLEVU + b), __ldg(r + R_PKLEVD + b), tcb, sdif[j], cl);
-            if (MC) {
-                if (cl) {
-                    const float efclrfr = 1.0f - (1.0f - rexp(-(sdif[j] * tcb)));
-                    radtotu[j] = radtotu[j] * t.trng * efclrfr + t.gassrcu + (t.totsrcu - t.gassrcu);
-                } else {
-                    radtotu[j] = radtotu[j] * t.trng + t.gassrcu;
-                }
-                radclru[j] = radclru[j] * t.trng + t.gassrcu;
-            } else {
-                if (lst) { totradu[j] = clfr * radtotu[j]; clrradu[j] = radtotu[j] - totradu[j]; rad[j] = 0; }
-                if (cl) {
-                    totradu[j] = totradu[j] * t.trnt + clfr * t.totsrcu;
-                    clrradu[j] = clrradu[j] * t.trng + (1.0f - clfr) * t.gassrcu;
-                    radtotu[j] = totradu[j] + clrradu[j];
-                    radclru[j] = radclru[j] * t.trng + t.gassrcu;
-                    const float radmod = rad[j] * (c1 * t.trng + d1 * t.trnt) - m1 * t.gassrcu + m2 * t.totsrcu;
-                    rad[j] = -radmod + c2 * (clrradu[j] + radmod) - d2 * (totradu[j] - radmod);
-                    totradu[j] = totradu[j] + rad[j];
-                    clrradu[j] = clrradu[j] - rad[j];
-                } else {
-                    radtotu[j] = radtotu[j] * t.trng + t.gassrcu;
-                    radclru[j] = radclru[j] * t.trng + t.gassrcu;
-                }
-            }
-            if (val[j]) sum += (double)radtotu[j];
-        }
-        sum = warp_sum(sum);
-        if (lane == 0) fup[warp][k] = sum;
+        const double v = layer(k, false);
+        if (lane == 0) fup[warp][k] = v;              // U(k) - U(k-1), summed over g
     }
     double t_tu = 0, t_cu = 0;
 #pragma unroll
     for (int j = 0; j < LW3_SLOTS; ++j)
-        if (val[j]) { t_tu += (double)radtotu[j]; t_cu += (double)radclru[j]; }
+        if (val[j]) { t_tu += (double)radtot[j]; t_cu += (double)radclr[j]; }
     t_tu = warp_sum(t_tu);
     t_cu = warp_sum(t_cu);
     __syncwarp();
-    // ---- outputs: fluxes x flxfac, heating rates from float64 net-flux differences (rtrnmr post)
+    // ---- outputs: fluxes x flxfac; heating rates from the per-layer net-flux changes (rtrnmr post)
     const double pi = 3.14159265358979323846;
     const double flxfac = 0.5 * pi * 2.0e4;
     const double heatfac = 9.80665 * 1.0e-2 / 1.0046e3;
     for (int k = lane; k < nlay; k += 32) {
-        const double uk = fup[warp][k], uk1 = fup[warp][k + 1];
-        const double dk = fdn[warp][k], dk1 = k + 1 < nlay ? fdn[warp][k + 1] : 0.0;
+        // layer k + 1 (surface first): (U(k) - D(k)) - (U(k+1) - D(k+1)) = -(dU + dD)
+        const double du = fup[warp][k + 1], dd = fdn[warp][k];
         const int kin = nlay - 1 - k;
         const double dl = (double)__ldg(a.plvl + (size_t)(kin + 1) * N + col) - (double)__ldg(a.plvl + (size_t)kin * N + col);
-        a.htlw[(size_t)kin * N + col] = (float)(((uk - dk) - (uk1 - dk1)) * flxfac * (heatfac / dl));
+        a.htlw[(size_t)kin * N + col] = (float)(-(du + dd) * flxfac * (heatfac / dl));
     }
     if (lane == 0) {
         a.topflw[col] = (float)(t_tu * flxfac);
