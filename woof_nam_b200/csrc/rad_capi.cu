@@ -403,24 +403,27 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
         const bool mc = cfg.route == RAD_ROUTE_MCICA;
         const int64_t lwc = fixed ? 0 : lw3_chunk(cfg);
         if (sizeof(R) == 4 && lwc > 0) {
-            // per chunk: gas optics into the scratch, the float64 thin-layer optics, then one warp per column
-            // sweeps
+            // per chunk: gas optics into the scratch, one warp per column sweeps, then (NAM route) the flagged
+            // columns -- a cloudy layer under 1 hPa -- again by the float64 column kernel
             LwLut<float> fl;
             fl.ex = h->d_lwf; fl.tfn = h->d_lwf + 10001; fl.tau = h->d_lwf + 2 * 10001;
             LwLut<double> dl;
             dl.ex = h->d_lwd; dl.tfn = h->d_lwd + 10001; dl.tau = h->d_lwd + 2 * 10001;
-            const size_t smem1 = sizeof(LwSetup<float>);
+            const size_t smem1 = sizeof(LwSetup<float>), smemd = sizeof(LwShared<double>);
             RAD_CUDA(h, cudaFuncSetAttribute((void*)lw3_optics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
+            RAD_CUDA(h, cudaFuncSetAttribute((void*)lw3_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemd));
             for (int64_t c0 = 0; c0 < ntot; c0 += lwc) {
                 const int64_t nc = std::min(lwc, ntot - c0);
                 lw3_optics_kernel<<<(unsigned)nc, LW_THREADS, smem1, st>>>(bt, c0, h->d_lw3, h->d_err);
-                lw3_thin_kernel<<<(unsigned)nc, LW_THREADS, 0, st>>>(bt, c0, h->d_lw3);
                 const unsigned g2 = (unsigned)((nc + LW3_SWEEP_WARPS - 1) / LW3_SWEEP_WARPS);
-                if (mc)
-                    lw3_sweep_kernel<true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, dl);
-                else
-                    lw3_sweep_kernel<false><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, dl);
-                h->launches += 3;
+                if (mc) {
+                    lw3_sweep_kernel<true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                    h->launches += 2;
+                } else {
+                    lw3_sweep_kernel<false><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                    lw3_fp64_kernel<<<(unsigned)nc, LW_THREADS, smemd, st>>>(bt, c0, h->d_lw3, dl, h->d_err);
+                    h->launches += 3;
+                }
             }
             RAD_CUDA(h, cudaGetLastError());
         } else {

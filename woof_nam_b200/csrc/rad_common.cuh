@@ -61,15 +61,6 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-// One value read and written through array syntax (any index): lets a single layer stand in for the
-// per-layer arrays of a shared-memory layout in code written against those arrays.
-template <class T>
-struct Slot {
-    T v;
-    __device__ __forceinline__ T& operator[](int) { return v; }
-    __device__ __forceinline__ const T& operator[](int) const { return v; }
-};
-
 // Visit every (g-point, layer) pair of a column with the CTA's warps such that each warp works on one band
 // at a time: lane l of a task of band b takes g-point ns[b] + l % ng and layer k0 + l / ng (ng = the band's
 // g-point count, 32 / ng layers per task).  Neighbouring lanes then read neighbouring g entries of the

@@ -903,15 +903,17 @@ __device__ __forceinline__ void lw_setup(LwShared<R>& s, const LwIn& a, int64_t 
 
 using LwBatch = ReqBatch<LwIn>;
 
+// The whole LW column gc (of the launch's concatenated column space) by one CTA: set-up, gas optics and the
+// rtrnmr sweeps with one g-point per thread.  R = double is the plain FP64 kernel.
 template <class R>
-__global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(const __grid_constant__ LwBatch bt, LwLut<R> lut, int* err)
+__device__ __forceinline__ void lw_column_body(const LwBatch& bt, const LwLut<R>& lut, int* err, int64_t gc)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LwShared<R>& s = *reinterpret_cast<LwShared<R>*>(smem_raw);
-    const int rq = bt.find((int64_t)blockIdx.x);
+    const int rq = bt.find(gc);
     const LwIn& a = bt.req[rq];
     const int nlay = a.nlay;
-    const int64_t col = (int64_t)blockIdx.x - bt.off[rq];
+    const int64_t col = gc - bt.off[rq];
     const int64_t N = a.ncol;
     const int tid = threadIdx.x;
     if (nlay > NLAY_MAX || col >= N) {
@@ -1054,6 +1056,13 @@ __global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(const __grid_cons
         a.sfcflw[2 * N + col] = (float)(sc[4] * flxfac);
         a.sfcflw[3 * N + col] = (float)(sc[5] * flxfac);
     }
+}
+
+
+template <class R>
+__global__ void __launch_bounds__(LW_THREADS) lw_column_kernel(const __grid_constant__ LwBatch bt, LwLut<R> lut, int* err)
+{
+    lw_column_body<R>(bt, lut, err, (int64_t)blockIdx.x);
 }
 
 }  // namespace rad

@@ -8,23 +8,23 @@
 //                      cldprop, setcoef, Planck functions, taugb01..16, the max-random overlap factors of
 //                      rtrnmr), with taug / fracs written straight to the chunk's scratch and the sweep inputs
 //                      copied after them.  Shared memory is the set-up data only (~32 KB).
-//   lw3_thin_kernel    one CTA per column, for layers thinner than LW3_THIN hPa only (most columns have none
-//                      and exit at once): that layer's absorber amounts, setcoef, cloud optics, Planck values
-//                      and gas optics again in float64, with the column's precipitable water and diffusivity
-//                      secants in float64.  A float optical depth puts some g-points of such a layer on the
-//                      neighbouring entry of the 10,001-entry transmittance table; in a 0.1 hPa cloudy layer
-//                      cooling at thousands of K/day that alone is ~1e-5 of the heating rate.
 //   lw3_sweep_kernel   one warp per column: lane l carries g-points l, l + 32, ..., l + 128 (five independent
 //                      recurrences interleaved per lane), reading each layer's optical depths as coalesced
 //                      128-byte rows.  Per layer each g-point's radiance CHANGE across the layer is formed
 //                      directly (source minus radiance x absorptance) and summed over g-points in float64; the
 //                      heating rates come from those changes, not from differences of ~300 W/m^2 level
-//                      fluxes.  Thin layers take this step in float64 from the float64 optics.
+//                      fluxes.
+//   lw3_fp64_kernel    the plain float64 LW column (lw_column_body<double>) for the columns the optics kernel
+//                      flags: a cloudy layer thinner than LW3_THIN hPa.  Such a layer (a cloud in the 0.1 hPa
+//                      top layer of the precision-stress request) cools at thousands of K/day, and 1e-5 of
+//                      that is already above 0.01 K/day: float optical depths put some g-points on the
+//                      neighbouring entry of the 10,001-entry transmittance table, and float radiances
+//                      carry ~1e-6 through the column.  Other columns exit at once.
 //
 // Scratch block of one column (floats, 128-byte aligned): taug [nlay][160], fracs [nlay][160] (g-points
 // 140..159 unused), then one 80-word record per layer k = 1..nlay holding everything the sweeps read at that
-// layer (so a layer step touches one contiguous record) and a head record (k = 0) for the surface, then the
-// float64 thin-layer area.  The arithmetic of every term and recurrence is that of rad_lw2.cuh (rtrnmr,
+// layer (so a layer step touches one contiguous record) and a head record (k = 0) for the surface.  The
+// arithmetic of every term and recurrence is that of rad_lw2.cuh (rtrnmr,
 // phys_rrtm_lw_rtrnmr_body.cuh:130-330; rtrnmc, phys_rrtm_lw_rtrnmc.cu:85-310).
 #pragma once
 #include "rad_lw2.cuh"
@@ -45,37 +45,18 @@ constexpr int R_LSTU = 65;      // int lstu[k]
 constexpr int R_LSTD = 66;      // int lstd[k]
 constexpr int R_FACD = 67;      // [6] downward factors at k - 1: clr1 cld1 cmb1 cmb2 clr2 cld2
 constexpr int R_FACU = 73;      // [6] upward factors at k + 1, same order
-constexpr int R_THIN = 79;      // int: slot of the layer in the float64 thin-layer area, or -1
 // head record (k = 0)
 constexpr int H_PKLAY0 = 0;     // [16] pklay[0] (surface)
 constexpr int H_SECDIFF = 16;   // [16]
 constexpr int H_SEMISS = 32;    // [16]
-constexpr int H_NTHIN = 48;     // int: number of thin layers (the thin kernel's first read)
+constexpr int H_FP64 = 48;      // int: 1 when the column is to be solved in float64 (lw3_fp64_kernel)
 
-// float64 thin-layer area: secdiff [16], then LW3_NTHIN slots of LW3_TSLOT doubles
-constexpr float LW3_THIN = 1.0f;   // hPa: layers thinner than this get the float64 step
-constexpr int LW3_NTHIN = 2;       // at most this many per column (the top-most ones)
-constexpr int LW3_TSLOT = 352;
-constexpr int T_TAUG = 1, T_FRACS = 141, T_PKLAY = 281, T_PKUP = 297, T_PKDN = 313, T_TAUCLD = 329;
-constexpr int LW3_THIN_FLOATS = 2 * (16 + LW3_NTHIN * LW3_TSLOT);
+constexpr float LW3_THIN = 1.0f;   // hPa: a cloudy layer thinner than this sends the column to float64
 
 __host__ __device__ constexpr int64_t lw3_rec_floats(int nlay) { return ((((int64_t)nlay + 1) * LW3_REC + 31) / 32) * 32; }
 __host__ __device__ constexpr int64_t lw3_block_floats(int nlay)
 {
-    return (int64_t)2 * nlay * LW3_GSTRIDE + lw3_rec_floats(nlay) + LW3_THIN_FLOATS;
-}
-
-// The thin layers of a column (float layer thicknesses, top first); the optics and thin kernels agree on it.
-__device__ __forceinline__ int lw3_thin_layers(const LwIn& a, int64_t col, int* k0s)
-{
-    const int nlay = a.nlay;
-    const int64_t N = a.ncol;
-    int n = 0;
-    for (int k0 = nlay - 1; k0 >= 0 && n < LW3_NTHIN; --k0) {
-        const float dlp = __ldg(a.plvl + (size_t)(nlay - k0) * N + col) - __ldg(a.plvl + (size_t)(nlay - k0 - 1) * N + col);
-        if (dlp < LW3_THIN) k0s[n++] = k0;
-    }
-    return n;
+    return (int64_t)2 * nlay * LW3_GSTRIDE + lw3_rec_floats(nlay);
 }
 
 __global__ void __launch_bounds__(LW_THREADS, 3) lw3_optics_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
@@ -101,9 +82,6 @@ __global__ void __launch_bounds__(LW_THREADS, 3) lw3_optics_kernel(const __grid_
         fro[k0 * LW3_GSTRIDE + g] = fr;
     });
     float* aux = blk + (size_t)2 * nlay * LW3_GSTRIDE;
-    int thin[LW3_NTHIN], nthin = 0;                  // lw3_thin_layers, from the same float thicknesses
-    for (int k0 = nlay - 1; k0 >= 0 && nthin < LW3_NTHIN; --k0)
-        if (s.delp[k0] < LW3_THIN) thin[nthin++] = k0;
     for (int i = tid; i < nlay * 64; i += LW_THREADS) {
         const int k = 1 + (i >> 6), w = i & 63, b = w & 15;
         float* r = aux + (size_t)k * LW3_REC;
@@ -119,99 +97,32 @@ __global__ void __launch_bounds__(LW_THREADS, 3) lw3_optics_kernel(const __grid_
         const float fu[6] = {s.facclr1u[k + 1], s.faccld1u[k + 1], s.faccmb1u[k + 1], s.faccmb2u[k + 1],
                              s.facclr2u[k + 1], s.faccld2u[k + 1]};
         for (int f = 0; f < 6; ++f) { r[R_FACD + f] = fd[f]; r[R_FACU + f] = fu[f]; }
-        int slot = -1;
-        for (int i = 0; i < nthin; ++i)
-            if (thin[i] == k - 1) slot = i;
-        r[R_THIN] = __int_as_float(slot);
+        r[LW3_REC - 1] = 0.0f;
     }
     if (tid < 16) {
         aux[H_PKLAY0 + tid] = s.pklay[0][tid];
         aux[H_SECDIFF + tid] = s.secdiff[tid];
         aux[H_SEMISS + tid] = s.semiss[tid];
     }
-    if (tid == 0) aux[H_NTHIN] = __int_as_float(nthin);
+    if (tid == 0) {
+        int fp64 = 0;
+        for (int k0 = 0; k0 < nlay; ++k0)
+            fp64 |= s.delp[k0] < LW3_THIN && s.cldfrc[k0 + 1] > 1.0e-6f;
+        aux[H_FP64] = __int_as_float(fp64);
+    }
 }
 
-// One layer of the LW set-up in float64, read and written through the shared-layout names (lw_gas,
-// lw_prep_layer, lw_setcoef_layer, lw_cldprop_layer take it like the CTA's shared arrays).
-struct LwOneLayer {
-    Slot<double> pavel, tavel, delp, coldry, colbrd, h2ovmr;
-    Slot<double> fac00, fac01, fac10, fac11, selffac, selffrac, forfac, forfrac, minorfrac, scaleminor, scaleminorn2;
-    Slot<int> lower, jp, jt, jt1, indself, indfor, indminor;
-    Slot<double> colamt[7], wx[4], rfrate[2][6], tauaer[16], taucld[16];
-};
-
-__global__ void __launch_bounds__(LW_THREADS) lw3_thin_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
-                                                              float* __restrict__ scr)
+// The flagged columns of a chunk in float64 (one CTA per column of the chunk; unflagged columns return).
+__global__ void __launch_bounds__(LW_THREADS) lw3_fp64_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
+                                                              const float* __restrict__ scr, LwLut<double> lutd,
+                                                              int* err)
 {
-    __shared__ LwOneLayer L;
-    __shared__ double pwv;
-    __shared__ int lcf1;
     const int64_t gc = c0 + blockIdx.x;
-    const int rq = bt.find(gc);
-    const LwIn& a = bt.req[rq];
-    const int nlay = a.nlay;
-    const int64_t col = gc - bt.off[rq];
-    const int64_t N = a.ncol;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (nlay > NLAY_MAX || col >= N) return;
-    const float* aux = scr + (int64_t)blockIdx.x * lw3_block_floats(nlay) + (size_t)2 * nlay * LW3_GSTRIDE;
-    if (__float_as_int(__ldg(aux + H_NTHIN)) == 0) return;   // the optics kernel's count: most columns stop here
-    int thin[LW3_NTHIN];
-    const int nthin = lw3_thin_layers(a, col, thin);
-    double* th = reinterpret_cast<double*>(const_cast<float*>(aux) + lw3_rec_floats(nlay));
-    // precipitable water (lwrad.cu:245-260) and the cloud flag lcf1, in float64 from the inputs
-    if (warp == 0) {
-        double t1 = 0, t2 = 0;
-        int cl = 0;
-        for (int k0 = lane; k0 < nlay; k0 += 32) {
-            double h;
-            const double cd = lw_coldry<double>(a, col, k0, h);
-            const double c0w = fmax(0.0, cd * h);
-            t1 += cd + c0w;
-            t2 += c0w;
-            cl |= (double)__ldg(a.clouds + (size_t)(nlay - 1 - k0) * N + col) > (double)1.0e-6f;
-        }
-        t1 = warp_sum(t1);
-        t2 = warp_sum(t2);
-        cl = __any_sync(0xffffffffu, cl);
-        if (lane == 0) {
-            const double amdw = (double)28.9644 / (double)18.0154;
-            pwv = (double)10.0 * t2 / (amdw * t1 * (double)9.80665) * (double)__ldg(a.plvl + (size_t)nlay * N + col);
-            lcf1 = cl;
-        }
-    }
-    __syncthreads();
-    if (tid < 16) th[tid] = lw_secdiff<double>(tid, pwv);
-    const int ilwcliq = a.diagnostic ? 0 : 1;
-    for (int i = 0; i < nthin; ++i) {
-        const int k0 = thin[i];
-        if (tid == 0) {
-            lw_prep_layer<double>(L, a, col, k0);
-            lw_setcoef_layer<double>(L, k0);
-            lw_cldprop_layer<double>(L, a, col, k0, lcf1, ilwcliq);
-        }
-        __syncthreads();
-        double* o = th + 16 + i * LW3_TSLOT;
-        if (tid < LW_NGPT) {
-            int b = 0;
-            while (tid >= c_lw_ns[b + 1]) ++b;
-            double tg, fr;
-            lw_gas(L, tid, k0, tg, fr, b);
-            o[T_TAUG + tid] = tg + L.tauaer[b][k0];
-            o[T_FRACS + tid] = fr;
-        } else if (tid < LW_NGPT + 16) {
-            const int b = tid - LW_NGPT;
-            double lay, lev, lay0, lev0;
-            lw_planck<double>(a, col, k0 + 1, b, lay, lev);
-            lw_planck<double>(a, col, k0, b, lay0, lev0);
-            o[T_PKLAY + b] = lay;
-            o[T_PKUP + b] = lev;
-            o[T_PKDN + b] = lev0;
-            o[T_TAUCLD + b] = L.taucld[b][k0];
-        }
-        __syncthreads();
-    }
+    const LwIn& a = bt.req[bt.find(gc)];
+    if (a.nlay > NLAY_MAX) return;
+    const float* aux = scr + (int64_t)blockIdx.x * lw3_block_floats(a.nlay) + (size_t)2 * a.nlay * LW3_GSTRIDE;
+    if (__float_as_int(__ldg(aux + H_FP64)) == 0) return;    // uniform over the CTA
+    lw_column_body<double>(bt, lutd, err, gc);
 }
 
 // Layer k (1-based, surface first) terms of one g-point (lw2_terms arithmetic), in float or float64.
@@ -322,9 +233,9 @@ __device__ __forceinline__ void lw3_prefetch_layer(const float* tg, const float*
 }
 
 template <bool MC>
-__global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32, 4) lw3_sweep_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
+__global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
                                                                          int64_t nc, const float* __restrict__ scr,
-                                                                         LwLut<float> lut, LwLut<double> lutd)
+                                                                         LwLut<float> lut)
 {
     __shared__ double fup[LW3_SWEEP_WARPS][NLAY_MAX + 1], fdn[LW3_SWEEP_WARPS][NLAY_MAX + 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -341,7 +252,6 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32, 4) lw3_sweep_kernel(cons
     const float* tg = blk;
     const float* fr = blk + (size_t)nlay * LW3_GSTRIDE;
     const float* aux = blk + (size_t)2 * nlay * LW3_GSTRIDE;
-    const double* thin = reinterpret_cast<const double*>(aux + lw3_rec_floats(nlay));
     lw3_prefetch_layer(tg, fr, aux, nlay, lane);
     const float eps = 1.0e-6f;
     int gi[LW3_SLOTS], band[LW3_SLOTS];
@@ -368,37 +278,20 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32, 4) lw3_sweep_kernel(cons
         const float* r = aux + (size_t)k * LW3_REC;
         const float clfr = __ldg(r + R_CLDFRC);
         const bool lst = __float_as_int(__ldg(r + (down ? R_LSTD : R_LSTU))) != 0;
-        const int th = __float_as_int(__ldg(r + R_THIN));
         float f[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) f[i] = __ldg(r + (down ? R_FACD : R_FACU) + i);
         double sum = 0.0;
-        if (th < 0) {
 #pragma unroll
-            for (int j = 0; j < LW3_SLOTS; ++j) {
-                const int g = gi[j], b = band[j];
-                const bool cl = MC ? mask_bit(j, k) : clfr >= eps;
-                const float tcb = __ldg(r + R_TAUCLD + b);
-                const LwTerms<float> t = lw3_terms<float>(lut, __ldg(tgr + g), __ldg(frr + g), __ldg(r + R_PKLAY + b),
-                                                          __ldg(r + R_PKLEVU + b), __ldg(r + R_PKLEVD + b), tcb,
-                                                          sdif[j], cl);
-                const float inc = lw3_step<float, MC>(radtot[j], radclr[j], trad[j], crad[j], rad[j], t, down, cl, lst,
-                                                      clfr, f, sdif[j] * tcb);
-                if (val[j]) sum += (double)inc;
-            }
-        } else {
-            const double* o = thin + 16 + th * LW3_TSLOT;
-#pragma unroll
-            for (int j = 0; j < LW3_SLOTS; ++j) {
-                const int g = gi[j], b = band[j];
-                const bool cl = MC ? mask_bit(j, k) : clfr >= eps;
-                const double sd = thin[b], tcb = o[T_TAUCLD + b];
-                const LwTerms<double> t = lw3_terms<double>(lutd, o[T_TAUG + g], o[T_FRACS + g], o[T_PKLAY + b],
-                                                            o[T_PKUP + b], o[T_PKDN + b], tcb, sd, cl);
-                const double inc = lw3_step<double, MC>(radtot[j], radclr[j], trad[j], crad[j], rad[j], t, down, cl,
-                                                        lst, (double)clfr, f, sd * tcb);
-                if (val[j]) sum += inc;
-            }
+        for (int j = 0; j < LW3_SLOTS; ++j) {
+            const int g = gi[j], b = band[j];
+            const bool cl = MC ? mask_bit(j, k) : clfr >= eps;
+            const float tcb = __ldg(r + R_TAUCLD + b);
+            const LwTerms<float> t = lw3_terms<float>(lut, __ldg(tgr + g), __ldg(frr + g), __ldg(r + R_PKLAY + b),
+                                                      __ldg(r + R_PKLEVU + b), __ldg(r + R_PKLEVD + b), tcb, sdif[j], cl);
+            const float inc = lw3_step<float, MC>(radtot[j], radclr[j], trad[j], crad[j], rad[j], t, down, cl, lst,
+                                                  clfr, f, sdif[j] * tcb);
+            if (val[j]) sum += (double)inc;
         }
         return warp_sum(sum);
     };
