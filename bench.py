@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 kernel leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
+    ap.add_argument("--lw-chunk", type=int, default=None,
+                    help="LW chunk size (columns); default: the autotuner's choice for this device")
     ap.add_argument("--ncol", type=int, default=None,
                     help="solve this many columns of the workload's generator instead of the full domain "
                          "(small cases for profiling)")
@@ -194,7 +196,12 @@ def main():
     # weak scaling: rank r solves ensemble member r (same generator, seed offset by the rank)
     cols = make_columns(n, seed + 7919 * rank, stress)
     nday = int((cols.coszen >= np.float32(1e-4)).sum())
-    mixed = RadSolver(precision="mixed", diagnostic=stress)
+    # launch shape (LW chunk) from the autotuner, measured outside the timed region and cached per device
+    from woof_nam_b200.solver import SolverConfig
+    from woof_nam_b200.tune import tuned_config
+    mcfg = SolverConfig(precision="mixed", diagnostic=stress)
+    mcfg = tuned_config(n, mcfg) if args.lw_chunk is None else SolverConfig(**{**mcfg.__dict__, "lw_chunk": args.lw_chunk})
+    mixed = RadSolver(mcfg)
     d = mixed.to_device(cols, device=dev)
     out = mixed.alloc_outputs(n, device=dev)
     in_bytes = sum(d[k].numel() * 4 for k in INPUT_FIELDS)
@@ -300,7 +307,8 @@ def main():
                        "columns": n, "day_columns": nday, "layers": cols.nlay,
                        "input_bytes": in_bytes, "output_bytes": out_bytes,
                        "l2": f"inputs ({in_bytes / 1e9:.1f} GB) larger than L2 (126 MB); no flush",
-                       "parallelism": f"replicas x{ws} (one ensemble member per GPU)"},
+                       "parallelism": f"replicas x{ws} (one ensemble member per GPU)",
+                       "lw_chunk": mcfg.lw_chunk},
             "roofline": {"bound": "fp32", "kernel": dom, "achieved": achieved, "peak": peak_tf,
                          "unit": "TFLOP/s", "frac": achieved / peak_tf, "traffic": traffic,
                          "peak_source": f"nominal FP32 pipe 148 SM x 128 lanes x 2 at the measured sm_max "

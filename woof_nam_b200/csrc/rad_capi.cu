@@ -58,6 +58,8 @@ struct RadHandle {
     size_t cub_bytes = 0;
     float* d_lw3 = nullptr;                        // two-kernel LW: gas optics and sweep inputs of one chunk
     int64_t lw3_cap = 0;                           // columns d_lw3 holds
+    int* d_lw3list = nullptr;                      // [1 + lw3_cap]: count, then the chunk's float64 columns
+    int nsm = 148;                                 // SMs of the device (grid of the float64 column kernel)
     std::string err;
     // kernel accounting
     int64_t launches = 0;
@@ -294,9 +296,12 @@ int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
         const int64_t need = std::min(lwc, ntot);
         if (need > h->lw3_cap) {
             if (h->d_lw3) cudaFree(h->d_lw3);
+            if (h->d_lw3list) cudaFree(h->d_lw3list);
             h->d_lw3 = nullptr;
+            h->d_lw3list = nullptr;
             h->lw3_cap = 0;
             RAD_CUDA(h, cudaMalloc((void**)&h->d_lw3, (size_t)need * lw3_block_floats(h->cfg.nlay) * sizeof(float)));
+            RAD_CUDA(h, cudaMalloc((void**)&h->d_lw3list, (size_t)(need + 1) * sizeof(int)));
             h->lw3_cap = need;
         }
     }
@@ -414,14 +419,15 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
             RAD_CUDA(h, cudaFuncSetAttribute((void*)lw3_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemd));
             for (int64_t c0 = 0; c0 < ntot; c0 += lwc) {
                 const int64_t nc = std::min(lwc, ntot - c0);
-                lw3_optics_kernel<<<(unsigned)nc, LW_THREADS, smem1, st>>>(bt, c0, h->d_lw3, h->d_err);
+                RAD_CUDA(h, cudaMemsetAsync(h->d_lw3list, 0, sizeof(int), st));
+                lw3_optics_kernel<<<(unsigned)nc, LW_THREADS, smem1, st>>>(bt, c0, h->d_lw3, h->d_lw3list, h->d_err);
                 const unsigned g2 = (unsigned)((nc + LW3_SWEEP_WARPS - 1) / LW3_SWEEP_WARPS);
                 if (mc) {
                     lw3_sweep_kernel<true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
                     h->launches += 2;
                 } else {
                     lw3_sweep_kernel<false><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
-                    lw3_fp64_kernel<<<(unsigned)nc, LW_THREADS, smemd, st>>>(bt, c0, h->d_lw3, dl, h->d_err);
+                    lw3_fp64_kernel<<<(unsigned)h->nsm, LW_THREADS, smemd, st>>>(bt, c0, h->d_lw3list, dl, h->d_err);
                     h->launches += 3;
                 }
             }
@@ -538,6 +544,7 @@ int rad_create(const RadConfig* cfg, RadHandle** out)
     RadHandle* h = new RadHandle();
     h->cfg = *cfg;
     cudaGetDevice(&h->device);
+    cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device);
     if (cudaMalloc((void**)&h->d_err, sizeof(int)) != cudaSuccess ||
         cudaMalloc((void**)&h->d_nday, sizeof(int)) != cudaSuccess) {
         delete h;
@@ -924,7 +931,7 @@ void rad_destroy(RadHandle* h)
     for (void* p : {(void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
                     (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
                     (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub, (void*)h->d_lwm,
-                    (void*)h->d_swm, (void*)h->d_lw3})
+                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list})
         if (p) cudaFree(p);
     delete h;
 }

@@ -60,7 +60,7 @@ __host__ __device__ constexpr int64_t lw3_block_floats(int nlay)
 }
 
 __global__ void __launch_bounds__(LW_THREADS, 3) lw3_optics_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
-                                                                   float* __restrict__ scr, int* err)
+                                                                   float* __restrict__ scr, int* fp64list, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LwSetup<float>& s = *reinterpret_cast<LwSetup<float>*>(smem_raw);
@@ -109,20 +109,21 @@ __global__ void __launch_bounds__(LW_THREADS, 3) lw3_optics_kernel(const __grid_
         for (int k0 = 0; k0 < nlay; ++k0)
             fp64 |= s.delp[k0] < LW3_THIN && s.cldfrc[k0 + 1] > 1.0e-6f;
         aux[H_FP64] = __int_as_float(fp64);
+        if (fp64) fp64list[1 + atomicAdd(fp64list, 1)] = blockIdx.x;    // the chunk's list for lw3_fp64_kernel
     }
 }
 
-// The flagged columns of a chunk in float64 (one CTA per column of the chunk; unflagged columns return).
+// The flagged columns of a chunk in float64: list = [count, chunk-local columns...] appended by the optics
+// kernel; a grid of one CTA per SM walks it (the float64 layout's shared memory allows one CTA per SM).
 __global__ void __launch_bounds__(LW_THREADS) lw3_fp64_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
-                                                              const float* __restrict__ scr, LwLut<double> lutd,
+                                                              const int* __restrict__ list, LwLut<double> lutd,
                                                               int* err)
 {
-    const int64_t gc = c0 + blockIdx.x;
-    const LwIn& a = bt.req[bt.find(gc)];
-    if (a.nlay > NLAY_MAX) return;
-    const float* aux = scr + (int64_t)blockIdx.x * lw3_block_floats(a.nlay) + (size_t)2 * a.nlay * LW3_GSTRIDE;
-    if (__float_as_int(__ldg(aux + H_FP64)) == 0) return;    // uniform over the CTA
-    lw_column_body<double>(bt, lutd, err, gc);
+    const int n = list[0];
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        lw_column_body<double>(bt, lutd, err, c0 + list[1 + i]);
+        __syncthreads();                          // shared memory is reused by the next column
+    }
 }
 
 // Layer k (1-based, surface first) terms of one g-point (lw2_terms arithmetic), in float or float64.

@@ -68,7 +68,11 @@ class RadServer:
         self.resident = sum(t.numel() * t.element_size() for dom in states.values() for m in dom for t in m.values())
         if self.resident > self.budget:
             raise MemoryError(f"resident column state {self.resident / 1e9:.1f} GB exceeds the HBM budget")
-        self.slots = [_Slot(RadSolver(precision=precision), torch.cuda.Stream()) for _ in range(slots)]
+        from .solver import SolverConfig
+        from .tune import tuned_config
+        largest = max(int(m["coszen"].shape[-1]) for dom in states.values() for m in dom)
+        cfg = tuned_config(largest, SolverConfig(precision=precision))   # launch shape for the largest domain
+        self.slots = [_Slot(RadSolver(cfg), torch.cuda.Stream()) for _ in range(slots)]
         self.in_use = 0
         self.keep = keep_outputs
 
