@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 kernel leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the uneven-batch leg (parent grid + three nests in one graph-captured launch set)")
     ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
     ap.add_argument("--lw-chunk", type=int, default=None,
                     help="LW chunk size (columns); default: the autotuner's choice for this device")
@@ -274,6 +276,33 @@ def main():
     barrier()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
 
+    # uneven batch: the parent grid plus the 3 km nests (333x333, 600x450, 180x180) as one batched solve
+    # captured in a CUDA graph, replayed per step; the nests' inputs are resident too
+    batch = None
+    if not args.no_batch and args.ncol is None:
+        from woof_nam_b200.columns import NESTS
+        nest_cols = [make_columns(jm * im, seed + 101 * (i + 1) + 7919 * rank, stress) for i, (jm, im) in enumerate(NESTS)]
+        reqs = [d] + [mixed.to_device(c, device=dev) for c in nest_cols]
+        graph = mixed.capture(reqs, [cols.solcon] + [c.solcon for c in nest_cols])
+        for _ in range(args.warmup):
+            graph.launch(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            graph.launch(stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms_b = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        nb = n + sum(c.ncol for c in nest_cols)
+        batch = {"value": ws * nb / (ms_b * 1e-3), "unit": UNIT, "ms_per_step": ms_b, "columns": nb,
+                 "requests": 1 + len(nest_cols), "graph": True,
+                 "workload": "954x835 parent + 333x333, 600x450, 180x180 nests, one batched launch set per step"}
+        graph.close()
+        del reqs, graph
+
     # roofline of the dominant kernel (FP32 pipe; algorithmic FLOPs from the oracle's operation-count table)
     pk = peaks()
     peak_tf, mhz = fp32_peak_tflops(pk)
@@ -325,6 +354,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": ws * n / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": in_bytes,
                     "d2h_bytes_per_step": out_bytes, "ms_per_step": ms_e2e},
+            "batch_c3": batch,
             "gpu_launches": launches,
             "clocks": clocks,
         }
