@@ -58,7 +58,7 @@ def test_serve_budget_admission():
     torch.cuda.synchronize()
     probe = RadServer(states, SOLCON, slots=1)
     one = probe.request_bytes(4096, probe.slots[0].solver)
-    budget = (probe.resident + one * 1.5) / 1e9
+    budget = (probe.resident + 3 * probe.held + one * 1.5) / 1e9     # three slots' scratch, 1.5 requests
     srv = RadServer(states, SOLCON, slots=3, hbm_budget_gb=budget)
     reqs = [Request(i, "c", 0, 0.0) for i in range(4)]
     srv.run(reqs)

@@ -32,6 +32,7 @@ def test_measures_once_then_remembers(tmp_path):
     assert c1.lw_chunk == c2.lw_chunk == 32768 and calls == [300000]
     tune.tuned_config(1000, cache_path=cache, timer=timer, device="gpu-x")          # new bucket
     assert len(calls) == 2
+    assert tune.tuned_config(300000, cache_path=cache, timer=timer, device="gpu-x", max_chunk=16384).lw_chunk == 8192
     assert tune.tuned_config(300000, base=SolverConfig(precision="fp64"), cache_path=cache, timer=timer,
                              device="gpu-x").lw_chunk == 0                           # FP64: nothing to tune
 

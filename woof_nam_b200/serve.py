@@ -4,8 +4,9 @@ Requests are radiation solves of whole domains (the 12 km parent, the 3 km nests
 arriving over time.  The server
 
   * keeps each member's column state resident on the device (uploaded once, refreshed in place),
-  * admits a request when its output buffers and the library scratch fit the HBM budget and a stream slot
-    is free, so requests that arrive while others run start at once and overlap on the device,
+  * admits a request when its output buffers fit the HBM budget beside the resident state and the slots'
+    library scratch (held per slot from start-up) and a stream slot is free, so requests that arrive while
+    others run start at once and overlap on the device,
   * runs every admitted solve on its own CUDA stream and library handle (a handle's scratch is not shared
     between concurrent solves), tracks completion with CUDA events,
   * reports latency from arrival to completion (p50 / p99) and throughput in columns/s.
@@ -71,14 +72,21 @@ class RadServer:
         from .solver import SolverConfig
         from .tune import tuned_config
         largest = max(int(m["coszen"].shape[-1]) for dom in states.values() for m in dom)
-        cfg = tuned_config(largest, SolverConfig(precision=precision))   # launch shape for the largest domain
+        # launch shape for the largest domain, LW chunks of at most 32,768 columns (3.1 GB of scratch a slot)
+        cfg = tuned_config(largest, SolverConfig(precision=precision), max_chunk=32768)
         self.slots = [_Slot(RadSolver(cfg), torch.cuda.Stream()) for _ in range(slots)]
+        # each slot's handle keeps the scratch it grows to (up to the largest request) until it is closed
+        self.held = sum(sl.solver.workspace_bytes(largest) for sl in self.slots)
+        if self.resident + self.held > self.budget:
+            raise MemoryError(f"resident state {self.resident / 1e9:.1f} GB and slot scratch "
+                              f"{self.held / 1e9:.1f} GB exceed the HBM budget")
         self.in_use = 0
         self.keep = keep_outputs
 
     def request_bytes(self, ncol: int, solver: RadSolver) -> int:
-        out = sum(int(np.prod(s)) * 4 for s in output_shapes(solver.cfg.nlay, ncol).values())
-        return out + solver.workspace_bytes(ncol)
+        """Device bytes a request adds while it is in flight: its output arrays (the slot's scratch is held
+        already and counted at start-up)."""
+        return sum(int(np.prod(s)) * 4 for s in output_shapes(solver.cfg.nlay, ncol).values())
 
     def _launch(self, slot: _Slot, req: Request, now: float):
         torch = self.torch
@@ -116,7 +124,7 @@ class RadServer:
                 if sl.req is None and queue:
                     r = queue[0]
                     need = self.request_bytes(int(self.states[r.domain][r.member]["coszen"].shape[-1]), sl.solver)
-                    if self.resident + self.in_use + need > self.budget:
+                    if self.resident + self.held + self.in_use + need > self.budget:
                         break
                     queue.pop(0)
                     self.in_use += need
@@ -131,7 +139,8 @@ class RadServer:
         cols = sum(r.ncol for r in done)
         return {"requests": nreq, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                 "mean_ms": float(lat.mean()), "columns": cols, "wall_s": wall, "columns_per_s": cols / wall,
-                "slots": len(self.slots), "resident_gb": self.resident / 1e9}
+                "slots": len(self.slots), "resident_gb": self.resident / 1e9, "slot_scratch_gb": self.held / 1e9,
+                "lw_chunk": self.slots[0].solver.cfg.lw_chunk}
 
 
 def poisson_requests(n: int, rate: float, members: int, seed: int = 7) -> list:

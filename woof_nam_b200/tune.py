@@ -86,10 +86,11 @@ def time_candidates(base: SolverConfig, ncol: int, candidates=CANDIDATES, reps: 
 
 
 def tuned_config(ncol: int, base: SolverConfig | None = None, cache_path: Path = CACHE, timer=None,
-                 device: str | None = None) -> SolverConfig:
+                 device: str | None = None, max_chunk: int | None = None) -> SolverConfig:
     """base (default SolverConfig()) with lw_chunk set to the fastest measured chunk for a request of ncol
-    columns on this device; measured once per cache key and remembered in cache_path.  timer(base, ncol)
-    -> {chunk: ms} replaces the device measurement (tests)."""
+    columns on this device; measured once per cache key and remembered in cache_path.  max_chunk bounds the
+    choice (and so the scratch a handle holds: 95 KB per column of a chunk).  timer(base, ncol) ->
+    {chunk: ms} replaces the device measurement (tests)."""
     base = base or SolverConfig()
     if base.precision != "mixed" or base.parts == "sw":
         return base
@@ -102,4 +103,9 @@ def tuned_config(ncol: int, base: SolverConfig | None = None, cache_path: Path =
         times = (timer or time_candidates)(base, ncol)
         cache[k] = {"lw_chunk": choose(times), "ms": {str(c): t for c, t in times.items()}}
         save_cache(cache, cache_path)
+    if max_chunk is not None:
+        times = {int(c): t for c, t in cache[k]["ms"].items() if int(c) <= max_chunk}
+        if times:
+            return replace(base, lw_chunk=choose(times))
+        return replace(base, lw_chunk=max_chunk)
     return replace(base, lw_chunk=int(cache[k]["lw_chunk"]))
