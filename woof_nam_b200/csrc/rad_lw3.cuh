@@ -10,7 +10,7 @@
 //                      copied after them.  Shared memory is the set-up data only (~32 KB).
 //   lw3_sweep_kernel   one warp per column: lane l carries g-points l, l + 32, ..., l + 128 (five independent
 //                      recurrences interleaved per lane), reading each layer's optical depths as coalesced
-//                      128-byte rows.  Per layer each g-point's radiance CHANGE across the layer is formed
+//                      128-byte rows staged through shared memory by asynchronous copies.  Per layer each g-point's radiance CHANGE across the layer is formed
 //                      directly (source minus radiance x absorptance) and summed over g-points in float64; the
 //                      heating rates come from those changes, not from differences of ~300 W/m^2 level
 //                      fluxes.
@@ -217,20 +217,31 @@ __device__ __forceinline__ R lw3_step(float& rtot, float& rclr, float& trad, flo
     return inc;
 }
 
-// L1 prefetch of one 128-byte line (PTX prefetch.global.L1): the sweeps fetch the next layer's rows and
-// record while the current layer computes, so the scratch's DRAM latency is not paid once per layer.
-__device__ __forceinline__ void lw3_prefetch(const void* p)
+// The sweeps stream each layer's taug row, fracs row and record (400 floats) through a three-stage ring in
+// shared memory with asynchronous 16-byte copies (cp.async.cg: L2 to shared, no L1 allocation), two layers
+// ahead of the one being computed, so the scratch's DRAM latency overlaps the arithmetic.
+constexpr int LW3_STAGE = 2 * LW3_GSTRIDE + LW3_REC;   // floats per stage
+constexpr int LW3_NSTAGE = 3;
+
+__device__ __forceinline__ void lw3_cp16(float* dst, const float* src)
 {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
 
-// Lanes 0..9 prefetch the five 128-byte lines of layer k's taug row and of its fracs row, lanes 10..12 the
-// (up to three) lines of its record.
-__device__ __forceinline__ void lw3_prefetch_layer(const float* tg, const float* fr, const float* aux, int k, int lane)
+// Layer k's rows and record into stage st: 100 16-byte pieces over the warp's lanes, one commit group.
+// Sources are 16-byte aligned: rows start at multiples of 640 bytes and records at multiples of 320 bytes
+// of a 128-byte aligned block.
+__device__ __forceinline__ void lw3_stage_layer(float* st, const float* tg, const float* fr, const float* aux, int k,
+                                                int lane)
 {
-    if (lane < 5) lw3_prefetch(tg + (size_t)(k - 1) * LW3_GSTRIDE + 32 * lane);
-    else if (lane < 10) lw3_prefetch(fr + (size_t)(k - 1) * LW3_GSTRIDE + 32 * (lane - 5));
-    else if (lane < 13) lw3_prefetch(aux + (size_t)k * LW3_REC + 32 * (lane - 10));
+    for (int c = lane; c < LW3_STAGE / 4; c += 32) {
+        const float* src = c < 40   ? tg + (size_t)(k - 1) * LW3_GSTRIDE + 4 * c
+                           : c < 80 ? fr + (size_t)(k - 1) * LW3_GSTRIDE + 4 * (c - 40)
+                                    : aux + (size_t)k * LW3_REC + 4 * (c - 80);
+        lw3_cp16(st + 4 * c, src);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 template <bool MC>
@@ -239,6 +250,7 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
                                                                          LwLut<float> lut)
 {
     __shared__ double fup[LW3_SWEEP_WARPS][NLAY_MAX + 1], fdn[LW3_SWEEP_WARPS][NLAY_MAX + 1];
+    __shared__ __align__(16) float ring[LW3_SWEEP_WARPS][LW3_NSTAGE][LW3_STAGE];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t lc = (int64_t)blockIdx.x * LW3_SWEEP_WARPS + warp;
     if (lc >= nc) return;
@@ -253,7 +265,11 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
     const float* tg = blk;
     const float* fr = blk + (size_t)nlay * LW3_GSTRIDE;
     const float* aux = blk + (size_t)2 * nlay * LW3_GSTRIDE;
-    lw3_prefetch_layer(tg, fr, aux, nlay, lane);
+    // sweep steps: s = 0 .. nlay-1 downward (layer nlay - s), s = nlay .. 2 nlay - 1 upward (layer s - nlay + 1)
+    const int nstep = 2 * nlay;
+    auto layer_of = [&](int st) { return st < nlay ? nlay - st : st - nlay + 1; };
+    lw3_stage_layer(ring[warp][0], tg, fr, aux, layer_of(0), lane);
+    lw3_stage_layer(ring[warp][1], tg, fr, aux, layer_of(1), lane);
     const float eps = 1.0e-6f;
     int gi[LW3_SLOTS], band[LW3_SLOTS];
     float sdif[LW3_SLOTS];
@@ -273,61 +289,67 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
     };
     float radtot[LW3_SLOTS], radclr[LW3_SLOTS], trad[LW3_SLOTS], crad[LW3_SLOTS], rad[LW3_SLOTS];
     // One layer of the sweep for the warp's g-points; returns the warp's float64 sum of the radiance changes.
-    auto layer = [&](int k, bool down) -> double {
-        const float* tgr = tg + (size_t)(k - 1) * LW3_GSTRIDE;
-        const float* frr = fr + (size_t)(k - 1) * LW3_GSTRIDE;
-        const float* r = aux + (size_t)k * LW3_REC;
-        const float clfr = __ldg(r + R_CLDFRC);
-        const bool lst = __float_as_int(__ldg(r + (down ? R_LSTD : R_LSTU))) != 0;
+    auto layer = [&](const float* stg, int k, bool down) -> double {
+        const float* tgr = stg;
+        const float* frr = stg + LW3_GSTRIDE;
+        const float* r = stg + 2 * LW3_GSTRIDE;
+        const float clfr = r[R_CLDFRC];
+        const bool lst = __float_as_int(r[down ? R_LSTD : R_LSTU]) != 0;
         float f[6];
 #pragma unroll
-        for (int i = 0; i < 6; ++i) f[i] = __ldg(r + (down ? R_FACD : R_FACU) + i);
+        for (int i = 0; i < 6; ++i) f[i] = r[(down ? R_FACD : R_FACU) + i];
         double sum = 0.0;
 #pragma unroll
         for (int j = 0; j < LW3_SLOTS; ++j) {
             const int g = gi[j], b = band[j];
             const bool cl = MC ? mask_bit(j, k) : clfr >= eps;
-            const float tcb = __ldg(r + R_TAUCLD + b);
-            const LwTerms<float> t = lw3_terms<float>(lut, __ldg(tgr + g), __ldg(frr + g), __ldg(r + R_PKLAY + b),
-                                                      __ldg(r + R_PKLEVU + b), __ldg(r + R_PKLEVD + b), tcb, sdif[j], cl);
+            const float tcb = r[R_TAUCLD + b];
+            const LwTerms<float> t = lw3_terms<float>(lut, tgr[g], frr[g], r[R_PKLAY + b], r[R_PKLEVU + b],
+                                                      r[R_PKLEVD + b], tcb, sdif[j], cl);
             const float inc = lw3_step<float, MC>(radtot[j], radclr[j], trad[j], crad[j], rad[j], t, down, cl, lst,
                                                   clfr, f, sdif[j] * tcb);
             if (val[j]) sum += (double)inc;
         }
         return warp_sum(sum);
     };
-    // ---- downward sweep
+    // ---- the sweeps: downward, the surface, upward; layer s + 2 is copied in while layer s computes
 #pragma unroll
     for (int j = 0; j < LW3_SLOTS; ++j) { radtot[j] = 0; radclr[j] = 0; trad[j] = 0; crad[j] = 0; rad[j] = 0; }
-    for (int k = nlay; k >= 1; --k) {
-        if (k > 1) lw3_prefetch_layer(tg, fr, aux, k - 1, lane);
-        const double v = layer(k, true);
-        if (lane == 0) fdn[warp][k - 1] = v;          // D(k-1) - D(k), summed over g
-    }
-    // ---- surface: emission and reflection
-    lw3_prefetch_layer(tg, fr, aux, 1, lane);
     double s_tu = 0, s_cu = 0, s_td = 0, s_cd = 0;
+    for (int st = 0; st < nstep; ++st) {
+        if (st + 2 < nstep)
+            lw3_stage_layer(ring[warp][(st + 2) % LW3_NSTAGE], tg, fr, aux, layer_of(st + 2), lane);
+        else
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 2;" ::: "memory");   // this lane's copies of step st have landed
+        __syncwarp();                                            // ... and every lane's
+        if (st == nlay) {
+            // surface: emission and reflection
 #pragma unroll
-    for (int j = 0; j < LW3_SLOTS; ++j) {
-        const int b = band[j];
-        const float semi = __ldg(aux + H_SEMISS + b);
-        const float reflct = 1.0f - semi;
-        const float rad0 = semi * __ldg(fr + gi[j]) * __ldg(aux + H_PKLAY0 + b);
-        const float rtd = radtot[j], rcd = radclr[j];
-        radtot[j] = rad0 + reflct * rtd;
-        radclr[j] = rad0 + reflct * rcd;
-        if (val[j]) {
-            s_tu += (double)radtot[j]; s_cu += (double)radclr[j];
-            s_td += (double)rtd; s_cd += (double)rcd;
+            for (int j = 0; j < LW3_SLOTS; ++j) {
+                const int b = band[j];
+                const float semi = __ldg(aux + H_SEMISS + b);
+                const float reflct = 1.0f - semi;
+                const float rad0 = semi * __ldg(fr + gi[j]) * __ldg(aux + H_PKLAY0 + b);
+                const float rtd = radtot[j], rcd = radclr[j];
+                radtot[j] = rad0 + reflct * rtd;
+                radclr[j] = rad0 + reflct * rcd;
+                if (val[j]) {
+                    s_tu += (double)radtot[j]; s_cu += (double)radclr[j];
+                    s_td += (double)rtd; s_cd += (double)rcd;
+                }
+                trad[j] = 0; crad[j] = 0; rad[j] = 0;
+            }
+            s_tu = warp_sum(s_tu); s_cu = warp_sum(s_cu); s_td = warp_sum(s_td); s_cd = warp_sum(s_cd);
         }
-        trad[j] = 0; crad[j] = 0; rad[j] = 0;
-    }
-    s_tu = warp_sum(s_tu); s_cu = warp_sum(s_cu); s_td = warp_sum(s_td); s_cd = warp_sum(s_cd);
-    // ---- upward sweep
-    for (int k = 1; k <= nlay; ++k) {
-        if (k < nlay) lw3_prefetch_layer(tg, fr, aux, k + 1, lane);
-        const double v = layer(k, false);
-        if (lane == 0) fup[warp][k] = v;              // U(k) - U(k-1), summed over g
+        const bool down = st < nlay;
+        const int k = layer_of(st);
+        const double v = layer(ring[warp][st % LW3_NSTAGE], k, down);
+        if (lane == 0) {
+            if (down) fdn[warp][k - 1] = v;           // D(k-1) - D(k), summed over g
+            else fup[warp][k] = v;                    // U(k) - U(k-1), summed over g
+        }
+        __syncwarp();                                 // the stage is free for the copy two steps on
     }
     double t_tu = 0, t_cu = 0;
 #pragma unroll
