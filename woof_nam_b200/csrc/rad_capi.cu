@@ -420,7 +420,7 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
             for (int64_t c0 = 0; c0 < ntot; c0 += lwc) {
                 const int64_t nc = std::min(lwc, ntot - c0);
                 RAD_CUDA(h, cudaMemsetAsync(h->d_lw3list, 0, sizeof(int), st));
-                lw3_optics_kernel<<<(unsigned)nc, LW_THREADS, smem1, st>>>(bt, c0, h->d_lw3, h->d_lw3list, h->d_err);
+                lw3_optics_kernel<<<(unsigned)nc, LW3_OPT_THREADS, smem1, st>>>(bt, c0, h->d_lw3, h->d_lw3list, h->d_err);
                 const unsigned g2 = (unsigned)((nc + LW3_SWEEP_WARPS - 1) / LW3_SWEEP_WARPS);
                 if (mc) {
                     lw3_sweep_kernel<true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);

@@ -59,7 +59,10 @@ __host__ __device__ constexpr int64_t lw3_block_floats(int nlay)
     return (int64_t)2 * nlay * LW3_GSTRIDE + lw3_rec_floats(nlay);
 }
 
-__global__ void __launch_bounds__(LW_THREADS, 3) lw3_optics_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
+constexpr int LW3_OPT_THREADS = 160;   // optics CTA: 5 warps
+constexpr int LW3_OPT_MINB = 3;        // CTAs per SM the optics kernel is compiled for
+
+__global__ void __launch_bounds__(LW3_OPT_THREADS, LW3_OPT_MINB) lw3_optics_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
                                                                    float* __restrict__ scr, int* fp64list, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -77,17 +80,17 @@ __global__ void __launch_bounds__(LW_THREADS, 3) lw3_optics_kernel(const __grid_
     float* blk = scr + (int64_t)blockIdx.x * lw3_block_floats(nlay);
     float* tgo = blk;
     float* fro = blk + (size_t)nlay * LW3_GSTRIDE;
-    lw_setup_core<float, LW_THREADS>(s, a, col, tid, [&](int g, int k0, float tg, float fr) {
+    lw_setup_core<float, LW3_OPT_THREADS>(s, a, col, tid, [&](int g, int k0, float tg, float fr) {
         tgo[k0 * LW3_GSTRIDE + g] = tg;
         fro[k0 * LW3_GSTRIDE + g] = fr;
     });
     float* aux = blk + (size_t)2 * nlay * LW3_GSTRIDE;
-    for (int i = tid; i < nlay * 64; i += LW_THREADS) {
+    for (int i = tid; i < nlay * 64; i += LW3_OPT_THREADS) {
         const int k = 1 + (i >> 6), w = i & 63, b = w & 15;
         float* r = aux + (size_t)k * LW3_REC;
         r[w] = w < 16 ? s.pklay[k][b] : w < 32 ? s.pklev[k][b] : w < 48 ? s.pklev[k - 1][b] : s.taucld[b][k - 1];
     }
-    for (int k = 1 + tid; k <= nlay; k += LW_THREADS) {
+    for (int k = 1 + tid; k <= nlay; k += LW3_OPT_THREADS) {
         float* r = aux + (size_t)k * LW3_REC;
         r[R_CLDFRC] = s.cldfrc[k];
         r[R_LSTU] = __int_as_float(s.lstu[k]);
