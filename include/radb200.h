@@ -191,6 +191,28 @@ typedef struct {
 int rad_post_outputs(RadHandle* h, const RadPostIn* in, const RadPostOut* out, int64_t ncol, int32_t lm,
                      int32_t kd, int32_t cloud_block, int32_t lw_step, void* stream);
 
+/* RDTEMP, the radiative temperature change of every model step (rdtemp_apply, namgpu/kernels/
+ * drv_rdtemp.cu:140-198; module_RA_GFDL.F90:116-233): the solar zenith cosine CZEN of this step on the
+ * tile, and T += (RSWTT x CZEN / CZMEAN + RLWTT) x DT on the interior, every level.  Arrays [level][jm][im]
+ * or [jm][im], float32, device pointers; limits 1-based inclusive as in the loop-limit table. */
+typedef struct {
+    int32_t ntsd;                /* step counter */
+    float dt;                    /* model step, s */
+    int32_t julday, julyr, ihrst, leap_seen;   /* start day of year, year, hour; sticky leap flag */
+    const float* glat;           /* [jm][im] latitude, radians */
+    const float* glon;           /* [jm][im] longitude, radians */
+    const float* czmean;         /* [jm][im] mean cos(zenith) of the last SW call (CZMEAN) */
+    const float* rswtt;          /* [lm][jm][im] SW heating, K/s (RSWTT) */
+    const float* rlwtt;          /* [lm][jm][im] LW heating, K/s (RLWTT) */
+    float* czen;                 /* [jm][im] out: cos(zenith) of this step, on the tile */
+    float* t;                    /* [lm][jm][im] in/out: temperature, on the interior */
+    int32_t im, jm, lm;
+    int32_t its, ite, jts, jte;              /* tile */
+    int32_t its_b1, ite_b1, jts_b1, jte_b1;  /* interior (T update) */
+} RadRdtemp;
+
+int rad_rdtemp(RadHandle* h, const RadRdtemp* p, void* stream);
+
 /* Device-time accounting of the library's own kernels (instrumentation; no counterpart in the reference,
  * which has none).  While enabled, rad_solve records CUDA events on its stream around the LW kernel, the
  * SW day-list kernels and the SW kernel; rad_profile_read waits for the last recorded event and returns

@@ -94,6 +94,9 @@ namespace r_swmc {
 namespace r_post {
 #include "phys_rrtm_driver_post.cu"
 }
+namespace r_rdt {
+#include "drv_rdtemp.cu"
+}
 namespace r_swrad {
 #include "phys_rrtm_sw_swrad.cu"
 }
@@ -1107,6 +1110,19 @@ int ref_post_outputs(int ncol, int lm, int icwp, int lw_step, const float* hlw, 
                                   cldsa, cw, t, cu_cloud, rlwtt, rswtt, cldfra, csmid, rlwin, rswin, rswinc,
                                   rswout, rlwtoa, rswtoa, czmean, sigt4, coszdg, cfracl, cfracm, cfrach, acfrst,
                                   acfrcv, ncfrst, ncfrcv);
+    });
+    return 0;
+}
+
+// RDTEMP from the reference kernel rdtemp_apply (drv_rdtemp.cu:140-198) on the host; lim is the
+// loop-limit table (1-based values at the DL_* slots), one row slab (JOFF = 0).
+int ref_rdtemp(int ntsd, float dt, int julday, int julyr, int ihrst, int leap_seen, const float* glat,
+               const float* glon, float* czen, const float* czmean, float* t, const float* rswtt,
+               const float* rlwtt, int im, int jm, int lm, const int* lim)
+{
+    drv::launch(drv::cdiv((long)im * jm, 128), 1, 1, 128, [&] {
+        r_rdt::rdtemp_apply(ntsd, dt, julday, julyr, ihrst, leap_seen, glat, glon, czen, czmean, t, rswtt, rlwtt,
+                            im, jm, lm, lim, 0);
     });
     return 0;
 }

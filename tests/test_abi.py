@@ -38,7 +38,8 @@ def test_every_declared_symbol_is_exported_and_bound(lib):
 def test_struct_layout_matches_header(tmp_path):
     probe = tmp_path / "probe.c"
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
-    for st in (_lib.RadConfig, _lib.RadColumns, _lib.RadOutputs, _lib.RadProfile, _lib.RadPostIn, _lib.RadPostOut):
+    for st in (_lib.RadConfig, _lib.RadColumns, _lib.RadOutputs, _lib.RadProfile, _lib.RadPostIn, _lib.RadPostOut,
+               _lib.RadRdtemp):
         lines.append(f'printf("{st.__name__} size %zu\\n", sizeof({st.__name__}));')
         for f, _ in st._fields_:
             lines.append(f'printf("{st.__name__}.{f} %zu\\n", offsetof({st.__name__}, {f}));')
@@ -48,7 +49,8 @@ def test_struct_layout_matches_header(tmp_path):
     subprocess.run(["gcc", "-std=c11", "-o", str(exe), str(probe)], check=True)
     got = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], capture_output=True, text=True,
                                                                check=True).stdout.splitlines())
-    for st in (_lib.RadConfig, _lib.RadColumns, _lib.RadOutputs, _lib.RadProfile, _lib.RadPostIn, _lib.RadPostOut):
+    for st in (_lib.RadConfig, _lib.RadColumns, _lib.RadOutputs, _lib.RadProfile, _lib.RadPostIn, _lib.RadPostOut,
+               _lib.RadRdtemp):
         assert int(got[f"{st.__name__} size"]) == ctypes.sizeof(st), st.__name__
         for f, _ in st._fields_:
             assert int(got[f"{st.__name__}.{f}"]) == getattr(st, f).offset, f"{st.__name__}.{f}"

@@ -170,3 +170,26 @@ def test_driver_post_equals_oracle():
     for k in driver.POST_OUTPUTS_2D:
         assert np.array_equal(st[k].cpu().numpy().reshape(-1), ref[k.lower()]), k
     assert np.array_equal(st["cldcov"].cpu().numpy().reshape(lm, n), ref["cldcov"])
+
+
+@pytest.mark.gpu
+def test_rdtemp_unit_equals_oracle():
+    """rdtemp_run on a state under the reference's names (GLAT, GLON, CZMEAN, RSWTT, RLWTT, T, CZEN)."""
+    import datetime
+    import torch
+    from oracle import rdtemp
+    im, jm, lm = 40, 30, 12
+    p = rdtemp.make_case(im, jm, lm, 4, ntsd=240, julday=59, julyr=2026, ihrst=6)
+    ref = rdtemp.rdtemp(p)
+    st = State()
+    for name, key in (("GLAT", "glat"), ("GLON", "glon"), ("CZMEAN", "czmean"), ("RSWTT", "rswtt"),
+                      ("RLWTT", "rlwtt"), ("T", "t"), ("CZEN", "czen")):
+        st[name] = torch.from_numpy(np.ascontiguousarray(p[key])).cuda()
+    ctx = SimpleNamespace(st=st, grid=SimpleNamespace(jm=jm, im=im, lm=lm), cfg=None, tables={}, stream=None,
+                          ntimestep=240, dt=p["dt"], start=datetime.datetime(2026, 2, 28, 6))
+    driver.rdtemp_run(ctx)
+    torch.cuda.synchronize()
+    assert ctx.tables["RDTEMP_CAL"] == (59, 2026, 6, 0)
+    assert np.max(np.abs(st["CZEN"].cpu().numpy() - ref["czen"])) < 3e-5      # float angle resolution
+    changed = st["T"].cpu().numpy() != p["t"]
+    assert changed[:, 1:-1, 1:-1].any() and not changed[:, 0, :].any()       # interior only

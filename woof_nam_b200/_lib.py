@@ -64,6 +64,17 @@ class RadPostOut(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in POST_OUT_FIELDS]
 
 
+class RadRdtemp(ctypes.Structure):
+    _fields_ = [("ntsd", ctypes.c_int32), ("dt", ctypes.c_float), ("julday", ctypes.c_int32),
+                ("julyr", ctypes.c_int32), ("ihrst", ctypes.c_int32), ("leap_seen", ctypes.c_int32),
+                ("glat", ctypes.c_void_p), ("glon", ctypes.c_void_p), ("czmean", ctypes.c_void_p),
+                ("rswtt", ctypes.c_void_p), ("rlwtt", ctypes.c_void_p), ("czen", ctypes.c_void_p),
+                ("t", ctypes.c_void_p), ("im", ctypes.c_int32), ("jm", ctypes.c_int32), ("lm", ctypes.c_int32),
+                ("its", ctypes.c_int32), ("ite", ctypes.c_int32), ("jts", ctypes.c_int32), ("jte", ctypes.c_int32),
+                ("its_b1", ctypes.c_int32), ("ite_b1", ctypes.c_int32), ("jts_b1", ctypes.c_int32),
+                ("jte_b1", ctypes.c_int32)]
+
+
 # Every symbol include/radb200.h declares, with its ctypes signature.
 SIGNATURES = {
     "rad_version": ([], ctypes.c_int),
@@ -83,6 +94,7 @@ SIGNATURES = {
                            ctypes.c_void_p], ctypes.c_int),
     "rad_post_outputs": ([ctypes.c_void_p, ctypes.POINTER(RadPostIn), ctypes.POINTER(RadPostOut), ctypes.c_int64,
                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p], ctypes.c_int),
+    "rad_rdtemp": ([ctypes.c_void_p, ctypes.POINTER(RadRdtemp), ctypes.c_void_p], ctypes.c_int),
     "rad_profile_enable": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rad_profile_read": ([ctypes.c_void_p, ctypes.POINTER(RadProfile)], ctypes.c_int),
     "rad_last_error": ([ctypes.c_void_p], ctypes.c_char_p),

@@ -37,6 +37,7 @@ __constant__ int c_sw_ns[15] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94
 #include "rad_lw3.cuh"
 #include "rad_mcica.cuh"
 #include "rad_post.cuh"
+#include "rad_rdtemp.cuh"
 
 using namespace rad;
 
@@ -890,6 +891,23 @@ int rad_post_outputs(RadHandle* h, const RadPostIn* in, const RadPostOut* out, i
                lw_step ? 1 : 0};
     const unsigned grid = (unsigned)((ncol + 255) / 256);
     k_post_outputs<<<grid, 256, 0, (cudaStream_t)stream>>>(a);
+    h->launches += 1;
+    RAD_CUDA(h, cudaGetLastError());
+    return RAD_OK;
+}
+
+int rad_rdtemp(RadHandle* h, const RadRdtemp* p, void* stream)
+{
+    if (!h || !p) return fail(h, RAD_E_INVALID, "rad_rdtemp: null argument");
+    if (p->im < 1 || p->jm < 1 || p->lm < 1) return fail(h, RAD_E_INVALID, "rad_rdtemp: empty grid");
+    if (!p->glat || !p->glon || !p->czmean || !p->rswtt || !p->rlwtt || !p->czen || !p->t)
+        return fail(h, RAD_E_INVALID, "rad_rdtemp: a required pointer is null");
+    if (p->julday < 1 || p->julday > 366) return fail(h, RAD_E_INVALID, "rad_rdtemp: julday out of range");
+    RdtempArgs a{p->ntsd, p->dt, p->julday, p->julyr, p->ihrst, p->leap_seen, p->glat, p->glon, p->czmean,
+                 p->rswtt, p->rlwtt, p->czen, p->t, p->im, p->jm, p->lm, p->its, p->ite, p->jts, p->jte,
+                 p->its_b1, p->ite_b1, p->jts_b1, p->jte_b1};
+    const int64_t n = (int64_t)p->im * p->jm;
+    k_rdtemp<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a);
     h->launches += 1;
     RAD_CUDA(h, cudaGetLastError());
     return RAD_OK;

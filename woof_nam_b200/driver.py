@@ -315,6 +315,53 @@ def driver_post_run(ctx, *, icwp: int = 1, ntimestep: int | None = None, lssav: 
     s.post_outputs(inp, out, lm, kd=0, cloud_block=True, lw_step=lw_step, stream=_stream(ctx))
 
 
+_MONTH = (31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31)
+
+
+def rdtemp_run(ctx) -> None:
+    """Drop-in for drv_rdtemp.run (namgpu/steps/drv_rdtemp.py): the radiative temperature change of every
+    step, one rad_rdtemp launch.  Reads GLAT, GLON, CZMEAN [JM, IM], RSWTT, RLWTT [LM, JM, IM], updates T
+    in place and writes CZEN on the tile.  Calendar (JULDAY, JULYR, start hour, leap flag) from ctx.start,
+    derived once and kept in ctx.tables["RDTEMP_CAL"]; the tile and interior from
+    ctx.tables["drv_loop_limits"] (ITS, ITE, JTS, JTE, ITS_B1, ITE_B1, JTS_B1, JTE_B1, 1-based) when
+    present, else the whole grid and its interior without the edge rows and columns."""
+    unit = "drv-rdtemp"
+    st, g = ctx.st, ctx.grid
+    im, jm, lm = int(g.im), int(g.jm), int(g.lm)
+    tabs = ctx.tables
+    cal = tabs.get("RDTEMP_CAL")
+    if cal is None:
+        s0 = getattr(ctx, "start", None)
+        if s0 is None:
+            raise RuntimeError(f"{unit}: ctx.start (the initial time) is not set")
+        month = list(_MONTH)
+        leap = s0.year % 4 == 0
+        if leap:
+            month[1] = 29
+        cal = (sum(month[: s0.month - 1]) + s0.day, int(s0.year), int(s0.hour), int(leap))
+        tabs["RDTEMP_CAL"] = cal
+    lim = tabs.get("drv_loop_limits") or {"ITS": 1, "ITE": im, "JTS": 1, "JTE": jm, "ITS_B1": 2, "ITE_B1": im - 1,
+                                           "JTS_B1": 2, "JTE_B1": jm - 1}
+    f = _fields(st)
+
+    def need(name, shape):
+        if name not in f:
+            raise KeyError(f"{unit}: ctx.st['{name}'] is missing")
+        t = _as_tensor(f[name], name, unit)
+        if tuple(t.shape) != shape:
+            raise ValueError(f"{unit}: {name} has shape {tuple(t.shape)}, expected {shape}")
+        return t
+
+    czen = _as_tensor(_add(st, "CZEN", (jm, im)) if "CZEN" not in f else f["CZEN"], "CZEN", unit)
+    p = {"ntsd": int(ctx.ntimestep), "dt": float(ctx.dt), "julday": int(cal[0]), "julyr": int(cal[1]),
+         "ihrst": int(cal[2]), "leap_seen": int(cal[3]), "glat": need("GLAT", (jm, im)), "glon": need("GLON", (jm, im)),
+         "czmean": need("CZMEAN", (jm, im)), "rswtt": need("RSWTT", (lm, jm, im)), "rlwtt": need("RLWTT", (lm, jm, im)),
+         "czen": czen, "t": need("T", (lm, jm, im)), "im": im, "jm": jm, "lm": lm,
+         "its": lim["ITS"], "ite": lim["ITE"], "jts": lim["JTS"], "jte": lim["JTE"],
+         "its_b1": lim["ITS_B1"], "ite_b1": lim["ITE_B1"], "jts_b1": lim["JTS_B1"], "jte_b1": lim["JTE_B1"]}
+    _solver(ctx, "both", 1.5, lm + 1).rdtemp(p, stream=_stream(ctx))
+
+
 @contextlib.contextmanager
 def bound_units():
     """Bind the reference's grrad units to this library's column units for the duration of the block."""

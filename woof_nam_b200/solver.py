@@ -227,6 +227,24 @@ class RadSolver:
         _lib.check(self.lib, self.handle, rc, "rad_post_outputs")
         return out
 
+    def rdtemp(self, p: dict, stream=None) -> None:
+        """RDTEMP on the device (rad_rdtemp; rdtemp_apply of the reference, drv_rdtemp.cu:140-198): p holds
+        the scalars of RadRdtemp and the CUDA tensors glat, glon, czmean ([jm, im]), rswtt, rlwtt, t
+        ([lm, jm, im]) and czen ([jm, im]); t and czen are updated in place."""
+        torch = _torch()
+        r = _lib.RadRdtemp()
+        for k, _ in r._fields_:
+            v = p[k]
+            if isinstance(v, torch.Tensor):
+                if not (v.is_cuda and v.dtype == torch.float32 and v.is_contiguous()):
+                    raise TypeError(f"rdtemp: {k} must be a contiguous float32 CUDA tensor")
+                setattr(r, k, v.data_ptr())
+            else:
+                setattr(r, k, v)
+        st = stream if stream is not None else torch.cuda.current_stream()
+        _lib.check(self.lib, self.handle, self.lib.rad_rdtemp(self.handle, ctypes.byref(r), ctypes.c_void_p(st.cuda_stream)),
+                   "rad_rdtemp")
+
     def profile(self, on: bool = True) -> None:
         """Start (or stop) device-time accounting of the library's kernels on this handle."""
         _lib.check(self.lib, self.handle, self.lib.rad_profile_enable(self.handle, int(on)), "rad_profile_enable")
