@@ -49,12 +49,16 @@ typedef struct RadHandle RadHandle;
 typedef struct {
     int32_t nlay;            /* radiation layers, including the extra top layer (61 for 60 model layers) */
     int32_t precision;       /* RAD_PREC_FP64 or RAD_PREC_MIXED */
-    int32_t route;           /* RAD_ROUTE_NAM (rtrnmr + spcvrtc) or RAD_ROUTE_MCICA */
+    int32_t route;           /* RAD_ROUTE_NAM (rtrnmr or rtrn + spcvrtc) or RAD_ROUTE_MCICA */
     int32_t iswmode;         /* SW two-stream: 1 delta-Eddington, 2 PIFM, 3 discrete ordinates */
     int32_t diagnostic;      /* 1: clouds hold optical depth / SSA / asymmetry (ilwcliq = iswcliq = 0) */
     int32_t window_cols;     /* columns per SW MINVAL(laytrop) window, 0 = the whole request */
     int32_t sw_chunk;        /* SW day columns per chunk (reference 32768) */
-    int32_t iovrlw, iovrsw;  /* McICA overlap (0 random, 1 max-random, 2 maximum) */
+    int32_t iovrlw, iovrsw;  /* cloud overlap, 0 random, 1 max-random, 2 maximum.  McICA route: the sub-column
+                                generators' overlap.  NAM route: iovrlw 0 runs rtrn (random overlap,
+                                phys_rrtm_lw_rtrn.cu), 1 or 2 rtrnmr (lwrad's dispatch,
+                                phys_rrtm_lw_lwrad.py:102-111); iovrsw sets swrad's clear-sky view fraction
+                                zcf0 (phys_rrtm_sw_swrad.cu:251-279) */
     int32_t lw_seed0, sw_seed0;   /* McICA permutation seed offsets (ipsdlw0 = 140, ipsdsw0 = 1) */
     float cpathfac;          /* LW cloud-path factor (1.5) */
     int32_t parts;           /* RAD_PART_LW | RAD_PART_SW (default both): which solves rad_solve runs, for

@@ -136,8 +136,9 @@ def set_debug(sw_tau_scale: float = 1.0, which: str = "port") -> None:
     lib(which).orc_set_debug(ctypes.c_double(sw_tau_scale))
 
 
-def sw_stages(cols, which: str = "port", iswmode: int = 2) -> dict:
-    """SW stage outputs (float statements) of the request's day columns, layers surface first."""
+def sw_stages(cols, which: str = "port", iswmode: int = 2, iovrsw: int = 1) -> dict:
+    """SW stage outputs (float statements) of the request's day columns, layers surface first; iovrsw is the
+    overlap of the clear-sky view fraction zcf (0 random, 1 maximum-random, 2 maximum)."""
     L = lib(which)
     nlay, ncol = cols.nlay, cols.ncol
     nday = int((cols.coszen >= np.float32(1e-4)).sum())
@@ -146,7 +147,7 @@ def sw_stages(cols, which: str = "port", iswmode: int = 2) -> dict:
            "ssacw": np.zeros((nday, 14, nlay), np.float32), "asycw": np.zeros((nday, 14, nlay), np.float32),
            "cldfrc": np.zeros((nday, nlay), np.float32), "zcf": np.zeros((nday, 2), np.float32),
            "laytrop": np.zeros(nday, np.int32)}
-    cfg = np.array([iswmode, int(cols.diagnostic_clouds)], dtype=np.int32)
+    cfg = np.array([iswmode, int(cols.diagnostic_clouds), iovrsw], dtype=np.int32)
     keep = {f: _f(getattr(cols, f)) for f in cols.FIELDS}
     rc = L.orc_sw_stages(cfg.ctypes.data_as(_I), ctypes.c_int(nlay), ctypes.c_int(ncol),
                          *[keep[f].ctypes.data_as(_F) for f in ("plyr", "plvl", "tlyr", "tlvl", "qlyr", "olyr",

@@ -83,6 +83,9 @@ namespace r_b16 {
 namespace r_rtrnmr {
 #include "phys_rrtm_lw_rtrnmr.cu"
 }
+namespace r_rtrn {
+#include "phys_rrtm_lw_rtrn.cu"
+}
 namespace r_lwmc {
 #include "phys_rrtm_lw_mcica_subcol.cu"
 }
@@ -227,6 +230,7 @@ struct Req {
     double cpathfac, solcon;
     const float *plyr, *plvl, *tlyr, *tlvl, *qlyr, *olyr, *gasvmr, *clouds, *faerlw, *faersw, *sfcemis, *tsfg,
         *sfcalb, *coszen;
+    int iovrlw = 1, iovrsw = 1;   // lwrad's transfer (0: rtrn, random overlap; > 0: rtrnmr), swrad's zcf0 overlap
 };
 
 // ---------------------------------------------------------------------------------------------- LW
@@ -558,6 +562,49 @@ void run_lw(const Req& q, double* htlw, double* topflw, double* sfcflw)
     FV totuflux(P), totdflux(P), totuclfl(P), totdclfl(P), htr(L), htrcl(L), htrb(16 * L);
     const float heatfac = 9.80665f * 1.0e-2f / 1.0046e3f;
     const float fluxfac = (float)((double)(float)(2.0 * std::asin(1.0)) * 2.0e4);
+    if (q.iovrlw <= 0) {
+        // rtrn (phys_rrtm_lw_rtrn.py:84-108): NAM slot order, layer k (surface first, 1-based) in slot
+        // nlay - k, interface m in slot nlay - m, pklay / pklev as [16][nlay + 1][ncol]
+        const int LM = nlay, LMK = nlp1;
+        if (LM > 60) throw std::runtime_error("the reference's rtrn holds at most 60 layers");
+        FV delp_t(L), cf_t(L), taucld_t(16 * L), taug_t(140 * L), fracs_t(140 * L), pklay_t(P * 16), pklev_t(P * 16),
+            tuf_t(P), tdf_t(P), tuc_t(P), tdc_t(P), htr_t(L), htrcl_t(L), htrb_t(16 * L);
+        for (int k0 = 0; k0 < LM; ++k0)
+            for (int c = 0; c < n; ++c) {
+                const size_t s = (size_t)(LM - 1 - k0) * n + c, f = (size_t)k0 * n + c;
+                delp_t[s] = delp[f];
+                cf_t[s] = cldfrc[(size_t)(k0 + 1) * n + c];
+                for (int ib = 0; ib < 16; ++ib) taucld_t[(size_t)ib * L + s] = taucld[(size_t)ib * L + f];
+                for (int g = 0; g < 140; ++g) {
+                    taug_t[(size_t)g * L + s] = taug[(size_t)g * L + f];
+                    fracs_t[(size_t)g * L + s] = fracs[(size_t)g * L + f];
+                }
+            }
+        for (int m = 0; m <= LM; ++m)
+            for (int ib = 0; ib < 16; ++ib)
+                for (int c = 0; c < n; ++c) {
+                    const size_t s = ((size_t)ib * LMK + (LM - m)) * n + c, f = ((size_t)m * 16 + ib) * n + c;
+                    pklay_t[s] = pklay[f];
+                    pklev_t[s] = pklev[f];
+                }
+        IV ngb(140);
+        for (int b = 0; b < 16; ++b)
+            for (int g = NGB_NS[b]; g < NGB_NS[b + 1]; ++g) ngb[g] = b + 1;
+        launch(cdiv(n, 128), 1, 1, 128, [&] {
+            r_rtrn::phys_rrtm_lw_rtrn(semiss.data(), delp_t.data(), cf_t.data(), taucld_t.data(), taug_t.data(),
+                                      pklay_t.data(), pklev_t.data(), fracs_t.data(), secdiff.data(), ngb.data(),
+                                      tau_tbl.data(), exp_tbl.data(), tfn_tbl.data(), tuf_t.data(), tdf_t.data(),
+                                      tuc_t.data(), tdc_t.data(), htr_t.data(), htrcl_t.data(), htrb_t.data(),
+                                      fluxfac, heatfac, 0, 0, IM, JM, LM);
+        });
+        for (int m = 0; m <= LM; ++m)
+            for (int c = 0; c < n; ++c) {
+                const size_t s = (size_t)(LM - m) * n + c, f = (size_t)m * n + c;
+                totuflux[f] = tuf_t[s]; totdflux[f] = tdf_t[s]; totuclfl[f] = tuc_t[s]; totdclfl[f] = tdc_t[s];
+            }
+        for (int k0 = 0; k0 < LM; ++k0)
+            for (int c = 0; c < n; ++c) htr[(size_t)k0 * n + c] = htr_t[(size_t)(LM - 1 - k0) * n + c];
+    } else {
     launch(cdiv(n, 128), 1, 1, 128, [&] {
         r_rtrnmr::phys_rrtm_lw_rtrnmr_sf(IM, JM, nlay, 0, 0, heatfac, fluxfac, exp_tbl.data(), tfn_tbl.data(),
                                          tau_tbl.data(), semiss.data(), delp.data(), cldfrc.data(), taucld.data(),
@@ -565,6 +612,7 @@ void run_lw(const Req& q, double* htlw, double* topflw, double* sfcflw)
                                          totuflux.data(), totdflux.data(), htr.data(), totuclfl.data(),
                                          totdclfl.data(), htrcl.data(), htrb.data());
     });
+    }
     // lwrad_post
     FV o_top_c(n), o_top_0(n), o_sfc_uc(n), o_sfc_u0(n), o_sfc_dc(n), o_sfc_d0(n), hlwc(L), dum(1);
     launch(cdiv(n, 128), 1, 1, 128, [&] {
@@ -598,7 +646,7 @@ void run_sw_chunk(const Req& q, const IV& idxday, int cstart, int nc, int kminw,
     launch(cdiv(nc, 128), 1, 1, 128, [&] {
         r_swrad::swrad_prep(q.plyr, q.plvl, q.tlyr, q.qlyr, q.olyr, q.gasvmr, q.clouds, faersw.data(), q.coszen,
                             q.sfcalb, icsdsw.data(), idxday.data(), ndayp.data(), cstart, nc, nlay, nlp1, im, jm, 0, 1,
-                            iswcliq, 1, 0, 1, (float)q.solcon, pavel.data(), tavel.data(), delp.data(),
+                            iswcliq, q.iovrsw, 0, 1, (float)q.solcon, pavel.data(), tavel.data(), delp.data(),
                             coldry.data(), colmol.data(), h2ovmr.data(), o3vmr.data(), temcol.data(), colamt.data(),
                             cfrac.data(), cliqp.data(), reliq.data(), cicep.data(), reice.data(), cdat1.data(),
                             cdat2.data(), cdat3.data(), cdat4.data(), tauae.data(), ssaae.data(), asyae.data(),
@@ -1038,7 +1086,7 @@ int orc_sw_stages(const int* cfg_i, int nlay, int ncol, const float* plyr, const
 {
     try {
         drv::Req q{nlay, ncol, cfg_i[1], 0, 1 << 30, cfg_i[0], 1.5, solcon, plyr, plvl, tlyr, tlvl, qlyr, olyr,
-                   gasvmr, clouds, nullptr, nullptr, nullptr, nullptr, sfcalb, coszen};
+                   gasvmr, clouds, nullptr, nullptr, nullptr, nullptr, sfcalb, coszen, 1, cfg_i[2]};
         drv::g_cap = drv::SwCapture{taug, taur, sfluxzen, taucw, ssacw, asycw, cldfrc, zcf, laytrop, true};
         std::vector<double> h((size_t)nlay * ncol), t3(3 * (size_t)ncol), s4(4 * (size_t)ncol);
         drv::run_sw(q, h.data(), t3.data(), s4.data(), nullptr);
@@ -1069,7 +1117,8 @@ int orc_add_itable(const char* name, const int* data, long n)
 }
 
 // Same entry as the restatement's (oracle/rrtm_oracle.cpp); the reference kernels are float32 only, the
-// McICA route and the optional profiles are not driven here.
+// McICA route and the optional profiles are not driven here.  iovrlw <= 0 runs the reference's rtrn, which
+// holds at most 60 layers (phys_rrtm_lw_rtrn.py:60).
 int orc_solve(int precision, const int* cfg_i, double cpathfac, int nlay, int ncol, const float* plyr,
               const float* plvl, const float* tlyr, const float* tlvl, const float* qlyr, const float* olyr,
               const float* gasvmr, const float* clouds, const float* faerlw, const float* faersw,
@@ -1082,7 +1131,8 @@ int orc_solve(int precision, const int* cfg_i, double cpathfac, int nlay, int nc
     try {
         if (cfg_i[4] != 0) throw std::runtime_error("the reference driver runs the NAM route only");
         drv::Req q{nlay, ncol, cfg_i[1], cfg_i[2], cfg_i[3] > 0 ? cfg_i[3] : 32768, cfg_i[0], cpathfac, solcon,
-                   plyr, plvl, tlyr, tlvl, qlyr, olyr, gasvmr, clouds, faerlw, faersw, sfcemis, tsfg, sfcalb, coszen};
+                   plyr, plvl, tlyr, tlvl, qlyr, olyr, gasvmr, clouds, faerlw, faersw, sfcemis, tsfg, sfcalb, coszen,
+                   cfg_i[5], cfg_i[6]};
         drv::run_lw(q, htlw, topflw, sfcflw);
         drv::run_sw(q, htsw, topfsw, sfcfsw, fdncmp);
     } catch (const std::exception& e) {

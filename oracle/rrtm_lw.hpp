@@ -6,6 +6,7 @@
 //   setcoef           namgpu/kernels/phys_rrtm_lw_setcoef.cu:82-244
 //   taumol bands      namgpu/kernels/phys_rrtm_lw_taugb01.cu .. taugb16.cu (+ tautot, lw_core.py:83-90)
 //   rtrnmr            namgpu/kernels/phys_rrtm_lw_rtrnmr_body.cuh:9-365 (surface-first variant)
+//   rtrn              namgpu/kernels/phys_rrtm_lw_rtrn.cu:94-330 (random overlap, iovrlw = 0)
 //   lwrad_post        namgpu/kernels/phys_rrtm_lw_lwrad.cu:316-366
 // and the grrad glue around it (cloud-path factor, phys_rrtm_grrad_lw.cu:58-80).
 // Test infrastructure only: never linked into the product.
@@ -1243,6 +1244,114 @@ void lw_rtrnmr(LwColumn<R>& c, const LwTables<R>& tb, R heatfac, R fluxfac)
     for (int k = 1; k <= nlay; ++k) {
         fnet[k] = tuf[k] - tdf[k];
         c.htr[k - 1] = (fnet[k - 1] - fnet[k]) * rfdelp[k];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// rtrn, random cloud overlap (phys_rrtm_lw_rtrn.cu:94-330; Fortran radlw_main_nmmb.f:2127-2484), the LW
+// transfer of the NAM route when iovrlw = 0; lhlw0 = lhlwb = 0.  Surface-first indices as above (layer k,
+// interface m); the kernel's top-first slot map is a storage order only.  A cloudy layer (clfr >= 1e-6)
+// blends cloud and gas sources by clfr and scales the gas transmittance by the effective clear fraction
+// efclrfr = 1 - (1 - exp(-odcld)) clfr; the clear-sky radiances ignore the cloud.
+template <class R>
+void lw_rtrn(LwColumn<R>& c, const LwTables<R>& tb, R heatfac, R fluxfac)
+{
+    const int nlay = c.nlay, nlp1 = nlay + 1;
+    const R eps = (R)1.0e-6f, bpade = (R)1.0f / (R)0.278f, wtdiff = (R)0.5f, tblint = (R)10000,
+            rec_6 = (R)0.166667f, c06 = (R)0.06f;
+    const R flxfac = wtdiff * fluxfac;
+    auto PKL = [&](int ib, int s) { return c.pklay[(size_t)s * 16 + ib]; };
+    auto PKV = [&](int ib, int s) { return c.pklev[(size_t)s * 16 + ib]; };
+    // layer k terms of g-point ig in band ib (rtrn_layer, phys_rrtm_lw_rtrn.cu:94-164)
+    struct Lay { R trng, gassrcd, gassrcu, efclrfr, totsrcd, totsrcu, clfr; bool cloudy; };
+    auto layer = [&](int k, int ig, int ib) {
+        Lay t{};
+        const R sdif = c.secdiff[ib];
+        R odepth = fmaxR((R)0, sdif * c.TG(ig, k - 1));
+        R atrgas, gasfac;
+        if (odepth <= c06) {
+            atrgas = odepth - (R)0.5f * odepth * odepth;
+            t.trng = (R)1 - atrgas;
+            gasfac = rec_6 * odepth;
+        } else {
+            const R tblind = odepth / (bpade + odepth);
+            const int itgas = (int)(tblint * tblind + (R)0.5f);
+            t.trng = tb.ex[itgas]; atrgas = (R)1 - t.trng; gasfac = tb.tfn[itgas]; odepth = tb.tau[itgas];
+        }
+        const R plfrac = c.FR(ig, k - 1);
+        const R blay = PKL(ib, k);
+        const R dplnku = PKV(ib, k) - blay;
+        const R dplnkd = PKV(ib, k - 1) - blay;
+        t.gassrcd = plfrac * (blay + dplnkd * gasfac) * atrgas;
+        t.gassrcu = plfrac * (blay + dplnku * gasfac) * atrgas;
+        t.clfr = c.cldfrc[k];
+        t.cloudy = t.clfr >= eps;
+        t.efclrfr = 1; t.totsrcd = 0; t.totsrcu = 0;
+        if (t.cloudy) {
+            const R odcld = sdif * c.taucld[(size_t)ib * nlay + (k - 1)];
+            t.efclrfr = (R)1 - ((R)1 - mexp(-odcld)) * t.clfr;
+            const R odtot = odepth + odcld;
+            R totfac, atrtot;
+            if (odtot < c06) {
+                totfac = rec_6 * odtot; atrtot = odtot - (R)0.5f * odtot * odtot;
+            } else {
+                const R tblind = odtot / (bpade + odtot);
+                const int ittot = (int)(tblint * tblind + (R)0.5f);
+                totfac = tb.tfn[ittot]; atrtot = (R)1 - tb.ex[ittot];
+            }
+            t.totsrcd = plfrac * (blay + dplnkd * totfac) * atrtot;
+            t.totsrcu = plfrac * (blay + dplnku * totfac) * atrtot;
+        }
+        return t;
+    };
+    std::vector<R> tuf(nlp1, 0), tdf(nlp1, 0), tuc(nlp1, 0), tdc(nlp1, 0);
+    std::vector<R> bu(nlp1), bd(nlp1), cu(nlp1), cd(nlp1);
+    for (int ib = 0; ib < 16; ++ib) {
+        for (int m = 0; m <= nlay; ++m) { bu[m] = 0; bd[m] = 0; cu[m] = 0; cd[m] = 0; }
+        const R semi = c.semiss[ib], reflct = (R)1 - semi;
+        for (int ig = LW_NS[ib]; ig < LW_NS[ib] + LW_NG[ib]; ++ig) {
+            R radtotd = 0, radclrd = 0;
+            for (int k = nlay; k >= 1; --k) {
+                const Lay t = layer(k, ig, ib);
+                if (t.cloudy)
+                    radtotd = radtotd * t.trng * t.efclrfr + t.gassrcd + t.clfr * (t.totsrcd - t.gassrcd);
+                else
+                    radtotd = radtotd * t.trng + t.gassrcd;
+                bd[k - 1] = bd[k - 1] + radtotd;
+                radclrd = radclrd * t.trng + t.gassrcd;
+                cd[k - 1] = cd[k - 1] + radclrd;
+            }
+            const R rad0 = semi * c.FR(ig, 0) * PKL(ib, 0);
+            R radtotu = rad0 + reflct * radtotd;
+            bu[0] = bu[0] + radtotu;
+            R radclru = rad0 + reflct * radclrd;
+            cu[0] = cu[0] + radclru;
+            for (int k = 1; k <= nlay; ++k) {
+                const Lay t = layer(k, ig, ib);
+                if (t.cloudy)
+                    radtotu = radtotu * t.trng * t.efclrfr + t.gassrcu + t.clfr * (t.totsrcu - t.gassrcu);
+                else
+                    radtotu = radtotu * t.trng + t.gassrcu;
+                bu[k] = bu[k] + radtotu;
+                radclru = radclru * t.trng + t.gassrcu;
+                cu[k] = cu[k] + radclru;
+            }
+        }
+        for (int m = 0; m <= nlay; ++m) {
+            tuf[m] = tuf[m] + bu[m]; tdf[m] = tdf[m] + bd[m];
+            tuc[m] = tuc[m] + cu[m]; tdc[m] = tdc[m] + cd[m];
+        }
+    }
+    for (int m = 0; m <= nlay; ++m) {
+        tuf[m] = tuf[m] * flxfac; tdf[m] = tdf[m] * flxfac; tuc[m] = tuc[m] * flxfac; tdc[m] = tdc[m] * flxfac;
+        c.totuflux[m] = tuf[m]; c.totdflux[m] = tdf[m]; c.totuclfl[m] = tuc[m]; c.totdclfl[m] = tdc[m];
+    }
+    R fprev = tuf[0] - tdf[0];
+    for (int k = 1; k <= nlay; ++k) {
+        const R rfdelp = heatfac / c.delp[k - 1];
+        const R fk = tuf[k] - tdf[k];
+        c.htr[k - 1] = (fprev - fk) * rfdelp;
+        fprev = fk;
     }
 }
 

@@ -52,6 +52,8 @@ static void run_lw(const Config& cfg, const Inputs& in, const Outputs& out)
         if (cfg.route == 1) {
             lw_mcica<R>(c, cl.data(), ilwcliq, cfg, in, col, out.lw_mask);
             lw_rtrnmc(c, tb, heatfac, fluxfac);
+        } else if (cfg.iovrlw <= 0) {       // lwrad's transfer dispatch (phys_rrtm_lw_lwrad.py:102-111)
+            lw_rtrn(c, tb, heatfac, fluxfac);
         } else {
             lw_rtrnmr(c, tb, heatfac, fluxfac);
         }
@@ -136,7 +138,7 @@ static void run_sw(const Config& cfg, const Inputs& in, const Outputs& out)
 #pragma omp parallel for schedule(dynamic, 16)
     for (int d = 0; d < nday; ++d) {
         SwColumn<R> c(nlay);
-        sw_prep(c, in, day[d], iswcliq);
+        sw_prep(c, in, day[d], iswcliq, cfg.iovrsw);
         sw_setcoef(c);
         lt[d] = c.laytrop;
     }
@@ -146,7 +148,7 @@ static void run_sw(const Config& cfg, const Inputs& in, const Outputs& out)
     for (int d = 0; d < nday; ++d) {
         const int col = day[d];
         SwColumn<R> c(nlay);
-        sw_prep(c, in, col, iswcliq);
+        sw_prep(c, in, col, iswcliq, cfg.iovrsw);
         sw_cldprop(c, iswcliq);
         sw_setcoef(c);
         sw_taumol(c, kmin8[d], kminw[d]);
@@ -227,6 +229,7 @@ int orc_sw_stages(const int* cfg_i, int nlay, int ncol, const float* plyr, const
         Config cfg;
         cfg.iswmode = cfg_i[0];
         cfg.diagnostic = cfg_i[1];
+        cfg.iovrsw = cfg_i[2];
         cfg.sw_chunk = 1 << 30;
         Inputs in{plyr, plvl, tlyr, tlvl, qlyr, olyr, gasvmr, clouds, nullptr, nullptr, nullptr, nullptr,
                   sfcalb, coszen, nullptr, solcon, nlay, ncol};
@@ -238,7 +241,7 @@ int orc_sw_stages(const int* cfg_i, int nlay, int ncol, const float* plyr, const
         std::vector<int> lt(nday);
         for (int d = 0; d < nday; ++d) {
             SwColumn<float> c(nlay);
-            sw_prep(c, in, day[d], iswcliq);
+            sw_prep(c, in, day[d], iswcliq, cfg.iovrsw);
             sw_setcoef(c);
             lt[d] = c.laytrop;
         }
@@ -246,7 +249,7 @@ int orc_sw_stages(const int* cfg_i, int nlay, int ncol, const float* plyr, const
         sw_groups(day, lt, cfg, ncol, kmin8, kminw);
         for (int d = 0; d < nday; ++d) {
             SwColumn<float> c(nlay);
-            sw_prep(c, in, day[d], iswcliq);
+            sw_prep(c, in, day[d], iswcliq, cfg.iovrsw);
             sw_cldprop(c, iswcliq);
             sw_setcoef(c);
             sw_taumol(c, kmin8[d], kminw[d]);

@@ -1,7 +1,7 @@
 // rrtm_sw.hpp -- CPU oracle: RRTM shortwave column solve (NAM route: spcvrtc, iswmode 2), serial.
 //
 // Restates the reference's SW chain for one day column:
-//   swrad_prep          namgpu/kernels/phys_rrtm_sw_swrad.cu:127-279 (ivflip 0, iovrsw 1)
+//   swrad_prep          namgpu/kernels/phys_rrtm_sw_swrad.cu:127-279 (ivflip 0, iovrsw 0 / 1 / 2)
 //   cldprop             namgpu/kernels/phys_rrtm_sw_cldprop.cu:76 (iswcliq 1, iswcice 3; or iswcliq 0)
 //   setcoef             namgpu/kernels/phys_rrtm_sw_setcoef.cu:131-191
 //   taumol (sfluxzen)   namgpu/kernels/phys_rrtm_sw_taumol.cu:59-120
@@ -55,7 +55,7 @@ struct SwColumn {
 // ---------------------------------------------------------------------------------------------------
 // swrad_prep (phys_rrtm_sw_swrad.cu:127-279) for one day column.
 template <class R>
-void sw_prep(SwColumn<R>& c, const Inputs& in, int col, int iswcliq)
+void sw_prep(SwColumn<R>& c, const Inputs& in, int col, int iswcliq, int iovrsw = 1)
 {
     const int nlay = c.nlay, N = in.ncol;
     auto IN = [&](const float* a, int lev) { return (R)a[(size_t)lev * N + col]; };
@@ -111,15 +111,22 @@ void sw_prep(SwColumn<R>& c, const Inputs& in, int col, int iswcliq)
             c.cfrac[k0] = CLD(0); c.cdat1[k0] = CLD(1); c.cdat2[k0] = CLD(2); c.cdat3[k0] = CLD(3);
         }
     }
-    // clear-sky view fraction, maximum-random overlap (iovrsw = 1)
+    // clear-sky view fraction (phys_rrtm_sw_swrad.cu:251-279): iovrsw 0 random, 1 maximum-random,
+    // 2 maximum overlap of the layer cloud fractions
     const R ftiny = (R)1.0e-12f, oneminus = (R)1.0f - (R)1.0e-6f;
     R z0 = 1, z1 = 1;
-    for (int k0 = 0; k0 < nlay; ++k0) {
-        const R cf = c.cfrac[k0];
-        if (cf > ftiny) z1 = fminR(z1, (R)1 - cf);
-        else if (z1 < (R)1) { z0 = z0 * z1; z1 = 1; }
+    if (iovrsw == 0) {
+        for (int k0 = 0; k0 < nlay; ++k0) z0 = z0 * ((R)1 - c.cfrac[k0]);
+    } else if (iovrsw == 1) {
+        for (int k0 = 0; k0 < nlay; ++k0) {
+            const R cf = c.cfrac[k0];
+            if (cf > ftiny) z1 = fminR(z1, (R)1 - cf);
+            else if (z1 < (R)1) { z0 = z0 * z1; z1 = 1; }
+        }
+        z0 = z0 * z1;
+    } else if (iovrsw == 2) {
+        for (int k0 = 0; k0 < nlay; ++k0) z0 = fminR(z0, (R)1 - c.cfrac[k0]);
     }
-    z0 = z0 * z1;
     if (z0 <= ftiny) z0 = 0;
     if (z0 > oneminus) z0 = 1;
     c.zcf0 = z0;

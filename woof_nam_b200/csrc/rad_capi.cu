@@ -401,7 +401,7 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
             const RadOutputs* out = outs + r;
             bt.req[r] = LwIn{in->plyr, in->plvl, in->tlyr, in->tlvl, in->qlyr, in->olyr, in->gasvmr, in->clouds,
                              in->faerlw, in->sfcemis, in->tsfg, out->htlw, out->topflw, out->sfcflw, ncols[r], nlay,
-                             cfg.diagnostic, cfg.cpathfac, lwm[r]};
+                             cfg.diagnostic, cfg.cpathfac, lwm[r], cfg.route == RAD_ROUTE_NAM && cfg.iovrlw == 0};
         }
         LwLut<R> lut;
         const R* base = sizeof(R) == 4 ? (const R*)h->d_lwf : (const R*)h->d_lwd;
@@ -424,10 +424,13 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                 lw3_optics_kernel<<<(unsigned)nc, LW3_OPT_THREADS, smem1, st>>>(bt, c0, h->d_lw3, h->d_lw3list, h->d_err);
                 const unsigned g2 = (unsigned)((nc + LW3_SWEEP_WARPS - 1) / LW3_SWEEP_WARPS);
                 if (mc) {
-                    lw3_sweep_kernel<true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                    lw3_sweep_kernel<LW_OVR_MCICA><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
                     h->launches += 2;
                 } else {
-                    lw3_sweep_kernel<false><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                    if (cfg.iovrlw == 0)
+                        lw3_sweep_kernel<LW_OVR_RANDOM><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                    else
+                        lw3_sweep_kernel<LW_OVR_MAXRAN><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
                     lw3_fp64_kernel<<<(unsigned)h->nsm, LW_THREADS, smemd, st>>>(bt, c0, h->d_lw3list, dl, h->d_err);
                     h->launches += 3;
                 }
@@ -482,7 +485,8 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
             const RadOutputs* out = outs + r;
             bt.req[r] = SwIn{in->plyr, in->plvl, in->tlyr, in->qlyr, in->olyr, in->gasvmr, in->clouds, in->faersw,
                              in->sfcalb, in->coszen, sc.daycol, sc.nday, sc.k8, sc.kw, out->htsw, out->topfsw,
-                             out->sfcfsw, out->fdncmp, ncols[r], nlay, cfg.diagnostic, cfg.iswmode, in->solcon, swm[r]};
+                             out->sfcfsw, out->fdncmp, ncols[r], nlay, cfg.diagnostic, cfg.iswmode, in->solcon, swm[r],
+                             cfg.iovrsw};
         }
         if ((mrc = mark_if(2))) return mrc;
         if (sizeof(R) == 4) {
@@ -540,7 +544,7 @@ int rad_create(const RadConfig* cfg, RadHandle** out)
         return fail(nullptr, RAD_E_INVALID, "rad_create: unknown route");
     if (cfg->route == RAD_ROUTE_MCICA && cfg->precision != RAD_PREC_MIXED)
         return fail(nullptr, RAD_E_INVALID, "rad_create: the McICA route runs in the mixed precision");
-    if (cfg->route == RAD_ROUTE_MCICA && (cfg->iovrlw < 0 || cfg->iovrlw > 2 || cfg->iovrsw < 0 || cfg->iovrsw > 2))
+    if (cfg->iovrlw < 0 || cfg->iovrlw > 2 || cfg->iovrsw < 0 || cfg->iovrsw > 2)
         return fail(nullptr, RAD_E_INVALID, "rad_create: iovrlw and iovrsw must be 0, 1 or 2");
     RadHandle* h = new RadHandle();
     h->cfg = *cfg;

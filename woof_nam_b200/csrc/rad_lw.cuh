@@ -523,6 +523,7 @@ struct LwIn {
     int nlay, diagnostic;
     float cpathfac;
     const uint32_t* mask;     // McICA route: sub-column cloud words [5][nlay][ncol] (null: NAM route)
+    int rnd;                  // NAM route: 1 = random cloud overlap (rtrn, iovrlw 0), 0 = maximum-random (rtrnmr)
 };
 
 // ------------------------------------------------------------------------------------------------------
@@ -904,7 +905,7 @@ __device__ __forceinline__ void lw_setup(LwShared<R>& s, const LwIn& a, int64_t 
 using LwBatch = ReqBatch<LwIn>;
 
 // The whole LW column gc (of the launch's concatenated column space) by one CTA: set-up, gas optics and the
-// rtrnmr sweeps with one g-point per thread.  R = double is the plain FP64 kernel.
+// rtrnmr sweeps (rtrn when a.rnd) with one g-point per thread.  R = double is the plain FP64 kernel.
 template <class R>
 __device__ __forceinline__ void lw_column_body(const LwBatch& bt, const LwLut<R>& lut, int* err, int64_t gc)
 {
@@ -922,7 +923,8 @@ __device__ __forceinline__ void lw_column_body(const LwBatch& bt, const LwLut<R>
     }
     lw_setup<R, LW_THREADS>(s, a, col, tid);
     const R eps = (R)1.0e-6f;
-    // ---- phase C: rtrnmr sweeps, one g-point per lane
+    const bool rnd = a.rnd != 0;
+    // ---- phase C: rtrnmr (or rtrn) sweeps, one g-point per lane
     const int warp = tid >> 5, lane = tid & 31;
     const int g = tid;
     const bool act = g < LW_NGPT;
@@ -954,9 +956,10 @@ __device__ __forceinline__ void lw_column_body(const LwBatch& bt, const LwLut<R>
             gassrcu[k] = plfrac * (blay + dplnku * gasfac) * atrgas;
             trngas[k] = trng;
             const R clfr = s.cldfrc[k];
-            if (s.lstd[k]) { totradd = clfr * radtotd; clrradd = radtotd - totradd; rad = 0; }
+            if (s.lstd[k] && !rnd) { totradd = clfr * radtotd; clrradd = radtotd - totradd; rad = 0; }
             if (clfr >= eps) {
-                const R odtot = odepth + sdif * s.taucld[band][k - 1];
+                const R odcld = sdif * s.taucld[band][k - 1];
+                const R odtot = odepth + odcld;
                 R totfac, atrtot, trnt;
                 if (odtot < c06) {
                     totfac = rec_6 * odtot; atrtot = odtot - (R)0.5f * odtot * odtot; trnt = (R)1 - atrtot;
@@ -967,6 +970,16 @@ __device__ __forceinline__ void lw_column_body(const LwBatch& bt, const LwLut<R>
                 }
                 const R totsrcd = plfrac * (blay + dplnkd * totfac) * atrtot;
                 totsrcu[k] = plfrac * (blay + dplnku * totfac) * atrtot;
+                if (rnd) {
+                    // rtrn (phys_rrtm_lw_rtrn.cu:141-142, 232-233): the cloud fraction blends the cloudy and gas
+                    // sources; trntot holds the effective clear fraction for the upward sweep
+                    const R efclrfr = (R)1 - ((R)1 - rexp(-odcld)) * clfr;
+                    trntot[k] = efclrfr;
+                    radtotd = radtotd * trng * efclrfr + gassrcd + clfr * (totsrcd - gassrcd);
+                    radclrd = radclrd * trng + gassrcd;
+                    dn[k - 1] = radtotd;
+                    continue;
+                }
                 trntot[k] = trnt;
                 totradd = totradd * trnt + clfr * totsrcd;
                 clrradd = clrradd * trng + ((R)1 - clfr) * gassrcd;
@@ -1006,8 +1019,11 @@ __device__ __forceinline__ void lw_column_body(const LwBatch& bt, const LwLut<R>
     for (int k = 1; k <= nlay; ++k) {
         if (act) {
             const R clfr = s.cldfrc[k], trng = trngas[k], gasu = gassrcu[k];
-            if (s.lstu[k]) { totradu = clfr * radtotu; clrradu = radtotu - totradu; rad = 0; }
-            if (clfr >= eps) {
+            if (s.lstu[k] && !rnd) { totradu = clfr * radtotu; clrradu = radtotu - totradu; rad = 0; }
+            if (rnd && clfr >= eps) {
+                radtotu = radtotu * trng * trntot[k] + gasu + clfr * (totsrcu[k] - gasu);
+                radclru = radclru * trng + gasu;
+            } else if (clfr >= eps) {
                 const R trnt = trntot[k], totu = totsrcu[k];
                 totradu = totradu * trnt + clfr * totu;
                 clrradu = clrradu * trng + ((R)1 - clfr) * gasu;

@@ -15,6 +15,11 @@ namespace rad {
 
 constexpr int LW2_LANES = 28;   // g-points per warp
 
+// LW cloud-overlap transfer of a sweep: lwrad's dispatch (phys_rrtm_lw_lwrad.py:102-111)
+constexpr int LW_OVR_MAXRAN = 0;   // rtrnmr: NAM route, iovrlw > 0
+constexpr int LW_OVR_MCICA = 1;    // rtrnmc: McICA route
+constexpr int LW_OVR_RANDOM = 2;   // rtrn: NAM route, iovrlw = 0
+
 // Layer k (1-based, surface first) of g-point g: gas and total (cloudy) transmittance and the downward /
 // upward layer sources of rtrnmr (phys_rrtm_lw_rtrnmr_body.cuh:130-190).
 template <class R>
@@ -66,9 +71,12 @@ __device__ __forceinline__ LwTerms<R> lw2_terms(const LwShared<R>& s, const LwLu
     return t;
 }
 
-// MC = false: the NAM route (rtrnmr, maximum-random overlap of the layer cloud fractions).
+// MC = false: the NAM route, rtrnmr (maximum-random overlap of the layer cloud fractions), or rtrn when
+// a.rnd (random overlap, phys_rrtm_lw_rtrn.cu:94-330): a layer with cloud fraction clfr >= 1e-6 scales the
+// gas transmittance by the effective clear fraction 1 - (1 - exp(-odcld)) clfr and adds clfr x (cloudy
+// source - gas source).
 // MC = true: the McICA route (rtrnmc, phys_rrtm_lw_rtrnmc.cu:85-310): a layer is cloudy for g-point g
-// when its sub-column bit is set, with effective clear fraction 1 - (1 - exp(-odcld)).
+// when its sub-column bit is set, with effective clear fraction 1 - (1 - exp(-odcld)) -- rtrn with clfr = 1.
 template <class R, bool MC>
 __global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(const __grid_constant__ LwBatch bt, LwLut<R> lut, int* err)
 {
@@ -95,15 +103,17 @@ __global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(const __grid_
     int band = 0;
     while (g >= c_lw_ns[band + 1]) ++band;
     const R sdif = s.secdiff[band];
+    const bool rnd = !MC && a.rnd != 0;
     // ---- downward sweep (top to surface): per level, the warp's sum of the total-sky radiance
     R radtotd = 0, radclrd = 0, totradd = 0, clrradd = 0, rad = 0;
     for (int k = nlay; k >= 1; --k) {
-        if (MC) {
-            const bool cl = (s.mcw[g >> 5][k - 1] >> (g & 31)) & 1u;
+        if (MC || rnd) {
+            const R cf = MC ? (R)1 : s.cldfrc[k];
+            const bool cl = MC ? ((s.mcw[g >> 5][k - 1] >> (g & 31)) & 1u) != 0 : cf >= eps;
             const LwTerms<R> t = lw2_terms(s, lut, g, band, k, sdif, cl);
             if (cl) {
-                const R efclrfr = (R)1 - ((R)1 - rexp(-(sdif * s.taucld[band][k - 1])));
-                radtotd = radtotd * t.trng * efclrfr + t.gassrcd + (t.totsrcd - t.gassrcd);
+                const R efclrfr = (R)1 - ((R)1 - rexp(-(sdif * s.taucld[band][k - 1]))) * cf;
+                radtotd = radtotd * t.trng * efclrfr + t.gassrcd + cf * (t.totsrcd - t.gassrcd);
             } else {
                 radtotd = radtotd * t.trng + t.gassrcd;
             }
@@ -151,12 +161,13 @@ __global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(const __grid_
     R totradu = 0, clrradu = 0;
     rad = 0;
     for (int k = 1; k <= nlay; ++k) {
-        if (MC) {
-            const bool cl = (s.mcw[g >> 5][k - 1] >> (g & 31)) & 1u;
+        if (MC || rnd) {
+            const R cf = MC ? (R)1 : s.cldfrc[k];
+            const bool cl = MC ? ((s.mcw[g >> 5][k - 1] >> (g & 31)) & 1u) != 0 : cf >= eps;
             const LwTerms<R> t = lw2_terms(s, lut, g, band, k, sdif, cl);
             if (cl) {
-                const R efclrfr = (R)1 - ((R)1 - rexp(-(sdif * s.taucld[band][k - 1])));
-                radtotu = radtotu * t.trng * efclrfr + t.gassrcu + (t.totsrcu - t.gassrcu);
+                const R efclrfr = (R)1 - ((R)1 - rexp(-(sdif * s.taucld[band][k - 1]))) * cf;
+                radtotu = radtotu * t.trng * efclrfr + t.gassrcu + cf * (t.totsrcu - t.gassrcu);
             } else {
                 radtotu = radtotu * t.trng + t.gassrcu;
             }

@@ -25,7 +25,8 @@
 // 140..159 unused), then one 80-word record per layer k = 1..nlay holding everything the sweeps read at that
 // layer (so a layer step touches one contiguous record) and a head record (k = 0) for the surface.  The
 // arithmetic of every term and recurrence is that of rad_lw2.cuh (rtrnmr,
-// phys_rrtm_lw_rtrnmr_body.cuh:130-330; rtrnmc, phys_rrtm_lw_rtrnmc.cu:85-310).
+// phys_rrtm_lw_rtrnmr_body.cuh:130-330; rtrnmc, phys_rrtm_lw_rtrnmc.cu:85-310; rtrn,
+// phys_rrtm_lw_rtrn.cu:94-330).
 #pragma once
 #include "rad_lw2.cuh"
 
@@ -170,24 +171,26 @@ __device__ __forceinline__ LwTerms<R> lw3_terms(const LwLut<R>& lut, R taug, R p
     return t;
 }
 
-// One layer of one g-point's sweep in arithmetic R on the float state (radtot, radclr and, on the NAM
-// route, totrad / clrrad / rad of the max-random overlap): the recurrences of rtrnmr / rtrnmc.  Returns the
-// total-sky radiance change across the layer formed directly -- source - radiance x absorptance, per
-// overlap part -- so it keeps its relative precision however small it is beside the radiance.
-// f = the layer's six overlap factors (clr1 cld1 cmb1 cmb2 clr2 cld2), x = sdif x cloud optical depth.
-template <class R, bool MC>
+// One layer of one g-point's sweep in arithmetic R on the float state (radtot, radclr and, with the
+// max-random overlap, totrad / clrrad / rad): the recurrences of rtrnmr, rtrnmc and rtrn (OVR, the
+// LW_OVR_* transfer).  Returns the total-sky radiance change across the layer formed directly -- source -
+// radiance x absorptance, per overlap part -- so it keeps its relative precision however small it is beside
+// the radiance.  f = the layer's six max-random overlap factors (clr1 cld1 cmb1 cmb2 clr2 cld2), x = sdif x
+// cloud optical depth.  rtrnmc is rtrn with a cloud fraction of 1 in its cloudy sub-columns.
+template <class R, int OVR>
 __device__ __forceinline__ R lw3_step(float& rtot, float& rclr, float& trad, float& crad, float& radv,
                                       const LwTerms<R>& t, bool down, bool cl, bool lst, R clfr, const float* f, R x)
 {
     const R src = down ? t.gassrcd : t.gassrcu, tsrc = down ? t.totsrcd : t.totsrcu;
     const R prev = (R)rtot;
     R inc;
-    if (MC) {
+    if (OVR != LW_OVR_MAXRAN) {
         if (cl) {
-            const R efclrfr = (R)1 - ((R)1 - rexp(-x));
-            const R S = src + (tsrc - src);
+            const R cf = OVR == LW_OVR_MCICA ? (R)1 : clfr;
+            const R efclrfr = (R)1 - ((R)1 - rexp(-x)) * cf;
+            const R S = src + cf * (tsrc - src);
             rtot = (float)(prev * t.trng * efclrfr + S);
-            const R cabs = -expm1(-x);             // 1 - efclrfr without the cancellation
+            const R cabs = -expm1(-x) * cf;        // 1 - efclrfr without the cancellation
             inc = S - prev * (t.atrg + cabs - t.atrg * cabs);
         } else {
             rtot = (float)(prev * t.trng + src);
@@ -247,7 +250,7 @@ __device__ __forceinline__ void lw3_stage_layer(float* st, const float* tg, cons
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-template <bool MC>
+template <int OVR>
 __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
                                                                          int64_t nc, const float* __restrict__ scr,
                                                                          LwLut<float> lut)
@@ -305,11 +308,11 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
 #pragma unroll
         for (int j = 0; j < LW3_SLOTS; ++j) {
             const int g = gi[j], b = band[j];
-            const bool cl = MC ? mask_bit(j, k) : clfr >= eps;
+            const bool cl = OVR == LW_OVR_MCICA ? mask_bit(j, k) : clfr >= eps;
             const float tcb = r[R_TAUCLD + b];
             const LwTerms<float> t = lw3_terms<float>(lut, tgr[g], frr[g], r[R_PKLAY + b], r[R_PKLEVU + b],
                                                       r[R_PKLEVD + b], tcb, sdif[j], cl);
-            const float inc = lw3_step<float, MC>(radtot[j], radclr[j], trad[j], crad[j], rad[j], t, down, cl, lst,
+            const float inc = lw3_step<float, OVR>(radtot[j], radclr[j], trad[j], crad[j], rad[j], t, down, cl, lst,
                                                   clfr, f, sdif[j] * tcb);
             if (val[j]) sum += (double)inc;
         }

@@ -54,7 +54,33 @@ struct SwIn {
     int nlay, diagnostic, iswmode;
     float solcon;
     const uint32_t* mask;     // McICA route: sub-column cloud words [4][nlay][ncol] (null: NAM route)
+    int iovr;                 // overlap of the clear-sky view fraction: 0 random, 1 maximum-random, 2 maximum
 };
+
+// Clear-sky view fraction zcf0 of swrad_prep (phys_rrtm_sw_swrad.cu:251-279) from the layer cloud fractions
+// (surface first): the product of clear fractions (random overlap), of the clear fractions of contiguous
+// cloud blocks (maximum-random) or the smallest clear fraction (maximum), then the ftiny / oneminus snaps.
+template <class R, class T>
+__device__ __forceinline__ R sw_zcf0(const T* cfrac, int nlay, int iovr)
+{
+    const R ftiny = (R)1.0e-12f, oneminus = (R)1.0f - (R)1.0e-6f;
+    R z0 = 1, z1 = 1;
+    if (iovr == 0) {
+        for (int k0 = 0; k0 < nlay; ++k0) z0 = z0 * ((R)1 - (R)cfrac[k0]);
+    } else if (iovr == 1) {
+        for (int k0 = 0; k0 < nlay; ++k0) {
+            const R cf = (R)cfrac[k0];
+            if (cf > ftiny) z1 = fminR(z1, (R)1 - cf);
+            else if (z1 < (R)1) { z0 = z0 * z1; z1 = 1; }
+        }
+        z0 = z0 * z1;
+    } else if (iovr == 2) {
+        for (int k0 = 0; k0 < nlay; ++k0) z0 = fminR(z0, (R)1 - (R)cfrac[k0]);
+    }
+    if (z0 <= ftiny) z0 = 0;
+    if (z0 > oneminus) z0 = 1;
+    return z0;
+}
 
 template <class R>
 struct SwLut {
@@ -635,16 +661,7 @@ __global__ void __launch_bounds__(SW_THREADS) sw_column_kernel(const __grid_cons
         s.albdf[0] = (R)__ldg(a.sfcalb + N + col);
         s.albbm[1] = (R)__ldg(a.sfcalb + 2 * N + col);
         s.albdf[1] = (R)__ldg(a.sfcalb + 3 * N + col);
-        const R ftiny = (R)1.0e-12f, oneminus = (R)1.0f - (R)1.0e-6f;
-        R z0 = 1, z1 = 1;
-        for (int k0 = 0; k0 < nlay; ++k0) {
-            const R cf = s.cfrac[k0];
-            if (cf > ftiny) z1 = fminR(z1, (R)1 - cf);
-            else if (z1 < (R)1) { z0 = z0 * z1; z1 = 1; }
-        }
-        z0 = z0 * z1;
-        if (z0 <= ftiny) z0 = 0;
-        if (z0 > oneminus) z0 = 1;
+        const R z0 = sw_zcf0<R>(s.cfrac, nlay, a.iovr);
         s.zcf0 = z0;
         s.zcf1 = (R)1 - z0;
         int lt = nlay;

@@ -614,16 +614,7 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
         s.albdf[0] = __ldg(a.sfcalb + N + col);
         s.albbm[1] = __ldg(a.sfcalb + 2 * N + col);
         s.albdf[1] = __ldg(a.sfcalb + 3 * N + col);
-        const float ftiny = 1.0e-12f, oneminus = 1.0f - 1.0e-6f;
-        float z0 = 1, z1 = 1;
-        for (int k0 = 0; k0 < nlay; ++k0) {
-            const float cf = s.cfrac[k0];
-            if (cf > ftiny) z1 = fminf(z1, 1.0f - cf);
-            else if (z1 < 1.0f) { z0 = z0 * z1; z1 = 1; }
-        }
-        z0 = z0 * z1;
-        if (z0 <= ftiny) z0 = 0;
-        if (z0 > oneminus) z0 = 1;
+        const float z0 = sw_zcf0<float>(s.cfrac, nlay, a.iovr);
         s.zcf0 = z0;
         s.zcf1 = 1.0f - z0;
         int lt = nlay;

@@ -38,8 +38,8 @@ class SolverConfig:
     window_cols: int = 0             # SW MINVAL(laytrop) window in columns (0 = whole request)
     sw_chunk: int = 32768
     cpathfac: float = 1.5
-    iovrlw: int = 1                  # McICA overlap: 0 random, 1 maximum-random, 2 maximum
-    iovrsw: int = 1
+    iovrlw: int = 1                  # cloud overlap, 0 random, 1 maximum-random, 2 maximum: McICA generators;
+    iovrsw: int = 1                  # on the NAM route iovrlw 0 = rtrn (else rtrnmr), iovrsw = swrad's zcf0
     lw_seed0: int = 140              # McICA seed offsets (ipsdlw0, ipsdsw0)
     sw_seed0: int = 1
     parts: str = "both"              # "lw", "sw" or "both": which solves run (lslwr / lsswr steps)
