@@ -3,12 +3,12 @@
 // Same column physics as rad_sw.cuh (swrad prep, cldprop, setcoef, taumol16..29, spcvrtc + swflux,
 // namgpu/kernels/phys_rrtm_sw_*.cu), organised for throughput:
 //
-//  * 256 threads per sunlit column.  Phase A: threads = layers / (band, layer) pairs / bands build the
+//  * 128 threads per sunlit column.  Phase A: threads = layers / (band, layer) pairs / bands build the
 //    layer coefficients, cloud optics and solar source in shared memory.  Phase B: threads = (g, layer)
 //    pairs in g-major order compute the gas and Rayleigh optical depths once (a warp stays inside one
-//    band, so the band switch does not diverge).  Phase C: warps 0-3 run the clear pass and warps 4-7 the
-//    cloudy pass of spcvrtc, one g-point per lane (28/28/30/26 lanes per warp, the Rayleigh-dominated
-//    bands 23-26 grouped in one warp).
+//    band, so the band switch does not diverge).  Phase C: one g-point per lane (28/28/30/26 lanes per
+//    warp, the Rayleigh-dominated bands 23-26 grouped in one warp), each lane carrying the clear and the
+//    cloudy pass of spcvrtc.
 //  * No per-thread layer arrays.  The adding method needs the upward reflectances of every level while
 //    it walks down; the upward sweep keeps only one checkpoint per segment of SEG layers (shared memory),
 //    and the downward sweep recomputes each segment's layer R/T into registers before walking through it.
@@ -23,9 +23,11 @@
 //    and thin layers need no float64.
 //  * Within 1 % of the two-stream resonance k mu0 = 1 the reference's formula divides two small
 //    quantities, clamps 1 - (k mu0)^2 at 1e-8 and compares exp-table entries of two nearly equal depths;
-//    there the layer's optical properties are recomputed from the column inputs in float64 (prep,
-//    setcoef, gas, aerosol and cloud optics) and the reference's statements are evaluated in float64, so
-//    the result follows the reference's own arithmetic (about 0.4 % of the layer evaluations).
+//    there the R/T is evaluated in float64 from the float optical properties, and where a table entry it
+//    takes could differ from the one the float64 optical properties select, the layer's optical properties
+//    are recomputed from the column inputs in float64 (prep, setcoef, gas, aerosol and cloud optics) and
+//    the reference's statements are evaluated in float64 (sw2_exact), so the result follows the
+//    reference's own arithmetic.  Both run inline in the lane that needs them.
 //  * Flux sums over g-points and bands and the heating-rate flux differences are float64.
 #pragma once
 #include "rad_sw.cuh"
@@ -38,8 +40,8 @@ constexpr int SW2_WARPS = 4, SW2_THREADS = 128;
 #endif
 constexpr int SW2_SEG = RAD_SW2_SEG;                              // layers per checkpoint segment
 constexpr int SW2_NSEG = (NLAY_MAX + SW2_SEG - 1) / SW2_SEG;
-constexpr float SW2_RESONANCE = 1.0e-2f;                          // exact recompute where |1-(k mu0)^2| < this
-constexpr int SW2_QCAP = 192;                                     // queued exact recomputes per column
+constexpr float SW2_RESONANCE = 1.0e-2f;                          // float64 R/T where |1-(k mu0)^2| < this
+constexpr double SW2_TBL_MARGIN = 0.01;                           // table-index rounding margin (see sw2_tbl_sure)
 
 // Rain and snow optical coefficients per SW band (phys_rrtm_sw_cldprop.cu): b0r, c0r, b0s, b1s, c0s.
 __constant__ float c_sw_rain_snow[5][14] = {
@@ -357,10 +359,7 @@ struct SwSh2 {
     int laytrop, kmin8, kminw;
     unsigned char low[NLAY_MAX];
     uint32_t mcw[4][NLAY_MAX];                 // McICA route: the column's sub-column cloud words
-    int nexact;                                // layer evaluations queued for the float64 recompute
     int task_next;                             // phase B task counter (for_each_band_pair)
-    int qkey[SW2_QCAP];                        // thread | layer << 8 | cloud << 15
-    float qval[SW2_QCAP][6];                   // their rb, rd, tb, td, e3, e4
 };
 // Dynamic tail: the aerosol block (present only with aerosol inputs) and the segment checkpoints.
 struct SwAer {
@@ -427,31 +426,53 @@ __device__ __noinline__ void sw2_exact(const SwExactCtx& x, int k0, int g, int i
     e4 = sw_expm(t0 * x.snt, x.exd, true);
 }
 
-__device__ __forceinline__ int sw2_qkey(int tid, int k0, bool cloud) { return tid | (k0 << 8) | ((int)cloud << 15); }
+// True when exp(-zb) takes the same entry of the reference's 10,001-entry table (or the same side of its
+// 0.06 expansion switch) for every zb within the float optical properties' rounding: the float64 R/T
+// below gets zb from float optics, whose relative error (~2e-6) moves the rounded table position
+// 10^4 zb / (bpade + zb) + 1/2 by at most ~5e-3.
+__device__ __forceinline__ bool sw2_tbl_sure(double zb)
+{
+    if (zb > 0.06 * (1.0 - 1.0e-5) && zb < 0.06 * (1.0 + 1.0e-5)) return false;
+    if (zb <= 0.06) return true;
+    const double t = 10000.0 * (zb / ((double)1.0f / (double)0.278f + zb)) + 0.5;
+    const double f = t - floor(t);
+    return f > SW2_TBL_MARGIN && f < 1.0 - SW2_TBL_MARGIN;
+}
 
-// One optical-property set of a layer -> R/T and direct transmissions: float, or near the resonance the
-// float64 recompute -- taken from the column's queue, where the pre-pass put it, or done here.
-__device__ __forceinline__ void sw2_rt_mixed(const SwSh2& s, float t0, float tabs, float s0, float y0, float cz,
-                                             float snt, const float* ex, const SwExactCtx& x, int k0, int g, int ib,
-                                             bool cloud, float& rb, float& rd, float& tb, float& td, float& e3,
-                                             float& e4)
+// R/T of a layer near the two-stream resonance in float64 from its float optical properties.  Returns false
+// when the result depends on more than those: a table entry of e1 = exp(-k tau1) or e2 = exp(-tau1 / mu0)
+// that the float rounding could move (the resonance amplifies the neighbouring entry's 1e-4 to ~1e-2), or
+// |1 - (k mu0)^2| within reach of the reference's 1e-8 clamp.
+__device__ __noinline__ bool sw2_rt_double(float t0, float tabs, float s0, float y0, const SwExactCtx& x, float& rb,
+                                           float& rd, float& tb, float& td)
+{
+    const SwPro<double> pd = sw2_prologue<double>((double)t0, (double)tabs, (double)s0, (double)y0, x.mode, x.cz);
+    double a, b, c, d;
+    sw2_rt_tail<double>(pd, x.cz, x.snt, x.exd, a, b, c, d);
+    rb = (float)a; rd = (float)b; tb = (float)c; td = (float)d;
+    return fabs(pd.zrpp) > 1.0e-5 && sw2_tbl_sure(fmin(pd.zrk * pd.ztau1, 500.0)) &&
+           sw2_tbl_sure(fmin(pd.ztau1 * x.snt, 500.0));
+}
+
+// One optical-property set of a layer -> R/T and direct transmissions: float; near the resonance
+// (|1 - (k mu0)^2| < SW2_RESONANCE, where the float R/T loses ~1e-7 / |1 - (k mu0)^2| of relative accuracy)
+// float64 from the float optics; where even that is not decided by the float optics, the float64 recompute
+// of the layer from the column inputs (sw2_exact).
+__device__ __forceinline__ void sw2_rt_mixed(float t0, float tabs, float s0, float y0, float cz, float snt,
+                                             const float* ex, const SwExactCtx& x, int k0, int g, int ib, bool cloud,
+                                             float& rb, float& rd, float& tb, float& td, float& e3, float& e4)
 {
     const SwPro<float> p = sw2_prologue<float>(t0, tabs, s0, y0, x.mode, cz);
     if (fabsf(p.zrpp) < SW2_RESONANCE) {
-        const int key = sw2_qkey(threadIdx.x, k0, cloud);
-        const int nq = min(s.nexact, SW2_QCAP);
-        for (int i = 0; i < nq; ++i)
-            if (s.qkey[i] == key) {
-                rb = s.qval[i][0]; rd = s.qval[i][1]; tb = s.qval[i][2]; td = s.qval[i][3];
-                e3 = s.qval[i][4]; e4 = s.qval[i][5];
-                return;
-            }
-        double a, b, c, d, f3, f4;
-        sw2_exact(x, k0, g, ib, cloud, a, b, c, d, f3, f4);
-        rb = (float)a; rd = (float)b; tb = (float)c; td = (float)d; e3 = (float)f3; e4 = (float)f4;
-        return;
+        if (!sw2_rt_double(t0, tabs, s0, y0, x, rb, rd, tb, td)) {
+            double a, b, c, d, f3, f4;
+            sw2_exact(x, k0, g, ib, cloud, a, b, c, d, f3, f4);
+            rb = (float)a; rd = (float)b; tb = (float)c; td = (float)d; e3 = (float)f3; e4 = (float)f4;
+            return;
+        }
+    } else {
+        sw2_rt_tail<float>(p, cz, snt, ex, rb, rd, tb, td);
     }
-    sw2_rt_tail<float>(p, cz, snt, ex, rb, rd, tb, td);
     e3 = sw_expm(p.ztau1 * snt, ex, true);
     e4 = sw_expm(t0 * snt, ex, true);
 }
@@ -492,7 +513,7 @@ __device__ __noinline__ SwLayerRT2 sw2_layer(const SwSh2& s, const SwAer* aer, c
     float ta = 0, tasa = 0, tay = 0, taab = 0;
     if (aer) { ta = aer->tau[ib][k0]; tasa = aer->tasa[ib][k0]; tay = aer->tay[ib][k0]; taab = aer->tabs[ib][k0]; }
     const float ct0 = fmaxf(1.0e-12f, tr + tg + ta), cs0 = tr + tasa, cy0 = tay, cab = tg + taab;
-    sw2_rt_mixed(s, ct0, cab, cs0, cy0, cz, snt, ex, x, k0, g, ib, false, c.rb, c.rd, c.tb, c.td, c.e3, c.e4);
+    sw2_rt_mixed(ct0, cab, cs0, cy0, cz, snt, ex, x, k0, g, ib, false, c.rb, c.rd, c.tb, c.td, c.e3, c.e4);
     o = c;
     if (cloudy && sw2_cloud_layer(s, mc, g, k0)) {
         {
@@ -500,7 +521,7 @@ __device__ __noinline__ SwLayerRT2 sw2_layer(const SwSh2& s, const SwAer* aer, c
             const float ot0 = ct0 + s.taucw[ib][k0], os0 = cs0 + s.ssacw[ib][k0], oy0 = cy0 + s.asycw[ib][k0];
             const float oab = cab + s.tabsc[ib][k0];
             float rb2, rd2, tb2, td2, e32, e42;
-            sw2_rt_mixed(s, ot0, oab, os0, oy0, cz, snt, ex, x, k0, g, ib, true, rb2, rd2, tb2, td2, e32, e42);
+            sw2_rt_mixed(ot0, oab, os0, oy0, cz, snt, ex, x, k0, g, ib, true, rb2, rd2, tb2, td2, e32, e42);
             if (mc) {
                 o.rb = rb2; o.rd = rd2; o.tb = tb2; o.td = td2; o.e3 = e32; o.e4 = e42;
                 return r;
@@ -623,7 +644,6 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
         s.laytrop = lt;
         s.kmin8 = a.kmin8[d];
         s.kminw = a.kminw[d];
-        s.nexact = 0;
         s.task_next = 0;
     }
     if (a.mask)
@@ -664,42 +684,6 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
     const float ad = ibd ? s.albdf[ibd - 1] : 0.5f * (s.albdf[0] + s.albdf[1]);
     SwExactCtx x{&a, col, s.laytrop, s.kmin8, s.kminw, a.iswmode, (double)__ldg(a.coszen + col),
                  1.0 / (double)__ldg(a.coszen + col), exd};
-    // ---- phase C0: layer evaluations near the two-stream resonance (|1 - (k mu0)^2| < SW2_RESONANCE) are
-    // queued and recomputed in float64 by all threads of the column, instead of by one lane of a warp
-    // while the other lanes wait; the sweeps read them back from the queue.
-    if (act) {
-        for (int k0 = 0; k0 < nlay; ++k0) {
-            const float tr = sw2_taur(s, g, k0), tg = s.taug[g][k0];
-            float ta = 0, tasa = 0, tay = 0, taab = 0;
-            if (aer) { ta = aer->tau[ib0][k0]; tasa = aer->tasa[ib0][k0]; tay = aer->tay[ib0][k0]; taab = aer->tabs[ib0][k0]; }
-            const float ct0 = fmaxf(1.0e-12f, tr + tg + ta), cs0 = tr + tasa, cy0 = tay, cab = tg + taab;
-            if (fabsf(sw2_prologue<float>(ct0, cab, cs0, cy0, x.mode, cz).zrpp) < SW2_RESONANCE) {
-                const int i = atomicAdd(&s.nexact, 1);
-                if (i < SW2_QCAP) s.qkey[i] = sw2_qkey(tid, k0, false);
-            }
-            if (cloudy && sw2_cloud_layer(s, mc, g, k0)) {
-                const float ot0 = ct0 + s.taucw[ib0][k0], os0 = cs0 + s.ssacw[ib0][k0], oy0 = cy0 + s.asycw[ib0][k0];
-                const float oab = cab + s.tabsc[ib0][k0];
-                if (fabsf(sw2_prologue<float>(ot0, oab, os0, oy0, x.mode, cz).zrpp) < SW2_RESONANCE) {
-                    const int i = atomicAdd(&s.nexact, 1);
-                    if (i < SW2_QCAP) s.qkey[i] = sw2_qkey(tid, k0, true);
-                }
-            }
-        }
-    }
-    __syncthreads();
-    for (int i = tid; i < min(s.nexact, SW2_QCAP); i += SW2_THREADS) {
-        const int key = s.qkey[i];
-        const int t = key & 255, k0 = (key >> 8) & 127;
-        bool act_t;
-        const int gt = sw2_lane_g(t, act_t);
-        int ibt = 0;
-        while (gt >= c_sw_ns[ibt + 1]) ++ibt;
-        double v[6];
-        sw2_exact(x, k0, gt, ibt, (key >> 15) != 0, v[0], v[1], v[2], v[3], v[4], v[5]);
-        for (int j = 0; j < 6; ++j) s.qval[i][j] = (float)v[j];
-    }
-    __syncthreads();
     const int nseg = (nlay + SW2_SEG - 1) / SW2_SEG;
     float* ck = ckpt + tid;
     auto CK = [&](int sg, int q) -> float& { return ck[((sg - 1) * 4 + q) * SW2_THREADS]; };
