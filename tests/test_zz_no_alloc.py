@@ -36,8 +36,9 @@ def test_noalloc_equals_solve_twice(precision):
         assert rc == 0, s.lib.rad_last_error(s.handle)
         torch.cuda.synchronize()
         for k, v in ref.items():
-            # the same kernels on the same inputs: equal to the bit (far inside the 0.05 W/m^2 / 0.01 K/day
-            # tolerance of the mixed path)
+            # the same arithmetic on the same inputs (the SW here recomputes its layer R/T where rad_solve
+            # reads them back from its store): equal to the bit, far inside the 0.05 W/m^2 / 0.01 K/day
+            # tolerance of the mixed path
             assert torch.equal(v, got[k]), (precision, n, k)
 
 

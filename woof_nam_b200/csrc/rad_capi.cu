@@ -60,6 +60,7 @@ struct RadHandle {
     float* d_lw3 = nullptr;                        // two-kernel LW: gas optics and sweep inputs of one chunk
     int64_t lw3_cap = 0;                           // columns d_lw3 holds
     int* d_lw3list = nullptr;                      // [1 + lw3_cap]: count, then the chunk's float64 columns
+    float* d_swrt = nullptr;                       // SW layer R/T stores, sw2_rt_floats() per CTA of the SW grid
     int nsm = 148;                                 // SMs of the device (grid of the float64 column kernel)
     std::string err;
     // kernel accounting
@@ -306,6 +307,8 @@ int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
             h->lw3_cap = need;
         }
     }
+    if (h->cfg.precision == RAD_PREC_MIXED && (h->cfg.parts & RAD_PART_SW) && !h->d_swrt)
+        RAD_CUDA(h, cudaMalloc((void**)&h->d_swrt, (size_t)sw2_rt_bytes(h->nsm)));
     if (h->cfg.route == RAD_ROUTE_MCICA && ntot * h->cfg.nlay > h->mask_cap) {
         if (h->d_lwm) cudaFree(h->d_lwm);
         h->d_lwm = nullptr;
@@ -491,8 +494,15 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
         if ((mrc = mark_if(2))) return mrc;
         if (sizeof(R) == 4) {
             const size_t smem = sw2_smem_bytes(any_aer);
-            RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            sw2_column_kernel<<<(unsigned)ntot, SW2_THREADS, smem, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, h->d_err);
+            if (fixed) {   // no scratch: one CTA per sunlit column, R/T recomputed on the way down
+                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                sw2_column_kernel<false><<<(unsigned)ntot, SW2_THREADS, smem, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd,
+                                                                                     h->d_err, nullptr);
+            } else {       // SW2_CTAS_PER_SM CTAs per SM walk the day list, each with its R/T store
+                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                sw2_column_kernel<true><<<(unsigned)(SW2_CTAS_PER_SM * h->nsm), SW2_THREADS, smem, st>>>(
+                    bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, h->d_err, h->d_swrt);
+            }
         } else {
             SwLut<R> lut;
             lut.ex = (const R*)h->d_swd;
@@ -672,6 +682,7 @@ int64_t rad_workspace_bytes(const RadHandle* h, int64_t ncol)
         if (lwc > 0 && (h->cfg.parts & RAD_PART_LW))
             b += std::min(lwc, ncol) * lw3_block_floats(h->cfg.nlay) * (int64_t)sizeof(float);
         if (h->cfg.route == RAD_ROUTE_MCICA) b += 9 * (int64_t)h->cfg.nlay * ncol * (int64_t)sizeof(uint32_t);
+        if (h->cfg.precision == RAD_PREC_MIXED && (h->cfg.parts & RAD_PART_SW)) b += sw2_rt_bytes(h->nsm);
     }
     return b;
 }
@@ -953,7 +964,7 @@ void rad_destroy(RadHandle* h)
     for (void* p : {(void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
                     (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
                     (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub, (void*)h->d_lwm,
-                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list})
+                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt})
         if (p) cudaFree(p);
     delete h;
 }

@@ -11,7 +11,9 @@
 //    cloudy pass of spcvrtc.
 //  * No per-thread layer arrays.  The adding method needs the upward reflectances of every level while
 //    it walks down; the upward sweep keeps only one checkpoint per segment of SEG layers (shared memory),
-//    and the downward sweep recomputes each segment's layer R/T into registers before walking through it.
+//    and the downward sweep rebuilds each segment's upward states from it.  The layer R/T of the upward
+//    sweep go to a per-CTA store in global memory (~340 KB, L2-resident across the grid's CTAs) and the
+//    downward sweep reads them back; without a store (rad_solve_noalloc) it recomputes them.
 //  * Level fluxes are summed over the g-points of a warp in float64 (shuffles) and over warps in a fixed
 //    order: results are bit-reproducible and do not depend on what else runs on the GPU.
 //
@@ -576,13 +578,25 @@ __device__ __forceinline__ int sw2_lane_g(int t, bool& act)
 }
 
 // ------------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(SW2_THREADS, 2)
-sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, const double* exd, int* err)
+// Layer R/T store of one CTA (rad_solve's SW): the upward sweep writes each layer's clear and cloudy
+// rb, rd, tb, td, e3 ([layer][field][thread], coalesced) and each segment's product of the direct-beam
+// transmissions e4 ([segment][pass][thread]); the downward sweep reads them back instead of recomputing the
+// R/T.  The values are the ones the recompute would give, so the outputs do not change.
+constexpr int SW2_RT_FIELDS = 10;
+constexpr int SW2_CTAS_PER_SM = 2;                                 // the kernel's launch bound
+__host__ __device__ constexpr int64_t sw2_rt_floats()
+{
+    return ((int64_t)NLAY_MAX * SW2_RT_FIELDS + (int64_t)SW2_NSEG * 2) * SW2_THREADS;
+}
+inline int64_t sw2_rt_bytes(int nsm) { return (int64_t)SW2_CTAS_PER_SM * nsm * sw2_rt_floats() * (int64_t)sizeof(float); }
+
+// One sunlit column (day index d) by the CTA; STORE: rt = the CTA's R/T store, else the R/T is recomputed.
+template <bool STORE>
+__device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const float* ex, const double* exd,
+                                           int* err, int d, float* rt)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SwSh2& s = *reinterpret_cast<SwSh2*>(smem_raw);
-    const int d = blockIdx.x;
-    if (d >= *bt.req[0].nday) return;
     const int64_t gcol = bt.req[0].daycol[d];
     const int rq = bt.find(gcol);
     const SwIn& a = bt.req[rq];
@@ -689,13 +703,32 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
     auto CK = [&](int sg, int q) -> float& { return ck[((sg - 1) * 4 + q) * SW2_THREADS]; };
     // upward sweep: reflectances of the atmosphere below each level, clear (c) and cloudy (o) passes
     float ubc = ab, udc = ad, ubo = ab, udo = ad;
+    float* const rtl = STORE ? rt + tid : nullptr;
+    auto RT = [&](int k0, int f) -> float& { return rtl[((size_t)k0 * SW2_RT_FIELDS + f) * SW2_THREADS]; };
+    auto RS = [&](int sg, int q) -> float& {
+        return rtl[((size_t)NLAY_MAX * SW2_RT_FIELDS + (size_t)sg * 2 + q) * SW2_THREADS];
+    };
     for (int sg = 0; sg < nseg; ++sg) {
         if (sg > 0) { CK(sg, 0) = ubc; CK(sg, 1) = udc; CK(sg, 2) = ubo; CK(sg, 3) = udo; }
+        float e4c = 1, e4o = 1;
         for (int j = 0; j < SW2_SEG; ++j) {
-            const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, mc, cz, snt, ex);
+            const int k0 = sg * SW2_SEG + j;
+            const SwLayerRT2 L = sw2_layer(s, aer, x, k0, g, ib0, cloudy, mc, cz, snt, ex);
             sw2_up(L.c, ubc, udc);
             if (cloudy) sw2_up(L.o, ubo, udo);
+            if (STORE) {
+                e4c = e4c * L.c.e4;
+                if (cloudy) e4o = e4o * L.o.e4;
+                if (k0 < nlay) {
+                    RT(k0, 0) = L.c.rb; RT(k0, 1) = L.c.rd; RT(k0, 2) = L.c.tb; RT(k0, 3) = L.c.td; RT(k0, 4) = L.c.e3;
+                    if (cloudy) {
+                        RT(k0, 5) = L.o.rb; RT(k0, 6) = L.o.rd; RT(k0, 7) = L.o.tb; RT(k0, 8) = L.o.td;
+                        RT(k0, 9) = L.o.e3;
+                    }
+                }
+            }
         }
+        if (STORE) { RS(sg, 0) = e4c; RS(sg, 1) = e4o; }
     }
     // downward sweep, segment by segment from the top: recompute the segment's R/T and upward states into
     // registers from its checkpoint, then walk down through it
@@ -710,18 +743,43 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
         zubo[0] = sg ? CK(sg, 2) : ab;
         zudo[0] = sg ? CK(sg, 3) : ad;
         float e4c = 1, e4o = 1;
+        if (STORE) {
+            // the segment's R/T from the store (the layers above the model top are transparent)
+#pragma unroll
+            for (int j = 0; j < SW2_SEG; ++j) {
+                const int k0 = sg * SW2_SEG + j;
+                if (k0 < nlay) {
+                    Lc[j].rb = RT(k0, 0); Lc[j].rd = RT(k0, 1); Lc[j].tb = RT(k0, 2); Lc[j].td = RT(k0, 3);
+                    Lc[j].e3 = RT(k0, 4);
+                    if (cloudy) {
+                        Lo[j].rb = RT(k0, 5); Lo[j].rd = RT(k0, 6); Lo[j].tb = RT(k0, 7); Lo[j].td = RT(k0, 8);
+                        Lo[j].e3 = RT(k0, 9);
+                    } else {
+                        Lo[j] = Lc[j];
+                    }
+                } else {
+                    Lc[j].rb = 0; Lc[j].rd = 0; Lc[j].tb = 1; Lc[j].td = 1; Lc[j].e3 = 1;
+                    Lo[j] = Lc[j];
+                }
+                Lc[j].e4 = 1; Lo[j].e4 = 1;
+            }
+            e4c = RS(sg, 0);
+            e4o = RS(sg, 1);
+        }
 #pragma unroll
         for (int j = 0; j < SW2_SEG; ++j) {
-            const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, mc, cz, snt, ex);
-            Lc[j] = L.c;
-            Lo[j] = L.o;
+            if (!STORE) {
+                const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, mc, cz, snt, ex);
+                Lc[j] = L.c;
+                Lo[j] = L.o;
+                e4c = e4c * Lc[j].e4;
+                if (cloudy) e4o = e4o * Lo[j].e4;
+            }
             zubc[j + 1] = zubc[j]; zudc[j + 1] = zudc[j];
             sw2_up(Lc[j], zubc[j + 1], zudc[j + 1]);
-            e4c = e4c * Lc[j].e4;
             if (cloudy) {
                 zubo[j + 1] = zubo[j]; zudo[j + 1] = zudo[j];
                 sw2_up(Lo[j], zubo[j + 1], zudo[j + 1]);
-                e4o = e4o * Lo[j].e4;
             }
         }
 #pragma unroll
@@ -813,6 +871,26 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
             a.fdncmp[4 * N + col] = (float)tot(c[6], t[6]);
             a.fdncmp[5 * N + col] = (float)tot(c[7], t[7]);
         }
+    }
+}
+
+// STORE = false: one CTA per entry of the day list, R/T recomputed in the downward sweep (no scratch).
+// STORE = true: a grid of SW2_CTAS_PER_SM CTAs per SM walks the day list; CTA b keeps its layer R/T in
+// rts + b * sw2_rt_floats().
+template <bool STORE>
+__global__ void __launch_bounds__(SW2_THREADS, SW2_CTAS_PER_SM)
+sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, const double* exd, int* err,
+                  float* rts)
+{
+    const int nday = *bt.req[0].nday;
+    if (!STORE) {
+        if ((int)blockIdx.x < nday) sw2_column<false>(bt, any_aer, ex, exd, err, blockIdx.x, nullptr);
+        return;
+    }
+    float* rt = rts + (int64_t)blockIdx.x * sw2_rt_floats();
+    for (int d = blockIdx.x; d < nday; d += gridDim.x) {
+        sw2_column<true>(bt, any_aer, ex, exd, err, d, rt);
+        __syncthreads();                       // shared memory is reused by the next column
     }
 }
 
