@@ -342,17 +342,20 @@ __device__ __forceinline__ float sw2_rayl_coef(int g)
 }
 
 // ------------------------------------------------------------------------------------------------------
-// Shared memory of one sunlit column.
+// Shared memory of one sunlit column.  Arrays that phase C reads at [g-point or band][layer], with the lanes
+// of a warp on different g-points, have a row stride of NLAY_MAX + 1 words so those lanes fall in different
+// banks.
+constexpr int SW2_KS = NLAY_MAX + 1;
 struct SwSh2 {
     float fac00[NLAY_MAX], fac01[NLAY_MAX], fac10[NLAY_MAX], fac11[NLAY_MAX];
     float selffac[NLAY_MAX], selffrac[NLAY_MAX], forfac[NLAY_MAX], forfrac[NLAY_MAX], colmol[NLAY_MAX];
     float colamt[6][NLAY_MAX];
     int jp[NLAY_MAX], jt[NLAY_MAX], jt1[NLAY_MAX], indself[NLAY_MAX], indfor[NLAY_MAX];
     float cfrac[NLAY_MAX], cldfrc[NLAY_MAX];
-    float taucw[14][NLAY_MAX], ssacw[14][NLAY_MAX], asycw[14][NLAY_MAX], tabsc[14][NLAY_MAX];
-    float taug[SW_NGPT][NLAY_MAX];
+    float taucw[14][SW2_KS], ssacw[14][SW2_KS], asycw[14][SW2_KS], tabsc[14][SW2_KS];
+    float taug[SW_NGPT][SW2_KS];
     float raylc[SW_NGPT];                      // Rayleigh optical depth per unit colmol (band 24: upper atmosphere)
-    float taur24[8][NLAY_MAX];                 // band 24 Rayleigh optical depth below laytrop
+    float taur24[8][SW2_KS];                   // band 24 Rayleigh optical depth below laytrop
     float sfluxzen[SW_NGPT];
     double rdelp[NLAY_MAX];                    // heatfac / delp, float64
     double fn[SW2_WARPS][NLAY_MAX + 2];        // per-warp level sums of zsolar * (down - up), passes combined
@@ -365,7 +368,7 @@ struct SwSh2 {
 };
 // Dynamic tail: the aerosol block (present only with aerosol inputs) and the segment checkpoints.
 struct SwAer {
-    float tau[14][NLAY_MAX], tasa[14][NLAY_MAX], tay[14][NLAY_MAX], tabs[14][NLAY_MAX];
+    float tau[14][SW2_KS], tasa[14][SW2_KS], tay[14][SW2_KS], tabs[14][SW2_KS];
 };
 __host__ __device__ constexpr size_t sw2_ckpt_bytes() { return (size_t)(SW2_NSEG - 1) * 4 * SW2_THREADS * sizeof(float); }
 __host__ __device__ constexpr size_t sw2_smem_bytes(bool aer)
@@ -735,6 +738,20 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
     const double w0 = cloudy ? (mc ? 0.0 : (double)s.zcf0) : 1.0, w1 = cloudy ? (mc ? 1.0 : (double)s.zcf1) : 0.0;
     float tdnc = 1, rdnc = 0, tdbc = 1, tdbc0 = 1, tdno = 1, rdno = 0, tdbo = 1, tdbo0 = 1;
     float toa_c = 0, toa_o = 0;
+    // store path: segment sg's R/T are loaded into pf while segment sg + 1 is walked
+    float pf[SW2_SEG][SW2_RT_FIELDS], pe4c = 1, pe4o = 1;
+    auto fetch = [&](int sg) {
+#pragma unroll
+        for (int j = 0; j < SW2_SEG; ++j) {
+            const int k0 = sg * SW2_SEG + j;
+#pragma unroll
+            for (int f = 0; f < SW2_RT_FIELDS; ++f)
+                pf[j][f] = k0 < nlay && (f < 5 || cloudy) ? RT(k0, f) : 0.0f;
+        }
+        pe4c = RS(sg, 0);
+        pe4o = RS(sg, 1);
+    };
+    if (STORE) fetch(nseg - 1);
     for (int sg = nseg - 1; sg >= 0; --sg) {
         SwLayerRT Lc[SW2_SEG], Lo[SW2_SEG];
         float zubc[SW2_SEG + 1], zudc[SW2_SEG + 1], zubo[SW2_SEG + 1], zudo[SW2_SEG + 1];
@@ -749,11 +766,11 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
             for (int j = 0; j < SW2_SEG; ++j) {
                 const int k0 = sg * SW2_SEG + j;
                 if (k0 < nlay) {
-                    Lc[j].rb = RT(k0, 0); Lc[j].rd = RT(k0, 1); Lc[j].tb = RT(k0, 2); Lc[j].td = RT(k0, 3);
-                    Lc[j].e3 = RT(k0, 4);
+                    Lc[j].rb = pf[j][0]; Lc[j].rd = pf[j][1]; Lc[j].tb = pf[j][2]; Lc[j].td = pf[j][3];
+                    Lc[j].e3 = pf[j][4];
                     if (cloudy) {
-                        Lo[j].rb = RT(k0, 5); Lo[j].rd = RT(k0, 6); Lo[j].tb = RT(k0, 7); Lo[j].td = RT(k0, 8);
-                        Lo[j].e3 = RT(k0, 9);
+                        Lo[j].rb = pf[j][5]; Lo[j].rd = pf[j][6]; Lo[j].tb = pf[j][7]; Lo[j].td = pf[j][8];
+                        Lo[j].e3 = pf[j][9];
                     } else {
                         Lo[j] = Lc[j];
                     }
@@ -763,8 +780,9 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
                 }
                 Lc[j].e4 = 1; Lo[j].e4 = 1;
             }
-            e4c = RS(sg, 0);
-            e4o = RS(sg, 1);
+            e4c = pe4c;
+            e4o = pe4o;
+            if (sg > 0) fetch(sg - 1);
         }
 #pragma unroll
         for (int j = 0; j < SW2_SEG; ++j) {
