@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the uneven-batch leg (parent grid + three nests in one graph-captured launch set)")
     ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
+    ap.add_argument("--no-aer", action="store_true", help="skip the aerosol-optics leg")
     ap.add_argument("--lw-chunk", type=int, default=None,
                     help="LW chunk size (columns); default: the autotuner's choice for this device")
     ap.add_argument("--ncol", type=int, default=None,
@@ -303,6 +304,44 @@ def main():
         graph.close()
         del reqs, graph
 
+    # climatological aerosol optics (setaer / aer_property, NAM iaer = 11) of the same columns: the kernel alone
+    # (HBM roofline: 5 nlay + 4 input words and 90 nlay output words per column), then the radiation step with
+    # aerosol (optics + the solve reading them)
+    aer = None
+    if not args.no_aer:
+        from woof_nam_b200 import aerosols
+        A = aerosols.Aerosols(mixed, month=1)
+        ai = {k: torch.as_tensor(np.ascontiguousarray(v), device=dev)
+              for k, v in aerosols.make_inputs(cols, seed + rank, "nam").items()}
+        da = dict(d)
+        da["faersw"], da["faerlw"] = A.optics(d, ai["rhly"], ai["xlon"], ai["xlat"], ai["slmsk"])
+        opt = lambda: A.optics(d, ai["rhly"], ai["xlon"], ai["xlat"], ai["slmsk"], out=(da["faersw"], da["faerlw"]))  # noqa: E731
+
+        def tstep(fn, steps, warmup):
+            for _ in range(warmup):
+                fn()
+            torch.cuda.synchronize()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            return max_over_ranks(e0.elapsed_time(e1) / steps)
+
+        ms_a = tstep(opt, args.steps, args.warmup)
+        ms_as = tstep(lambda: (opt(), mixed.solve(da, cols.solcon, out)), args.steps, args.warmup)
+        nl = cols.nlay
+        bpc = 4 * ((5 * nl + 1 + 3) + 3 * 30 * nl)
+        hbm = float(peaks().get("hbm_gbs", 6650.0))
+        aer = {"kernel": "k_setaer", "month": 1, "ms": ms_a, "columns_per_s": ws * n / (ms_a * 1e-3),
+               "bytes_per_column": bpc, "achieved_gbs": bpc * n / (ms_a * 1e-3) / 1e9, "peak_gbs": hbm,
+               "frac": bpc * n / (ms_a * 1e-3) / 1e9 / hbm,
+               "step_with_aerosol": {"value": ws * n / (ms_as * 1e-3), "unit": UNIT, "ms_per_step": ms_as}}
+        del da, A
+
     # roofline of the dominant kernel (FP32 pipe; algorithmic FLOPs from the oracle's operation-count table)
     pk = peaks()
     peak_tf, mhz = fp32_peak_tflops(pk)
@@ -355,6 +394,7 @@ def main():
             "e2e": {"value": ws * n / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": in_bytes,
                     "d2h_bytes_per_step": out_bytes, "ms_per_step": ms_e2e},
             "batch_c3": batch,
+            "aerosols": aer,
             "gpu_launches": launches,
             "clocks": clocks,
         }

@@ -217,6 +217,50 @@ typedef struct {
 
 int rad_rdtemp(RadHandle* h, const RadRdtemp* p, void* stream);
 
+/* ---- climatological aerosol optics (NAM iaer = 11: SW and LW aerosol, no volcanic term) ----
+ * The monthly 5-degree OPAC climatology as packed (woof_nam_b200/data/aer_tables.npz from the NAM data file
+ * nam_climaeropac_global.txt), host pointers. */
+typedef struct {
+    const int32_t* iendwv;      /* [61] ending wavenumber of each OPAC band, cm-1 */
+    const float* haer;          /* [7][5] scale height, km, per profile structure and domain */
+    const float* prsref;        /* [7][5] reference pressure of each domain's top, mb */
+    const float* rhid;          /* [4][6][61] extinction, scattering, single-scattering albedo, asymmetry of the
+                                   six humidity-independent species per OPAC band */
+    const float* rhdp;          /* [4][4][8][61] the same of the four humidity-dependent species at 8 humidities */
+    const float* straext0;      /* [61] stratospheric background extinction */
+    const int32_t* nwvns0;      /* [151] wavenumbers of each interval of the solar spectrum */
+    const float* s0intv;        /* [151] solar flux per wavenumber of each interval */
+    const int32_t* month_idx;   /* [37][72][5] component (1..10, 0 = none) of each 5-degree cell of the month */
+    const double* month_cmix;   /* [37][72][5] its mixing ratio */
+    const int32_t* month_kprf;  /* [37][72] profile structure (1..7) */
+    const double* month_denn;   /* [37][72] number density of the mixing layer */
+} RadAerClim;
+
+/* The band tables of one month (aer_init's set_spectrum, clim_aerinit's set_aercoef and optavg, aer_update's
+ * month fill: namgpu/physics/rrtm/phys_rrtm_aer_init.py, phys_rrtm_clim_aerinit.py:196-235,
+ * phys_rrtm_aer_update.py:139-165), built on the host and copied to the handle's device (synchronous; call it
+ * at start-up and at each month change, outside stream capture). */
+int rad_load_aerosols(RadHandle* h, const RadAerClim* c);
+
+/* Column inputs of rad_setaer (device pointers, float32, levels top first). */
+typedef struct {
+    const float* plvl;          /* [nlay + 1][ncol] interface pressure, mb (RAD_PLVL) */
+    const float* plyr;          /* [nlay][ncol] layer pressure, mb (RAD_PLYR) */
+    const float* tlyr;          /* [nlay][ncol] layer temperature, K */
+    const float* qlyr;          /* [nlay][ncol] specific humidity, kg/kg */
+    const float* rhly;          /* [nlay][ncol] layer relative humidity, 0..1 (RAD_RHLY) */
+    const float* xlon;          /* [ncol] longitude, radians (XLON) */
+    const float* xlat;          /* [ncol] latitude, radians (XLAT) */
+    const float* slmsk;         /* [ncol] sea-land mask: 0 sea, 1 land, 2 sea ice (SLMSK) */
+} RadAerColumns;
+
+/* The aerosol optics of ncol columns (setaer with aer_property, ivflip 0: replaces the setaer call of grrad,
+ * namgpu/physics/rrtm/phys_rrtm_grrad_aerosols.py:85-121, phys_rrtm_setaer.py, phys_rrtm_aer_property.py:176):
+ * faersw [3][14][nlay][ncol] and faerlw [3][16][nlay][ncol] (optical depth, single-scattering albedo,
+ * asymmetry per band; the layouts RadColumns.faersw / faerlw take), nlay = the handle's.  Asynchronous on
+ * stream; needs rad_load_aerosols first. */
+int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faersw, float* faerlw, void* stream);
+
 /* Device-time accounting of the library's own kernels (instrumentation; no counterpart in the reference,
  * which has none).  While enabled, rad_solve records CUDA events on its stream around the LW kernel, the
  * SW day-list kernels and the SW kernel; rad_profile_read waits for the last recorded event and returns

@@ -207,3 +207,50 @@ def mcica_masks(cols, which: str = "port", iovrlw: int = 1, iovrsw: int = 1, lw_
     if rc != 0:
         raise RuntimeError("mcica_masks failed")
     return {"lw": lw, "sw": sw}
+
+
+# Derived aerosol tables as orc_aerosols writes them into `tab` (name, element count), in order.
+AER_TAB_FIELDS = (("sigref", 35), ("extrhi", 180), ("scarhi", 180), ("ssarhi", 180), ("asyrhi", 180),
+                  ("extrhd", 960), ("scarhd", 960), ("ssarhd", 960), ("asyrhd", 960), ("extstra", 30),
+                  ("solbnd", 14), ("eirbnd", 16), ("cmixg", 13320), ("denng", 5328), ("idxcg", 13320),
+                  ("kprfg", 2664))
+
+
+def aer_climatology(month: int, path=None) -> dict:
+    """The packed climatology (woof_nam_b200/data/aer_tables.npz) with one month's records (1..12)."""
+    from woof_nam_b200 import aerosols
+    return aerosols.climatology(month, path)
+
+
+def aerosols(clim: dict, cols, aer_in: dict, which: str = "port", tables: bool = False) -> dict:
+    """Aerosol optics of a request: faersw [3][14][nlay][ncol], faerlw [3][16][nlay][ncol] (float32) from the
+    restatement (which="port") or the reference's kernels (which="ref"); with tables=True also the derived
+    tables (AER_TAB_FIELDS)."""
+    L = lib(which)
+    nlay, ncol = cols.nlay, cols.ncol
+    c = {k: np.ascontiguousarray(v) for k, v in clim.items()}
+    ints = {k: np.ascontiguousarray(c[k], dtype=np.int32) for k in ("iendwv", "nwvns0", "month_idx", "month_kprf")}
+    rhid = np.ascontiguousarray(np.stack([c["rhidext0"], c["rhidsca0"], c["rhidssa0"], c["rhidasy0"]]), np.float32)
+    rhdp = np.ascontiguousarray(np.stack([c["rhdpext0"], c["rhdpsca0"], c["rhdpssa0"], c["rhdpasy0"]]), np.float32)
+    f = {k: _f(c[k]) for k in ("haer", "prsref", "straext0", "s0intv")}
+    d = {k: np.ascontiguousarray(c[k], dtype=np.float64) for k in ("month_cmix", "month_denn")}
+    keep = [_f(getattr(cols, k)) for k in ("plvl", "plyr", "tlyr", "qlyr")] + \
+           [_f(aer_in[k]) for k in ("rhly", "xlon", "xlat", "slmsk")]
+    sw = np.zeros((3, 14, nlay, ncol), np.float32)
+    lw = np.zeros((3, 16, nlay, ncol), np.float32)
+    tab = np.zeros(sum(n for _, n in AER_TAB_FIELDS), np.float32) if tables else None
+    p = lambda a, t: a.ctypes.data_as(t) if a is not None else None  # noqa: E731
+    rc = L.orc_aerosols(p(ints["iendwv"], _I), p(f["haer"], _F), p(f["prsref"], _F), p(rhid, _F), p(rhdp, _F),
+                        p(f["straext0"], _F), p(ints["nwvns0"], _I), p(f["s0intv"], _F), p(ints["month_idx"], _I),
+                        p(d["month_cmix"], _D), p(ints["month_kprf"], _I), p(d["month_denn"], _D),
+                        ctypes.c_int(nlay), ctypes.c_int(ncol), *[p(a, _F) for a in keep], p(sw, _F), p(lw, _F),
+                        p(tab, _F))
+    if rc != 0:
+        raise RuntimeError("aerosols failed")
+    out = {"faersw": sw, "faerlw": lw}
+    if tables:
+        o = 0
+        for name, n in AER_TAB_FIELDS:
+            out[name] = tab[o:o + n].copy()
+            o += n
+    return out

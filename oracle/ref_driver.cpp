@@ -103,6 +103,21 @@ namespace r_rdt {
 namespace r_swrad {
 #include "phys_rrtm_sw_swrad.cu"
 }
+namespace r_aeri {
+#include "phys_rrtm_aer_init.cu"
+}
+namespace r_aerc {
+#include "phys_rrtm_clim_aerinit.cu"
+}
+namespace r_aeru {
+#include "phys_rrtm_aer_update.cu"
+}
+namespace r_seta {
+#include "phys_rrtm_setaer.cu"
+}
+namespace r_aerp {
+#include "phys_rrtm_aer_property.cu"
+}
 namespace r_swcld {
 #include "phys_rrtm_sw_cldprop.cu"
 }
@@ -1173,6 +1188,86 @@ int ref_rdtemp(int ntsd, float dt, int julday, int julyr, int ihrst, int leap_se
     drv::launch(drv::cdiv((long)im * jm, 128), 1, 1, 128, [&] {
         r_rdt::rdtemp_apply(ntsd, dt, julday, julyr, ihrst, leap_seen, glat, glon, czen, czmean, t, rswtt, rlwtt,
                             im, jm, lm, lim, 0);
+    });
+    return 0;
+}
+
+// Climatological aerosol optics from the reference's kernels, in the reference's order: aer_init
+// (phys_rrtm_aer_init.py: flags, set_spectrum), clim_aerinit (phys_rrtm_clim_aerinit.py:196-235: bands, then
+// optavg), aer_update's month fill (phys_rrtm_aer_update.py:139-165), setaer (phys_rrtm_setaer.py: zero, prep,
+// then aer_property as phys_rrtm_aer_property.py:176-200 binds it, cmixg / denng cast to float), for the NAM
+// settings iaer 11 (SW and LW on, volcanic off), ivflip 0, one row of ncol columns.  Same signature as the
+// oracle's orc_aerosols.
+int orc_aerosols(const int* iendwv, const float* haer, const float* prsref, const float* rhid, const float* rhdp,
+                 const float* straext0, const int* nwvns0, const float* s0intv, const int* midx, const double* mcmix,
+                 const int* mkprf, const double* mdenn, int nlay, int ncol, const float* plvl, const float* plyr,
+                 const float* tlyr, const float* qlyr, const float* rhly, const float* xlon, const float* xlat,
+                 const float* slmsk, float* aerosw, float* aerolw, float* tab)
+{
+    (void)nwvns0; (void)s0intv;   // the reference kernel carries the solar spectrum itself
+    using FV = std::vector<float>;
+    using IV = std::vector<int>;
+    const int kNAER = 61, kNSW = 14, kNLW = 16, kNBT = 30, kNCM1 = 6, kNCM2 = 4, kNRH = 8, kNDM = 5, kNAE = 7;
+    const int kNCELL = 37 * 72, kNXC = 5;
+    int rip[16] = {0};
+    rip[4] = 11; rip[5] = 1; rip[6] = 1; rip[7] = 0; rip[8] = 0;     // iaerflg, laswflg, lalwflg, lavoflg, iaermdl
+    IV aflags(16, 0);
+    drv::launch(1, 1, 1, 1, [&] { r_aeri::aer_init_flags(rip, aflags.data()); });
+    FV solfwv(57600), eirfwv(4000);
+    drv::launch(drv::cdiv(57600, 128), 1, 1, 128, [&] { r_aeri::aer_init_solfwv(solfwv.data(), aflags.data()); });
+    drv::launch(drv::cdiv(4000, 128), 1, 1, 128, [&] { r_aeri::aer_init_eirfwv(eirfwv.data(), aflags.data()); });
+    FV wsw1(r_seta::SA_WVNSW1, r_seta::SA_WVNSW1 + kNSW), wsw2(r_seta::SA_WVNSW2, r_seta::SA_WVNSW2 + kNSW),
+        wlw1(r_seta::SA_WVNLW1, r_seta::SA_WVNLW1 + kNLW), wlw2(r_seta::SA_WVNLW2, r_seta::SA_WVNLW2 + kNLW);
+    FV sigref(kNAE * kNDM), solbnd(kNSW), solwaer(kNAER * kNSW), eirbnd(kNLW), eirwaer(kNAER * kNLW);
+    IV nv1(kNSW), nv2(kNSW), nr1(kNLW), nr2(kNLW);
+    const int nb1 = kNSW + kNLW + kNAE * kNDM;
+    drv::launch(drv::cdiv(nb1, 128), 1, 1, 128, [&] {
+        r_aerc::clim_aerinit_bands(solfwv.data(), eirfwv.data(), iendwv, wsw1.data(), wsw2.data(), wlw1.data(),
+                                   wlw2.data(), prsref, sigref.data(), solbnd.data(), solwaer.data(), nv1.data(),
+                                   nv2.data(), eirbnd.data(), eirwaer.data(), nr1.data(), nr2.data(), kNSW, kNLW, 1, 1);
+    });
+    const size_t R1 = (size_t)kNCM1 * kNAER, R2 = (size_t)kNCM2 * kNRH * kNAER, ND = (size_t)kNBT * kNCM2 * kNRH;
+    FV extrhi(kNBT * kNCM1), scarhi(kNBT * kNCM1), ssarhi(kNBT * kNCM1), asyrhi(kNBT * kNCM1), extrhd(ND), scarhd(ND),
+        ssarhd(ND), asyrhd(ND), extstra(kNBT);
+    const int nb2 = kNBT * (kNCM1 + kNCM2 * kNRH + 1);
+    drv::launch(drv::cdiv(nb2, 128), 1, 1, 128, [&] {
+        r_aerc::clim_aerinit_optavg(rhid, rhid + R1, rhid + 2 * R1, rhid + 3 * R1, rhdp, rhdp + R2, rhdp + 2 * R2,
+                                    rhdp + 3 * R2, straext0, solbnd.data(), solwaer.data(), nv1.data(), nv2.data(),
+                                    eirbnd.data(), eirwaer.data(), nr1.data(), nr2.data(), extrhi.data(),
+                                    scarhi.data(), ssarhi.data(), asyrhi.data(), extrhd.data(), scarhd.data(),
+                                    ssarhd.data(), asyrhd.data(), extstra.data(), kNSW, kNLW, 1, 1);
+    });
+    IV idxcg(kNCELL * kNXC), kprfg(kNCELL);
+    std::vector<double> cmixd(kNCELL * kNXC), denngd(kNCELL * 2);
+    drv::launch(drv::cdiv(kNCELL, 128), 1, 1, 128, [&] {
+        r_aeru::aer_trop_fill(midx, mcmix, mkprf, mdenn, idxcg.data(), cmixd.data(), denngd.data(), kprfg.data());
+    });
+    FV cmixg(cmixd.begin(), cmixd.end()), denng(denngd.begin(), denngd.end());
+    if (tab) {
+        float* o = tab;
+        auto put = [&](const FV& a) { std::copy(a.begin(), a.end(), o); o += a.size(); };
+        put(sigref); put(extrhi); put(scarhi); put(ssarhi); put(asyrhi); put(extrhd); put(scarhd); put(ssarhd);
+        put(asyrhd); put(extstra); put(solbnd); put(eirbnd); put(cmixg); put(denng);
+        for (int v : idxcg) *o++ = (float)v;
+        for (int v : kprfg) *o++ = (float)v;
+    }
+    if (ncol <= 0) return 0;
+    const int nlp1 = nlay + 1;
+    FV alon(ncol), alat(ncol), dz((size_t)nlay * ncol), hz((size_t)nlp1 * ncol);
+    drv::launch(drv::cdiv(ncol, 128), 1, 1, 128, [&] {
+        r_seta::phys_rrtm_setaer_prep(plvl, plyr, tlyr, qlyr, xlon, xlat, alon.data(), alat.data(), dz.data(),
+                                      hz.data(), ncol, nlay, nlp1, 0, 1);
+    });
+    const size_t nsw = (size_t)3 * kNSW * nlay * ncol, nlw = (size_t)3 * kNLW * nlay * ncol;
+    drv::launch(1, 1, 1, 1, [&] { r_seta::phys_rrtm_setaer_zero(aerosw, aerolw, nsw, nlw); });
+    const float rhlev[8] = {0.0f, 0.5f, 0.7f, 0.8f, 0.9f, 0.95f, 0.98f, 0.99f};
+    drv::launch(drv::cdiv(ncol, 128), 1, 1, 128, [&] {
+        r_aerp::phys_rrtm_aer_property_column(plvl, dz.data(), hz.data(), rhly, alon.data(), alat.data(), slmsk, haer,
+                                              prsref, sigref.data(), rhlev, extrhi.data(), scarhi.data(),
+                                              ssarhi.data(), asyrhi.data(), extrhd.data(), scarhd.data(),
+                                              ssarhd.data(), asyrhd.data(), extstra.data(), cmixg.data(),
+                                              denng.data(), idxcg.data(), kprfg.data(), aerosw, aerolw, ncol, 1, nlay,
+                                              1, 1, 0, kNSW, kNLW, kNBT);
     });
     return 0;
 }

@@ -10,6 +10,7 @@
 #include "rrtm_lw.hpp"
 #include "rrtm_sw.hpp"
 #include "rrtm_mcica.hpp"
+#include "rrtm_aer.hpp"
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -381,3 +382,47 @@ int orc_solve(int precision, const int* cfg_i, double cpathfac, int nlay, int nc
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------------------
+// Climatological aerosol optics of a request (rrtm_aer.hpp).  Same signature as the reference driver's
+// (oracle/ref_driver.cpp, the reference's kernels): the climatology as packed (rhid [4][6][61], rhdp
+// [4][4][8][61], one month's records), columns top first ([level][ncol]; xlon / xlat in radians), outputs
+// aerosw [3][14][nlay][ncol], aerolw [3][16][nlay][ncol] and, when tab is not null, the derived tables
+// (AER_TAB_FIELDS in oracle/oracle.py).
+extern "C" int orc_aerosols(const int* iendwv, const float* haer, const float* prsref, const float* rhid,
+                            const float* rhdp, const float* straext0, const int* nwvns0, const float* s0intv,
+                            const int* midx, const double* mcmix, const int* mkprf, const double* mdenn, int nlay,
+                            int ncol, const float* plvl, const float* plyr, const float* tlyr, const float* qlyr,
+                            const float* rhly, const float* xlon, const float* xlat, const float* slmsk,
+                            float* aerosw, float* aerolw, float* tab)
+{
+    using namespace orc::aer;
+    const Clim c{iendwv, haer, prsref, rhid, rhdp, straext0, nwvns0, s0intv, midx, mcmix, mkprf, mdenn};
+    Tables t;
+    build(c, t);
+    if (tab) {
+        float* o = tab;
+        auto put = [&](const float* a, size_t n) { std::copy(a, a + n, o); o += n; };
+        put(t.sigref, NAE * NDM);
+        put(t.extrhi, NBT * NCM1); put(t.scarhi, NBT * NCM1); put(t.ssarhi, NBT * NCM1); put(t.asyrhi, NBT * NCM1);
+        const size_t nd = (size_t)NBT * NCM2 * NRHLEV;
+        put(t.extrhd, nd); put(t.scarhd, nd); put(t.ssarhd, nd); put(t.asyrhd, nd);
+        put(t.extstra, NBT); put(t.solbnd, NSW); put(t.eirbnd, NLW);
+        put(t.cmixg.data(), t.cmixg.size()); put(t.denng.data(), t.denng.size());
+        for (int v : t.idxcg) *o++ = (float)v;
+        for (int v : t.kprfg) *o++ = (float)v;
+    }
+    if (ncol <= 0) return 0;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int col = 0; col < ncol; ++col) {
+        std::vector<float> pi(nlay + 1), pl(nlay), tl(nlay), ql(nlay), rh(nlay);
+        for (int k = 0; k <= nlay; ++k) pi[k] = plvl[(size_t)k * ncol + col];
+        for (int k = 0; k < nlay; ++k) {
+            pl[k] = plyr[(size_t)k * ncol + col]; tl[k] = tlyr[(size_t)k * ncol + col];
+            ql[k] = qlyr[(size_t)k * ncol + col]; rh[k] = rhly[(size_t)k * ncol + col];
+        }
+        column(t, c, nlay, pi.data(), pl.data(), tl.data(), ql.data(), rh.data(), xlon[col], xlat[col], slmsk[col],
+               aerosw + col, aerolw + col, (size_t)ncol);
+    }
+    return 0;
+}

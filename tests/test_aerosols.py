@@ -1,0 +1,77 @@
+"""The climatological aerosol optics (setaer / aer_property, NAM iaer = 11) in the oracle, pinned to the
+reference's own kernels: the float restatement reproduces the golden vectors of aer_init, clim_aerinit,
+aer_update's month fill, setaer and aer_property bit for bit, and the packed climatology has the shape and
+ranges the kernels assume."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from woof_nam_b200 import aerosols
+from woof_nam_b200.columns import Columns, make_columns
+
+GOLDEN = Path(__file__).resolve().parent / "golden" / "aer_golden.npz"
+CASES = ("jan_nam", "jul_globe")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLDEN)
+
+
+def golden_request(z, case):
+    """(month, a Columns carrying plvl / plyr / tlyr / qlyr, the aerosol inputs)."""
+    base = make_columns(z[f"{case}_in_plyr"].shape[1], 1)
+    kw = {f: getattr(base, f) for f in Columns.FIELDS}
+    for k in ("plvl", "plyr", "tlyr", "qlyr"):
+        kw[k] = z[f"{case}_in_{k}"]
+    ai = {k: z[f"{case}_in_{k}"] for k in ("rhly", "xlon", "xlat", "slmsk")}
+    return int(z[f"{case}_in_month"][0]), Columns(**kw), ai
+
+
+def test_packed_climatology():
+    c = aerosols.climatology(3)
+    assert c["month_idx"].shape == (37, 72, 5) and c["month_kprf"].shape == (37, 72)
+    assert c["month_kprf"].min() >= 1 and c["month_kprf"].max() <= 7
+    assert c["month_idx"].min() >= 0 and c["month_idx"].max() <= 10
+    assert int(c["nwvns0"].sum()) == 57600 and c["iendwv"].shape == (61,)
+    assert np.all(np.diff(c["iendwv"]) > 0)
+    with pytest.raises(ValueError):
+        aerosols.climatology(13)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_tables_bit_exact(gold, case):
+    month, cols, ai = golden_request(gold, case)
+    r = oracle.aerosols(aerosols.climatology(month), cols, ai, tables=True)
+    for name, _ in oracle.AER_TAB_FIELDS:
+        assert np.array_equal(r[name], gold[f"{case}_tab_{name}"]), name
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_optics_bit_exact(gold, case):
+    month, cols, ai = golden_request(gold, case)
+    r = oracle.aerosols(aerosols.climatology(month), cols, ai)
+    assert np.array_equal(r["faersw"], gold[f"{case}_faersw"])
+    assert np.array_equal(r["faerlw"], gold[f"{case}_faerlw"])
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_optics_ranges(gold, case):
+    for k in ("faersw", "faerlw"):
+        a = gold[f"{case}_{k}"]
+        assert np.isfinite(a).all()
+        assert (a[0] >= 0).all() and a[0].max() > 0            # optical depth
+        assert ((a[1] >= 0) & (a[1] <= 1)).all()                # single-scattering albedo
+        assert ((a[2] >= 0) & (a[2] <= 1)).all()                # asymmetry
+
+
+def test_inputs_in_range():
+    cols = make_columns(64, 5)
+    for region in ("nam", "globe"):
+        ai = aerosols.make_inputs(cols, 9, region)
+        assert ai["rhly"].shape == (cols.nlay, cols.ncol) and 0 <= ai["rhly"].min() and ai["rhly"].max() <= 1
+        assert np.abs(ai["xlat"]).max() <= np.pi / 2

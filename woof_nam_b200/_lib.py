@@ -76,6 +76,19 @@ class RadRdtemp(ctypes.Structure):
 
 
 # Every symbol include/radb200.h declares, with its ctypes signature.
+AER_CLIM_FIELDS = ("iendwv", "haer", "prsref", "rhid", "rhdp", "straext0", "nwvns0", "s0intv", "month_idx",
+                   "month_cmix", "month_kprf", "month_denn")
+AER_COL_FIELDS = ("plvl", "plyr", "tlyr", "qlyr", "rhly", "xlon", "xlat", "slmsk")
+
+
+class RadAerClim(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in AER_CLIM_FIELDS]
+
+
+class RadAerColumns(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in AER_COL_FIELDS]
+
+
 SIGNATURES = {
     "rad_version": ([], ctypes.c_int),
     "rad_config_default": ([ctypes.POINTER(RadConfig), ctypes.c_int32], None),
@@ -95,6 +108,9 @@ SIGNATURES = {
     "rad_post_outputs": ([ctypes.c_void_p, ctypes.POINTER(RadPostIn), ctypes.POINTER(RadPostOut), ctypes.c_int64,
                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p], ctypes.c_int),
     "rad_rdtemp": ([ctypes.c_void_p, ctypes.POINTER(RadRdtemp), ctypes.c_void_p], ctypes.c_int),
+    "rad_load_aerosols": ([ctypes.c_void_p, ctypes.POINTER(RadAerClim)], ctypes.c_int),
+    "rad_setaer": ([ctypes.c_void_p, ctypes.POINTER(RadAerColumns), ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                    ctypes.c_void_p], ctypes.c_int),
     "rad_profile_enable": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rad_profile_read": ([ctypes.c_void_p, ctypes.POINTER(RadProfile)], ctypes.c_int),
     "rad_last_error": ([ctypes.c_void_p], ctypes.c_char_p),

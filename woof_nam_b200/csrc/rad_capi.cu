@@ -38,6 +38,7 @@ __constant__ int c_sw_ns[15] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94
 #include "rad_mcica.cuh"
 #include "rad_post.cuh"
 #include "rad_rdtemp.cuh"
+#include "rad_aer.cuh"
 
 using namespace rad;
 
@@ -61,6 +62,8 @@ struct RadHandle {
     int64_t lw3_cap = 0;                           // columns d_lw3 holds
     int* d_lw3list = nullptr;                      // [1 + lw3_cap]: count, then the chunk's float64 columns
     float* d_swrt = nullptr;                       // SW layer R/T stores, sw2_rt_floats() per CTA of the SW grid
+    float* d_aerf = nullptr;                       // aerosol band tables of the loaded month (AF_* offsets)
+    int* d_aeri = nullptr;                         // their integer part (AI_* offsets)
     int nsm = 148;                                 // SMs of the device (grid of the float64 column kernel)
     std::string err;
     // kernel accounting
@@ -911,6 +914,56 @@ int rad_post_outputs(RadHandle* h, const RadPostIn* in, const RadPostOut* out, i
     return RAD_OK;
 }
 
+int rad_load_aerosols(RadHandle* h, const RadAerClim* c)
+{
+    if (!h || !c) return fail(h, RAD_E_INVALID, "rad_load_aerosols: null argument");
+    if (!c->iendwv || !c->haer || !c->prsref || !c->rhid || !c->rhdp || !c->straext0 || !c->nwvns0 || !c->s0intv ||
+        !c->month_idx || !c->month_cmix || !c->month_kprf || !c->month_denn)
+        return fail(h, RAD_E_INVALID, "rad_load_aerosols: a climatology pointer is null");
+    int64_t nw = 0;
+    for (int b = 0; b < 151; ++b) nw += c->nwvns0[b];
+    if (nw != 57600) return fail(h, RAD_E_INVALID, "rad_load_aerosols: the solar spectrum must cover 57,600 wavenumbers");
+    for (int i = 0; i < AER_NCELL; ++i)
+        if (c->month_kprf[i] < 1 || c->month_kprf[i] > AER_NAE)
+            return fail(h, RAD_E_INVALID, "rad_load_aerosols: a profile structure is outside 1..7");
+    for (int i = 0; i < AER_NCELL * AER_NXC; ++i)
+        if (c->month_idx[i] < 0 || c->month_idx[i] > AER_NCM)
+            return fail(h, RAD_E_INVALID, "rad_load_aerosols: a component index is outside 0..10");
+    std::vector<float> fb;
+    std::vector<int> ib;
+    aerh::build(*c, fb, ib);
+    RAD_CUDA(h, cudaSetDevice(h->device));
+    if (!h->d_aerf) RAD_CUDA(h, cudaMalloc((void**)&h->d_aerf, (size_t)AF_TOTAL * sizeof(float)));
+    if (!h->d_aeri) RAD_CUDA(h, cudaMalloc((void**)&h->d_aeri, (size_t)AI_TOTAL * sizeof(int)));
+    RAD_CUDA(h, cudaMemcpy(h->d_aerf, fb.data(), fb.size() * sizeof(float), cudaMemcpyHostToDevice));
+    RAD_CUDA(h, cudaMemcpy(h->d_aeri, ib.data(), ib.size() * sizeof(int), cudaMemcpyHostToDevice));
+    return RAD_OK;
+}
+
+int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faersw, float* faerlw, void* stream)
+{
+    if (!h || !in) return fail(h, RAD_E_INVALID, "rad_setaer: null argument");
+    if (!h->d_aerf) return fail(h, RAD_E_INVALID, "rad_setaer: no climatology loaded (rad_load_aerosols)");
+    if (ncol < 0 || ncol > (int64_t)std::numeric_limits<int>::max() - 1)
+        return fail(h, RAD_E_INVALID, "rad_setaer: ncol out of range");
+    if (ncol == 0) return RAD_OK;
+    if (!in->plvl || !in->plyr || !in->tlyr || !in->qlyr || !in->rhly || !in->xlon || !in->xlat || !in->slmsk ||
+        !faersw || !faerlw)
+        return fail(h, RAD_E_INVALID, "rad_setaer: a required pointer is null");
+    if (h->cfg.nlay > NLAY_MAX) return fail(h, RAD_E_INVALID, "rad_setaer: nlay above NLAY_MAX");
+    const float* f = h->d_aerf;
+    const int* i = h->d_aeri;
+    AerTab t{f + AF_HAER, f + AF_PRSREF, f + AF_SIGREF, f + AF_EXTRHI, f + AF_SCARHI, f + AF_SSARHI, f + AF_ASYRHI,
+             f + AF_EXTRHD, f + AF_SCARHD, f + AF_SSARHD, f + AF_ASYRHD, f + AF_EXTSTRA, f + AF_CMIXG, f + AF_DENNG,
+             i + AI_IDXCG, i + AI_KPRFG};
+    AerArgs a{in->plvl, in->plyr, in->tlyr, in->qlyr, in->rhly, in->xlon, in->xlat, in->slmsk, faersw, faerlw, ncol,
+              h->cfg.nlay};
+    k_setaer<<<(unsigned)((ncol + AER_THREADS - 1) / AER_THREADS), AER_THREADS, 0, (cudaStream_t)stream>>>(a, t);
+    h->launches += 1;
+    RAD_CUDA(h, cudaGetLastError());
+    return RAD_OK;
+}
+
 int rad_rdtemp(RadHandle* h, const RadRdtemp* p, void* stream)
 {
     if (!h || !p) return fail(h, RAD_E_INVALID, "rad_rdtemp: null argument");
@@ -964,7 +1017,8 @@ void rad_destroy(RadHandle* h)
     for (void* p : {(void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
                     (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
                     (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub, (void*)h->d_lwm,
-                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt})
+                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt, (void*)h->d_aerf,
+                    (void*)h->d_aeri})
         if (p) cudaFree(p);
     delete h;
 }
