@@ -17,19 +17,21 @@
 // interpolation, the optics of the five domains in the 30 bands, and the smoothing of optical depth across
 // domain boundaries.
 //
-// k_setaer: one thread per column (64 per CTA), so every output row is one coalesced store per warp.  The
-// reference keeps per-layer arrays per thread and walks them once per band; here the layers run top to
-// bottom once, all 30 bands per layer, and the smoothing -- which couples layer k and k - 1 of a band --
-// carries each band's previous optical depth in shared memory and writes it when the next layer has
-// settled it.  Heights and domain indices, which build up from the surface, come from a bottom-up pass into
-// shared memory ([level][thread]).  The output (22 KB per column of 61 layers) makes the pass HBM-bound.
+// k_setaer: a CTA takes 32 columns, one per lane, and 8 warps.  Warp 0 maps the climatology onto its
+// columns and walks each column up from the surface for the level heights and layer domains (the parts
+// that build up layer by layer); then all warps, layers side by side, form each layer's effective thickness
+// and humidity bracket into shared memory ([layer][column]); then warp w runs bands w, w + 8, ... down the
+// layers, the smoothing (which couples a band's adjacent layers) carried in a register and each optical
+// depth stored once the layer below has settled it.  Every store is a 128-byte row of 32 columns.  The
+// reference runs one thread per column through 61 layers x 30 bands; splitting the bands over warps cuts
+// each thread's dependent chain eightfold.  The output (22 KB per column of 61 layers) bounds it at HBM.
 #pragma once
 
 namespace rad {
 
 constexpr int AER_NAERBND = 61, AER_NRHLEV = 8, AER_NCM1 = 6, AER_NCM2 = 4, AER_NCM = 10, AER_NDM = 5, AER_NAE = 7;
 constexpr int AER_IMXAE = 72, AER_JMXAE = 37, AER_NXC = 5, AER_NSW = 14, AER_NLW = 16, AER_NBT = 30;
-constexpr int AER_THREADS = 64;
+constexpr int AER_COLS = 32, AER_WARPS = 8, AER_THREADS = AER_COLS * AER_WARPS;   // k_setaer CTA
 constexpr int AER_NCELL = AER_IMXAE * AER_JMXAE;
 
 // Device tables (one float blob and one int blob of the handle).
@@ -175,130 +177,168 @@ struct AerArgs {
     int nlay;
 };
 
-__global__ void __launch_bounds__(AER_THREADS) k_setaer(const __grid_constant__ AerArgs a, const __grid_constant__ AerTab t)
+__global__ void __launch_bounds__(AER_THREADS, 2) k_setaer(const __grid_constant__ AerArgs a, const __grid_constant__ AerTab t)
 {
-    __shared__ float s_hz[NLAY_MAX + 1][AER_THREADS];       // level heights, level 0 = model top
-    __shared__ unsigned char s_dom[NLAY_MAX][AER_THREADS];   // domain index of each layer
-    __shared__ float s_prev[AER_NBT][AER_THREADS];           // each band's optical depth of the layer above
-    const int tid = threadIdx.x;
-    const int64_t col = (int64_t)blockIdx.x * AER_THREADS + tid;
-    if (col >= a.n) return;
+    __shared__ float s_hz[NLAY_MAX + 1][AER_COLS];        // level heights, level 0 = model top
+    __shared__ float s_delz[NLAY_MAX][AER_COLS];          // layer thickness, then effective thickness
+    __shared__ float s_fr[NLAY_MAX][AER_COLS];            // sigma of the layer top, then humidity weight
+    __shared__ int s_code[NLAY_MAX][AER_COLS];            // domain | low humidity level << 4 | high << 8
+    __shared__ float s_cmix[AER_NCM + 1][AER_COLS];       // the column's component mixing ratios
+    __shared__ float s_col[4][AER_COLS];                  // denn[1], denn[2], h1, profile structure
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t col = (int64_t)blockIdx.x * AER_COLS + lane;
+    const bool live = col < a.n;
     const int nlay = a.nlay;
     const int64_t N = a.n;
-    auto L = [&](const float* p, int k) { return __ldg(p + (size_t)k * N + col); };   // [level][col], 0-based
-
-    // setaer prep: degrees; layer thickness from the hypsometric equation (the top layer from its mid-level
-    // pressure, doubled), heights summed up from the surface
-    const float pi = 3.1415926535897931f;
-    const float rdg = 180.0f / pi, rovg = 0.001f * 2.8705e+2f / 9.80665e+0f, fvirt = 4.6150e+2f / 2.8705e+2f - 1.0f;
-    float alon = __ldg(a.xlon + col) * rdg;
-    if (alon < 0.0f) alon = alon + 360.0f;
-    float alat = __ldg(a.xlat + col) * rdg;
-    if (alat < -90.0f) alat = -90.0f;
-    if (alat > 90.0f) alat = 90.0f;
-    const float slm = __ldg(a.slmsk + col);
-
-    // the 5-degree cells around the column, the profile structure and the domain-overlay rules
-    const float dltg = 360.0f / (float)AER_IMXAE, hdlt = 0.5f * dltg, rdlt = 1.0f / dltg;
-    int i3 = 1;
-    float dtmp = alon < 0.0f ? 0.0f : alon;
-    while (dtmp > dltg && i3 < AER_IMXAE) { ++i3; dtmp = alon - dltg * (float)(i3 - 1); }
-    const int i1 = i3, i2 = i3 % AER_IMXAE + 1;
-    const float wi = dtmp * rdlt;
-    const int kpi = dtmp <= hdlt ? i3 : i2;
-    int j3 = 1;
-    float dtl = 90.0f - alat;
-    while (dtl > dltg && j3 < AER_JMXAE) { ++j3; dtl = (90.0f - dltg * (float)(j3 - 1)) - alat; }
-    const int j1 = j3, j2 = j3 + 1 > AER_JMXAE ? AER_JMXAE : j3 + 1;
-    const float wj = dtl * rdlt;
-    const int kpj = dtl <= hdlt ? j3 : j2;
-    auto CELL = [&](int i, int j) { return (j - 1) * AER_IMXAE + (i - 1); };
+    const int64_t c = live ? col : a.n - 1;           // idle lanes of the last CTA mirror a real column
+    auto L = [&](const float* p, int k) { return __ldg(p + (size_t)k * N + c); };   // [level][col], 0-based
     auto HA = [&](int d, int kp) { return __ldg(t.haer + (kp - 1) * AER_NDM + (d - 1)); };
-    int kp = __ldg(t.kprfg + CELL(kpi, kpj));
-    const int kpa = max(max(__ldg(t.kprfg + CELL(i1, j1)), __ldg(t.kprfg + CELL(i1, j2))),
-                        max(__ldg(t.kprfg + CELL(i2, j1)), __ldg(t.kprfg + CELL(i2, j2))));
-    float h1 = HA(1, kp);
-    int nden = 1;
-    if (kp != kpa) {
-        if (kpa == 6 || kpa == 7) {                    // mineral transport over the ocean / land profile
-            nden = 2;
-            const bool land = slm > 0.0f;
-            if ((kpa == 6) == land) { kp = kpa == 6 ? 7 : 6; h1 = 0.5f * (HA(1, 6) + HA(1, 7)); }
-            else { kp = kpa; h1 = HA(1, kpa); }
-        } else {
-            h1 = HA(1, kpa);
-            kp = kpa;
-        }
-    }
-    const float w11 = (1.0f - wi) * (1.0f - wj), w12 = (1.0f - wi) * wj, w21 = wi * (1.0f - wj), w22 = wi * wj;
-    const int c11 = CELL(i1, j1), c12 = CELL(i1, j2), c21 = CELL(i2, j1), c22 = CELL(i2, j2);
-    float denn[3] = {0.0f, 0.0f, 0.0f};
-    for (int m = 1; m <= nden; ++m)
-        denn[m] = w11 * __ldg(t.denng + 2 * c11 + m - 1) + w12 * __ldg(t.denng + 2 * c12 + m - 1) +
-                  w21 * __ldg(t.denng + 2 * c21 + m - 1) + w22 * __ldg(t.denng + 2 * c22 + m - 1);
-    float cmix[AER_NCM + 1];
-#pragma unroll
-    for (int q = 0; q <= AER_NCM; ++q) cmix[q] = 0.0f;
-    for (int m = 0; m < AER_NXC; ++m) {
-        const int cc[4] = {c11, c12, c21, c22};
-        const float ww[4] = {w11, w12, w21, w22};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int ic = __ldg(t.idxcg + cc[q] * AER_NXC + m);
-            const float v = ww[q] * __ldg(t.cmixg + cc[q] * AER_NXC + m);
-#pragma unroll
-            for (int s = 1; s <= AER_NCM; ++s)        // register-indexed accumulation (ic = 0: no component)
-                if (ic == s) cmix[s] = cmix[s] + v;
-        }
-    }
-
+    const float pi = 3.1415926535897931f;
+    const float rovg = 0.001f * 2.8705e+2f / 9.80665e+0f, fvirt = 4.6150e+2f / 2.8705e+2f - 1.0f;
     // layer thickness (k 0-based, top first): hypsometric, the top layer from its mid-level pressure, doubled
     auto DZ = [&](int k) {
         const float lo = k == 0 ? logf(L(a.plyr, 0)) : logf(L(a.plvl, k));
         const float dz = rovg * (logf(L(a.plvl, k + 1)) - lo) * L(a.tlyr, k) * (1.0f + fvirt * L(a.qlyr, k));
         return k == 0 ? 2.0f * dz : dz;
     };
-    // bottom-up pass: heights (surface 0) and each layer's domain, walking up through the profile's
-    // reference sigma levels
-    const float rps = __fdiv_rn(1.0f, L(a.plvl, nlay));   // decides domains: IEEE division, not the fast one
-    s_hz[nlay][tid] = 0.0f;
-    float hz = 0.0f;
-    int d = 1;
-    for (int k = nlay - 1; k >= 0; --k) {
-        hz = hz + DZ(k);
-        s_hz[k][tid] = hz;
-        if (d <= AER_NDM && L(a.plvl, k) * rps < __ldg(t.sigref + (kp - 1) * AER_NDM + (d - 1))) {
-            d = d + 1;
-            if (d == 2 && __ldg(t.prsref + (kp - 1) * AER_NDM + 1) == __ldg(t.prsref + (kp - 1) * AER_NDM + 2)) d = 3;
-        }
-        s_dom[k][tid] = (unsigned char)d;
-    }
 
-    // top-down pass: per layer all 30 bands; optical depth smoothed against the layer above and stored one
-    // layer late, albedo and asymmetry stored at once
-    auto OUT = [&](int band, int f, int k) -> float* {
-        return band < AER_NSW ? a.faersw + (((size_t)f * AER_NSW + band) * nlay + k) * N + col
-                              : a.faerlw + (((size_t)f * AER_NLW + (band - AER_NSW)) * nlay + k) * N + col;
-    };
-    for (int k = 0; k < nlay; ++k) {
-        const int dom = s_dom[k][tid];
-        const float hl = dom > 1 ? (dom <= AER_NDM ? HA(dom, kp) : 0.0f) : h1;
-        float delz;
-        if (hl > 0.0f) {
-            const float r = 1.0f / hl;
-            delz = hl * (expf(-s_hz[k + 1][tid] * r) - expf(-s_hz[k][tid] * r));
-        } else {                                       // the layer's own thickness
-            delz = DZ(k);
+    // layers side by side: thickness and the sigma of each layer's top interface
+    {
+        const float rps = __fdiv_rn(1.0f, L(a.plvl, nlay));   // decides domains: IEEE division, not the fast one
+        for (int k = warp; k < nlay; k += AER_WARPS) {
+            s_delz[k][lane] = DZ(k);
+            s_fr[k][lane] = L(a.plvl, k) * rps;
         }
-        const float rh = L(a.rhly, k);
-        int r2 = 1;
-        while (r2 <= AER_NRHLEV && rh > c_aer_rhlev[r2 - 1]) ++r2;
-        const int r1 = max(1, r2 - 1);
-        r2 = min(AER_NRHLEV, r2);
-        const float fr = r1 == r2 ? 0.0f : (rh - c_aer_rhlev[r1 - 1]) / (c_aer_rhlev[r2 - 1] - c_aer_rhlev[r1 - 1]);
-        for (int b = 0; b < AER_NBT; ++b) {
-            const bool sw = b < AER_NSW;
-            auto RI = [&](const float* x, int s) { return __ldg(x + b * AER_NCM1 + (s - 1)); };
+    }
+    __syncthreads();
+    if (warp == 0) {
+        // setaer prep: degrees; the 5-degree cells around the column, profile structure, domain-overlay rules
+        const float rdg = 180.0f / pi;
+        float alon = __ldg(a.xlon + c) * rdg;
+        if (alon < 0.0f) alon = alon + 360.0f;
+        float alat = __ldg(a.xlat + c) * rdg;
+        if (alat < -90.0f) alat = -90.0f;
+        if (alat > 90.0f) alat = 90.0f;
+        const float slm = __ldg(a.slmsk + c);
+        const float dltg = 360.0f / (float)AER_IMXAE, hdlt = 0.5f * dltg, rdlt = 1.0f / dltg;
+        // the reference steps cell by cell to the first i with f(i) <= dltg (f(1) = max(alon, 0),
+        // f(i) = alon - dltg (i - 1)); f falls with i, so start next to the answer and step to it
+        auto fi = [&](int i) { return i == 1 ? (alon < 0.0f ? 0.0f : alon) : alon - dltg * (float)(i - 1); };
+        int i3 = min(AER_IMXAE, max(1, (int)(alon * rdlt)));
+        while (i3 > 1 && fi(i3 - 1) <= dltg) --i3;
+        while (i3 < AER_IMXAE && fi(i3) > dltg) ++i3;
+        const float dtmp = fi(i3);
+        const int i1 = i3, i2 = i3 % AER_IMXAE + 1;
+        const float wi = dtmp * rdlt;
+        const int kpi = dtmp <= hdlt ? i3 : i2;
+        auto fj = [&](int j) { return j == 1 ? 90.0f - alat : (90.0f - dltg * (float)(j - 1)) - alat; };
+        int j3 = min(AER_JMXAE, max(1, (int)((90.0f - alat) * rdlt)));
+        while (j3 > 1 && fj(j3 - 1) <= dltg) --j3;
+        while (j3 < AER_JMXAE && fj(j3) > dltg) ++j3;
+        const float dtl = fj(j3);
+        const int j1 = j3, j2 = j3 + 1 > AER_JMXAE ? AER_JMXAE : j3 + 1;
+        const float wj = dtl * rdlt;
+        const int kpj = dtl <= hdlt ? j3 : j2;
+        auto CELL = [&](int i, int j) { return (j - 1) * AER_IMXAE + (i - 1); };
+        int kp = __ldg(t.kprfg + CELL(kpi, kpj));
+        const int kpa = max(max(__ldg(t.kprfg + CELL(i1, j1)), __ldg(t.kprfg + CELL(i1, j2))),
+                            max(__ldg(t.kprfg + CELL(i2, j1)), __ldg(t.kprfg + CELL(i2, j2))));
+        float h1 = HA(1, kp);
+        int nden = 1;
+        if (kp != kpa) {
+            if (kpa == 6 || kpa == 7) {                // mineral transport over the ocean / land profile
+                nden = 2;
+                const bool land = slm > 0.0f;
+                if ((kpa == 6) == land) { kp = kpa == 6 ? 7 : 6; h1 = 0.5f * (HA(1, 6) + HA(1, 7)); }
+                else { kp = kpa; h1 = HA(1, kpa); }
+            } else {
+                h1 = HA(1, kpa);
+                kp = kpa;
+            }
+        }
+        const float w11 = (1.0f - wi) * (1.0f - wj), w12 = (1.0f - wi) * wj, w21 = wi * (1.0f - wj), w22 = wi * wj;
+        const int c11 = CELL(i1, j1), c12 = CELL(i1, j2), c21 = CELL(i2, j1), c22 = CELL(i2, j2);
+        float denn[3] = {0.0f, 0.0f, 0.0f};
+        for (int m = 1; m <= nden; ++m)
+            denn[m] = w11 * __ldg(t.denng + 2 * c11 + m - 1) + w12 * __ldg(t.denng + 2 * c12 + m - 1) +
+                      w21 * __ldg(t.denng + 2 * c21 + m - 1) + w22 * __ldg(t.denng + 2 * c22 + m - 1);
+        float cmix[AER_NCM + 1];
+#pragma unroll
+        for (int q = 0; q <= AER_NCM; ++q) cmix[q] = 0.0f;
+        for (int m = 0; m < AER_NXC; ++m) {
+            const int cc[4] = {c11, c12, c21, c22};
+            const float ww[4] = {w11, w12, w21, w22};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int ic = __ldg(t.idxcg + cc[q] * AER_NXC + m);
+                const float v = ww[q] * __ldg(t.cmixg + cc[q] * AER_NXC + m);
+#pragma unroll
+                for (int s = 1; s <= AER_NCM; ++s)    // register-indexed accumulation (ic = 0: no component)
+                    if (ic == s) cmix[s] = cmix[s] + v;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q <= AER_NCM; ++q) s_cmix[q][lane] = cmix[q];
+        s_col[0][lane] = denn[1];
+        s_col[1][lane] = denn[2];
+        s_col[2][lane] = h1;
+        s_col[3][lane] = __int_as_float(kp);
+        // bottom-up: heights (surface 0) and each layer's domain, walking up through the profile's
+        // reference sigma levels
+        s_hz[nlay][lane] = 0.0f;
+        float hz = 0.0f;
+        int d = 1;
+        for (int k = nlay - 1; k >= 0; --k) {
+            hz = hz + s_delz[k][lane];
+            s_hz[k][lane] = hz;
+            if (d <= AER_NDM && s_fr[k][lane] < __ldg(t.sigref + (kp - 1) * AER_NDM + (d - 1))) {
+                d = d + 1;
+                if (d == 2 && __ldg(t.prsref + (kp - 1) * AER_NDM + 1) == __ldg(t.prsref + (kp - 1) * AER_NDM + 2)) d = 3;
+            }
+            s_code[k][lane] = d;
+        }
+    }
+    __syncthreads();
+    // per layer, the warps side by side: effective thickness and the humidity bracket
+    {
+        const int kp = __float_as_int(s_col[3][lane]);
+        const float h1 = s_col[2][lane];
+        for (int k = warp; k < nlay; k += AER_WARPS) {
+            const int dom = s_code[k][lane];
+            const float hl = dom > 1 ? (dom <= AER_NDM ? HA(dom, kp) : 0.0f) : h1;
+            float delz;
+            if (hl > 0.0f) {
+                const float r = 1.0f / hl;
+                delz = hl * (expf(-s_hz[k + 1][lane] * r) - expf(-s_hz[k][lane] * r));
+            } else {                                   // the layer's own thickness
+                delz = s_delz[k][lane];
+            }
+            const float rh = L(a.rhly, k);
+            int r2 = 1;
+            while (r2 <= AER_NRHLEV && rh > c_aer_rhlev[r2 - 1]) ++r2;
+            const int r1 = max(1, r2 - 1);
+            r2 = min(AER_NRHLEV, r2);
+            s_fr[k][lane] = r1 == r2 ? 0.0f : (rh - c_aer_rhlev[r1 - 1]) / (c_aer_rhlev[r2 - 1] - c_aer_rhlev[r1 - 1]);
+            s_delz[k][lane] = delz;
+            s_code[k][lane] = dom | (r1 << 4) | (r2 << 8);
+        }
+    }
+    __syncthreads();
+    if (!live) return;
+    // per band (warp w: bands w, w + AER_WARPS, ...): the layers top to bottom; the smoothing against the
+    // layer above settles that layer's optical depth, which is stored one layer late
+    const float dn1 = s_col[0][lane], dn2 = s_col[1][lane];
+    for (int b = warp; b < AER_NBT; b += AER_WARPS) {
+        const bool sw = b < AER_NSW;
+        float* const o0 = sw ? a.faersw + ((size_t)(0 * AER_NSW + b) * nlay) * N + col
+                             : a.faerlw + ((size_t)(0 * AER_NLW + b - AER_NSW) * nlay) * N + col;
+        const size_t fstride = (size_t)(sw ? AER_NSW : AER_NLW) * nlay * N;   // field to field
+        auto RI = [&](const float* x, int s) { return __ldg(x + b * AER_NCM1 + (s - 1)); };
+        float up = 0.0f;
+        for (int k = 0; k < nlay; ++k) {
+            const int code = s_code[k][lane];
+            const int dom = code & 15, r1 = (code >> 4) & 15, r2 = code >> 8;
+            const float fr = s_fr[k][lane], delz = s_delz[k][lane];
             auto RD = [&](const float* x, int s) {
                 const float* p = x + (b * AER_NCM2 + (s - 1)) * AER_NRHLEV;
                 const float v1 = __ldg(p + r1 - 1);
@@ -324,7 +364,7 @@ __global__ void __launch_bounds__(AER_THREADS) k_setaer(const __grid_constant__ 
                 float ext = 0.0f, sca = 0.0f, se = 0.0f, sg = 0.0f;
 #pragma unroll
                 for (int s = 1; s <= AER_NCM; ++s) {
-                    const float cm = cmix[s];
+                    const float cm = s_cmix[s][lane];
                     if (!(cm > 0.0f)) continue;
                     float e, sc, al, g;
                     if (s <= AER_NCM1) { e = RI(t.extrhi, s); sc = RI(t.scarhi, s); al = RI(t.ssarhi, s); g = RI(t.asyrhi, s); }
@@ -334,11 +374,11 @@ __global__ void __launch_bounds__(AER_THREADS) k_setaer(const __grid_constant__ 
                     se = se + cm * al * e;
                     sg = sg + cm * g * sc;
                 }
-                tau = ext * denn[1] * delz;
+                tau = ext * dn1 * delz;
                 ssa = ext > 0.0f ? fminf(1.0f, se / ext) : 1.0f;
                 asy = sca > 0.0f ? fminf(1.0f, sg / sca) : 0.0f;
             } else if (dom == 2) {                     // mineral transport layers
-                tau = RI(t.extrhi, 6) * denn[2] * delz;
+                tau = RI(t.extrhi, 6) * dn2 * delz;
                 ssa = RI(t.ssarhi, 6);
                 asy = RI(t.asyrhi, 6);
             } else {                                   // above every domain: no aerosol
@@ -347,19 +387,18 @@ __global__ void __launch_bounds__(AER_THREADS) k_setaer(const __grid_constant__ 
                 asy = 0.0f;
             }
             if (k > 0) {                               // smoothing against the layer above (top to surface)
-                float up = s_prev[b][tid];
                 const float ratio = tau > 0.0f ? __fdiv_rn(up, tau) : 1.0f;
                 const float sum = tau + up, lo = 0.2f * sum, hi = sum - lo;
                 if (ratio > 30.0f) { tau = lo; up = hi; }
                 if (ratio < 0.03333f) { tau = hi; up = lo; }
-                *OUT(b, 0, k - 1) = up;
+                o0[(size_t)(k - 1) * N] = up;
             }
-            s_prev[b][tid] = tau;
-            *OUT(b, 1, k) = ssa;
-            *OUT(b, 2, k) = asy;
+            up = tau;
+            o0[fstride + (size_t)k * N] = ssa;
+            o0[2 * fstride + (size_t)k * N] = asy;
         }
+        o0[(size_t)(nlay - 1) * N] = up;
     }
-    for (int b = 0; b < AER_NBT; ++b) *OUT(b, 0, nlay - 1) = s_prev[b][tid];
 }
 
 }  // namespace rad

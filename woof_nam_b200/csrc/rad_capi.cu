@@ -958,7 +958,7 @@ int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faers
              i + AI_IDXCG, i + AI_KPRFG};
     AerArgs a{in->plvl, in->plyr, in->tlyr, in->qlyr, in->rhly, in->xlon, in->xlat, in->slmsk, faersw, faerlw, ncol,
               h->cfg.nlay};
-    k_setaer<<<(unsigned)((ncol + AER_THREADS - 1) / AER_THREADS), AER_THREADS, 0, (cudaStream_t)stream>>>(a, t);
+    k_setaer<<<(unsigned)((ncol + AER_COLS - 1) / AER_COLS), AER_THREADS, 0, (cudaStream_t)stream>>>(a, t);
     h->launches += 1;
     RAD_CUDA(h, cudaGetLastError());
     return RAD_OK;
