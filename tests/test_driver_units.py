@@ -193,3 +193,38 @@ def test_rdtemp_unit_equals_oracle():
     assert np.max(np.abs(st["CZEN"].cpu().numpy() - ref["czen"])) < 3e-5      # float angle resolution
     changed = st["T"].cpu().numpy() != p["t"]
     assert changed[:, 1:-1, 1:-1].any() and not changed[:, 0, :].any()       # interior only
+
+
+@pytest.mark.gpu
+def test_grrad_aerosols_unit_feeds_the_solve():
+    """grrad_aerosols.run on a state under the reference's names (RAD_PLVL, RAD_PLYR, RAD_TLYR, RAD_QLYR,
+    RAD_RHLY, XLON, XLAT, SLMSK) writes rrtm_faersw / rrtm_faerlw equal to the aerosol optics called
+    directly, and the column solve then reads them as the solver does the same optics."""
+    import datetime
+
+    import torch
+    from woof_nam_b200 import aerosols, grrad_aerosols
+    from woof_nam_b200.solver import RadSolver
+    cols = make_columns(JM * IM, 23)
+    ai = aerosols.make_inputs(cols, 6, "nam")
+    ctx = _ctx(cols)
+    ctx.start = datetime.datetime(2026, 5, 1)
+    for name, key in (("RAD_RHLY", "rhly"),):
+        ctx.st[name] = torch.from_numpy(ai[key].reshape(cols.nlay, JM, IM).copy()).cuda()
+    for name, key in (("XLON", "xlon"), ("XLAT", "xlat"), ("SLMSK", "slmsk")):
+        ctx.st[name] = torch.from_numpy(ai[key].reshape(JM, IM).copy()).cuda()
+    o = grrad_aerosols.run(ctx, lsswr=True, lslwr=True)
+    driver.column_solve(ctx)
+    torch.cuda.synchronize()
+    s = RadSolver()
+    dev = s.to_device(cols)
+    aer = aerosols.Aerosols(s, 5)
+    t = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in ai.items()}
+    fsw, flw = aer.optics(dev, t["rhly"], t["xlon"], t["xlat"], t["slmsk"])
+    torch.cuda.synchronize()
+    assert torch.equal(o["faersw"].reshape(fsw.shape), fsw) and torch.equal(o["faerlw"].reshape(flw.shape), flw)
+    dev["faersw"], dev["faerlw"] = fsw, flw
+    ref = s.solve(dev, cols.solcon)
+    torch.cuda.synchronize()
+    assert torch.equal(ctx.st["htlwc"].reshape(ref["htlw"].shape), ref["htlw"])
+    assert torch.equal(ctx.st["HTSWC"].reshape(ref["htsw"].shape), ref["htsw"])

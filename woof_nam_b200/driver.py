@@ -362,6 +362,66 @@ def rdtemp_run(ctx) -> None:
     _solver(ctx, "both", 1.5, lm + 1).rdtemp(p, stream=_stream(ctx))
 
 
+# grrad's setaer inputs: the unit's name, the grrad-setup / model state name (phys_rrtm_grrad_aerosols.py:12-22)
+AER_INPUTS = {
+    "plvl": ("RAD_PLVL", "phys-rrtm-grrad-setup"), "plyr": ("RAD_PLYR", "phys-rrtm-grrad-setup"),
+    "tlyr": ("RAD_TLYR", "phys-rrtm-grrad-setup"), "qlyr": ("RAD_QLYR", "phys-rrtm-grrad-setup"),
+    "rhly": ("RAD_RHLY", "phys-rrtm-grrad-setup"), "xlon": ("XLON", "the model grid"),
+    "xlat": ("XLAT", "the model grid"), "slmsk": ("SLMSK", "the model state"),
+}
+
+
+def _aer_month(ctx) -> int:
+    """The month of the aerosol climatology: ctx.tables["aer_month"] when the driver's calendar sets it
+    (aer_update runs at month changes), else ctx.clock.idate[1], else the month of ctx.start."""
+    tabs = getattr(ctx, "tables", None) or {}
+    if tabs.get("aer_month"):
+        return int(tabs["aer_month"])
+    clock = getattr(ctx, "clock", None)
+    if clock is not None and getattr(clock, "idate", None) is not None:
+        return int(clock.idate[1])
+    start = getattr(ctx, "start", None)
+    if start is None:
+        raise RuntimeError("phys-rrtm-grrad-aerosols: no month (ctx.tables['aer_month'], ctx.clock or ctx.start)")
+    return int(start.month)
+
+
+def grrad_aerosols_run(ctx, *, lsswr: bool = True, lslwr: bool = True) -> dict:
+    """Drop-in for phys_rrtm_grrad_aerosols.run(ctx, lsswr=, lslwr=) (phys_rrtm_grrad_aerosols.py:124-136):
+    the climatological aerosol optics of every column of ctx.grid (NAM iaer = 11: SW and LW, no volcanic term),
+    written to ctx.tables["rrtm_faersw"] [3, 14, LMK, JM, IM] and ["rrtm_faerlw"] [3, 16, LMK, JM, IM], where
+    lwrad / swrad read them.  The month's tables are (re)loaded when the month changes."""
+    from .aerosols import Aerosols
+    unit = "phys-rrtm-grrad-aerosols"
+    st, g = ctx.st, ctx.grid
+    jm, im, nlay = int(g.jm), int(g.im), int(g.lm) + 1
+    cols = {}
+    for k, (alias, producer) in AER_INPUTS.items():
+        t = _as_tensor(_get(st, unit, k, alias, producer), k, unit)
+        if tuple(t.shape[-2:]) != (jm, im):
+            raise ValueError(f"{unit}: {k} has trailing shape {tuple(t.shape[-2:])}, expected ({jm}, {im})")
+        cols[k] = t.reshape(*t.shape[:-2], jm * im)
+    s = _solver(ctx, "both", 1.5, nlay)
+    tabs = ctx.tables
+    aer = tabs.get(_KEY + ":aerosols")
+    month = _aer_month(ctx)
+    if aer is None or aer.solver is not s:
+        aer = Aerosols(s, month)
+        tabs[_KEY + ":aerosols"] = aer
+    elif aer.month != month:
+        aer.load(month)
+    torch = _torch()
+    fsw, flw = tabs.get("rrtm_faersw"), tabs.get("rrtm_faerlw")
+    if fsw is None or tuple(fsw.shape) != (3, 14, nlay, jm, im):
+        fsw = torch.zeros((3, 14, nlay, jm, im), dtype=torch.float32, device="cuda")
+        flw = torch.zeros((3, 16, nlay, jm, im), dtype=torch.float32, device="cuda")
+    stream = _stream(ctx)
+    out = (fsw.view(3, 14, nlay, jm * im), flw.view(3, 16, nlay, jm * im))
+    aer.optics(cols, cols["rhly"], cols["xlon"], cols["xlat"], cols["slmsk"], out=out, stream=stream)
+    tabs["rrtm_faersw"], tabs["rrtm_faerlw"] = fsw, flw
+    return {"faersw": fsw, "faerlw": flw}
+
+
 @contextlib.contextmanager
 def bound_units():
     """Bind the reference's grrad units to this library's column units for the duration of the block."""
