@@ -49,7 +49,7 @@ __device__ __forceinline__ double rfmod1(double x) { return fmod(x, 1.0); }
 template <class R>
 __device__ __forceinline__ R interp(const R* t, int ng, int ind, int ig, R frac)
 {
-    const R a = ldt(t + (size_t)(ind - 1) * ng + ig), b = ldt(t + (size_t)ind * ng + ig);
+    const R a = ldt(t + ((ind - 1) * ng + ig)), b = ldt(t + (ind * ng + ig));   // tables < 2^31 entries
     return a + frac * (b - a);
 }
 

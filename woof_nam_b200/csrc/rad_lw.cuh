@@ -99,7 +99,7 @@ template <class R>
 __device__ __forceinline__ R major12(const R* absa, int ng, int ig, R sc, const Sel<R>& s0, R f00, R f10, R sc1,
                                      const Sel<R>& s1, R f01, R f11)
 {
-    auto A = [&](int id) { return ldt(absa + (size_t)(id - 1) * ng + ig); };
+    auto A = [&](int id) { return ldt(absa + ((id - 1) * ng + ig)); };
     const R fac000 = s0.fk0 * f00, fac100 = s0.fk1 * f00, fac200 = s0.fk2 * f00;
     const R fac010 = s0.fk0 * f10, fac110 = s0.fk1 * f10, fac210 = s0.fk2 * f10;
     const R fac001 = s1.fk0 * f01, fac101 = s1.fk1 * f01, fac201 = s1.fk2 * f01;
@@ -119,7 +119,7 @@ __device__ __forceinline__ R adjcol(R col, R temp, R thr, R off, R ex)   // the 
 template <class R>
 __device__ __forceinline__ R minor2d(const R* t, int nj, int ng, int j, R fj, int m, R fm, int ig)  // t[m][j][g]
 {
-    auto K = [&](int jj, int mm) { return ldt(t + ((size_t)(mm - 1) * nj + (jj - 1)) * ng + ig); };
+    auto K = [&](int jj, int mm) { return ldt(t + (((mm - 1) * nj + (jj - 1)) * ng + ig)); };
     const R m1 = K(j, m) + fj * (K(j + 1, m) - K(j, m));
     const R m2 = K(j, m + 1) + fj * (K(j + 1, m + 1) - K(j, m + 1));
     return m1 + fm * (m2 - m1);
@@ -127,7 +127,8 @@ __device__ __forceinline__ R minor2d(const R* t, int nj, int ng, int j, R fj, in
 
 // ------------------------------------------------------------------------------------------------------
 // Gas optical depth and Planck fraction of LW g-point g (0..139) at layer k0: the band kernels of the
-// reference restated per (g, layer).  Statement order follows each band's reference kernel.
+// reference restated per (g, layer).  Statement order follows each band's reference kernel.  Table offsets
+// are formed in 32-bit integers (every table is far below 2^31 entries), one wide add per address.
 template <class R, class S>
 __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = -1)
 {
@@ -138,9 +139,9 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
     const R sfac = s.selffac[k0], sfr = s.selffrac[k0], ffac = s.forfac[k0], ffr = s.forfrac[k0],
             mf = s.minorfrac[k0];
     const R* chi = tab<R>(T_LW_CHI_MLS);
-    auto CHI = [&](int gg, int lev) { return ldt(chi + (size_t)(lev - 1) * 7 + (gg - 1)); };
+    auto CHI = [&](int gg, int lev) { return ldt(chi + ((lev - 1) * 7 + (gg - 1))); };
     auto A4 = [&](const R* t, int ng, int ig, int i0, int i1) {
-        auto a = [&](int id) { return ldt(t + (size_t)(id - 1) * ng + ig); };
+        auto a = [&](int id) { return ldt(t + ((id - 1) * ng + ig)); };
         return f00 * a(i0) + f10 * a(i0 + 1) + f01 * a(i1) + f11 * a(i1 + 1);
     };
     const int ind0l = (jpk - 1) * 5 + (jtk - 1) + 1, ind1l = jpk * 5 + (jt1k - 1) + 1;
@@ -227,7 +228,7 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
             spec(ka1, rpb, c2, (R)4, scp, spp, jpl, fpl);
             const R fac000 = ((R)1 - fs) * f00, fac010 = ((R)1 - fs) * f10, fac100 = fs * f00, fac110 = fs * f10;
             const R fac001 = ((R)1 - fs1) * f01, fac011 = ((R)1 - fs1) * f11, fac101 = fs1 * f01, fac111 = fs1 * f11;
-            auto B = [&](int id) { return ldt(absb + (size_t)(id - 1) * NG + ig); };
+            auto B = [&](int id) { return ldt(absb + ((id - 1) * NG + ig)); };
             const R t0 = sc * (fac000 * B(ind0) + fac010 * B(ind0 + 5) + fac100 * B(ind0 + 1) + fac110 * B(ind0 + 6));
             const R t1 = sc1 * (fac001 * B(ind1) + fac011 * B(ind1 + 5) + fac101 * B(ind1 + 1) + fac111 * B(ind1 + 6));
             if (b3) {
@@ -276,7 +277,7 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
             const R fac000 = ((R)1 - fs) * f00, fac010 = ((R)1 - fs) * f10, fac100 = fs * f00, fac110 = fs * f10;
             const R fac001 = ((R)1 - fs1) * f01, fac011 = ((R)1 - fs1) * f11, fac101 = fs1 * f01, fac111 = fs1 * f11;
             const R* absb = tab<R>(T_LW05_ABSB);
-            auto B = [&](int id) { return ldt(absb + (size_t)(id - 1) * NG + ig); };
+            auto B = [&](int id) { return ldt(absb + ((id - 1) * NG + ig)); };
             tg = sc * (fac000 * B(ind0) + fac010 * B(ind0 + 5) + fac100 * B(ind0 + 1) + fac110 * B(ind0 + 6)) +
                  sc1 * (fac001 * B(ind1) + fac011 * B(ind1 + 5) + fac101 * B(ind1 + 1) + fac111 * B(ind1 + 6)) + wxk * ccl4;
             fr = interp(tab<R>(T_LW05_FRACREFB), NG, jpl, ig, fpl);
@@ -489,7 +490,7 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
             const R taufor = ffac * interp(tab<R>(T_LW15_FORREF), NG, indf, ig, ffr);
             const R taun2 = scalen2 * minor2d(tab<R>(T_LW15_KA_MN2), 9, NG, jm, fm, indm, mf, ig);
             const R* absa = tab<R>(T_LW15_ABSA);
-            auto A = [&](int id) { return ldt(absa + (size_t)(id - 1) * NG + ig); };
+            auto A = [&](int id) { return ldt(absa + ((id - 1) * NG + ig)); };
             const R sumA = s0.fk0 * f00 * A(s0.id[0]) + s0.fk0 * f10 * A(s0.id[1]) + s0.fk1 * f00 * A(s0.id[2]) +
                            s0.fk1 * f10 * A(s0.id[3]) + s0.fk2 * f00 * A(s0.id[4]) + s0.fk2 * f10 * A(s0.id[5]);
             const R sumB = s1.fk0 * f01 * A(s1.id[0]) + s1.fk0 * f11 * A(s1.id[1]) + s1.fk1 * f01 * A(s1.id[2]) +
