@@ -261,6 +261,33 @@ typedef struct {
  * stream; needs rad_load_aerosols first. */
 int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faersw, float* faerlw, void* stream);
 
+/* ---- solar geometry of a radiation call ---- */
+typedef struct {
+    int32_t year, month, day, hour, minute, second;   /* forecast time (JDAT 1, 2, 3, 5, 6, 7) */
+    float deltsw;            /* SW calling interval, s */
+    float deltim;            /* model time step, s */
+    double solc0;            /* solar constant at 1 AU, W/m^2 (the year's table value, or 1366) */
+} RadSolarIn;
+typedef struct {
+    float sollag;            /* equation of time, radians */
+    float sindec, cosdec;    /* sin / cos of the solar declination */
+    float anginc;            /* solar angle increment per zenith-angle sample */
+    float solcon;            /* solar constant at today's sun-earth distance, W/m^2 */
+    int32_t nstp;            /* zenith-angle samples per SW call */
+} RadSolarState;
+
+/* The sun at the forecast time (sol_update_nmmb with solar, namgpu/physics/rrtm/phys_rrtm_sol_update.py,
+ * namgpu/kernels/phys_rrtm_sol_update.cu:60-210), on the host: no handle, no device. */
+int rad_sol_update(const RadSolarIn* in, RadSolarState* out);
+
+/* Mean cosine of the solar zenith angle of n columns over the SW interval (coszmn_nmmb,
+ * namgpu/physics/rrtm/phys_rrtm_coszmn.py:51-67, namgpu/kernels/phys_rrtm_coszmn.cu:60-114): glon, glat [n]
+ * radians (device); solhr = hours after 00 UTC; dtswav = SW interval in hours, sampled nrads times.  Writes
+ * coszen [n] (daytime mean: SW_COSZEN / COSZEN_V) and coszdg [n] (whole-interval mean: COSZDG_V).
+ * Asynchronous on stream. */
+int rad_coszmn(RadHandle* h, const RadSolarState* s, const float* glon, const float* glat, int64_t n, float solhr,
+               float dtswav, int32_t nrads, float* coszen, float* coszdg, void* stream);
+
 /* Device-time accounting of the library's own kernels (instrumentation; no counterpart in the reference,
  * which has none).  While enabled, rad_solve records CUDA events on its stream around the LW kernel, the
  * SW day-list kernels and the SW kernel; rad_profile_read waits for the last recorded event and returns

@@ -254,3 +254,30 @@ def aerosols(clim: dict, cols, aer_in: dict, which: str = "port", tables: bool =
             out[name] = tab[o:o + n].copy()
             o += n
     return out
+
+
+def solar(date, deltsw: float, deltim: float, solc0: float, glon=None, glat=None, solhr: float = 0.0,
+          dtswav: float = 1.0, nrads: int = 1, which: str = "port") -> dict:
+    """Solar geometry: sollag, sindec, cosdec, anginc, solcon, nstp of the forecast time date = (year, month,
+    day, hour, minute, second), and, for columns glon / glat (radians), coszen / coszdg."""
+    L = lib(which)
+    d = np.ascontiguousarray(date, dtype=np.int32)
+    st = np.zeros(5, np.float32)
+    nstp = np.zeros(1, np.int32)
+    n = 0 if glon is None else int(np.size(glon))
+    lo = _f(glon if glon is not None else np.zeros(1))
+    la = _f(glat if glat is not None else np.zeros(1))
+    cz = np.zeros(max(n, 1), np.float32)
+    cd = np.zeros(max(n, 1), np.float32)
+    rc = L.orc_solar(d.ctypes.data_as(_I), ctypes.c_float(deltsw), ctypes.c_float(deltim), ctypes.c_double(solc0),
+                     st.ctypes.data_as(_F), nstp.ctypes.data_as(_I), ctypes.c_int(n), lo.ctypes.data_as(_F),
+                     la.ctypes.data_as(_F), ctypes.c_float(solhr), ctypes.c_float(dtswav), ctypes.c_int(nrads),
+                     cz.ctypes.data_as(_F), cd.ctypes.data_as(_F))
+    if rc != 0:
+        raise RuntimeError("solar failed")
+    out = dict(zip(("sollag", "sindec", "cosdec", "anginc", "solcon"), st.tolist()))
+    out["state"] = st
+    out["nstp"] = int(nstp[0])
+    if n:
+        out["coszen"], out["coszdg"] = cz[:n], cd[:n]
+    return out

@@ -118,6 +118,12 @@ namespace r_seta {
 namespace r_aerp {
 #include "phys_rrtm_aer_property.cu"
 }
+namespace r_solu {
+#include "phys_rrtm_sol_update.cu"
+}
+namespace r_cosz {
+#include "phys_rrtm_coszmn.cu"
+}
 namespace r_swcld {
 #include "phys_rrtm_sw_cldprop.cu"
 }
@@ -1269,6 +1275,24 @@ int orc_aerosols(const int* iendwv, const float* haer, const float* prsref, cons
                                               denng.data(), idxcg.data(), kprfg.data(), aerosw, aerolw, ncol, 1, nlay,
                                               1, 1, 0, kNSW, kNLW, kNBT);
     });
+    return 0;
+}
+
+// Solar geometry from the reference's kernels sol_update_nmmb (phys_rrtm_sol_update.py: one thread) and
+// phys_rrtm_coszmn (phys_rrtm_coszmn.py:51-67, one row of n columns).  Same signature as the oracle's.
+int orc_solar(const int* date, float deltsw, float deltim, double solc0, float* state, int* nstp, int n,
+              const float* glon, const float* glat, float solhr, float dtswav, int nrads, float* coszen, float* coszdg)
+{
+    float out[4], st[4];
+    drv::launch(1, 1, 1, 1, [&] {
+        r_solu::sol_update_nmmb(date[0], date[1], date[2], date[3], date[4], date[5], deltsw, deltim, &solc0, out, st,
+                                nstp);
+    });
+    state[0] = st[0]; state[1] = st[1]; state[2] = st[2]; state[3] = st[3]; state[4] = out[3];
+    if (n > 0)
+        drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+            r_cosz::phys_rrtm_coszmn(glon, glat, coszen, coszdg, solhr, dtswav, nrads, st, n, 1);
+        });
     return 0;
 }
 }

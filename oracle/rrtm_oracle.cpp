@@ -11,6 +11,7 @@
 #include "rrtm_sw.hpp"
 #include "rrtm_mcica.hpp"
 #include "rrtm_aer.hpp"
+#include "rrtm_solar.hpp"
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -424,5 +425,17 @@ extern "C" int orc_aerosols(const int* iendwv, const float* haer, const float* p
         column(t, c, nlay, pi.data(), pl.data(), tl.data(), ql.data(), rh.data(), xlon[col], xlat[col], slmsk[col],
                aerosw + col, aerolw + col, (size_t)ncol);
     }
+    return 0;
+}
+
+// Solar geometry (rrtm_solar.hpp).  Same signature as the reference driver's: date[6] = year, month, day,
+// hour, minute, second; state[5] = sollag, sindec, cosdec, anginc, solcon; then coszen / coszdg of n columns.
+extern "C" int orc_solar(const int* date, float deltsw, float deltim, double solc0, float* state, int* nstp, int n,
+                         const float* glon, const float* glat, float solhr, float dtswav, int nrads, float* coszen,
+                         float* coszdg)
+{
+    orc::solar::update(date[0], date[1], date[2], date[3], date[4], date[5], deltsw, deltim, solc0, state, nstp);
+    for (int i = 0; i < n; ++i)
+        orc::solar::coszmn(glon[i], glat[i], state[0], state[1], state[2], solhr, dtswav, nrads, coszen[i], coszdg[i]);
     return 0;
 }

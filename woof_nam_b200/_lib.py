@@ -89,6 +89,17 @@ class RadAerColumns(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in AER_COL_FIELDS]
 
 
+class RadSolarIn(ctypes.Structure):
+    _fields_ = [("year", ctypes.c_int32), ("month", ctypes.c_int32), ("day", ctypes.c_int32),
+                ("hour", ctypes.c_int32), ("minute", ctypes.c_int32), ("second", ctypes.c_int32),
+                ("deltsw", ctypes.c_float), ("deltim", ctypes.c_float), ("solc0", ctypes.c_double)]
+
+
+class RadSolarState(ctypes.Structure):
+    _fields_ = [("sollag", ctypes.c_float), ("sindec", ctypes.c_float), ("cosdec", ctypes.c_float),
+                ("anginc", ctypes.c_float), ("solcon", ctypes.c_float), ("nstp", ctypes.c_int32)]
+
+
 SIGNATURES = {
     "rad_version": ([], ctypes.c_int),
     "rad_config_default": ([ctypes.POINTER(RadConfig), ctypes.c_int32], None),
@@ -109,6 +120,10 @@ SIGNATURES = {
                           ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p], ctypes.c_int),
     "rad_rdtemp": ([ctypes.c_void_p, ctypes.POINTER(RadRdtemp), ctypes.c_void_p], ctypes.c_int),
     "rad_load_aerosols": ([ctypes.c_void_p, ctypes.POINTER(RadAerClim)], ctypes.c_int),
+    "rad_sol_update": ([ctypes.POINTER(RadSolarIn), ctypes.POINTER(RadSolarState)], ctypes.c_int),
+    "rad_coszmn": ([ctypes.c_void_p, ctypes.POINTER(RadSolarState), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                    ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+                   ctypes.c_int),
     "rad_setaer": ([ctypes.c_void_p, ctypes.POINTER(RadAerColumns), ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                     ctypes.c_void_p], ctypes.c_int),
     "rad_profile_enable": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),

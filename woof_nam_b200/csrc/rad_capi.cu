@@ -39,6 +39,7 @@ __constant__ int c_sw_ns[15] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94
 #include "rad_post.cuh"
 #include "rad_rdtemp.cuh"
 #include "rad_aer.cuh"
+#include "rad_solar.cuh"
 
 using namespace rad;
 
@@ -959,6 +960,32 @@ int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faers
     AerArgs a{in->plvl, in->plyr, in->tlyr, in->qlyr, in->rhly, in->xlon, in->xlat, in->slmsk, faersw, faerlw, ncol,
               h->cfg.nlay};
     k_setaer<<<(unsigned)((ncol + AER_COLS - 1) / AER_COLS), AER_THREADS, 0, (cudaStream_t)stream>>>(a, t);
+    h->launches += 1;
+    RAD_CUDA(h, cudaGetLastError());
+    return RAD_OK;
+}
+
+int rad_sol_update(const RadSolarIn* in, RadSolarState* out)
+{
+    if (!in || !out) return fail(nullptr, RAD_E_INVALID, "rad_sol_update: null argument");
+    if (in->month < 1 || in->month > 12 || in->day < 1 || in->day > 31 || in->hour < 0 || in->hour > 23 ||
+        in->minute < 0 || in->minute > 59 || in->second < 0 || in->second > 60)
+        return fail(nullptr, RAD_E_INVALID, "rad_sol_update: date or time out of range");
+    if (!(in->deltim > 0.0f) || !(in->deltsw > 0.0f) || !(in->solc0 > 0.0))
+        return fail(nullptr, RAD_E_INVALID, "rad_sol_update: deltsw, deltim and solc0 must be positive");
+    solh::update(*in, *out);
+    return RAD_OK;
+}
+
+int rad_coszmn(RadHandle* h, const RadSolarState* s, const float* glon, const float* glat, int64_t n, float solhr,
+               float dtswav, int32_t nrads, float* coszen, float* coszdg, void* stream)
+{
+    if (!h || !s) return fail(h, RAD_E_INVALID, "rad_coszmn: null argument");
+    if (n < 0 || nrads < 1 || !(dtswav > 0.0f)) return fail(h, RAD_E_INVALID, "rad_coszmn: n, nrads or dtswav out of range");
+    if (n == 0) return RAD_OK;
+    if (!glon || !glat || !coszen || !coszdg) return fail(h, RAD_E_INVALID, "rad_coszmn: a required pointer is null");
+    CoszArgs a{glon, glat, coszen, coszdg, n, s->sollag, s->sindec, s->cosdec, solhr, dtswav, nrads};
+    k_coszmn<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a);
     h->launches += 1;
     RAD_CUDA(h, cudaGetLastError());
     return RAD_OK;
