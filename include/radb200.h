@@ -261,6 +261,35 @@ typedef struct {
  * stream; needs rad_load_aerosols first. */
 int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faersw, float* faerlw, void* stream);
 
+/* ---- grrad's radiation layers from the model state ---- */
+typedef struct {              /* model state of ncol columns: device pointers, float32, levels top first */
+    const float* pint;        /* [lm + 1][ncol] interface pressure, Pa (PINT) */
+    const float* pmid;        /* [lm][ncol] layer pressure, Pa (P_PHY) */
+    const float* prslk;       /* [lm][ncol] Exner function of the layer pressure (PRSLK) */
+    const float* t;           /* [lm][ncol] temperature, K (T) */
+    const float* q;           /* [lm][ncol] specific humidity, kg/kg (Q) */
+    const float* tsfc;        /* [ncol] surface (skin) temperature, K (TSFC) */
+} RadModelColumns;
+typedef struct {              /* radiation layers: device pointers, float32, lmk = lm + 1 layers, top first */
+    float* plvl;              /* [lmk + 1][ncol] level pressure, mb (RAD_PLVL; RadColumns.plvl) */
+    float* plyr;              /* [lmk][ncol] layer pressure, mb (RAD_PLYR) */
+    float* tlyr;              /* [lmk][ncol] layer temperature, K (RAD_TLYR) */
+    float* tlvl;              /* [lmk + 1][ncol] level temperature, K (TLVL) */
+    float* qlyr;              /* [lmk][ncol] specific humidity with the moisture floor (QLYR) */
+    float* rhly;              /* [lmk][ncol] relative humidity (RAD_RHLY; RadAerColumns.rhly) */
+    float* qstl;              /* [lmk][ncol] saturation specific humidity (RAD_QSTL) */
+    float* prslk1;            /* [lmk][ncol] Exner function (RAD_PRSLK1) */
+    float* tvly;              /* [lmk][ncol] virtual temperature, K (RAD_TVLY) */
+    float* tsfg;              /* [ncol] ground temperature, K (RAD_TSFG) */
+} RadLayerFields;
+
+/* grrad_nmmb's set-up of the radiation layers (phys-rrtm-grrad-setup and the layer part of
+ * phys-rrtm-grrad-gases: namgpu/physics/rrtm/phys_rrtm_grrad_setup.py, phys_rrtm_grrad_gases.cu:55-110),
+ * for the NAM orientation (model top first) with the extra top layer: lm model layers -> lm + 1 radiation
+ * layers.  Asynchronous on stream. */
+int rad_grrad_setup(RadHandle* h, const RadModelColumns* in, int64_t ncol, int32_t lm, const RadLayerFields* out,
+                    void* stream);
+
 /* ---- solar geometry of a radiation call ---- */
 typedef struct {
     int32_t year, month, day, hour, minute, second;   /* forecast time (JDAT 1, 2, 3, 5, 6, 7) */

@@ -281,3 +281,26 @@ def solar(date, deltsw: float, deltim: float, solc0: float, glon=None, glat=None
     if n:
         out["coszen"], out["coszdg"] = cz[:n], cd[:n]
     return out
+
+
+GRRAD_FIELDS = ("plvl", "plyr", "tlyr", "tlvl", "qlyr", "rhly", "qstl", "prslk1", "tvly", "tsfg")
+
+
+def grrad_setup(model: dict, which: str = "port") -> dict:
+    """grrad's radiation layers of a model state (pint [lm + 1][n], pmid, prslk, t, q [lm][n] in Pa / K,
+    tsfc [n]): plvl, tlvl [lm + 2][n], plyr, tlyr, qlyr, rhly, qstl, prslk1, tvly [lm + 1][n], tsfg [n]."""
+    L = lib(which)
+    lm, n = model["pmid"].shape
+    keep = [_f(model[k]) for k in ("pint", "pmid", "prslk", "t", "q", "tsfc")]
+    lmk, lmp = lm + 1, lm + 2
+    sizes = {"plvl": lmp, "plyr": lmk, "tlyr": lmk, "tlvl": lmp, "qlyr": lmk, "rhly": lmk, "qstl": lmk,
+             "prslk1": lmk, "tvly": lmk, "tsfg": 1}
+    out = np.zeros(sum(sizes.values()) * n, np.float32)
+    rc = L.orc_grrad_setup(ctypes.c_int(lm), ctypes.c_int(n), *[a.ctypes.data_as(_F) for a in keep], out.ctypes.data_as(_F))
+    if rc != 0:
+        raise RuntimeError("grrad_setup failed")
+    res, o = {}, 0
+    for k in GRRAD_FIELDS:
+        res[k] = out[o:o + sizes[k] * n].reshape(sizes[k], n) if k != "tsfg" else out[o:o + n]
+        o += sizes[k] * n
+    return res

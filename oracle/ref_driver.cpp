@@ -124,6 +124,12 @@ namespace r_solu {
 namespace r_cosz {
 #include "phys_rrtm_coszmn.cu"
 }
+namespace r_grs {
+#include "phys_rrtm_grrad_setup.cu"
+}
+namespace r_grg {
+#include "phys_rrtm_grrad_gases.cu"
+}
 namespace r_swcld {
 #include "phys_rrtm_sw_cldprop.cu"
 }
@@ -1293,6 +1299,31 @@ int orc_solar(const int* date, float deltsw, float deltim, double solc0, float* 
         drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
             r_cosz::phys_rrtm_coszmn(glon, glat, coszen, coszdg, solhr, dtswav, nrads, st, n, 1);
         });
+    return 0;
+}
+
+// grrad's radiation-layer set-up from the reference's kernels rrtm_grrad_setup (phys_rrtm_grrad_setup.py: one
+// tracer, np3d 0, ntoz 0, ivflip 0) then phys_rrtm_grrad_gases (ivflip 0), one row of n columns.  Same
+// signature as the oracle's orc_grrad_setup.
+int orc_grrad_setup(int lm, int n, const float* pint, const float* pmid, const float* prslk, const float* t,
+                    const float* q, const float* tsfc, float* out)
+{
+    const int lmk = lm + 1, lmp = lm + 2;
+    const size_t L = (size_t)lmk * n, P = (size_t)lmp * n, M = (size_t)lm * n;
+    float *plvl = out, *plyr = plvl + P, *tlyr = plyr + L, *tlvl = tlyr + L, *qlyr = tlvl + P, *rhly = qlyr + L,
+          *qstl = rhly + L, *prslk1 = qstl + L, *tvly = prslk1 + L, *tsfg = tvly + L;
+    std::vector<float> tracer(M, 0.0f), cldf(M, 0.0f), dum(M, 0.0f), cldfk1(L), tracer1(L), gdum(L), olyr(L), tskn(n),
+        tem2da(L), tem2db(P), tsfa(n);
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_grs::rrtm_grrad_setup(pint, pmid, prslk, t, q, tracer.data(), cldf.data(), dum.data(), dum.data(), dum.data(),
+                                tsfc, plvl, plyr, tlyr, prslk1, rhly, qstl, cldfk1.data(), tracer1.data(), gdum.data(),
+                                gdum.data(), gdum.data(), olyr.data(), tskn.data(), tsfg, qlyr, tvly, n, 1, lm, 1, 0, 0,
+                                0);
+    });
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_grg::phys_rrtm_grrad_gases(plyr, plvl, tlyr, tskn.data(), t, q, tlvl, tvly, qlyr, tem2da.data(),
+                                     tem2db.data(), tsfa.data(), n, 1, lm, 0);
+    });
     return 0;
 }
 }

@@ -12,6 +12,7 @@
 #include "rrtm_mcica.hpp"
 #include "rrtm_aer.hpp"
 #include "rrtm_solar.hpp"
+#include "rrtm_grrad.hpp"
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -439,3 +440,37 @@ extern "C" int orc_solar(const int* date, float deltsw, float deltim, double sol
         orc::solar::coszmn(glon[i], glat[i], state[0], state[1], state[2], solhr, dtswav, nrads, coszen[i], coszdg[i]);
     return 0;
 }
+
+// grrad's radiation-layer set-up (rrtm_grrad.hpp) of n columns, [level][n] top first.  out = plvl [lm + 2],
+// plyr, tlyr [lm + 1], tlvl [lm + 2], qlyr, rhly, qstl, prslk1, tvly [lm + 1] (each [..][n]) and tsfg [n],
+// concatenated in that order.  Same signature as the reference driver's.
+extern "C" int orc_grrad_setup(int lm, int n, const float* pint, const float* pmid, const float* prslk,
+                               const float* t, const float* q, const float* tsfc, float* out)
+{
+    const int lmk = lm + 1, lmp = lm + 2;
+    const size_t L = (size_t)lmk * n, P = (size_t)lmp * n;
+    float *plvl = out, *plyr = plvl + P, *tlyr = plyr + L, *tlvl = tlyr + L, *qlyr = tlvl + P, *rhly = qlyr + L,
+          *qstl = rhly + L, *prslk1 = qstl + L, *tvly = prslk1 + L, *tsfg = tvly + L;
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < n; ++c) {
+        std::vector<float> pi(lm + 1), pm(lm), pk(lm), tt(lm), qq(lm);
+        for (int k = 0; k <= lm; ++k) pi[k] = pint[(size_t)k * n + c];
+        for (int k = 0; k < lm; ++k) {
+            pm[k] = pmid[(size_t)k * n + c]; pk[k] = prslk[(size_t)k * n + c];
+            tt[k] = t[(size_t)k * n + c]; qq[k] = q[(size_t)k * n + c];
+        }
+        std::vector<float> a(lmp), b(lmk), tl(lmk), tv(lmp), ql(lmk), rh(lmk), qs(lmk), p1(lmk), vy(lmk);
+        float ts;
+        orc::grrad::column(lm, pi.data(), pm.data(), pk.data(), tt.data(), qq.data(), tsfc[c], a.data(), b.data(),
+                           tl.data(), tv.data(), ql.data(), rh.data(), qs.data(), p1.data(), vy.data(), ts);
+        for (int k = 0; k < lmp; ++k) { plvl[(size_t)k * n + c] = a[k]; tlvl[(size_t)k * n + c] = tv[k]; }
+        for (int k = 0; k < lmk; ++k) {
+            plyr[(size_t)k * n + c] = b[k]; tlyr[(size_t)k * n + c] = tl[k]; qlyr[(size_t)k * n + c] = ql[k];
+            rhly[(size_t)k * n + c] = rh[k]; qstl[(size_t)k * n + c] = qs[k]; prslk1[(size_t)k * n + c] = p1[k];
+            tvly[(size_t)k * n + c] = vy[k];
+        }
+        tsfg[c] = ts;
+    }
+    return 0;
+}
+

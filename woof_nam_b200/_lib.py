@@ -89,6 +89,18 @@ class RadAerColumns(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in AER_COL_FIELDS]
 
 
+MODEL_FIELDS = ("pint", "pmid", "prslk", "t", "q", "tsfc")
+LAYER_FIELDS = ("plvl", "plyr", "tlyr", "tlvl", "qlyr", "rhly", "qstl", "prslk1", "tvly", "tsfg")
+
+
+class RadModelColumns(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in MODEL_FIELDS]
+
+
+class RadLayerFields(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in LAYER_FIELDS]
+
+
 class RadSolarIn(ctypes.Structure):
     _fields_ = [("year", ctypes.c_int32), ("month", ctypes.c_int32), ("day", ctypes.c_int32),
                 ("hour", ctypes.c_int32), ("minute", ctypes.c_int32), ("second", ctypes.c_int32),
@@ -121,6 +133,8 @@ SIGNATURES = {
     "rad_rdtemp": ([ctypes.c_void_p, ctypes.POINTER(RadRdtemp), ctypes.c_void_p], ctypes.c_int),
     "rad_load_aerosols": ([ctypes.c_void_p, ctypes.POINTER(RadAerClim)], ctypes.c_int),
     "rad_sol_update": ([ctypes.POINTER(RadSolarIn), ctypes.POINTER(RadSolarState)], ctypes.c_int),
+    "rad_grrad_setup": ([ctypes.c_void_p, ctypes.POINTER(RadModelColumns), ctypes.c_int64, ctypes.c_int32,
+                         ctypes.POINTER(RadLayerFields), ctypes.c_void_p], ctypes.c_int),
     "rad_coszmn": ([ctypes.c_void_p, ctypes.POINTER(RadSolarState), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                     ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                    ctypes.c_int),

@@ -227,3 +227,17 @@ WORKLOADS = {
 def workload(name: str, ncol: int | None = None) -> Columns:
     n, seed, stress = WORKLOADS[name]
     return make_columns(n if ncol is None else ncol, seed, stress)
+
+
+def model_state(cols: "Columns") -> dict:
+    """The model state a request's radiation layers come from (grrad's inputs): the lm = nlay - 1 model
+    layers of the columns without the extra top layer -- interface and layer pressure in Pa, the Exner
+    function (p / 1e5)^(Rd / cp), temperature, specific humidity -- and the skin temperature."""
+    pmid = (cols.plyr[1:].astype(np.float64) * 100.0)
+    return {"pint": (cols.plvl[1:].astype(np.float64) * 100.0).astype(np.float32),
+            "pmid": pmid.astype(np.float32),
+            "prslk": ((pmid / 1.0e5) ** (2.8705e2 / 1.0046e3)).astype(np.float32),
+            "t": np.ascontiguousarray(cols.tlyr[1:], dtype=np.float32),
+            "q": np.ascontiguousarray(cols.qlyr[1:], dtype=np.float32),
+            "tsfc": np.ascontiguousarray(cols.tsfg, dtype=np.float32)}
+

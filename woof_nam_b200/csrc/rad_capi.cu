@@ -40,6 +40,7 @@ __constant__ int c_sw_ns[15] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94
 #include "rad_rdtemp.cuh"
 #include "rad_aer.cuh"
 #include "rad_solar.cuh"
+#include "rad_grrad.cuh"
 
 using namespace rad;
 
@@ -960,6 +961,23 @@ int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faers
     AerArgs a{in->plvl, in->plyr, in->tlyr, in->qlyr, in->rhly, in->xlon, in->xlat, in->slmsk, faersw, faerlw, ncol,
               h->cfg.nlay};
     k_setaer<<<(unsigned)((ncol + AER_COLS - 1) / AER_COLS), AER_THREADS, 0, (cudaStream_t)stream>>>(a, t);
+    h->launches += 1;
+    RAD_CUDA(h, cudaGetLastError());
+    return RAD_OK;
+}
+
+int rad_grrad_setup(RadHandle* h, const RadModelColumns* in, int64_t ncol, int32_t lm, const RadLayerFields* out,
+                    void* stream)
+{
+    if (!h || !in || !out) return fail(h, RAD_E_INVALID, "rad_grrad_setup: null argument");
+    if (ncol < 0 || lm < 1 || lm + 1 > NLAY_MAX) return fail(h, RAD_E_INVALID, "rad_grrad_setup: ncol or lm out of range");
+    if (ncol == 0) return RAD_OK;
+    if (!in->pint || !in->pmid || !in->prslk || !in->t || !in->q || !in->tsfc || !out->plvl || !out->plyr ||
+        !out->tlyr || !out->tlvl || !out->qlyr || !out->rhly || !out->qstl || !out->prslk1 || !out->tvly || !out->tsfg)
+        return fail(h, RAD_E_INVALID, "rad_grrad_setup: a required pointer is null");
+    GrradArgs a{in->pint, in->pmid, in->prslk, in->t, in->q, in->tsfc, out->plvl, out->plyr, out->tlyr, out->tlvl,
+                out->qlyr, out->rhly, out->qstl, out->prslk1, out->tvly, out->tsfg, ncol, lm};
+    k_grrad_setup<<<(unsigned)((ncol + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a);
     h->launches += 1;
     RAD_CUDA(h, cudaGetLastError());
     return RAD_OK;
