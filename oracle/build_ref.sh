@@ -1,7 +1,7 @@
 #!/usr/bin/env bash
 # Build oracle/_ref/libref_rrtm.so: the reference's own RRTM kernel sources (read in place from the
 # reference tree, never copied) compiled as host C++ behind oracle/ref_shim.h and driven by
-# oracle/ref_driver.cpp.  Needs the reference tree; the GPU box uses the prebuilt library.
+# oracle/ref_driver.cpp.  Needs the reference tree; machines without it use the prebuilt library.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 REF="${1:-/root/reference}"
