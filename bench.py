@@ -349,8 +349,10 @@ def main():
     lw_ms, sw_ms = prof["lw_ms"] / max(prof["solves"], 1), prof["sw_ms"] / max(prof["solves"], 1)
     lw_tf = ops["lw_flops_per_col"] * n / (lw_ms * 1e-3) / 1e12
     sw_tf = ops["sw_flops_per_daycol"] * nday / (sw_ms * 1e-3) / 1e12
-    # the mixed precision runs the two-kernel LW (gas optics, then sweeps, per chunk) and sw2_column_kernel
-    lw_name, sw_name = "lw3_optics_kernel+lw3_sweep_kernel", "sw2_column_kernel"
+    # the mixed precision runs the two-kernel LW (gas optics, then sweeps, per chunk) and the two-kernel SW
+    # (set-up and optics into shared-memory images, then sweeps, per chunk of day columns)
+    lw_name = "lw3_optics_kernel+lw3_sweep_kernel"
+    sw_name = "sw2_column_kernel" if mcfg.sw_sweep_chunk < 0 else "sw3_optics_kernel+sw3_sweep_kernel"
     dom = sw_name if sw_ms >= lw_ms else lw_name
     achieved = sw_tf if dom == sw_name else lw_tf
     traffic = None
@@ -376,7 +378,7 @@ def main():
                        "input_bytes": in_bytes, "output_bytes": out_bytes,
                        "l2": f"inputs ({in_bytes / 1e9:.1f} GB) larger than L2 (126 MB); no flush",
                        "parallelism": f"replicas x{ws} (one ensemble member per GPU)",
-                       "lw_chunk": mcfg.lw_chunk},
+                       "lw_chunk": mcfg.lw_chunk, "sw_sweep_chunk": mcfg.sw_sweep_chunk},
             "roofline": {"bound": "fp32", "kernel": dom, "achieved": achieved, "peak": peak_tf,
                          "unit": "TFLOP/s", "frac": achieved / peak_tf, "traffic": traffic,
                          "peak_source": f"nominal FP32 pipe 148 SM x 128 lanes x 2 at the measured sm_max "

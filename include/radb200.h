@@ -68,6 +68,9 @@ typedef struct {
     int32_t lw_chunk;        /* mixed precision: columns per LW chunk of the two-kernel LW (gas optics through
                                 ~95 KB per column of scratch, then the sweeps); 0 = 32768; negative = the
                                 single-kernel LW (gas optics in shared memory, no scratch) */
+    int32_t sw_sweep_chunk;  /* mixed precision: day columns per chunk of the two-kernel SW (set-up, cloud and
+                                gas optics through ~64 KB per column of scratch, then the sweeps); 0 = 65536;
+                                negative = the single-kernel SW (no scratch besides the R/T stores) */
 } RadConfig;
 
 /* Column inputs (device pointers, float32).  ncol columns, nlay layers, nlp1 = nlay + 1 levels. */

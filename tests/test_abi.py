@@ -65,6 +65,7 @@ def test_version_and_defaults(lib):
     assert (c.nlay, c.precision, c.route, c.iswmode, c.diagnostic) == (61, _lib.PREC["mixed"], 0, 2, 0)
     assert (c.iovrlw, c.iovrsw, c.lw_seed0, c.sw_seed0) == (1, 1, 140, 1)
     assert c.sw_chunk == 32768 and abs(c.cpathfac - 1.5) < 1e-7
+    assert c.lw_chunk == 0 and c.sw_sweep_chunk == 0
 
 
 @pytest.mark.parametrize("field,value", [("nlay", 1), ("nlay", 100000), ("iswmode", 0), ("iswmode", 4),

@@ -27,7 +27,8 @@ class RadConfig(ctypes.Structure):
                 ("iswmode", ctypes.c_int32), ("diagnostic", ctypes.c_int32), ("window_cols", ctypes.c_int32),
                 ("sw_chunk", ctypes.c_int32), ("iovrlw", ctypes.c_int32), ("iovrsw", ctypes.c_int32),
                 ("lw_seed0", ctypes.c_int32), ("sw_seed0", ctypes.c_int32), ("cpathfac", ctypes.c_float),
-                ("parts", ctypes.c_int32), ("lw_chunk", ctypes.c_int32)]
+                ("parts", ctypes.c_int32), ("lw_chunk", ctypes.c_int32),
+                ("sw_sweep_chunk", ctypes.c_int32)]
 
 
 class RadColumns(ctypes.Structure):

@@ -64,6 +64,8 @@ struct RadHandle {
     int64_t lw3_cap = 0;                           // columns d_lw3 holds
     int* d_lw3list = nullptr;                      // [1 + lw3_cap]: count, then the chunk's float64 columns
     float* d_swrt = nullptr;                       // SW layer R/T stores, sw2_rt_floats() per CTA of the SW grid
+    int4* d_swimg = nullptr;                       // two-kernel SW: shared-memory images of one chunk's columns
+    int64_t swimg_cap = 0;                         // columns d_swimg holds
     float* d_aerf = nullptr;                       // aerosol band tables of the loaded month (AF_* offsets)
     int* d_aeri = nullptr;                         // their integer part (AI_* offsets)
     int nsm = 148;                                 // SMs of the device (grid of the float64 column kernel)
@@ -286,6 +288,13 @@ int64_t lw3_chunk(const RadConfig& cfg)
     return cfg.lw_chunk > 0 ? cfg.lw_chunk : 32768;
 }
 
+// Day columns per chunk of the two-kernel SW (mixed precision), 0 when the single-kernel SW runs.
+int64_t sw3_chunk(const RadConfig& cfg)
+{
+    if (cfg.precision != RAD_PREC_MIXED || cfg.sw_sweep_chunk < 0) return 0;
+    return cfg.sw_sweep_chunk > 0 ? cfg.sw_sweep_chunk : 65536;
+}
+
 // Scratch for a launch of ntot columns: day list arrays, CUB temp, chunk minima, McICA words.
 int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
 {
@@ -314,6 +323,15 @@ int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
     }
     if (h->cfg.precision == RAD_PREC_MIXED && (h->cfg.parts & RAD_PART_SW) && !h->d_swrt)
         RAD_CUDA(h, cudaMalloc((void**)&h->d_swrt, (size_t)sw2_rt_bytes(h->nsm)));
+    const int64_t swc = sw3_chunk(h->cfg);
+    if (swc > 0 && (h->cfg.parts & RAD_PART_SW) && std::min(swc, ntot) > h->swimg_cap) {
+        if (h->d_swimg) cudaFree(h->d_swimg);
+        h->d_swimg = nullptr;
+        h->swimg_cap = 0;
+        const int64_t need = std::min(swc, ntot);
+        RAD_CUDA(h, cudaMalloc((void**)&h->d_swimg, (size_t)need * sw2_image_bytes(true)));
+        h->swimg_cap = need;
+    }
     if (h->cfg.route == RAD_ROUTE_MCICA && ntot * h->cfg.nlay > h->mask_cap) {
         if (h->d_lwm) cudaFree(h->d_lwm);
         h->d_lwm = nullptr;
@@ -503,6 +521,22 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 sw2_column_kernel<false><<<(unsigned)ntot, SW2_THREADS, smem, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd,
                                                                                      h->d_err, nullptr);
+            } else if (sw3_chunk(cfg) > 0) {
+                // per chunk of day indices (the day count stays on the device: chunks past it exit at once):
+                // set-up and optics one CTA per column into the images, then the sweeps walk the chunk
+                const int64_t swc = sw3_chunk(cfg);
+                const size_t smem1 = sw2_image_begin() + sw2_image_bytes(any_aer);
+                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw3_optics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
+                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw3_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                for (int64_t d0 = 0; d0 < ntot; d0 += swc) {
+                    const int64_t nc = std::min(swc, ntot - d0);
+                    sw3_optics_kernel<<<(unsigned)nc, SW2_THREADS, smem1, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd,
+                                                                             h->d_err, (int)d0, h->d_swimg);
+                    sw3_sweep_kernel<<<(unsigned)(SW2_CTAS_PER_SM * h->nsm), SW2_THREADS, smem, st>>>(
+                        bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, h->d_err, (int)d0, (int)nc, h->d_swimg, h->d_swrt);
+                    h->launches += 2;
+                }
+                h->launches -= 1;      // the one launch counted below
             } else {       // SW2_CTAS_PER_SM CTAs per SM walk the day list, each with its R/T store
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 sw2_column_kernel<true><<<(unsigned)(SW2_CTAS_PER_SM * h->nsm), SW2_THREADS, smem, st>>>(
@@ -544,6 +578,7 @@ void rad_config_default(RadConfig* cfg, int32_t nlay)
     cfg->cpathfac = 1.5f;
     cfg->parts = RAD_PART_LW | RAD_PART_SW;
     cfg->lw_chunk = 0;
+    cfg->sw_sweep_chunk = 0;
 }
 
 int rad_create(const RadConfig* cfg, RadHandle** out)
@@ -688,6 +723,8 @@ int64_t rad_workspace_bytes(const RadHandle* h, int64_t ncol)
             b += std::min(lwc, ncol) * lw3_block_floats(h->cfg.nlay) * (int64_t)sizeof(float);
         if (h->cfg.route == RAD_ROUTE_MCICA) b += 9 * (int64_t)h->cfg.nlay * ncol * (int64_t)sizeof(uint32_t);
         if (h->cfg.precision == RAD_PREC_MIXED && (h->cfg.parts & RAD_PART_SW)) b += sw2_rt_bytes(h->nsm);
+        const int64_t swc = sw3_chunk(h->cfg);
+        if (swc > 0 && (h->cfg.parts & RAD_PART_SW)) b += std::min(swc, ncol) * (int64_t)sw2_image_bytes(true);
     }
     return b;
 }
@@ -1062,7 +1099,7 @@ void rad_destroy(RadHandle* h)
     for (void* p : {(void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
                     (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
                     (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub, (void*)h->d_lwm,
-                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt, (void*)h->d_aerf,
+                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt, (void*)h->d_swimg, (void*)h->d_aerf,
                     (void*)h->d_aeri})
         if (p) cudaFree(p);
     delete h;

@@ -347,24 +347,28 @@ __device__ __forceinline__ float sw2_rayl_coef(int g)
 // banks.
 constexpr int SW2_KS = NLAY_MAX + 1;
 struct SwSh2 {
+    // read by the set-up and optics phases only, and the sweep phase's reduction scratch
+    double fn[SW2_WARPS][NLAY_MAX + 2];        // per-warp level sums of zsolar * (down - up), passes combined
+    double sc[SW2_WARPS][18];                  // per-warp scalar sums, clear (0..8) and cloudy (9..17)
     float fac00[NLAY_MAX], fac01[NLAY_MAX], fac10[NLAY_MAX], fac11[NLAY_MAX];
-    float selffac[NLAY_MAX], selffrac[NLAY_MAX], forfac[NLAY_MAX], forfrac[NLAY_MAX], colmol[NLAY_MAX];
+    float selffac[NLAY_MAX], selffrac[NLAY_MAX], forfac[NLAY_MAX], forfrac[NLAY_MAX];
     float colamt[6][NLAY_MAX];
     int jp[NLAY_MAX], jt[NLAY_MAX], jt1[NLAY_MAX], indself[NLAY_MAX], indfor[NLAY_MAX];
-    float cfrac[NLAY_MAX], cldfrc[NLAY_MAX];
+    float cfrac[NLAY_MAX];
+    unsigned char low[NLAY_MAX];
+    int task_next;                             // phase B task counter (for_each_band_pair)
+    // read by the sweep phase: from here to the end (and the aerosol block) is the column's image
+    alignas(16) float colmol[NLAY_MAX];
+    float cldfrc[NLAY_MAX];
     float taucw[14][SW2_KS], ssacw[14][SW2_KS], asycw[14][SW2_KS], tabsc[14][SW2_KS];
     float taug[SW_NGPT][SW2_KS];
     float raylc[SW_NGPT];                      // Rayleigh optical depth per unit colmol (band 24: upper atmosphere)
     float taur24[8][SW2_KS];                   // band 24 Rayleigh optical depth below laytrop
     float sfluxzen[SW_NGPT];
     double rdelp[NLAY_MAX];                    // heatfac / delp, float64
-    double fn[SW2_WARPS][NLAY_MAX + 2];        // per-warp level sums of zsolar * (down - up), passes combined
-    double sc[SW2_WARPS][18];                  // per-warp scalar sums, clear (0..8) and cloudy (9..17)
     float cosz, sntz, ssolar, albbm[2], albdf[2], zcf0, zcf1;
     int laytrop, kmin8, kminw;
-    unsigned char low[NLAY_MAX];
     uint32_t mcw[4][NLAY_MAX];                 // McICA route: the column's sub-column cloud words
-    int task_next;                             // phase B task counter (for_each_band_pair)
 };
 // Dynamic tail: the aerosol block (present only with aerosol inputs) and the segment checkpoints.
 struct SwAer {
@@ -593,10 +597,24 @@ __host__ __device__ constexpr int64_t sw2_rt_floats()
 }
 inline int64_t sw2_rt_bytes(int nsm) { return (int64_t)SW2_CTAS_PER_SM * nsm * sw2_rt_floats() * (int64_t)sizeof(float); }
 
+// Parts of the column solve a call runs: all of it, or (split over two kernels) phases A and B into a
+// shared-memory image in global memory, then phase C from that image.
+constexpr int SW2_ALL = 0, SW2_OPTICS = 1, SW2_SWEEP = 2;
+// The shared-memory image phase C reads: from SwSh2::colmol to the end of SwSh2 and, with aerosol, the
+// aerosol block after it; sw2_image_bytes rounds it up to 16-byte units.
+__host__ __device__ constexpr size_t sw2_image_begin() { return offsetof(SwSh2, colmol); }
+__host__ __device__ constexpr size_t sw2_image_bytes(bool aer)
+{
+    return ((sizeof(SwSh2) - sw2_image_begin() + (aer ? sizeof(SwAer) : 0)) + 15) / 16 * 16;
+}
+static_assert(offsetof(SwSh2, colmol) % 16 == 0, "the image starts on a 16-byte boundary");
+
 // One sunlit column (day index d) by the CTA; STORE: rt = the CTA's R/T store, else the R/T is recomputed.
-template <bool STORE>
+// PART: SW2_ALL, or SW2_OPTICS (phases A and B, the shared memory then copied to img) / SW2_SWEEP (shared
+// memory loaded from img, then phase C).
+template <bool STORE, int PART = SW2_ALL>
 __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const float* ex, const double* exd,
-                                           int* err, int d, float* rt)
+                                           int* err, int d, float* rt, int4* img = nullptr)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SwSh2& s = *reinterpret_cast<SwSh2*>(smem_raw);
@@ -615,6 +633,14 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
     const int64_t col = gcol - bt.off[rq];
     const int tid = threadIdx.x;
     const double heatfac = 9.80665 * 1.0e-2 / 1.0046e3;
+    if (PART == SW2_SWEEP) {   // every 16-byte piece of the image in flight at once (cp.async.cg: L2 to shared)
+        const uint32_t sb = (uint32_t)__cvta_generic_to_shared(smem_raw + sw2_image_begin());
+        for (int i = tid; i < (int)(sw2_image_bytes(any_aer) / 16); i += SW2_THREADS)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sb + 16u * (uint32_t)i), "l"(img + i)
+                         : "memory");
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
+    } else {
     // ---- phase A1: layer coefficients (threads = layers), aerosol, heating factors
     for (int k0 = tid; k0 < nlay; k0 += SW2_THREADS) {
         SwCoef<float> c;
@@ -686,6 +712,12 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
         if (g >= 66 && g < 74 && k0 < s.laytrop) s.taur24[g - 66][k0] = tr;
     });
     __syncthreads();
+    }
+    if (PART == SW2_OPTICS) {
+        const int4* sm = reinterpret_cast<const int4*>(smem_raw + sw2_image_begin());
+        for (int i = tid; i < (int)(sw2_image_bytes(any_aer) / 16); i += SW2_THREADS) img[i] = sm[i];
+        return;
+    }
     // ---- phase C: spcvrtc, one g-point per lane, both passes
     const int warp = tid >> 5, lane = tid & 31;
     bool act;
@@ -908,6 +940,33 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
     float* rt = rts + (int64_t)blockIdx.x * sw2_rt_floats();
     for (int d = blockIdx.x; d < nday; d += gridDim.x) {
         sw2_column<true>(bt, any_aer, ex, exd, err, d, rt);
+        __syncthreads();                       // shared memory is reused by the next column
+    }
+}
+
+// The SW solve split in two kernels per chunk of day indices [d0, d0 + nc): sw3_optics_kernel, one CTA per
+// column, runs phases A and B (set-up, cloud and gas optics: no sweep registers, so three CTAs per SM) and
+// writes the shared-memory image; sw3_sweep_kernel, SW2_CTAS_PER_SM CTAs per SM walking the chunk, loads
+// each image and runs phase C with its R/T store.  Same arithmetic as sw2_column_kernel<true>, same bits.
+constexpr int SW3_CHUNK = 32768;                               // day columns per optics / sweep pair
+__global__ void __launch_bounds__(SW2_THREADS, 3)
+sw3_optics_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, const double* exd, int* err,
+                  int d0, int4* img)
+{
+    const int d = d0 + (int)blockIdx.x;
+    if (d >= *bt.req[0].nday) return;
+    sw2_column<false, SW2_OPTICS>(bt, any_aer, ex, exd, err, d, nullptr,
+                                  img + (size_t)blockIdx.x * (sw2_image_bytes(any_aer) / 16));
+}
+__global__ void __launch_bounds__(SW2_THREADS, SW2_CTAS_PER_SM)
+sw3_sweep_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, const double* exd, int* err,
+                 int d0, int nc, const int4* img, float* rts)
+{
+    const int nday = *bt.req[0].nday;
+    float* rt = rts + (int64_t)blockIdx.x * sw2_rt_floats();
+    for (int i = blockIdx.x; i < nc && d0 + i < nday; i += gridDim.x) {
+        sw2_column<true, SW2_SWEEP>(bt, any_aer, ex, exd, err, d0 + i, rt,
+                                    const_cast<int4*>(img) + (size_t)i * (sw2_image_bytes(any_aer) / 16));
         __syncthreads();                       // shared memory is reused by the next column
     }
 }

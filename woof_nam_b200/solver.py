@@ -44,6 +44,7 @@ class SolverConfig:
     sw_seed0: int = 1
     parts: str = "both"              # "lw", "sw" or "both": which solves run (lslwr / lsswr steps)
     lw_chunk: int = 0                # mixed: columns per two-kernel LW chunk (0 = 32768, < 0 single kernel)
+    sw_sweep_chunk: int = 0          # mixed: day columns per two-kernel SW chunk (0 = 65536, < 0 single kernel)
 
 
 def output_shapes(nlay: int, ncol: int, route: str = "nam") -> dict:
@@ -77,6 +78,7 @@ class RadSolver:
         c.cpathfac = self.cfg.cpathfac
         c.parts = _lib.PARTS[self.cfg.parts]
         c.lw_chunk = self.cfg.lw_chunk
+        c.sw_sweep_chunk = self.cfg.sw_sweep_chunk
         c.iovrlw, c.iovrsw = self.cfg.iovrlw, self.cfg.iovrsw
         c.lw_seed0, c.sw_seed0 = self.cfg.lw_seed0, self.cfg.sw_seed0
         h = ctypes.c_void_p()
