@@ -66,6 +66,8 @@ struct RadHandle {
     float* d_swrt = nullptr;                       // SW layer R/T stores, sw2_rt_floats() per CTA of the SW grid
     int4* d_swimg = nullptr;                       // two-kernel SW: shared-memory images of one chunk's columns
     int64_t swimg_cap = 0;                         // columns d_swimg holds
+    int* d_swq = nullptr;                          // two-kernel SW: one column counter per chunk
+    int64_t swq_cap = 0;
     float* d_aerf = nullptr;                       // aerosol band tables of the loaded month (AF_* offsets)
     int* d_aeri = nullptr;                         // their integer part (AI_* offsets)
     int nsm = 148;                                 // SMs of the device (grid of the float64 column kernel)
@@ -332,6 +334,14 @@ int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
         RAD_CUDA(h, cudaMalloc((void**)&h->d_swimg, (size_t)need * sw2_image_bytes(true)));
         h->swimg_cap = need;
     }
+    if (swc > 0 && (h->cfg.parts & RAD_PART_SW) && (ntot + swc - 1) / swc > h->swq_cap) {
+        if (h->d_swq) cudaFree(h->d_swq);
+        h->d_swq = nullptr;
+        h->swq_cap = 0;
+        const int64_t need = (ntot + swc - 1) / swc;
+        RAD_CUDA(h, cudaMalloc((void**)&h->d_swq, (size_t)need * sizeof(int)));
+        h->swq_cap = need;
+    }
     if (h->cfg.route == RAD_ROUTE_MCICA && ntot * h->cfg.nlay > h->mask_cap) {
         if (h->d_lwm) cudaFree(h->d_lwm);
         h->d_lwm = nullptr;
@@ -528,12 +538,14 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                 const size_t smem1 = sw2_image_begin() + sw2_image_bytes(any_aer);
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw3_optics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw3_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                RAD_CUDA(h, cudaMemsetAsync(h->d_swq, 0, (size_t)((ntot + swc - 1) / swc) * sizeof(int), st));
                 for (int64_t d0 = 0; d0 < ntot; d0 += swc) {
                     const int64_t nc = std::min(swc, ntot - d0);
                     sw3_optics_kernel<<<(unsigned)nc, SW2_THREADS, smem1, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd,
                                                                              h->d_err, (int)d0, h->d_swimg);
                     sw3_sweep_kernel<<<(unsigned)(SW2_CTAS_PER_SM * h->nsm), SW2_THREADS, smem, st>>>(
-                        bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, h->d_err, (int)d0, (int)nc, h->d_swimg, h->d_swrt);
+                        bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, h->d_err, (int)d0, (int)nc, h->d_swimg, h->d_swrt,
+                        h->d_swq + d0 / swc);
                     h->launches += 2;
                 }
                 h->launches -= 1;      // the one launch counted below
@@ -1099,7 +1111,7 @@ void rad_destroy(RadHandle* h)
     for (void* p : {(void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
                     (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
                     (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub, (void*)h->d_lwm,
-                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt, (void*)h->d_swimg, (void*)h->d_aerf,
+                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt, (void*)h->d_swimg, (void*)h->d_swq, (void*)h->d_aerf,
                     (void*)h->d_aeri})
         if (p) cudaFree(p);
     delete h;

@@ -958,16 +958,22 @@ sw3_optics_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
     sw2_column<false, SW2_OPTICS>(bt, any_aer, ex, exd, err, d, nullptr,
                                   img + (size_t)blockIdx.x * (sw2_image_bytes(any_aer) / 16));
 }
+// Columns go to CTAs as they free up (q: the chunk's counter, zero at launch): cloudy columns take about
+// twice as long as clear ones, so a fixed stride would leave the kernel waiting on the unluckiest CTA.
 __global__ void __launch_bounds__(SW2_THREADS, SW2_CTAS_PER_SM)
 sw3_sweep_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, const double* exd, int* err,
-                 int d0, int nc, const int4* img, float* rts)
+                 int d0, int nc, const int4* img, float* rts, int* q)
 {
+    __shared__ int next;
     const int nday = *bt.req[0].nday;
     float* rt = rts + (int64_t)blockIdx.x * sw2_rt_floats();
-    for (int i = blockIdx.x; i < nc && d0 + i < nday; i += gridDim.x) {
+    for (int i = blockIdx.x; i < nc && d0 + i < nday;) {
         sw2_column<true, SW2_SWEEP>(bt, any_aer, ex, exd, err, d0 + i, rt,
                                     const_cast<int4*>(img) + (size_t)i * (sw2_image_bytes(any_aer) / 16));
         __syncthreads();                       // shared memory is reused by the next column
+        if (threadIdx.x == 0) next = (int)gridDim.x + atomicAdd(q, 1);
+        __syncthreads();
+        i = next;
     }
 }
 
