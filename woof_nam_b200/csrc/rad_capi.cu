@@ -535,7 +535,7 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                 // per chunk of day indices (the day count stays on the device: chunks past it exit at once):
                 // set-up and optics one CTA per column into the images, then the sweeps walk the chunk
                 const int64_t swc = sw3_chunk(cfg);
-                const size_t smem1 = sw2_image_begin() + sw2_image_bytes(any_aer);
+                const size_t smem1 = sw3_optics_smem(any_aer);
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw3_optics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw3_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 RAD_CUDA(h, cudaMemsetAsync(h->d_swq, 0, (size_t)((ntot + swc - 1) / swc) * sizeof(int), st));

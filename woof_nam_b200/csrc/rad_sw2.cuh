@@ -361,7 +361,6 @@ struct SwSh2 {
     alignas(16) float colmol[NLAY_MAX];
     float cldfrc[NLAY_MAX];
     float taucw[14][SW2_KS], ssacw[14][SW2_KS], asycw[14][SW2_KS], tabsc[14][SW2_KS];
-    float taug[SW_NGPT][SW2_KS];
     float raylc[SW_NGPT];                      // Rayleigh optical depth per unit colmol (band 24: upper atmosphere)
     float taur24[8][SW2_KS];                   // band 24 Rayleigh optical depth below laytrop
     float sfluxzen[SW_NGPT];
@@ -369,6 +368,8 @@ struct SwSh2 {
     float cosz, sntz, ssolar, albbm[2], albdf[2], zcf0, zcf1;
     int laytrop, kmin8, kminw;
     uint32_t mcw[4][NLAY_MAX];                 // McICA route: the column's sub-column cloud words
+    // last, so that the optics kernel can leave it out of shared memory (it writes it to the image directly)
+    alignas(16) float taug[SW_NGPT][SW2_KS];
 };
 // Dynamic tail: the aerosol block (present only with aerosol inputs) and the segment checkpoints.
 struct SwAer {
@@ -608,6 +609,13 @@ __host__ __device__ constexpr size_t sw2_image_bytes(bool aer)
     return ((sizeof(SwSh2) - sw2_image_begin() + (aer ? sizeof(SwAer) : 0)) + 15) / 16 * 16;
 }
 static_assert(offsetof(SwSh2, colmol) % 16 == 0, "the image starts on a 16-byte boundary");
+static_assert(offsetof(SwSh2, taug) + sizeof(SwSh2::taug) == sizeof(SwSh2) && sizeof(SwAer) % 16 == 0,
+              "taug closes SwSh2 and the aerosol block is whole 16-byte units");
+// Shared memory of the optics kernel: SwSh2 up to taug, then the aerosol block.
+__host__ __device__ constexpr size_t sw3_optics_smem(bool aer)
+{
+    return offsetof(SwSh2, taug) + (aer ? sizeof(SwAer) : 0);
+}
 
 // One sunlit column (day index d) by the CTA; STORE: rt = the CTA's R/T store, else the R/T is recomputed.
 // PART: SW2_ALL, or SW2_OPTICS (phases A and B, the shared memory then copied to img) / SW2_SWEEP (shared
@@ -621,8 +629,14 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
     const int64_t gcol = bt.req[0].daycol[d];
     const int rq = bt.find(gcol);
     const SwIn& a = bt.req[rq];
-    // the aerosol block is reserved when any request of the launch has aerosol; used when this one does
-    SwAer* aer = a.faersw ? reinterpret_cast<SwAer*>(smem_raw + sizeof(SwSh2)) : nullptr;
+    // the aerosol block is reserved when any request of the launch has aerosol; used when this one does.  The
+    // optics kernel keeps it where taug would be: taug goes straight to the image.
+    SwAer* aer = a.faersw ? reinterpret_cast<SwAer*>(smem_raw + (PART == SW2_OPTICS ? offsetof(SwSh2, taug)
+                                                                                      : sizeof(SwSh2)))
+                          : nullptr;
+    float* img_taug = PART == SW2_OPTICS ? reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(img) +
+                                                                    (offsetof(SwSh2, taug) - sw2_image_begin()))
+                                         : nullptr;
     float* ckpt = reinterpret_cast<float*>(smem_raw + sizeof(SwSh2) + (any_aer ? sizeof(SwAer) : 0));
     const int nlay = a.nlay, nlp1 = nlay + 1;
     if (nlay > NLAY_MAX) {
@@ -708,14 +722,20 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
     for_each_band_pair(c_sw_ns, 14, nlay, &s.task_next, tid & 31, [&](int g, int k0, int b) {
         float tg, tr;
         sw_gas<float>(s, g, k0, tg, tr, b);
-        s.taug[g][k0] = tg;
+        if (PART == SW2_OPTICS)
+            img_taug[g * SW2_KS + k0] = tg;
+        else
+            s.taug[g][k0] = tg;
         if (g >= 66 && g < 74 && k0 < s.laytrop) s.taur24[g - 66][k0] = tr;
     });
     __syncthreads();
     }
-    if (PART == SW2_OPTICS) {
+    if (PART == SW2_OPTICS) {   // the image up to taug, then the aerosol block after taug's place
         const int4* sm = reinterpret_cast<const int4*>(smem_raw + sw2_image_begin());
-        for (int i = tid; i < (int)(sw2_image_bytes(any_aer) / 16); i += SW2_THREADS) img[i] = sm[i];
+        const int n1 = (int)((offsetof(SwSh2, taug) - sw2_image_begin()) / 16);
+        const int n2 = any_aer ? (int)(sizeof(SwAer) / 16) : 0;
+        const int skip = (int)(sizeof(SwSh2::taug) / 16);
+        for (int i = tid; i < n1 + n2; i += SW2_THREADS) img[i < n1 ? i : i + skip] = sm[i];
         return;
     }
     // ---- phase C: spcvrtc, one g-point per lane, both passes
@@ -945,11 +965,12 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
 }
 
 // The SW solve split in two kernels per chunk of day indices [d0, d0 + nc): sw3_optics_kernel, one CTA per
-// column, runs phases A and B (set-up, cloud and gas optics: no sweep registers, so three CTAs per SM) and
-// writes the shared-memory image; sw3_sweep_kernel, SW2_CTAS_PER_SM CTAs per SM walking the chunk, loads
-// each image and runs phase C with its R/T store.  Same arithmetic as sw2_column_kernel<true>, same bits.
+// column, runs phases A and B (set-up, cloud and gas optics: no sweep registers and no taug in shared
+// memory, so five CTAs per SM) and writes the image; sw3_sweep_kernel, SW2_CTAS_PER_SM CTAs per SM walking
+// the chunk, loads each image and runs phase C with its R/T store.  Same arithmetic as
+// sw2_column_kernel<true>, same bits.
 constexpr int SW3_CHUNK = 32768;                               // day columns per optics / sweep pair
-__global__ void __launch_bounds__(SW2_THREADS, 3)
+__global__ void __launch_bounds__(SW2_THREADS, 5)
 sw3_optics_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, const double* exd, int* err,
                   int d0, int4* img)
 {
