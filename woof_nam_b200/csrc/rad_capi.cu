@@ -525,6 +525,7 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                              cfg.iovrsw};
         }
         if ((mrc = mark_if(2))) return mrc;
+        int64_t nlaunch = 1;
         if (sizeof(R) == 4) {
             const size_t smem = sw2_smem_bytes(any_aer);
             if (fixed) {   // no scratch: one CTA per sunlit column, R/T recomputed on the way down
@@ -533,7 +534,8 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                                                                                      h->d_err, nullptr);
             } else if (sw3_chunk(cfg) > 0) {
                 // per chunk of day indices (the day count stays on the device: chunks past it exit at once):
-                // set-up and optics one CTA per column into the images, then the sweeps walk the chunk
+                // set-up and optics one CTA per column into the images, then the sweeps take the chunk's
+                // columns from its counter
                 const int64_t swc = sw3_chunk(cfg);
                 const size_t smem1 = sw3_optics_smem(any_aer);
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw3_optics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
@@ -546,9 +548,8 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                     sw3_sweep_kernel<<<(unsigned)(SW2_CTAS_PER_SM * h->nsm), SW2_THREADS, smem, st>>>(
                         bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, h->d_err, (int)d0, (int)nc, h->d_swimg, h->d_swrt,
                         h->d_swq + d0 / swc);
-                    h->launches += 2;
                 }
-                h->launches -= 1;      // the one launch counted below
+                nlaunch = 2 * ((ntot + swc - 1) / swc);
             } else {       // SW2_CTAS_PER_SM CTAs per SM walk the day list, each with its R/T store
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 sw2_column_kernel<true><<<(unsigned)(SW2_CTAS_PER_SM * h->nsm), SW2_THREADS, smem, st>>>(
@@ -561,7 +562,7 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
             RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_sw<R>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             sw_column_kernel<R><<<(unsigned)ntot, SW_THREADS, smem, st>>>(bt, lut, h->d_swd, h->d_err);
         }
-        h->launches += 1;
+        h->launches += nlaunch;
         RAD_CUDA(h, cudaGetLastError());
     }
     return mark_if(3);
