@@ -153,12 +153,14 @@ void rad_graph_destroy(RadGraph* g);
  * budget, may not want the library to allocate in the middle of a time step at all.  This entry runs the
  * same kernels with that scratch in a fixed device array of the library (about 2 MB), so it takes at most
  * RAD_NOALLOC_MAX_COLS columns (larger requests fail with RAD_E_INVALID) and, on the McICA route, needs the
- * caller's lw_mask and sw_mask buffers.  The first call on a device resolves the array's address (a
- * runtime query, no allocation); make that first call before any stream capture.  Every call on every
+ * caller's lw_mask and sw_mask buffers.  Every call looks the array's address up on the current device (a
+ * runtime query, no allocation); the library's first use on a device may load its kernels and the array
+ * there, so make the first call of the library on a device before any stream capture.  Every call on every
  * handle of the process shares the one array: calls whose work may overlap on the device (other streams,
  * other host threads) race on it, so issue them on one stream or one after another.  Profiling events are
- * not recorded by this entry.  The LW runs in its single-kernel form (no scratch), so results equal
- * rad_solve's on a handle configured with lw_chunk < 0. */
+ * not recorded by this entry.  The LW runs in its single-kernel form (no scratch; columns with a cloudy layer
+ * thinner than 1 hPa are solved again in float64 from a list kept in the array), so results equal rad_solve's
+ * on a handle configured with lw_chunk < 0. */
 #define RAD_NOALLOC_MAX_COLS 65536
 int rad_solve_noalloc(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream);
 

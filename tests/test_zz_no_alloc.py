@@ -61,6 +61,35 @@ def test_noalloc_mcica_with_caller_masks():
     assert rc == _lib.RAD_E_INVALID and b"lw_mask" in s.lib.rad_last_error(s.handle)
 
 
+def test_noalloc_fresh_handle_allocates_nothing():
+    """A handle that has never solved: rad_solve_noalloc leaves the device's free memory unchanged (no
+    scratch is created for it), twice in a row, and its outputs agree with rad_solve's within the mixed
+    path's tolerance (0.05 W/m^2, 0.01 K/day: rad_solve runs the two-kernel LW here, the entry the single-
+    kernel LW)."""
+    import torch
+    from conftest import assert_within
+    from woof_nam_b200.solver import RadSolver
+    warm = RadSolver(precision="mixed")                 # the library's first use on the device happens here
+    c = make_columns(512, 45)
+    rc, _ = _call(warm, warm.to_device(c), c.solcon, None, torch.cuda.current_stream())
+    assert rc == 0, warm.lib.rad_last_error(warm.handle)
+    s = RadSolver(precision="mixed")
+    st = torch.cuda.current_stream()
+    for n, seed in ((4000, 46), (2500, 47)):
+        c = make_columns(n, seed)
+        d = s.to_device(c)
+        out = s.alloc_outputs(n)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        rc, got = _call(s, d, c.solcon, out, st)
+        assert rc == 0, s.lib.rad_last_error(s.handle)
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0, "rad_solve_noalloc changed the device's free memory"
+        got = {k: v.cpu().numpy() for k, v in got.items()}
+        ref = s.solve_host(c)
+        assert_within(got, ref, what="rad_solve_noalloc vs rad_solve")
+
+
 def test_noalloc_refuses_above_max():
     import torch
     from woof_nam_b200.solver import RadSolver

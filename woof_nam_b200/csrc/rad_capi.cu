@@ -475,13 +475,24 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
         } else {
         const size_t smem = sizeof(LwShared<R>);
         RAD_CUDA(h, cudaFuncSetAttribute(kernel_ptr_lw<R>(mc), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        if (sizeof(R) == 4 && mc)
-            lw2_column_kernel<R, true><<<(unsigned)ntot, LW_THREADS, smem, st>>>(bt, lut, h->d_err);
-        else if (sizeof(R) == 4)
-            lw2_column_kernel<R, false><<<(unsigned)ntot, LW_THREADS, smem, st>>>(bt, lut, h->d_err);
-        else
+        if (sizeof(R) == 4 && mc) {
+            lw2_column_kernel<R, true><<<(unsigned)ntot, LW_THREADS, smem, st>>>(bt, lut, h->d_err, nullptr);
+            h->launches += 1;
+        } else if (sizeof(R) == 4) {
+            // NAM route: columns with a cloudy layer under 1 hPa go to the float64 column kernel through a list
+            // in the day-list scratch's pos array (ntot + 1 words; the SW part rewrites it afterwards)
+            LwLut<double> dl;
+            dl.ex = h->d_lwd; dl.tfn = h->d_lwd + 10001; dl.tau = h->d_lwd + 2 * 10001;
+            const size_t smemd = sizeof(LwShared<double>);
+            RAD_CUDA(h, cudaFuncSetAttribute((void*)lw3_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemd));
+            RAD_CUDA(h, cudaMemsetAsync(sc.pos, 0, sizeof(int), st));
+            lw2_column_kernel<R, false><<<(unsigned)ntot, LW_THREADS, smem, st>>>(bt, lut, h->d_err, sc.pos);
+            lw3_fp64_kernel<<<(unsigned)h->nsm, LW_THREADS, smemd, st>>>(bt, 0, sc.pos, dl, h->d_err);
+            h->launches += 2;
+        } else {
             lw_column_kernel<R><<<(unsigned)ntot, LW_THREADS, smem, st>>>(bt, lut, h->d_err);
-        h->launches += 1;
+            h->launches += 1;
+        }
         RAD_CUDA(h, cudaGetLastError());
         }
     }
@@ -865,53 +876,43 @@ int rad_solve(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t
 // ---------------------------------------------------------------------------- fixed-scratch solve
 // rad_solve_noalloc: the day-list scratch of a solve lives in this file-scope device array instead of the
 // handle's growing buffers, so the call reaches no allocator.  Layout in 32-bit words, each part 256-byte
-// aligned: flag, pos, daycol, lt, k8, kw ([NA_W] each), cmin ([2 NA_W]), nday ([64]), CUB scan temp.
-// Nothing in it has to start at zero: every word a solve reads is written earlier in the same solve.
+// aligned: flag, pos, daycol, lt, k8, kw ([NA_W] each), cmin ([2 NA_W]), nday ([64]), CUB scan temp.  The LW
+// part uses pos first, as the [count, columns...] list of the columns it leaves to the float64 column kernel.
+// Nothing else in it has to start at zero (the list count is cleared by the solve): every word a solve reads is
+// written earlier in the same solve.
 namespace {
 constexpr int64_t NA_W = ((RAD_NOALLOC_MAX_COLS + 1 + 63) / 64) * 64;
 constexpr int64_t NA_CUB_WORDS = 16384;   // 64 KiB for the device-wide scan
 constexpr int64_t NA_WORDS = 8 * NA_W + 64 + NA_CUB_WORDS;
 __device__ __align__(256) uint32_t g_noalloc_scratch[NA_WORDS];
 
-struct NoallocSlot {
-    bool ready = false;
-    LaunchScratch sc{};
-};
-std::mutex g_na_mu;
-NoallocSlot g_na[64];   // per device ordinal
-
-// Resolve the array's address on the current device (once per device) and check the scan's temp size.
-int noalloc_scratch(RadHandle* h, int dev, LaunchScratch* out)
+// The array's address on the current device and the layout over it.  cudaGetSymbolAddress is a runtime
+// query that allocates nothing; resolving it on every call keeps the address right after a device reset
+// (which gives the array a new address).
+int noalloc_scratch(RadHandle* h, LaunchScratch* out)
 {
-    std::lock_guard<std::mutex> lock(g_na_mu);
-    if (dev < 0 || dev >= 64) return fail(h, RAD_E_INVALID, "rad_solve_noalloc: device ordinal above 63");
-    NoallocSlot& s = g_na[dev];
-    if (!s.ready) {
-        uint32_t* base = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress((void**)&base, g_noalloc_scratch);
-        if (e != cudaSuccess)
-            return fail(h, RAD_E_CUDA, std::string("rad_solve_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        size_t need = 0;
-        RAD_CUDA(h, cub::DeviceScan::ExclusiveSum(nullptr, need, (int*)nullptr, (int*)nullptr, (int)(RAD_NOALLOC_MAX_COLS + 1)));
-        if (need > (size_t)NA_CUB_WORDS * 4)
-            return fail(h, RAD_E_INVALID, "rad_solve_noalloc: the scan needs more temp space than the fixed region holds");
-        int* w = (int*)base;
-        LaunchScratch& c = s.sc;
-        c.flag = w;
-        c.pos = w + NA_W;
-        c.daycol = w + 2 * NA_W;
-        c.lt = w + 3 * NA_W;
-        c.k8 = w + 4 * NA_W;
-        c.kw = w + 5 * NA_W;
-        c.cmin = w + 6 * NA_W;
-        c.nday = w + 8 * NA_W;
-        c.cub = (void*)(w + 8 * NA_W + 64);
-        c.cub_bytes = (size_t)NA_CUB_WORDS * 4;
-        c.max_cols = RAD_NOALLOC_MAX_COLS;
-        c.max_cmin = 2 * NA_W;
-        s.ready = true;
-    }
-    *out = s.sc;
+    uint32_t* base = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&base, g_noalloc_scratch);
+    if (e != cudaSuccess)
+        return fail(h, RAD_E_CUDA, std::string("rad_solve_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    size_t need = 0;
+    RAD_CUDA(h, cub::DeviceScan::ExclusiveSum(nullptr, need, (int*)nullptr, (int*)nullptr, (int)(RAD_NOALLOC_MAX_COLS + 1)));
+    if (need > (size_t)NA_CUB_WORDS * 4)
+        return fail(h, RAD_E_INVALID, "rad_solve_noalloc: the scan needs more temp space than the fixed region holds");
+    int* w = (int*)base;
+    LaunchScratch& c = *out;
+    c.flag = w;
+    c.pos = w + NA_W;
+    c.daycol = w + 2 * NA_W;
+    c.lt = w + 3 * NA_W;
+    c.k8 = w + 4 * NA_W;
+    c.kw = w + 5 * NA_W;
+    c.cmin = w + 6 * NA_W;
+    c.nday = w + 8 * NA_W;
+    c.cub = (void*)(w + 8 * NA_W + 64);
+    c.cub_bytes = (size_t)NA_CUB_WORDS * 4;
+    c.max_cols = RAD_NOALLOC_MAX_COLS;
+    c.max_cmin = 2 * NA_W;
     return RAD_OK;
 }
 }  // namespace
@@ -927,11 +928,12 @@ int rad_solve_noalloc(RadHandle* h, const RadColumns* in, const RadOutputs* out,
     if (h->cfg.route == RAD_ROUTE_MCICA && (!out->lw_mask || !out->sw_mask))
         return fail(h, RAD_E_INVALID, "rad_solve_noalloc: the McICA route needs the caller's lw_mask and sw_mask buffers");
     int dev = 0;
-    cudaGetDevice(&dev);
+    const cudaError_t de = cudaGetDevice(&dev);
+    if (de != cudaSuccess) return fail(h, RAD_E_CUDA, std::string("rad_solve_noalloc: cudaGetDevice: ") + cudaGetErrorString(de));
     if (dev != h->device) return fail(h, RAD_E_INVALID, "rad_solve_noalloc: handle belongs to another device");
     if (ncol == 0) return RAD_OK;
     LaunchScratch sc;
-    if ((rc = noalloc_scratch(h, dev, &sc))) return rc;
+    if ((rc = noalloc_scratch(h, &sc))) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     return h->cfg.precision == RAD_PREC_FP64 ? launch_batch<double>(h, 1, in, out, &ncol, st, &sc)
                                              : launch_batch<float>(h, 1, in, out, &ncol, st, &sc);

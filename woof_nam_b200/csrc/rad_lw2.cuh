@@ -77,8 +77,16 @@ __device__ __forceinline__ LwTerms<R> lw2_terms(const LwShared<R>& s, const LwLu
 // source - gas source).
 // MC = true: the McICA route (rtrnmc, phys_rrtm_lw_rtrnmc.cu:85-310): a layer is cloudy for g-point g
 // when its sub-column bit is set, with effective clear fraction 1 - (1 - exp(-odcld)) -- rtrn with clfr = 1.
+// A column with a cloudy layer thinner than LW_THIN hPa is solved in float64 (lw3_fp64_kernel): such a layer cools
+// at thousands of K/day, so 1e-5 of it is already above 0.01 K/day, and its float optical depths put some
+// g-points on the neighbouring entry of the 10,001-entry transmittance table.
+constexpr float LW_THIN = 1.0f;
+
+// fp64list (NAM route, float, may be null): [count, columns...] of the launch; a listed column is left to the
+// float64 column kernel, which runs after this launch.
 template <class R, bool MC>
-__global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(const __grid_constant__ LwBatch bt, LwLut<R> lut, int* err)
+__global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(const __grid_constant__ LwBatch bt, LwLut<R> lut, int* err,
+                                                                   int* fp64list)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     LwShared<R>& s = *reinterpret_cast<LwShared<R>*>(smem_raw);
@@ -96,6 +104,17 @@ __global__ void __launch_bounds__(LW_THREADS, 2) lw2_column_kernel(const __grid_
         for (int i = tid; i < 5 * nlay; i += LW_THREADS)
             s.mcw[i / nlay][i % nlay] = __ldg(a.mask + ((size_t)(i / nlay) * nlay + (i % nlay)) * N + col);
     lw_setup<R, LW_THREADS>(s, a, col, tid);
+    if (!MC && sizeof(R) == 4 && fp64list) {
+        __shared__ int thin;
+        if (tid == 0) {
+            int f = 0;
+            for (int k0 = 0; k0 < nlay; ++k0) f |= s.delp[k0] < (R)LW_THIN && s.cldfrc[k0 + 1] > (R)1.0e-6f;
+            thin = f;
+            if (f) fp64list[1 + atomicAdd(fp64list, 1)] = (int)blockIdx.x;
+        }
+        __syncthreads();
+        if (thin) return;
+    }
     const R eps = (R)1.0e-6f;
     const int warp = tid >> 5, lane = tid & 31;
     const bool act = lane < LW2_LANES;

@@ -52,7 +52,7 @@ constexpr int H_SECDIFF = 16;   // [16]
 constexpr int H_SEMISS = 32;    // [16]
 constexpr int H_FP64 = 48;      // int: 1 when the column is to be solved in float64 (lw3_fp64_kernel)
 
-constexpr float LW3_THIN = 1.0f;   // hPa: a cloudy layer thinner than this sends the column to float64
+constexpr float LW3_THIN = LW_THIN;   // hPa: a cloudy layer thinner than this sends the column to float64
 
 __host__ __device__ constexpr int64_t lw3_rec_floats(int nlay) { return ((((int64_t)nlay + 1) * LW3_REC + 31) / 32) * 32; }
 __host__ __device__ constexpr int64_t lw3_block_floats(int nlay)

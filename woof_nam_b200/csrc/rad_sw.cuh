@@ -27,6 +27,7 @@ constexpr int SW_WARPS = SW_THREADS / 32;
 
 template <class R>
 struct SwShared {
+    static constexpr bool kRatio64 = false;
     R pavel[NLAY_MAX], tavel[NLAY_MAX], delp[NLAY_MAX], coldry[NLAY_MAX], colmol[NLAY_MAX], h2ovmr[NLAY_MAX];
     R colamt[6][NLAY_MAX];
     R fac00[NLAY_MAX], fac01[NLAY_MAX], fac10[NLAY_MAX], fac11[NLAY_MAX];
@@ -92,6 +93,30 @@ __constant__ int c_sw_nspa[14] = {9, 9, 9, 9, 1, 9, 9, 1, 9, 1, 0, 1, 9, 1};
 __constant__ int c_sw_nspb[14] = {1, 5, 1, 1, 1, 5, 1, 0, 1, 0, 0, 1, 5, 1};
 
 // ------------------------------------------------------------------------------------------------------
+// Key-species parameter of the SW bands that interpolate their k-tables in a species ratio (taumol16..19, 21,
+// 22, 24, 28: slots 0..7): sm = mult * min(om, x1 / sc) with sc = x1 + strrat x2, entry js = 1 + int(sm), fraction
+// fs = sm - int(sm) (guard: ratio 0 when sc <= 0, as bands 18 and 22 write it).  The entries of neighbouring js
+// may differ by an order of magnitude, so fs carries the float division's error into the optical depth almost
+// tenfold; a layout that holds the ratio of each slot and layer in float64 (kRatio64: `spr`, formed from the
+// float64 column amounts) takes it from there and rounds fs once.
+template <class R, class S>
+__device__ __forceinline__ void sw_species(const S& s, int slot, int k0, R x1, R sc, R mult, R om, bool guard, int& js,
+                                           R& fs)
+{
+    if constexpr (S::kRatio64) {
+        const double sm = (double)mult * fmin((double)om, s.spr[slot][k0]);
+        const int j = (int)sm;
+        js = 1 + j;
+        fs = (R)(sm - (double)j);
+    } else {
+        const R ratio = guard ? (sc > 0 ? x1 / sc : (R)0) : x1 / sc;
+        const R sm = mult * fminR(om, ratio);
+        js = 1 + (int)sm;
+        fs = guard ? sm - (R)(int)sm : rfmod1(sm);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------
 // Gas and Rayleigh optical depths of SW g-point g (0..111) at layer k0 (phys_rrtm_sw_taumol16..29.cu with
 // the reference's handling of the layer k = laytrop).
 template <class R, class S>
@@ -133,11 +158,10 @@ __device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr, int band_of_g = 
         auto a = [&](int i) { return ldt(A + (size_t)(i - 1) * ng + ig); };
         return f00 * a(i01) + f10 * a(i02) + f01 * a(i11) + f11 * a(i12);
     };
-    auto jsfs = [&](R x1, R strr, R x2, R mult, R om, R& sc, int& js, R& fs) {
+    // key-species ratio parameter of the band's layer (sw_species); sc = x1 + strr x2 multiplies the sum
+    auto jsfs = [&](int slot, R x1, R strr, R x2, R mult, R om, R& sc, int& js, R& fs, bool guard = false) {
         sc = x1 + strr * x2;
-        const R sm = mult * fminR(om, x1 / sc);
-        js = 1 + (int)sm;
-        fs = rfmod1(sm);
+        sw_species<R>(s, slot, k0, x1, sc, mult, om, guard, js, fs);
     };
     auto SF = [&](int id, int ng) { return sfac * interp(tab<R>(id), ng, inds, ig, sfrac); };
     auto FF = [&](int id, int ng) { return ffac * interp(tab<R>(id), ng, indf, ig, ffrac); };
@@ -150,7 +174,7 @@ __device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr, int band_of_g = 
         tg = 0;
         if (k <= lt) {
             R sc, fs; int js;
-            jsfs(c1, ldt(tab<R>(T_SW16_STRRAT)), c5, (R)8, oneminus, sc, js, fs);
+            jsfs(0, c1, ldt(tab<R>(T_SW16_STRRAT)), c5, (R)8, oneminus, sc, js, fs);
             tg = sc * sum8(tab<R>(T_SW16_ABSA), NG, 585, id0, id1, js, fs, 9, 10) +
                  c1 * (SF(T_SW16_SELFREF, NG) + FF(T_SW16_FORREF, NG));
         }
@@ -163,12 +187,12 @@ __device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr, int band_of_g = 
         tr = cm * (R)6.86e-10f;
         R sc, fs; int js;
         if (k0 < lt) {
-            jsfs(c1, strr, c2, (R)8, oneminus, sc, js, fs);
+            jsfs(1, c1, strr, c2, (R)8, oneminus, sc, js, fs);
             const int i0 = ((jpk - 1) * 5 + (jtk - 1)) * 9, i1 = (jpk * 5 + (jt1k - 1)) * 9;
             const R selfpart = inds > 0 ? SF(T_SW17_SELFREF, NG) : (R)0;
             tg = sc * sum8(tab<R>(T_SW17_ABSA), NG, 585, i0, i1, js, fs, 9, 10) + c1 * (selfpart + FF(T_SW17_FORREF, NG));
         } else {
-            jsfs(c1, strr, c2, (R)4, oneminus, sc, js, fs);
+            jsfs(1, c1, strr, c2, (R)4, oneminus, sc, js, fs);
             const int i0 = ((jpk - 13) * 5 + (jtk - 1)) * 5, i1 = ((jpk - 12) * 5 + (jt1k - 1)) * 5;
             tg = sc * sum8(tab<R>(T_SW17_ABSB), NG, 1175, i0, i1, js, fs, 5, 6) + (c1 * ffac) * interp(tab<R>(T_SW17_FORREF), NG, indf, ig, ffrac);
         }
@@ -179,11 +203,9 @@ __device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr, int band_of_g = 
         tr = cm * ldt(tab<R>(T_SW18_RAYL));
         idx(18, id0, id1);
         if (k <= lt) {
-            const R sc = c1 + (R)ldt(tab<R>(T_SW_STRRAT) + 2) * c5;
-            const R ratio = sc > 0 ? c1 / sc : (R)0;
-            const R sm = (R)8 * fminR(swom, ratio);
-            const int jsi = (int)sm;
-            tg = sc * sum8(tab<R>(T_SW18_ABSA), NG, 585, id0, id1, 1 + jsi, sm - (R)jsi, 9, 10) +
+            R sc, fs; int js;
+            jsfs(2, c1, (R)ldt(tab<R>(T_SW_STRRAT) + 2), c5, (R)8, swom, sc, js, fs, true);
+            tg = sc * sum8(tab<R>(T_SW18_ABSA), NG, 585, id0, id1, js, fs, 9, 10) +
                  c1 * (SF(T_SW18_SELFREF, NG) + FF(T_SW18_FORREF, NG));
         } else {
             tg = c5 * sum4(tab<R>(T_SW18_ABSB), NG, 235, id0, id1);
@@ -196,9 +218,9 @@ __device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr, int band_of_g = 
         idx(19, id0, id1);
         tg = 0;
         if (k <= lt) {
-            const R sc = c1 + (R)5.49281e+0f * c2;
-            const R sm = (R)8 * fminR(swom, c1 / sc);
-            tg = sc * sum8(tab<R>(T_SW19_ABSA), NG, 585, id0, id1, 1 + (int)sm, rfmod1(sm), 9, 10) +
+            R sc, fs; int js;
+            jsfs(3, c1, (R)5.49281e+0f, c2, (R)8, swom, sc, js, fs);
+            tg = sc * sum8(tab<R>(T_SW19_ABSA), NG, 585, id0, id1, js, fs, 9, 10) +
                  c1 * (SF(T_SW19_SELFREF, NG) + FF(T_SW19_FORREF, NG));
         }
         if (k >= lt && k >= s.kmin8 + 1) tg = c2 * sum4(tab<R>(T_SW19_ABSB), NG, 235, id0, id1);
@@ -227,12 +249,12 @@ __device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr, int band_of_g = 
         tg = 0;
         R sc, fs; int js;
         if (k < lt) {
-            jsfs(c1, strr, c2, (R)8, oneminus, sc, js, fs);
+            jsfs(4, c1, strr, c2, (R)8, oneminus, sc, js, fs);
             tg = sc * sum8(tab<R>(T_SW21_ABSA), NG, 585, id0, id1, js, fs, 9, 10) +
                  c1 * (SF(T_SW21_SELFREF, NG) + FF(T_SW21_FORREF, NG));
         }
         if (k >= lt) {
-            jsfs(c1, strr, c2, (R)4, oneminus, sc, js, fs);
+            jsfs(4, c1, strr, c2, (R)4, oneminus, sc, js, fs);
             tg = sc * sum8(tab<R>(T_SW21_ABSB), NG, 1175, id0, id1, js, fs, 5, 6) +
                  c1 * ffac * interp(tab<R>(T_SW21_FORREF), NG, indf, ig, ffrac);
         }
@@ -244,10 +266,9 @@ __device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr, int band_of_g = 
         tr = cm * (R)1.54e-08f;
         const R o2cont = (R)4.35e-4f / ((R)350.0f * (R)2.0f) * c6;
         if (k <= lt) {
-            const R sc = c1 + (R)3.63328e-02f * c6;
-            const R ratio = sc > 0 ? c1 / sc : (R)0;
-            const R sm = (R)8 * fminR(oneminus, ratio);
-            tg = sc * (sum8(tab<R>(T_SW22_ABSA), NG, 585, id0, id1, 1 + (int)sm, rfmod1(sm), 9, 10)) +
+            R sc, fs; int js;
+            jsfs(5, c1, (R)3.63328e-02f, c6, (R)8, oneminus, sc, js, fs, true);
+            tg = sc * (sum8(tab<R>(T_SW22_ABSA), NG, 585, id0, id1, js, fs, 9, 10)) +
                  c1 * (SF(T_SW22_SELFREF, NG) + FF(T_SW22_FORREF, NG)) + o2cont;
         } else {
             tg = c6 * (R)1.6f * (sum4(tab<R>(T_SW22_ABSB), NG, 235, id0, id1)) + o2cont;
@@ -270,11 +291,8 @@ __device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr, int band_of_g = 
         const int NG = 8;
         idx(24, id0, id1);
         if (k <= lt) {
-            const R sc = c1 + (R)1.24692e-1f * c6;
-            const R sm = (R)8 * fminR(swom, c1 / sc);
-            const int jsi = (int)sm;
-            const int js = 1 + jsi;
-            const R fs = sm - (R)jsi;
+            R sc, fs; int js;
+            jsfs(6, c1, (R)1.24692e-1f, c6, (R)8, swom, sc, js, fs);
             tg = sc * sum8(tab<R>(T_SW24_ABSA), NG, 585, id0, id1, js, fs, 9, 10) + c3 * ldt(tab<R>(T_SW24_ABSO3A) + ig) +
                  c1 * (SF(T_SW24_SELFREF, NG) + FF(T_SW24_FORREF, NG));
             const R r0 = ldt(tab<R>(T_SW24_RAYLA) + (size_t)(js - 1) * NG + ig), r1 = ldt(tab<R>(T_SW24_RAYLA) + (size_t)js * NG + ig);
@@ -317,14 +335,14 @@ __device__ void sw_gas(const S& s, int g, int k0, R& tg, R& tr, int band_of_g = 
         const R strr = ldt(tab<R>(T_SW28_STRRAT));
         tg = 0;
         if (k <= lt) {
-            const R sc = c3 + strr * c6;
-            const R sm = (R)8 * fminR(swom, c3 / sc);
-            tg = sc * sum8(tab<R>(T_SW28_ABSA), NG, 585, id0, id1, 1 + (int)sm, rfmod1(sm), 9, 10);
+            R sc, fs; int js;
+            jsfs(7, c3, strr, c6, (R)8, swom, sc, js, fs);
+            tg = sc * sum8(tab<R>(T_SW28_ABSA), NG, 585, id0, id1, js, fs, 9, 10);
         }
         if (k >= s.kminw + 1 && k >= lt) {
-            const R sc = c3 + strr * c6;
-            const R sm = (R)4 * fminR(swom, c3 / sc);
-            tg = sc * sum8(tab<R>(T_SW28_ABSB), NG, 1175, id0, id1, 1 + (int)sm, rfmod1(sm), 5, 6);
+            R sc, fs; int js;
+            jsfs(7, c3, strr, c6, (R)4, swom, sc, js, fs);
+            tg = sc * sum8(tab<R>(T_SW28_ABSB), NG, 1175, id0, id1, js, fs, 5, 6);
         }
         break;
     }

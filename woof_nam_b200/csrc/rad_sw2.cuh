@@ -30,6 +30,11 @@
 //    are recomputed from the column inputs in float64 (prep, setcoef, gas, aerosol and cloud optics) and
 //    the reference's statements are evaluated in float64 (sw2_exact), so the result follows the
 //    reference's own arithmetic.  Both run inline in the lane that needs them.
+//  * The layer coefficients and the key-species ratios are formed in float64 and rounded once, so a float
+//    exponent argument is within ~2e-6 of the float64 one.  Where an argument lies that close to a bound of
+//    the reference's exp table and taking the neighbouring entry would move the layer's heating or the
+//    surface beam by more than the guard allows (sw2_near, sw2_flip_matters), the layer is recomputed in
+//    float64 (sw2_exact): one entry step can move a thin layer's heating by ~0.05 K/day.
 //  * Flux sums over g-points and bands and the heating-rate flux differences are float64.
 #pragma once
 #include "rad_sw.cuh"
@@ -44,6 +49,12 @@ constexpr int SW2_SEG = RAD_SW2_SEG;                              // layers per 
 constexpr int SW2_NSEG = (NLAY_MAX + SW2_SEG - 1) / SW2_SEG;
 constexpr float SW2_RESONANCE = 1.0e-2f;                          // float64 R/T where |1-(k mu0)^2| < this
 constexpr double SW2_TBL_MARGIN = 0.01;                           // table-index rounding margin (see sw2_tbl_sure)
+// Table-entry guard of the float R/T (sw2_near, sw2_flip_matters): relative error bound of a float exponent
+// argument against the float64 one, and the largest output change one entry of the 10,001-entry exp table may
+// make unchecked (the heating weight carries a safety factor of 1.5 on top).
+constexpr float SW2_ZB_EPS = 2.0e-6f;
+constexpr float SW2_HEAT_T = 2.0e-3f;                             // K/day
+constexpr float SW2_FLUX_T = 5.0e-3f;                             // W/m^2
 
 // Rain and snow optical coefficients per SW band (phys_rrtm_sw_cldprop.cu): b0r, c0r, b0s, b1s, c0s.
 __constant__ float c_sw_rain_snow[5][14] = {
@@ -206,6 +217,7 @@ __device__ void sw2_cloud(const SwIn& a, int64_t col, int k0, int ib, R cf, R& t
 
 // Layer coefficients of one layer in float64, read with the shared-memory array syntax by sw_gas.
 struct SwOne {
+    static constexpr bool kRatio64 = false;
     One<double> fac00, fac01, fac10, fac11, selffac, selffrac, forfac, forfrac, colmol;
     One<double> colamt[6];
     One<int> jp, jt, jt1, indself, indfor;
@@ -286,17 +298,16 @@ __device__ __forceinline__ SwPro<T> sw2_prologue(T ztau0, T tabs, T zssa0, T zas
     return p;
 }
 
-// R/T from the prologue (1 - (k mu0)^2 clamped at 1e-8 as the reference does).
+// R/T from the prologue and the two exponentials e1 = exp(-k tau1), e2 = exp(-tau1 / mu0) with their
+// complements (1 - (k mu0)^2 clamped at 1e-8 as the reference does).
 template <class T>
-__device__ __forceinline__ void sw2_rt_tail(const SwPro<T>& p, T cz, T snt, const T* ex, T& rb, T& rd, T& tb, T& td)
+__device__ __forceinline__ void sw2_rt_core(const SwPro<T>& p, T cz, T e1, T em1, T e2, T em2, T& rb, T& rd, T& tb,
+                                            T& td)
 {
     const T eps1 = (T)1.0e-8f;
     const T zrpp = fabs(p.zrpp) < eps1 ? (p.zrpp < 0 ? -eps1 : eps1) : p.zrpp;
     const T g1 = p.g1, g2 = p.g2, g3 = p.g3, g4 = p.g4, zrk = p.zrk, zrp = p.zrp;
     const T za1 = g1 * g4 + g2 * g3, za2 = g1 * g3 + g2 * g4;
-    T em1, em2;
-    const T e1 = sw2_expm_c(fminR(zrk * p.ztau1, (T)500), ex, em1);
-    const T e2 = sw2_expm_c(fminR(p.ztau1 * snt, (T)500), ex, em2);
     const T e11 = e1 * e1, em11 = em1 * ((T)2 - em1);
     const T B = zrk * ((T)1 + e11) + g1 * em11;
     const T D = zrpp * B;                                        // (reference ze1r45) * exp(-k tau)
@@ -312,6 +323,16 @@ __device__ __forceinline__ void sw2_rt_tail(const SwPro<T>& p, T cz, T snt, cons
     }
     rd = fmaxR((T)0, fminR((T)1, g2 * em11 / B));
     td = fmaxR((T)0, fminR((T)1, (T)2 * zrk * e1 / B));
+}
+
+// R/T from the prologue, the exponentials from the reference's table (sw_expm's nearest-entry rule).
+template <class T>
+__device__ __forceinline__ void sw2_rt_tail(const SwPro<T>& p, T cz, T snt, const T* ex, T& rb, T& rd, T& tb, T& td)
+{
+    T em1, em2;
+    const T e1 = sw2_expm_c(fminR(p.zrk * p.ztau1, (T)500), ex, em1);
+    const T e2 = sw2_expm_c(fminR(p.ztau1 * snt, (T)500), ex, em2);
+    sw2_rt_core<T>(p, cz, e1, em1, e2, em2, rb, rd, tb, td);
 }
 
 // ------------------------------------------------------------------------------------------------------
@@ -347,9 +368,11 @@ __device__ __forceinline__ float sw2_rayl_coef(int g)
 // banks.
 constexpr int SW2_KS = NLAY_MAX + 1;
 struct SwSh2 {
+    static constexpr bool kRatio64 = true;     // sw_species reads the key-species ratios from spr
     // read by the set-up and optics phases only, and the sweep phase's reduction scratch
     double fn[SW2_WARPS][NLAY_MAX + 2];        // per-warp level sums of zsolar * (down - up), passes combined
     double sc[SW2_WARPS][18];                  // per-warp scalar sums, clear (0..8) and cloudy (9..17)
+    double spr[8][NLAY_MAX];                   // key-species ratio of each species-interpolating band (sw_species)
     float fac00[NLAY_MAX], fac01[NLAY_MAX], fac10[NLAY_MAX], fac11[NLAY_MAX];
     float selffac[NLAY_MAX], selffrac[NLAY_MAX], forfac[NLAY_MAX], forfrac[NLAY_MAX];
     float colamt[6][NLAY_MAX];
@@ -381,13 +404,16 @@ __host__ __device__ constexpr size_t sw2_smem_bytes(bool aer)
     return sizeof(SwSh2) + (aer ? sizeof(SwAer) : 0) + sw2_ckpt_bytes();
 }
 
-// Everything the float64 recompute of a layer needs besides the layer index and g-point.
+// Everything the float64 recompute of a layer needs besides the layer index and g-point, and the weights of
+// the table-entry guard: wh = 1.5 zsolar 86400 / SW2_HEAT_T (times heatfac / delp of the layer: the heating
+// change per unit change of the layer's R/T, relative to its limit), wf = zsolar / SW2_FLUX_T.
 struct SwExactCtx {
     const SwIn* a;
     int64_t col;
     int laytrop, kmin8, kminw, mode;
     double cz, snt;
     const double* exd;
+    float wh, wf;
 };
 
 // The layer's clear (cloud = false) or cloud-mixture optical properties recomputed from the column
@@ -449,6 +475,65 @@ __device__ __forceinline__ bool sw2_tbl_sure(double zb)
     return f > SW2_TBL_MARGIN && f < 1.0 - SW2_TBL_MARGIN;
 }
 
+// Table-entry guard.  exp(-zb) comes from the reference's 10,001-entry table, entry int(10^4 zb / (bpade + zb)
+// + 1/2).  A float argument that lies within its rounding (SW2_ZB_EPS relative, and the float evaluation of the
+// entry position) of an entry bound may take the neighbouring entry where the float64 optics take the other.
+// One entry step is ~3e-4 of the exponential; near the two-stream resonance the layer R/T amplify it by
+// ~1 / |1 - (k mu0)^2|, and on a thin layer under a strong g-point one step moves the layer's heating rate by
+// up to ~0.05 K/day: the reference's own outputs change that much when its optical depths change by 1e-7.
+// sw2_near: the argument is that close to a bound (or to the 0.06 switch to the series).
+__device__ __forceinline__ bool sw2_near(float zb)
+{
+    if (zb <= 0.06f * (1.0f + SW2_ZB_EPS)) return zb > 0.06f * (1.0f - SW2_ZB_EPS);
+    const float ft = zb / ((float)1.0f / (float)0.278f + zb);
+    const float pos = ft * (float)10000 + (float)0.5f;            // sw_expm's entry position
+    const float fr = pos - floorf(pos);
+    const float m = 10000.0f * ft * (SW2_ZB_EPS * (1.0f - ft) + 3.0e-7f);
+    return fr < m || fr > 1.0f - m;
+}
+// exp(-zb) and its complement as the neighbouring entry across the nearer bound gives them (the series on the
+// other side of 0.06).
+__device__ __forceinline__ float sw2_expm_alt(float zb, const float* ex, float& em)
+{
+    const float ft = zb / ((float)1.0f / (float)0.278f + zb);
+    const float pos = ft * (float)10000 + (float)0.5f;
+    const int it = min(10000, (int)pos);
+    if (zb <= 0.06f) {                                            // the table entry instead of the series
+        em = 1.0f - __ldg(ex + it);
+        return __ldg(ex + it);
+    }
+    if (zb <= 0.06f * (1.0f + SW2_ZB_EPS)) {                      // the series instead of the table entry
+        em = zb - 0.5f * zb * zb;
+        return 1.0f - zb + 0.5f * zb * zb;
+    }
+    const int nb = pos - (float)it < 0.5f ? max(it - 1, 0) : min(it + 1, 10000);
+    em = 1.0f - __ldg(ex + nb);
+    return __ldg(ex + nb);
+}
+// True when taking the other entry for e1 (n1) or e2 (n2) changes the layer's R/T and direct transmission
+// (e3 shares e2's entry) by more than 1 / w.  Rare (arguments near a bound); the R/T are evaluated again.
+__device__ __noinline__ bool sw2_flip_matters(const SwPro<float>& p, float cz, float snt, const float* ex, bool n1,
+                                              bool n2, float w, float rb, float rd, float tb, float td)
+{
+    float em1, em2;
+    const float zb1 = fminf(p.zrk * p.ztau1, 500.0f), zb2 = fminf(p.ztau1 * snt, 500.0f);
+    const float e1 = sw2_expm_c(zb1, ex, em1), e2 = sw2_expm_c(zb2, ex, em2);
+    float d = 0.0f;
+    if (n1) {
+        float a1m, rb1, rd1, tb1, td1;
+        const float a1 = sw2_expm_alt(zb1, ex, a1m);
+        sw2_rt_core<float>(p, cz, a1, a1m, e2, em2, rb1, rd1, tb1, td1);
+        d = fabsf(rb1 - rb) + fabsf(rd1 - rd) + fabsf(tb1 - tb) + fabsf(td1 - td);
+    }
+    if (n2) {
+        float a2m, rb2, rd2, tb2, td2;
+        const float a2 = sw2_expm_alt(zb2, ex, a2m);
+        sw2_rt_core<float>(p, cz, e1, em1, a2, a2m, rb2, rd2, tb2, td2);
+        d = fmaxf(d, fabsf(rb2 - rb) + fabsf(rd2 - rd) + fabsf(tb2 - tb) + fabsf(td2 - td) + fabsf(a2 - e2));
+    }
+    return d * w > 1.0f;
+}
+
 // R/T of a layer near the two-stream resonance in float64 from its float optical properties.  Returns false
 // when the result depends on more than those: a table entry of e1 = exp(-k tau1) or e2 = exp(-tau1 / mu0)
 // that the float rounding could move (the resonance amplifies the neighbouring entry's 1e-4 to ~1e-2), or
@@ -467,24 +552,37 @@ __device__ __noinline__ bool sw2_rt_double(float t0, float tabs, float s0, float
 // One optical-property set of a layer -> R/T and direct transmissions: float; near the resonance
 // (|1 - (k mu0)^2| < SW2_RESONANCE, where the float R/T loses ~1e-7 / |1 - (k mu0)^2| of relative accuracy)
 // float64 from the float optics; where even that is not decided by the float optics, the float64 recompute
-// of the layer from the column inputs (sw2_exact).
+// of the layer from the column inputs (sw2_exact).  The float64 recompute also replaces the float R/T where an
+// exponential's argument lies within its rounding of a table-entry bound and the other entry matters: wk
+// weighs the change of the R/T and of the direct transmission (the layer's heating, x.wh times its heatfac /
+// delp), x.wf the step of exp(-tau0 / mu0) (the surface direct beam alone).
 __device__ __forceinline__ void sw2_rt_mixed(float t0, float tabs, float s0, float y0, float cz, float snt,
                                              const float* ex, const SwExactCtx& x, int k0, int g, int ib, bool cloud,
-                                             float& rb, float& rd, float& tb, float& td, float& e3, float& e4)
+                                             float wk, float& rb, float& rd, float& tb, float& td, float& e3,
+                                             float& e4)
 {
     const SwPro<float> p = sw2_prologue<float>(t0, tabs, s0, y0, x.mode, cz);
+    bool exact = false;
     if (fabsf(p.zrpp) < SW2_RESONANCE) {
-        if (!sw2_rt_double(t0, tabs, s0, y0, x, rb, rd, tb, td)) {
-            double a, b, c, d, f3, f4;
-            sw2_exact(x, k0, g, ib, cloud, a, b, c, d, f3, f4);
-            rb = (float)a; rd = (float)b; tb = (float)c; td = (float)d; e3 = (float)f3; e4 = (float)f4;
-            return;
-        }
+        exact = !sw2_rt_double(t0, tabs, s0, y0, x, rb, rd, tb, td);
     } else {
         sw2_rt_tail<float>(p, cz, snt, ex, rb, rd, tb, td);
+        const bool n1 = sw2_near(fminf(p.zrk * p.ztau1, 500.0f)), n2 = sw2_near(fminf(p.ztau1 * snt, 500.0f));
+        if ((n1 || n2) && wk > 0.0f) exact = sw2_flip_matters(p, cz, snt, ex, n1, n2, wk, rb, rd, tb, td);
+    }
+    const float zb4 = t0 * snt;
+    if (!exact && x.wf * 4.0e-4f > 1.0f && sw2_near(zb4)) {
+        float am;
+        exact = fabsf(sw2_expm_alt(zb4, ex, am) - sw_expm(zb4, ex, true)) * x.wf > 1.0f;
+    }
+    if (exact) {
+        double a, b, c, d, f3, f4;
+        sw2_exact(x, k0, g, ib, cloud, a, b, c, d, f3, f4);
+        rb = (float)a; rd = (float)b; tb = (float)c; td = (float)d; e3 = (float)f3; e4 = (float)f4;
+        return;
     }
     e3 = sw_expm(p.ztau1 * snt, ex, true);
-    e4 = sw_expm(t0 * snt, ex, true);
+    e4 = sw_expm(zb4, ex, true);
 }
 
 struct SwLayerRT {
@@ -523,7 +621,8 @@ __device__ __noinline__ SwLayerRT2 sw2_layer(const SwSh2& s, const SwAer* aer, c
     float ta = 0, tasa = 0, tay = 0, taab = 0;
     if (aer) { ta = aer->tau[ib][k0]; tasa = aer->tasa[ib][k0]; tay = aer->tay[ib][k0]; taab = aer->tabs[ib][k0]; }
     const float ct0 = fmaxf(1.0e-12f, tr + tg + ta), cs0 = tr + tasa, cy0 = tay, cab = tg + taab;
-    sw2_rt_mixed(ct0, cab, cs0, cy0, cz, snt, ex, x, k0, g, ib, false, c.rb, c.rd, c.tb, c.td, c.e3, c.e4);
+    const float wk = x.wh * (float)s.rdelp[k0];
+    sw2_rt_mixed(ct0, cab, cs0, cy0, cz, snt, ex, x, k0, g, ib, false, wk, c.rb, c.rd, c.tb, c.td, c.e3, c.e4);
     o = c;
     if (cloudy && sw2_cloud_layer(s, mc, g, k0)) {
         {
@@ -531,7 +630,7 @@ __device__ __noinline__ SwLayerRT2 sw2_layer(const SwSh2& s, const SwAer* aer, c
             const float ot0 = ct0 + s.taucw[ib][k0], os0 = cs0 + s.ssacw[ib][k0], oy0 = cy0 + s.asycw[ib][k0];
             const float oab = cab + s.tabsc[ib][k0];
             float rb2, rd2, tb2, td2, e32, e42;
-            sw2_rt_mixed(ot0, oab, os0, oy0, cz, snt, ex, x, k0, g, ib, true, rb2, rd2, tb2, td2, e32, e42);
+            sw2_rt_mixed(ot0, oab, os0, oy0, cz, snt, ex, x, k0, g, ib, true, wk, rb2, rd2, tb2, td2, e32, e42);
             if (mc) {
                 o.rb = rb2; o.rd = rd2; o.tb = tb2; o.td = td2; o.e3 = e32; o.e4 = e42;
                 return r;
@@ -655,14 +754,33 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
         asm volatile("cp.async.wait_all;" ::: "memory");
         __syncthreads();
     } else {
-    // ---- phase A1: layer coefficients (threads = layers), aerosol, heating factors
+    // ---- phase A1: layer coefficients (threads = layers), aerosol, heating factors.  The coefficients are
+    // formed in float64 and rounded once: the interpolation weights take a difference of logarithms, which
+    // float would carry with ~1e-6 of the gas optical depths' error (and move their exp-table entries).
     for (int k0 = tid; k0 < nlay; k0 += SW2_THREADS) {
-        SwCoef<float> c;
-        sw2_layer_coef<float>(a, col, k0, c);
-        s.fac00[k0] = c.fac00; s.fac01[k0] = c.fac01; s.fac10[k0] = c.fac10; s.fac11[k0] = c.fac11;
-        s.selffac[k0] = c.selffac; s.selffrac[k0] = c.selffrac; s.forfac[k0] = c.forfac; s.forfrac[k0] = c.forfrac;
-        s.colmol[k0] = c.colmol;
-        for (int m = 0; m < 6; ++m) s.colamt[m][k0] = c.colamt[m];
+        SwCoef<double> c;
+        sw2_layer_coef<double>(a, col, k0, c);
+        s.fac00[k0] = (float)c.fac00; s.fac01[k0] = (float)c.fac01; s.fac10[k0] = (float)c.fac10;
+        s.fac11[k0] = (float)c.fac11;
+        s.selffac[k0] = (float)c.selffac; s.selffrac[k0] = (float)c.selffrac; s.forfac[k0] = (float)c.forfac;
+        s.forfrac[k0] = (float)c.forfrac;
+        s.colmol[k0] = (float)c.colmol;
+        for (int m = 0; m < 6; ++m) s.colamt[m][k0] = (float)c.colamt[m];
+        {   // key-species ratios x1 / (x1 + strrat x2) of bands 16-19, 21, 22, 24, 28 (sw_species slots 0..7)
+            const double h = c.colamt[0], c2 = c.colamt[1], o3 = c.colamt[2], ch4 = c.colamt[4], o2 = c.colamt[5];
+            auto ratio = [](double x1, double strr, double x2, bool guard) {
+                const double sc = x1 + strr * x2;
+                return guard ? (sc > 0 ? x1 / sc : 0.0) : x1 / sc;
+            };
+            s.spr[0][k0] = ratio(h, (double)ldt(tab<float>(T_SW16_STRRAT)), ch4, false);
+            s.spr[1][k0] = ratio(h, (double)ldt(tab<float>(T_SW_STRRAT) + 1), c2, false);
+            s.spr[2][k0] = ratio(h, (double)ldt(tab<float>(T_SW_STRRAT) + 2), ch4, true);
+            s.spr[3][k0] = ratio(h, (double)5.49281e+0f, c2, false);
+            s.spr[4][k0] = ratio(h, (double)4.53210e-03f, c2, false);
+            s.spr[5][k0] = ratio(h, (double)3.63328e-02f, o2, true);
+            s.spr[6][k0] = ratio(h, (double)1.24692e-1f, o2, false);
+            s.spr[7][k0] = ratio(o3, (double)ldt(tab<float>(T_SW28_STRRAT)), o2, false);
+        }
         s.jp[k0] = c.jp; s.jt[k0] = c.jt; s.jt1[k0] = c.jt1; s.indself[k0] = c.indself; s.indfor[k0] = c.indfor;
         s.low[k0] = c.low ? 1 : 0;
         const int kk0 = nlay - 1 - k0;
@@ -752,7 +870,8 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
     const float ab = ibd ? s.albbm[ibd - 1] : 0.5f * (s.albbm[0] + s.albbm[1]);
     const float ad = ibd ? s.albdf[ibd - 1] : 0.5f * (s.albdf[0] + s.albdf[1]);
     SwExactCtx x{&a, col, s.laytrop, s.kmin8, s.kminw, a.iswmode, (double)__ldg(a.coszen + col),
-                 1.0 / (double)__ldg(a.coszen + col), exd};
+                 1.0 / (double)__ldg(a.coszen + col), exd, zsolar * (1.5f * 86400.0f / SW2_HEAT_T),
+                 zsolar * (1.0f / SW2_FLUX_T)};
     const int nseg = (nlay + SW2_SEG - 1) / SW2_SEG;
     float* ck = ckpt + tid;
     auto CK = [&](int sg, int q) -> float& { return ck[((sg - 1) * 4 + q) * SW2_THREADS]; };
