@@ -350,9 +350,9 @@ def main():
     lw_tf = ops["lw_flops_per_col"] * n / (lw_ms * 1e-3) / 1e12
     sw_tf = ops["sw_flops_per_daycol"] * nday / (sw_ms * 1e-3) / 1e12
     # the mixed precision runs the two-kernel LW (gas optics, then sweeps, per chunk) and the two-kernel SW
-    # (set-up and optics into shared-memory images, then sweeps, per chunk of day columns)
+    # (set-up, optics and layer R/T into the chunk scratch, then the adding sweeps, per chunk of day columns)
     lw_name = "lw3_optics_kernel+lw3_sweep_kernel"
-    sw_name = "sw2_column_kernel" if mcfg.sw_sweep_chunk < 0 else "sw3_optics_kernel+sw3_sweep_kernel"
+    sw_name = "sw2_column_kernel" if mcfg.sw_sweep_chunk < 0 else "sw4_optics_kernel+sw4_sweep_kernel"
     dom = sw_name if sw_ms >= lw_ms else lw_name
     achieved = sw_tf if dom == sw_name else lw_tf
     traffic = None

@@ -68,9 +68,10 @@ typedef struct {
     int32_t lw_chunk;        /* mixed precision: columns per LW chunk of the two-kernel LW (gas optics through
                                 ~95 KB per column of scratch, then the sweeps); 0 = 32768; negative = the
                                 single-kernel LW (gas optics in shared memory, no scratch) */
-    int32_t sw_sweep_chunk;  /* mixed precision: day columns per chunk of the two-kernel SW (set-up, cloud and
-                                gas optics through ~64 KB per column of scratch, then the sweeps); 0 = 65536;
-                                negative = the single-kernel SW (no scratch besides the R/T stores) */
+    int32_t sw_sweep_chunk;  /* mixed precision: day columns per chunk of the two-kernel SW (set-up, optics and
+                                the layer reflectances / transmittances through ~330 KB per column of scratch, then
+                                the adding sweeps); 0 = 16384; negative = the single-kernel SW (no scratch besides
+                                the R/T stores) */
 } RadConfig;
 
 /* Column inputs (device pointers, float32).  ncol columns, nlay layers, nlp1 = nlay + 1 levels. */
@@ -159,8 +160,8 @@ void rad_graph_destroy(RadGraph* g);
  * handle of the process shares the one array: calls whose work may overlap on the device (other streams,
  * other host threads) race on it, so issue them on one stream or one after another.  Profiling events are
  * not recorded by this entry.  The LW runs in its single-kernel form (no scratch; columns with a cloudy layer
- * thinner than 1 hPa are solved again in float64 from a list kept in the array), so results equal rad_solve's
- * on a handle configured with lw_chunk < 0. */
+ * thinner than 1 hPa are solved again in float64 from a list kept in the array) and the SW in its single-kernel
+ * form, so results equal rad_solve's on a handle configured with lw_chunk < 0 and sw_sweep_chunk < 0. */
 #define RAD_NOALLOC_MAX_COLS 65536
 int rad_solve_noalloc(RadHandle* h, const RadColumns* in, const RadOutputs* out, int64_t ncol, void* stream);
 

@@ -1,9 +1,10 @@
-"""The two-kernel SW (sw3_optics_kernel + sw3_sweep_kernel: set-up and optics of a chunk of day columns into
-shared-memory images, then the sweeps from them) against the single-kernel SW (sw_sweep_chunk < 0) through
-the C-ABI: the same arithmetic, so every output bit is equal, with chunks smaller than the day count
-(several chunks, a ragged last one, chunks past the day count that exit at once), with aerosol optics, on
-the McICA route, and against the float64 oracle within the mixed-precision tolerances (0.05 W/m^2,
-0.01 K/day)."""
+"""The two-kernel SW (sw4_optics_kernel + sw4_sweep_kernel: set-up, optics and the layer R/T of a chunk of day
+columns into the chunk scratch, then the adding sweeps from it) against the single-kernel SW (sw_sweep_chunk
+< 0) through the C-ABI, with chunks smaller than the day count (several chunks, a ragged last one, chunks past
+the day count that exit at once), with aerosol optics, on the McICA route, and against the float64 oracle
+within the mixed-precision tolerances (0.05 W/m^2, 0.01 K/day).  Both forms run the same statements and make
+the same float64 / table-entry decisions; the compiler may fuse a multiply and an add differently in the two
+kernels, so the outputs agree to float rounding (relative 1e-5 of each output's scale), not to the bit."""
 from __future__ import annotations
 
 import numpy as np
@@ -40,7 +41,9 @@ def _aerosol(ncol, nlay=61, seed=12):
 
 def _equal(a, b, what):
     for k in a:
-        assert np.array_equal(a[k], b[k]), f"{what}: {k} differs (max {np.abs(a[k] - b[k]).max():.3e})"
+        scale = max(float(np.abs(b[k]).max()), 1e-30)
+        d = float(np.abs(a[k].astype(np.float64) - b[k]).max())
+        assert d <= 1e-5 * scale, f"{what}: {k} differs by {d:.3e} (scale {scale:.3e})"
 
 
 @pytest.mark.parametrize("chunk", [0, 333, 512])

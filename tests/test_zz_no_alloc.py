@@ -1,6 +1,7 @@
 """rad_solve_noalloc (fixed scratch array, no allocator) against rad_solve through the C ABI: two calls in
-a row give rad_solve's outputs (on a handle with the single-kernel LW, lw_chunk < 0, the form the
-no-allocation entry runs), and requests the fixed region cannot hold are refused before any launch.
+a row give rad_solve's outputs (on a handle with the single-kernel LW and SW, lw_chunk < 0 and
+sw_sweep_chunk < 0, the forms the no-allocation entry runs), and requests the fixed region cannot hold are
+refused before any launch.
 The file name sorts last so the test also runs after every other GPU test of the session."""
 from __future__ import annotations
 
@@ -26,7 +27,7 @@ def _call(s, cols, solcon, out, stream):
 def test_noalloc_equals_solve_twice(precision):
     import torch
     from woof_nam_b200.solver import RadSolver
-    s = RadSolver(precision=precision, lw_chunk=-1)
+    s = RadSolver(precision=precision, lw_chunk=-1, sw_sweep_chunk=-1)
     st = torch.cuda.current_stream()
     for n, seed in ((3001, 41), (777, 42)):           # two calls in a row, the second smaller
         c = make_columns(n, seed)
@@ -45,7 +46,7 @@ def test_noalloc_equals_solve_twice(precision):
 def test_noalloc_mcica_with_caller_masks():
     import torch
     from woof_nam_b200.solver import RadSolver
-    s = RadSolver(precision="mixed", route="mcica", lw_chunk=-1)
+    s = RadSolver(precision="mixed", route="mcica", lw_chunk=-1, sw_sweep_chunk=-1)
     c = make_columns(1500, 43)
     d = s.to_device(c)
     ref = s.solve(d, c.solcon)

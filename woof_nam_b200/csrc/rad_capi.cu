@@ -35,6 +35,7 @@ __constant__ int c_sw_ns[15] = {0, 6, 18, 26, 34, 44, 54, 56, 66, 74, 80, 86, 94
 #include "rad_sw2.cuh"
 #include "rad_lw2.cuh"
 #include "rad_lw3.cuh"
+#include "rad_sw4.cuh"
 #include "rad_mcica.cuh"
 #include "rad_post.cuh"
 #include "rad_rdtemp.cuh"
@@ -64,10 +65,9 @@ struct RadHandle {
     int64_t lw3_cap = 0;                           // columns d_lw3 holds
     int* d_lw3list = nullptr;                      // [1 + lw3_cap]: count, then the chunk's float64 columns
     float* d_swrt = nullptr;                       // SW layer R/T stores, sw2_rt_floats() per CTA of the SW grid
-    int4* d_swimg = nullptr;                       // two-kernel SW: shared-memory images of one chunk's columns
-    int64_t swimg_cap = 0;                         // columns d_swimg holds
-    int* d_swq = nullptr;                          // two-kernel SW: one column counter per chunk
-    int64_t swq_cap = 0;
+    int4* d_sw4img = nullptr;                      // chunked SW: set-up and gas-optics images of one chunk's columns
+    unsigned char* d_sw4 = nullptr;                // chunked SW: header and layer R/T of one chunk's columns
+    int64_t sw4_cap = 0;                           // columns d_sw4 and d_sw4img hold
     float* d_aerf = nullptr;                       // aerosol band tables of the loaded month (AF_* offsets)
     int* d_aeri = nullptr;                         // their integer part (AI_* offsets)
     int nsm = 148;                                 // SMs of the device (grid of the float64 column kernel)
@@ -291,10 +291,10 @@ int64_t lw3_chunk(const RadConfig& cfg)
 }
 
 // Day columns per chunk of the two-kernel SW (mixed precision), 0 when the single-kernel SW runs.
-int64_t sw3_chunk(const RadConfig& cfg)
+int64_t sw4_chunk(const RadConfig& cfg)
 {
     if (cfg.precision != RAD_PREC_MIXED || cfg.sw_sweep_chunk < 0) return 0;
-    return cfg.sw_sweep_chunk > 0 ? cfg.sw_sweep_chunk : 65536;
+    return cfg.sw_sweep_chunk > 0 ? cfg.sw_sweep_chunk : 16384;
 }
 
 // Scratch for a launch of ntot columns: day list arrays, CUB temp, chunk minima, McICA words.
@@ -323,24 +323,19 @@ int ensure_launch_scratch(RadHandle* h, int64_t ntot, int64_t ncmin)
             h->lw3_cap = need;
         }
     }
-    if (h->cfg.precision == RAD_PREC_MIXED && (h->cfg.parts & RAD_PART_SW) && !h->d_swrt)
+    const int64_t swc = sw4_chunk(h->cfg);
+    if (h->cfg.precision == RAD_PREC_MIXED && (h->cfg.parts & RAD_PART_SW) && swc <= 0 && !h->d_swrt)
         RAD_CUDA(h, cudaMalloc((void**)&h->d_swrt, (size_t)sw2_rt_bytes(h->nsm)));
-    const int64_t swc = sw3_chunk(h->cfg);
-    if (swc > 0 && (h->cfg.parts & RAD_PART_SW) && std::min(swc, ntot) > h->swimg_cap) {
-        if (h->d_swimg) cudaFree(h->d_swimg);
-        h->d_swimg = nullptr;
-        h->swimg_cap = 0;
+    if (swc > 0 && (h->cfg.parts & RAD_PART_SW) && std::min(swc, ntot) > h->sw4_cap) {
+        if (h->d_sw4) cudaFree(h->d_sw4);
+        if (h->d_sw4img) cudaFree(h->d_sw4img);
+        h->d_sw4 = nullptr;
+        h->d_sw4img = nullptr;
+        h->sw4_cap = 0;
         const int64_t need = std::min(swc, ntot);
-        RAD_CUDA(h, cudaMalloc((void**)&h->d_swimg, (size_t)need * sw2_image_bytes(true)));
-        h->swimg_cap = need;
-    }
-    if (swc > 0 && (h->cfg.parts & RAD_PART_SW) && (ntot + swc - 1) / swc > h->swq_cap) {
-        if (h->d_swq) cudaFree(h->d_swq);
-        h->d_swq = nullptr;
-        h->swq_cap = 0;
-        const int64_t need = (ntot + swc - 1) / swc;
-        RAD_CUDA(h, cudaMalloc((void**)&h->d_swq, (size_t)need * sizeof(int)));
-        h->swq_cap = need;
+        RAD_CUDA(h, cudaMalloc((void**)&h->d_sw4, (size_t)need * sw4_block_bytes(h->cfg.nlay)));
+        RAD_CUDA(h, cudaMalloc((void**)&h->d_sw4img, (size_t)need * sw4_image_bytes(true)));
+        h->sw4_cap = need;
     }
     if (h->cfg.route == RAD_ROUTE_MCICA && ntot * h->cfg.nlay > h->mask_cap) {
         if (h->d_lwm) cudaFree(h->d_lwm);
@@ -543,24 +538,26 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 sw2_column_kernel<false><<<(unsigned)ntot, SW2_THREADS, smem, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd,
                                                                                      h->d_err, nullptr);
-            } else if (sw3_chunk(cfg) > 0) {
+            } else if (sw4_chunk(cfg) > 0) {
                 // per chunk of day indices (the day count stays on the device: chunks past it exit at once):
-                // set-up and optics one CTA per column into the images, then the sweeps take the chunk's
-                // columns from its counter
-                const int64_t swc = sw3_chunk(cfg);
-                const size_t smem1 = sw3_optics_smem(any_aer);
-                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw3_optics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
-                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw3_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                RAD_CUDA(h, cudaMemsetAsync(h->d_swq, 0, (size_t)((ntot + swc - 1) / swc) * sizeof(int), st));
+                // set-up and gas optics one CTA per column into the images, the layer R/T one CTA per column
+                // into the chunk scratch, then the adding sweeps one CTA per column
+                const int64_t swc = sw4_chunk(cfg);
+                const size_t smem0 = sw4_gas_smem(any_aer);
+                const size_t smem1 = sizeof(SwSh2) + (any_aer ? sizeof(SwAer) : 0);
+                const size_t smem2 = (size_t)(SW2_NSEG - 1) * 4 * SW2_THREADS * sizeof(float);
+                const size_t bb = sw4_block_bytes(nlay);
+                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw4_gas_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
+                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw4_rt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
+                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw4_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
                 for (int64_t d0 = 0; d0 < ntot; d0 += swc) {
                     const int64_t nc = std::min(swc, ntot - d0);
-                    sw3_optics_kernel<<<(unsigned)nc, SW2_THREADS, smem1, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd,
-                                                                             h->d_err, (int)d0, h->d_swimg);
-                    sw3_sweep_kernel<<<(unsigned)(SW2_CTAS_PER_SM * h->nsm), SW2_THREADS, smem, st>>>(
-                        bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, h->d_err, (int)d0, (int)nc, h->d_swimg, h->d_swrt,
-                        h->d_swq + d0 / swc);
+                    sw4_gas_kernel<<<(unsigned)nc, SW2_THREADS, smem0, st>>>(bt, any_aer ? 1 : 0, h->d_err, (int)d0, h->d_sw4img);
+                    sw4_rt_kernel<<<(unsigned)nc, SW2_THREADS, smem1, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, (int)d0,
+                                                                         h->d_sw4img, h->d_sw4, bb);
+                    sw4_sweep_kernel<<<(unsigned)nc, SW2_THREADS, smem2, st>>>(bt, h->d_err, (int)d0, (int)nc, h->d_sw4, bb);
                 }
-                nlaunch = 2 * ((ntot + swc - 1) / swc);
+                nlaunch = 3 * ((ntot + swc - 1) / swc);
             } else {       // SW2_CTAS_PER_SM CTAs per SM walk the day list, each with its R/T store
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 sw2_column_kernel<true><<<(unsigned)(SW2_CTAS_PER_SM * h->nsm), SW2_THREADS, smem, st>>>(
@@ -746,9 +743,10 @@ int64_t rad_workspace_bytes(const RadHandle* h, int64_t ncol)
         if (lwc > 0 && (h->cfg.parts & RAD_PART_LW))
             b += std::min(lwc, ncol) * lw3_block_floats(h->cfg.nlay) * (int64_t)sizeof(float);
         if (h->cfg.route == RAD_ROUTE_MCICA) b += 9 * (int64_t)h->cfg.nlay * ncol * (int64_t)sizeof(uint32_t);
-        if (h->cfg.precision == RAD_PREC_MIXED && (h->cfg.parts & RAD_PART_SW)) b += sw2_rt_bytes(h->nsm);
-        const int64_t swc = sw3_chunk(h->cfg);
-        if (swc > 0 && (h->cfg.parts & RAD_PART_SW)) b += std::min(swc, ncol) * (int64_t)sw2_image_bytes(true);
+        const int64_t swc = sw4_chunk(h->cfg);
+        if (h->cfg.precision == RAD_PREC_MIXED && (h->cfg.parts & RAD_PART_SW) && swc <= 0) b += sw2_rt_bytes(h->nsm);
+        if (swc > 0 && (h->cfg.parts & RAD_PART_SW))
+            b += std::min(swc, ncol) * (int64_t)(sw4_block_bytes(h->cfg.nlay) + sw4_image_bytes(true));
     }
     return b;
 }
@@ -1114,7 +1112,7 @@ void rad_destroy(RadHandle* h)
     for (void* p : {(void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
                     (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
                     (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub, (void*)h->d_lwm,
-                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt, (void*)h->d_swimg, (void*)h->d_swq, (void*)h->d_aerf,
+                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt, (void*)h->d_sw4, (void*)h->d_sw4img, (void*)h->d_aerf,
                     (void*)h->d_aeri})
         if (p) cudaFree(p);
     delete h;

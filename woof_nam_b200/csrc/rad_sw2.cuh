@@ -558,8 +558,7 @@ __device__ __noinline__ bool sw2_rt_double(float t0, float tabs, float s0, float
 // delp), x.wf the step of exp(-tau0 / mu0) (the surface direct beam alone).
 __device__ __forceinline__ void sw2_rt_mixed(float t0, float tabs, float s0, float y0, float cz, float snt,
                                              const float* ex, const SwExactCtx& x, int k0, int g, int ib, bool cloud,
-                                             float wk, float& rb, float& rd, float& tb, float& td, float& e3,
-                                             float& e4)
+                                             float wk, float& rb, float& rd, float& tb, float& td, float& e3, float& e4)
 {
     const SwPro<float> p = sw2_prologue<float>(t0, tabs, s0, y0, x.mode, cz);
     bool exact = false;
@@ -583,6 +582,44 @@ __device__ __forceinline__ void sw2_rt_mixed(float t0, float tabs, float s0, flo
     }
     e3 = sw_expm(p.ztau1 * snt, ex, true);
     e4 = sw_expm(zb4, ex, true);
+}
+
+// Entry int(10^4 zb / (bpade + zb) + 1/2) of the reference's exp table, exp(-bpade i / (10^4 - i)) (1e-20 for
+// the last), evaluated instead of loaded (the float R/T of sw2_rt_float; within a few float ulps of the table's
+// float value for the arguments that matter, ~1e-5 relative where exp is below 1e-13), with the series below
+// 0.06 as sw_expm; em = its complement.
+__device__ __forceinline__ float sw2_tblexp(float zb, float& em)
+{
+    if (zb <= 0.06f) {
+        em = zb - 0.5f * zb * zb;
+        return 1.0f - zb + 0.5f * zb * zb;
+    }
+    const float ftind = zb / ((float)1.0f / (float)0.278f + zb);
+    const int it = min(10000, (int)(ftind * (float)10000 + (float)0.5f));
+    const float e = it >= 10000 ? 1.0e-20f : __expf(-(3.59712230f * (float)it) / (float)(10000 - it));
+    em = 1.0f - e;
+    return e;
+}
+
+// The float R/T of sw2_rt_mixed alone: false (and nothing final) where sw2_rt_mixed would take any float64 step
+// or test the neighbouring table entry -- the resonance, an argument near a table-entry bound with a weight.
+// Where it returns true the outputs are exactly sw2_rt_mixed's.
+__device__ __forceinline__ bool sw2_rt_float(float t0, float tabs, float s0, float y0, float cz, float snt,
+                                             const float* ex, int mode, float wk, float wf, float& rb, float& rd,
+                                             float& tb, float& td, float& e3, float& e4)
+{
+    const SwPro<float> p = sw2_prologue<float>(t0, tabs, s0, y0, mode, cz);
+    if (fabsf(p.zrpp) < SW2_RESONANCE) return false;
+    if (wk > 0.0f && (sw2_near(fminf(p.zrk * p.ztau1, 500.0f)) || sw2_near(fminf(p.ztau1 * snt, 500.0f)))) return false;
+    const float zb4 = t0 * snt;
+    if (wf * 4.0e-4f > 1.0f && sw2_near(zb4)) return false;
+    float em1, em2, em;
+    const float e1 = sw2_tblexp(fminf(p.zrk * p.ztau1, 500.0f), em1);
+    const float e2 = sw2_tblexp(fminf(p.ztau1 * snt, 500.0f), em2);
+    sw2_rt_core<float>(p, cz, e1, em1, e2, em2, rb, rd, tb, td);
+    e3 = sw2_tblexp(p.ztau1 * snt, em);
+    e4 = sw2_tblexp(zb4, em);
+    return true;
 }
 
 struct SwLayerRT {
@@ -697,63 +734,14 @@ __host__ __device__ constexpr int64_t sw2_rt_floats()
 }
 inline int64_t sw2_rt_bytes(int nsm) { return (int64_t)SW2_CTAS_PER_SM * nsm * sw2_rt_floats() * (int64_t)sizeof(float); }
 
-// Parts of the column solve a call runs: all of it, or (split over two kernels) phases A and B into a
-// shared-memory image in global memory, then phase C from that image.
-constexpr int SW2_ALL = 0, SW2_OPTICS = 1, SW2_SWEEP = 2;
-// The shared-memory image phase C reads: from SwSh2::colmol to the end of SwSh2 and, with aerosol, the
-// aerosol block after it; sw2_image_bytes rounds it up to 16-byte units.
-__host__ __device__ constexpr size_t sw2_image_begin() { return offsetof(SwSh2, colmol); }
-__host__ __device__ constexpr size_t sw2_image_bytes(bool aer)
+// Phases A1 and A2 of one sunlit column (day index d, column col of request a) into shared memory s (aer: the
+// aerosol block or null): layer coefficients, aerosol, heating factors, column scalars, cloud optics per (band,
+// layer), solar source, Rayleigh coefficients.  Ends with a barrier.
+__device__ __forceinline__ void sw2_setup(SwSh2& s, SwAer* aer, const SwIn& a, int64_t col, int d, int tid)
 {
-    return ((sizeof(SwSh2) - sw2_image_begin() + (aer ? sizeof(SwAer) : 0)) + 15) / 16 * 16;
-}
-static_assert(offsetof(SwSh2, colmol) % 16 == 0, "the image starts on a 16-byte boundary");
-static_assert(offsetof(SwSh2, taug) + sizeof(SwSh2::taug) == sizeof(SwSh2) && sizeof(SwAer) % 16 == 0,
-              "taug closes SwSh2 and the aerosol block is whole 16-byte units");
-// Shared memory of the optics kernel: SwSh2 up to taug, then the aerosol block.
-__host__ __device__ constexpr size_t sw3_optics_smem(bool aer)
-{
-    return offsetof(SwSh2, taug) + (aer ? sizeof(SwAer) : 0);
-}
-
-// One sunlit column (day index d) by the CTA; STORE: rt = the CTA's R/T store, else the R/T is recomputed.
-// PART: SW2_ALL, or SW2_OPTICS (phases A and B, the shared memory then copied to img) / SW2_SWEEP (shared
-// memory loaded from img, then phase C).
-template <bool STORE, int PART = SW2_ALL>
-__device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const float* ex, const double* exd,
-                                           int* err, int d, float* rt, int4* img = nullptr)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SwSh2& s = *reinterpret_cast<SwSh2*>(smem_raw);
-    const int64_t gcol = bt.req[0].daycol[d];
-    const int rq = bt.find(gcol);
-    const SwIn& a = bt.req[rq];
-    // the aerosol block is reserved when any request of the launch has aerosol; used when this one does.  The
-    // optics kernel keeps it where taug would be: taug goes straight to the image.
-    SwAer* aer = a.faersw ? reinterpret_cast<SwAer*>(smem_raw + (PART == SW2_OPTICS ? offsetof(SwSh2, taug)
-                                                                                      : sizeof(SwSh2)))
-                          : nullptr;
-    float* img_taug = PART == SW2_OPTICS ? reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(img) +
-                                                                    (offsetof(SwSh2, taug) - sw2_image_begin()))
-                                         : nullptr;
-    float* ckpt = reinterpret_cast<float*>(smem_raw + sizeof(SwSh2) + (any_aer ? sizeof(SwAer) : 0));
-    const int nlay = a.nlay, nlp1 = nlay + 1;
-    if (nlay > NLAY_MAX) {
-        if (threadIdx.x == 0) atomicExch(err, RAD_DEV_NLAY);
-        return;
-    }
+    const int nlay = a.nlay;
     const int64_t N = a.ncol;
-    const int64_t col = gcol - bt.off[rq];
-    const int tid = threadIdx.x;
     const double heatfac = 9.80665 * 1.0e-2 / 1.0046e3;
-    if (PART == SW2_SWEEP) {   // every 16-byte piece of the image in flight at once (cp.async.cg: L2 to shared)
-        const uint32_t sb = (uint32_t)__cvta_generic_to_shared(smem_raw + sw2_image_begin());
-        for (int i = tid; i < (int)(sw2_image_bytes(any_aer) / 16); i += SW2_THREADS)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sb + 16u * (uint32_t)i), "l"(img + i)
-                         : "memory");
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        __syncthreads();
-    } else {
     // ---- phase A1: layer coefficients (threads = layers), aerosol, heating factors.  The coefficients are
     // formed in float64 and rounded once: the interpolation weights take a difference of logarithms, which
     // float would carry with ~1e-6 of the gas optical depths' error (and move their exp-table entries).
@@ -836,26 +824,38 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
     if (tid < 14) sw_sfluxzen<float>(s, tid, nlay);
     for (int g = tid; g < SW_NGPT; g += SW2_THREADS) s.raylc[g] = sw2_rayl_coef(g);
     __syncthreads();
+}
+
+// One sunlit column (day index d) by the CTA; STORE: rt = the CTA's R/T store, else the R/T is recomputed.
+template <bool STORE>
+__device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const float* ex, const double* exd,
+                                           int* err, int d, float* rt)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SwSh2& s = *reinterpret_cast<SwSh2*>(smem_raw);
+    const int64_t gcol = bt.req[0].daycol[d];
+    const int rq = bt.find(gcol);
+    const SwIn& a = bt.req[rq];
+    // the aerosol block is reserved when any request of the launch has aerosol; used when this one does
+    SwAer* aer = a.faersw ? reinterpret_cast<SwAer*>(smem_raw + sizeof(SwSh2)) : nullptr;
+    float* ckpt = reinterpret_cast<float*>(smem_raw + sizeof(SwSh2) + (any_aer ? sizeof(SwAer) : 0));
+    const int nlay = a.nlay, nlp1 = nlay + 1;
+    if (nlay > NLAY_MAX) {
+        if (threadIdx.x == 0) atomicExch(err, RAD_DEV_NLAY);
+        return;
+    }
+    const int64_t N = a.ncol;
+    const int64_t col = gcol - bt.off[rq];
+    const int tid = threadIdx.x;
+    sw2_setup(s, aer, a, col, d, tid);
     // ---- phase B: gas and Rayleigh optical depths per (g, layer), band by band
     for_each_band_pair(c_sw_ns, 14, nlay, &s.task_next, tid & 31, [&](int g, int k0, int b) {
         float tg, tr;
         sw_gas<float>(s, g, k0, tg, tr, b);
-        if (PART == SW2_OPTICS)
-            img_taug[g * SW2_KS + k0] = tg;
-        else
-            s.taug[g][k0] = tg;
+        s.taug[g][k0] = tg;
         if (g >= 66 && g < 74 && k0 < s.laytrop) s.taur24[g - 66][k0] = tr;
     });
     __syncthreads();
-    }
-    if (PART == SW2_OPTICS) {   // the image up to taug, then the aerosol block after taug's place
-        const int4* sm = reinterpret_cast<const int4*>(smem_raw + sw2_image_begin());
-        const int n1 = (int)((offsetof(SwSh2, taug) - sw2_image_begin()) / 16);
-        const int n2 = any_aer ? (int)(sizeof(SwAer) / 16) : 0;
-        const int skip = (int)(sizeof(SwSh2::taug) / 16);
-        for (int i = tid; i < n1 + n2; i += SW2_THREADS) img[i < n1 ? i : i + skip] = sm[i];
-        return;
-    }
     // ---- phase C: spcvrtc, one g-point per lane, both passes
     const int warp = tid >> 5, lane = tid & 31;
     bool act;
@@ -1080,40 +1080,6 @@ sw2_column_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* 
     for (int d = blockIdx.x; d < nday; d += gridDim.x) {
         sw2_column<true>(bt, any_aer, ex, exd, err, d, rt);
         __syncthreads();                       // shared memory is reused by the next column
-    }
-}
-
-// The SW solve split in two kernels per chunk of day indices [d0, d0 + nc): sw3_optics_kernel, one CTA per
-// column, runs phases A and B (set-up, cloud and gas optics: no sweep registers and no taug in shared
-// memory, so five CTAs per SM) and writes the image; sw3_sweep_kernel, SW2_CTAS_PER_SM CTAs per SM walking
-// the chunk, loads each image and runs phase C with its R/T store.  Same arithmetic as
-// sw2_column_kernel<true>, same bits.
-constexpr int SW3_CHUNK = 32768;                               // day columns per optics / sweep pair
-__global__ void __launch_bounds__(SW2_THREADS, 5)
-sw3_optics_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, const double* exd, int* err,
-                  int d0, int4* img)
-{
-    const int d = d0 + (int)blockIdx.x;
-    if (d >= *bt.req[0].nday) return;
-    sw2_column<false, SW2_OPTICS>(bt, any_aer, ex, exd, err, d, nullptr,
-                                  img + (size_t)blockIdx.x * (sw2_image_bytes(any_aer) / 16));
-}
-// Columns go to CTAs as they free up (q: the chunk's counter, zero at launch): cloudy columns take about
-// twice as long as clear ones, so a fixed stride would leave the kernel waiting on the unluckiest CTA.
-__global__ void __launch_bounds__(SW2_THREADS, SW2_CTAS_PER_SM)
-sw3_sweep_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, const double* exd, int* err,
-                 int d0, int nc, const int4* img, float* rts, int* q)
-{
-    __shared__ int next;
-    const int nday = *bt.req[0].nday;
-    float* rt = rts + (int64_t)blockIdx.x * sw2_rt_floats();
-    for (int i = blockIdx.x; i < nc && d0 + i < nday;) {
-        sw2_column<true, SW2_SWEEP>(bt, any_aer, ex, exd, err, d0 + i, rt,
-                                    const_cast<int4*>(img) + (size_t)i * (sw2_image_bytes(any_aer) / 16));
-        __syncthreads();                       // shared memory is reused by the next column
-        if (threadIdx.x == 0) next = (int)gridDim.x + atomicAdd(q, 1);
-        __syncthreads();
-        i = next;
     }
 }
 

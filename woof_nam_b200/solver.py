@@ -44,7 +44,7 @@ class SolverConfig:
     sw_seed0: int = 1
     parts: str = "both"              # "lw", "sw" or "both": which solves run (lslwr / lsswr steps)
     lw_chunk: int = 0                # mixed: columns per two-kernel LW chunk (0 = 32768, < 0 single kernel)
-    sw_sweep_chunk: int = 0          # mixed: day columns per two-kernel SW chunk (0 = 65536, < 0 single kernel)
+    sw_sweep_chunk: int = 0          # mixed: day columns per two-kernel SW chunk (0 = 16384, < 0 single kernel)
 
 
 def output_shapes(nlay: int, ncol: int, route: str = "nam") -> dict:
