@@ -48,6 +48,10 @@ def parse():
                     help="skip the uneven-batch leg (parent grid + three nests in one graph-captured launch set)")
     ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
     ap.add_argument("--no-aer", action="store_true", help="skip the aerosol-optics leg")
+    ap.add_argument("--no-parity", action="store_true", help="skip the parity block (errors against the oracle)")
+    ap.add_argument("--parity-sample", type=int, default=16384)
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-requests", type=int, default=40)
     ap.add_argument("--lw-chunk", type=int, default=None,
                     help="LW chunk size (columns); default: the autotuner's choice for this device")
     ap.add_argument("--ncol", type=int, default=None,
@@ -164,6 +168,68 @@ def cpu_baseline(cols, n_sample):
             "sample": f"first {sub.ncol} columns of the timed workload, one solve, FP32 "
                       f"{'reference kernels compiled for the host' if which == 'ref' else 'oracle restatement'}, "
                       f"{dt:.1f} s"}
+
+
+def parity_block(cols, mcfg, n_sample):
+    """Errors of the timed path against the float64 oracle on the first n_sample columns of the timed workload,
+    through the same solver configuration with lwrad's / swrad's optional outputs on: the largest absolute error
+    of every output (heating K/day, fluxes W/m^2), of every band's heating (hlwb 16 LW bands, htswb 14 SW bands),
+    and the count of values above the tolerances (0.01 K/day, 0.05 W/m^2)."""
+    from oracle import oracle
+    from woof_nam_b200.solver import RadSolver, SolverConfig
+    sub = cols.slice(0, min(n_sample, cols.ncol))
+    flags = dict(lhsw0=True, lhswb=True, lhlw0=True, lhlwb=True, lflxprf=True)
+    s = RadSolver(SolverConfig(**{**mcfg.__dict__, **flags}))
+    got = s.solve_host(sub)
+    s.close()
+    ref = oracle.solve(sub, precision="double", diag=True, nthreads=oracle.host_threads())
+    heat = ("htlw", "htsw", "hlw0", "hsw0", "hlwb", "htswb")
+    flux = ("topflw", "sfcflw", "topfsw", "sfcfsw", "fdncmp", "lwflxprf", "swflxprf")
+
+    def err(k):
+        o, r = np.asarray(got[k], np.float64), np.asarray(ref[k], np.float64)
+        d = np.where(np.isfinite(o) & np.isfinite(r), np.abs(o - r), np.inf)
+        return d * (86400.0 if k in heat else 1.0)
+
+    e = {k: err(k) for k in heat + flux}
+    return {
+        "sample": f"first {sub.ncol} columns of the timed workload ({int((sub.coszen >= 1e-4).sum())} sunlit), "
+                  f"float64 oracle (C++ restatement of the reference statements)",
+        "tolerance": {"heating_K_per_day": 0.01, "flux_W_per_m2": 0.05},
+        "max_abs": {k: float(v.max()) for k, v in e.items() if k not in ("hlwb", "htswb")},
+        "max_abs_per_band": {"hlwb": [float(x) for x in e["hlwb"].reshape(16, -1).max(axis=1)],
+                             "htswb": [float(x) for x in e["htswb"].reshape(14, -1).max(axis=1)]},
+        "values_over_tolerance": {k: int((v > (0.01 if k in heat else 0.05)).sum()) for k, v in e.items()},
+        "values": int(sum(v.size for v in e.values())),
+    }
+
+
+def serving_block(members: int, n_req: int, seed: int = 7) -> dict:
+    """The serving workload (Poisson arrivals of whole-domain solves drawn from the parent grid and the three
+    nests, ensemble members resident on the device, admission by a 120 GB HBM budget, 4 slots): once at the
+    configured 40 requests/s, which offers ~12 M columns/s (beyond what one GPU serves, so latency there is
+    queueing), and once at 80 % of the rate the GPU sustained in that run, where the queue stays short.  Latency
+    from arrival to completion; offered and served columns/s."""
+    from woof_nam_b200 import serve
+    from woof_nam_b200.columns import SOLCON
+    states = serve.member_states(members)
+    srv = serve.RadServer(states, SOLCON, slots=4, hbm_budget_gb=120.0)
+    srv.run([serve.Request(-1, name, 0, 0.0) for name in serve.DOMAINS])
+    mean_cols = float(np.mean(list(serve.DOMAINS.values())))
+
+    def leg(rate, s):
+        r = srv.run(serve.poisson_requests(n_req, rate, members, seed=s))
+        return {"rate_per_s": rate, "offered_columns_per_s": rate * mean_cols, "served_columns_per_s": r["columns_per_s"],
+                "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "mean_ms": r["mean_ms"], "requests": r["requests"]}
+
+    sat = leg(40.0, seed)
+    sus = leg(0.8 * sat["served_columns_per_s"] / mean_cols, seed + 1)
+    res = {"workload": f"Poisson arrivals, domains uniform over {list(serve.DOMAINS)} x 61 layers, {members} members "
+                       f"resident ({srv.resident / 1e9:.1f} GB), HBM budget 120 GB, 4 slots "
+                       f"({srv.held / 1e9:.1f} GB of slot scratch)",
+           "at_40_per_s": sat, "sustainable": sus}
+    del srv, states
+    return res
 
 
 def main():
@@ -366,6 +432,18 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(cols, args.cpu_sample)
+    parity = None
+    if rank == 0 and ws == 1 and not args.no_parity:
+        parity = parity_block(cols, mcfg, args.parity_sample)
+    serving = None
+    if ws == 1 and not args.no_serve and args.ncol is None:
+        del mixed
+        d.clear()
+        out.clear()
+        hin.clear()
+        hout.clear()
+        torch.cuda.empty_cache()
+        serving = serving_block(10, args.serve_requests)
 
     if rank == 0:
         line = {
@@ -393,6 +471,8 @@ def main():
                                  "unit": "GB/s", "frac": (in_bytes + out_bytes) / (ms * 1e-3) / 1e9 / hbm_peak}},
             "plain_fp64": fp64,
             "cpu_baseline": cpu,
+            "parity": parity,
+            "serving": serving,
             "e2e": {"value": ws * n / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": in_bytes,
                     "d2h_bytes_per_step": out_bytes, "ms_per_step": ms_e2e},
             "batch_c3": batch,

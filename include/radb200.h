@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define RAD_ABI_VERSION 1
+#define RAD_ABI_VERSION 2
 
 enum {
     RAD_OK = 0,
@@ -107,6 +107,18 @@ typedef struct {
     uint32_t* lw_mask;       /* [5][nlay][ncol] McICA LW sub-column cloud words, optional (McICA route):
                                 bit g & 31 of word g >> 5 for g-point g, layers surface first (lcloudy) */
     uint32_t* sw_mask;       /* [4][nlay][ncol] McICA SW sub-column cloud words, optional, same packing */
+    /* Optional outputs of lwrad / swrad (NULL = not wanted), levels top first, as the reference's units write
+     * them when their switches are on (phys_rrtm_sw_swrad.py:49-51, phys_rrtm_lw_lwrad.py:47-50; kernels
+     * phys_rrtm_sw_swrad.cu:393-418, phys_rrtm_lw_rtrnmr_body.cuh:328-362, phys_rrtm_lw_lwrad.cu:343-363).
+     * They run on rad_solve's mixed-precision path with the chunked LW and SW (lw_chunk >= 0,
+     * sw_sweep_chunk >= 0); another configuration, or rad_solve_noalloc, refuses them with RAD_E_INVALID. */
+    float* hsw0;             /* [nlay][ncol] SW clear-sky heating rate, K/s (HSW0, lhsw0) */
+    float* htswb;            /* [14][nlay][ncol] SW heating rate per band, K/s (HTSWB, lhswb) */
+    float* swflxprf;         /* [4][nlay + 1][ncol] SW level fluxes: up total, down total, up clear, down clear
+                                (FLXPRF, lflxprf) */
+    float* hlw0;             /* [nlay][ncol] LW clear-sky heating rate, K/s (htlw0, lhlw0) */
+    float* hlwb;             /* [16][nlay][ncol] LW heating rate per band, K/s (htlwb, lhlwb) */
+    float* lwflxprf;         /* [4][nlay + 1][ncol] LW level fluxes, same order (flwprf, lflxprf) */
 } RadOutputs;
 
 /* Library version (RAD_ABI_VERSION).  Replaces: nothing in the reference (a versioned ABI). */

@@ -81,8 +81,11 @@ def _f(a):
 def solve(cols, precision: str = "double", iswmode: int = 2, window_cols: int = 0, sw_chunk: int = 32768,
           route: int = 0, iovrlw: int = 1, iovrsw: int = 1, lw_seed0: int = 140, sw_seed0: int = 1,
           cpathfac: float = 1.5, nthreads: int = 0, which: str = "port", want_profiles: bool = False,
-          icseed=None, faerlw=None, faersw=None) -> dict:
-    """Run the oracle on a ``woof_nam_b200.columns.Columns`` request; returns float64 outputs."""
+          icseed=None, faerlw=None, faersw=None, diag: bool = False) -> dict:
+    """Run the oracle on a ``woof_nam_b200.columns.Columns`` request; returns float64 outputs.  diag (the
+    restatement only) adds lwrad's / swrad's optional outputs: hlw0, hlwb [16], hsw0, htswb [14] (K/s, top
+    first) and the level-flux profiles lwflxprf / swflxprf [4][nlay+1] (up total, down total, up clear, down
+    clear, top first)."""
     L = lib(which)
     nlay, ncol = cols.nlay, cols.ncol
     cfg = np.array([iswmode, int(cols.diagnostic_clouds), window_cols, sw_chunk, route, iovrlw, iovrsw,
@@ -92,9 +95,16 @@ def solve(cols, precision: str = "double", iswmode: int = 2, window_cols: int = 
         "topflw": np.zeros((2, ncol)), "sfcflw": np.zeros((4, ncol)),
         "topfsw": np.zeros((3, ncol)), "sfcfsw": np.zeros((4, ncol)), "fdncmp": np.zeros((6, ncol)),
     }
-    if want_profiles:
+    if want_profiles or diag:
         out["lwflx"] = np.zeros((4, nlay + 1, ncol))
         out["swflx"] = np.zeros((4, nlay + 1, ncol))
+    if diag:
+        if which != "port":
+            raise ValueError("diag outputs come from the restatement (which='port')")
+        out["hlw0"] = np.zeros((nlay, ncol))
+        out["hlwb"] = np.zeros((16, nlay, ncol))
+        out["hsw0"] = np.zeros((nlay, ncol))
+        out["htswb"] = np.zeros((14, nlay, ncol))
     if route == 1:
         out["lw_mask"] = np.zeros((5, nlay, ncol), dtype=np.uint32)
         out["sw_mask"] = np.zeros((4, nlay, ncol), dtype=np.uint32)
@@ -106,15 +116,19 @@ def solve(cols, precision: str = "double", iswmode: int = 2, window_cols: int = 
     def p(a, t):
         return a.ctypes.data_as(t) if a is not None else None
 
-    rc = L.orc_solve(
-        ctypes.c_int(0 if precision == "float" else 1), p(cfg, _I), ctypes.c_double(cpathfac),
-        ctypes.c_int(nlay), ctypes.c_int(ncol),
-        *[p(a, _F) for a in keep[:8]], p(fa, _F), p(fs, _F), *[p(a, _F) for a in keep[8:]],
-        p(seeds, _I), ctypes.c_double(cols.solcon),
-        p(out["htlw"], _D), p(out["htsw"], _D), p(out["topflw"], _D), p(out["sfcflw"], _D),
-        p(out["topfsw"], _D), p(out["sfcfsw"], _D), p(out["fdncmp"], _D),
-        p(out.get("lwflx"), _D), p(out.get("swflx"), _D), p(out.get("lw_mask"), _U), p(out.get("sw_mask"), _U),
-        ctypes.c_int(nthreads))
+    args = [ctypes.c_int(0 if precision == "float" else 1), p(cfg, _I), ctypes.c_double(cpathfac),
+            ctypes.c_int(nlay), ctypes.c_int(ncol),
+            *[p(a, _F) for a in keep[:8]], p(fa, _F), p(fs, _F), *[p(a, _F) for a in keep[8:]],
+            p(seeds, _I), ctypes.c_double(cols.solcon),
+            p(out["htlw"], _D), p(out["htsw"], _D), p(out["topflw"], _D), p(out["sfcflw"], _D),
+            p(out["topfsw"], _D), p(out["sfcfsw"], _D), p(out["fdncmp"], _D),
+            p(out.get("lwflx"), _D), p(out.get("swflx"), _D), p(out.get("lw_mask"), _U), p(out.get("sw_mask"), _U)]
+    if diag:
+        rc = L.orc_solve_diag(*args, p(out["hlw0"], _D), p(out["hlwb"], _D), p(out["hsw0"], _D),
+                              p(out["htswb"], _D), ctypes.c_int(nthreads))
+        out["lwflxprf"], out["swflxprf"] = out["lwflx"], out["swflx"]
+    else:
+        rc = L.orc_solve(*args, ctypes.c_int(nthreads))
     if rc != 0:
         raise RuntimeError(f"oracle solve failed ({rc})")
     return out

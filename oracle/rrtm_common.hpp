@@ -105,6 +105,10 @@ struct Outputs {
     double *swflx;                    // optional [4][nlay+1][ncol] up/dn total, up/dn clear (top first)
     unsigned int* lw_mask;            // optional McICA masks [5][nlay][ncol]
     unsigned int* sw_mask;            // optional McICA masks [4][nlay][ncol]
+    double* hlw0 = nullptr;           // optional [nlay][ncol] LW clear-sky heating, K/s (lhlw0)
+    double* hlwb = nullptr;           // optional [16][nlay][ncol] LW heating per band (lhlwb)
+    double* hsw0 = nullptr;           // optional [nlay][ncol] SW clear-sky heating (lhsw0)
+    double* htswb = nullptr;          // optional [14][nlay][ncol] SW heating per band (lhswb)
 };
 
 }  // namespace orc

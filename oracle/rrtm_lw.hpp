@@ -36,6 +36,7 @@ struct LwColumn {
     std::vector<R> taug, fracs;   // [140][nlay]
     // rtrnmr outputs (internal order)
     std::vector<R> totuflux, totdflux, totuclfl, totdclfl, htr;
+    std::vector<R> fnetb;         // [16][nlay+1] net flux of each band, (up - down) x flxfac (lhlwb's fnet)
     std::vector<R> cldfmc;        // McICA route: [140][nlay]
 
     explicit LwColumn(int n) : nlay(n) {
@@ -54,6 +55,7 @@ struct LwColumn {
         taug.assign(140 * L, 0); fracs.assign(140 * L, 0);
         totuflux.assign(P, 0); totdflux.assign(P, 0); totuclfl.assign(P, 0); totdclfl.assign(P, 0);
         htr.assign(L, 0);
+        fnetb.assign(16 * P, 0);
     }
     R& CA(int m, int k0) { return colamt[(size_t)m * nlay + k0]; }     // colamt(k, m+1)
     R& WX(int m, int k0) { return wx[(size_t)m * nlay + k0]; }
@@ -1233,6 +1235,7 @@ void lw_rtrnmr(LwColumn<R>& c, const LwTables<R>& tb, R heatfac, R fluxfac)
         for (int k = 0; k <= nlay; ++k) {
             tuf[k] = tuf[k] + toturad[k]; tdf[k] = tdf[k] + totdrad[k];
             tuc[k] = tuc[k] + clrurad[k]; tdc[k] = tdc[k] + clrdrad[k];
+            c.fnetb[(size_t)ib * nlp1 + k] = (toturad[k] - totdrad[k]) * flxfac;   // the lhlwb block's fnet
         }
     }
     for (int k = 0; k <= nlay; ++k) {
@@ -1340,6 +1343,7 @@ void lw_rtrn(LwColumn<R>& c, const LwTables<R>& tb, R heatfac, R fluxfac)
         for (int m = 0; m <= nlay; ++m) {
             tuf[m] = tuf[m] + bu[m]; tdf[m] = tdf[m] + bd[m];
             tuc[m] = tuc[m] + cu[m]; tdc[m] = tdc[m] + cd[m];
+            c.fnetb[(size_t)ib * nlp1 + m] = (bu[m] - bd[m]) * flxfac;
         }
     }
     for (int m = 0; m <= nlay; ++m) {

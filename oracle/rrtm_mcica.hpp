@@ -202,6 +202,7 @@ void lw_rtrnmc(LwColumn<R>& c, const LwTables<R>& tb, R heatfac, R fluxfac)
         for (int k = 0; k <= nlay; ++k) {
             tuf[k] = tuf[k] + tur[k]; tdf[k] = tdf[k] + tdr[k];
             tuc[k] = tuc[k] + cur[k]; tdc[k] = tdc[k] + cdr[k];
+            c.fnetb[(size_t)ib * (nlay + 1) + k] = (tur[k] - tdr[k]) * flxfac;
         }
     }
     for (int k = 0; k <= nlay; ++k) {

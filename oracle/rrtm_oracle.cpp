@@ -67,6 +67,20 @@ static void run_lw(const Config& cfg, const Inputs& in, const Outputs& out)
         out.sfcflw[1 * (size_t)ncol + col] = (double)c.totuclfl[0];
         out.sfcflw[2 * (size_t)ncol + col] = (double)c.totdflux[0];
         out.sfcflw[3 * (size_t)ncol + col] = (double)c.totdclfl[0];
+        if (out.hlw0 || out.hlwb) {   // rtrnmr's lhlw0 / lhlwb blocks (phys_rrtm_lw_rtrnmr_body.cuh:328-362)
+            for (int k = 1; k <= nlay; ++k) {
+                const R rfdelp = heatfac / c.delp[k - 1];
+                const size_t lev = (size_t)(nlay - k);
+                if (out.hlw0) {
+                    const R f0 = c.totuclfl[k - 1] - c.totdclfl[k - 1], f1 = c.totuclfl[k] - c.totdclfl[k];
+                    out.hlw0[lev * ncol + col] = (double)((f0 - f1) * rfdelp);
+                }
+                if (out.hlwb)
+                    for (int ib = 0; ib < 16; ++ib)
+                        out.hlwb[((size_t)ib * nlay + lev) * ncol + col] =
+                            (double)((c.fnetb[(size_t)ib * nlp1 + k - 1] - c.fnetb[(size_t)ib * nlp1 + k]) * rfdelp);
+            }
+        }
         if (out.lwflx) {
             for (int k = 0; k <= nlay; ++k) {
                 const size_t lev = (size_t)(nlay - k);
@@ -124,6 +138,10 @@ static void run_sw(const Config& cfg, const Inputs& in, const Outputs& out)
         for (int i = 0; i < 6 * ncol; ++i) out.fdncmp[i] = 0;
     if (out.swflx)
         for (size_t i = 0; i < (size_t)4 * nlp1 * ncol; ++i) out.swflx[i] = 0;
+    if (out.hsw0)
+        for (size_t i = 0; i < (size_t)nlay * ncol; ++i) out.hsw0[i] = 0;
+    if (out.htswb)
+        for (size_t i = 0; i < (size_t)14 * nlay * ncol; ++i) out.htswb[i] = 0;
     if (cfg.route == 1 && out.sw_mask) {   // the SW generator runs over every column, as the reference's does
 #pragma omp parallel for schedule(dynamic, 64)
         for (int col = 0; col < ncol; ++col) {
@@ -178,6 +196,28 @@ static void run_sw(const Config& cfg, const Inputs& in, const Outputs& out)
             const R rf = heatfac / c.delp[k - 1];
             const R h = (fnet[k] - fnet[k - 1]) * rf;
             out.htsw[(size_t)(nlp1 - 1 - k) * ncol + col] = (double)h;
+        }
+        if (out.hsw0 || out.htswb) {   // swrad_post's lhsw0 / lhswb blocks (phys_rrtm_sw_swrad.cu:393-411)
+            std::vector<R> f(nlp1);
+            if (out.hsw0) {
+                for (int k = 0; k < nlp1; ++k) {
+                    R su0 = 0, sd0 = 0;
+                    for (int ib = 0; ib < 14; ++ib) {
+                        su0 = su0 + c.fxup0[(size_t)ib * nlp1 + k];
+                        sd0 = sd0 + c.fxdn0[(size_t)ib * nlp1 + k];
+                    }
+                    f[k] = sd0 - su0;
+                }
+                for (int k = 1; k < nlp1; ++k)
+                    out.hsw0[(size_t)(nlp1 - 1 - k) * ncol + col] = (double)((f[k] - f[k - 1]) * (heatfac / c.delp[k - 1]));
+            }
+            if (out.htswb)
+                for (int mb = 0; mb < 14; ++mb) {
+                    for (int k = 0; k < nlp1; ++k) f[k] = c.fxdnc[(size_t)mb * nlp1 + k] - c.fxupc[(size_t)mb * nlp1 + k];
+                    for (int k = 1; k < nlp1; ++k)
+                        out.htswb[((size_t)mb * nlay + (nlp1 - 1 - k)) * ncol + col] =
+                            (double)((f[k] - f[k - 1]) * (heatfac / c.delp[k - 1]));
+                }
         }
         out.topfsw[0 * (size_t)ncol + col] = (double)c.ftoauc;
         out.topfsw[1 * (size_t)ncol + col] = (double)c.ftoadc;
@@ -369,6 +409,52 @@ int orc_solve(int precision, const int* cfg_i, double cpathfac, int nlay, int nc
         orc::Inputs in{plyr, plvl, tlyr, tlvl, qlyr, olyr, gasvmr, clouds, faerlw, faersw, sfcemis, tsfg,
                        sfcalb, coszen, icseed, solcon, nlay, ncol};
         orc::Outputs out{htlw, htsw, topflw, sfcflw, topfsw, sfcfsw, fdncmp, lwflx, swflx, lw_mask, sw_mask};
+        if (precision == 0) {
+            orc::run_lw<float>(cfg, in, out);
+            orc::run_sw<float>(cfg, in, out);
+        } else {
+            orc::run_lw<double>(cfg, in, out);
+            orc::run_sw<double>(cfg, in, out);
+        }
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "oracle: %s\n", e.what());
+        return -1;
+    }
+    return 0;
+}
+
+// orc_solve with the optional outputs of lwrad / swrad (each may be null): hlw0 [nlay][ncol], hlwb
+// [16][nlay][ncol], hsw0 [nlay][ncol], htswb [14][nlay][ncol], K/s, levels top first.
+int orc_solve_diag(int precision, const int* cfg_i, double cpathfac, int nlay, int ncol, const float* plyr,
+                   const float* plvl, const float* tlyr, const float* tlvl, const float* qlyr, const float* olyr,
+                   const float* gasvmr, const float* clouds, const float* faerlw, const float* faersw,
+                   const float* sfcemis, const float* tsfg, const float* sfcalb, const float* coszen,
+                   const int* icseed, double solcon, double* htlw, double* htsw, double* topflw, double* sfcflw,
+                   double* topfsw, double* sfcfsw, double* fdncmp, double* lwflx, double* swflx,
+                   unsigned int* lw_mask, unsigned int* sw_mask, double* hlw0, double* hlwb, double* hsw0,
+                   double* htswb, int nthreads)
+{
+    try {
+#ifdef _OPENMP
+        if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+        (void)nthreads;
+#endif
+        orc::Config cfg;
+        cfg.iswmode = cfg_i[0];
+        cfg.diagnostic = cfg_i[1];
+        cfg.window_cols = cfg_i[2];
+        cfg.sw_chunk = cfg_i[3] > 0 ? cfg_i[3] : 32768;
+        cfg.route = cfg_i[4];
+        cfg.iovrlw = cfg_i[5];
+        cfg.iovrsw = cfg_i[6];
+        cfg.lw_seed0 = cfg_i[7];
+        cfg.sw_seed0 = cfg_i[8];
+        cfg.cpathfac = cpathfac;
+        orc::Inputs in{plyr, plvl, tlyr, tlvl, qlyr, olyr, gasvmr, clouds, faerlw, faersw, sfcemis, tsfg,
+                       sfcalb, coszen, icseed, solcon, nlay, ncol};
+        orc::Outputs out{htlw, htsw, topflw, sfcflw, topfsw, sfcfsw, fdncmp, lwflx, swflx, lw_mask, sw_mask,
+                         hlw0, hlwb, hsw0, htswb};
         if (precision == 0) {
             orc::run_lw<float>(cfg, in, out);
             orc::run_sw<float>(cfg, in, out);

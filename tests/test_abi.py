@@ -59,7 +59,7 @@ def test_struct_layout_matches_header(tmp_path):
 
 
 def test_version_and_defaults(lib):
-    assert lib.rad_version() == 1
+    assert lib.rad_version() == 2
     c = _lib.RadConfig()
     lib.rad_config_default(ctypes.byref(c), 61)
     assert (c.nlay, c.precision, c.route, c.iswmode, c.diagnostic) == (61, _lib.PREC["mixed"], 0, 2, 0)

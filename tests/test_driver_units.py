@@ -63,13 +63,40 @@ def test_missing_input_named_with_producer():
         driver.swrad_run(ctx)
 
 
-def test_unsupported_sw_outputs_refused():
-    ctx = SimpleNamespace(st=State(), grid=SimpleNamespace(jm=JM, im=IM, lm=60), tables={},
-                          cfg=SimpleNamespace(lhsw0=True), stream=None)
-    with pytest.raises(NotImplementedError):
-        driver.swrad_run(ctx)
-    with pytest.raises(NotImplementedError):
-        driver.swrad_run(SimpleNamespace(st=State(), grid=None, tables={}, cfg=None, stream=None), has_htrswb=True)
+@pytest.mark.gpu
+def test_units_write_optional_outputs():
+    """swrad with has_htrswb, lhsw0, lflxprf and lwrad with lhlw0, lhlwb, lflxprf write HTSWB / HSW0 / FLXPRF
+    and htlwb / htlw0 / flwprf by the reference's names, equal to the solver's optional outputs."""
+    import torch
+    from woof_nam_b200.solver import RadSolver
+    cols = make_columns(JM * IM, 79)
+    flags = dict(lhsw0=True, lhswb=True, lhlw0=True, lhlwb=True, lflxprf=True)
+    ctx = _ctx(cols)
+    ctx.cfg.lhsw0 = ctx.cfg.lflxprf = ctx.cfg.lhlw0 = ctx.cfg.lhlwb = True
+    o = driver.swrad_run(ctx, has_htrswb=True)
+    torch.cuda.synchronize()
+    r = RadSolver(precision="mixed", parts="sw", **flags).solve_host(cols)
+    for name, key in (("HTSWB", "htswb"), ("HSW0", "hsw0"), ("FLXPRF", "swflxprf")):
+        got = o[name].cpu().numpy()
+        assert np.array_equal(got.reshape(r[key].shape), r[key]), name
+        assert ctx.st.fields[name] is o[name]
+    ctx = _ctx(cols, cloud_scale=np.float32(1.5))
+    ctx.cfg.lhlw0 = ctx.cfg.lhlwb = ctx.cfg.lflxprf = True
+    o = driver.lwrad_run(ctx)
+    torch.cuda.synchronize()
+    r = RadSolver(precision="mixed", parts="lw", cpathfac=1.0, **flags).solve_host(_scaled(cols))
+    for name, key, out in (("htlw0", "hlw0", "hlw0"), ("htlwb", "hlwb", "hlwb"), ("flwprf", "lwflxprf", "flxprf")):
+        assert np.array_equal(o[out].cpu().numpy().reshape(r[key].shape), r[key]), name
+        assert ctx.st.fields[name] is o[out]
+
+
+def _scaled(cols):
+    """The request with grrad-lw's cloud-path factor applied to the liquid and ice paths."""
+    from woof_nam_b200.columns import Columns
+    kw = {f: np.array(getattr(cols, f)) for f in Columns.FIELDS}
+    kw["clouds"][1] *= np.float32(1.5)
+    kw["clouds"][3] *= np.float32(1.5)
+    return Columns(**kw, solcon=cols.solcon, diagnostic_clouds=cols.diagnostic_clouds)
 
 
 @pytest.mark.gpu

@@ -43,7 +43,9 @@ class RadColumns(ctypes.Structure):
 class RadOutputs(ctypes.Structure):
     _fields_ = [("htlw", ctypes.c_void_p), ("htsw", ctypes.c_void_p), ("topflw", ctypes.c_void_p),
                 ("sfcflw", ctypes.c_void_p), ("topfsw", ctypes.c_void_p), ("sfcfsw", ctypes.c_void_p),
-                ("fdncmp", ctypes.c_void_p), ("lw_mask", ctypes.c_void_p), ("sw_mask", ctypes.c_void_p)]
+                ("fdncmp", ctypes.c_void_p), ("lw_mask", ctypes.c_void_p), ("sw_mask", ctypes.c_void_p),
+                ("hsw0", ctypes.c_void_p), ("htswb", ctypes.c_void_p), ("swflxprf", ctypes.c_void_p),
+                ("hlw0", ctypes.c_void_p), ("hlwb", ctypes.c_void_p), ("lwflxprf", ctypes.c_void_p)]
 
 
 class RadProfile(ctypes.Structure):

@@ -65,6 +65,9 @@ struct RadHandle {
     int64_t lw3_cap = 0;                           // columns d_lw3 holds
     int* d_lw3list = nullptr;                      // [1 + lw3_cap]: count, then the chunk's float64 columns
     float* d_swrt = nullptr;                       // SW layer R/T stores, sw2_rt_floats() per CTA of the SW grid
+    float* d_lwpg = nullptr;                       // optional LW outputs: g-point profiles of one chunk (DIAG sweeps)
+    float* d_swpg = nullptr;                       // optional SW outputs: g-point level fluxes of one chunk
+    int64_t lwpg_cap = 0, swpg_cap = 0;            // columns they hold
     int4* d_sw4img = nullptr;                      // chunked SW: set-up and gas-optics images of one chunk's columns
     unsigned char* d_sw4 = nullptr;                // chunked SW: header and layer R/T of one chunk's columns
     int64_t sw4_cap = 0;                           // columns d_sw4 and d_sw4img hold
@@ -252,6 +255,38 @@ int ensure_scratch(RadHandle* h, int64_t n)
     return RAD_OK;
 }
 
+// Columns per LW chunk when the optional LW outputs are wanted (their g-point profiles: 278 KB per column).
+constexpr int64_t LW_DIAG_CHUNK = 8192;
+int64_t sw4_chunk(const RadConfig& cfg);
+int64_t lw3_chunk(const RadConfig& cfg);
+
+// The g-point profile buffers of the optional outputs (allocated on the first solve that asks for them).
+int ensure_diag_scratch(RadHandle* h, int64_t ntot, bool lw, bool sw)
+{
+    const int nlay = h->cfg.nlay;
+    if (lw) {
+        const int64_t need = std::min(std::min(lw3_chunk(h->cfg), LW_DIAG_CHUNK), ntot);
+        if (need > h->lwpg_cap) {
+            if (h->d_lwpg) cudaFree(h->d_lwpg);
+            h->d_lwpg = nullptr;
+            h->lwpg_cap = 0;
+            RAD_CUDA(h, cudaMalloc((void**)&h->d_lwpg, (size_t)need * lw3_pg_floats(nlay) * sizeof(float)));
+            h->lwpg_cap = need;
+        }
+    }
+    if (sw) {
+        const int64_t need = std::min(sw4_chunk(h->cfg), ntot);
+        if (need > h->swpg_cap) {
+            if (h->d_swpg) cudaFree(h->d_swpg);
+            h->d_swpg = nullptr;
+            h->swpg_cap = 0;
+            RAD_CUDA(h, cudaMalloc((void**)&h->d_swpg, (size_t)need * sw4_pg_floats(nlay) * sizeof(float)));
+            h->swpg_cap = need;
+        }
+    }
+    return RAD_OK;
+}
+
 // McICA: LW and SW sub-column words of every column of request r, into the caller's mask outputs when
 // given, else into the handle's scratch at the request's column offset (scratch holds the launch's columns).
 // Seeds: icseed [2][ncol] (LW row, SW row) or seed0 + column + 1.
@@ -422,6 +457,25 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
             if (ncols[r] > 0 && (rc = mcica_masks(h, ins + r, outs + r, ncols[r], db.off[r], st, &lwm[r], &swm[r])))
                 return rc;
     const bool do_lw = cfg.parts & RAD_PART_LW, do_sw = cfg.parts & RAD_PART_SW;
+    // lwrad's / swrad's optional outputs: profiles of every g-point from the chunked sweeps, then per chunk a
+    // reduction into the requested fields
+    DiagOuts dout{};
+    bool diag_lw = false, diag_sw = false;
+    for (int r = 0; r < nreq; ++r) {
+        const RadOutputs* o = outs + r;
+        dout.p[r][0] = o->hlw0; dout.p[r][1] = o->hlwb; dout.p[r][2] = o->lwflxprf;
+        dout.p[r][3] = o->hsw0; dout.p[r][4] = o->htswb; dout.p[r][5] = o->swflxprf;
+        diag_lw = diag_lw || (do_lw && (o->hlw0 || o->hlwb || o->lwflxprf));
+        diag_sw = diag_sw || (do_sw && (o->hsw0 || o->htswb || o->swflxprf));
+    }
+    if ((diag_lw && (fixed || sizeof(R) != 4 || lw3_chunk(cfg) <= 0)) ||
+        (diag_sw && (fixed || sizeof(R) != 4 || sw4_chunk(cfg) <= 0)))
+        return fail(h, RAD_E_INVALID, "optional outputs (hlw0, hlwb, lwflxprf, hsw0, htswb, swflxprf) are produced by "
+                                      "rad_solve's mixed precision with the chunked LW and SW (lw_chunk >= 0, "
+                                      "sw_sweep_chunk >= 0)");
+    if (diag_lw || diag_sw) {
+        if ((rc = ensure_diag_scratch(h, ntot, diag_lw, diag_sw))) return rc;
+    }
     // ---- LW over every column
     if (do_lw) {
         LwBatch bt{};
@@ -449,21 +503,31 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
             const size_t smem1 = sizeof(LwSetup<float>), smemd = sizeof(LwShared<double>);
             RAD_CUDA(h, cudaFuncSetAttribute((void*)lw3_optics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
             RAD_CUDA(h, cudaFuncSetAttribute((void*)lw3_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemd));
-            for (int64_t c0 = 0; c0 < ntot; c0 += lwc) {
-                const int64_t nc = std::min(lwc, ntot - c0);
+            const int64_t lstep = diag_lw ? std::min(lwc, (int64_t)LW_DIAG_CHUNK) : lwc;
+            for (int64_t c0 = 0; c0 < ntot; c0 += lstep) {
+                const int64_t nc = std::min(lstep, ntot - c0);
                 RAD_CUDA(h, cudaMemsetAsync(h->d_lw3list, 0, sizeof(int), st));
                 lw3_optics_kernel<<<(unsigned)nc, LW3_OPT_THREADS, smem1, st>>>(bt, c0, h->d_lw3, h->d_lw3list, h->d_err);
                 const unsigned g2 = (unsigned)((nc + LW3_SWEEP_WARPS - 1) / LW3_SWEEP_WARPS);
+                float* pg = h->d_lwpg;
                 if (mc) {
-                    lw3_sweep_kernel<LW_OVR_MCICA><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                    if (diag_lw) lw3_sweep_kernel<LW_OVR_MCICA, true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, pg);
+                    else lw3_sweep_kernel<LW_OVR_MCICA><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
                     h->launches += 2;
                 } else {
-                    if (cfg.iovrlw == 0)
-                        lw3_sweep_kernel<LW_OVR_RANDOM><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
-                    else
-                        lw3_sweep_kernel<LW_OVR_MAXRAN><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                    if (cfg.iovrlw == 0) {
+                        if (diag_lw) lw3_sweep_kernel<LW_OVR_RANDOM, true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, pg);
+                        else lw3_sweep_kernel<LW_OVR_RANDOM><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                    } else {
+                        if (diag_lw) lw3_sweep_kernel<LW_OVR_MAXRAN, true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, pg);
+                        else lw3_sweep_kernel<LW_OVR_MAXRAN><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                    }
                     lw3_fp64_kernel<<<(unsigned)h->nsm, LW_THREADS, smemd, st>>>(bt, c0, h->d_lw3list, dl, h->d_err);
                     h->launches += 3;
+                }
+                if (diag_lw) {
+                    k_lw_diag<<<(unsigned)((nc + 3) / 4), 128, 0, st>>>(bt, c0, nc, pg, dout);
+                    h->launches += 1;
                 }
             }
             RAD_CUDA(h, cudaGetLastError());
@@ -517,6 +581,9 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
         RAD_CUDA(h, cudaMemsetAsync(out->topfsw, 0, (size_t)3 * n * sizeof(float), st));
         RAD_CUDA(h, cudaMemsetAsync(out->sfcfsw, 0, (size_t)4 * n * sizeof(float), st));
         if (out->fdncmp) RAD_CUDA(h, cudaMemsetAsync(out->fdncmp, 0, (size_t)6 * n * sizeof(float), st));
+        if (out->hsw0) RAD_CUDA(h, cudaMemsetAsync(out->hsw0, 0, (size_t)nlay * n * sizeof(float), st));
+        if (out->htswb) RAD_CUDA(h, cudaMemsetAsync(out->htswb, 0, (size_t)14 * nlay * n * sizeof(float), st));
+        if (out->swflxprf) RAD_CUDA(h, cudaMemsetAsync(out->swflxprf, 0, (size_t)4 * (nlay + 1) * n * sizeof(float), st));
     }
     {
         SwBatch bt{};
@@ -549,15 +616,23 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                 const size_t bb = sw4_block_bytes(nlay);
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw4_gas_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw4_rt_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
-                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw4_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw4_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+                RAD_CUDA(h, cudaFuncSetAttribute((void*)sw4_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
                 for (int64_t d0 = 0; d0 < ntot; d0 += swc) {
                     const int64_t nc = std::min(swc, ntot - d0);
                     sw4_gas_kernel<<<(unsigned)nc, SW2_THREADS, smem0, st>>>(bt, any_aer ? 1 : 0, h->d_err, (int)d0, h->d_sw4img);
                     sw4_rt_kernel<<<(unsigned)nc, SW2_THREADS, smem1, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, (int)d0,
                                                                          h->d_sw4img, h->d_sw4, bb);
-                    sw4_sweep_kernel<<<(unsigned)nc, SW2_THREADS, smem2, st>>>(bt, h->d_err, (int)d0, (int)nc, h->d_sw4, bb);
+                    if (diag_sw) {
+                        sw4_sweep_kernel<true><<<(unsigned)nc, SW2_THREADS, smem2, st>>>(bt, h->d_err, (int)d0, (int)nc,
+                                                                                        h->d_sw4, bb, h->d_swpg);
+                        k_sw_diag<<<(unsigned)((nc + 3) / 4), 128, 0, st>>>(bt, (int)d0, (int)nc, h->d_sw4, bb, h->d_swpg, dout);
+                    } else {
+                        sw4_sweep_kernel<false><<<(unsigned)nc, SW2_THREADS, smem2, st>>>(bt, h->d_err, (int)d0, (int)nc,
+                                                                                         h->d_sw4, bb);
+                    }
                 }
-                nlaunch = 3 * ((ntot + swc - 1) / swc);
+                nlaunch = (diag_sw ? 4 : 3) * ((ntot + swc - 1) / swc);
             } else {       // SW2_CTAS_PER_SM CTAs per SM walk the day list, each with its R/T store
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw2_column_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
                 sw2_column_kernel<true><<<(unsigned)(SW2_CTAS_PER_SM * h->nsm), SW2_THREADS, smem, st>>>(
@@ -1112,7 +1187,7 @@ void rad_destroy(RadHandle* h)
     for (void* p : {(void*)h->d_lwf, (void*)h->d_swf, (void*)h->d_lwd, (void*)h->d_swd,
                     (void*)h->d_err, (void*)h->d_flag, (void*)h->d_pos, (void*)h->d_daycol, (void*)h->d_lt,
                     (void*)h->d_k8, (void*)h->d_kw, (void*)h->d_cmin, (void*)h->d_nday, h->d_cub, (void*)h->d_lwm,
-                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt, (void*)h->d_sw4, (void*)h->d_sw4img, (void*)h->d_aerf,
+                    (void*)h->d_swm, (void*)h->d_lw3, (void*)h->d_lw3list, (void*)h->d_swrt, (void*)h->d_sw4, (void*)h->d_sw4img, (void*)h->d_lwpg, (void*)h->d_swpg, (void*)h->d_aerf,
                     (void*)h->d_aeri})
         if (p) cudaFree(p);
     delete h;

@@ -250,10 +250,17 @@ __device__ __forceinline__ void lw3_stage_layer(float* st, const float* tg, cons
     asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-template <int OVR>
+// Per-g-point profiles of one column for lwrad's optional outputs (DIAG sweeps): [nlay + 1][LW3_PGQ][LW_NGPT]
+// floats: at level L (surface first) the upward and downward radiance, total sky then clear sky (q 0..3); at
+// layer L (1..nlay) the radiance changes across it formed directly, upward pass U(L) - U(L-1) and downward
+// pass D(L-1) - D(L), total sky then clear sky (q 4..7).
+constexpr int LW3_PGQ = 8;
+__host__ __device__ constexpr int64_t lw3_pg_floats(int nlay) { return (int64_t)(nlay + 1) * LW3_PGQ * LW_NGPT; }
+
+template <int OVR, bool DIAG = false>
 __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
                                                                          int64_t nc, const float* __restrict__ scr,
-                                                                         LwLut<float> lut)
+                                                                         LwLut<float> lut, float* __restrict__ pg = nullptr)
 {
     __shared__ double fup[LW3_SWEEP_WARPS][NLAY_MAX + 1], fdn[LW3_SWEEP_WARPS][NLAY_MAX + 1];
     __shared__ __align__(16) float ring[LW3_SWEEP_WARPS][LW3_NSTAGE][LW3_STAGE];
@@ -271,6 +278,7 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
     const float* tg = blk;
     const float* fr = blk + (size_t)nlay * LW3_GSTRIDE;
     const float* aux = blk + (size_t)2 * nlay * LW3_GSTRIDE;
+    if (DIAG) pg += lc * lw3_pg_floats(nlay);
     // sweep steps: s = 0 .. nlay-1 downward (layer nlay - s), s = nlay .. 2 nlay - 1 upward (layer s - nlay + 1)
     const int nstep = 2 * nlay;
     auto layer_of = [&](int st) { return st < nlay ? nlay - st : st - nlay + 1; };
@@ -312,9 +320,21 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
             const float tcb = r[R_TAUCLD + b];
             const LwTerms<float> t = lw3_terms<float>(lut, tgr[g], frr[g], r[R_PKLAY + b], r[R_PKLEVU + b],
                                                       r[R_PKLEVD + b], tcb, sdif[j], cl);
+            const float pclr = radclr[j];
             const float inc = lw3_step<float, OVR>(radtot[j], radclr[j], trad[j], crad[j], rad[j], t, down, cl, lst,
                                                   clfr, f, sdif[j] * tcb);
             if (val[j]) sum += (double)inc;
+            if (DIAG && val[j]) {
+                // the clear-sky change across the layer, formed directly like inc; the radiances at the level
+                // the step ends on (k - 1 going down, k going up)
+                const float incc = (down ? t.gassrcd : t.gassrcu) - pclr * t.atrg;
+                float* p = pg + (size_t)k * LW3_PGQ * LW_NGPT + g;
+                p[(down ? 5 : 4) * LW_NGPT] = inc;
+                p[(down ? 7 : 6) * LW_NGPT] = incc;
+                float* q = pg + (size_t)(down ? k - 1 : k) * LW3_PGQ * LW_NGPT + g;
+                q[(down ? 1 : 0) * LW_NGPT] = radtot[j];
+                q[(down ? 3 : 2) * LW_NGPT] = radclr[j];
+            }
         }
         return warp_sum(sum);
     };
@@ -340,6 +360,12 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
                 const float rtd = radtot[j], rcd = radclr[j];
                 radtot[j] = rad0 + reflct * rtd;
                 radclr[j] = rad0 + reflct * rcd;
+                if (DIAG && val[j]) {   // the upward radiances leaving the surface; nothing comes down at the top
+                    pg[(size_t)0 * LW_NGPT + gi[j]] = radtot[j];
+                    pg[(size_t)2 * LW_NGPT + gi[j]] = radclr[j];
+                    pg[((size_t)nlay * LW3_PGQ + 1) * LW_NGPT + gi[j]] = 0.0f;
+                    pg[((size_t)nlay * LW3_PGQ + 3) * LW_NGPT + gi[j]] = 0.0f;
+                }
                 if (val[j]) {
                     s_tu += (double)radtot[j]; s_cu += (double)radclr[j];
                     s_td += (double)rtd; s_cd += (double)rcd;
@@ -383,6 +409,53 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
         a.sfcflw[2 * N + col] = (float)(s_td * flxfac);
         a.sfcflw[3 * N + col] = (float)(s_cd * flxfac);
     }
+}
+
+// lwrad's optional outputs of a chunk from the DIAG sweeps' profiles: one warp per column, lane q < 16 band q
+// (hlwb: htrb of rtrnmr's lhlwb block, from the band's per-layer changes), lane 16 the totals (lwflxprf, the
+// level fluxes; hlw0 from the clear-sky per-layer changes).  Sums over g-points in float64 in g order, times
+// flxfac; heating as the sweeps form htlw: -(dU + dD) flxfac heatfac / delp.
+// Optional-output pointers of a launch's requests: hlw0, hlwb, lwflxprf, hsw0, htswb, swflxprf (null = not wanted).
+struct DiagOuts {
+    float* p[RAD_MAXREQ][6];
+};
+__global__ void __launch_bounds__(128) k_lw_diag(const __grid_constant__ LwBatch bt, int64_t c0, int64_t nc,
+                                                 const float* __restrict__ pg, const __grid_constant__ DiagOuts outs)
+{
+    const int64_t lc = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
+    const int q = threadIdx.x & 31;
+    if (lc >= nc || q > 16) return;
+    const int64_t gc = c0 + lc;
+    const int rq = bt.find(gc);
+    const LwIn& a = bt.req[rq];
+    const int nlay = a.nlay;
+    const int64_t col = gc - bt.off[rq], N = a.ncol;
+    if (nlay > NLAY_MAX || col >= N) return;
+    float* hlw0 = outs.p[rq][0];
+    float* hlwb = outs.p[rq][1];
+    float* flx = outs.p[rq][2];
+    const float* p = pg + lc * lw3_pg_floats(nlay);
+    const double flxfac = 0.5 * 3.14159265358979323846 * 2.0e4;
+    const double heatfac = 9.80665 * 1.0e-2 / 1.0046e3;
+    const int g0 = q < 16 ? c_lw_ns[q] : 0, g1 = q < 16 ? c_lw_ns[q + 1] : LW_NGPT;
+    auto S = [&](int L, int f) {
+        double v = 0.0;
+        for (int g = g0; g < g1; ++g) v += (double)p[((size_t)L * LW3_PGQ + f) * LW_NGPT + g];
+        return v;
+    };
+    for (int k = 1; k <= nlay; ++k) {
+        const int kin = nlay - k;   // top-first index of layer k
+        const double dl = (double)__ldg(a.plvl + (size_t)(kin + 1) * N + col) - (double)__ldg(a.plvl + (size_t)kin * N + col);
+        const double rf = flxfac * (heatfac / dl);
+        if (q < 16) {
+            if (hlwb) hlwb[((size_t)q * nlay + kin) * N + col] = (float)(-(S(k, 4) + S(k, 5)) * rf);
+        } else if (hlw0) {
+            hlw0[(size_t)kin * N + col] = (float)(-(S(k, 6) + S(k, 7)) * rf);
+        }
+    }
+    if (q == 16 && flx)
+        for (int L = 0; L <= nlay; ++L)
+            for (int f = 0; f < 4; ++f) flx[((size_t)f * (nlay + 1) + (nlay - L)) * N + col] = (float)(S(L, f) * flxfac);
 }
 
 }  // namespace rad

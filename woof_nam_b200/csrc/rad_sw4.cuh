@@ -399,11 +399,33 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
     for (int j = tid; j < nq; j += SW2_THREADS) full(qe[j]);
 }
 
+// Per-g-point level fluxes of one sunlit column for swrad's optional outputs (DIAG sweeps):
+// [nlay + 1][SW4_PGQ][SW_NGPT] floats at level L (surface first), each x zsolar: up total, down total, up clear,
+// down clear, net (down - up) total, net clear.
+constexpr int SW4_PGQ = 6;
+__host__ __device__ constexpr int64_t sw4_pg_floats(int nlay) { return (int64_t)(nlay + 1) * SW4_PGQ * SW_NGPT; }
+
+// One level of the DIAG profile of g-point g (see sw4_pg_floats): clear fluxes fu / fd, cloudy-pass fuo / fdo,
+// pass weights w0 / w1 and the sweep's net total.
+__device__ __forceinline__ void sw4_pg_level(float* pg, int L, int g, float zsolar, bool cloudy, double w0, double w1,
+                                             float fu, float fd, float fuo, float fdo, double net)
+{
+    const double zs = (double)zsolar;
+    float* p = pg + (size_t)L * SW4_PGQ * SW_NGPT + g;
+    p[0] = (float)(zs * (cloudy ? w0 * fu + w1 * fuo : (double)fu));
+    p[SW_NGPT] = (float)(zs * (cloudy ? w0 * fd + w1 * fdo : (double)fd));
+    p[2 * SW_NGPT] = (float)(zs * fu);
+    p[3 * SW_NGPT] = (float)(zs * fd);
+    p[4 * SW_NGPT] = (float)(zs * net);
+    p[5 * SW_NGPT] = (float)(zs * ((double)fd - (double)fu));
+}
+
 // The adding method of one sunlit column from its block (sw2_column phase C with the R/T read instead of
 // formed; the same operations in the same order).
+template <bool DIAG = false>
 __global__ void __launch_bounds__(SW2_THREADS, SW4_SWEEP_MINB)
 sw4_sweep_kernel(const __grid_constant__ SwBatch bt, int* err, int d0, int nc, const unsigned char* scr,
-                 size_t blk_bytes)
+                 size_t blk_bytes, float* __restrict__ pg = nullptr)
 {
     extern __shared__ __align__(16) float ckpt[];                  // [(nseg - 1) x 4][SW2_THREADS]
     __shared__ __align__(16) Sw4Hdr H;
@@ -429,6 +451,7 @@ sw4_sweep_kernel(const __grid_constant__ SwBatch bt, int* err, int d0, int nc, c
     __syncthreads();
     const float* rtc = reinterpret_cast<const float*>(blk + sw4_hdr_bytes());
     const float* rto = rtc + (size_t)nlay * SW4_LAYER;
+    if (DIAG) pg += (int64_t)i * sw4_pg_floats(nlay);
     const int warp = tid >> 5, lane = tid & 31;
     bool act;
     const int g = sw2_lane_g(tid, act);
@@ -505,18 +528,18 @@ sw4_sweep_kernel(const __grid_constant__ SwBatch bt, int* err, int d0, int nc, c
         for (int j = SW2_SEG - 1; j >= 0; --j) {
             const int lev = sg * SW2_SEG + j + 2;        // level above layer j (1 = surface)
             if (lev <= nlp1) {
-                float fu, fd;
+                float fu, fd, fuo = 0, fdo = 0;
                 sw2_flux(zubc[j + 1], zudc[j + 1], tdnc, rdnc, tdbc, fu, fd);
                 double net = w0 * ((double)fd - (double)fu);
                 if (lev == nlp1) toa_c = fu;
                 if (cloudy) {
-                    float fuo, fdo;
                     sw2_flux(zubo[j + 1], zudo[j + 1], tdno, rdno, tdbo, fuo, fdo);
                     net += w1 * ((double)fdo - (double)fuo);
                     if (lev == nlp1) toa_o = fuo;
                 }
                 const double v = warp_sum(act ? (double)zsolar * net : 0.0);
                 if (lane == 0) fn[warp][lev - 1] = v;
+                if (DIAG && act) sw4_pg_level(pg, lev - 1, g, zsolar, cloudy, w0, w1, fu, fd, fuo, fdo, net);
             }
             sw2_down(Lc[j], tdnc, rdnc, tdbc);
             if (cloudy) sw2_down(Lo[j], tdno, rdno, tdbo);
@@ -538,6 +561,7 @@ sw4_sweep_kernel(const __grid_constant__ SwBatch bt, int* err, int d0, int nc, c
         }
         const double v = warp_sum(act ? (double)zsolar * net : 0.0);
         if (lane == 0) fn[warp][0] = v;
+        if (DIAG && act) sw4_pg_level(pg, 0, g, zsolar, cloudy, w0, w1, fu, fd, fuo, fdo, net);
         if (act) {
             const double zs = (double)zsolar;
             // slots: 0 toa up, 1 sfc up, 2 sfc dn, 3 uv-b, 4 nir beam, 5 nir diffuse, 6 vis beam, 7 vis diffuse, 8 toa down
@@ -591,6 +615,59 @@ sw4_sweep_kernel(const __grid_constant__ SwBatch bt, int* err, int d0, int nc, c
         }
     }
     (void)err;
+}
+
+// swrad's optional outputs of a chunk from the DIAG sweeps' profiles (swrad_post's lhsw0 / lhswb / lflxprf
+// blocks): one warp per sunlit column, lane q < 14 band q (htswb from the band's net fluxes), lane 14 the totals
+// (swflxprf, hsw0 from the clear net fluxes).  Sums over g-points in float64 in g order; heating
+// (F(k + 1) - F(k)) heatfac / delp as the sweeps form htsw.
+__global__ void __launch_bounds__(128) k_sw_diag(const __grid_constant__ SwBatch bt, int d0, int nc,
+                                                 const unsigned char* scr, size_t blk_bytes,
+                                                 const float* __restrict__ pg, const __grid_constant__ DiagOuts outs)
+{
+    const int i = (int)blockIdx.x * 4 + (threadIdx.x >> 5);
+    const int q = threadIdx.x & 31;
+    const int d = d0 + i;
+    if (i >= nc || q > 14 || d >= *bt.req[0].nday) return;
+    const int64_t gcol = bt.req[0].daycol[d];
+    const int rq = bt.find(gcol);
+    const SwIn& a = bt.req[rq];
+    const int nlay = a.nlay, nlp1 = nlay + 1;
+    if (nlay > NLAY_MAX) return;
+    const int64_t col = gcol - bt.off[rq], N = a.ncol;
+    const Sw4Hdr& H = *reinterpret_cast<const Sw4Hdr*>(scr + (size_t)i * blk_bytes);
+    const float* p = pg + (int64_t)i * sw4_pg_floats(nlay);
+    float* hsw0 = outs.p[rq][3];
+    float* htswb = outs.p[rq][4];
+    float* flx = outs.p[rq][5];
+    const int g0 = q < 14 ? c_sw_ns[q] : 0, g1 = q < 14 ? c_sw_ns[q + 1] : SW_NGPT;
+    auto S = [&](int L, int f) {
+        double v = 0.0;
+        for (int g = g0; g < g1; ++g) v += (double)p[((size_t)L * SW4_PGQ + f) * SW_NGPT + g];
+        return v;
+    };
+    if (q < 14) {
+        if (htswb) {
+            double f0 = S(0, 4);
+            for (int k0 = 0; k0 < nlay; ++k0) {
+                const double f1 = S(k0 + 1, 4);
+                htswb[((size_t)q * nlay + (nlay - 1 - k0)) * N + col] = (float)((f1 - f0) * H.rdelp[k0]);
+                f0 = f1;
+            }
+        }
+        return;
+    }
+    if (hsw0) {
+        double f0 = S(0, 5);
+        for (int k0 = 0; k0 < nlay; ++k0) {
+            const double f1 = S(k0 + 1, 5);
+            hsw0[(size_t)(nlay - 1 - k0) * N + col] = (float)((f1 - f0) * H.rdelp[k0]);
+            f0 = f1;
+        }
+    }
+    if (flx)
+        for (int L = 0; L < nlp1; ++L)
+            for (int f = 0; f < 4; ++f) flx[((size_t)f * nlp1 + (nlp1 - 1 - L)) * N + col] = (float)S(L, f);
 }
 
 }  // namespace rad

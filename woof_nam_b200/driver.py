@@ -156,10 +156,20 @@ def lwrad_run(ctx) -> dict:
     s = _solver(ctx, "lw", 1.0, nlay)
     stream = _stream(ctx)
     torch = _torch()
+    cfg = getattr(ctx, "cfg", None)
+    opt = {"hlw0": ("htlw0", (nlay, jm, im)) if getattr(cfg, "lhlw0", False) else None,
+           "hlwb": ("htlwb", (16, nlay, jm, im)) if getattr(cfg, "lhlwb", False) else None,
+           "lwflxprf": ("flwprf", (4, nlay + 1, jm, im)) if getattr(cfg, "lflxprf", False) else None}
     with torch.cuda.stream(stream):
         hl = _as_tensor(_add(st, "htlwc", (nlay, jm, im)), "htlwc", unit)
         out = s.alloc_outputs(jm * im)
         out["htlw"] = hl.reshape(nlay, jm * im)     # solved in place into the state's htlwc
+        ret = {}
+        for k, spec in opt.items():
+            if spec is not None:
+                name, shape = spec
+                ret[k] = _as_tensor(_add(st, name, shape), name, unit)
+                out[k] = ret[k].reshape(shape[0], -1) if len(shape) == 3 else ret[k].reshape(shape[0], shape[1], -1)
         s.solve(cols, _solcon(ctx), out, stream=stream)
         o = {}
         for i, n in enumerate(LW_FLUXES):
@@ -168,7 +178,7 @@ def lwrad_run(ctx) -> dict:
             dst.view(-1).copy_(src)
             o[n] = dst
     o["hlwc"] = hl
-    o["hlw0"] = o["hlwb"] = o["flxprf"] = None
+    o["hlw0"], o["hlwb"], o["flxprf"] = ret.get("hlw0"), ret.get("hlwb"), ret.get("lwflxprf")
     return o
 
 
@@ -177,13 +187,11 @@ def swrad_run(ctx, has_htrswb: bool = False, nc: int = 0) -> dict:
     the sunlit columns (SW_COSZEN >= 1e-4, the grrad-sw day predicate), zeros elsewhere.  Writes HTSWC
     [LMK, JM, IM], TOPFLX [3, JM, IM], SFCFLX [4, JM, IM] and, with ctx.cfg.lfdncmp, FDNCMP [6, JM, IM].
     The day list is built on the device inside the solve; nc (the reference's chunk size) has no effect
-    on the result and is accepted for the signature.  Spectral band heating (has_htrswb), clear-sky
-    heating (lhsw0) and flux profiles (lflxprf) are not produced: asking for them raises."""
+    on the result and is accepted for the signature.  With has_htrswb, ctx.cfg.lhsw0 and ctx.cfg.lflxprf
+    it also writes HTSWB [14, LMK, JM, IM], HSW0 [LMK, JM, IM] and FLXPRF [4, LMK+1, JM, IM]."""
     unit = "phys-rrtm-sw-swrad"
     del nc
     cfg = getattr(ctx, "cfg", None)
-    if has_htrswb or getattr(cfg, "lhsw0", False) or getattr(cfg, "lflxprf", False):
-        raise NotImplementedError(f"{unit}: HTSWB / HSW0 / FLXPRF outputs are not produced by this library")
     st = ctx.st
     g = ctx.grid
     jm, im, nlay = int(g.jm), int(g.im), int(g.lm) + 1
@@ -204,6 +212,15 @@ def swrad_run(ctx, has_htrswb: bool = False, nc: int = 0) -> dict:
         if getattr(cfg, "lfdncmp", False):
             o["FDNCMP"] = _as_tensor(_add(st, "FDNCMP", (6, jm, im)), "FDNCMP", unit)
             out["fdncmp"] = o["FDNCMP"].reshape(6, n)
+        if has_htrswb:
+            o["HTSWB"] = _as_tensor(_add(st, "HTSWB", (14, nlay, jm, im)), "HTSWB", unit)
+            out["htswb"] = o["HTSWB"].reshape(14, nlay, n)
+        if getattr(cfg, "lhsw0", False):
+            o["HSW0"] = _as_tensor(_add(st, "HSW0", (nlay, jm, im)), "HSW0", unit)
+            out["hsw0"] = o["HSW0"].reshape(nlay, n)
+        if getattr(cfg, "lflxprf", False):
+            o["FLXPRF"] = _as_tensor(_add(st, "FLXPRF", (4, nlay + 1, jm, im)), "FLXPRF", unit)
+            out["swflxprf"] = o["FLXPRF"].reshape(4, nlay + 1, n)
         s.solve(cols, _solcon(ctx), out, stream=stream)
     return o
 

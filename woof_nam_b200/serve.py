@@ -72,8 +72,9 @@ class RadServer:
         from .solver import SolverConfig
         from .tune import tuned_config
         largest = max(int(m["coszen"].shape[-1]) for dom in states.values() for m in dom)
-        # launch shape for the largest domain, LW chunks of at most 32,768 columns (3.1 GB of scratch a slot)
-        cfg = tuned_config(largest, SolverConfig(precision=precision), max_chunk=32768)
+        # launch shape for the largest domain, LW chunks of at most 32,768 columns (3.1 GB of scratch a slot),
+        # SW chunks of 8,192 day columns (3.2 GB a slot)
+        cfg = tuned_config(largest, SolverConfig(precision=precision, sw_sweep_chunk=8192), max_chunk=32768)
         self.slots = [_Slot(RadSolver(cfg), torch.cuda.Stream()) for _ in range(slots)]
         # each slot's handle keeps the scratch it grows to (up to the largest request) until it is closed
         self.held = sum(sl.solver.workspace_bytes(largest) for sl in self.slots)

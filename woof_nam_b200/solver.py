@@ -45,16 +45,38 @@ class SolverConfig:
     parts: str = "both"              # "lw", "sw" or "both": which solves run (lslwr / lsswr steps)
     lw_chunk: int = 0                # mixed: columns per two-kernel LW chunk (0 = 32768, < 0 single kernel)
     sw_sweep_chunk: int = 0          # mixed: day columns per two-kernel SW chunk (0 = 16384, < 0 single kernel)
+    # optional outputs of lwrad / swrad (the reference's lhlw0, lhlwb, lhsw0, lhswb / has_htrswb, lflxprf switches)
+    lhlw0: bool = False              # hlw0 [nlay][ncol]: LW clear-sky heating
+    lhlwb: bool = False              # hlwb [16][nlay][ncol]: LW heating per band
+    lhsw0: bool = False              # hsw0 [nlay][ncol]: SW clear-sky heating
+    lhswb: bool = False              # htswb [14][nlay][ncol]: SW heating per band
+    lflxprf: bool = False            # lwflxprf / swflxprf [4][nlay + 1][ncol]: level fluxes
 
 
-def output_shapes(nlay: int, ncol: int, route: str = "nam") -> dict:
+OPTIONAL_OUTPUTS = ("hsw0", "htswb", "swflxprf", "hlw0", "hlwb", "lwflxprf")
+
+
+def output_shapes(nlay: int, ncol: int, route: str = "nam", cfg: "SolverConfig | None" = None) -> dict:
     """Output arrays of a solve; the McICA route adds the sub-column cloud words (int32 storage of the
-    uint32 words, [word][layer][column], layers surface first, bit g & 31 of word g >> 5)."""
+    uint32 words, [word][layer][column], layers surface first, bit g & 31 of word g >> 5); cfg's switches add
+    the optional outputs (levels top first)."""
     d = {"htlw": (nlay, ncol), "htsw": (nlay, ncol), "topflw": (2, ncol), "sfcflw": (4, ncol),
          "topfsw": (3, ncol), "sfcfsw": (4, ncol), "fdncmp": (6, ncol)}
     if route == "mcica":
         d["lw_mask"] = (5, nlay, ncol)
         d["sw_mask"] = (4, nlay, ncol)
+    if cfg is not None:
+        if cfg.lhsw0:
+            d["hsw0"] = (nlay, ncol)
+        if cfg.lhswb:
+            d["htswb"] = (14, nlay, ncol)
+        if cfg.lhlw0:
+            d["hlw0"] = (nlay, ncol)
+        if cfg.lhlwb:
+            d["hlwb"] = (16, nlay, ncol)
+        if cfg.lflxprf:
+            d["swflxprf"] = (4, nlay + 1, ncol)
+            d["lwflxprf"] = (4, nlay + 1, ncol)
     return d
 
 
@@ -102,10 +124,10 @@ class RadSolver:
     def alloc_outputs(self, ncol: int, device=None) -> dict:
         """Output tensors of a solve of ncol columns (those of the configured parts only)."""
         torch = _torch()
-        skip = {"lw": ("htsw", "topfsw", "sfcfsw", "fdncmp"), "sw": ("htlw", "topflw", "sfcflw"),
-                "both": ()}[self.cfg.parts]
+        skip = {"lw": ("htsw", "topfsw", "sfcfsw", "fdncmp", "hsw0", "htswb", "swflxprf"),
+                "sw": ("htlw", "topflw", "sfcflw", "hlw0", "hlwb", "lwflxprf"), "both": ()}[self.cfg.parts]
         return {k: torch.empty(s, dtype=torch.int32 if k in MASK_KEYS else torch.float32, device=device or "cuda")
-                for k, s in output_shapes(self.cfg.nlay, ncol, self.cfg.route).items() if k not in skip}
+                for k, s in output_shapes(self.cfg.nlay, ncol, self.cfg.route, self.cfg).items() if k not in skip}
 
     def _abi_args(self, cols: dict, solcon: float, out: dict | None):
         torch = _torch()
@@ -135,7 +157,7 @@ class RadSolver:
             setattr(ci, k, t.data_ptr() if t is not None else None)
         ci.solcon = float(solcon)
         co = _lib.RadOutputs()
-        for k in output_shapes(1, 1, "mcica"):
+        for k in tuple(output_shapes(1, 1, "mcica")) + OPTIONAL_OUTPUTS:
             t = out.get(k)
             setattr(co, k, t.data_ptr() if t is not None else None)
         return ci, co, ncol, out
