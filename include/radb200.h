@@ -160,6 +160,35 @@ int rad_graph_create(RadHandle* h, int32_t nreq, const RadColumns* ins, const Ra
 int rad_graph_launch(RadGraph* g, void* stream);
 void rad_graph_destroy(RadGraph* g);
 
+/* ---- serving queue: continuous batching of whole-request solves (the rad_submit / rad_poll pair of the
+ * boundary; the reference has no serving path -- its rrtm_call is synchronous per model step,
+ * namgpu/physics/rrtm/rrtm_call.py:246) ----
+ * A queue owns one CUDA stream per slot handle.  rad_submit starts a request's solve at once on a free slot,
+ * so requests submitted while others run overlap on the device; the caller keeps its own arrival queue and
+ * retries on RAD_E_BUSY / RAD_E_BUDGET.  Results are the same bits as rad_solve on that slot's handle. */
+typedef struct RadQueue RadQueue;
+
+/* slots: handles with tables loaded, one per solve that may run at a time (the queue does not own them;
+ * destroy the queue first).  hbm_budget_bytes: the library scratch (rad_workspace_bytes) that the requests
+ * in flight may hold together, 0 = no limit. */
+int rad_queue_create(RadHandle* const* slots, int32_t nslots, int64_t hbm_budget_bytes, RadQueue** out);
+
+/* Start the solve of ncol columns (device pointers, as rad_solve) and return its ticket (>= 1).
+ * RAD_E_BUSY: every slot is in use; RAD_E_BUDGET: its scratch does not fit beside the requests in flight
+ * (a request larger than the whole budget is refused with RAD_E_INVALID).  Inputs must stay valid and outputs
+ * untouched until the ticket is done. */
+int rad_submit(RadQueue* q, const RadColumns* in, const RadOutputs* out, int64_t ncol, int64_t* ticket);
+
+/* *done = 1 once the ticket's solve has completed (its outputs are then valid for any reader), which frees
+ * its slot; 0 while it runs.  A ticket never issued is RAD_E_INVALID. */
+int rad_poll(RadQueue* q, int64_t ticket, int32_t* done);
+
+/* Poll until the ticket is done or timeout_ms elapse: RAD_OK or RAD_E_TIMEOUT (the solve keeps running). */
+int rad_wait(RadQueue* q, int64_t ticket, int32_t timeout_ms);
+
+/* Waits for the solves in flight, then releases the streams and events. */
+void rad_queue_destroy(RadQueue* q);
+
 /* Solve without reaching any allocator (no counterpart in the reference).  rad_solve grows the handle's
  * day-list scratch with cudaMalloc / cudaFree when a request is larger than any before it; cudaFree waits
  * for the whole device, and a host model that has handed its memory to its own pool, or keeps a fixed HBM

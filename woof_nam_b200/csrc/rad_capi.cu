@@ -18,6 +18,8 @@
 #include <limits>
 #include <map>
 #include <mutex>
+#include <chrono>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -1149,6 +1151,116 @@ int rad_rdtemp(RadHandle* h, const RadRdtemp* p, void* stream)
     h->launches += 1;
     RAD_CUDA(h, cudaGetLastError());
     return RAD_OK;
+}
+
+// ------------------------------------------------------------------------------------------------- queue
+struct RadQueue {
+    struct Slot {
+        RadHandle* h = nullptr;
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        int64_t ticket = 0;          // 0: free
+        int64_t bytes = 0;           // scratch charged against the budget while the ticket runs
+    };
+    std::vector<Slot> slots;
+    int64_t budget = 0, in_use = 0, next = 1;
+    std::mutex mu;
+};
+
+int rad_queue_create(RadHandle* const* slots, int32_t nslots, int64_t hbm_budget_bytes, RadQueue** out)
+{
+    if (!slots || !out || nslots < 1 || hbm_budget_bytes < 0)
+        return fail(nullptr, RAD_E_INVALID, "rad_queue_create: null argument, no slot or a negative budget");
+    *out = nullptr;
+    RadQueue* q = new RadQueue();
+    q->budget = hbm_budget_bytes;
+    for (int i = 0; i < nslots; ++i) {
+        RadQueue::Slot sl;
+        sl.h = slots[i];
+        if (!sl.h || !sl.h->tables_ok ||
+            cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess) {
+            if (sl.st) cudaStreamDestroy(sl.st);
+            q->slots.push_back(sl);
+            rad_queue_destroy(q);
+            return fail(nullptr, RAD_E_INVALID, "rad_queue_create: a slot handle is null or has no tables, or a "
+                                                 "stream / event could not be created");
+        }
+        q->slots.push_back(sl);
+    }
+    *out = q;
+    return RAD_OK;
+}
+
+int rad_submit(RadQueue* q, const RadColumns* in, const RadOutputs* out, int64_t ncol, int64_t* ticket)
+{
+    if (!q || !in || !out || !ticket) return fail(nullptr, RAD_E_INVALID, "rad_submit: null argument");
+    std::lock_guard<std::mutex> lock(q->mu);
+    *ticket = 0;
+    RadQueue::Slot* free_slot = nullptr;
+    for (auto& sl : q->slots)
+        if (!sl.ticket) { free_slot = &sl; break; }
+    if (!free_slot) return fail(nullptr, RAD_E_BUSY, "rad_submit: every slot is in use");
+    const int64_t need = rad_workspace_bytes(free_slot->h, ncol);
+    if (q->budget > 0 && need > q->budget)
+        return fail(free_slot->h, RAD_E_INVALID, "rad_submit: the request's scratch exceeds the whole HBM budget");
+    if (q->budget > 0 && q->in_use + need > q->budget)
+        return fail(free_slot->h, RAD_E_BUDGET, "rad_submit: the request's scratch does not fit beside those in flight");
+    int rc = rad_solve(free_slot->h, in, out, ncol, free_slot->st);
+    if (rc) return rc;
+    RAD_CUDA(free_slot->h, cudaEventRecord(free_slot->ev, free_slot->st));
+    free_slot->ticket = q->next++;
+    free_slot->bytes = need;
+    q->in_use += need;
+    *ticket = free_slot->ticket;
+    return RAD_OK;
+}
+
+int rad_poll(RadQueue* q, int64_t ticket, int32_t* done)
+{
+    if (!q || !done) return fail(nullptr, RAD_E_INVALID, "rad_poll: null argument");
+    std::lock_guard<std::mutex> lock(q->mu);
+    *done = 0;
+    if (ticket < 1 || ticket >= q->next) return fail(nullptr, RAD_E_INVALID, "rad_poll: unknown ticket");
+    for (auto& sl : q->slots) {
+        if (sl.ticket != ticket) continue;
+        const cudaError_t e = cudaEventQuery(sl.ev);
+        if (e == cudaErrorNotReady) return RAD_OK;
+        sl.ticket = 0;
+        q->in_use -= sl.bytes;
+        sl.bytes = 0;
+        if (e != cudaSuccess) return fail(sl.h, RAD_E_CUDA, std::string("rad_poll: ") + cudaGetErrorString(e));
+        *done = 1;
+        return RAD_OK;
+    }
+    *done = 1;   // completed and reaped by an earlier poll
+    return RAD_OK;
+}
+
+int rad_wait(RadQueue* q, int64_t ticket, int32_t timeout_ms)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        int32_t done = 0;
+        const int rc = rad_poll(q, ticket, &done);
+        if (rc || done) return rc;
+        if (std::chrono::steady_clock::now() - t0 >= std::chrono::milliseconds(std::max(timeout_ms, 0)))
+            return fail(nullptr, RAD_E_TIMEOUT, "rad_wait: the ticket is still running");
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+void rad_queue_destroy(RadQueue* q)
+{
+    if (!q) return;
+    for (auto& sl : q->slots) {
+        if (sl.st) {
+            cudaStreamSynchronize(sl.st);
+            cudaStreamDestroy(sl.st);
+        }
+        if (sl.ev) cudaEventDestroy(sl.ev);
+    }
+    delete q;
 }
 
 int rad_profile_enable(RadHandle* h, int on)
