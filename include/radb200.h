@@ -364,6 +364,115 @@ int rad_sol_update(const RadSolarIn* in, RadSolarState* out);
 int rad_coszmn(RadHandle* h, const RadSolarState* s, const float* glon, const float* glat, int64_t n, float solhr,
                float dtswav, int32_t nrads, float* coszen, float* coszdg, void* stream);
 
+/* ---- grrad's front end: the solve's inputs from the model state, the surface and the climatologies ----
+ * Each entry is one kernel, asynchronous on stream, over device pointers in the solve's layout ([field][level]
+ * [column], column = row * im + point, levels top first for ivflip 0).  Column counts of 0 do nothing. */
+
+/* DAYPARTS (grrad_nmmb.f:606-656 with coszmn_nmmb; replaces phys_rrtm_dayparts.dayparts,
+ * namgpu/physics/rrtm/phys_rrtm_dayparts.py:67, and its three kernels phys_rrtm_dayparts_cosz / _scatter / _len,
+ * namgpu/kernels/phys_rrtm_dayparts.cu:76,108,125, and the library scan between them): for jm rows of im points
+ * (im <= 24576), xlon, sinlat, coslat [jm * im], the sun of s (sollag, sindec, cosdec), solhr = hours after
+ * 00 UTC and the SW interval dtswav (hours) sampled nrads times.  Writes coszen, coszdg [jm * im] (as
+ * rad_coszmn), the run table of each row -- run k of row j in slot j * im + k for k < ndayparts[j]: dp_start
+ * (1-based point in the row), dp_len (points), dp_day (0 / 1: coszen >= 1e-4) -- and ndayparts [jm].  Slots
+ * past a row's runs are not written. */
+typedef struct {
+    float* coszen;           /* [jm * im] */
+    float* coszdg;           /* [jm * im] */
+    int32_t* dp_start;       /* [jm * im] */
+    int32_t* dp_len;         /* [jm * im] */
+    int32_t* dp_day;         /* [jm * im] */
+    int32_t* ndayparts;      /* [jm] */
+} RadDayparts;
+int rad_dayparts(RadHandle* h, const RadSolarState* s, const float* xlon, const float* sinlat, const float* coslat,
+                 int32_t im, int32_t jm, float solhr, float dtswav, int32_t nrads, const RadDayparts* out,
+                 void* stream);
+
+/* The CO2 set-up getgases reads (module variables of gas_init / gas_update, device pointers). */
+typedef struct {
+    const float* co2_glb;    /* [1] global mean CO2 volume mixing ratio */
+    const float* gco2cyc;    /* [12] its seasonal cycle */
+    const float* co2vmr_sav; /* [12][12][24] monthly 15-degree CO2 map ([month][latitude from 90N][longitude]) */
+    int32_t ico2flg;         /* 0: prescribed default, 1: global mean + cycle, 2: the map below 788 mb */
+    int32_t kmonsav;         /* month 1..12 (ico2flg 1, 2) */
+    int32_t ivflip;          /* 0: level 0 is the model top (NAM); 1: the surface */
+} RadGasSetup;
+
+/* getgases (radiation_gases_nmmb.f:843-979; replaces phys_rrtm_getgases.getgases,
+ * namgpu/physics/rrtm/phys_rrtm_getgases.py:65, kernel phys_rrtm_getgases.cu:67): the 10 gases' volume mixing
+ * ratios gasvmr [10][lmax][ncol] (RadColumns.gasvmr) from plvl [lmax + 1][ncol] (mb) and xlon, xlat [ncol]
+ * (radians).  RAD_E_INVALID for ico2flg outside 0..2, kmonsav outside 1..12 where used, ivflip outside 0..1. */
+int rad_getgases(RadHandle* h, const float* plvl, const float* xlon, const float* xlat, int64_t ncol, int32_t lmax,
+                 const RadGasSetup* g, float* gasvmr, void* stream);
+
+/* The ozone climatology getozn reads (gas_init / gas_update module variables; o3r and pkstr on the device). */
+typedef struct {
+    const float* o3r;        /* [12][loz][jmr] mass mixing ratio ([month][level][latitude]) */
+    const float* pkstr;      /* [loz] Exner function of its levels (increasing) */
+    int32_t jmr, loz;        /* latitudes (<= 360), levels (<= 64) */
+    int32_t k1oz, k2oz;      /* the two months interpolated, 1..12 */
+    float facoz;             /* weight of k2oz */
+    float blte, dlte;        /* first latitude and spacing, degrees */
+    int32_t ivflip;
+} RadOzoneClim;
+
+/* getozn (radiation_gases_nmmb.f:984-1094; replaces the phys_rrtm_getozn kernel launch,
+ * namgpu/physics/rrtm/phys_rrtm_getozn.py:117, kernel phys_rrtm_getozn.cu:43): ozone mass mixing ratio o3mmr
+ * [nlev][ncol] from the Exner function prslk [nlev][ncol] (grrad's prslk1) and xlat [ncol].  A level whose
+ * Exner function equals the climatology's first level, or a column with a NaN latitude, is not written (the
+ * routine leaves it as it was). */
+int rad_getozn(RadHandle* h, const float* prslk, const float* xlat, int64_t ncol, int32_t nlev, const RadOzoneClim* oz,
+               float* o3mmr, void* stream);
+
+/* setalb's inputs (device pointers, [ncol] each; grrad's names and units: snowf mm of water, zorlf cm). */
+typedef struct {
+    const float *slmsk, *snowf, *sncovr, *snoalb, *zorlf, *coszf, *tsknf, *hprif;
+    const float *alvsf, *alnsf, *alvwf, *alnwf, *facsf, *facwf, *fice, *tisfc;
+} RadAlbedoIn;
+
+/* setalb (radiation_surface_nmmb.f:407-725; replaces phys_rrtm_setalb.run, namgpu/physics/rrtm/
+ * phys_rrtm_setalb.py:78, kernel phys_rrtm_setalb.cu:35): sfcalb [4][ncol] (RadColumns.sfcalb: near-IR direct,
+ * near-IR diffuse, visible direct, visible diffuse) by Briegleb's scheme (ialbflg 0), MODIS land albedo with the
+ * land model's snow cover (1) or the provided albedos as they are (2, the NAM path; only alvsf..alnwf read). */
+int rad_setalb(RadHandle* h, const RadAlbedoIn* in, int64_t ncol, int32_t ialbflg, float* sfcalb, void* stream);
+
+/* setemis's inputs (device pointers, [ncol] each; SM 1 sea / 0 land, SICE > 0.5 sea ice, SI snow mm, Z0 m). */
+typedef struct {
+    const float *glon, *glat, *sm, *sice, *si, *sncovr, *z0, *stdh, *tskin;
+    const int32_t* idxems;   /* [180][360] surface type of the 1-degree map (read when iemslw is 1) */
+} RadEmisIn;
+
+/* setemis (radiation_surface_nmmb.f:730-897; replaces phys_rrtm_setemis.run, namgpu/physics/rrtm/
+ * phys_rrtm_setemis.py:54, kernel phys_rrtm_setemis.cu:40, whose sfc_flags [ialbflg, iemsflg, iemslw] come as
+ * ialbflg and iemslw): sfcemis [ncol] (RadColumns.sfcemis). */
+int rad_setemis(RadHandle* h, const RadEmisIn* in, int64_t ncol, int32_t ialbflg, int32_t iemslw, float* sfcemis,
+                void* stream);
+
+/* progcld2's inputs: the radiation layers ([nlay][ncol], plvl [nlay + 1][ncol], mb / K / kg/kg) and xlat. */
+typedef struct {
+    const float *plyr, *plvl, *tlyr, *tvly, *qlyr, *qstl, *rhly;
+    const float *clw;        /* total condensate (grrad clw) */
+    const float *f_ice, *f_rain, *r_rime;   /* Ferrier fractions (r_rime is not read) */
+    const float *cldfk1;     /* Thompson cloud fraction (read when cld_fraction != 0) */
+    const float *xlat;       /* [ncol] radians */
+} RadCloudIn;
+typedef struct {
+    int32_t ivflip, llyr;    /* llyr: 1-based boundary-layer top layer (1..nlay) */
+    int32_t iovr;            /* 0 random, else maximum-random overlap in gethml */
+    int32_t lcrick, lcnorm, lnoprec, lsashal, cld_fraction;
+} RadCloudCfg;
+typedef struct {
+    float* clouds;           /* [9][nlay][ncol] RadColumns.clouds */
+    float* clds;             /* [5][ncol] high, middle, low, total, boundary-layer cloud */
+    int32_t* mtop;           /* [3][ncol] 1-based top layer of the high, middle, low deck */
+    int32_t* mbot;           /* [3][ncol] 1-based base layer */
+} RadCloudOut;
+
+/* progcld2 with gethml (radiation_clouds_nmmb.f:787-1323, 2167-2494; replaces phys_rrtm_progcld2.run,
+ * namgpu/physics/rrtm/phys_rrtm_progcld2.py:75, kernel phys_rrtm_progcld2.cu:92).  2 <= nlay <= 128. */
+int rad_progcld2(RadHandle* h, const RadCloudIn* in, int64_t ncol, int32_t nlay, const RadCloudCfg* cfg,
+                 const RadCloudOut* out, void* stream);
+
 /* Device-time accounting of the library's own kernels (instrumentation; no counterpart in the reference,
  * which has none).  While enabled, rad_solve records CUDA events on its stream around the LW kernel, the
  * SW day-list kernels and the SW kernel; rad_profile_read waits for the last recorded event and returns

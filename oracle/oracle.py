@@ -318,3 +318,106 @@ def grrad_setup(model: dict, which: str = "port") -> dict:
         res[k] = out[o:o + sizes[k] * n].reshape(sizes[k], n) if k != "tsfg" else out[o:o + n]
         o += sizes[k] * n
     return res
+
+
+# ---- grrad's front end (rrtm_front.hpp; which="ref": the reference's own kernels) ----
+
+def _ip(a):
+    return a.ctypes.data_as(_I)
+
+
+def _fp(a):
+    return a.ctypes.data_as(_F)
+
+
+def _ptrs(arrs):
+    """A C array of float pointers to the (kept alive) float32 copies of arrs."""
+    keep = [_f(a) for a in arrs]
+    return keep, (_F * len(keep))(*[_fp(a) for a in keep])
+
+
+def dayparts(xlon, sinlat, coslat, im: int, solhr: float, dtswav: float, nrads: int, sol, which: str = "port") -> dict:
+    """DAYPARTS of n = jm * im points (row-major): coszen, coszdg [n], the run table dp_start, dp_len, dp_day [n]
+    (slot row * im + k, valid for k < ndayparts[row], others -1) and ndayparts [jm].  sol = sollag, sindec, cosdec."""
+    L = lib(which)
+    lo, sl, cl = _f(xlon), _f(sinlat), _f(coslat)
+    n = lo.size
+    jm = n // im
+    s = _f(np.asarray(sol, np.float32)[:3])
+    out = {"coszen": np.zeros(n, np.float32), "coszdg": np.zeros(n, np.float32)}
+    for k in ("dp_start", "dp_len", "dp_day"):
+        out[k] = np.full(n, -1, np.int32)
+    out["ndayparts"] = np.zeros(jm, np.int32)
+    L.orc_dayparts(ctypes.c_int(im), ctypes.c_int(jm), _fp(lo), _fp(sl), _fp(cl), ctypes.c_float(solhr),
+                   ctypes.c_float(dtswav), ctypes.c_int(nrads), _fp(s), _fp(out["coszen"]), _fp(out["coszdg"]),
+                   _ip(out["dp_start"]), _ip(out["dp_len"]), _ip(out["dp_day"]), _ip(out["ndayparts"]))
+    return out
+
+
+def getgases(plvl, xlon, xlat, co2_glb: float, gco2cyc, co2vmr_sav, ico2flg: int, kmonsav: int, ivflip: int,
+             which: str = "port") -> np.ndarray:
+    """Gas volume mixing ratios [10][lmax][n] from plvl [lmax + 1][n] (mb) and xlon / xlat [n] (radians)."""
+    L = lib(which)
+    pl, lo, la, cy, cs = _f(plvl), _f(xlon), _f(xlat), _f(gco2cyc), _f(co2vmr_sav)
+    lmax, n = pl.shape[0] - 1, pl.shape[1]
+    out = np.zeros((10, lmax, n), np.float32)
+    L.orc_getgases(ctypes.c_int(n), ctypes.c_int(lmax), _fp(pl), _fp(lo), _fp(la), ctypes.c_float(co2_glb), _fp(cy),
+                   _fp(cs), ctypes.c_int(ico2flg), ctypes.c_int(kmonsav), ctypes.c_int(ivflip), _fp(out))
+    return out
+
+
+def getozn(prslk, xlat, o3r, pkstr, k1oz: int, k2oz: int, facoz: float, blte: float, dlte: float, ivflip: int,
+           init=None, which: str = "port") -> np.ndarray:
+    """Ozone mass mixing ratio [nlev][n] from the Exner function prslk [nlev][n] and the climatology o3r
+    [12][loz][jmr] on pkstr [loz]; levels the routine leaves alone keep init (default NaN)."""
+    L = lib(which)
+    pk, la, o3, ps = _f(prslk), _f(xlat), _f(o3r), _f(pkstr)
+    nlev, n = pk.shape
+    out = np.full((nlev, n), np.nan, np.float32) if init is None else _f(init).copy()
+    L.orc_getozn(ctypes.c_int(n), ctypes.c_int(nlev), _fp(pk), _fp(la), _fp(o3), _fp(ps), ctypes.c_int(o3.shape[2]),
+                 ctypes.c_int(o3.shape[1]), ctypes.c_int(k1oz), ctypes.c_int(k2oz), ctypes.c_float(facoz),
+                 ctypes.c_float(blte), ctypes.c_float(dlte), ctypes.c_int(ivflip), _fp(out))
+    return out
+
+
+ALB_FIELDS = ("slmsk", "snowf", "sncovr", "snoalb", "zorlf", "coszf", "tsknf", "hprif", "alvsf", "alnsf", "alvwf",
+              "alnwf", "facsf", "facwf", "fice", "tisfc")
+EMIS_FIELDS = ("glon", "glat", "sm", "sice", "si", "sncovr", "z0", "stdh", "tskin")
+CLD_FIELDS = ("plyr", "plvl", "tlyr", "tvly", "qlyr", "qstl", "rhly", "clw", "f_ice", "f_rain", "r_rime", "cldfk1",
+              "xlat")
+CLD_CFG = ("ivflip", "llyr", "iovr", "lcrick", "lcnorm", "lnoprec", "lsashal", "cld_fraction")
+
+
+def setalb(sfc: dict, ialbflg: int, which: str = "port") -> np.ndarray:
+    """Surface albedo [4][n] of the SW call from the ALB_FIELDS of sfc ([n] each)."""
+    L = lib(which)
+    keep, pp = _ptrs([sfc[k] for k in ALB_FIELDS])
+    n = keep[0].size
+    out = np.zeros((4, n), np.float32)
+    L.orc_setalb(ctypes.c_int(n), pp, ctypes.c_int(ialbflg), _fp(out))
+    return out
+
+
+def setemis(sfc: dict, idxems, ialbflg: int, iemslw: int, which: str = "port") -> np.ndarray:
+    """Surface emissivity [n] of the LW call from the EMIS_FIELDS of sfc and the type map idxems [180][360]."""
+    L = lib(which)
+    keep, pp = _ptrs([sfc[k] for k in EMIS_FIELDS])
+    ix = np.ascontiguousarray(idxems, dtype=np.int32)
+    n = keep[0].size
+    out = np.zeros(n, np.float32)
+    L.orc_setemis(ctypes.c_int(n), pp, _ip(ix), ctypes.c_int(ialbflg), ctypes.c_int(iemslw), _fp(out))
+    return out
+
+
+def progcld2(cld: dict, cfg: dict, which: str = "port") -> dict:
+    """Ferrier cloud properties of the CLD_FIELDS of cld ([nlay][n], plvl [nlay + 1][n], xlat [n]) under the
+    CLD_CFG switches: clouds [9][nlay][n], clds [5][n], mtop, mbot [3][n]."""
+    L = lib(which)
+    keep, pp = _ptrs([cld[k] for k in CLD_FIELDS])
+    nlay, n = keep[0].shape
+    c = np.array([int(cfg[k]) for k in CLD_CFG], np.int32)
+    out = {"clouds": np.zeros((9, nlay, n), np.float32), "clds": np.zeros((5, n), np.float32),
+           "mtop": np.zeros((3, n), np.int32), "mbot": np.zeros((3, n), np.int32)}
+    L.orc_progcld2(ctypes.c_int(n), ctypes.c_int(nlay), pp, _ip(c), _fp(out["clouds"]), _fp(out["clds"]),
+                   _ip(out["mtop"]), _ip(out["mbot"]))
+    return out

@@ -186,6 +186,25 @@ namespace r_spcv {
 }
 
 // ------------------------------------------------------------------------------------------------------
+namespace r_dayp {
+#include "phys_rrtm_dayparts.cu"
+}
+namespace r_ggas {
+#include "phys_rrtm_getgases.cu"
+}
+namespace r_gozn {
+#include "phys_rrtm_getozn.cu"
+}
+namespace r_salb {
+#include "phys_rrtm_setalb.cu"
+}
+namespace r_sems {
+#include "phys_rrtm_setemis.cu"
+}
+namespace r_pc2 {
+#include "phys_rrtm_progcld2.cu"
+}
+
 namespace drv {
 
 using FV = std::vector<float>;
@@ -1323,6 +1342,82 @@ int orc_grrad_setup(int lm, int n, const float* pint, const float* pmid, const f
     drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
         r_grg::phys_rrtm_grrad_gases(plyr, plvl, tlyr, tskn.data(), t, q, tlvl, tvly, qlyr, tem2da.data(),
                                      tem2db.data(), tsfa.data(), n, 1, lm, 0);
+    });
+    return 0;
+}
+
+// ---- grrad's front end from the reference's kernels, one row of n columns (jm = 1, im = n) except DAYPARTS,
+// which takes its rows as they are.  Same signatures as the oracle's. ----
+
+// DAYPARTS (phys_rrtm_dayparts.py:67-105): the per-point kernel, the inclusive scan of the run starts (a library
+// cumsum in the reference, a host prefix sum here), then the scatter and length kernels.
+int orc_dayparts(int im, int jm, const float* xlon, const float* sinlat, const float* coslat, float solhr, float dtswav,
+                 int nrads, const float* sol, float* coszen, float* coszdg, int* dp_start, int* dp_len, int* dp_day,
+                 int* ndayparts)
+{
+    const int n = im * jm;
+    std::vector<int> day(n), start(n), scan(n);
+    const float st[4] = {sol[0], sol[1], sol[2], 0.0f};
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_dayp::phys_rrtm_dayparts_cosz(xlon, sinlat, coslat, solhr, dtswav, nrads, st, n, im, coszen, coszdg,
+                                        day.data(), start.data());
+    });
+    int acc = 0;
+    for (int p = 0; p < n; ++p) scan[p] = (acc += start[p]);
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_dayp::phys_rrtm_dayparts_scatter(start.data(), scan.data(), day.data(), n, im, dp_start, dp_day);
+    });
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_dayp::phys_rrtm_dayparts_len(dp_start, scan.data(), n, im, dp_len, ndayparts);
+    });
+    return 0;
+}
+
+int orc_getgases(int n, int lmax, const float* plvl, const float* xlon, const float* xlat, float co2_glb,
+                 const float* gco2cyc, const float* co2vmr_sav, int ico2flg, int kmonsav, int ivflip, float* gasvmr)
+{
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_ggas::phys_rrtm_getgases(plvl, xlon, xlat, &co2_glb, gco2cyc, co2vmr_sav, gasvmr, n, 1, lmax, ico2flg,
+                                   kmonsav, ivflip);
+    });
+    return 0;
+}
+
+int orc_getozn(int n, int nlev, const float* prslk, const float* xlat, const float* o3r, const float* pkstr, int jmr,
+               int loz, int k1oz, int k2oz, float facoz, float blte, float dlte, int ivflip, float* o3mmr)
+{
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_gozn::phys_rrtm_getozn(prslk, xlat, o3r, pkstr, o3mmr, n, 1, nlev, jmr, loz, k1oz, k2oz, facoz, blte, dlte,
+                                 ivflip);
+    });
+    return 0;
+}
+
+int orc_setalb(int n, const float* const* f, int ialbflg, float* sfcalb)
+{
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_salb::phys_rrtm_setalb(f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9], f[10], f[11], f[12], f[13],
+                                 f[14], f[15], ialbflg, n, 1, sfcalb);
+    });
+    return 0;
+}
+
+int orc_setemis(int n, const float* const* f, const int* idxems, int ialbflg, int iemslw, float* sfcemis)
+{
+    const int flags[3] = {ialbflg, iemslw, iemslw};
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_sems::phys_rrtm_setemis(f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], idxems, flags, sfcemis, n, 1);
+    });
+    return 0;
+}
+
+int orc_progcld2(int n, int nlay, const float* const* f, const int* cfg, float* clouds, float* clds, int* mtop,
+                 int* mbot)
+{
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_pc2::phys_rrtm_progcld2_column(n, 1, nlay, cfg[0], cfg[1], cfg[2], cfg[3], cfg[4], cfg[5], cfg[6], cfg[7],
+                                         f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9], f[10], f[11], f[12],
+                                         clouds, clds, mtop, mbot);
     });
     return 0;
 }

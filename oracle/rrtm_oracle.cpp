@@ -13,6 +13,7 @@
 #include "rrtm_aer.hpp"
 #include "rrtm_solar.hpp"
 #include "rrtm_grrad.hpp"
+#include "rrtm_front.hpp"
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -560,3 +561,60 @@ extern "C" int orc_grrad_setup(int lm, int n, const float* pint, const float* pm
     return 0;
 }
 
+
+// ---- grrad's front end (rrtm_front.hpp).  Same signatures as the reference driver's. ----
+
+// DAYPARTS of jm rows of im points; sol = sollag, sindec, cosdec.
+extern "C" int orc_dayparts(int im, int jm, const float* xlon, const float* sinlat, const float* coslat, float solhr,
+                            float dtswav, int nrads, const float* sol, float* coszen, float* coszdg, int* dp_start,
+                            int* dp_len, int* dp_day, int* ndayparts)
+{
+    orc::front::dayparts(im, jm, xlon, sinlat, coslat, solhr, dtswav, nrads, sol[0], sol[1], sol[2], coszen, coszdg,
+                         dp_start, dp_len, dp_day, ndayparts);
+    return 0;
+}
+
+extern "C" int orc_getgases(int n, int lmax, const float* plvl, const float* xlon, const float* xlat, float co2_glb,
+                            const float* gco2cyc, const float* co2vmr_sav, int ico2flg, int kmonsav, int ivflip,
+                            float* gasvmr)
+{
+    orc::front::getgases(n, lmax, plvl, xlon, xlat, co2_glb, gco2cyc, co2vmr_sav, ico2flg, kmonsav, ivflip, gasvmr);
+    return 0;
+}
+
+extern "C" int orc_getozn(int n, int nlev, const float* prslk, const float* xlat, const float* o3r, const float* pkstr,
+                          int jmr, int loz, int k1oz, int k2oz, float facoz, float blte, float dlte, int ivflip,
+                          float* o3mmr)
+{
+    orc::front::getozn(n, nlev, prslk, xlat, o3r, pkstr, jmr, loz, k1oz, k2oz, facoz, blte, dlte, ivflip, o3mmr);
+    return 0;
+}
+
+// f = slmsk, snowf, sncovr, snoalb, zorlf, coszf, tsknf, hprif, alvsf, alnsf, alvwf, alnwf, facsf, facwf, fice,
+// tisfc.
+extern "C" int orc_setalb(int n, const float* const* f, int ialbflg, float* sfcalb)
+{
+    const orc::front::AlbIn a{f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9], f[10], f[11], f[12], f[13],
+                              f[14], f[15]};
+    orc::front::setalb(n, a, ialbflg, sfcalb);
+    return 0;
+}
+
+// f = glon, glat, sm, sice, si, sncovr, z0, stdh, tskin.
+extern "C" int orc_setemis(int n, const float* const* f, const int* idxems, int ialbflg, int iemslw, float* sfcemis)
+{
+    const orc::front::EmisIn e{f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], idxems};
+    orc::front::setemis(n, e, ialbflg, iemslw, sfcemis);
+    return 0;
+}
+
+// f = plyr, plvl, tlyr, tvly, qlyr, qstl, rhly, clw, f_ice, f_rain, r_rime, cldfk1, xlat; cfg = ivflip, llyr,
+// iovr, lcrick, lcnorm, lnoprec, lsashal, cld_fraction.
+extern "C" int orc_progcld2(int n, int nlay, const float* const* f, const int* cfg, float* clouds, float* clds,
+                            int* mtop, int* mbot)
+{
+    const orc::front::CldIn in{f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9], f[11], f[12]};
+    const orc::front::CldCfg c{cfg[0], cfg[1], cfg[2], cfg[3], cfg[4], cfg[5], cfg[6], cfg[7]};
+    orc::front::progcld2(n, nlay, in, c, clouds, clds, mtop, mbot);
+    return 0;
+}

@@ -40,7 +40,8 @@ def test_struct_layout_matches_header(tmp_path):
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for st in (_lib.RadConfig, _lib.RadColumns, _lib.RadOutputs, _lib.RadProfile, _lib.RadPostIn, _lib.RadPostOut,
                _lib.RadRdtemp, _lib.RadAerClim, _lib.RadAerColumns, _lib.RadSolarIn, _lib.RadSolarState, _lib.RadModelColumns,
-               _lib.RadLayerFields):
+               _lib.RadLayerFields, _lib.RadDayparts, _lib.RadGasSetup, _lib.RadOzoneClim, _lib.RadAlbedoIn,
+               _lib.RadEmisIn, _lib.RadCloudIn, _lib.RadCloudCfg, _lib.RadCloudOut):
         lines.append(f'printf("{st.__name__} size %zu\\n", sizeof({st.__name__}));')
         for f, _ in st._fields_:
             lines.append(f'printf("{st.__name__}.{f} %zu\\n", offsetof({st.__name__}, {f}));')
@@ -52,7 +53,8 @@ def test_struct_layout_matches_header(tmp_path):
                                                                check=True).stdout.splitlines())
     for st in (_lib.RadConfig, _lib.RadColumns, _lib.RadOutputs, _lib.RadProfile, _lib.RadPostIn, _lib.RadPostOut,
                _lib.RadRdtemp, _lib.RadAerClim, _lib.RadAerColumns, _lib.RadSolarIn, _lib.RadSolarState, _lib.RadModelColumns,
-               _lib.RadLayerFields):
+               _lib.RadLayerFields, _lib.RadDayparts, _lib.RadGasSetup, _lib.RadOzoneClim, _lib.RadAlbedoIn,
+               _lib.RadEmisIn, _lib.RadCloudIn, _lib.RadCloudCfg, _lib.RadCloudOut):
         assert int(got[f"{st.__name__} size"]) == ctypes.sizeof(st), st.__name__
         for f, _ in st._fields_:
             assert int(got[f"{st.__name__}.{f}"]) == getattr(st, f).offset, f"{st.__name__}.{f}"

@@ -115,6 +115,51 @@ class RadSolarState(ctypes.Structure):
                 ("anginc", ctypes.c_float), ("solcon", ctypes.c_float), ("nstp", ctypes.c_int32)]
 
 
+DAYPARTS_FIELDS = ("coszen", "coszdg", "dp_start", "dp_len", "dp_day", "ndayparts")
+ALBEDO_FIELDS = ("slmsk", "snowf", "sncovr", "snoalb", "zorlf", "coszf", "tsknf", "hprif", "alvsf", "alnsf", "alvwf",
+                 "alnwf", "facsf", "facwf", "fice", "tisfc")
+EMIS_FIELDS = ("glon", "glat", "sm", "sice", "si", "sncovr", "z0", "stdh", "tskin", "idxems")
+CLOUD_IN_FIELDS = ("plyr", "plvl", "tlyr", "tvly", "qlyr", "qstl", "rhly", "clw", "f_ice", "f_rain", "r_rime", "cldfk1",
+                   "xlat")
+CLOUD_CFG_FIELDS = ("ivflip", "llyr", "iovr", "lcrick", "lcnorm", "lnoprec", "lsashal", "cld_fraction")
+CLOUD_OUT_FIELDS = ("clouds", "clds", "mtop", "mbot")
+
+
+class RadDayparts(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in DAYPARTS_FIELDS]
+
+
+class RadGasSetup(ctypes.Structure):
+    _fields_ = [("co2_glb", ctypes.c_void_p), ("gco2cyc", ctypes.c_void_p), ("co2vmr_sav", ctypes.c_void_p),
+                ("ico2flg", ctypes.c_int32), ("kmonsav", ctypes.c_int32), ("ivflip", ctypes.c_int32)]
+
+
+class RadOzoneClim(ctypes.Structure):
+    _fields_ = [("o3r", ctypes.c_void_p), ("pkstr", ctypes.c_void_p), ("jmr", ctypes.c_int32), ("loz", ctypes.c_int32),
+                ("k1oz", ctypes.c_int32), ("k2oz", ctypes.c_int32), ("facoz", ctypes.c_float),
+                ("blte", ctypes.c_float), ("dlte", ctypes.c_float), ("ivflip", ctypes.c_int32)]
+
+
+class RadAlbedoIn(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in ALBEDO_FIELDS]
+
+
+class RadEmisIn(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in EMIS_FIELDS]
+
+
+class RadCloudIn(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in CLOUD_IN_FIELDS]
+
+
+class RadCloudCfg(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int32) for k in CLOUD_CFG_FIELDS]
+
+
+class RadCloudOut(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in CLOUD_OUT_FIELDS]
+
+
 SIGNATURES = {
     "rad_version": ([], ctypes.c_int),
     "rad_config_default": ([ctypes.POINTER(RadConfig), ctypes.c_int32], None),
@@ -141,6 +186,19 @@ SIGNATURES = {
     "rad_coszmn": ([ctypes.c_void_p, ctypes.POINTER(RadSolarState), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                     ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
                    ctypes.c_int),
+    "rad_dayparts": ([ctypes.c_void_p, ctypes.POINTER(RadSolarState), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                      ctypes.c_int32, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_int32,
+                      ctypes.POINTER(RadDayparts), ctypes.c_void_p], ctypes.c_int),
+    "rad_getgases": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                      ctypes.POINTER(RadGasSetup), ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rad_getozn": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                    ctypes.POINTER(RadOzoneClim), ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rad_setalb": ([ctypes.c_void_p, ctypes.POINTER(RadAlbedoIn), ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p,
+                    ctypes.c_void_p], ctypes.c_int),
+    "rad_setemis": ([ctypes.c_void_p, ctypes.POINTER(RadEmisIn), ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                     ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rad_progcld2": ([ctypes.c_void_p, ctypes.POINTER(RadCloudIn), ctypes.c_int64, ctypes.c_int32,
+                      ctypes.POINTER(RadCloudCfg), ctypes.POINTER(RadCloudOut), ctypes.c_void_p], ctypes.c_int),
     "rad_setaer": ([ctypes.c_void_p, ctypes.POINTER(RadAerColumns), ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                     ctypes.c_void_p], ctypes.c_int),
     "rad_queue_create": ([ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int64,

@@ -4,6 +4,7 @@ from __future__ import annotations
 import os
 import shutil
 import subprocess
+import tempfile
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -25,20 +26,28 @@ def sources():
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile csrc/rad_capi.cu (which includes the kernel headers) into libradb200.so."""
+    """Compile csrc/rad_capi.cu (which includes the solve's kernel headers) and csrc/rad_front.cu (grrad's front
+    end, its own translation unit) and link them into libradb200.so."""
     if not force and LIB.exists() and all(p.stat().st_mtime <= LIB.stat().st_mtime for p in sources()):
         return LIB
-    # float division / square root to within 2 ulp and float denormals flushed: the mixed kernels'
-    # arithmetic is arranged so that neither changes results beyond the float rounding they already carry;
-    # the plain FP64 kernels and every float64 statement are unaffected.
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-prec-div=false", "-prec-sqrt=false", "-ftz=true",
-           "-Xcompiler", "-fPIC", "-shared",
-           "-o", str(LIB), str(SRC / "rad_capi.cu")]
+    base = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+        base.append("-Xptxas=-v")
+    # The solve: float division / square root to within 2 ulp and float denormals flushed -- the mixed kernels'
+    # arithmetic is arranged so that neither changes results beyond the float rounding they already carry; the
+    # plain FP64 kernels and every float64 statement are unaffected.
+    solve = ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"]
+    # The front end: every statement rounded as written (IEEE division and square root, denormals kept, no
+    # multiply-add contraction), as the single-precision routines it restates.
+    front = ["-prec-div=true", "-prec-sqrt=true", "-ftz=false", "-fmad=false"]
+    with tempfile.TemporaryDirectory() as tmp:
+        objs = []
+        for src, flags in (("rad_capi.cu", solve), ("rad_front.cu", front)):
+            obj = str(Path(tmp) / (src + ".o"))
+            subprocess.run([*base, *flags, "-c", "-o", obj, str(SRC / src)], check=True)
+            objs.append(obj)
+        subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *objs], check=True)
     return LIB
-
 
 if __name__ == "__main__":
     build(force=True, verbose=True)

@@ -241,3 +241,85 @@ def model_state(cols: "Columns") -> dict:
             "q": np.ascontiguousarray(cols.qlyr[1:], dtype=np.float32),
             "tsfc": np.ascontiguousarray(cols.tsfg, dtype=np.float32)}
 
+
+
+# ---- synthetic inputs of grrad's front end (the reference's climatology files are not part of its tree) ----
+
+OZONE_PSTR = (1.0, 2.0, 3.0, 5.0, 7.0, 10.0, 20.0, 30.0, 50.0, 70.0, 100.0, 150.0, 200.0, 300.0, 500.0, 700.0,
+              1000.0)   # 17 climatology levels, hPa, top first (loz 17, as the NAM climatology)
+
+
+def front_tables(seed: int = 77) -> dict:
+    """Seeded stand-ins for the climatologies the front end reads, with the reference's shapes: the monthly
+    15-degree CO2 map co2vmr_sav [12][12][24] with its global mean co2_glb and seasonal cycle gco2cyc [12]
+    (gas_init), the ozone climatology o3r [12][17][18] on the Exner levels pkstr [17] with blte -85,
+    dlte 10 (gas_init, module_SOLVER_GRID_COMP.F90 ozone settings), and the 1-degree surface-type map idxems
+    [180][360] (sfc_init; values 0..9 so that the clamps of setemis are reached)."""
+    r = np.random.default_rng(seed)
+    lat = -85.0 + 10.0 * np.arange(18)
+    lev = np.arange(17)
+    prof = 2.0e-6 + 8.0e-6 * np.exp(-((lev - 6.0) / 3.5) ** 2)          # stratospheric peak
+    o3r = np.empty((12, 17, 18), np.float32)
+    for m in range(12):
+        season = 1.0 + 0.25 * np.cos(2.0 * np.pi * (m / 12.0) + np.deg2rad(lat) * 2.0)
+        o3r[m] = (prof[:, None] * season[None, :] * (1.0 + 0.05 * r.standard_normal((17, 18)))).astype(np.float32)
+    pkstr = ((np.asarray(OZONE_PSTR) / 1000.0) ** (2.8705e2 / 1.0046e3)).astype(np.float32)
+    return {"co2_glb": np.float32(3.95e-4),
+            "gco2cyc": (3.0e-6 * np.sin(2.0 * np.pi * np.arange(12) / 12.0)).astype(np.float32),
+            "co2vmr_sav": (3.95e-4 + 4.0e-6 * r.standard_normal((12, 12, 24))).astype(np.float32),
+            "o3r": o3r, "pkstr": pkstr, "jmr": 18, "loz": 17, "blte": -85.0, "dlte": 10.0,
+            "idxems": r.integers(0, 10, size=(180, 360)).astype(np.int32)}
+
+
+def surface_state(n: int, seed: int) -> dict:
+    """The surface fields setalb and setemis read, for n columns: sea / land / sea-ice masks, snow (mm, many
+    columns without), roughness, orography spread, skin and ice temperatures through the freezing range, the
+    four background albedos and their strong / weak zenith fractions, and the grid position."""
+    r = np.random.default_rng(seed)
+    f = lambda lo, hi: r.uniform(lo, hi, n).astype(np.float32)           # noqa: E731
+    slmsk = r.choice(np.array([0.0, 1.0, 2.0], np.float32), n, p=[0.45, 0.45, 0.10])
+    snow = np.where(r.random(n) < 0.6, 0.0, r.exponential(20.0, n)).astype(np.float32)
+    cz = f(-0.3, 1.0)
+    cz[r.random(n) < 0.05] = 0.0
+    ts = f(235.0, 310.0)
+    ts = np.where(r.random(n) < 0.2, f(270.9, 273.3), ts).astype(np.float32)
+    sice = np.where(r.random(n) < 0.15, f(0.3, 1.0), 0.0).astype(np.float32)
+    return {"slmsk": slmsk, "snowf": snow, "sncovr": f(0.0, 1.0), "snoalb": f(0.5, 0.85),
+            "zorlf": np.exp(f(np.log(0.01), np.log(300.0))).astype(np.float32), "coszf": cz, "tsknf": ts,
+            "hprif": f(0.0, 900.0), "alvsf": f(0.04, 0.35), "alnsf": f(0.05, 0.45), "alvwf": f(0.04, 0.35),
+            "alnwf": f(0.05, 0.45), "facsf": f(0.0, 0.8), "facwf": f(0.0, 0.6), "fice": f(0.0, 1.0),
+            "tisfc": f(245.0, 275.0),
+            # setemis's names for the same kind of fields (SM: 1 sea, 0 land; Z0 in m)
+            "glon": f(-np.pi, np.pi), "glat": f(-np.pi / 2, np.pi / 2),
+            "sm": np.where(slmsk == 0.0, 1.0, 0.0).astype(np.float32), "sice": sice, "si": snow,
+            "z0": np.exp(f(np.log(1e-4), np.log(3.0))).astype(np.float32), "stdh": f(0.0, 900.0), "tskin": ts}
+
+
+def cloud_state(layers: dict, seed: int) -> dict:
+    """progcld2's inputs beside the radiation layers of grrad's set-up (plyr, plvl, tlyr, tvly, qlyr, qstl, rhly
+    [lmk (+1)][n], mb / K / kg/kg): total condensate clw in 0-3 decks per column (1-10 layers each, log-uniform
+    1e-8..3e-4 kg/kg, so that thin, broken and overcast layers and the high / middle / low split all occur),
+    the ice and rain fractions (slightly outside [0, 1] so that the clips act), the rime factor, the Thompson
+    cloud fraction cldfk1 and the latitude."""
+    tl = np.asarray(layers["tlyr"])
+    lmk, n = tl.shape
+    r = np.random.default_rng(seed)
+    clw = np.zeros((lmk, n))
+    ndeck = r.integers(0, 4, n)
+    for d in range(3):
+        has = ndeck > d
+        top = r.integers(1, lmk - 1, n)
+        thick = r.integers(1, 11, n)
+        amt = np.exp(r.uniform(np.log(1e-8), np.log(3e-4), n))
+        k = np.arange(lmk)[:, None]
+        inside = has[None, :] & (k >= top[None, :]) & (k < np.minimum(top + thick, lmk)[None, :])
+        clw = np.where(inside, clw + amt[None, :] * r.uniform(0.3, 1.0, (lmk, n)), clw)
+    out = {k: np.ascontiguousarray(layers[k], dtype=np.float32)
+           for k in ("plyr", "plvl", "tlyr", "tvly", "qlyr", "qstl", "rhly")}
+    out.update({"clw": clw.astype(np.float32),
+                "f_ice": r.uniform(-0.1, 1.1, (lmk, n)).astype(np.float32),
+                "f_rain": r.uniform(-0.1, 1.1, (lmk, n)).astype(np.float32),
+                "r_rime": r.uniform(1.0, 5.0, (lmk, n)).astype(np.float32),
+                "cldfk1": np.where(clw > 0, np.clip(r.uniform(-0.2, 1.2, (lmk, n)), 0.0, 1.0), 0.0).astype(np.float32),
+                "xlat": r.uniform(-np.pi / 2, np.pi / 2, n).astype(np.float32)})
+    return out

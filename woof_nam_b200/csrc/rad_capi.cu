@@ -26,6 +26,7 @@
 #define RAD_WANT_TABLE_NAMES
 #include "../../include/radb200.h"
 #include "rad_tabids.h"
+#include "rad_front.h"
 
 namespace rad {
 __constant__ int c_lw_ns[17] = {0, 10, 22, 38, 52, 68, 76, 88, 96, 108, 114, 122, 130, 134, 136, 138, 140};
@@ -1133,6 +1134,125 @@ int rad_coszmn(RadHandle* h, const RadSolarState* s, const float* glon, const fl
     k_coszmn<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a);
     h->launches += 1;
     RAD_CUDA(h, cudaGetLastError());
+    return RAD_OK;
+}
+
+// ---- grrad's front end (kernels in rad_front.cu) ----
+
+int rad_dayparts(RadHandle* h, const RadSolarState* s, const float* xlon, const float* sinlat, const float* coslat,
+                 int32_t im, int32_t jm, float solhr, float dtswav, int32_t nrads, const RadDayparts* out, void* stream)
+{
+    if (!h || !s || !out) return fail(h, RAD_E_INVALID, "rad_dayparts: null argument");
+    if (im < 0 || jm < 0 || nrads < 1 || !(dtswav > 0.0f))
+        return fail(h, RAD_E_INVALID, "rad_dayparts: im, jm, nrads or dtswav out of range");
+    if (im > front::DAYPARTS_MAX_IM) return fail(h, RAD_E_INVALID, "rad_dayparts: a row is longer than 24576 points");
+    if ((int64_t)im * jm == 0) return RAD_OK;
+    if (!xlon || !sinlat || !coslat || !out->coszen || !out->coszdg || !out->dp_start || !out->dp_len ||
+        !out->dp_day || !out->ndayparts)
+        return fail(h, RAD_E_INVALID, "rad_dayparts: a required pointer is null");
+    const front::DaypartsArgs a{xlon, sinlat, coslat, out->coszen, out->coszdg, out->dp_start, out->dp_len,
+                                out->dp_day, out->ndayparts, im, jm, nrads, solhr, dtswav, s->sollag, s->sindec,
+                                s->cosdec};
+    h->launches += 1;
+    RAD_CUDA(h, front::dayparts(a, (cudaStream_t)stream));
+    return RAD_OK;
+}
+
+int rad_getgases(RadHandle* h, const float* plvl, const float* xlon, const float* xlat, int64_t ncol, int32_t lmax,
+                 const RadGasSetup* g, float* gasvmr, void* stream)
+{
+    if (!h || !g) return fail(h, RAD_E_INVALID, "rad_getgases: null argument");
+    if (ncol < 0 || lmax < 1) return fail(h, RAD_E_INVALID, "rad_getgases: ncol or lmax out of range");
+    if (g->ico2flg < 0 || g->ico2flg > 2) return fail(h, RAD_E_INVALID, "rad_getgases: ico2flg is not 0, 1 or 2");
+    if (g->ico2flg != 0 && (g->kmonsav < 1 || g->kmonsav > 12))
+        return fail(h, RAD_E_INVALID, "rad_getgases: kmonsav must be 1..12 when ico2flg is 1 or 2");
+    if (g->ivflip != 0 && g->ivflip != 1) return fail(h, RAD_E_INVALID, "rad_getgases: ivflip must be 0 or 1");
+    if (ncol == 0) return RAD_OK;
+    if (!gasvmr || (g->ico2flg != 0 && (!g->co2_glb || !g->gco2cyc)) ||
+        (g->ico2flg == 2 && (!plvl || !xlon || !xlat || !g->co2vmr_sav)))
+        return fail(h, RAD_E_INVALID, "rad_getgases: a required pointer is null");
+    const front::GasArgs a{plvl, xlon, xlat, g->co2_glb, g->gco2cyc, g->co2vmr_sav, gasvmr, ncol, lmax, g->ico2flg,
+                           g->kmonsav, g->ivflip};
+    h->launches += 1;
+    RAD_CUDA(h, front::getgases(a, (cudaStream_t)stream));
+    return RAD_OK;
+}
+
+int rad_getozn(RadHandle* h, const float* prslk, const float* xlat, int64_t ncol, int32_t nlev, const RadOzoneClim* oz,
+               float* o3mmr, void* stream)
+{
+    if (!h || !oz) return fail(h, RAD_E_INVALID, "rad_getozn: null argument");
+    if (ncol < 0 || nlev < 1) return fail(h, RAD_E_INVALID, "rad_getozn: ncol or nlev out of range");
+    if (oz->loz < 2 || oz->loz > front::OZONE_MAX_LOZ || oz->jmr < 1 || oz->jmr > front::OZONE_MAX_JMR)
+        return fail(h, RAD_E_INVALID, "rad_getozn: loz must be 2..64 and jmr 1..360");
+    if (oz->k1oz < 1 || oz->k1oz > 12 || oz->k2oz < 1 || oz->k2oz > 12)
+        return fail(h, RAD_E_INVALID, "rad_getozn: the ozone months are not set (k1oz, k2oz must be 1..12)");
+    if (oz->ivflip != 0 && oz->ivflip != 1) return fail(h, RAD_E_INVALID, "rad_getozn: ivflip must be 0 or 1");
+    if (!(oz->dlte > 0.0f)) return fail(h, RAD_E_INVALID, "rad_getozn: dlte must be positive");
+    if (ncol == 0) return RAD_OK;
+    if (!prslk || !xlat || !oz->o3r || !oz->pkstr || !o3mmr)
+        return fail(h, RAD_E_INVALID, "rad_getozn: a required pointer is null");
+    const front::OzoneArgs a{prslk, xlat, oz->o3r, oz->pkstr, o3mmr, ncol, nlev, oz->jmr, oz->loz, oz->k1oz, oz->k2oz,
+                             oz->ivflip, oz->facoz, oz->blte, oz->dlte};
+    h->launches += 1;
+    RAD_CUDA(h, front::getozn(a, (cudaStream_t)stream));
+    return RAD_OK;
+}
+
+int rad_setalb(RadHandle* h, const RadAlbedoIn* in, int64_t ncol, int32_t ialbflg, float* sfcalb, void* stream)
+{
+    if (!h || !in) return fail(h, RAD_E_INVALID, "rad_setalb: null argument");
+    if (ncol < 0) return fail(h, RAD_E_INVALID, "rad_setalb: ncol out of range");
+    if (ncol == 0) return RAD_OK;
+    const bool all = ialbflg == 0 || ialbflg == 1;
+    if (!sfcalb || !in->alvsf || !in->alnsf || !in->alvwf || !in->alnwf ||
+        (all && (!in->slmsk || !in->snowf || !in->zorlf || !in->coszf || !in->tsknf || !in->hprif || !in->facsf ||
+                 !in->facwf || !in->fice || !in->tisfc)) ||
+        (ialbflg == 1 && (!in->sncovr || !in->snoalb)))
+        return fail(h, RAD_E_INVALID, "rad_setalb: a required pointer is null");
+    const front::AlbedoArgs a{in->slmsk, in->snowf, in->sncovr, in->snoalb, in->zorlf, in->coszf, in->tsknf, in->hprif,
+                              in->alvsf, in->alnsf, in->alvwf, in->alnwf, in->facsf, in->facwf, in->fice, in->tisfc,
+                              sfcalb, ncol, ialbflg};
+    h->launches += 1;
+    RAD_CUDA(h, front::setalb(a, (cudaStream_t)stream));
+    return RAD_OK;
+}
+
+int rad_setemis(RadHandle* h, const RadEmisIn* in, int64_t ncol, int32_t ialbflg, int32_t iemslw, float* sfcemis,
+                void* stream)
+{
+    if (!h || !in) return fail(h, RAD_E_INVALID, "rad_setemis: null argument");
+    if (ncol < 0) return fail(h, RAD_E_INVALID, "rad_setemis: ncol out of range");
+    if (ncol == 0) return RAD_OK;
+    if (!sfcemis || (iemslw != 0 && (!in->glon || !in->glat || !in->sm || !in->sice || !in->si || !in->z0 ||
+                                     !in->stdh || !in->tskin || !in->idxems || (ialbflg == 1 && !in->sncovr))))
+        return fail(h, RAD_E_INVALID, "rad_setemis: a required pointer is null");
+    const front::EmisArgs a{in->glon, in->glat, in->sm, in->sice, in->si, in->sncovr, in->z0, in->stdh, in->tskin,
+                            in->idxems, sfcemis, ncol, ialbflg, iemslw};
+    h->launches += 1;
+    RAD_CUDA(h, front::setemis(a, (cudaStream_t)stream));
+    return RAD_OK;
+}
+
+int rad_progcld2(RadHandle* h, const RadCloudIn* in, int64_t ncol, int32_t nlay, const RadCloudCfg* cfg,
+                 const RadCloudOut* out, void* stream)
+{
+    if (!h || !in || !cfg || !out) return fail(h, RAD_E_INVALID, "rad_progcld2: null argument");
+    if (ncol < 0 || nlay < 2 || nlay > front::CLOUD_MAX_LAY)
+        return fail(h, RAD_E_INVALID, "rad_progcld2: ncol or nlay out of range (2 <= nlay <= 128)");
+    if (cfg->ivflip != 0 && cfg->ivflip != 1) return fail(h, RAD_E_INVALID, "rad_progcld2: ivflip must be 0 or 1");
+    if (cfg->llyr < 1 || cfg->llyr > nlay) return fail(h, RAD_E_INVALID, "rad_progcld2: llyr outside 1..nlay");
+    if (ncol == 0) return RAD_OK;
+    if (!in->plyr || !in->plvl || !in->tlyr || !in->tvly || !in->qlyr || !in->qstl || !in->rhly || !in->clw ||
+        !in->f_ice || !in->f_rain || !in->xlat || (cfg->cld_fraction != 0 && !in->cldfk1) || !out->clouds ||
+        !out->clds || !out->mtop || !out->mbot)
+        return fail(h, RAD_E_INVALID, "rad_progcld2: a required pointer is null");
+    const front::CloudArgs a{in->plyr, in->plvl, in->tlyr, in->tvly, in->qlyr, in->qstl, in->rhly, in->clw, in->f_ice,
+                             in->f_rain, in->cldfk1, in->xlat, out->clouds, out->clds, out->mtop, out->mbot, ncol,
+                             nlay, cfg->ivflip, cfg->llyr, cfg->iovr, cfg->lcrick, cfg->lcnorm, cfg->lnoprec,
+                             cfg->lsashal, cfg->cld_fraction};
+    h->launches += 1;
+    RAD_CUDA(h, front::progcld2(a, (cudaStream_t)stream));
     return RAD_OK;
 }
 

@@ -112,7 +112,9 @@ def solar_spectrum(cu: Path) -> dict:
 
 
 def main():
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        raise SystemExit("usage: python pack_aer_tables.py <reference tree>")
+    root = Path(sys.argv[1])
     t = parse(root / "namgpu" / "parm" / "nam_climaeropac_global.txt")
     t.update(solar_spectrum(root / "namgpu" / "kernels" / "phys_rrtm_aer_init.cu"))
     out = Path(__file__).resolve().parent / "aer_tables.npz"

@@ -126,7 +126,9 @@ def pack(ref_root: Path) -> dict:
 
 
 def main(argv):
-    ref_root = Path(argv[1]) if len(argv) > 1 else Path("/root/reference")
+    if len(argv) < 2:
+        raise SystemExit("usage: python pack_tables.py <reference tree>")
+    ref_root = Path(argv[1])
     out = pack(ref_root)
     dst = Path(__file__).resolve().parent / "rrtm_tables.npz"
     np.savez_compressed(dst, **out)

@@ -1,0 +1,167 @@
+"""grrad's front end on the GPU: the column solve's inputs from the model state, the surface fields and the
+climatologies, one library kernel per routine (rad_dayparts, rad_getgases, rad_getozn, rad_setalb, rad_setemis,
+rad_progcld2).  The functions mirror the reference's units (namgpu/physics/rrtm/phys_rrtm_dayparts.py,
+phys_rrtm_getgases.py, phys_rrtm_getozn.py, phys_rrtm_setalb.py, phys_rrtm_setemis.py, phys_rrtm_progcld2.py):
+the same names, argument meaning and checks, with CUDA float32 tensors in the solve's layout ([field][level]
+[column], column = row * im + point) where the reference takes CuPy arrays [.., JM, IM].
+
+    from woof_nam_b200 import front
+    dp = front.dayparts(solver, glon, torch.sin(glat), torch.cos(glat), solhr, dtswav, nrads, sun, im)
+    gas = front.getgases(solver, lay["plvl"], glon, glat, gasvmr, co2_glb=..., gco2cyc=..., co2vmr_sav=...,
+                         ico2flg=1, kmonsav=7, ivflip=0)
+
+Every function launches on the given stream (default: torch's current one) and returns its outputs; nothing
+is read back to the host.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _lib
+
+NF_VGAS = 10
+NF_CLDS = 9
+NF_ALBD = 4
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _dev(t, name: str, unit: str, dtype=None):
+    torch = _torch()
+    dtype = dtype or torch.float32
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == dtype and t.is_contiguous()):
+        raise TypeError(f"{unit}: {name} must be a contiguous {dtype} CUDA tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    torch = _torch()
+    return ctypes.c_void_p((stream if stream is not None else torch.cuda.current_stream()).cuda_stream)
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def dayparts(solver, xlon, sinlat, coslat, solhr: float, dtswav: float, nrads: int, sun: dict, im: int,
+             out: dict | None = None, stream=None) -> dict:
+    """DAYPARTS of n = jm * im points (phys_rrtm_dayparts.dayparts): coszen, coszdg [n], the run table dp_start,
+    dp_len, dp_day [n] (run k of row j in slot j * im + k, valid for k < ndayparts[j]) and ndayparts [jm].  sun is
+    solar.sol_update's dict (sollag, sindec, cosdec)."""
+    torch = _torch()
+    n = xlon.numel()
+    if im < 1 or n % im != 0:
+        raise ValueError(f"dayparts: n={n} is not a whole number of rows of im={im}")
+    jm = n // im
+    if out is None:
+        dev = xlon.device
+        out = {"coszen": torch.empty(n, dtype=torch.float32, device=dev),
+               "coszdg": torch.empty(n, dtype=torch.float32, device=dev)}
+        for k in ("dp_start", "dp_len", "dp_day"):
+            out[k] = torch.zeros(n, dtype=torch.int32, device=dev)
+        out["ndayparts"] = torch.zeros(jm, dtype=torch.int32, device=dev)
+    o = _lib.RadDayparts(*[_ptr(out[k]) for k in _lib.DAYPARTS_FIELDS])
+    args = [_dev(t, k, "dayparts") for k, t in (("xlon", xlon), ("sinlat", sinlat), ("coslat", coslat))]
+    rc = solver.lib.rad_dayparts(solver.handle, ctypes.byref(sun["_state"]), *args, int(im), int(jm), float(solhr),
+                                 float(dtswav), int(nrads), ctypes.byref(o), _stream(stream))
+    _lib.check(solver.lib, solver.handle, rc, "rad_dayparts")
+    return out
+
+
+def getgases(solver, plvl, xlon, xlat, gasvmr=None, *, co2_glb, gco2cyc, co2vmr_sav, ico2flg: int, kmonsav,
+             ivflip: int, stream=None):
+    """Gas volume mixing ratios gasvmr [10][lmax][n] (phys_rrtm_getgases.getgases) from plvl [lmax + 1][n] (mb),
+    xlon, xlat [n]; co2_glb [1], gco2cyc [12], co2vmr_sav [12][12][24] device tensors (gas_init's)."""
+    torch = _torch()
+    lmax, n = plvl.shape[0] - 1, plvl.shape[1]
+    if gasvmr is None:
+        gasvmr = torch.empty((NF_VGAS, lmax, n), dtype=torch.float32, device=plvl.device)
+    if tuple(gasvmr.shape) != (NF_VGAS, lmax, n):
+        raise ValueError(f"getgases: gasvmr shape {tuple(gasvmr.shape)} does not match [10, {lmax}, {n}]")
+    g = _lib.RadGasSetup(_ptr(co2_glb), _ptr(gco2cyc), _ptr(co2vmr_sav), int(ico2flg),
+                         int(kmonsav) if kmonsav is not None else 0, int(ivflip))
+    rc = solver.lib.rad_getgases(solver.handle, _dev(plvl, "plvl", "getgases"), _dev(xlon, "xlon", "getgases"),
+                                 _dev(xlat, "xlat", "getgases"), n, lmax, ctypes.byref(g),
+                                 _dev(gasvmr, "gasvmr", "getgases"), _stream(stream))
+    _lib.check(solver.lib, solver.handle, rc, "rad_getgases")
+    return gasvmr
+
+
+def getozn(solver, prslk, xlat, o3mmr=None, *, o3r, pkstr, k1oz: int, k2oz: int, facoz: float, blte: float,
+           dlte: float, ivflip: int = 0, stream=None):
+    """Climatological ozone o3mmr [nlev][n] (phys_rrtm_getozn) from the Exner function prslk [nlev][n] and xlat
+    [n]; o3r [12][loz][jmr], pkstr [loz] device tensors, k1oz / k2oz / facoz from gas_update."""
+    torch = _torch()
+    nlev, n = prslk.shape
+    if o3mmr is None:
+        o3mmr = torch.zeros((nlev, n), dtype=torch.float32, device=prslk.device)
+    c = _lib.RadOzoneClim(_ptr(o3r), _ptr(pkstr), int(o3r.shape[2]), int(o3r.shape[1]), int(k1oz), int(k2oz),
+                          float(facoz), float(blte), float(dlte), int(ivflip))
+    rc = solver.lib.rad_getozn(solver.handle, _dev(prslk, "prslk", "getozn"), _dev(xlat, "xlat", "getozn"), n, nlev,
+                               ctypes.byref(c), _dev(o3mmr, "o3mmr", "getozn"), _stream(stream))
+    _lib.check(solver.lib, solver.handle, rc, "rad_getozn")
+    return o3mmr
+
+
+def setalb(solver, sfc: dict, ialbflg: int, sfcalb=None, stream=None):
+    """Surface albedo sfcalb [4][n] (phys_rrtm_setalb) from the ALBEDO_FIELDS of sfc ([n] CUDA tensors; zorlf in
+    cm, snowf in mm).  ialbflg 2 reads only alvsf, alnsf, alvwf, alnwf."""
+    torch = _torch()
+    n = sfc["alvsf"].numel()
+    if sfcalb is None:
+        sfcalb = torch.empty((NF_ALBD, n), dtype=torch.float32, device=sfc["alvsf"].device)
+    a = _lib.RadAlbedoIn(*[_ptr(sfc.get(k)) for k in _lib.ALBEDO_FIELDS])
+    rc = solver.lib.rad_setalb(solver.handle, ctypes.byref(a), n, int(ialbflg), _dev(sfcalb, "sfcalb", "setalb"),
+                               _stream(stream))
+    _lib.check(solver.lib, solver.handle, rc, "rad_setalb")
+    return sfcalb
+
+
+def setemis(solver, sfc: dict, idxems, ialbflg: int, iemslw: int, sfcemis=None, stream=None):
+    """Surface emissivity sfcemis [n] (phys_rrtm_setemis) from glon, glat, sm, sice, si, sncovr, z0, stdh, tskin
+    [n] of sfc and the int32 type map idxems [180][360]."""
+    torch = _torch()
+    n = sfc["glon"].numel()
+    if sfcemis is None:
+        sfcemis = torch.empty(n, dtype=torch.float32, device=sfc["glon"].device)
+    if idxems is not None:
+        _dev(idxems, "idxems", "setemis", torch.int32)
+    vals = [_ptr(sfc.get(k)) for k in _lib.EMIS_FIELDS[:-1]] + [_ptr(idxems)]
+    e = _lib.RadEmisIn(*vals)
+    rc = solver.lib.rad_setemis(solver.handle, ctypes.byref(e), n, int(ialbflg), int(iemslw),
+                                _dev(sfcemis, "sfcemis", "setemis"), _stream(stream))
+    _lib.check(solver.lib, solver.handle, rc, "rad_setemis")
+    return sfcemis
+
+
+def progcld2(solver, inputs: dict, *, ivflip: int, llyr: int, iovr: int, lcrick: bool = False, lcnorm: bool = False,
+             lnoprec: bool = False, lsashal: bool = False, cld_fraction: int = 0, out: dict | None = None,
+             stream=None) -> dict:
+    """Ferrier cloud properties (phys_rrtm_progcld2.run) of the CLOUD_IN_FIELDS of inputs: clouds [9][nlay][n],
+    clds [5][n], mtop, mbot [3][n] (1-based layers) -- the dict keys the reference's unit returns as clouds,
+    clds, mtopa, mbota."""
+    torch = _torch()
+    nlay, n = inputs["plyr"].shape
+    if cld_fraction != 0 and inputs.get("cldfk1") is None:
+        raise RuntimeError(f"progcld2: cld_fraction={cld_fraction} needs cldfk1 (Thompson)")
+    if out is None:
+        dev = inputs["plyr"].device
+        out = {"clouds": torch.empty((NF_CLDS, nlay, n), dtype=torch.float32, device=dev),
+               "clds": torch.empty((5, n), dtype=torch.float32, device=dev),
+               "mtop": torch.empty((3, n), dtype=torch.int32, device=dev),
+               "mbot": torch.empty((3, n), dtype=torch.int32, device=dev)}
+    for k in _lib.CLOUD_IN_FIELDS:
+        if inputs.get(k) is not None:
+            _dev(inputs[k], k, "progcld2")
+    ci = _lib.RadCloudIn(*[_ptr(inputs.get(k)) for k in _lib.CLOUD_IN_FIELDS])
+    cfg = _lib.RadCloudCfg(int(ivflip), int(llyr), int(iovr), int(bool(lcrick)), int(bool(lcnorm)), int(bool(lnoprec)),
+                           int(bool(lsashal)), int(cld_fraction))
+    co = _lib.RadCloudOut(*[_ptr(out[k]) for k in _lib.CLOUD_OUT_FIELDS])
+    rc = solver.lib.rad_progcld2(solver.handle, ctypes.byref(ci), n, nlay, ctypes.byref(cfg), ctypes.byref(co),
+                                 _stream(stream))
+    _lib.check(solver.lib, solver.handle, rc, "rad_progcld2")
+    out["mtopa"], out["mbota"] = out["mtop"], out["mbot"]
+    return out
