@@ -48,6 +48,7 @@ def parse():
                     help="skip the uneven-batch leg (parent grid + three nests in one graph-captured launch set)")
     ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE)
     ap.add_argument("--no-aer", action="store_true", help="skip the aerosol-optics leg")
+    ap.add_argument("--no-front", action="store_true", help="skip the grrad front-end leg")
     ap.add_argument("--no-parity", action="store_true", help="skip the parity block (errors against the oracle)")
     ap.add_argument("--parity-sample", type=int, default=16384)
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
@@ -232,6 +233,92 @@ def serving_block(members: int, n_req: int, seed: int = 7) -> dict:
     return res
 
 
+def front_block(mixed, cols, dev, seed: int, tstep, steps: int, warmup: int, im: int = 954) -> dict:
+    """grrad's front end for the timed domain: each front-end kernel alone (HBM roofline: the algorithmic bytes
+    of a column -- every input word read once, every output word written once -- times the columns, over the
+    kernel's CUDA-event time), then the whole radiation call (chain.radiation_call: the front end feeding the
+    solve, one stream) per step.  The NAM settings: ico2flg 1, ntoz 0 climatological ozone, Ferrier clouds
+    (np3d 3, ivflip 0), ialbflg 2 (and the MODIS branch 1 for comparison), iemslw 1.  Inputs: the columns'
+    model state (model_state), seeded surface fields and climatologies (columns.surface_state, front_tables)
+    and cloud fields (cloud_state of a 65,536-column tile repeated across the domain), on a NAM-like grid
+    (-140..-60 E, 10..60 N)."""
+    import torch
+    from woof_nam_b200 import front, solar
+    from woof_nam_b200.chain import CLOUD_NAM, radiation_call
+    from woof_nam_b200.columns import cloud_state, front_tables, model_state, surface_state
+    from woof_nam_b200.grrad import layers as grrad_layers
+    n = cols.ncol
+    jm = n // im
+    T = lambda a, dt=None: torch.as_tensor(np.ascontiguousarray(a, dtype=dt), device=dev)  # noqa: E731
+    model = {k: T(v) for k, v in model_state(cols).items()}
+    lm = model["pmid"].shape[0]
+    lmk = lm + 1
+    lay = grrad_layers(mixed, model)
+    tile = min(n, 65536)
+    lay_t = {k: v[..., :tile].cpu().numpy() for k, v in lay.items()}
+    cld_t = cloud_state(lay_t, seed)
+    reps = -(-n // tile)
+    cld = {k: T(np.tile(cld_t[k], (1, reps))[:, :n] if cld_t[k].ndim == 2 else np.tile(cld_t[k], reps)[:n])
+           for k in ("clw", "f_ice", "f_rain", "r_rime", "cldfk1")}
+    sfc_h = surface_state(n, seed + 1)
+    lon = np.deg2rad(np.linspace(-140.0, -60.0, im))[None, :].repeat(jm, 0).ravel()
+    lat = np.deg2rad(np.linspace(10.0, 60.0, jm))[:, None].repeat(im, 1).ravel()
+    sfc_h.update(glon=lon, glat=lat, sinlat=np.sin(lat), coslat=np.cos(lat))
+    sfc = {k: T(v, np.float32) for k, v in sfc_h.items()}
+    tab_h = front_tables(seed + 2)
+    tab = {k: (T(v) if isinstance(v, np.ndarray) else v) for k, v in tab_h.items()}
+    tab["co2_glb"] = T(np.atleast_1d(np.float32(tab_h["co2_glb"])))
+    sun = solar.sol_update((2026, 7, 1, 18, 0, 0), deltsw=1200.0, deltim=25.0)
+    call = dict(solhr=18.0, dtswav=1200.0 / 3600.0, nrads=48)
+    f32 = dict(dtype=torch.float32, device=dev)
+    gas, oz = torch.empty((10, lmk, n), **f32), torch.zeros((lmk, n), **f32)
+    alb, ems = torch.empty((4, n), **f32), torch.empty(n, **f32)
+    dp = front.dayparts(mixed, sfc["glon"], sfc["sinlat"], sfc["coslat"], sun=sun, im=im, **call)
+    sfc["coszf"] = dp["coszen"]
+    cin = {k: lay[k] for k in ("plyr", "plvl", "tlyr", "tvly", "qlyr", "qstl", "rhly")}
+    cin.update(cld, xlat=sfc["glat"])
+    cl = front.progcld2(mixed, cin, **CLOUD_NAM)
+    run = {
+        "k_grrad_setup": (lambda: grrad_layers(mixed, model, out=lay), 4 * (14 * lm + 14)),
+        "k_dayparts": (lambda: front.dayparts(mixed, sfc["glon"], sfc["sinlat"], sfc["coslat"], sun=sun, im=im, out=dp,
+                                              **call), 20),
+        "k_getozn": (lambda: front.getozn(mixed, lay["prslk1"], sfc["glat"], oz, o3r=tab["o3r"], pkstr=tab["pkstr"],
+                                          k1oz=6, k2oz=7, facoz=0.4, blte=tab["blte"], dlte=tab["dlte"]),
+                     4 * (2 * lmk + 1)),
+        "k_getgases": (lambda: front.getgases(mixed, lay["plvl"], sfc["glon"], sfc["glat"], gas, co2_glb=tab["co2_glb"],
+                                              gco2cyc=tab["gco2cyc"], co2vmr_sav=tab["co2vmr_sav"], ico2flg=1,
+                                              kmonsav=7, ivflip=0), 4 * 10 * lmk),
+        "k_progcld2": (lambda: front.progcld2(mixed, cin, out=cl, **CLOUD_NAM), 4 * (8 * lmk + 2 + 9 * lmk + 11)),
+        "k_setalb(ialbflg 2)": (lambda: front.setalb(mixed, sfc, 2, alb), 32),
+        "k_setalb(ialbflg 1)": (lambda: front.setalb(mixed, sfc, 1, alb), 4 * (16 + 4)),
+        "k_setemis": (lambda: front.setemis(mixed, sfc, tab["idxems"], 2, 1, ems), 4 * (9 + 1)),
+    }
+    hbm = float(peaks().get("hbm_gbs", 6650.0))
+    kern = {}
+    for name, (fn, bpc) in run.items():
+        ms = tstep(fn, steps, warmup)
+        gbs = bpc * n / (ms * 1e-3) / 1e9
+        kern[name] = {"ms": ms, "bytes_per_column": bpc, "achieved_gbs": gbs, "frac": gbs / hbm}
+    state = dict(model)
+    state.update(cld)
+    state.update(sfc)
+    clim = dict(tab)
+    kw = dict(sun=sun, im=im, kmonsav=7, k1oz=6, k2oz=7, facoz=0.4, ico2flg=1, ialbflg=2, iemslw=1, **call)
+    first = radiation_call(mixed, state, clim, **kw)
+    work, outs = first["work"], {k: v for k, v in first.items() if k != "work"}
+    ms_call = tstep(lambda: radiation_call(mixed, state, clim, work=work, out=outs, **kw), steps, warmup)
+    front_ms = sum(v["ms"] for k, v in kern.items() if k != "k_setalb(ialbflg 1)")
+    res = {"workload": f"{im}x{jm} columns x {lmk} layers, NAM settings (ico2flg 1, climatological ozone, Ferrier "
+                       f"clouds, ialbflg 2, iemslw 1); seeded surface / cloud / climatology stand-ins",
+           "kernels": kern, "front_end_ms": front_ms, "peak_gbs": hbm,
+           "radiation_call": {"value": n / (ms_call * 1e-3), "unit": UNIT, "ms_per_step": ms_call,
+                              "what": "chain.radiation_call: grrad set-up, dayparts, getozn, getgases, progcld2, "
+                                      "setalb, setemis and the LW+SW solve of the whole domain, one stream, "
+                                      "no row windows"}}
+    del state, clim, work, outs, first, model, lay, cld, sfc, tab
+    return res
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -301,6 +388,20 @@ def main():
         if profile:
             solver.profile(False)
         return ms, prof, prof["launches"] - launches0, clocks
+
+    def tstep(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / steps)
 
     bus = None
     try:
@@ -383,20 +484,6 @@ def main():
         da["faersw"], da["faerlw"] = A.optics(d, ai["rhly"], ai["xlon"], ai["xlat"], ai["slmsk"])
         opt = lambda: A.optics(d, ai["rhly"], ai["xlon"], ai["xlat"], ai["slmsk"], out=(da["faersw"], da["faerlw"]))  # noqa: E731
 
-        def tstep(fn, steps, warmup):
-            for _ in range(warmup):
-                fn()
-            torch.cuda.synchronize()
-            barrier()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(steps):
-                fn()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            barrier()
-            return max_over_ranks(e0.elapsed_time(e1) / steps)
-
         ms_a = tstep(opt, args.steps, args.warmup)
         ms_as = tstep(lambda: (opt(), mixed.solve(da, cols.solcon, out)), args.steps, args.warmup)
         nl = cols.nlay
@@ -407,6 +494,11 @@ def main():
                "frac": bpc * n / (ms_a * 1e-3) / 1e9 / hbm,
                "step_with_aerosol": {"value": ws * n / (ms_as * 1e-3), "unit": UNIT, "ms_per_step": ms_as}}
         del da, A
+
+    # grrad's front end of the same domain and the whole radiation call (front end + solve)
+    front_leg = None
+    if not args.no_front and args.ncol is None:
+        front_leg = front_block(mixed, cols, dev, seed + rank, tstep, args.steps, args.warmup)
 
     # roofline of the dominant kernel (FP32 pipe; algorithmic FLOPs from the oracle's operation-count table)
     pk = peaks()
@@ -477,6 +569,7 @@ def main():
                     "d2h_bytes_per_step": out_bytes, "ms_per_step": ms_e2e},
             "batch_c3": batch,
             "aerosols": aer,
+            "front_end": front_leg,
             "gpu_launches": launches,
             "clocks": clocks,
         }

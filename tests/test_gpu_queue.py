@@ -52,7 +52,6 @@ def test_submitted_requests_overlap_and_equal_solve():
     assert busy_seen                                   # 5 requests, 3 slots
     lib.rad_queue_destroy(q)
     torch.cuda.synchronize()
-    del s2
     ref = RadSolver(precision="mixed")
     for c, o in zip(reqs, outs):
         r = ref.solve_host(c)
