@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=40)
     ap.add_argument("--lw-chunk", type=int, default=None,
                     help="LW chunk size (columns); default: the autotuner's choice for this device")
+    ap.add_argument("--sw-chunk", type=int, default=None,
+                    help="SW tile of sunlit columns; default: the autotuner's choice (with --lw-chunk: 16384)")
     ap.add_argument("--ncol", type=int, default=None,
                     help="solve this many columns of the workload's generator instead of the full domain "
                          "(small cases for profiling)")
@@ -268,8 +270,10 @@ def front_block(mixed, cols, dev, seed: int, tstep, steps: int, warmup: int, im:
     tab_h = front_tables(seed + 2)
     tab = {k: (T(v) if isinstance(v, np.ndarray) else v) for k, v in tab_h.items()}
     tab["co2_glb"] = T(np.atleast_1d(np.float32(tab_h["co2_glb"])))
-    sun = solar.sol_update((2026, 7, 1, 18, 0, 0), deltsw=1200.0, deltim=25.0)
-    call = dict(solhr=18.0, dtswav=1200.0 / 3600.0, nrads=48)
+    # 12:40 UTC: the morning terminator crosses the middle of the grid, so about half of it is sunlit (as the
+    # solve's columns are) and the call's SW work compares with the solve's
+    sun = solar.sol_update((2026, 7, 1, 12, 40, 0), deltsw=1200.0, deltim=25.0)
+    call = dict(solhr=12.0 + 40.0 / 60.0, dtswav=1200.0 / 3600.0, nrads=48)
     f32 = dict(dtype=torch.float32, device=dev)
     gas, oz = torch.empty((10, lmk, n), **f32), torch.zeros((lmk, n), **f32)
     alb, ems = torch.empty((4, n), **f32), torch.empty(n, **f32)
@@ -308,10 +312,11 @@ def front_block(mixed, cols, dev, seed: int, tstep, steps: int, warmup: int, im:
     work, outs = first["work"], {k: v for k, v in first.items() if k != "work"}
     ms_call = tstep(lambda: radiation_call(mixed, state, clim, work=work, out=outs, **kw), steps, warmup)
     front_ms = sum(v["ms"] for k, v in kern.items() if k != "k_setalb(ialbflg 1)")
+    nday = int((dp["coszen"] >= 1e-4).sum().item())
     res = {"workload": f"{im}x{jm} columns x {lmk} layers, NAM settings (ico2flg 1, climatological ozone, Ferrier "
                        f"clouds, ialbflg 2, iemslw 1); seeded surface / cloud / climatology stand-ins",
            "kernels": kern, "front_end_ms": front_ms, "peak_gbs": hbm,
-           "radiation_call": {"value": n / (ms_call * 1e-3), "unit": UNIT, "ms_per_step": ms_call,
+           "radiation_call": {"value": n / (ms_call * 1e-3), "unit": UNIT, "ms_per_step": ms_call, "day_columns": nday,
                               "what": "chain.radiation_call: grrad set-up, dayparts, getozn, getgases, progcld2, "
                                       "setalb, setemis and the LW+SW solve of the whole domain, one stream, "
                                       "no row windows"}}
@@ -356,7 +361,10 @@ def main():
     from woof_nam_b200.solver import SolverConfig
     from woof_nam_b200.tune import tuned_config
     mcfg = SolverConfig(precision="mixed", diagnostic=stress)
-    mcfg = tuned_config(n, mcfg) if args.lw_chunk is None else SolverConfig(**{**mcfg.__dict__, "lw_chunk": args.lw_chunk})
+    if args.lw_chunk is None and args.sw_chunk is None:
+        mcfg = tuned_config(n, mcfg)
+    else:
+        mcfg = SolverConfig(**{**mcfg.__dict__, "lw_chunk": args.lw_chunk or 32768, "sw_sweep_chunk": args.sw_chunk or 0})
     mixed = RadSolver(mcfg)
     d = mixed.to_device(cols, device=dev)
     out = mixed.alloc_outputs(n, device=dev)

@@ -56,6 +56,48 @@ def test_fp64_stress_matches_oracle(stress):
     assert_within(out, ref, flux_tol=2e-3, heat_tol=2e-3, what="fp64 kernel, stress")
 
 
+def _absorbing_aerosol_columns():
+    """Clear columns under a strongly absorbing aerosol: optical depth 0.02 per layer and band, single-scattering
+    albedo 0.2, asymmetry 0.6 (faersw [3][14][nlay][ncol]).  Every layer's single-scattering albedo then stays
+    below 0.75 in every g-point, Rayleigh included."""
+    cols = make_columns(2048, 4242)
+    cols.clouds[:] = 0.0
+    fsw = np.zeros((3, 14, cols.nlay, cols.ncol), np.float32)
+    fsw[0], fsw[1], fsw[2] = 0.02, 0.2, 0.6
+    return cols, fsw
+
+
+def _solve_with_aerosol(cols, fsw, **kw):
+    import torch
+    s = _solver(**kw)
+    d = s.to_device(cols)
+    d["faersw"] = torch.as_tensor(fsw, device="cuda")
+    out = s.solve(d, cols.solcon)
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_delta_eddington_where_finite(precision):
+    """iswmode 1 (delta-Eddington).  The reference forms zgam2 = -0.25 - w (1 - zasy3)
+    (namgpu/kernels/phys_rrtm_sw_spcvrtc.cu:95-98, zasy3 = 0.75 g) where Joseph et al. (1976) have
+    -0.25 + w (1 - 0.75 g).  With that sign zgam1 + zgam2 = 1.5 - 2 w, so the layer's
+    sqrt((zgam1 - zgam2)(zgam1 + zgam2)) is NaN for a single-scattering albedo w above 0.75, and every sunlit
+    column of a realistic request is NaN in the reference, the float64 oracle and this library alike (the
+    reference's sign is kept: it defines the scheme being replaced).  Under the absorbing aerosol every w is
+    below 0.75 and the outputs are finite (heating up to ~110 K/day); there the FP64 kernel agrees with the
+    float64 oracle to float32 output rounding and the mixed kernel within the tolerances."""
+    cols, fsw = _absorbing_aerosol_columns()
+    ref = oracle.solve(cols, precision="double", iswmode=1, faersw=fsw)
+    day = cols.coszen >= np.float32(1e-4)
+    assert day.any() and np.isfinite(ref["htsw"]).all() and np.isfinite(ref["sfcfsw"]).all()
+    out = _solve_with_aerosol(cols, fsw, precision=precision, iswmode=1)
+    if precision == "fp64":
+        assert_within(out, ref, flux_tol=2e-3, heat_tol=1e-3, what="fp64 iswmode 1")
+    else:
+        assert_within(out, ref, what="mixed iswmode 1")
+
+
 @pytest.mark.parametrize("iswmode", [3])
 def test_other_two_stream_modes(iswmode):
     """Discrete ordinates (iswmode 3).  The reference's delta-Eddington branch (iswmode 1) forms
