@@ -614,7 +614,7 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                 // into the chunk scratch, then the adding sweeps one CTA per column
                 const int64_t swc = sw4_chunk(cfg);
                 const size_t smem0 = sw4_gas_smem(any_aer);
-                const size_t smem1 = sizeof(SwSh2) + (any_aer ? sizeof(SwAer) : 0);
+                const size_t smem1 = sw4_gas_smem(any_aer);   // the image without taug (read from the image)
                 const size_t smem2 = (size_t)(SW2_NSEG - 1) * 4 * SW2_THREADS * sizeof(float);
                 const size_t bb = sw4_block_bytes(nlay);
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw4_gas_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem0));

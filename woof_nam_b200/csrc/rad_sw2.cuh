@@ -644,7 +644,8 @@ __device__ __forceinline__ bool sw2_cloud_layer(const SwSh2& s, bool mc, int g, 
 }
 
 __device__ __noinline__ SwLayerRT2 sw2_layer(const SwSh2& s, const SwAer* aer, const SwExactCtx& x, int k0, int g,
-                                             int ib, bool cloudy, bool mc, float cz, float snt, const float* ex)
+                                             int ib, bool cloudy, bool mc, float cz, float snt, const float* ex,
+                                             float tg)
 {
     SwLayerRT2 r;
     SwLayerRT& c = r.c;
@@ -654,7 +655,7 @@ __device__ __noinline__ SwLayerRT2 sw2_layer(const SwSh2& s, const SwAer* aer, c
         o = c;
         return r;
     }
-    const float tr = sw2_taur(s, g, k0), tg = s.taug[g][k0];
+    const float tr = sw2_taur(s, g, k0);
     float ta = 0, tasa = 0, tay = 0, taab = 0;
     if (aer) { ta = aer->tau[ib][k0]; tasa = aer->tasa[ib][k0]; tay = aer->tay[ib][k0]; taab = aer->tabs[ib][k0]; }
     const float ct0 = fmaxf(1.0e-12f, tr + tg + ta), cs0 = tr + tasa, cy0 = tay, cab = tg + taab;
@@ -887,7 +888,7 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
         float e4c = 1, e4o = 1;
         for (int j = 0; j < SW2_SEG; ++j) {
             const int k0 = sg * SW2_SEG + j;
-            const SwLayerRT2 L = sw2_layer(s, aer, x, k0, g, ib0, cloudy, mc, cz, snt, ex);
+            const SwLayerRT2 L = sw2_layer(s, aer, x, k0, g, ib0, cloudy, mc, cz, snt, ex, s.taug[g][k0]);
             sw2_up(L.c, ubc, udc);
             if (cloudy) sw2_up(L.o, ubo, udo);
             if (STORE) {
@@ -958,7 +959,8 @@ __device__ __forceinline__ void sw2_column(const SwBatch& bt, int any_aer, const
 #pragma unroll
         for (int j = 0; j < SW2_SEG; ++j) {
             if (!STORE) {
-                const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, mc, cz, snt, ex);
+                const SwLayerRT2 L = sw2_layer(s, aer, x, sg * SW2_SEG + j, g, ib0, cloudy, mc, cz, snt, ex,
+                                               s.taug[g][sg * SW2_SEG + j]);
                 Lc[j] = L.c;
                 Lo[j] = L.o;
                 e4c = e4c * Lc[j].e4;

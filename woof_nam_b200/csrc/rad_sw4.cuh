@@ -28,7 +28,8 @@ namespace rad {
 
 constexpr int SW4_FIELDS = 6;                       // rb, rd, tb, td, e3 (delta-scaled beam), e4 (unscaled beam)
 constexpr int SW4_LAYER = SW4_FIELDS * SW_NGPT;     // floats per layer and pass, [field][g]
-constexpr int SW4_OPT_MINB = 3;                     // CTAs per SM the R/T kernel is compiled for
+constexpr int SW4_OPT_MINB = 4;                     // CTAs per SM the R/T kernel is compiled for
+constexpr bool SW4_RT_PAIR = false;                 // two R/T tasks per thread side by side (else one)
 constexpr int SW4_SWEEP_MINB = 4;                   // ... and the sweep kernel
 
 struct Sw4Hdr {
@@ -153,6 +154,14 @@ static_assert(offsetof(SwSh2, taug) + sizeof(SwSh2::taug) == sizeof(SwSh2) && si
 // where taug would be.
 __host__ __device__ constexpr size_t sw4_gas_smem(bool aer) { return offsetof(SwSh2, taug) + (aer ? sizeof(SwAer) : 0); }
 
+// The image's taug part holds the gas optical depths as [layer][g-point]: the R/T kernel reads them straight from
+// the image, 32 consecutive (layer, g-point) tasks per warp on one 128-byte line, instead of staging them.
+static_assert((size_t)NLAY_MAX * SW_NGPT * sizeof(float) <= sizeof(SwSh2::taug), "[layer][g] fits the taug part");
+__host__ __device__ inline const float* sw4_image_taug(const int4* im)
+{
+    return reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(im) + (offsetof(SwSh2, taug) - sw4_image_begin()));
+}
+
 // Set-up, cloud optics and gas optics of one sunlit column (one CTA, five per SM) into its image.
 __global__ void __launch_bounds__(SW2_THREADS, 5)
 sw4_gas_kernel(const __grid_constant__ SwBatch bt, int any_aer, int* err, int d0, int4* img)
@@ -178,7 +187,7 @@ sw4_gas_kernel(const __grid_constant__ SwBatch bt, int any_aer, int* err, int d0
     for_each_band_pair(c_sw_ns, 14, nlay, &s.task_next, tid & 31, [&](int g, int k0, int b) {
         float tg, tr;
         sw_gas<float>(s, g, k0, tg, tr, b);
-        img_taug[g * SW2_KS + k0] = tg;
+        img_taug[k0 * SW_NGPT + g] = tg;
         if (g >= 66 && g < 74 && k0 < s.laytrop) s.taur24[g - 66][k0] = tr;
     });
     __syncthreads();
@@ -203,14 +212,20 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
     const SwIn& a = bt.req[rq];
     const int nlay = a.nlay;
     if (nlay > NLAY_MAX) return;                                   // flagged by the gas-optics kernel
-    SwAer* aer = a.faersw ? reinterpret_cast<SwAer*>(smem_raw + sizeof(SwSh2)) : nullptr;
+    SwAer* aer = a.faersw ? reinterpret_cast<SwAer*>(smem_raw + offsetof(SwSh2, taug)) : nullptr;
     const int64_t col = gcol - bt.off[rq];
     const int tid = threadIdx.x;
-    {   // the column's image into shared memory, every 16-byte piece in flight at once (cp.async.cg: L2 to shared)
-        const int4* im = img + (size_t)blockIdx.x * (sw4_image_bytes(any_aer) / 16);
+    const int4* im = img + (size_t)blockIdx.x * (sw4_image_bytes(any_aer) / 16);
+    const float* tgi = sw4_image_taug(im);   // [layer][g], read from the image as the tasks need it
+    {   // the rest of the image into shared memory (the aerosol block where taug would be), every 16-byte piece
+        // in flight at once (cp.async.cg: L2 to shared)
         const uint32_t sb = (uint32_t)__cvta_generic_to_shared(smem_raw + sw4_image_begin());
-        for (int i = tid; i < (int)(sw4_image_bytes(any_aer) / 16); i += SW2_THREADS)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sb + 16u * (uint32_t)i), "l"(im + i)
+        const int n1 = (int)((offsetof(SwSh2, taug) - sw4_image_begin()) / 16);
+        const int n2 = any_aer ? (int)(sizeof(SwAer) / 16) : 0;
+        const int skip = (int)(sizeof(SwSh2::taug) / 16);
+        for (int i = tid; i < n1 + n2; i += SW2_THREADS)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sb + 16u * (uint32_t)i),
+                         "l"(im + (i < n1 ? i : i + skip))
                          : "memory");
         asm volatile("cp.async.wait_all;" ::: "memory");
         __syncthreads();
@@ -270,7 +285,7 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
         const float zsolar = s.ssolar * s.sfluxzen[g];
         const SwExactCtx x{&a, col, s.laytrop, s.kmin8, s.kminw, a.iswmode, czd, 1.0 / czd, exd,
                            zsolar * (1.5f * 86400.0f / SW2_HEAT_T), zsolar * (1.0f / SW2_FLUX_T)};
-        store(k0, g, sw2_layer(s, aer, x, k0, g, ib, cloudy, mc, cz, snt, ex));
+        store(k0, g, sw2_layer(s, aer, x, k0, g, ib, cloudy, mc, cz, snt, ex, __ldg(tgi + i)));
     };
     // ---- layer R/T in two passes over the column, each with lanes on 32 consecutive (layer, g-point) tasks and
     // two tasks per thread side by side; a task whose R/T needs a float64 step or a table-entry test is queued
@@ -292,7 +307,7 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
     auto inputs = [&](int i, float& t0, float& ab, float& s0, float& y0, int& ib) {
         const int k0 = i / SW_NGPT, g = i - k0 * SW_NGPT;
         ib = gband[g];
-        const float tr = sw2_taur(s, g, k0), tg = s.taug[g][k0];
+        const float tr = sw2_taur(s, g, k0), tg = __ldg(tgi + i);
         float ta = 0, tasa = 0, tay = 0, taab = 0;
         if (aer) { ta = aer->tau[ib][k0]; tasa = aer->tasa[ib][k0]; tay = aer->tay[ib][k0]; taab = aer->tabs[ib][k0]; }
         t0 = fmaxf(1.0e-12f, tr + tg + ta); s0 = tr + tasa; y0 = tay; ab = tg + taab;
@@ -314,7 +329,20 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
         constexpr int MODE = decltype(mode_tag)::value;
         const int nt = nlay * SW_NGPT;
         // clear pass
-        for (int i0 = tid; i0 < nt; i0 += 2 * SW2_THREADS) {
+        if constexpr (!SW4_RT_PAIR) {
+            for (int i0 = tid; i0 < nt; i0 += SW2_THREADS) {
+                float t0a, aba, s0a, y0a, wka, wfa;
+                int iba;
+                inputs(i0, t0a, aba, s0a, y0a, iba);
+                weights(i0, wka, wfa);
+                SwLayerRT ra;
+                bool oka;
+                sw4_rt<MODE>(t0a, aba, s0a, y0a, cz, snt, wka, wfa, ra, oka);
+                put(rtc, i0, ra);
+                if (!oka) enqueue(i0);
+            }
+        }
+        for (int i0 = tid; SW4_RT_PAIR && i0 < nt; i0 += 2 * SW2_THREADS) {
             const int i1 = min(i0 + SW2_THREADS, nt - 1);
             float t0a, aba, s0a, y0a, t0b, abb, s0b, y0b, wka, wfa, wkb, wfb;
             int iba, ibb;
@@ -367,7 +395,20 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
                 o.e4 = zc0 * c.e4 + zc1 * m.e4;
             }
         };
-        for (int j0 = tid; j0 < nc2; j0 += 2 * SW2_THREADS) {
+        if constexpr (!SW4_RT_PAIR) {
+            for (int j0 = tid; j0 < nc2; j0 += SW2_THREADS) {
+                SwLayerRT oa;
+                bool oka;
+                int ia;
+                mix(j0, oa, oka, ia);
+                const int k0 = ia / SW_NGPT, g = ia - k0 * SW_NGPT;
+                if (!(qbit[k0][g >> 5] & (1u << (g & 31)))) {
+                    put(rto, (int)(slot[k0]) * SW_NGPT + g, oa);
+                    if (!oka) enqueue(ia);
+                }
+            }
+        }
+        for (int j0 = tid; SW4_RT_PAIR && j0 < nc2; j0 += 2 * SW2_THREADS) {
             const int j1 = min(j0 + SW2_THREADS, nc2 - 1);
             SwLayerRT oa, ob;
             bool oka, okb;
