@@ -42,8 +42,12 @@ __device__ __forceinline__ float rpow(float x, float y) { return powf(x, y); }
 __device__ __forceinline__ double rpow(double x, double y) { return pow(x, y); }
 __device__ __forceinline__ float sqrtR(float x) { return sqrtf(x); }
 __device__ __forceinline__ double sqrtR(double x) { return sqrt(x); }
-__device__ __forceinline__ float rfmod1(float x) { return fmodf(x, 1.0f); }
-__device__ __forceinline__ double rfmod1(double x) { return fmod(x, 1.0); }
+// MOD(x, 1.0): by fmod's definition x - n with n = trunc(x / 1) = trunc(x).  The subtraction is exact for every
+// finite x (x and trunc(x) share x's exponent range and the difference is its fraction bits), and inf / NaN give
+// NaN as fmod does, so this is fmod(x, 1) bit for bit -- at two instructions instead of the library's general
+// remainder loop, in the per-(g-point, layer) species keys of the gas optics.
+__device__ __forceinline__ float rfmod1(float x) { return x - truncf(x); }
+__device__ __forceinline__ double rfmod1(double x) { return x - trunc(x); }
 
 // t(ig, ind) + frac * (t(ig, ind+1) - t(ig, ind)) for a [ind][g] table, 1-based ind.
 template <class R>

@@ -19,6 +19,8 @@ namespace rad {
 constexpr int LW_THREADS = 160;     // 5 warps: lanes 0..139 carry g-points in the sweeps
 constexpr int LW_WARPS = LW_THREADS / 32;
 
+constexpr int LW_NADJ = 5;    // adjcol terms per layer: bands 3 and 9 (same term), 6, 7, 8, 13
+constexpr int LW_NCHIR = 11;  // chi ratios: band 3 (3), 7, 9 (2), 12, 16, 13 (3)
 template <class R>
 struct LwSetup {
     R pavel[NLAY_MAX], tavel[NLAY_MAX], coldry[NLAY_MAX], colbrd[NLAY_MAX], h2ovmr[NLAY_MAX], delp[NLAY_MAX];
@@ -40,6 +42,11 @@ struct LwSetup {
     R stemp, pwvcm;
     int laytrop, lcf1;
     int task_next;            // phase B task counter (for_each_band_pair)
+    // per-layer and per-column terms of the band kernels that do not depend on the g-point, formed once in phase
+    // A2 instead of in every (g-point, layer) task: the minor-gas column adjustments (adjcol) of bands 3 / 9, 6,
+    // 7, 8, 13, and the ratios of reference mixing ratios (chi) that key the minor / Planck-fraction species
+    R adjc[LW_NADJ][NLAY_MAX];
+    R chir[LW_NCHIR];
 };
 
 // The single-kernel layout: set-up data plus the column's gas optics and the sweeps' partial sums.
@@ -138,8 +145,6 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
     const int inds = s.indself[k0], indf = s.indfor[k0], indm = s.indminor[k0];
     const R sfac = s.selffac[k0], sfr = s.selffrac[k0], ffac = s.forfac[k0], ffr = s.forfrac[k0],
             mf = s.minorfrac[k0];
-    const R* chi = tab<R>(T_LW_CHI_MLS);
-    auto CHI = [&](int gg, int lev) { return ldt(chi + ((lev - 1) * 7 + (gg - 1))); };
     auto A4 = [&](const R* t, int ng, int ig, int i0, int i1) {
         auto a = [&](int id) { return ldt(t + ((id - 1) * ng + ig)); };
         return f00 * a(i0) + f10 * a(i0 + 1) + f01 * a(i1) + f11 * a(i1 + 1);
@@ -193,10 +198,10 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
         const R *absa = tab<R>(b3 ? T_LW03_ABSA : T_LW04_ABSA), *absb = tab<R>(b3 ? T_LW03_ABSB : T_LW04_ABSB),
                 *fa = tab<R>(b3 ? T_LW03_FRACREFA : T_LW04_FRACREFA), *fb = tab<R>(b3 ? T_LW03_FRACREFB : T_LW04_FRACREFB);
         R rpa, rpb, rma = 0, rmb = 0;
-        if (b3) { rpa = CHI(1, 9) / CHI(2, 9); rpb = CHI(1, 13) / CHI(2, 13); rma = CHI(1, 3) / CHI(2, 3); rmb = CHI(1, 13) / CHI(2, 13); }
+        if (b3) { rpa = s.chir[0]; rpb = s.chir[1]; rma = s.chir[2]; rmb = s.chir[1]; }
         else { rpa = (R)c_lwk.b4_rpa; rpb = (R)c_lwk.b4_rpb; }
         R adjn2o = 0;
-        if (b3) adjn2o = adjcol(s.colamt[3][k0], s.coldry[k0] * CHI(4, jpk + 1), (R)1.5f, (R)0.5f, (R)0.65f);
+        if (b3) adjn2o = s.adjc[0][k0];
         if (low) {
             R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fmn = 0, fpl;
             int js, js1, jmn = 1, jpl;
@@ -289,7 +294,7 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
         const R wx2 = s.wx[1][k0], wx3 = s.wx[2][k0];
         const R xsec = wx2 * ldt(tab<R>(T_LW06_CFC11ADJ) + ig) + wx3 * ldt(tab<R>(T_LW06_CFC12) + ig);
         if (low) {
-            const R adj = adjcol(s.colamt[1][k0], s.coldry[k0] * CHI(2, jpk + 1), (R)3, (R)2, (R)0.77f);
+            const R adj = s.adjc[1][k0];
             const R tauself = sfac * interp(tab<R>(T_LW06_SELFREF), NG, inds, ig, sfr);
             const R taufor = ffac * interp(tab<R>(T_LW06_FORREF), NG, indf, ig, ffr);
             const R absco2 = interp(tab<R>(T_LW06_KA_MCO2), NG, indm, ig, mf);
@@ -302,17 +307,16 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
     }
     case 7: {
         const int NG = 12;
-        const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0], c3 = s.colamt[2][k0];
-        const R temp = s.coldry[k0] * CHI(2, jpk + 1);
+        const R c1 = s.colamt[0][k0], c3 = s.colamt[2][k0];
         if (low) {
-            const R rr = CHI(1, 3) / CHI(3, 3);
+            const R rr = s.chir[3];
             R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fm, fpl;
             int js, js1, jm, jpl;
             spec(c1, s.rfrate[0][1][k0], c3, (R)8, sc, sp, js, fs);
             spec(c1, s.rfrate[1][1][k0], c3, (R)8, sc1, sp1, js1, fs1);
             spec(c1, rr, c3, (R)8, scm, spm, jm, fm);
             spec(c1, rr, c3, (R)8, scp, spp, jpl, fpl);
-            const R adj = adjcol(c2, temp, (R)3, (R)3, (R)0.79f);
+            const R adj = s.adjc[2][k0];
             const int br = br_joint(sp, sp1);
             const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
             const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
@@ -322,7 +326,7 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
                  adj * minor2d(tab<R>(T_LW07_KA_MCO2), 9, NG, jm, fm, indm, mf, ig);
             fr = interp(tab<R>(T_LW07_FRACREFA), NG, jpl, ig, fpl);
         } else {
-            const R adj = adjcol(c2, temp, (R)3, (R)2, (R)0.79f);
+            const R adj = s.adjc[2][k0];
             const R absco2 = interp(tab<R>(T_LW07_KB_MCO2), NG, indm, ig, mf);
             tg = c3 * A4(tab<R>(T_LW07_ABSB), NG, ig, ind0u, ind1u) + adj * absco2;
             if (ig >= 5 && ig <= 10) {
@@ -335,7 +339,7 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
     }
     case 8: {
         const int NG = 8;
-        const R adj = adjcol(s.colamt[1][k0], s.coldry[k0] * CHI(2, jpk + 1), (R)3, (R)2, (R)0.65f);
+        const R adj = s.adjc[3][k0];
         const R xsec = s.wx[2][k0] * ldt(tab<R>(T_LW08_CFC12) + ig) + s.wx[3][k0] * ldt(tab<R>(T_LW08_CFC22ADJ) + ig);
         if (low) {
             const R tauself = sfac * interp(tab<R>(T_LW08_SELFREF), NG, inds, ig, sfr);
@@ -357,10 +361,10 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
     }
     case 9: {
         const int NG = 12;
-        const R c1 = s.colamt[0][k0], c4 = s.colamt[3][k0], c5 = s.colamt[4][k0];
-        const R adj = adjcol(c4, s.coldry[k0] * CHI(4, jpk + 1), (R)1.5f, (R)0.5f, (R)0.65f);
+        const R c1 = s.colamt[0][k0], c5 = s.colamt[4][k0];
+        const R adj = s.adjc[0][k0];
         if (low) {
-            const R rpa = CHI(1, 9) / CHI(6, 9), rma = CHI(1, 3) / CHI(6, 3);
+            const R rpa = s.chir[4], rma = s.chir[5];
             R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fm, fpl;
             int js, js1, jm, jpl;
             spec(c1, s.rfrate[0][3][k0], c5, (R)8, sc, sp, js, fs);
@@ -415,7 +419,7 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
         if (low) {
             const R c1 = s.colamt[0][k0], c2 = b12 ? s.colamt[1][k0] : s.colamt[4][k0];
             const int rate = b12 ? 0 : 3;
-            const R rpa = b12 ? CHI(1, 10) / CHI(2, 10) : CHI(1, 6) / CHI(6, 6);
+            const R rpa = b12 ? s.chir[6] : s.chir[7];
             R sc, sp, sc1, sp1, fs, fs1;
             int js, js1;
             spec(c1, s.rfrate[0][rate][k0], c2, (R)8, sc, sp, js, fs);
@@ -446,8 +450,8 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
     case 13: {
         const int NG = 4;
         if (low) {
-            const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0], c4 = s.colamt[3][k0], c7 = s.colamt[6][k0];
-            const R rpa = CHI(1, 5) / CHI(4, 5), rma = CHI(1, 1) / CHI(4, 1), rma3 = CHI(1, 3) / CHI(4, 3);
+            const R c1 = s.colamt[0][k0], c4 = s.colamt[3][k0], c7 = s.colamt[6][k0];
+            const R rpa = s.chir[8], rma = s.chir[9], rma3 = s.chir[10];
             R sc, sp, sc1, sp1, scm, spm, scc, spc, scp, spp, fs, fs1, fm, fmc, fpl;
             int js, js1, jm, jmc, jpl;
             spec(c1, s.rfrate[0][2][k0], c4, (R)8, sc, sp, js, fs);
@@ -455,7 +459,7 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
             spec(c1, rma, c4, (R)8, scm, spm, jm, fm);
             spec(c1, rma3, c4, (R)8, scc, spc, jmc, fmc);
             spec(c1, rpa, c4, (R)8, scp, spp, jpl, fpl);
-            const R adj = adjcol(c2, s.coldry[k0] * (R)3.55e-4f, (R)3, (R)2, (R)0.68f);
+            const R adj = s.adjc[4][k0];
             const int br = br_joint(sp, sp1);
             const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
             const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
@@ -707,6 +711,35 @@ __device__ __forceinline__ void lw_setcoef_layer(S& s, int k0)
     s.forfac[k0] = s.colamt[0][k0] * forf;
 }
 
+// The g-point-independent terms of the band kernels for layer k0 (after setcoef): the minor-gas column
+// adjustments of taugb03 / taugb09 (N2O), taugb06, taugb07, taugb08 (CO2) and taugb13 (CO2), each the statement
+// of its band kernel (adjcol), evaluated once per layer rather than in every g-point's task.
+template <class R, class S>
+__device__ __forceinline__ void lw_keys_layer(S& s, int k0)
+{
+    const R* chi = tab<R>(T_LW_CHI_MLS);
+    auto CHI = [&](int gg, int lev) { return ldt(chi + ((lev - 1) * 7 + (gg - 1))); };
+    const int jpk = s.jp[k0];
+    const R c2 = s.colamt[1][k0], c4 = s.colamt[3][k0], dry = s.coldry[k0];
+    const R t2 = dry * CHI(2, jpk + 1);
+    s.adjc[0][k0] = adjcol(c4, dry * CHI(4, jpk + 1), (R)1.5f, (R)0.5f, (R)0.65f);
+    s.adjc[1][k0] = adjcol(c2, t2, (R)3, (R)2, (R)0.77f);
+    s.adjc[2][k0] = s.lower[k0] ? adjcol(c2, t2, (R)3, (R)3, (R)0.79f) : adjcol(c2, t2, (R)3, (R)2, (R)0.79f);
+    s.adjc[3][k0] = adjcol(c2, t2, (R)3, (R)2, (R)0.65f);
+    s.adjc[4][k0] = adjcol(c2, dry * (R)3.55e-4f, (R)3, (R)2, (R)0.68f);
+}
+// The column-independent ratios of reference mixing ratios the band kernels key their minor-gas and Planck-
+// fraction species by (taugb03, 07, 09, 12, 13, 16), formed once per column by threads 0..LW_NCHIR-1.
+template <class R, class S>
+__device__ __forceinline__ void lw_chi_ratio(S& s, int i)
+{
+    const R* chi = tab<R>(T_LW_CHI_MLS);
+    auto CHI = [&](int gg, int lev) { return ldt(chi + ((lev - 1) * 7 + (gg - 1))); };
+    const int num[LW_NCHIR] = {1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1}, den[LW_NCHIR] = {2, 2, 2, 3, 6, 6, 2, 6, 4, 4, 4};
+    const int lev[LW_NCHIR] = {9, 13, 3, 3, 9, 3, 10, 6, 5, 1, 3};
+    s.chir[i] = CHI(num[i], lev[i]) / CHI(den[i], lev[i]);
+}
+
 // Planck functions of band i at level / layer k (k = 0: the surface; phys_rrtm_lw_setcoef.cu:135-160).
 template <class R>
 __device__ __forceinline__ void lw_planck(const LwIn& a, int64_t col, int k, int i, R& lay, R& lev)
@@ -869,7 +902,9 @@ __device__ void lw_setup_core(LwSetup<R>& s, const LwIn& a, int64_t col, int tid
     for (int k0 = tid; k0 < nlay; k0 += NT) {
         lw_cldprop_layer<R>(s, a, col, k0, s.lcf1, ilwcliq);
         lw_setcoef_layer<R>(s, k0);
+        lw_keys_layer<R>(s, k0);
     }
+    if (tid < LW_NCHIR) lw_chi_ratio<R>(s, tid);
     // Planck functions at levels 0..nlay and bands (setcoef.cu:135-160)
     {
         for (int p = tid; p < nlp1 * 16; p += NT) {

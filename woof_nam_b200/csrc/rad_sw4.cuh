@@ -4,7 +4,7 @@
 // Same statements as sw2_column (rad_sw2.cuh), split where the work changes shape, and each kernel small enough
 // that the CTAs resident on an SM run out of the instruction cache (one kernel with all three phases spent most
 // of its stalls waiting for instructions):
-//  * sw4_gas_kernel, one CTA (128 threads) per sunlit column, five per SM: set-up and cloud optics
+//  * sw4_gas_kernel, one CTA (128 threads) per sunlit column, six per SM: set-up and cloud optics
 //    (sw2_setup), gas and Rayleigh optical depths per (g-point, layer); writes the column image (the part of the
 //    shared-memory layout the later phases read, taug included).
 //  * sw4_rt_kernel, one CTA per column: loads the image, then the layer R/T of the clear pass and, in the
@@ -30,7 +30,8 @@ constexpr int SW4_FIELDS = 6;                       // rb, rd, tb, td, e3 (delta
 constexpr int SW4_LAYER = SW4_FIELDS * SW_NGPT;     // floats per layer and pass, [field][g]
 constexpr int SW4_OPT_MINB = 4;                     // CTAs per SM the R/T kernel is compiled for
 constexpr bool SW4_RT_PAIR = false;                 // two R/T tasks per thread side by side (else one)
-constexpr int SW4_SWEEP_MINB = 4;                   // ... and the sweep kernel
+constexpr int SW4_SWEEP_MINB = 6;                   // ... and the sweep kernel
+constexpr int SW4_GAS_MINB = 6;                     // ... and the gas-optics kernel
 
 struct Sw4Hdr {
     double rdelp[NLAY_MAX];          // heatfac / delp, float64
@@ -162,8 +163,8 @@ __host__ __device__ inline const float* sw4_image_taug(const int4* im)
     return reinterpret_cast<const float*>(reinterpret_cast<const unsigned char*>(im) + (offsetof(SwSh2, taug) - sw4_image_begin()));
 }
 
-// Set-up, cloud optics and gas optics of one sunlit column (one CTA, five per SM) into its image.
-__global__ void __launch_bounds__(SW2_THREADS, 5)
+// Set-up, cloud optics and gas optics of one sunlit column (one CTA, six per SM) into its image.
+__global__ void __launch_bounds__(SW2_THREADS, SW4_GAS_MINB)
 sw4_gas_kernel(const __grid_constant__ SwBatch bt, int any_aer, int* err, int d0, int4* img)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
