@@ -452,6 +452,26 @@ def main():
     barrier()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1) / args.steps)
 
+    # the same, double-buffered through the public HostPipeline: each step's host->device copy overlaps the previous
+    # step's solve and its device->host copy the next one's (two device buffer sets, three streams)
+    from woof_nam_b200.pipeline import HostPipeline
+    pipe = HostPipeline(mixed, n, depth=2, device=dev)
+    for _ in range(args.warmup):
+        pipe.submit(hin, cols.solcon, hout)
+    pipe.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    pipe.start_after(stream)
+    for _ in range(args.steps):
+        pipe.submit(hin, cols.solcon, hout)
+    pipe.wait_on(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms_pipe = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    del pipe
+
     # uneven batch: the parent grid plus the 3 km nests (333x333, 600x450, 180x180) as one batched solve
     # captured in a CUDA graph, replayed per step; the nests' inputs are resident too
     batch = None
@@ -573,8 +593,13 @@ def main():
             "cpu_baseline": cpu,
             "parity": parity,
             "serving": serving,
-            "e2e": {"value": ws * n / (ms_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": in_bytes,
-                    "d2h_bytes_per_step": out_bytes, "ms_per_step": ms_e2e},
+            "e2e": {"value": ws * n / (ms_pipe * 1e-3), "unit": UNIT, "h2d_bytes_per_step": in_bytes,
+                    "d2h_bytes_per_step": out_bytes, "ms_per_step": ms_pipe,
+                    "how": "woof_nam_b200.pipeline.HostPipeline: every step copies its inputs from pinned host "
+                           "memory and its outputs back, overlapped with the neighbouring steps' solves (two "
+                           "device buffer sets)",
+                    "serial": {"value": ws * n / (ms_e2e * 1e-3), "ms_per_step": ms_e2e,
+                               "how": "RadSolver.solve between the two copies on one stream"}},
             "batch_c3": batch,
             "aerosols": aer,
             "front_end": front_leg,
