@@ -49,6 +49,16 @@ __device__ __forceinline__ double sqrtR(double x) { return sqrt(x); }
 __device__ __forceinline__ float rfmod1(float x) { return x - truncf(x); }
 __device__ __forceinline__ double rfmod1(double x) { return x - trunc(x); }
 
+// Bulk prefetch of [p, p + bytes) from global memory into L2 (cp.async.bulk.prefetch.L2, no shared memory, no
+// multicast): one instruction brings a contiguous run of a column's scratch in ahead of the loads that read it.
+// p must be 16-byte aligned and bytes a multiple of 16; the range must lie inside one allocation.
+__device__ __forceinline__ void l2_prefetch(const void* p, uint32_t bytes)
+{
+    if (bytes == 0) return;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(bytes)
+                 : "memory");
+}
+
 // t(ig, ind) + frac * (t(ig, ind+1) - t(ig, ind)) for a [ind][g] table, 1-based ind.
 template <class R>
 __device__ __forceinline__ R interp(const R* t, int ng, int ind, int ig, R frac)

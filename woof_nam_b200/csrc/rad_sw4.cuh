@@ -32,6 +32,7 @@ constexpr int SW4_OPT_MINB = 4;                     // CTAs per SM the R/T kerne
 constexpr bool SW4_RT_PAIR = false;                 // two R/T tasks per thread side by side (else one)
 constexpr int SW4_SWEEP_MINB = 6;                   // ... and the sweep kernel
 constexpr int SW4_GAS_MINB = 6;                     // ... and the gas-optics kernel
+constexpr bool SW4_L2PF = true;                     // the sweeps prefetch the R/T rows two segments ahead into L2
 
 struct Sw4Hdr {
     double rdelp[NLAY_MAX];          // heatfac / delp, float64
@@ -527,9 +528,25 @@ sw4_sweep_kernel(const __grid_constant__ SwBatch bt, int* err, int d0, int nc, c
             o = c;
         }
     };
+    // The R/T rows of segment sg into L2 ahead of its loads (thread 0, one bulk prefetch per pass): the clear rows
+    // of its layers and the cloudy rows of their slots, each a contiguous run inside the column's block.
+    auto prefetch = [&](int sg) {
+        if (!SW4_L2PF || tid != 0 || sg < 0 || sg >= nseg) return;
+        const int k0 = sg * SW2_SEG, k1 = min(nlay, k0 + SW2_SEG);
+        if (k0 >= k1) return;
+        l2_prefetch(rtc + (size_t)k0 * SW4_LAYER, (uint32_t)((k1 - k0) * SW4_LAYER * sizeof(float)));
+        if (!cloudy) return;
+        int s0 = -1, s1 = -1;
+        for (int k = k0; k < k1; ++k)
+            if (H.slot[k] >= 0) { if (s0 < 0) s0 = H.slot[k]; s1 = H.slot[k]; }
+        if (s0 >= 0) l2_prefetch(rto + (size_t)s0 * SW4_LAYER, (uint32_t)((s1 - s0 + 1) * SW4_LAYER * sizeof(float)));
+    };
     // ---- upward sweep: reflectances of the atmosphere below each level, clear (c) and cloudy (o) passes
     float ubc = ab, udc = ad, ubo = ab, udo = ad;
+    prefetch(0);
+    prefetch(1);
     for (int sg = 0; sg < nseg; ++sg) {
+        prefetch(sg + 2);
         if (sg > 0) { CK(sg, 0) = ubc; CK(sg, 1) = udc; CK(sg, 2) = ubo; CK(sg, 3) = udo; }
         SwLayerRT Lc[SW2_SEG], Lo[SW2_SEG];
 #pragma unroll
@@ -545,7 +562,9 @@ sw4_sweep_kernel(const __grid_constant__ SwBatch bt, int* err, int d0, int nc, c
     const double w0 = cloudy ? (mc ? 0.0 : (double)H.zcf0) : 1.0, w1 = cloudy ? (mc ? 1.0 : (double)H.zcf1) : 0.0;
     float tdnc = 1, rdnc = 0, tdbc = 1, tdbc0 = 1, tdno = 1, rdno = 0, tdbo = 1, tdbo0 = 1;
     float toa_c = 0, toa_o = 0;
+    prefetch(nseg - 2);
     for (int sg = nseg - 1; sg >= 0; --sg) {
+        prefetch(sg - 2);
         SwLayerRT Lc[SW2_SEG], Lo[SW2_SEG];
         float zubc[SW2_SEG + 1], zudc[SW2_SEG + 1], zubo[SW2_SEG + 1], zudo[SW2_SEG + 1];
         zubc[0] = sg ? CK(sg, 0) : ab;
