@@ -223,9 +223,9 @@ __device__ __forceinline__ R lw3_step(float& rtot, float& rclr, float& trad, flo
     return inc;
 }
 
-// The sweeps stream each layer's taug row, fracs row and record (400 floats) through a three-stage ring in
-// shared memory with asynchronous 16-byte copies (cp.async.cg: L2 to shared, no L1 allocation), two layers
-// ahead of the one being computed, so the scratch's DRAM latency overlaps the arithmetic.
+// The sweeps stream each layer's taug row, fracs row and record (400 floats) through a LW3_NSTAGE-stage ring in
+// shared memory with asynchronous 16-byte copies (cp.async.cg: L2 to shared, no L1 allocation), LW3_NSTAGE - 1
+// layers ahead of the one being computed, so the scratch's DRAM latency overlaps the arithmetic.
 constexpr int LW3_STAGE = 2 * LW3_GSTRIDE + LW3_REC;   // floats per stage
 constexpr int LW3_NSTAGE = 3;
 
@@ -282,8 +282,8 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
     // sweep steps: s = 0 .. nlay-1 downward (layer nlay - s), s = nlay .. 2 nlay - 1 upward (layer s - nlay + 1)
     const int nstep = 2 * nlay;
     auto layer_of = [&](int st) { return st < nlay ? nlay - st : st - nlay + 1; };
-    lw3_stage_layer(ring[warp][0], tg, fr, aux, layer_of(0), lane);
-    lw3_stage_layer(ring[warp][1], tg, fr, aux, layer_of(1), lane);
+#pragma unroll
+    for (int q = 0; q < LW3_NSTAGE - 1; ++q) lw3_stage_layer(ring[warp][q], tg, fr, aux, layer_of(q), lane);
     const float eps = 1.0e-6f;
     int gi[LW3_SLOTS], band[LW3_SLOTS];
     float sdif[LW3_SLOTS];
@@ -338,16 +338,18 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
         }
         return warp_sum(sum);
     };
-    // ---- the sweeps: downward, the surface, upward; layer s + 2 is copied in while layer s computes
+    // ---- the sweeps: downward, the surface, upward; layer s + LW3_NSTAGE - 1 is copied in while layer s computes
 #pragma unroll
     for (int j = 0; j < LW3_SLOTS; ++j) { radtot[j] = 0; radclr[j] = 0; trad[j] = 0; crad[j] = 0; rad[j] = 0; }
     double s_tu = 0, s_cu = 0, s_td = 0, s_cd = 0;
     for (int st = 0; st < nstep; ++st) {
-        if (st + 2 < nstep)
-            lw3_stage_layer(ring[warp][(st + 2) % LW3_NSTAGE], tg, fr, aux, layer_of(st + 2), lane);
+        if (st + LW3_NSTAGE - 1 < nstep)
+            lw3_stage_layer(ring[warp][(st + LW3_NSTAGE - 1) % LW3_NSTAGE], tg, fr, aux, layer_of(st + LW3_NSTAGE - 1),
+                            lane);
         else
             asm volatile("cp.async.commit_group;" ::: "memory");
-        asm volatile("cp.async.wait_group 2;" ::: "memory");   // this lane's copies of step st have landed
+        // this lane's copies of step st have landed (the LW3_NSTAGE - 1 later groups may still be in flight)
+        asm volatile("cp.async.wait_group %0;" ::"n"(LW3_NSTAGE - 1) : "memory");
         __syncwarp();                                            // ... and every lane's
         if (st == nlay) {
             // surface: emission and reflection

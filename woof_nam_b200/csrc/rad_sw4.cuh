@@ -219,6 +219,7 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
     const int tid = threadIdx.x;
     const int4* im = img + (size_t)blockIdx.x * (sw4_image_bytes(any_aer) / 16);
     const float* tgi = sw4_image_taug(im);   // [layer][g], read from the image as the tasks need it
+    if (SW4_L2PF && tid == 0) l2_prefetch(tgi, (uint32_t)(nlay * SW_NGPT * sizeof(float)));
     {   // the rest of the image into shared memory (the aerosol block where taug would be), every 16-byte piece
         // in flight at once (cp.async.cg: L2 to shared)
         const uint32_t sb = (uint32_t)__cvta_generic_to_shared(smem_raw + sw4_image_begin());
