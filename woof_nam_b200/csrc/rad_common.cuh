@@ -85,18 +85,29 @@ template <class F>
 __device__ __forceinline__ void for_each_band_pair(const int* ns, int nbands, int nlay, int* next, int lane, F f)
 {
     int b = 0, t0 = 0;   // band of the current task and the index of its first task
-    int ng = ns[1] - ns[0], kpw = 32 / ng, nt = (nlay + kpw - 1) / kpw;
+    // the band's shape and this lane's (layer, g-point) offset in its tasks, formed when the band changes
+    int ng, kpw, nt, kk, jg;
+    auto shape = [&](int bb) {
+        ng = ns[bb + 1] - ns[bb];
+        kpw = 32 / ng;
+        nt = (nlay + kpw - 1) / kpw;
+        kk = lane / ng;
+        jg = lane - kk * ng;
+    };
+    shape(0);
+    // the next task is claimed while the current one runs, so the atomic's latency is hidden behind it (a warp
+    // claims one id past the end before it stops; ids only grow, so no task is skipped or repeated)
+    int tn = 0;
+    if (lane == 0) tn = atomicAdd(next, 1);
     for (;;) {
-        int t = 0;
-        if (lane == 0) t = atomicAdd(next, 1);
-        t = __shfl_sync(0xffffffffu, t, 0);
+        const int t = __shfl_sync(0xffffffffu, tn, 0);
+        if (lane == 0) tn = atomicAdd(next, 1);
         while (b < nbands && t >= t0 + nt) {
             t0 += nt;
             ++b;
-            if (b < nbands) { ng = ns[b + 1] - ns[b]; kpw = 32 / ng; nt = (nlay + kpw - 1) / kpw; }
+            if (b < nbands) shape(b);
         }
         if (b >= nbands) break;
-        const int kk = lane / ng, jg = lane - kk * ng;
         const int k0 = (t - t0) * kpw + kk;
         if (kk < kpw && k0 < nlay) f(ns[b] + jg, k0, b);
     }
