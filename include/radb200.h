@@ -473,6 +473,12 @@ typedef struct {
 int rad_progcld2(RadHandle* h, const RadCloudIn* in, int64_t ncol, int32_t nlay, const RadCloudCfg* cfg,
                  const RadCloudOut* out, void* stream);
 
+/* Reads and clears the handle's device error word: *code = 0, or the code a kernel flagged since the last read
+ * (1: a request with more layers than the kernels hold; 2: an index out of range; 3: a bounded wait inside a
+ * kernel gave up -- an asynchronous copy did not land -- and the kernel stopped that column).  Waits for the
+ * handle's device to finish its work first. */
+int rad_device_error(RadHandle* h, int32_t* code);
+
 /* Device-time accounting of the library's own kernels (instrumentation; no counterpart in the reference,
  * which has none).  While enabled, rad_solve records CUDA events on its stream around the LW kernel, the
  * SW day-list kernels and the SW kernel; rad_profile_read waits for the last recorded event and returns

@@ -221,3 +221,13 @@ def test_graph_replay_equals_solve():
     for k in ref:
         assert np.array_equal(ref[k], outs[0][k].cpu().numpy()), k
     g.close()
+
+
+def test_device_error_word_stays_clear(plain, stress):
+    """No kernel flags an error (bad layer count, index, or a bounded wait that gave up) on the plain and stress
+    requests, through the tiled LW and SW kernels; rad_device_error reads and clears the word."""
+    for cols, kw in ((plain[0], {}), (stress[0], {"diagnostic": True})):
+        s = _solver(precision="mixed", **kw)
+        s.solve_host(cols)
+        assert s.device_error() == 0
+        assert s.device_error() == 0

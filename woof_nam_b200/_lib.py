@@ -208,6 +208,7 @@ SIGNATURES = {
     "rad_poll": ([ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "rad_wait": ([ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32], ctypes.c_int),
     "rad_queue_destroy": ([ctypes.c_void_p], None),
+    "rad_device_error": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
     "rad_profile_enable": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "rad_profile_read": ([ctypes.c_void_p, ctypes.POINTER(RadProfile)], ctypes.c_int),
     "rad_last_error": ([ctypes.c_void_p], ctypes.c_char_p),

@@ -514,16 +514,16 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                 const unsigned g2 = (unsigned)((nc + LW3_SWEEP_WARPS - 1) / LW3_SWEEP_WARPS);
                 float* pg = h->d_lwpg;
                 if (mc) {
-                    if (diag_lw) lw3_sweep_kernel<LW_OVR_MCICA, true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, pg);
-                    else lw3_sweep_kernel<LW_OVR_MCICA><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                    if (diag_lw) lw3_sweep_kernel<LW_OVR_MCICA, true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, h->d_err, pg);
+                    else lw3_sweep_kernel<LW_OVR_MCICA><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, h->d_err);
                     h->launches += 2;
                 } else {
                     if (cfg.iovrlw == 0) {
-                        if (diag_lw) lw3_sweep_kernel<LW_OVR_RANDOM, true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, pg);
-                        else lw3_sweep_kernel<LW_OVR_RANDOM><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                        if (diag_lw) lw3_sweep_kernel<LW_OVR_RANDOM, true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, h->d_err, pg);
+                        else lw3_sweep_kernel<LW_OVR_RANDOM><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, h->d_err);
                     } else {
-                        if (diag_lw) lw3_sweep_kernel<LW_OVR_MAXRAN, true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, pg);
-                        else lw3_sweep_kernel<LW_OVR_MAXRAN><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl);
+                        if (diag_lw) lw3_sweep_kernel<LW_OVR_MAXRAN, true><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, h->d_err, pg);
+                        else lw3_sweep_kernel<LW_OVR_MAXRAN><<<g2, LW3_SWEEP_WARPS * 32, 0, st>>>(bt, c0, nc, h->d_lw3, fl, h->d_err);
                     }
                     lw3_fp64_kernel<<<(unsigned)h->nsm, LW_THREADS, smemd, st>>>(bt, c0, h->d_lw3list, dl, h->d_err);
                     h->launches += 3;
@@ -1381,6 +1381,16 @@ void rad_queue_destroy(RadQueue* q)
         if (sl.ev) cudaEventDestroy(sl.ev);
     }
     delete q;
+}
+
+int rad_device_error(RadHandle* h, int32_t* code)
+{
+    if (!h || !code) return fail(h, RAD_E_INVALID, "rad_device_error: null argument");
+    int v = 0;
+    RAD_CUDA(h, cudaMemcpy(&v, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    RAD_CUDA(h, cudaMemset(h->d_err, 0, sizeof(int)));
+    *code = v;
+    return RAD_OK;
 }
 
 int rad_profile_enable(RadHandle* h, int on)

@@ -49,6 +49,46 @@ __device__ __forceinline__ double sqrtR(double x) { return sqrt(x); }
 __device__ __forceinline__ float rfmod1(float x) { return x - truncf(x); }
 __device__ __forceinline__ double rfmod1(double x) { return x - trunc(x); }
 
+// ---- bulk copies into shared memory completed on an mbarrier (cp.async.bulk, no multicast) ----
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// Make the barriers' initialisation visible to the bulk-copy (async) proxy.
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Order this thread's earlier generic accesses to shared memory before the async proxy writes it.
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// One arrival that also expects `bytes` of bulk copies to complete the barrier's current phase.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// [dst, dst + bytes) <- [src, src + bytes): both 16-byte aligned, bytes a multiple of 16; completes on bar.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// One bounded test of the barrier's phase `parity` (the hardware suspends the thread for a while inside).
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// Wait for the phase with at most `limit` tests; false when it did not complete (the caller flags and stops).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int limit)
+{
+    for (int i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 // Bulk prefetch of [p, p + bytes) from global memory into L2 (cp.async.bulk.prefetch.L2, no shared memory, no
 // multicast): one instruction brings a contiguous run of a column's scratch in ahead of the loads that read it.
 // p must be 16-byte aligned and bytes a multiple of 16; the range must lie inside one allocation.
@@ -134,6 +174,6 @@ struct ReqBatch {
 };
 
 // Error word written by kernels on bad input (host reads it after a synchronising call).
-enum : int { RAD_DEV_OK = 0, RAD_DEV_NLAY = 1, RAD_DEV_INDEX = 2 };
+enum : int { RAD_DEV_OK = 0, RAD_DEV_NLAY = 1, RAD_DEV_INDEX = 2, RAD_DEV_TIMEOUT = 3 };
 
 }  // namespace rad

@@ -228,6 +228,11 @@ __device__ __forceinline__ R lw3_step(float& rtot, float& rclr, float& trad, flo
 // layers ahead of the one being computed, so the scratch's DRAM latency overlaps the arithmetic.
 constexpr int LW3_STAGE = 2 * LW3_GSTRIDE + LW3_REC;   // floats per stage
 constexpr int LW3_NSTAGE = 3;
+// LW3_TMA fills the ring by bulk copies instead (cp.async.bulk: the layer's taug row, fracs row and record, three
+// contiguous runs) that lane 0 issues and an mbarrier per slot completes.  Same bits; measured 2.5 % slower over
+// the LW on the B200 (lane 0 alone issues and waits, where the 16-byte copies spread over the warp), so off.
+constexpr bool LW3_TMA = false;
+constexpr int LW3_WAIT_LIMIT = 1 << 16;   // mbarrier tests before a wait gives up (flags RAD_DEV_TIMEOUT)
 
 __device__ __forceinline__ void lw3_cp16(float* dst, const float* src)
 {
@@ -260,10 +265,12 @@ __host__ __device__ constexpr int64_t lw3_pg_floats(int nlay) { return (int64_t)
 template <int OVR, bool DIAG = false>
 __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const __grid_constant__ LwBatch bt, int64_t c0,
                                                                          int64_t nc, const float* __restrict__ scr,
-                                                                         LwLut<float> lut, float* __restrict__ pg = nullptr)
+                                                                         LwLut<float> lut, int* err,
+                                                                         float* __restrict__ pg = nullptr)
 {
     __shared__ double fup[LW3_SWEEP_WARPS][NLAY_MAX + 1], fdn[LW3_SWEEP_WARPS][NLAY_MAX + 1];
     __shared__ __align__(16) float ring[LW3_SWEEP_WARPS][LW3_NSTAGE][LW3_STAGE];
+    __shared__ __align__(8) uint64_t rbar[LW3_SWEEP_WARPS][LW3_NSTAGE];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t lc = (int64_t)blockIdx.x * LW3_SWEEP_WARPS + warp;
     if (lc >= nc) return;
@@ -282,8 +289,33 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
     // sweep steps: s = 0 .. nlay-1 downward (layer nlay - s), s = nlay .. 2 nlay - 1 upward (layer s - nlay + 1)
     const int nstep = 2 * nlay;
     auto layer_of = [&](int st) { return st < nlay ? nlay - st : st - nlay + 1; };
+    if (LW3_TMA) {
+        if (lane == 0) {
+            for (int q = 0; q < LW3_NSTAGE; ++q) mbar_init(&rbar[warp][q], 1);
+            mbar_init_fence();
+        }
+        __syncwarp();
+    }
+    // layer k's rows and record into ring slot q: lane 0 issues three bulk copies completed on the slot's barrier,
+    // after the warp's reads of the slot's previous layer (ordered by the __syncwarp and the proxy fence)
+    auto stage = [&](int q, int k) {
+        if (LW3_TMA) {
+            __syncwarp();
+            if (lane == 0) {
+                async_proxy_fence();
+                uint64_t* b = &rbar[warp][q];
+                float* dst = ring[warp][q];
+                mbar_expect_tx(b, (unsigned)(LW3_STAGE * sizeof(float)));
+                bulk_copy_g2s(dst, tg + (size_t)(k - 1) * LW3_GSTRIDE, LW3_GSTRIDE * sizeof(float), b);
+                bulk_copy_g2s(dst + LW3_GSTRIDE, fr + (size_t)(k - 1) * LW3_GSTRIDE, LW3_GSTRIDE * sizeof(float), b);
+                bulk_copy_g2s(dst + 2 * LW3_GSTRIDE, aux + (size_t)k * LW3_REC, LW3_REC * sizeof(float), b);
+            }
+        } else {
+            lw3_stage_layer(ring[warp][q], tg, fr, aux, k, lane);
+        }
+    };
 #pragma unroll
-    for (int q = 0; q < LW3_NSTAGE - 1; ++q) lw3_stage_layer(ring[warp][q], tg, fr, aux, layer_of(q), lane);
+    for (int q = 0; q < LW3_NSTAGE - 1; ++q) stage(q, layer_of(q));
     const float eps = 1.0e-6f;
     int gi[LW3_SLOTS], band[LW3_SLOTS];
     float sdif[LW3_SLOTS];
@@ -344,13 +376,30 @@ __global__ void __launch_bounds__(LW3_SWEEP_WARPS * 32) lw3_sweep_kernel(const _
     double s_tu = 0, s_cu = 0, s_td = 0, s_cd = 0;
     for (int st = 0; st < nstep; ++st) {
         if (st + LW3_NSTAGE - 1 < nstep)
-            lw3_stage_layer(ring[warp][(st + LW3_NSTAGE - 1) % LW3_NSTAGE], tg, fr, aux, layer_of(st + LW3_NSTAGE - 1),
-                            lane);
-        else
+            stage((st + LW3_NSTAGE - 1) % LW3_NSTAGE, layer_of(st + LW3_NSTAGE - 1));
+        else if (!LW3_TMA)
             asm volatile("cp.async.commit_group;" ::: "memory");
-        // this lane's copies of step st have landed (the LW3_NSTAGE - 1 later groups may still be in flight)
-        asm volatile("cp.async.wait_group %0;" ::"n"(LW3_NSTAGE - 1) : "memory");
-        __syncwarp();                                            // ... and every lane's
+        if (LW3_TMA) {
+            // slot st % LW3_NSTAGE completes its (st / LW3_NSTAGE)-th phase when the step's copies have landed
+            // lane 0 waits for the phase; the __syncwarp then orders the landed data for the other lanes
+            bool ok = true;
+            if (lane == 0)
+                ok = mbar_wait_bounded(&rbar[warp][st % LW3_NSTAGE], (unsigned)((st / LW3_NSTAGE) & 1), LW3_WAIT_LIMIT);
+            __syncwarp();
+            if (!__shfl_sync(0xffffffffu, ok, 0)) {
+                // a copy did not land: flag it, wait (bounded) for the copies still in flight, stop this column
+                if (lane == 0) atomicExch(err, RAD_DEV_TIMEOUT);
+                if (lane == 0)
+                    for (int s2 = st + 1; s2 < min(nstep, st + LW3_NSTAGE); ++s2)
+                        mbar_wait_bounded(&rbar[warp][s2 % LW3_NSTAGE], (unsigned)((s2 / LW3_NSTAGE) & 1),
+                                          LW3_WAIT_LIMIT);
+                return;
+            }
+        } else {
+            // this lane's copies of step st have landed (the LW3_NSTAGE - 1 later groups may still be in flight)
+            asm volatile("cp.async.wait_group %0;" ::"n"(LW3_NSTAGE - 1) : "memory");
+            __syncwarp();                                        // ... and every lane's
+        }
         if (st == nlay) {
             // surface: emission and reflection
 #pragma unroll

@@ -269,6 +269,13 @@ class RadSolver:
         _lib.check(self.lib, self.handle, self.lib.rad_rdtemp(self.handle, ctypes.byref(r), ctypes.c_void_p(st.cuda_stream)),
                    "rad_rdtemp")
 
+    def device_error(self) -> int:
+        """The device error word since the last call (0: none; see rad_device_error), then cleared."""
+        code = ctypes.c_int32()
+        rc = self.lib.rad_device_error(self.handle, ctypes.byref(code))
+        _lib.check(self.lib, self.handle, rc, "rad_device_error")
+        return int(code.value)
+
     def profile(self, on: bool = True) -> None:
         """Start (or stop) device-time accounting of the library's kernels on this handle."""
         _lib.check(self.lib, self.handle, self.lib.rad_profile_enable(self.handle, int(on)), "rad_profile_enable")
