@@ -34,7 +34,7 @@ def build(force: bool = False) -> Path:
     srcs = list(HERE.glob("rrtm_*.?pp")) + list(HERE.glob("opcount.hpp"))
     if force or not all(p.exists() for p in (LIB, OPCOUNT_LIB)) or any(
             p.stat().st_mtime > min(LIB.stat().st_mtime, OPCOUNT_LIB.stat().st_mtime) for p in srcs):
-        subprocess.run(["make", "-C", str(HERE), "all"], check=True)
+        subprocess.run(["make", "-C", str(HERE), *(["-B"] if force else []), "all"], check=True)
     return LIB
 
 

@@ -41,11 +41,14 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     # multiply-add contraction), as the single-precision routines it restates.
     front = ["-prec-div=true", "-prec-sqrt=true", "-ftz=false", "-fmad=false"]
     with tempfile.TemporaryDirectory() as tmp:
-        objs = []
-        for src, flags in (("rad_capi.cu", solve), ("rad_front.cu", front)):
+        objs, procs = [], []
+        for src, flags in (("rad_capi.cu", solve), ("rad_front.cu", front)):   # the two units side by side
             obj = str(Path(tmp) / (src + ".o"))
-            subprocess.run([*base, *flags, "-c", "-o", obj, str(SRC / src)], check=True)
+            procs.append(subprocess.Popen([*base, *flags, "-c", "-o", obj, str(SRC / src)]))
             objs.append(obj)
+        for p, src in zip(procs, ("rad_capi.cu", "rad_front.cu")):
+            if p.wait() != 0:
+                raise subprocess.CalledProcessError(p.returncode, f"nvcc {src}")
         subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(LIB), *objs], check=True)
     return LIB
 
