@@ -503,7 +503,7 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
             fl.ex = h->d_lwf; fl.tfn = h->d_lwf + 10001; fl.tau = h->d_lwf + 2 * 10001;
             LwLut<double> dl;
             dl.ex = h->d_lwd; dl.tfn = h->d_lwd + 10001; dl.tau = h->d_lwd + 2 * 10001;
-            const size_t smem1 = sizeof(LwSetup<float>), smemd = sizeof(LwShared<double>);
+            const size_t smem1 = sizeof(LwSetupK<float>), smemd = sizeof(LwShared<double>);
             RAD_CUDA(h, cudaFuncSetAttribute((void*)lw3_optics_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
             RAD_CUDA(h, cudaFuncSetAttribute((void*)lw3_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemd));
             const int64_t lstep = diag_lw ? std::min(lwc, (int64_t)LW_DIAG_CHUNK) : lwc;

@@ -47,6 +47,24 @@ struct LwSetup {
     // 7, 8, 13, and the ratios of reference mixing ratios (chi) that key the minor / Planck-fraction species
     R adjc[LW_NADJ][NLAY_MAX];
     R chir[LW_NCHIR];
+    static constexpr bool kKeys = false;      // LwSetupK: the species keys of bands 3, 4, 5, 7, 9 are precomputed
+};
+
+// The species keys of one binary-species band at one layer (the specparm / js / fs statements of taugb03, 04, 05,
+// 07, 09 for the two temperature neighbours, the branch each selects, and the minor-gas and Planck-fraction keys),
+// formed once per (band, layer) instead of in each of the band's g-point tasks.  Slots: bands 3, 4, 5, 7, 9.
+template <class R>
+struct LwKey {
+    R sc, sc1, fs, fs1, fm, fpl;
+    int js, js1, jm, jpl, br0, br1;
+};
+constexpr int LW_NKEYB = 5;
+// The tiled LW's optics CTA layout: the set-up data and the keys (the single-kernel and float64 layouts keep their
+// shared memory and form the keys in the tasks).
+template <class R>
+struct LwSetupK : LwSetup<R> {
+    static constexpr bool kKeys = true;
+    LwKey<R> key[LW_NKEYB][NLAY_MAX];
 };
 
 // The single-kernel layout: set-up data plus the column's gas optics and the sweeps' partial sums.
@@ -149,6 +167,15 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
         auto a = [&](int id) { return ldt(t + ((id - 1) * ng + ig)); };
         return f00 * a(i0) + f10 * a(i0 + 1) + f01 * a(i1) + f11 * a(i1 + 1);
     };
+    // the precomputed species keys of band slot q at this layer (LwSetupK only)
+    auto keys = [&](int q, R& sc, R& sc1, R& fs, R& fs1, int& js, int& js1, int& jm, R& fm, int& jpl, R& fpl, int& br0,
+                    int& br1) {
+        if constexpr (S::kKeys) {
+            const LwKey<R>& K = s.key[q][k0];
+            sc = K.sc; sc1 = K.sc1; fs = K.fs; fs1 = K.fs1; js = K.js; js1 = K.js1; jm = K.jm; fm = K.fm;
+            jpl = K.jpl; fpl = K.fpl; br0 = K.br0; br1 = K.br1;
+        }
+    };
     const int ind0l = (jpk - 1) * 5 + (jtk - 1) + 1, ind1l = jpk * 5 + (jt1k - 1) + 1;
     const int ind0u = (jpk - 13) * 5 + (jtk - 1) + 1, ind1u = (jpk - 12) * 5 + (jt1k - 1) + 1;
     int band = band_of_g;
@@ -203,15 +230,22 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
         R adjn2o = 0;
         if (b3) adjn2o = s.adjc[0][k0];
         if (low) {
-            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fmn = 0, fpl;
-            int js, js1, jmn = 1, jpl;
-            const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0];
-            spec(c1, s.rfrate[0][0][k0], c2, (R)8, sc, sp, js, fs);
-            spec(c1, s.rfrate[1][0][k0], c2, (R)8, sc1, sp1, js1, fs1);
-            if (b3) spec(c1, rma, c2, (R)8, scm, spm, jmn, fmn);
-            spec(c1, rpa, c2, (R)8, scp, spp, jpl, fpl);
-            const Sel<R> s0 = sel_branch(br_of(sp), fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
-            const Sel<R> s1 = sel_branch(br_of(sp1), fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
+            R sc, sc1, fs, fs1, fmn = 0, fpl;
+            int js, js1, jmn = 1, jpl, br0, br1;
+            if constexpr (S::kKeys) {
+                keys(b3 ? 0 : 1, sc, sc1, fs, fs1, js, js1, jmn, fmn, jpl, fpl, br0, br1);
+            } else {
+                R sp, sp1, scm, spm, scp, spp;
+                const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0];
+                spec(c1, s.rfrate[0][0][k0], c2, (R)8, sc, sp, js, fs);
+                spec(c1, s.rfrate[1][0][k0], c2, (R)8, sc1, sp1, js1, fs1);
+                if (b3) spec(c1, rma, c2, (R)8, scm, spm, jmn, fmn);
+                spec(c1, rpa, c2, (R)8, scp, spp, jpl, fpl);
+                br0 = br_of(sp);
+                br1 = br_of(sp1);
+            }
+            const Sel<R> s0 = sel_branch(br0, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
+            const Sel<R> s1 = sel_branch(br1, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
             const R tauself = sfac * interp(tab<R>(b3 ? T_LW03_SELFREF : T_LW04_SELFREF), NG, inds, ig, sfr);
             const R taufor = ffac * interp(tab<R>(b3 ? T_LW03_FORREF : T_LW04_FORREF), NG, indf, ig, ffr);
             const R major = major12(absa, NG, ig, sc, s0, f00, f10, sc1, s1, f01, f11);
@@ -219,18 +253,24 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
             else tg = major + tauself + taufor;
             fr = interp(fa, NG, jpl, ig, fpl);
         } else {
-            const R ka1 = b3 ? s.colamt[0][k0] : s.colamt[2][k0];
-            const R r0 = b3 ? s.rfrate[0][0][k0] : s.rfrate[0][5][k0];
-            const R r1 = b3 ? s.rfrate[1][0][k0] : s.rfrate[1][5][k0];
-            const R c2 = s.colamt[1][k0];
-            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fmn = 0, fpl;
+            R sc, sc1, fs, fs1, fmn = 0, fpl;
             int js, js1, jmn = 1, jpl;
-            spec(ka1, r0, c2, (R)4, sc, sp, js, fs);
+            if constexpr (S::kKeys) {
+                int br0, br1;
+                keys(b3 ? 0 : 1, sc, sc1, fs, fs1, js, js1, jmn, fmn, jpl, fpl, br0, br1);
+            } else {
+                const R ka1 = b3 ? s.colamt[0][k0] : s.colamt[2][k0];
+                const R r0 = b3 ? s.rfrate[0][0][k0] : s.rfrate[0][5][k0];
+                const R r1 = b3 ? s.rfrate[1][0][k0] : s.rfrate[1][5][k0];
+                const R c2 = s.colamt[1][k0];
+                R sp, sp1, scm, spm, scp, spp;
+                spec(ka1, r0, c2, (R)4, sc, sp, js, fs);
+                spec(ka1, r1, c2, (R)4, sc1, sp1, js1, fs1);
+                if (b3) spec(ka1, rmb, c2, (R)4, scm, spm, jmn, fmn);
+                spec(ka1, rpb, c2, (R)4, scp, spp, jpl, fpl);
+            }
             const int ind0 = ((jpk - 13) * 5 + (jtk - 1)) * 5 + js;
-            spec(ka1, r1, c2, (R)4, sc1, sp1, js1, fs1);
             const int ind1 = ((jpk - 12) * 5 + (jt1k - 1)) * 5 + js1;
-            if (b3) spec(ka1, rmb, c2, (R)4, scm, spm, jmn, fmn);
-            spec(ka1, rpb, c2, (R)4, scp, spp, jpl, fpl);
             const R fac000 = ((R)1 - fs) * f00, fac010 = ((R)1 - fs) * f10, fac100 = fs * f00, fac110 = fs * f10;
             const R fac001 = ((R)1 - fs1) * f01, fac011 = ((R)1 - fs1) * f11, fac101 = fs1 * f01, fac111 = fs1 * f11;
             auto B = [&](int id) { return ldt(absb + ((id - 1) * NG + ig)); };
@@ -254,14 +294,19 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
         const int NG = 16;
         const R wxk = s.wx[0][k0], ccl4 = ldt(tab<R>(T_LW05_CCL4) + ig);
         if (low) {
-            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fm, fpl;
-            int js, js1, jm, jpl;
-            const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0];
-            spec(c1, s.rfrate[0][0][k0], c2, (R)8, sc, sp, js, fs);
-            spec(c1, s.rfrate[1][0][k0], c2, (R)8, sc1, sp1, js1, fs1);
-            spec(c1, (R)c_lwk.b5_rma, c2, (R)8, scm, spm, jm, fm);
-            spec(c1, (R)c_lwk.b5_rpa, c2, (R)8, scp, spp, jpl, fpl);
-            const int br = br_joint(sp, sp1);
+            R sc, sc1, fs, fs1, fm, fpl;
+            int js, js1, jm, jpl, br, br1;
+            if constexpr (S::kKeys) {
+                keys(2, sc, sc1, fs, fs1, js, js1, jm, fm, jpl, fpl, br, br1);
+            } else {
+                R sp, sp1, scm, spm, scp, spp;
+                const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0];
+                spec(c1, s.rfrate[0][0][k0], c2, (R)8, sc, sp, js, fs);
+                spec(c1, s.rfrate[1][0][k0], c2, (R)8, sc1, sp1, js1, fs1);
+                spec(c1, (R)c_lwk.b5_rma, c2, (R)8, scm, spm, jm, fm);
+                spec(c1, (R)c_lwk.b5_rpa, c2, (R)8, scp, spp, jpl, fpl);
+                br = br_joint(sp, sp1);
+            }
             const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
             const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
             const R tauself = sfac * interp(tab<R>(T_LW05_SELFREF), NG, inds, ig, sfr);
@@ -271,14 +316,21 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
                  abso3 * s.colamt[2][k0] + wxk * ccl4;
             fr = interp(tab<R>(T_LW05_FRACREFA), NG, jpl, ig, fpl);
         } else {
-            R sc, sp, sc1, sp1, scp, spp, fs, fs1, fpl;
+            R sc, sc1, fs, fs1, fpl;
             int js, js1, jpl;
-            const R c3 = s.colamt[2][k0], c2 = s.colamt[1][k0];
-            spec(c3, s.rfrate[0][5][k0], c2, (R)4, sc, sp, js, fs);
+            if constexpr (S::kKeys) {
+                R fm;
+                int jm, br0, br1;
+                keys(2, sc, sc1, fs, fs1, js, js1, jm, fm, jpl, fpl, br0, br1);
+            } else {
+                R sp, sp1, scp, spp;
+                const R c3 = s.colamt[2][k0], c2 = s.colamt[1][k0];
+                spec(c3, s.rfrate[0][5][k0], c2, (R)4, sc, sp, js, fs);
+                spec(c3, s.rfrate[1][5][k0], c2, (R)4, sc1, sp1, js1, fs1);
+                spec(c3, (R)c_lwk.b5_rpb, c2, (R)4, scp, spp, jpl, fpl);
+            }
             const int ind0 = ((jpk - 13) * 5 + (jtk - 1)) * 5 + js;
-            spec(c3, s.rfrate[1][5][k0], c2, (R)4, sc1, sp1, js1, fs1);
             const int ind1 = ((jpk - 12) * 5 + (jt1k - 1)) * 5 + js1;
-            spec(c3, (R)c_lwk.b5_rpb, c2, (R)4, scp, spp, jpl, fpl);
             const R fac000 = ((R)1 - fs) * f00, fac010 = ((R)1 - fs) * f10, fac100 = fs * f00, fac110 = fs * f10;
             const R fac001 = ((R)1 - fs1) * f01, fac011 = ((R)1 - fs1) * f11, fac101 = fs1 * f01, fac111 = fs1 * f11;
             const R* absb = tab<R>(T_LW05_ABSB);
@@ -309,15 +361,20 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
         const int NG = 12;
         const R c1 = s.colamt[0][k0], c3 = s.colamt[2][k0];
         if (low) {
-            const R rr = s.chir[3];
-            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fm, fpl;
-            int js, js1, jm, jpl;
-            spec(c1, s.rfrate[0][1][k0], c3, (R)8, sc, sp, js, fs);
-            spec(c1, s.rfrate[1][1][k0], c3, (R)8, sc1, sp1, js1, fs1);
-            spec(c1, rr, c3, (R)8, scm, spm, jm, fm);
-            spec(c1, rr, c3, (R)8, scp, spp, jpl, fpl);
+            R sc, sc1, fs, fs1, fm, fpl;
+            int js, js1, jm, jpl, br, br1;
+            if constexpr (S::kKeys) {
+                keys(3, sc, sc1, fs, fs1, js, js1, jm, fm, jpl, fpl, br, br1);
+            } else {
+                const R rr = s.chir[3];
+                R sp, sp1, scm, spm, scp, spp;
+                spec(c1, s.rfrate[0][1][k0], c3, (R)8, sc, sp, js, fs);
+                spec(c1, s.rfrate[1][1][k0], c3, (R)8, sc1, sp1, js1, fs1);
+                spec(c1, rr, c3, (R)8, scm, spm, jm, fm);
+                spec(c1, rr, c3, (R)8, scp, spp, jpl, fpl);
+                br = br_joint(sp, sp1);
+            }
             const R adj = s.adjc[2][k0];
-            const int br = br_joint(sp, sp1);
             const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
             const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
             const R tauself = sfac * interp(tab<R>(T_LW07_SELFREF), NG, inds, ig, sfr);
@@ -364,14 +421,19 @@ __device__ void lw_gas(const S& s, int g, int k0, R& tg, R& fr, int band_of_g = 
         const R c1 = s.colamt[0][k0], c5 = s.colamt[4][k0];
         const R adj = s.adjc[0][k0];
         if (low) {
-            const R rpa = s.chir[4], rma = s.chir[5];
-            R sc, sp, sc1, sp1, scm, spm, scp, spp, fs, fs1, fm, fpl;
-            int js, js1, jm, jpl;
-            spec(c1, s.rfrate[0][3][k0], c5, (R)8, sc, sp, js, fs);
-            spec(c1, s.rfrate[1][3][k0], c5, (R)8, sc1, sp1, js1, fs1);
-            spec(c1, rma, c5, (R)8, scm, spm, jm, fm);
-            spec(c1, rpa, c5, (R)8, scp, spp, jpl, fpl);
-            const int br = br_joint(sp, sp1);
+            R sc, sc1, fs, fs1, fm, fpl;
+            int js, js1, jm, jpl, br, br1;
+            if constexpr (S::kKeys) {
+                keys(4, sc, sc1, fs, fs1, js, js1, jm, fm, jpl, fpl, br, br1);
+            } else {
+                const R rpa = s.chir[4], rma = s.chir[5];
+                R sp, sp1, scm, spm, scp, spp;
+                spec(c1, s.rfrate[0][3][k0], c5, (R)8, sc, sp, js, fs);
+                spec(c1, s.rfrate[1][3][k0], c5, (R)8, sc1, sp1, js1, fs1);
+                spec(c1, rma, c5, (R)8, scm, spm, jm, fm);
+                spec(c1, rpa, c5, (R)8, scp, spp, jpl, fpl);
+                br = br_joint(sp, sp1);
+            }
             const Sel<R> s0 = sel_branch(br, fs, ((jpk - 1) * 5 + (jtk - 1)) * 9 + js);
             const Sel<R> s1 = sel_branch(br, fs1, (jpk * 5 + (jt1k - 1)) * 9 + js1);
             const R tauself = sfac * interp(tab<R>(T_LW09_SELFREF), NG, inds, ig, sfr);
@@ -740,6 +802,62 @@ __device__ __forceinline__ void lw_chi_ratio(S& s, int i)
     s.chir[i] = CHI(num[i], lev[i]) / CHI(den[i], lev[i]);
 }
 
+// The species keys of band slot q (bands 3, 4, 5, 7, 9) at layer k0 into s.key (LwSetupK): the statements of the
+// band kernels in lw_gas (taugb03 / 04 / 05 / 07 / 09), after setcoef and the chi ratios.
+template <class R, class S>
+__device__ __forceinline__ void lw_keys_band(S& s, int q, int k0)
+{
+    LwKey<R>& K = s.key[q][k0];
+    K.jm = 1; K.fm = 0; K.jpl = 1; K.fpl = 0; K.br0 = 2; K.br1 = 2;
+    K.sc = 0; K.sc1 = 0; K.fs = 0; K.fs1 = 0; K.js = 1; K.js1 = 1;
+    const bool low = s.lower[k0];
+    R sp = 0, sp1 = 0, scx, spx;
+    if (q <= 1) {                                   // bands 3, 4
+        const bool b3 = q == 0;
+        if (low) {
+            const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0];
+            spec(c1, s.rfrate[0][0][k0], c2, (R)8, K.sc, sp, K.js, K.fs);
+            spec(c1, s.rfrate[1][0][k0], c2, (R)8, K.sc1, sp1, K.js1, K.fs1);
+            if (b3) spec(c1, s.chir[2], c2, (R)8, scx, spx, K.jm, K.fm);
+            spec(c1, b3 ? s.chir[0] : (R)c_lwk.b4_rpa, c2, (R)8, scx, spx, K.jpl, K.fpl);
+            K.br0 = br_of(sp);
+            K.br1 = br_of(sp1);
+        } else {
+            const R ka1 = b3 ? s.colamt[0][k0] : s.colamt[2][k0];
+            const R r0 = b3 ? s.rfrate[0][0][k0] : s.rfrate[0][5][k0];
+            const R r1 = b3 ? s.rfrate[1][0][k0] : s.rfrate[1][5][k0];
+            const R c2 = s.colamt[1][k0];
+            spec(ka1, r0, c2, (R)4, K.sc, sp, K.js, K.fs);
+            spec(ka1, r1, c2, (R)4, K.sc1, sp1, K.js1, K.fs1);
+            if (b3) spec(ka1, s.chir[1], c2, (R)4, scx, spx, K.jm, K.fm);
+            spec(ka1, b3 ? s.chir[1] : (R)c_lwk.b4_rpb, c2, (R)4, scx, spx, K.jpl, K.fpl);
+        }
+    } else if (q == 2) {                            // band 5
+        if (low) {
+            const R c1 = s.colamt[0][k0], c2 = s.colamt[1][k0];
+            spec(c1, s.rfrate[0][0][k0], c2, (R)8, K.sc, sp, K.js, K.fs);
+            spec(c1, s.rfrate[1][0][k0], c2, (R)8, K.sc1, sp1, K.js1, K.fs1);
+            spec(c1, (R)c_lwk.b5_rma, c2, (R)8, scx, spx, K.jm, K.fm);
+            spec(c1, (R)c_lwk.b5_rpa, c2, (R)8, scx, spx, K.jpl, K.fpl);
+            K.br0 = K.br1 = br_joint(sp, sp1);
+        } else {
+            const R c3 = s.colamt[2][k0], c2 = s.colamt[1][k0];
+            spec(c3, s.rfrate[0][5][k0], c2, (R)4, K.sc, sp, K.js, K.fs);
+            spec(c3, s.rfrate[1][5][k0], c2, (R)4, K.sc1, sp1, K.js1, K.fs1);
+            spec(c3, (R)c_lwk.b5_rpb, c2, (R)4, scx, spx, K.jpl, K.fpl);
+        }
+    } else if (low) {                               // bands 7, 9: keys in the lower atmosphere only
+        const R c1 = s.colamt[0][k0], c2 = q == 3 ? s.colamt[2][k0] : s.colamt[4][k0];
+        const int r = q == 3 ? 1 : 3;
+        const R rm = q == 3 ? s.chir[3] : s.chir[5], rp = q == 3 ? s.chir[3] : s.chir[4];
+        spec(c1, s.rfrate[0][r][k0], c2, (R)8, K.sc, sp, K.js, K.fs);
+        spec(c1, s.rfrate[1][r][k0], c2, (R)8, K.sc1, sp1, K.js1, K.fs1);
+        spec(c1, rm, c2, (R)8, scx, spx, K.jm, K.fm);
+        spec(c1, rp, c2, (R)8, scx, spx, K.jpl, K.fpl);
+        K.br0 = K.br1 = br_joint(sp, sp1);
+    }
+}
+
 // Planck functions of band i at level / layer k (k = 0: the surface; phys_rrtm_lw_setcoef.cu:135-160).
 template <class R>
 __device__ __forceinline__ void lw_planck(const LwIn& a, int64_t col, int k, int i, R& lay, R& lev)
@@ -853,8 +971,8 @@ __device__ void lw_overlap(LwSetup<R>& s, int nlay)
 // Phases A and B of the LW column (everything before the sweeps), shared by the column kernels:
 // absorber amounts, cloud optics, setcoef, Planck functions, gas optics per (g, layer) and the
 // max-random overlap factors of rtrnmr, all in shared memory.  NT threads, tid = threadIdx.x.
-template <class R, int NT, class Sink>
-__device__ void lw_setup_core(LwSetup<R>& s, const LwIn& a, int64_t col, int tid, Sink sink)
+template <class R, int NT, class Sink, class S>
+__device__ void lw_setup_core(S& s, const LwIn& a, int64_t col, int tid, Sink sink)
 {
     const int nlay = a.nlay, nlp1 = nlay + 1;
     const int64_t N = a.ncol;
@@ -913,6 +1031,10 @@ __device__ void lw_setup_core(LwSetup<R>& s, const LwIn& a, int64_t col, int tid
         }
     }
     __syncthreads();
+    if constexpr (S::kKeys) {   // the species keys of bands 3, 4, 5, 7, 9 per layer (they read the chi ratios)
+        for (int i = tid; i < LW_NKEYB * nlay; i += NT) lw_keys_band<R>(s, i / nlay, i % nlay);
+        __syncthreads();
+    }
     // ---- phase B: gas optics per (g, layer), band by band; the last warp first computes the overlap
     // factors of rtrnmr (a serial recurrence in k, one lane) and then joins the task queue
     const int warp = tid >> 5, lane = tid & 31;

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(LW3_OPT_THREADS, LW3_OPT_MINB) lw3_optics_kern
                                                                    float* __restrict__ scr, int* fp64list, int* err)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    LwSetup<float>& s = *reinterpret_cast<LwSetup<float>*>(smem_raw);
+    LwSetupK<float>& s = *reinterpret_cast<LwSetupK<float>*>(smem_raw);
     const int64_t gc = c0 + blockIdx.x;
     const int rq = bt.find(gc);
     const LwIn& a = bt.req[rq];
