@@ -264,7 +264,7 @@ typedef struct {
 
 int rad_rdtemp(RadHandle* h, const RadRdtemp* p, void* stream);
 
-/* ---- climatological aerosol optics (NAM iaer = 11: SW and LW aerosol, no volcanic term) ----
+/* ---- climatological aerosol optics (NAM iaer = 11: SW and LW aerosol), and the volcanic term ----
  * The monthly 5-degree OPAC climatology as packed (woof_nam_b200/data/aer_tables.npz from the NAM data file
  * nam_climaeropac_global.txt), host pointers. */
 typedef struct {
@@ -307,6 +307,19 @@ typedef struct {
  * asymmetry per band; the layouts RadColumns.faersw / faerlw take), nlay = the handle's.  Asynchronous on
  * stream; needs rad_load_aerosols first. */
 int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faersw, float* faerlw, void* stream);
+
+/* setaer's stratospheric volcanic aerosol term (the lavoflg branch, iaer >= 100; off on NAM): replaces
+ * phys_rrtm_setaer_volc (namgpu/kernels/phys_rrtm_setaer.cu:178-330) as phys_rrtm_setaer.py:177-192 calls it
+ * after the climatological optics.  Adds, in place, each column's zone optical depth, spread over the layers
+ * between 5 mb and 150-250 mb by pressure depth, to the extinction (component 0) of faersw [3][14][nlay][ncol]
+ * (add_sw) and faerlw [3][16][nlay][ncol] (add_lw; lw1bd: the one-broad-band LW factor in all 16 bands), nlay =
+ * the handle's.  plvl [nlay + 1][ncol] interface pressure, mb, and xlat [ncol], radians: device pointers;
+ * levels top first (ivflip 0) or surface first (ivflip 1).  ivolae: HOST int32 [10][4][12] (year, zone,
+ * month) as the reference's table; the call reads year (kyrsav mod 10, non-negative) and month kmonsav
+ * (1..12).  Needs no climatology loaded.  Asynchronous on stream; nlay >= 4. */
+int rad_setaer_volc(RadHandle* h, const float* plvl, const float* xlat, int64_t ncol, int32_t ivflip,
+                    const int32_t* ivolae, int32_t kyrsav, int32_t kmonsav, int32_t add_sw, int32_t add_lw,
+                    int32_t lw1bd, float* faersw, float* faerlw, void* stream);
 
 /* ---- grrad's radiation layers from the model state ---- */
 typedef struct {              /* model state of ncol columns: device pointers, float32, levels top first */

@@ -270,6 +270,26 @@ def aerosols(clim: dict, cols, aer_in: dict, which: str = "port", tables: bool =
     return out
 
 
+def setaer_volc(plvl, xlat, ivolae, kyrsav: int, kmonsav: int, faersw, faerlw, ivflip: int = 0,
+                add_sw: bool = True, add_lw: bool = True, lw1bd: bool = False, which: str = "port") -> dict:
+    """setaer's volcanic stratospheric term (lavoflg) added to copies of faersw [3][14][nlay][n] and faerlw
+    [3][16][nlay][n]: plvl [nlay + 1][n] mb in the order of ivflip, xlat [n] radians, ivolae int32 [10][4][12]
+    (year, zone, month), kyrsav / kmonsav as the aerosol module keeps them."""
+    L = lib(which)
+    pl, xl = _f(plvl), _f(xlat)
+    iv = np.ascontiguousarray(ivolae, dtype=np.int32)
+    if iv.shape != (10, 4, 12):
+        raise ValueError("ivolae must be int32 [10, 4, 12]")
+    sw, lw = np.array(faersw, np.float32, copy=True, order="C"), np.array(faerlw, np.float32, copy=True, order="C")
+    nlay, n = pl.shape[0] - 1, pl.shape[1]
+    rc = L.orc_setaer_volc(ctypes.c_int(nlay), ctypes.c_int(n), ctypes.c_int(ivflip), _fp(pl), _fp(xl), _ip(iv),
+                           ctypes.c_int(kyrsav), ctypes.c_int(kmonsav), ctypes.c_int(int(add_sw)),
+                           ctypes.c_int(int(add_lw)), ctypes.c_int(int(lw1bd)), _fp(sw), _fp(lw))
+    if rc != 0:
+        raise ValueError("setaer_volc: invalid arguments")
+    return {"faersw": sw, "faerlw": lw}
+
+
 def solar(date, deltsw: float, deltim: float, solc0: float, glon=None, glat=None, solhr: float = 0.0,
           dtswav: float = 1.0, nrads: int = 1, which: str = "port") -> dict:
     """Solar geometry: sollag, sindec, cosdec, anginc, solcon, nstp of the forecast time date = (year, month,

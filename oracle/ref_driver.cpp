@@ -1303,6 +1303,27 @@ int orc_aerosols(const int* iendwv, const float* haer, const float* prsref, cons
     return 0;
 }
 
+// The volcanic term from the reference's kernels: phys_rrtm_setaer_prep for alat (do_dz 0), then
+// phys_rrtm_setaer_volc with year mod(kyrsav, 10) + 1 and month kmonsav as phys_rrtm_setaer.py:178-192 passes
+// them.  Same signature as the oracle's orc_setaer_volc.
+int orc_setaer_volc(int nlay, int ncol, int ivflip, const float* plvl, const float* xlat, const int* ivolae,
+                    int kyrsav, int kmonsav, int add_sw, int add_lw, int lw1bd, float* aerosw, float* aerolw)
+{
+    if (nlay < 4 || ncol < 0 || kmonsav < 1 || kmonsav > 12) return 1;
+    if (ncol == 0) return 0;
+    const int year1 = ((kyrsav % 10) + 10) % 10 + 1;
+    std::vector<float> zero((size_t)(nlay + 1) * ncol, 0.0f), xlon(ncol, 0.0f), alon(ncol), alat(ncol);
+    drv::launch(drv::cdiv(ncol, 128), 1, 1, 128, [&] {
+        r_seta::phys_rrtm_setaer_prep(plvl, zero.data(), zero.data(), zero.data(), xlon.data(), xlat, alon.data(),
+                                      alat.data(), nullptr, nullptr, ncol, nlay, nlay + 1, ivflip, 0);
+    });
+    drv::launch(drv::cdiv(ncol, 128), 1, 1, 128, [&] {
+        r_seta::phys_rrtm_setaer_volc(aerosw, aerolw, plvl, alat.data(), ivolae, ncol, nlay, ivflip, year1, kmonsav,
+                                      add_sw, add_lw, lw1bd);
+    });
+    return 0;
+}
+
 // Solar geometry from the reference's kernels sol_update_nmmb (phys_rrtm_sol_update.py: one thread) and
 // phys_rrtm_coszmn (phys_rrtm_coszmn.py:51-67, one row of n columns).  Same signature as the oracle's.
 int orc_solar(const int* date, float deltsw, float deltim, double solc0, float* state, int* nstp, int n,

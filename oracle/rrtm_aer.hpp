@@ -7,6 +7,8 @@
 //   trop_update fill  namgpu/kernels/phys_rrtm_aer_update.cu:40-63    the month's 5-degree climatology
 //   setaer prep       namgpu/kernels/phys_rrtm_setaer.cu:80-150       lon / lat in degrees, dz, hz (ivflip 0)
 //   aer_property      namgpu/kernels/phys_rrtm_aer_property.cu:117-434 (ivflip 0, NSWBND 14, NLWBND 16)
+//   volcanic term     namgpu/kernels/phys_rrtm_setaer.cu:178-330 (lavoflg; ivflip 0 and 1, NLWBND 16 or 1),
+//                     year and month from namgpu/physics/rrtm/phys_rrtm_setaer.py:178-192
 // Never linked into the product.
 #pragma once
 #include <algorithm>
@@ -347,6 +349,81 @@ inline void column(const Tables& t, const Clim& c, int nlay, const float* prsi, 
             o[(((size_t)0 * nb + m) * nlay + (k - 1)) * n] = tau[k];
             o[(((size_t)1 * nb + m) * nlay + (k - 1)) * n] = ssa[k];
             o[(((size_t)2 * nb + m) * nlay + (k - 1)) * n] = asy[k];
+        }
+    }
+}
+
+// The volcanic stratospheric term of one column, added to the extinction (component 0) of sw [3][NSW][nlay]
+// and lw [3][NLW][nlay] at stride n.  prsi [nlay + 1] in mb in the order of ivflip; xlat in radians; iv[4]
+// the table's values of the four latitude zones (90N-45N, 45N-0, 0-45S, 45S-90S) for the year and month.
+// Levels and layers are 0-based here: the reference's level k is prsi[k - 1], its layer k is index k - 1.
+inline void volcanic(int nlay, int ivflip, const float* prsi, float xlat, const int32_t iv[4], bool add_sw,
+                     bool add_lw, bool lw1bd, float* sw, float* lw, size_t n)
+{
+    const float pi = 3.1415926535897931f, rdg = 180.0f / pi, psrfh = 5.0f;
+    float lat = xlat * rdg;
+    if (lat < -90.0f) lat = -90.0f;
+    if (lat > 90.0f) lat = 90.0f;
+    // zone value, halved sums of two zones within a degree of 45N, the equator and 45S
+    float volcae;
+    if (lat > 46.0f)       volcae = 1.0e-4f * (float)iv[0];
+    else if (lat > 44.0f)  volcae = 5.0e-5f * (float)(iv[0] + iv[1]);
+    else if (lat > 1.0f)   volcae = 1.0e-4f * (float)iv[1];
+    else if (lat > -1.0f)  volcae = 5.0e-5f * (float)(iv[1] + iv[2]);
+    else if (lat > -44.0f) volcae = 1.0e-4f * (float)iv[2];
+    else if (lat > -46.0f) volcae = 5.0e-5f * (float)(iv[2] + iv[3]);
+    else                   volcae = 1.0e-4f * (float)iv[3];
+    // lower edge of the layer: 250 mb poleward of 70 degrees, 150 mb within 20, linear between
+    const float alat = std::fabs(lat);
+    const float psrfl = alat > 70.0f ? 250.0f : (alat < 20.0f ? 150.0f : 110.0f + 2.0f * alat);
+
+    // top layer kh and bottom layer kl of the aerosol (0-based layers), rdelp = 1 / their pressure depth
+    int kh, kl;
+    float rdelp;
+    if (ivflip == 0) {
+        kh = nlay - 2; kl = 1; rdelp = 1.0f / prsi[1];
+        for (int i = 1; i <= nlay - 3; ++i)
+            if (prsi[i] >= psrfh) { kh = i - 1; break; }
+        for (int i = 1; i <= nlay - 3; ++i)
+            if (prsi[i] >= psrfl) { kl = i - 1; rdelp = 1.0f / (prsi[i] - prsi[kh]); break; }
+    } else {
+        kh = 1; kl = nlay - 2; rdelp = 1.0f / prsi[nlay - 2];
+        for (int i = nlay - 2; i >= 1; --i)
+            if (prsi[i] >= psrfh) { kh = i; break; }
+        for (int i = nlay - 1; i >= 1; --i)
+            if (prsi[i] >= psrfl) { kl = i; rdelp = 1.0f / (prsi[i] - prsi[kh + 1]); break; }
+    }
+    // layer j's share of the column: its pressure depth times rdelp
+    auto share = [&](int j) {
+        return ivflip == 0 ? (prsi[j + 1] - prsi[j]) * rdelp : (prsi[j] - prsi[j + 1]) * rdelp;
+    };
+    const int j0 = ivflip == 0 ? kh : kl, j1 = ivflip == 0 ? kl : kh;
+    const int below = ivflip == 0 ? kl + 1 : kl - 1;     // the layer under the bottom one
+    if (add_sw) {
+        for (int b = 0; b < NSW; ++b) {
+            // wavelength exponent: 0.74 below 0.5 micron (above 20000 cm-1), 1.14 above it, 0.94 across it
+            const float e = WSW1[b] > 20000.0f ? 0.74f : (WSW2[b] < 20000.0f ? 1.14f : 0.94f);
+            const float tb = std::pow(0.275e-4f * (WSW2[b] + WSW1[b]), e);
+            float* x = sw + (size_t)b * nlay * n;
+            for (int j = j0; j <= j1; ++j) {
+                const float tmp2 = tb * share(j);
+                x[j * n] = x[j * n] + tmp2 * volcae;
+            }
+            if (x[kl * n] > 10.0f * x[below * n]) {      // spread a sharp bottom edge 80 / 20 over two layers
+                const float s2 = x[kl * n] + x[below * n];
+                x[kl * n] = 0.8f * s2;
+                x[below * n] = 0.2f * s2;
+            }
+        }
+    }
+    if (add_lw) {
+        for (int b = 0; b < NLW; ++b) {
+            const float tb = lw1bd ? std::pow(0.55f / 11.0f, 1.2f) : std::pow(0.275e-4f * (WLW2[b] + WLW1[b]), 1.2f);
+            float* x = lw + (size_t)b * nlay * n;
+            for (int j = j0; j <= j1; ++j) {
+                const float tmp2 = tb * share(j);
+                x[j * n] = x[j * n] + tmp2 * volcae;
+            }
         }
     }
 }

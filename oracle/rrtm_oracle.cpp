@@ -516,6 +516,27 @@ extern "C" int orc_aerosols(const int* iendwv, const float* haer, const float* p
     return 0;
 }
 
+// The volcanic stratospheric aerosol term (rrtm_aer.hpp volcanic), added in place to aerosw [3][14][nlay][ncol]
+// and aerolw [3][16][nlay][ncol]: plvl [nlay + 1][ncol] mb in the order of ivflip, xlat [ncol] radians, ivolae
+// [10][4][12] (year, zone, month); year mod(kyrsav, 10) + 1 as Python's modulo gives it, month kmonsav.
+extern "C" int orc_setaer_volc(int nlay, int ncol, int ivflip, const float* plvl, const float* xlat,
+                               const int* ivolae, int kyrsav, int kmonsav, int add_sw, int add_lw, int lw1bd,
+                               float* aerosw, float* aerolw)
+{
+    if (nlay < 4 || ncol < 0 || kmonsav < 1 || kmonsav > 12) return 1;
+    const int y = ((kyrsav % 10) + 10) % 10;
+    int32_t iv[4];
+    for (int z = 0; z < 4; ++z) iv[z] = ivolae[(y * 4 + z) * 12 + (kmonsav - 1)];
+#pragma omp parallel for schedule(static)
+    for (int col = 0; col < ncol; ++col) {
+        std::vector<float> pi(nlay + 1);
+        for (int k = 0; k <= nlay; ++k) pi[k] = plvl[(size_t)k * ncol + col];
+        orc::aer::volcanic(nlay, ivflip, pi.data(), xlat[col], iv, add_sw != 0, add_lw != 0, lw1bd != 0,
+                           aerosw + col, aerolw + col, (size_t)ncol);
+    }
+    return 0;
+}
+
 // Solar geometry (rrtm_solar.hpp).  Same signature as the reference driver's: date[6] = year, month, day,
 // hour, minute, second; state[5] = sollag, sindec, cosdec, anginc, solcon; then coszen / coszdg of n columns.
 extern "C" int orc_solar(const int* date, float deltsw, float deltim, double solc0, float* state, int* nstp, int n,

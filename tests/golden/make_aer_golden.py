@@ -10,6 +10,12 @@ Keys, per case ("jan_nam": January, 16 columns over the NAM domain; "jul_globe":
     faerlw      [3][16][nlay][ncol]
     tab_*       the derived tables (oracle.AER_TAB_FIELDS)
 
+and the volcanic term (setaer's lavoflg branch, orc_setaer_volc: phys_rrtm_setaer_prep then
+phys_rrtm_setaer_volc) added to the "jul_globe" optics, per case of VOLC_CASES (ivflip, lw1bd, kyrsav,
+kmonsav), on a seeded ivolae table and latitudes across the seven zone bands and their edges:
+    volc_in_ivolae, volc_in_xlat, volc_<case>_extsw [14][nlay][ncol], volc_<case>_extlw [16][nlay][ncol]
+(the term changes the extinction, component 0, only)
+
 Run from the repository root:  python tests/golden/make_aer_golden.py
 """
 from __future__ import annotations
@@ -28,6 +34,16 @@ from woof_nam_b200.columns import make_columns  # noqa: E402
 
 OUT = Path(__file__).resolve().parent / "aer_golden.npz"
 CASES = {"jan_nam": (1, 16, 301, "nam"), "jul_globe": (7, 16, 302, "globe")}
+VOLC_CASES = {"top_first": (0, 0, 2026, 7), "surface_first": (1, 0, 1991, 6), "one_lw_band": (0, 1, 7, 12)}
+
+
+def volc_inputs(ncol: int, seed: int = 303):
+    """ivolae int32 [10][4][12] and latitudes (radians) in every zone band and on the band edges."""
+    r = np.random.default_rng(seed)
+    ivolae = r.integers(0, 500, (10, 4, 12)).astype(np.int32)
+    deg = np.array([89.0, 72.0, 46.0, 45.5, 44.0, 30.0, 1.0, 0.25, -1.0, -20.0, -44.0, -45.0, -46.0, -70.0, -80.5,
+                    -90.0][:ncol], np.float32)
+    return ivolae, np.radians(deg).astype(np.float32)
 
 
 def main():
@@ -47,6 +63,16 @@ def main():
         blob[f"{case}_faerlw"] = r["faerlw"]
         for name, _ in oracle.AER_TAB_FIELDS:
             blob[f"{case}_tab_{name}"] = r[name]
+    ivolae, xlat = volc_inputs(16)
+    blob["volc_in_ivolae"], blob["volc_in_xlat"] = ivolae, xlat
+    plvl = blob["jul_globe_in_plvl"]
+    for case, (ivflip, lw1bd, kyrsav, kmonsav) in VOLC_CASES.items():
+        pl = plvl if ivflip == 0 else np.ascontiguousarray(plvl[::-1])
+        v = oracle.setaer_volc(pl, xlat, ivolae, kyrsav, kmonsav, blob["jul_globe_faersw"], blob["jul_globe_faerlw"],
+                               ivflip=ivflip, lw1bd=bool(lw1bd), which="ref")
+        for k in ("faersw", "faerlw"):
+            assert np.array_equal(v[k][1:], blob[f"jul_globe_{k}"][1:])
+        blob[f"volc_{case}_extsw"], blob[f"volc_{case}_extlw"] = v["faersw"][0], v["faerlw"][0]
     np.savez_compressed(OUT, **blob)
     print(f"wrote {OUT} ({OUT.stat().st_size / 1e3:.0f} kB)")
 

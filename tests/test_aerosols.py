@@ -1,7 +1,8 @@
 """The climatological aerosol optics (setaer / aer_property, NAM iaer = 11) in the oracle, pinned to the
 reference's own kernels: the float restatement reproduces the golden vectors of aer_init, clim_aerinit,
 aer_update's month fill, setaer and aer_property bit for bit, and the packed climatology has the shape and
-ranges the kernels assume."""
+ranges the kernels assume.  The volcanic term (setaer's lavoflg branch) reproduces phys_rrtm_setaer_volc's
+golden vectors in both level orders and with the one-broad-band LW factor."""
 from __future__ import annotations
 
 from pathlib import Path
@@ -15,6 +16,7 @@ from woof_nam_b200.columns import Columns, make_columns
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "aer_golden.npz"
 CASES = ("jan_nam", "jul_globe")
+VOLC_CASES = {"top_first": (0, 0, 2026, 7), "surface_first": (1, 0, 1991, 6), "one_lw_band": (0, 1, 7, 12)}
 
 
 @pytest.fixture(scope="module")
@@ -75,3 +77,32 @@ def test_inputs_in_range():
         ai = aerosols.make_inputs(cols, 9, region)
         assert ai["rhly"].shape == (cols.nlay, cols.ncol) and 0 <= ai["rhly"].min() and ai["rhly"].max() <= 1
         assert np.abs(ai["xlat"]).max() <= np.pi / 2
+
+
+@pytest.mark.parametrize("case", list(VOLC_CASES))
+def test_volcanic_bit_exact(gold, case):
+    ivflip, lw1bd, kyrsav, kmonsav = VOLC_CASES[case]
+    pl = gold["jul_globe_in_plvl"]
+    pl = pl if ivflip == 0 else np.ascontiguousarray(pl[::-1])
+    r = oracle.setaer_volc(pl, gold["volc_in_xlat"], gold["volc_in_ivolae"], kyrsav, kmonsav,
+                           gold["jul_globe_faersw"], gold["jul_globe_faerlw"], ivflip=ivflip, lw1bd=bool(lw1bd))
+    assert np.array_equal(r["faersw"][0], gold[f"volc_{case}_extsw"])
+    assert np.array_equal(r["faerlw"][0], gold[f"volc_{case}_extlw"])
+    assert np.array_equal(r["faersw"][1:], gold["jul_globe_faersw"][1:])
+    # the term lies between 5 mb and 250 mb at most, and adds to every column
+    added = r["faerlw"][0] - gold["jul_globe_faerlw"][0]
+    assert (added >= 0).all() and (added.sum(axis=(0, 1)) > 0).all()
+
+
+def test_volcanic_switches(gold):
+    pl, xl, iv = gold["jul_globe_in_plvl"], gold["volc_in_xlat"], gold["volc_in_ivolae"]
+    sw, lw = gold["jul_globe_faersw"], gold["jul_globe_faerlw"]
+    r = oracle.setaer_volc(pl, xl, iv, 3, 2, sw, lw, add_sw=False, add_lw=False)
+    assert np.array_equal(r["faersw"], sw) and np.array_equal(r["faerlw"], lw)
+    only_lw = oracle.setaer_volc(pl, xl, iv, 3, 2, sw, lw, add_sw=False)
+    both = oracle.setaer_volc(pl, xl, iv, 3, 2, sw, lw)
+    assert np.array_equal(only_lw["faersw"], sw) and np.array_equal(only_lw["faerlw"], both["faerlw"])
+    # the year index is kyrsav mod 10 as Python takes it: -7 and 3 read the same year
+    assert np.array_equal(oracle.setaer_volc(pl, xl, iv, -7, 2, sw, lw)["faersw"], both["faersw"])
+    with pytest.raises(ValueError):
+        oracle.setaer_volc(pl, xl, iv, 3, 13, sw, lw)

@@ -255,3 +255,43 @@ def test_grrad_aerosols_unit_feeds_the_solve():
     torch.cuda.synchronize()
     assert torch.equal(ctx.st["htlwc"].reshape(ref["htlw"].shape), ref["htlw"])
     assert torch.equal(ctx.st["HTSWC"].reshape(ref["htsw"].shape), ref["htsw"])
+
+
+@pytest.mark.gpu
+def test_grrad_aerosols_unit_flags_and_volcanic():
+    """The unit under rad_initialize's flags (ctx.tables["rad_physparam"]): iaer = 111 adds the volcanic term
+    from ctx.tables["aer_ivolae"] for the year and month of ctx.tables["aer_volc"] to the climatological
+    optics of the calls that are due (here SW only, so the LW optics are zeros), as setaer does
+    (phys_rrtm_setaer.py:150-192); iaer = 0 gives zeros."""
+    import datetime
+    from types import SimpleNamespace
+
+    import torch
+    from woof_nam_b200 import aerosols, grrad_aerosols
+    from woof_nam_b200.solver import RadSolver
+    cols = make_columns(JM * IM, 29)
+    ai = aerosols.make_inputs(cols, 7, "globe")
+    ctx = _ctx(cols)
+    ctx.start = datetime.datetime(2026, 9, 1)
+    ctx.st["RAD_RHLY"] = torch.from_numpy(ai["rhly"].reshape(cols.nlay, JM, IM).copy()).cuda()
+    for name, key in (("XLON", "xlon"), ("XLAT", "xlat"), ("SLMSK", "slmsk")):
+        ctx.st[name] = torch.from_numpy(ai[key].reshape(JM, IM).copy()).cuda()
+    iv = np.random.default_rng(2).integers(0, 600, (10, 4, 12)).astype(np.int32)
+    flags = np.zeros(26, np.int32)
+    flags[4:8] = (111, 1, 1, 1)                   # iaerflg, laswflg, lalwflg, lavoflg
+    ctx.tables.update(rad_physparam=flags, aer_ivolae=iv, aer_volc=SimpleNamespace(kyrsav=1994, kmonsav=9))
+    o = grrad_aerosols.run(ctx, lsswr=True, lslwr=False)
+    torch.cuda.synchronize()
+    s = RadSolver()
+    dev = s.to_device(cols)
+    t = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in ai.items()}
+    fsw, flw = aerosols.Aerosols(s, 9).optics(dev, t["rhly"], t["xlon"], t["xlat"], t["slmsk"])
+    aerosols.volcanic(s, dev["plvl"], t["xlat"], iv, 1994, 9, (fsw, flw), add_lw=False)
+    torch.cuda.synchronize()
+    assert torch.equal(o["faersw"].reshape(fsw.shape), fsw)
+    assert not o["faerlw"].any()
+    flags[4:8] = (0, 0, 0, 0)
+    ctx.tables.pop("aer_state", None)
+    o = grrad_aerosols.run(ctx, lsswr=True, lslwr=True)
+    torch.cuda.synchronize()
+    assert not o["faersw"].any() and not o["faerlw"].any()

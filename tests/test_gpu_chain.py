@@ -2,7 +2,8 @@
 getozn, getgases, progcld2, setalb, setemis, then the LW and SW solve, one stream) against the same chain in
 the oracle -- the restatement's front end feeding the float64 solve -- within the mixed-precision tolerances
 (0.05 W/m^2, 0.01 K/day).  A second call on the work tensors of the first gives the same bits, and so does
-a CUDA graph of the whole call."""
+a CUDA graph of the whole call.  With the climatological aerosol optics in the call (setaer, January) the same
+holds against the oracle's chain with its aerosol restatement."""
 from __future__ import annotations
 
 import numpy as np
@@ -39,7 +40,7 @@ def _sun():
     return solar.sol_update((2026, 7, 1, 14, 30, 0), deltsw=1200.0, deltim=25.0)
 
 
-def _oracle_chain(state, tab, lay, sun):
+def _oracle_chain(state, tab, lay, sun, month=None):
     n = IM * JM
     dp = oracle.dayparts(state["glon"], state["sinlat"], state["coslat"], IM, CALL["solhr"], CALL["dtswav"],
                          CALL["nrads"], [sun["sollag"], sun["sindec"], sun["cosdec"]])
@@ -57,7 +58,11 @@ def _oracle_chain(state, tab, lay, sun):
                    olyr=olyr, gasvmr=gas, clouds=cld["clouds"], sfcemis=ems, tsfg=lay["tsfg"], sfcalb=alb,
                    coszen=dp["coszen"], solcon=float(sun["solcon"]))
     assert 0 < (dp["coszen"] >= 1e-4).sum() < n          # day and night in the domain
-    return oracle.solve(cols, precision="double")
+    if month is None:
+        return oracle.solve(cols, precision="double")
+    aer = oracle.aerosols(oracle.aer_climatology(month), cols,
+                          {"rhly": lay["rhly"], "xlon": state["glon"], "xlat": state["glat"], "slmsk": state["slmsk"]})
+    return oracle.solve(cols, precision="double", faersw=aer["faersw"], faerlw=aer["faerlw"])
 
 
 def _dev(state, tab):
@@ -98,3 +103,20 @@ def test_chain_against_oracle_and_graph():
     torch.cuda.synchronize()
     for k in first:
         assert np.array_equal(outs[k].cpu().numpy(), first[k]), k
+
+
+def test_chain_with_aerosols():
+    import torch
+    from woof_nam_b200 import aerosols
+    from woof_nam_b200.chain import radiation_call
+    from woof_nam_b200.solver import RadSolver
+    state, tab, lay = _domain(57)
+    sun = _sun()
+    s = RadSolver(precision="mixed", nlay=lay["plyr"].shape[0])
+    d, c = _dev(state, tab)
+    out = radiation_call(s, d, c, sun=sun, im=IM, aerosols=aerosols.Aerosols(s, 1), **CALL)
+    torch.cuda.synchronize()
+    got = {k: v.cpu().numpy() for k, v in out.items() if k != "work"}
+    assert out["work"]["faer"][0].abs().sum().item() > 0
+    ref = _oracle_chain(state, tab, lay, sun, month=1)
+    assert_within(got, {k: ref[k] for k in got}, what="radiation call with aerosol")

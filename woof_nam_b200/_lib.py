@@ -201,6 +201,9 @@ SIGNATURES = {
                       ctypes.POINTER(RadCloudCfg), ctypes.POINTER(RadCloudOut), ctypes.c_void_p], ctypes.c_int),
     "rad_setaer": ([ctypes.c_void_p, ctypes.POINTER(RadAerColumns), ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                     ctypes.c_void_p], ctypes.c_int),
+    "rad_setaer_volc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                         ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                         ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "rad_queue_create": ([ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, ctypes.c_int64,
                           ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "rad_submit": ([ctypes.c_void_p, ctypes.POINTER(RadColumns), ctypes.POINTER(RadOutputs), ctypes.c_int64,

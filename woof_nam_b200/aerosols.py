@@ -134,3 +134,37 @@ class Aerosols:
                               ctypes.c_void_p(out[1].data_ptr()), ctypes.c_void_p(st.cuda_stream))
         _lib.check(s.lib, s.handle, rc, "rad_setaer")
         return out
+
+
+def volcanic(solver, plvl, xlat, ivolae, kyrsav: int, kmonsav: int, faer: tuple, ivflip: int = 0,
+             add_sw: bool = True, add_lw: bool = True, lw1bd: bool = False, stream=None) -> tuple:
+    """setaer's stratospheric volcanic term (lavoflg; rad_setaer_volc) added in place to the extinction of
+    faer = (faersw [3, 14, nlay, ncol], faerlw [3, 16, nlay, ncol]) CUDA float32, after Aerosols.optics.
+    plvl [nlay + 1, ncol] mb in the order of ivflip and xlat [ncol] radians: contiguous float32 CUDA tensors;
+    ivolae: the int32 [10, 4, 12] (year, zone, month) table on the host (numpy or a CPU tensor), read for year
+    kyrsav mod 10 and month kmonsav."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from . import _lib
+    for k, v in (("plvl", plvl), ("xlat", xlat), ("faersw", faer[0]), ("faerlw", faer[1])):
+        if not (isinstance(v, torch.Tensor) and v.is_cuda and v.dtype == torch.float32 and v.is_contiguous()):
+            raise TypeError(f"volcanic input {k} must be a contiguous float32 CUDA tensor")
+    iv = ivolae.cpu().numpy() if isinstance(ivolae, torch.Tensor) else ivolae
+    iv = np.ascontiguousarray(iv, dtype=np.int32)
+    if iv.shape != (10, 4, 12):
+        raise ValueError(f"ivolae must be int32 [10, 4, 12], got {iv.shape}")
+    ncol = plvl.shape[1]
+    if tuple(faer[0].shape[-1:]) != (ncol,) or tuple(faer[1].shape[-1:]) != (ncol,) or tuple(xlat.shape) != (ncol,):
+        raise ValueError("volcanic: plvl, xlat and faer disagree on the column count")
+    st = stream if stream is not None else torch.cuda.current_stream()
+    s = solver
+    rc = s.lib.rad_setaer_volc(s.handle, ctypes.c_void_p(plvl.data_ptr()), ctypes.c_void_p(xlat.data_ptr()), ncol,
+                               int(ivflip), iv.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), int(kyrsav),
+                               int(kmonsav), int(bool(add_sw)), int(bool(add_lw)), int(bool(lw1bd)),
+                               ctypes.c_void_p(faer[0].data_ptr()), ctypes.c_void_p(faer[1].data_ptr()),
+                               ctypes.c_void_p(st.cuda_stream))
+    _lib.check(s.lib, s.handle, rc, "rad_setaer_volc")
+    return faer

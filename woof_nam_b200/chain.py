@@ -10,6 +10,7 @@ its chain's scratch for the whole domain does not fit its cards and its SW group
     rad_dayparts      the SW interval's zenith cosine (coszen: the solve's day predicate) and the sunlit runs
     rad_getozn        olyr, climatological ozone on the layers (ntoz 0)
     rad_getgases      gasvmr on the layers
+    rad_setaer        faersw, faerlw: the climatological aerosol optics (iaer 11), when an Aerosols is given
     rad_progcld2      clouds (Ferrier, np3d 3) with gethml's deck fractions
     rad_setalb        sfcalb (from coszen for ialbflg 0 / 1)
     rad_setemis       sfcemis
@@ -37,10 +38,11 @@ CLOUD_NAM = dict(ivflip=0, llyr=2, iovr=1, lcrick=False, lcnorm=False, lnoprec=F
 
 def radiation_call(solver, state: dict, clim: dict, *, sun: dict, solhr: float, dtswav: float, nrads: int, im: int,
                    kmonsav: int, k1oz: int, k2oz: int, facoz: float, ico2flg: int = 1, ialbflg: int = 2,
-                   iemslw: int = 1, cloud: dict | None = None, work: dict | None = None, out: dict | None = None,
-                   stream=None) -> dict:
+                   iemslw: int = 1, cloud: dict | None = None, aerosols=None, work: dict | None = None,
+                   out: dict | None = None, stream=None) -> dict:
     """Run the call; returns the solve's outputs, with the front end's arrays under out["work"] (reused by the
-    next call when passed back as `work`)."""
+    next call when passed back as `work`).  aerosols: an aerosols.Aerosols with the month's climatology loaded
+    (the state then needs slmsk), or None for no aerosol; state faersw / faerlw are used when given instead."""
     cloud = {**CLOUD_NAM, **(cloud or {})}
     if cloud["ivflip"] != 0:
         raise ValueError("radiation_call: the layers of grrad's set-up are top first (ivflip 0)")
@@ -72,6 +74,9 @@ def radiation_call(solver, state: dict, clim: dict, *, sun: dict, solhr: float, 
     front.getgases(solver, lay["plvl"], state["glon"], state["glat"], w["gasvmr"], co2_glb=clim["co2_glb"],
                    gco2cyc=clim["gco2cyc"], co2vmr_sav=clim["co2vmr_sav"], ico2flg=ico2flg, kmonsav=kmonsav,
                    ivflip=0, stream=stream)
+    if aerosols is not None:
+        w["faer"] = aerosols.optics({k: lay[k] for k in ("plvl", "plyr", "tlyr", "qlyr")}, lay["rhly"], state["glon"],
+                                    state["glat"], state["slmsk"], out=w.get("faer"), stream=stream)
     cin = {k: lay[k] for k in ("plyr", "plvl", "tlyr", "tvly", "qlyr", "qstl", "rhly")}
     cin.update({k: state.get(k) for k in ("clw", "f_ice", "f_rain", "r_rime", "cldfk1")}, xlat=state["glat"])
     w["cloud"] = front.progcld2(solver, cin, **cloud, out=w["cloud"], stream=stream)
@@ -81,6 +86,8 @@ def radiation_call(solver, state: dict, clim: dict, *, sun: dict, solhr: float, 
     cols = {"plyr": lay["plyr"], "plvl": lay["plvl"], "tlyr": lay["tlyr"], "tlvl": lay["tlvl"], "qlyr": lay["qlyr"],
             "olyr": w["olyr"], "gasvmr": w["gasvmr"], "clouds": w["cloud"]["clouds"], "sfcemis": w["sfcemis"],
             "tsfg": lay["tsfg"], "sfcalb": w["sfcalb"], "coszen": coszen}
+    if aerosols is not None:
+        cols["faersw"], cols["faerlw"] = w["faer"]
     for k in ("faerlw", "faersw"):
         if state.get(k) is not None:
             cols[k] = state[k]

@@ -1094,6 +1094,38 @@ int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faers
     return RAD_OK;
 }
 
+int rad_setaer_volc(RadHandle* h, const float* plvl, const float* xlat, int64_t ncol, int32_t ivflip,
+                    const int32_t* ivolae, int32_t kyrsav, int32_t kmonsav, int32_t add_sw, int32_t add_lw,
+                    int32_t lw1bd, float* faersw, float* faerlw, void* stream)
+{
+    if (!h) return fail(h, RAD_E_INVALID, "rad_setaer_volc: null argument");
+    if (ncol < 0 || ncol > (int64_t)std::numeric_limits<int>::max() - 1)
+        return fail(h, RAD_E_INVALID, "rad_setaer_volc: ncol out of range");
+    if (h->cfg.nlay < 4 || h->cfg.nlay > NLAY_MAX) return fail(h, RAD_E_INVALID, "rad_setaer_volc: nlay out of range");
+    if (ivflip != 0 && ivflip != 1) return fail(h, RAD_E_INVALID, "rad_setaer_volc: ivflip must be 0 or 1");
+    if (kmonsav < 1 || kmonsav > 12) return fail(h, RAD_E_INVALID, "rad_setaer_volc: kmonsav outside 1..12");
+    if (!ivolae) return fail(h, RAD_E_INVALID, "rad_setaer_volc: ivolae is null");
+    if (ncol == 0 || (!add_sw && !add_lw)) return RAD_OK;
+    if (!plvl || !xlat || (add_sw && !faersw) || (add_lw && !faerlw))
+        return fail(h, RAD_E_INVALID, "rad_setaer_volc: a required pointer is null");
+    front::VolcArgs a{};
+    a.plvl = plvl; a.xlat = xlat; a.faersw = faersw; a.faerlw = faerlw; a.n = ncol;
+    a.nlay = h->cfg.nlay; a.ivflip = ivflip; a.add_sw = add_sw != 0; a.add_lw = add_lw != 0;
+    const int y = ((kyrsav % 10) + 10) % 10;                // Python's kyrsav % 10, as the reference's wrapper
+    for (int z = 0; z < 4; ++z) a.iv[z] = ivolae[(y * 4 + z) * 12 + (kmonsav - 1)];
+    for (int b = 0; b < AER_NSW; ++b) {
+        const float w1 = (float)aerh::WSW[0][b], w2 = (float)aerh::WSW[1][b];
+        const float e = w1 > 20000.0f ? 0.74f : (w2 < 20000.0f ? 1.14f : 0.94f);
+        a.tsw[b] = powf(0.275e-4f * (w2 + w1), e);
+    }
+    for (int b = 0; b < AER_NLW; ++b)
+        a.tlw[b] = lw1bd ? powf(0.55f / 11.0f, 1.2f)
+                         : powf(0.275e-4f * ((float)aerh::WLW[1][b] + (float)aerh::WLW[0][b]), 1.2f);
+    h->launches += 1;
+    RAD_CUDA(h, front::setaer_volc(a, (cudaStream_t)stream));
+    return RAD_OK;
+}
+
 int rad_grrad_setup(RadHandle* h, const RadModelColumns* in, int64_t ncol, int32_t lm, const RadLayerFields* out,
                     void* stream)
 {

@@ -25,6 +25,11 @@
 //   k_progcld2   progcld2 with rsipath2_tmp and gethml (radiation_clouds_nmmb.f:787-1323, 2167-2494,
 //                2779-2964; phys_rrtm_progcld2.cu:92-444): one thread per column; the layer cloud fractions
 //                that gethml walks twice are kept in shared memory, [layer][thread].
+//   k_setaer_volc  setaer's volcanic stratospheric term (radiation_aerosols.f 2092-2352, the lavoflg branch;
+//                namgpu/kernels/phys_rrtm_setaer.cu:178-330): one thread per column finds the aerosol's top
+//                (5 mb) and bottom (150-250 mb by latitude) layers and adds its zone's optical depth, spread
+//                by pressure depth, to the extinction of every band.  The per-band spectral factors are powf
+//                of constants, formed on the host so that they are the host's bits.
 //
 // Layouts: [field][level][column] with column = row * im + point, as the solve's inputs.  Every kernel is
 // HBM-bound: each input word is read once and each output word written once (the per-column bytes are in
@@ -589,6 +594,71 @@ __global__ void __launch_bounds__(CLD_THREADS) k_progcld2(const CloudArgs a)
     }
 }
 
+// ------------------------------------------------------------------------------------------ volcanic term
+// Per column (nlay + 1) * 4 bytes of pressure read, and the extinction of the 30 bands over the aerosol's
+// layers (about 15 of 61 on NAM's levels) read and written.
+__global__ void __launch_bounds__(256) k_setaer_volc(const __grid_constant__ VolcArgs a)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.n) return;
+    const size_t N = (size_t)a.n;
+    const int nlay = a.nlay;
+    auto P = [&](int i) { return __ldg(a.plvl + (size_t)i * N + c); };
+    const float pi = 3.1415926535897931f, rdg = 180.0f / pi, psrfh = 5.0f;
+    float lat = __ldg(a.xlat + c) * rdg;
+    if (lat < -90.0f) lat = -90.0f;
+    if (lat > 90.0f) lat = 90.0f;
+    float volcae;
+    if (lat > 46.0f)       volcae = 1.0e-4f * (float)a.iv[0];
+    else if (lat > 44.0f)  volcae = 5.0e-5f * (float)(a.iv[0] + a.iv[1]);
+    else if (lat > 1.0f)   volcae = 1.0e-4f * (float)a.iv[1];
+    else if (lat > -1.0f)  volcae = 5.0e-5f * (float)(a.iv[1] + a.iv[2]);
+    else if (lat > -44.0f) volcae = 1.0e-4f * (float)a.iv[2];
+    else if (lat > -46.0f) volcae = 5.0e-5f * (float)(a.iv[2] + a.iv[3]);
+    else                   volcae = 1.0e-4f * (float)a.iv[3];
+    const float alat = fabsf(lat);
+    const float psrfl = alat > 70.0f ? 250.0f : (alat < 20.0f ? 150.0f : 110.0f + 2.0f * alat);
+    // top and bottom layer (0-based) and 1 / the pressure depth between them
+    int kh, kl;
+    float rdelp;
+    if (a.ivflip == 0) {
+        kh = nlay - 2; kl = 1; rdelp = 1.0f / P(1);
+        for (int i = 1; i <= nlay - 3; ++i)
+            if (P(i) >= psrfh) { kh = i - 1; break; }
+        for (int i = 1; i <= nlay - 3; ++i)
+            if (P(i) >= psrfl) { kl = i - 1; rdelp = 1.0f / (P(i) - P(kh)); break; }
+    } else {
+        kh = 1; kl = nlay - 2; rdelp = 1.0f / P(nlay - 2);
+        for (int i = nlay - 2; i >= 1; --i)
+            if (P(i) >= psrfh) { kh = i; break; }
+        for (int i = nlay - 1; i >= 1; --i)
+            if (P(i) >= psrfl) { kl = i; rdelp = 1.0f / (P(i) - P(kh + 1)); break; }
+    }
+    const bool down = a.ivflip == 0;
+    const int j0 = down ? kh : kl, j1 = down ? kl : kh, below = down ? kl + 1 : kl - 1;
+    auto add = [&](float* x, float tb) {         // x: one band's [nlay][n] extinction at column c
+        for (int j = j0; j <= j1; ++j) {
+            const float share = down ? (P(j + 1) - P(j)) * rdelp : (P(j) - P(j + 1)) * rdelp;
+            const float tmp2 = tb * share;
+            x[(size_t)j * N] = x[(size_t)j * N] + tmp2 * volcae;
+        }
+    };
+    if (a.add_sw) {
+        for (int b = 0; b < 14; ++b) {
+            float* x = a.faersw + (size_t)b * nlay * N + c;
+            add(x, a.tsw[b]);
+            const float xl = x[(size_t)kl * N], xb = x[(size_t)below * N];
+            if (xl > 10.0f * xb) {                  // a sharp bottom edge is spread 80 / 20 over two layers
+                const float s2 = xl + xb;
+                x[(size_t)kl * N] = 0.8f * s2;
+                x[(size_t)below * N] = 0.2f * s2;
+            }
+        }
+    }
+    if (a.add_lw)
+        for (int b = 0; b < 16; ++b) add(a.faerlw + (size_t)b * nlay * N + c, a.tlw[b]);
+}
+
 inline unsigned blocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -641,6 +711,12 @@ cudaError_t progcld2(const CloudArgs& a, cudaStream_t st)
         if (e != cudaSuccess) return e;
     }
     k_progcld2<<<blocks(a.n, CLD_THREADS), CLD_THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t setaer_volc(const VolcArgs& a, cudaStream_t st)
+{
+    k_setaer_volc<<<blocks(a.n, 256), 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -76,5 +76,16 @@ struct CloudArgs {
 constexpr int CLOUD_MAX_LAY = 128;
 cudaError_t progcld2(const CloudArgs& a, cudaStream_t st);
 
+// setaer's volcanic stratospheric term on nlay layers of n columns, added in place to component 0 (extinction).
+struct VolcArgs {
+    const float *plvl, *xlat;                           // [nlay + 1][n] mb in the order of ivflip, [n] radians
+    float *faersw, *faerlw;                             // [3][14][nlay][n], [3][16][nlay][n]
+    int64_t n;
+    int32_t nlay, ivflip, add_sw, add_lw;
+    int32_t iv[4];                                      // the table's values of the 4 latitude zones, year and month
+    float tsw[14], tlw[16];                             // per band (0.275e-4 (w1 + w2))^e, by the host's powf
+};
+cudaError_t setaer_volc(const VolcArgs& a, cudaStream_t st);
+
 }  // namespace front
 }  // namespace rad

@@ -403,12 +403,38 @@ def _aer_month(ctx) -> int:
     return int(start.month)
 
 
+# Slots of rad_initialize's flag vector (namgpu/kernels/phys_rrtm_rad_initialize.cu:99-108).
+RI_IAERFLG, RI_LASWFLG, RI_LALWFLG, RI_LAVOFLG = 4, 5, 6, 7
+
+
+def _aer_flags(ctx) -> dict:
+    """setaer's module state (phys_rrtm_grrad_aerosols.py:63-85): ctx.tables["aer_state"] when grrad's aerosol
+    unit built it, else rad_initialize's flags in ctx.tables["rad_physparam"], else NAM's iaer = 11 (SW and LW
+    aerosol, no volcanic term).  kyrsav / kmonsav come from ctx.tables["aer_volc"] (default 1, 1)."""
+    tabs = getattr(ctx, "tables", None) or {}
+    st = tabs.get("aer_state")
+    if st is None:
+        p = tabs.get("rad_physparam")
+        if p is not None:
+            import numpy as np
+            p = np.asarray(p.get() if hasattr(p, "get") and not isinstance(p, dict) else p)
+            st = {"iaerflg": int(p[RI_IAERFLG]), "laswflg": bool(p[RI_LASWFLG]), "lalwflg": bool(p[RI_LALWFLG]),
+                  "lavoflg": bool(p[RI_LAVOFLG])}
+        else:
+            st = {"iaerflg": 11, "laswflg": True, "lalwflg": True, "lavoflg": False}
+        volc = tabs.get("aer_volc")
+        st = dict(st, kyrsav=int(getattr(volc, "kyrsav", 1)), kmonsav=int(getattr(volc, "kmonsav", 1)))
+    return st
+
+
 def grrad_aerosols_run(ctx, *, lsswr: bool = True, lslwr: bool = True) -> dict:
     """Drop-in for phys_rrtm_grrad_aerosols.run(ctx, lsswr=, lslwr=) (phys_rrtm_grrad_aerosols.py:124-136):
-    the climatological aerosol optics of every column of ctx.grid (NAM iaer = 11: SW and LW, no volcanic term),
-    written to ctx.tables["rrtm_faersw"] [3, 14, LMK, JM, IM] and ["rrtm_faerlw"] [3, 16, LMK, JM, IM], where
-    lwrad / swrad read them.  The month's tables are (re)loaded when the month changes."""
-    from .aerosols import Aerosols
+    setaer's aerosol optics of every column of ctx.grid, written to ctx.tables["rrtm_faersw"]
+    [3, 14, LMK, JM, IM] and ["rrtm_faerlw"] [3, 16, LMK, JM, IM], where lwrad / swrad read them, under the
+    module flags of _aer_flags (phys_rrtm_setaer.py:150-192): zeros unless a radiation call is due and iaerflg
+    > 0; the climatological optics of the calls the flags allow (the month's tables (re)loaded when the month
+    changes); then, with lavoflg, the volcanic term from ctx.tables["aer_ivolae"] (int32 [10, 4, 12])."""
+    from .aerosols import Aerosols, volcanic
     unit = "phys-rrtm-grrad-aerosols"
     st, g = ctx.st, ctx.grid
     jm, im, nlay = int(g.jm), int(g.im), int(g.lm) + 1
@@ -434,7 +460,28 @@ def grrad_aerosols_run(ctx, *, lsswr: bool = True, lslwr: bool = True) -> dict:
         flw = torch.zeros((3, 16, nlay, jm, im), dtype=torch.float32, device="cuda")
     stream = _stream(ctx)
     out = (fsw.view(3, 14, nlay, jm * im), flw.view(3, 16, nlay, jm * im))
-    aer.optics(cols, cols["rhly"], cols["xlon"], cols["xlat"], cols["slmsk"], out=out, stream=stream)
+    fl = _aer_flags(ctx)
+    laersw, laerlw = bool(lsswr and fl["laswflg"]), bool(lslwr and fl["lalwflg"])
+    with torch.cuda.stream(stream):
+        if fl["iaerflg"] > 0 and (lsswr or lslwr) and (fl["laswflg"] or fl["lalwflg"]):
+            aer.optics(cols, cols["rhly"], cols["xlon"], cols["xlat"], cols["slmsk"], out=out, stream=stream)
+            if not laersw:
+                fsw.zero_()
+            if not laerlw:
+                flw.zero_()
+        else:
+            fsw.zero_()
+            flw.zero_()
+    if fl["iaerflg"] > 0 and (lsswr or lslwr) and fl["lavoflg"]:
+        add_sw = bool(lsswr) if fl["iaerflg"] == 100 else laersw
+        add_lw = bool(lslwr) if fl["iaerflg"] == 100 else laerlw
+        iv = tabs.get("aer_ivolae")
+        if iv is None:
+            raise RuntimeError(f"{unit}: lavoflg needs ctx.tables['aer_ivolae'] (int32 [10, 4, 12])")
+        if hasattr(iv, "get") and not isinstance(iv, dict):
+            iv = iv.get()
+        volcanic(s, cols["plvl"], cols["xlat"], iv, fl["kyrsav"], fl["kmonsav"], out, add_sw=add_sw, add_lw=add_lw,
+                 stream=stream)
     tabs["rrtm_faersw"], tabs["rrtm_faerlw"] = fsw, flw
     return {"faersw": fsw, "faerlw": flw}
 
