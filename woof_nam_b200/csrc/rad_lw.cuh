@@ -41,7 +41,7 @@ struct LwSetup {
     R secdiff[16], semiss[16];
     R stemp, pwvcm;
     int laytrop, lcf1;
-    int task_next;            // phase B task counter (for_each_band_pair)
+    int task_next;            // phase B task counter (for_each_band_flat)
     // per-layer and per-column terms of the band kernels that do not depend on the g-point, formed once in phase
     // A2 instead of in every (g-point, layer) task: the minor-gas column adjustments (adjcol) of bands 3 / 9, 6,
     // 7, 8, 13, and the ratios of reference mixing ratios (chi) that key the minor / Planck-fraction species
@@ -1042,7 +1042,7 @@ __device__ void lw_setup_core(S& s, const LwIn& a, int64_t col, int tid, Sink si
         if (lane == 0) lw_overlap(s, nlay);
         __syncwarp();
     }
-    for_each_band_pair(c_lw_ns, 16, nlay, &s.task_next, lane, [&](int g, int k0, int band) {
+    for_each_band_flat(c_lw_ns, 16, nlay, &s.task_next, lane, [&](int g, int k0, int band) {
         R tg, fr;
         lw_gas(s, g, k0, tg, fr, band);
         sink(g, k0, tg + s.tauaer[band][k0], fr);

@@ -186,7 +186,7 @@ sw4_gas_kernel(const __grid_constant__ SwBatch bt, int any_aer, int* err, int d0
     int4* im = img + (size_t)blockIdx.x * (sw4_image_bytes(any_aer) / 16);
     float* img_taug = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(im) + (offsetof(SwSh2, taug) - sw4_image_begin()));
     sw2_setup(s, aer, a, col, d, tid);
-    for_each_band_pair(c_sw_ns, 14, nlay, &s.task_next, tid & 31, [&](int g, int k0, int b) {
+    for_each_band_flat(c_sw_ns, 14, nlay, &s.task_next, tid & 31, [&](int g, int k0, int b) {
         float tg, tr;
         sw_gas<float>(s, g, k0, tg, tr, b);
         img_taug[k0 * SW_NGPT + g] = tg;
