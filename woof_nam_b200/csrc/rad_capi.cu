@@ -695,10 +695,14 @@ int rad_create(const RadConfig* cfg, RadHandle** out)
         return fail(nullptr, RAD_E_INVALID, "rad_create: the McICA route runs in the mixed precision");
     if (cfg->iovrlw < 0 || cfg->iovrlw > 2 || cfg->iovrsw < 0 || cfg->iovrsw > 2)
         return fail(nullptr, RAD_E_INVALID, "rad_create: iovrlw and iovrsw must be 0, 1 or 2");
+    int device = 0, nsm = 0;
+    if (cudaGetDevice(&device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+        return fail(nullptr, RAD_E_CUDA, "rad_create: no usable CUDA device");
     RadHandle* h = new RadHandle();
     h->cfg = *cfg;
-    cudaGetDevice(&h->device);
-    cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device);
+    h->device = device;
+    h->nsm = nsm;
     if (cudaMalloc((void**)&h->d_err, sizeof(int)) != cudaSuccess ||
         cudaMalloc((void**)&h->d_nday, sizeof(int)) != cudaSuccess) {
         delete h;
@@ -856,7 +860,7 @@ int rad_solve_batch(RadHandle* h, int32_t nreq, const RadColumns* ins, const Rad
         if (rc) return rc;
     }
     int dev = 0;
-    cudaGetDevice(&dev);
+    RAD_CUDA(h, cudaGetDevice(&dev));
     if (dev != h->device) return fail(h, RAD_E_INVALID, "rad_solve: handle belongs to another device");
     cudaStream_t st = (cudaStream_t)stream;
     int32_t r0 = 0;
