@@ -623,8 +623,8 @@ int launch_batch(RadHandle* h, int nreq, const RadColumns* ins, const RadOutputs
                 RAD_CUDA(h, cudaFuncSetAttribute((void*)sw4_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
                 for (int64_t d0 = 0; d0 < ntot; d0 += swc) {
                     const int64_t nc = std::min(swc, ntot - d0);
-                    sw4_gas_kernel<<<(unsigned)nc, SW2_THREADS, smem0, st>>>(bt, any_aer ? 1 : 0, h->d_err, (int)d0, h->d_sw4img);
-                    sw4_rt_kernel<<<(unsigned)nc, SW2_THREADS, smem1, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, (int)d0,
+                    sw4_gas_kernel<<<(unsigned)nc, SW4_GAS_THREADS, smem0, st>>>(bt, any_aer ? 1 : 0, h->d_err, (int)d0, h->d_sw4img);
+                    sw4_rt_kernel<<<(unsigned)nc, SW4_RT_THREADS, smem1, st>>>(bt, any_aer ? 1 : 0, h->d_swf, h->d_swd, (int)d0,
                                                                          h->d_sw4img, h->d_sw4, bb);
                     if (diag_sw) {
                         sw4_sweep_kernel<true><<<(unsigned)nc, SW2_THREADS, smem2, st>>>(bt, h->d_err, (int)d0, (int)nc,

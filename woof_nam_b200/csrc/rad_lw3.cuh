@@ -4,7 +4,7 @@
 // 68 KB) in shared memory, so two CTAs fit an SM and the latency-bound table gathers and sweep recurrences
 // run with ten warps per SM.  Here the gas optics go through HBM instead:
 //
-//   lw3_optics_kernel  one CTA (160 threads) per column: phases A and B of lw_setup_core (absorber amounts,
+//   lw3_optics_kernel  one CTA (288 threads) per column: phases A and B of lw_setup_core (absorber amounts,
 //                      cldprop, setcoef, Planck functions, taugb01..16, the max-random overlap factors of
 //                      rtrnmr), with taug / fracs written straight to the chunk's scratch and the sweep inputs
 //                      copied after them.  Shared memory is the set-up data only (~32 KB).
@@ -60,7 +60,12 @@ __host__ __device__ constexpr int64_t lw3_block_floats(int nlay)
     return (int64_t)2 * nlay * LW3_GSTRIDE + lw3_rec_floats(nlay);
 }
 
-constexpr int LW3_OPT_THREADS = 160;   // optics CTA: 5 warps
+// Optics CTA: 9 warps, 3 CTAs per SM (27 warps, at most 72 registers a thread, no spills).  The CTAs per SM set
+// how many columns share an SM's L1 for the table gathers, and more than 3 cost more than they gain; more warps
+// per CTA share a column's (g-point, layer) tasks and hide the gathers' latency.  Measured over the LW of 262,144
+// columns: 160 threads 66.1 ms, 192 63.3, 224 61.4, 256 60.5, 288 60.0, 320 63.8 (spills); 4 CTAs of 224 / 256
+// threads 64.0 / 70.1, 2 of 320 / 384 threads 64.0 / 62.6.  Same bits for every shape.
+constexpr int LW3_OPT_THREADS = 288;
 constexpr int LW3_OPT_MINB = 3;        // CTAs per SM the optics kernel is compiled for
 
 __global__ void __launch_bounds__(LW3_OPT_THREADS, LW3_OPT_MINB) lw3_optics_kernel(const __grid_constant__ LwBatch bt, int64_t c0,

@@ -738,6 +738,7 @@ inline int64_t sw2_rt_bytes(int nsm) { return (int64_t)SW2_CTAS_PER_SM * nsm * s
 // Phases A1 and A2 of one sunlit column (day index d, column col of request a) into shared memory s (aer: the
 // aerosol block or null): layer coefficients, aerosol, heating factors, column scalars, cloud optics per (band,
 // layer), solar source, Rayleigh coefficients.  Ends with a barrier.
+template <int NT = SW2_THREADS>
 __device__ __forceinline__ void sw2_setup(SwSh2& s, SwAer* aer, const SwIn& a, int64_t col, int d, int tid)
 {
     const int nlay = a.nlay;
@@ -746,7 +747,7 @@ __device__ __forceinline__ void sw2_setup(SwSh2& s, SwAer* aer, const SwIn& a, i
     // ---- phase A1: layer coefficients (threads = layers), aerosol, heating factors.  The coefficients are
     // formed in float64 and rounded once: the interpolation weights take a difference of logarithms, which
     // float would carry with ~1e-6 of the gas optical depths' error (and move their exp-table entries).
-    for (int k0 = tid; k0 < nlay; k0 += SW2_THREADS) {
+    for (int k0 = tid; k0 < nlay; k0 += NT) {
         SwCoef<double> c;
         sw2_layer_coef<double>(a, col, k0, c);
         s.fac00[k0] = (float)c.fac00; s.fac01[k0] = (float)c.fac01; s.fac10[k0] = (float)c.fac10;
@@ -811,11 +812,11 @@ __device__ __forceinline__ void sw2_setup(SwSh2& s, SwAer* aer, const SwIn& a, i
         s.task_next = 0;
     }
     if (a.mask)
-        for (int i = tid; i < 4 * nlay; i += SW2_THREADS)
+        for (int i = tid; i < 4 * nlay; i += NT)
             s.mcw[i / nlay][i % nlay] = __ldg(a.mask + ((size_t)(i / nlay) * nlay + (i % nlay)) * N + col);
     __syncthreads();
     // ---- phase A2: cloud optics per (band, layer); solar source per band
-    for (int p = tid; p < 14 * nlay; p += SW2_THREADS) {
+    for (int p = tid; p < 14 * nlay; p += NT) {
         const int ib = p / nlay, k0 = p - ib * nlay;
         float tcw = 0, scw = 0, acw = 0, tab_ = 0;
         if (s.zcf1 > 0) sw2_cloud<float>(a, col, k0, ib, s.cfrac[k0], tcw, scw, acw, tab_);
@@ -823,7 +824,7 @@ __device__ __forceinline__ void sw2_setup(SwSh2& s, SwAer* aer, const SwIn& a, i
         if (ib == 0) s.cldfrc[k0] = s.zcf1 > 0 ? s.cfrac[k0] / s.zcf1 : 0.0f;
     }
     if (tid < 14) sw_sfluxzen<float>(s, tid, nlay);
-    for (int g = tid; g < SW_NGPT; g += SW2_THREADS) s.raylc[g] = sw2_rayl_coef(g);
+    for (int g = tid; g < SW_NGPT; g += NT) s.raylc[g] = sw2_rayl_coef(g);
     __syncthreads();
 }
 

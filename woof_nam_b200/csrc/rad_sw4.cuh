@@ -28,9 +28,14 @@ namespace rad {
 
 constexpr int SW4_FIELDS = 6;                       // rb, rd, tb, td, e3 (delta-scaled beam), e4 (unscaled beam)
 constexpr int SW4_LAYER = SW4_FIELDS * SW_NGPT;     // floats per layer and pass, [field][g]
+// CTA shapes of the three kernels, swept on the B200 (same bits): the gas-optics kernel at 128 threads x 6 CTAs
+// per SM against 160 x 5, 192 x 4, 256 x 3, 320 x 2, 384 x 2 (SW +0.2 to +9.8 %); the R/T kernel at 128 x 4
+// against 160 x 3, 192 x 3, 224 x 2, 256 x 2 (+1.8 to +8.3 %).
+constexpr int SW4_RT_THREADS = 128;                 // threads of an R/T CTA
 constexpr int SW4_OPT_MINB = 4;                     // CTAs per SM the R/T kernel is compiled for
 constexpr bool SW4_RT_PAIR = false;                 // two R/T tasks per thread side by side (else one)
 constexpr int SW4_SWEEP_MINB = 6;                   // ... and the sweep kernel
+constexpr int SW4_GAS_THREADS = 128;               // threads of a gas-optics CTA
 constexpr int SW4_GAS_MINB = 6;                     // ... and the gas-optics kernel
 constexpr bool SW4_L2PF = true;                     // the sweeps prefetch the R/T rows two segments ahead into L2
 
@@ -165,7 +170,7 @@ __host__ __device__ inline const float* sw4_image_taug(const int4* im)
 }
 
 // Set-up, cloud optics and gas optics of one sunlit column (one CTA, six per SM) into its image.
-__global__ void __launch_bounds__(SW2_THREADS, SW4_GAS_MINB)
+__global__ void __launch_bounds__(SW4_GAS_THREADS, SW4_GAS_MINB)
 sw4_gas_kernel(const __grid_constant__ SwBatch bt, int any_aer, int* err, int d0, int4* img)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -185,7 +190,7 @@ sw4_gas_kernel(const __grid_constant__ SwBatch bt, int any_aer, int* err, int d0
     const int tid = threadIdx.x;
     int4* im = img + (size_t)blockIdx.x * (sw4_image_bytes(any_aer) / 16);
     float* img_taug = reinterpret_cast<float*>(reinterpret_cast<unsigned char*>(im) + (offsetof(SwSh2, taug) - sw4_image_begin()));
-    sw2_setup(s, aer, a, col, d, tid);
+    sw2_setup<SW4_GAS_THREADS>(s, aer, a, col, d, tid);
     for_each_band_flat(c_sw_ns, 14, nlay, &s.task_next, tid & 31, [&](int g, int k0, int b) {
         float tg, tr;
         sw_gas<float>(s, g, k0, tg, tr, b);
@@ -197,10 +202,10 @@ sw4_gas_kernel(const __grid_constant__ SwBatch bt, int any_aer, int* err, int d0
     const int n1 = (int)((offsetof(SwSh2, taug) - sw4_image_begin()) / 16);
     const int n2 = any_aer ? (int)(sizeof(SwAer) / 16) : 0;
     const int skip = (int)(sizeof(SwSh2::taug) / 16);
-    for (int i = tid; i < n1 + n2; i += SW2_THREADS) im[i < n1 ? i : i + skip] = sm[i];
+    for (int i = tid; i < n1 + n2; i += SW4_GAS_THREADS) im[i < n1 ? i : i + skip] = sm[i];
 }
 
-__global__ void __launch_bounds__(SW2_THREADS, SW4_OPT_MINB)
+__global__ void __launch_bounds__(SW4_RT_THREADS, SW4_OPT_MINB)
 sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, const double* exd, int d0,
               const int4* img, unsigned char* scr, size_t blk_bytes)
 {
@@ -226,7 +231,7 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
         const int n1 = (int)((offsetof(SwSh2, taug) - sw4_image_begin()) / 16);
         const int n2 = any_aer ? (int)(sizeof(SwAer) / 16) : 0;
         const int skip = (int)(sizeof(SwSh2::taug) / 16);
-        for (int i = tid; i < n1 + n2; i += SW2_THREADS)
+        for (int i = tid; i < n1 + n2; i += SW4_RT_THREADS)
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sb + 16u * (uint32_t)i),
                          "l"(im + (i < n1 ? i : i + skip))
                          : "memory");
@@ -259,13 +264,13 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
         H.zcf0 = s.zcf0; H.zcf1 = s.zcf1;
         *qn = 0;
     }
-    for (int k0 = tid; k0 < nlay; k0 += SW2_THREADS) H.rdelp[k0] = s.rdelp[k0];
-    for (int g = tid; g < SW_NGPT; g += SW2_THREADS) H.zsolar[g] = s.ssolar * s.sfluxzen[g];
+    for (int k0 = tid; k0 < nlay; k0 += SW4_RT_THREADS) H.rdelp[k0] = s.rdelp[k0];
+    for (int g = tid; g < SW_NGPT; g += SW4_RT_THREADS) H.zsolar[g] = s.ssolar * s.sfluxzen[g];
     __syncthreads();
     const float cz = s.cosz, snt = s.sntz;
     const double czd = (double)__ldg(a.coszen + col);
     __shared__ unsigned char gband[SW_NGPT];
-    for (int g = tid; g < SW_NGPT; g += SW2_THREADS) {
+    for (int g = tid; g < SW_NGPT; g += SW4_RT_THREADS) {
         int ib = 0;
         while (g >= c_sw_ns[ib + 1]) ++ib;
         gband[g] = (unsigned char)ib;
@@ -295,7 +300,7 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
     // (qbit marks it) and formed afterwards by sw2_layer, one per thread
     __shared__ unsigned qbit[NLAY_MAX][4];
     __shared__ signed char slotk[NLAY_MAX];
-    for (int j = tid; j < NLAY_MAX * 4; j += SW2_THREADS) qbit[j >> 2][j & 3] = 0u;
+    for (int j = tid; j < NLAY_MAX * 4; j += SW4_RT_THREADS) qbit[j >> 2][j & 3] = 0u;
     if (tid < nlay && slot[tid] >= 0) slotk[slot[tid]] = (signed char)tid;
     __syncthreads();
     const int ncl = H.ncl;
@@ -333,7 +338,7 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
         const int nt = nlay * SW_NGPT;
         // clear pass
         if constexpr (!SW4_RT_PAIR) {
-            for (int i0 = tid; i0 < nt; i0 += SW2_THREADS) {
+            for (int i0 = tid; i0 < nt; i0 += SW4_RT_THREADS) {
                 float t0a, aba, s0a, y0a, wka, wfa;
                 int iba;
                 inputs(i0, t0a, aba, s0a, y0a, iba);
@@ -345,8 +350,8 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
                 if (!oka) enqueue(i0);
             }
         }
-        for (int i0 = tid; SW4_RT_PAIR && i0 < nt; i0 += 2 * SW2_THREADS) {
-            const int i1 = min(i0 + SW2_THREADS, nt - 1);
+        for (int i0 = tid; SW4_RT_PAIR && i0 < nt; i0 += 2 * SW4_RT_THREADS) {
+            const int i1 = min(i0 + SW4_RT_THREADS, nt - 1);
             float t0a, aba, s0a, y0a, t0b, abb, s0b, y0b, wka, wfa, wkb, wfb;
             int iba, ibb;
             inputs(i0, t0a, aba, s0a, y0a, iba);
@@ -359,7 +364,7 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
             sw4_rt<MODE>(t0b, abb, s0b, y0b, cz, snt, wkb, wfb, rb, okb);
             put(rtc, i0, ra);
             if (!oka) enqueue(i0);
-            if (i0 + SW2_THREADS < nt) {
+            if (i0 + SW4_RT_THREADS < nt) {
                 put(rtc, i1, rb);
                 if (!okb) enqueue(i1);
             }
@@ -399,7 +404,7 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
             }
         };
         if constexpr (!SW4_RT_PAIR) {
-            for (int j0 = tid; j0 < nc2; j0 += SW2_THREADS) {
+            for (int j0 = tid; j0 < nc2; j0 += SW4_RT_THREADS) {
                 SwLayerRT oa;
                 bool oka;
                 int ia;
@@ -411,8 +416,8 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
                 }
             }
         }
-        for (int j0 = tid; SW4_RT_PAIR && j0 < nc2; j0 += 2 * SW2_THREADS) {
-            const int j1 = min(j0 + SW2_THREADS, nc2 - 1);
+        for (int j0 = tid; SW4_RT_PAIR && j0 < nc2; j0 += 2 * SW4_RT_THREADS) {
+            const int j1 = min(j0 + SW4_RT_THREADS, nc2 - 1);
             SwLayerRT oa, ob;
             bool oka, okb;
             int ia, ib_;
@@ -425,7 +430,7 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
                     if (!oka) enqueue(ia);
                 }
             }
-            if (j0 + SW2_THREADS < nc2) {
+            if (j0 + SW4_RT_THREADS < nc2) {
                 const int k0 = ib_ / SW_NGPT, g = ib_ - k0 * SW_NGPT;
                 if (!(qbit[k0][g >> 5] & (1u << (g & 31)))) {
                     put(rto, (int)(slot[k0]) * SW_NGPT + g, ob);
@@ -440,7 +445,7 @@ sw4_rt_kernel(const __grid_constant__ SwBatch bt, int any_aer, const float* ex, 
     __syncthreads();
     // ---- the queued tasks with their float64 steps, one per thread
     const int nq = min(*qn, QCAP);
-    for (int j = tid; j < nq; j += SW2_THREADS) full(qe[j]);
+    for (int j = tid; j < nq; j += SW4_RT_THREADS) full(qe[j]);
 }
 
 // Per-g-point level fluxes of one sunlit column for swrad's optional outputs (DIAG sweeps):
