@@ -1017,18 +1017,32 @@ __device__ void lw_setup_core(S& s, const LwIn& a, int64_t col, int tid, Sink si
         const R sfe = (R)__ldg(a.sfcemis + col);
         s.semiss[tid] = (sfe > eps && sfe <= (R)1) ? sfe : (R)1;
     }
-    for (int k0 = tid; k0 < nlay; k0 += NT) {
-        lw_cldprop_layer<R>(s, a, col, k0, s.lcf1, ilwcliq);
-        lw_setcoef_layer<R>(s, k0);
-        lw_keys_layer<R>(s, k0);
-    }
-    if (tid < LW_NCHIR) lw_chi_ratio<R>(s, tid);
-    // Planck functions at levels 0..nlay and bands (setcoef.cu:135-160)
-    {
-        for (int p = tid; p < nlp1 * 16; p += NT) {
+    // Planck functions at levels 0..nlay and bands (setcoef.cu:135-160) and the chi ratios read only the inputs
+    // and the tables.  A CTA of at least 256 threads runs them on its threads past NLAY_MAX while the first
+    // NLAY_MAX take the layers (one each); a smaller CTA runs the three loops one after the other.
+    auto planck = [&](int p0, int stride) {
+        for (int p = p0; p < nlp1 * 16; p += stride) {
             const int k = p / 16, i = p % 16;
             lw_planck<R>(a, col, k, i, s.pklay[k][i], s.pklev[k][i]);
         }
+    };
+    auto layer_a2 = [&](int k0) {
+        lw_cldprop_layer<R>(s, a, col, k0, s.lcf1, ilwcliq);
+        lw_setcoef_layer<R>(s, k0);
+        lw_keys_layer<R>(s, k0);
+    };
+    if constexpr (NT >= 256) {
+        if (tid < NLAY_MAX) {
+            if (tid < nlay) layer_a2(tid);
+        } else {
+            const int u = tid - NLAY_MAX;
+            if (u < LW_NCHIR) lw_chi_ratio<R>(s, u);
+            planck(u, NT - NLAY_MAX);
+        }
+    } else {
+        for (int k0 = tid; k0 < nlay; k0 += NT) layer_a2(k0);
+        if (tid < LW_NCHIR) lw_chi_ratio<R>(s, tid);
+        planck(tid, NT);
     }
     __syncthreads();
     if constexpr (S::kKeys) {   // the species keys of bands 3, 4, 5, 7, 9 per layer (they read the chi ratios)
