@@ -1,5 +1,5 @@
 """Requests with other layer counts than the parent grid's 61: the top 21 layers dropped (40 layers, the model
-top near 100 hPa) and the three lowest layers split in two (64 layers, NLAY_MAX).  The gas-optics task tiling,
+top at 216 hPa) and the three lowest layers split in two (64 layers, NLAY_MAX).  The gas-optics task tiling,
 the per-layer set-up and the sweeps all index by the request's nlay, so the mixed kernels must stay within the
 tolerances (0.05 W/m^2, 0.01 K/day), on the tiled path and on the single-kernel forms, and the float64
 kernels close to the float64 oracle: 2e-3 W/m^2 and 2e-3 K/day, as in the float64 stress test (on these 2,048
