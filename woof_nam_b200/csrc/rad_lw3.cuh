@@ -7,11 +7,13 @@
 //   lw3_optics_kernel  one CTA (288 threads) per column: phases A and B of lw_setup_core (absorber amounts,
 //                      cldprop, setcoef, Planck functions, taugb01..16, the max-random overlap factors of
 //                      rtrnmr), with taug / fracs written straight to the chunk's scratch and the sweep inputs
-//                      copied after them.  Shared memory is the set-up data only (~32 KB).
+//                      copied after them.  Shared memory is the set-up data and the species keys of bands 3,
+//                      4, 5, 7 and 9 (LwSetupK, ~50 KB).
 //   lw3_sweep_kernel   one warp per column: lane l carries g-points l, l + 32, ..., l + 128 (five independent
 //                      recurrences interleaved per lane), reading each layer's optical depths as coalesced
-//                      128-byte rows staged through shared memory by asynchronous copies.  Per layer each g-point's radiance CHANGE across the layer is formed
-//                      directly (source minus radiance x absorptance) and summed over g-points in float64; the
+//                      128-byte rows staged through shared memory by asynchronous copies.  Per layer each
+//                      g-point's radiance CHANGE across the layer is formed directly (source minus radiance x
+//                      absorptance) and summed over g-points in float64; the
 //                      heating rates come from those changes, not from differences of ~300 W/m^2 level
 //                      fluxes.
 //   lw3_fp64_kernel    the plain float64 LW column (lw_column_body<double>) for the columns the optics kernel
