@@ -158,3 +158,29 @@ def test_volcanic_against_oracle(ivflip):
     assert np.array_equal(flw.cpu().numpy(), ref["faerlw"])
     with pytest.raises(Exception, match="kmonsav"):
         aerosols.volcanic(s, dev["plvl"], torch.as_tensor(ai["xlat"], device="cuda"), iv, 2031, 13, (fsw, flw))
+
+
+def test_shapes_checked_before_launch():
+    """Inputs or outputs whose shapes disagree with the solver's layer count are refused on the host (the kernels
+    index by the handle's nlay)."""
+    import torch
+    from woof_nam_b200.solver import RadSolver
+    cols = make_columns(64, 11)
+    ai = aerosols.make_inputs(cols, 12, "nam")
+    s = RadSolver()
+    dev = s.to_device(cols)
+    t = {k: torch.as_tensor(np.ascontiguousarray(v), device="cuda") for k, v in ai.items()}
+    aer = aerosols.Aerosols(s, 3)
+    with pytest.raises(ValueError):
+        aer.optics(dev, t["rhly"][:-1].contiguous(), t["xlon"], t["xlat"], t["slmsk"])
+    with pytest.raises(ValueError):
+        aer.optics(dev, t["rhly"], t["xlon"], t["xlat"], t["slmsk"],
+                   out=(torch.empty((3, 14, cols.nlay - 1, 64), device="cuda"),
+                        torch.empty((3, 16, cols.nlay - 1, 64), device="cuda")))
+    fsw, flw = aer.optics(dev, t["rhly"], t["xlon"], t["xlat"], t["slmsk"])
+    iv = np.zeros((10, 4, 12), np.int32)
+    with pytest.raises(ValueError):
+        aerosols.volcanic(s, dev["plvl"][1:].contiguous(), t["xlat"], iv, 1, 1, (fsw, flw))
+    with pytest.raises(ValueError):
+        aerosols.volcanic(RadSolver(nlay=40), dev["plvl"], t["xlat"], iv, 1, 1, (fsw, flw))
+    torch.cuda.synchronize()

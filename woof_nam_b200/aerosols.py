@@ -118,16 +118,25 @@ class Aerosols:
 
         from . import _lib
         nlay, ncol = dev["plyr"].shape
+        if nlay != self.solver.cfg.nlay:
+            raise ValueError(f"aerosol optics: the columns have {nlay} layers, the solver {self.solver.cfg.nlay}")
         a = _lib.RadAerColumns()
         src = {"plvl": dev["plvl"], "plyr": dev["plyr"], "tlyr": dev["tlyr"], "qlyr": dev["qlyr"], "rhly": rhly,
                "xlon": xlon, "xlat": xlat, "slmsk": slmsk}
+        shapes = {"plvl": (nlay + 1, ncol), "xlon": (ncol,), "xlat": (ncol,), "slmsk": (ncol,)}
         for k, v in src.items():
             if not (isinstance(v, torch.Tensor) and v.is_cuda and v.dtype == torch.float32 and v.is_contiguous()):
                 raise TypeError(f"aerosol input {k} must be a contiguous float32 CUDA tensor")
+            if tuple(v.shape) != shapes.get(k, (nlay, ncol)):
+                raise ValueError(f"aerosol input {k} has shape {tuple(v.shape)}, expected {shapes.get(k, (nlay, ncol))}")
             setattr(a, k, v.data_ptr())
         if out is None:
             out = (torch.empty((3, 14, nlay, ncol), dtype=torch.float32, device=dev["plyr"].device),
                    torch.empty((3, 16, nlay, ncol), dtype=torch.float32, device=dev["plyr"].device))
+        for o, nb in zip(out, (14, 16)):
+            if not (isinstance(o, torch.Tensor) and o.is_cuda and o.dtype == torch.float32 and o.is_contiguous()
+                    and tuple(o.shape) == (3, nb, nlay, ncol)):
+                raise ValueError(f"aerosol optics: out must be contiguous float32 CUDA tensors [3, {nb}, {nlay}, {ncol}]")
         st = stream if stream is not None else torch.cuda.current_stream()
         s = self.solver
         rc = s.lib.rad_setaer(s.handle, ctypes.byref(a), ncol, ctypes.c_void_p(out[0].data_ptr()),
@@ -156,9 +165,11 @@ def volcanic(solver, plvl, xlat, ivolae, kyrsav: int, kmonsav: int, faer: tuple,
     iv = np.ascontiguousarray(iv, dtype=np.int32)
     if iv.shape != (10, 4, 12):
         raise ValueError(f"ivolae must be int32 [10, 4, 12], got {iv.shape}")
-    ncol = plvl.shape[1]
-    if tuple(faer[0].shape[-1:]) != (ncol,) or tuple(faer[1].shape[-1:]) != (ncol,) or tuple(xlat.shape) != (ncol,):
-        raise ValueError("volcanic: plvl, xlat and faer disagree on the column count")
+    nlay, ncol = solver.cfg.nlay, plvl.shape[1]
+    if (tuple(plvl.shape) != (nlay + 1, ncol) or tuple(xlat.shape) != (ncol,)
+            or tuple(faer[0].shape) != (3, 14, nlay, ncol) or tuple(faer[1].shape) != (3, 16, nlay, ncol)):
+        raise ValueError(f"volcanic: expected plvl [{nlay + 1}, ncol], xlat [ncol], faersw [3, 14, {nlay}, ncol] and "
+                         f"faerlw [3, 16, {nlay}, ncol] (the solver's {nlay} layers)")
     st = stream if stream is not None else torch.cuda.current_stream()
     s = solver
     rc = s.lib.rad_setaer_volc(s.handle, ctypes.c_void_p(plvl.data_ptr()), ctypes.c_void_p(xlat.data_ptr()), ncol,
