@@ -37,6 +37,15 @@ def _dev(t, name: str, unit: str, dtype=None):
     return ctypes.c_void_p(t.data_ptr())
 
 
+def _chk(t, name: str, unit: str, shape: tuple, dtype=None):
+    """t must be a contiguous CUDA tensor of `dtype` (float32 by default) and `shape` (the kernels index by the
+    sizes passed beside the pointers, so a mismatch is refused here, before any launch)."""
+    _dev(t, name, unit, dtype)
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{unit}: {name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+    return t
+
+
 def _stream(stream):
     torch = _torch()
     return ctypes.c_void_p((stream if stream is not None else torch.cuda.current_stream()).cuda_stream)
@@ -63,6 +72,11 @@ def dayparts(solver, xlon, sinlat, coslat, solhr: float, dtswav: float, nrads: i
         for k in ("dp_start", "dp_len", "dp_day"):
             out[k] = torch.zeros(n, dtype=torch.int32, device=dev)
         out["ndayparts"] = torch.zeros(jm, dtype=torch.int32, device=dev)
+    for k in ("xlon", "sinlat", "coslat"):
+        _chk({"xlon": xlon, "sinlat": sinlat, "coslat": coslat}[k], k, "dayparts", (n,))
+    for k in _lib.DAYPARTS_FIELDS:
+        _chk(out[k], k, "dayparts", (jm,) if k == "ndayparts" else (n,),
+             torch.float32 if k in ("coszen", "coszdg") else torch.int32)
     o = _lib.RadDayparts(*[_ptr(out[k]) for k in _lib.DAYPARTS_FIELDS])
     args = [_dev(t, k, "dayparts") for k, t in (("xlon", xlon), ("sinlat", sinlat), ("coslat", coslat))]
     rc = solver.lib.rad_dayparts(solver.handle, ctypes.byref(sun["_state"]), *args, int(im), int(jm), float(solhr),
@@ -81,6 +95,11 @@ def getgases(solver, plvl, xlon, xlat, gasvmr=None, *, co2_glb, gco2cyc, co2vmr_
         gasvmr = torch.empty((NF_VGAS, lmax, n), dtype=torch.float32, device=plvl.device)
     if tuple(gasvmr.shape) != (NF_VGAS, lmax, n):
         raise ValueError(f"getgases: gasvmr shape {tuple(gasvmr.shape)} does not match [10, {lmax}, {n}]")
+    _chk(xlon, "xlon", "getgases", (n,))
+    _chk(xlat, "xlat", "getgases", (n,))
+    for k, t, m in (("co2_glb", co2_glb, 1), ("gco2cyc", gco2cyc, 12), ("co2vmr_sav", co2vmr_sav, 12 * 12 * 24)):
+        if t is not None:
+            _chk(t.reshape(-1) if t.is_contiguous() else t, k, "getgases", (m,))
     g = _lib.RadGasSetup(_ptr(co2_glb), _ptr(gco2cyc), _ptr(co2vmr_sav), int(ico2flg),
                          int(kmonsav) if kmonsav is not None else 0, int(ivflip))
     rc = solver.lib.rad_getgases(solver.handle, _dev(plvl, "plvl", "getgases"), _dev(xlon, "xlon", "getgases"),
@@ -98,6 +117,12 @@ def getozn(solver, prslk, xlat, o3mmr=None, *, o3r, pkstr, k1oz: int, k2oz: int,
     nlev, n = prslk.shape
     if o3mmr is None:
         o3mmr = torch.zeros((nlev, n), dtype=torch.float32, device=prslk.device)
+    _chk(xlat, "xlat", "getozn", (n,))
+    _chk(o3mmr, "o3mmr", "getozn", (nlev, n))
+    if o3r.dim() != 3 or o3r.shape[0] != 12:
+        raise ValueError(f"getozn: o3r must be [12, loz, jmr], got {tuple(o3r.shape)}")
+    _chk(o3r, "o3r", "getozn", tuple(o3r.shape))
+    _chk(pkstr, "pkstr", "getozn", (int(o3r.shape[1]),))
     c = _lib.RadOzoneClim(_ptr(o3r), _ptr(pkstr), int(o3r.shape[2]), int(o3r.shape[1]), int(k1oz), int(k2oz),
                           float(facoz), float(blte), float(dlte), int(ivflip))
     rc = solver.lib.rad_getozn(solver.handle, _dev(prslk, "prslk", "getozn"), _dev(xlat, "xlat", "getozn"), n, nlev,
@@ -113,6 +138,10 @@ def setalb(solver, sfc: dict, ialbflg: int, sfcalb=None, stream=None):
     n = sfc["alvsf"].numel()
     if sfcalb is None:
         sfcalb = torch.empty((NF_ALBD, n), dtype=torch.float32, device=sfc["alvsf"].device)
+    for k in _lib.ALBEDO_FIELDS:
+        if sfc.get(k) is not None:
+            _chk(sfc[k], k, "setalb", (n,))
+    _chk(sfcalb, "sfcalb", "setalb", (NF_ALBD, n))
     a = _lib.RadAlbedoIn(*[_ptr(sfc.get(k)) for k in _lib.ALBEDO_FIELDS])
     rc = solver.lib.rad_setalb(solver.handle, ctypes.byref(a), n, int(ialbflg), _dev(sfcalb, "sfcalb", "setalb"),
                                _stream(stream))
@@ -128,7 +157,11 @@ def setemis(solver, sfc: dict, idxems, ialbflg: int, iemslw: int, sfcemis=None, 
     if sfcemis is None:
         sfcemis = torch.empty(n, dtype=torch.float32, device=sfc["glon"].device)
     if idxems is not None:
-        _dev(idxems, "idxems", "setemis", torch.int32)
+        _chk(idxems, "idxems", "setemis", (180, 360), torch.int32)
+    for k in _lib.EMIS_FIELDS[:-1]:
+        if sfc.get(k) is not None:
+            _chk(sfc[k], k, "setemis", (n,))
+    _chk(sfcemis, "sfcemis", "setemis", (n,))
     vals = [_ptr(sfc.get(k)) for k in _lib.EMIS_FIELDS[:-1]] + [_ptr(idxems)]
     e = _lib.RadEmisIn(*vals)
     rc = solver.lib.rad_setemis(solver.handle, ctypes.byref(e), n, int(ialbflg), int(iemslw),
@@ -155,7 +188,10 @@ def progcld2(solver, inputs: dict, *, ivflip: int, llyr: int, iovr: int, lcrick:
                "mbot": torch.empty((3, n), dtype=torch.int32, device=dev)}
     for k in _lib.CLOUD_IN_FIELDS:
         if inputs.get(k) is not None:
-            _dev(inputs[k], k, "progcld2")
+            _chk(inputs[k], k, "progcld2", (nlay + 1, n) if k == "plvl" else (n,) if k == "xlat" else (nlay, n))
+    for k, shape, dt in (("clouds", (NF_CLDS, nlay, n), torch.float32), ("clds", (5, n), torch.float32),
+                         ("mtop", (3, n), torch.int32), ("mbot", (3, n), torch.int32)):
+        _chk(out[k], k, "progcld2", shape, dt)
     ci = _lib.RadCloudIn(*[_ptr(inputs.get(k)) for k in _lib.CLOUD_IN_FIELDS])
     cfg = _lib.RadCloudCfg(int(ivflip), int(llyr), int(iovr), int(bool(lcrick)), int(bool(lcnorm)), int(bool(lnoprec)),
                            int(bool(lsashal)), int(cld_fraction))
