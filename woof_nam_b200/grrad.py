@@ -23,9 +23,18 @@ def layers(solver, model: dict, out: dict | None = None, stream=None) -> dict:
             raise TypeError(f"grrad layers: {k} must be a contiguous float32 CUDA tensor")
     lm, n = model["pmid"].shape
     dev = model["pmid"].device
+    inshape = {"pint": (lm + 1, n), "tsfc": (n,)}
+    for k in _lib.MODEL_FIELDS:
+        if tuple(model[k].shape) != inshape.get(k, (lm, n)):
+            raise ValueError(f"grrad layers: {k} has shape {tuple(model[k].shape)}, expected {inshape.get(k, (lm, n))}")
+    shapes = {"plvl": (lm + 2, n), "tlvl": (lm + 2, n), "tsfg": (n,)}
     if out is None:
-        shapes = {"plvl": (lm + 2, n), "tlvl": (lm + 2, n), "tsfg": (n,)}
         out = {k: torch.empty(shapes.get(k, (lm + 1, n)), dtype=torch.float32, device=dev) for k in _lib.LAYER_FIELDS}
+    for k in _lib.LAYER_FIELDS:
+        v = out[k]
+        if not (isinstance(v, torch.Tensor) and v.is_cuda and v.dtype == torch.float32 and v.is_contiguous()
+                and tuple(v.shape) == shapes.get(k, (lm + 1, n))):
+            raise ValueError(f"grrad layers: out {k} must be a contiguous float32 CUDA tensor {shapes.get(k, (lm + 1, n))}")
     a, o = _lib.RadModelColumns(), _lib.RadLayerFields()
     for k in _lib.MODEL_FIELDS:
         setattr(a, k, model[k].data_ptr())

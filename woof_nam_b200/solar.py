@@ -37,8 +37,14 @@ def coszmn(solver, sun: dict, glon, glat, solhr: float, dtswav: float, nrads: in
     for name, t in (("glon", glon), ("glat", glat)):
         if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
             raise TypeError(f"coszmn: {name} must be a contiguous float32 CUDA tensor")
+    if glat.shape != glon.shape:
+        raise ValueError(f"coszmn: glat {tuple(glat.shape)} and glon {tuple(glon.shape)} differ")
     if out is None:
         out = (torch.empty_like(glon), torch.empty_like(glon))
+    for name, t in zip(("coszen", "coszdg"), out):
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()
+                and t.shape == glon.shape):
+            raise ValueError(f"coszmn: out {name} must be a contiguous float32 CUDA tensor shaped like glon")
     st = stream if stream is not None else torch.cuda.current_stream()
     rc = solver.lib.rad_coszmn(solver.handle, ctypes.byref(sun["_state"]), ctypes.c_void_p(glon.data_ptr()),
                                ctypes.c_void_p(glat.data_ptr()), glon.numel(), float(solhr), float(dtswav), int(nrads),
