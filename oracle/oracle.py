@@ -236,10 +236,28 @@ def aer_climatology(month: int, path=None) -> dict:
     return aerosols.climatology(month, path)
 
 
-def aerosols(clim: dict, cols, aer_in: dict, which: str = "port", tables: bool = False) -> dict:
+class _Flip:
+    """The layer fields of a request with the vertical order reversed (plvl, plyr, tlyr, qlyr; nlay, ncol)."""
+
+    def __init__(self, cols, fl):
+        self.nlay, self.ncol = cols.nlay, cols.ncol
+        for k in ("plvl", "plyr", "tlyr", "qlyr"):
+            setattr(self, k, fl(getattr(cols, k)))
+
+
+def aerosols(clim: dict, cols, aer_in: dict, which: str = "port", tables: bool = False, ivflip: int = 0) -> dict:
     """Aerosol optics of a request: faersw [3][14][nlay][ncol], faerlw [3][16][nlay][ncol] (float32) from the
     restatement (which="port") or the reference's kernels (which="ref"); with tables=True also the derived
-    tables (AER_TAB_FIELDS)."""
+    tables (AER_TAB_FIELDS).  ivflip 1: the request's layers (and the outputs') are surface first; the reference
+    runs its ivflip = 1 branches, the restatement the top-first statements on the flipped layers (the reference's
+    two branches mirror each other statement for statement, pinned by tests/test_aerosols.py)."""
+    if ivflip == 1 and which == "port":
+        fl = lambda a: np.ascontiguousarray(np.asarray(a)[::-1])  # noqa: E731
+        cf = _Flip(cols, fl)
+        r = aerosols(clim, cf, dict(aer_in, rhly=fl(aer_in["rhly"])), which, tables)
+        for k in ("faersw", "faerlw"):
+            r[k] = np.ascontiguousarray(r[k][:, :, ::-1])
+        return r
     L = lib(which)
     nlay, ncol = cols.nlay, cols.ncol
     c = {k: np.ascontiguousarray(v) for k, v in clim.items()}
@@ -254,11 +272,11 @@ def aerosols(clim: dict, cols, aer_in: dict, which: str = "port", tables: bool =
     lw = np.zeros((3, 16, nlay, ncol), np.float32)
     tab = np.zeros(sum(n for _, n in AER_TAB_FIELDS), np.float32) if tables else None
     p = lambda a, t: a.ctypes.data_as(t) if a is not None else None  # noqa: E731
-    rc = L.orc_aerosols(p(ints["iendwv"], _I), p(f["haer"], _F), p(f["prsref"], _F), p(rhid, _F), p(rhdp, _F),
-                        p(f["straext0"], _F), p(ints["nwvns0"], _I), p(f["s0intv"], _F), p(ints["month_idx"], _I),
-                        p(d["month_cmix"], _D), p(ints["month_kprf"], _I), p(d["month_denn"], _D),
-                        ctypes.c_int(nlay), ctypes.c_int(ncol), *[p(a, _F) for a in keep], p(sw, _F), p(lw, _F),
-                        p(tab, _F))
+    args = (p(ints["iendwv"], _I), p(f["haer"], _F), p(f["prsref"], _F), p(rhid, _F), p(rhdp, _F),
+            p(f["straext0"], _F), p(ints["nwvns0"], _I), p(f["s0intv"], _F), p(ints["month_idx"], _I),
+            p(d["month_cmix"], _D), p(ints["month_kprf"], _I), p(d["month_denn"], _D),
+            ctypes.c_int(nlay), ctypes.c_int(ncol), *[p(a, _F) for a in keep], p(sw, _F), p(lw, _F), p(tab, _F))
+    rc = L.orc_aerosols_iv(*args, ctypes.c_int(ivflip)) if ivflip else L.orc_aerosols(*args)
     if rc != 0:
         raise RuntimeError("aerosols failed")
     out = {"faersw": sw, "faerlw": lw}

@@ -1227,13 +1227,13 @@ int ref_rdtemp(int ntsd, float dt, int julday, int julyr, int ihrst, int leap_se
 // (phys_rrtm_aer_init.py: flags, set_spectrum), clim_aerinit (phys_rrtm_clim_aerinit.py:196-235: bands, then
 // optavg), aer_update's month fill (phys_rrtm_aer_update.py:139-165), setaer (phys_rrtm_setaer.py: zero, prep,
 // then aer_property as phys_rrtm_aer_property.py:176-200 binds it, cmixg / denng cast to float), for the NAM
-// settings iaer 11 (SW and LW on, volcanic off), ivflip 0, one row of ncol columns.  Same signature as the
-// oracle's orc_aerosols.
-int orc_aerosols(const int* iendwv, const float* haer, const float* prsref, const float* rhid, const float* rhdp,
-                 const float* straext0, const int* nwvns0, const float* s0intv, const int* midx, const double* mcmix,
-                 const int* mkprf, const double* mdenn, int nlay, int ncol, const float* plvl, const float* plyr,
-                 const float* tlyr, const float* qlyr, const float* rhly, const float* xlon, const float* xlat,
-                 const float* slmsk, float* aerosw, float* aerolw, float* tab)
+// settings iaer 11 (SW and LW on, volcanic off), one row of ncol columns, levels top first (ivflip 0) or surface
+// first (ivflip 1, the reference's other orientation).
+int orc_aerosols_iv(const int* iendwv, const float* haer, const float* prsref, const float* rhid, const float* rhdp,
+                    const float* straext0, const int* nwvns0, const float* s0intv, const int* midx, const double* mcmix,
+                    const int* mkprf, const double* mdenn, int nlay, int ncol, const float* plvl, const float* plyr,
+                    const float* tlyr, const float* qlyr, const float* rhly, const float* xlon, const float* xlat,
+                    const float* slmsk, float* aerosw, float* aerolw, float* tab, int ivflip)
 {
     (void)nwvns0; (void)s0intv;   // the reference kernel carries the solar spectrum itself
     using FV = std::vector<float>;
@@ -1287,7 +1287,7 @@ int orc_aerosols(const int* iendwv, const float* haer, const float* prsref, cons
     FV alon(ncol), alat(ncol), dz((size_t)nlay * ncol), hz((size_t)nlp1 * ncol);
     drv::launch(drv::cdiv(ncol, 128), 1, 1, 128, [&] {
         r_seta::phys_rrtm_setaer_prep(plvl, plyr, tlyr, qlyr, xlon, xlat, alon.data(), alat.data(), dz.data(),
-                                      hz.data(), ncol, nlay, nlp1, 0, 1);
+                                      hz.data(), ncol, nlay, nlp1, ivflip, 1);
     });
     const size_t nsw = (size_t)3 * kNSW * nlay * ncol, nlw = (size_t)3 * kNLW * nlay * ncol;
     drv::launch(1, 1, 1, 1, [&] { r_seta::phys_rrtm_setaer_zero(aerosw, aerolw, nsw, nlw); });
@@ -1298,9 +1298,20 @@ int orc_aerosols(const int* iendwv, const float* haer, const float* prsref, cons
                                               ssarhi.data(), asyrhi.data(), extrhd.data(), scarhd.data(),
                                               ssarhd.data(), asyrhd.data(), extstra.data(), cmixg.data(),
                                               denng.data(), idxcg.data(), kprfg.data(), aerosw, aerolw, ncol, 1, nlay,
-                                              1, 1, 0, kNSW, kNLW, kNBT);
+                                              1, 1, ivflip, kNSW, kNLW, kNBT);
     });
     return 0;
+}
+
+// The NAM orientation (ivflip 0, levels top first) of orc_aerosols_iv; same signature as the oracle's orc_aerosols.
+int orc_aerosols(const int* iendwv, const float* haer, const float* prsref, const float* rhid, const float* rhdp,
+                 const float* straext0, const int* nwvns0, const float* s0intv, const int* midx, const double* mcmix,
+                 const int* mkprf, const double* mdenn, int nlay, int ncol, const float* plvl, const float* plyr,
+                 const float* tlyr, const float* qlyr, const float* rhly, const float* xlon, const float* xlat,
+                 const float* slmsk, float* aerosw, float* aerolw, float* tab)
+{
+    return orc_aerosols_iv(iendwv, haer, prsref, rhid, rhdp, straext0, nwvns0, s0intv, midx, mcmix, mkprf, mdenn, nlay,
+                           ncol, plvl, plyr, tlyr, qlyr, rhly, xlon, xlat, slmsk, aerosw, aerolw, tab, 0);
 }
 
 // The volcanic term from the reference's kernels: phys_rrtm_setaer_prep for alat (do_dz 0), then

@@ -10,6 +10,10 @@ Keys, per case ("jan_nam": January, 16 columns over the NAM domain; "jul_globe":
     faerlw      [3][16][nlay][ncol]
     tab_*       the derived tables (oracle.AER_TAB_FIELDS)
 
+the surface-first orientation (ivflip 1) of the "jul_globe" request, its layers flipped, through the reference's
+ivflip = 1 branches of setaer's prep and aer_property:
+    flip_faersw, flip_faerlw   [3][14|16][nlay][ncol], layers surface first
+
 and the volcanic term (setaer's lavoflg branch, orc_setaer_volc: phys_rrtm_setaer_prep then
 phys_rrtm_setaer_volc) added to the "jul_globe" optics, per case of VOLC_CASES (ivflip, lw1bd, kyrsav,
 kmonsav), on a seeded ivolae table and latitudes across the seven zone bands and their edges:
@@ -63,6 +67,13 @@ def main():
         blob[f"{case}_faerlw"] = r["faerlw"]
         for name, _ in oracle.AER_TAB_FIELDS:
             blob[f"{case}_tab_{name}"] = r[name]
+    fl = lambda a: np.ascontiguousarray(np.asarray(a)[::-1])  # noqa: E731
+    month, ncol, seed, region = CASES["jul_globe"]
+    cols = make_columns(ncol, seed)
+    ai = aerosols.make_inputs(cols, seed, region)
+    r = oracle.aerosols(aerosols.climatology(month), oracle._Flip(cols, fl), dict(ai, rhly=fl(ai["rhly"])),
+                        which="ref", ivflip=1)
+    blob["flip_faersw"], blob["flip_faerlw"] = r["faersw"], r["faerlw"]
     ivolae, xlat = volc_inputs(16)
     blob["volc_in_ivolae"], blob["volc_in_xlat"] = ivolae, xlat
     plvl = blob["jul_globe_in_plvl"]

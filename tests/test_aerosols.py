@@ -2,7 +2,9 @@
 reference's own kernels: the float restatement reproduces the golden vectors of aer_init, clim_aerinit,
 aer_update's month fill, setaer and aer_property bit for bit, and the packed climatology has the shape and
 ranges the kernels assume.  The volcanic term (setaer's lavoflg branch) reproduces phys_rrtm_setaer_volc's
-golden vectors in both level orders and with the one-broad-band LW factor."""
+golden vectors in both level orders and with the one-broad-band LW factor.  The reference's surface-first
+branches (ivflip 1) of setaer and aer_property mirror its top-first ones bit for bit, which is what lets the
+restatement and the GPU path serve surface-first requests by reversing the layers."""
 from __future__ import annotations
 
 from pathlib import Path
@@ -106,3 +108,12 @@ def test_volcanic_switches(gold):
     assert np.array_equal(oracle.setaer_volc(pl, xl, iv, -7, 2, sw, lw)["faersw"], both["faersw"])
     with pytest.raises(ValueError):
         oracle.setaer_volc(pl, xl, iv, 3, 13, sw, lw)
+
+
+def test_surface_first_mirrors_top_first(gold):
+    fl = lambda a: np.ascontiguousarray(np.asarray(a)[::-1])  # noqa: E731
+    month, cols, ai = golden_request(gold, "jul_globe")
+    for k in ("faersw", "faerlw"):   # the reference's own ivflip = 1 output is its ivflip = 0 output, reversed
+        assert np.array_equal(gold[f"flip_{k}"], np.ascontiguousarray(gold[f"jul_globe_{k}"][:, :, ::-1]))
+    r = oracle.aerosols(aerosols.climatology(month), oracle._Flip(cols, fl), dict(ai, rhly=fl(ai["rhly"])), ivflip=1)
+    assert np.array_equal(r["faersw"], gold["flip_faersw"]) and np.array_equal(r["faerlw"], gold["flip_faerlw"])

@@ -184,3 +184,22 @@ def test_shapes_checked_before_launch():
     with pytest.raises(ValueError):
         aerosols.volcanic(RadSolver(nlay=40), dev["plvl"], t["xlat"], iv, 1, 1, (fsw, flw))
     torch.cuda.synchronize()
+
+
+def test_surface_first():
+    """ivflip 1: a surface-first request (the golden "jul_globe" request with its layers reversed) against the
+    reference's own ivflip = 1 output, and bit for bit the top-first optics reversed."""
+    import torch
+    from test_aerosols import golden_request
+    z = np.load(Path(__file__).resolve().parent / "golden" / "aer_golden.npz")
+    month, cols, ai = golden_request(z, "jul_globe")
+    s, dev, fsw, flw = _gpu(month, cols, ai)
+    aer = aerosols.Aerosols(s, month)
+    rev = {k: torch.flip(dev[k], dims=[0]).contiguous() for k in ("plvl", "plyr", "tlyr", "qlyr")}
+    t = {k: torch.as_tensor(np.ascontiguousarray(v), device="cuda") for k, v in ai.items()}
+    gsw, glw = aer.optics(rev, torch.flip(t["rhly"], dims=[0]).contiguous(), t["xlon"], t["xlat"], t["slmsk"],
+                          ivflip=1)
+    torch.cuda.synchronize()
+    _close(gsw, z["flip_faersw"], "surface-first faersw")
+    _close(glw, z["flip_faerlw"], "surface-first faerlw")
+    assert torch.equal(gsw, torch.flip(fsw, dims=[2])) and torch.equal(glw, torch.flip(flw, dims=[2]))

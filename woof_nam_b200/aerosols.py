@@ -108,15 +108,32 @@ class Aerosols:
         _lib.check(s.lib, s.handle, s.lib.rad_load_aerosols(s.handle, ctypes.byref(c)), "rad_load_aerosols")
         self.month = month
 
-    def optics(self, dev: dict, rhly, xlon, xlat, slmsk, out: tuple | None = None, stream=None) -> tuple:
+    def optics(self, dev: dict, rhly, xlon, xlat, slmsk, out: tuple | None = None, stream=None,
+               ivflip: int = 0) -> tuple:
         """faersw [3, 14, nlay, ncol], faerlw [3, 16, nlay, ncol] (CUDA float32) for the columns of `dev` (the
         tensors of RadSolver.to_device: plvl, plyr, tlyr, qlyr) and the CUDA tensors rhly [nlay, ncol], xlon,
-        xlat, slmsk [ncol] (radians, mask 0 / 1 / 2)."""
+        xlat, slmsk [ncol] (radians, mask 0 / 1 / 2).  ivflip 1: the layers of the inputs and of the outputs are
+        surface first (the reference's other orientation; its ivflip = 1 statements mirror the top-first ones,
+        so the top-first kernel runs on the reversed layers, through temporary tensors)."""
         import ctypes
 
         import torch
 
         from . import _lib
+        if ivflip not in (0, 1):
+            raise ValueError("aerosol optics: ivflip must be 0 or 1")
+        if ivflip == 1:
+            st = stream if stream is not None else torch.cuda.current_stream()
+            with torch.cuda.stream(st):
+                rev = {k: torch.flip(dev[k], dims=[0]).contiguous() for k in ("plvl", "plyr", "tlyr", "qlyr")}
+                top = self.optics(rev, torch.flip(rhly, dims=[0]).contiguous(), xlon, xlat, slmsk, stream=st)
+                if out is None:
+                    out = tuple(torch.empty_like(t) for t in top)
+                for o, t in zip(out, top):
+                    if tuple(o.shape) != tuple(t.shape):
+                        raise ValueError(f"aerosol optics: out must be {tuple(t.shape)}")
+                    o.copy_(torch.flip(t, dims=[2]))
+            return out
         nlay, ncol = dev["plyr"].shape
         if nlay != self.solver.cfg.nlay:
             raise ValueError(f"aerosol optics: the columns have {nlay} layers, the solver {self.solver.cfg.nlay}")

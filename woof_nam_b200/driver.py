@@ -404,7 +404,7 @@ def _aer_month(ctx) -> int:
 
 
 # Slots of rad_initialize's flag vector (namgpu/kernels/phys_rrtm_rad_initialize.cu:99-108).
-RI_IAERFLG, RI_LASWFLG, RI_LALWFLG, RI_LAVOFLG = 4, 5, 6, 7
+RI_IAERFLG, RI_LASWFLG, RI_LALWFLG, RI_LAVOFLG, RI_IVFLIP = 4, 5, 6, 7, 25
 
 
 def _aer_flags(ctx) -> dict:
@@ -419,9 +419,9 @@ def _aer_flags(ctx) -> dict:
             import numpy as np
             p = np.asarray(p.get() if hasattr(p, "get") and not isinstance(p, dict) else p)
             st = {"iaerflg": int(p[RI_IAERFLG]), "laswflg": bool(p[RI_LASWFLG]), "lalwflg": bool(p[RI_LALWFLG]),
-                  "lavoflg": bool(p[RI_LAVOFLG])}
+                  "lavoflg": bool(p[RI_LAVOFLG]), "ivflip": int(p[RI_IVFLIP]) if p.size > RI_IVFLIP else 0}
         else:
-            st = {"iaerflg": 11, "laswflg": True, "lalwflg": True, "lavoflg": False}
+            st = {"iaerflg": 11, "laswflg": True, "lalwflg": True, "lavoflg": False, "ivflip": 0}
         volc = tabs.get("aer_volc")
         st = dict(st, kyrsav=int(getattr(volc, "kyrsav", 1)), kmonsav=int(getattr(volc, "kmonsav", 1)))
     return st
@@ -464,7 +464,8 @@ def grrad_aerosols_run(ctx, *, lsswr: bool = True, lslwr: bool = True) -> dict:
     laersw, laerlw = bool(lsswr and fl["laswflg"]), bool(lslwr and fl["lalwflg"])
     with torch.cuda.stream(stream):
         if fl["iaerflg"] > 0 and (lsswr or lslwr) and (fl["laswflg"] or fl["lalwflg"]):
-            aer.optics(cols, cols["rhly"], cols["xlon"], cols["xlat"], cols["slmsk"], out=out, stream=stream)
+            aer.optics(cols, cols["rhly"], cols["xlon"], cols["xlat"], cols["slmsk"], out=out, stream=stream,
+                       ivflip=int(fl.get("ivflip", 0)))
             if not laersw:
                 fsw.zero_()
             if not laerlw:
@@ -480,8 +481,8 @@ def grrad_aerosols_run(ctx, *, lsswr: bool = True, lslwr: bool = True) -> dict:
             raise RuntimeError(f"{unit}: lavoflg needs ctx.tables['aer_ivolae'] (int32 [10, 4, 12])")
         if hasattr(iv, "get") and not isinstance(iv, dict):
             iv = iv.get()
-        volcanic(s, cols["plvl"], cols["xlat"], iv, fl["kyrsav"], fl["kmonsav"], out, add_sw=add_sw, add_lw=add_lw,
-                 stream=stream)
+        volcanic(s, cols["plvl"], cols["xlat"], iv, fl["kyrsav"], fl["kmonsav"], out, ivflip=int(fl.get("ivflip", 0)),
+                 add_sw=add_sw, add_lw=add_lw, stream=stream)
     tabs["rrtm_faersw"], tabs["rrtm_faerlw"] = fsw, flw
     return {"faersw": fsw, "faerlw": flw}
 
