@@ -447,6 +447,35 @@ def setemis(sfc: dict, idxems, ialbflg: int, iemslw: int, which: str = "port") -
     return out
 
 
+def grrad_clw(tracer, ntcw: int, ncld: int = 1, epsq: float = 1.0e-12, which: str = "port") -> np.ndarray:
+    """grrad's condensate clw [lmk][n] from the tracers [ntrac][lmk][n]: the ncld tracers from ntcw (1-based)."""
+    L = lib(which)
+    tr = _f(tracer)
+    ntrac, lmk, n = tr.shape
+    if ntcw < 1 or ntcw - 1 + ncld > ntrac:
+        raise ValueError(f"grrad_clw: tracers {ntcw}..{ntcw + ncld - 1} outside 1..{ntrac}")
+    out = np.zeros((lmk, n), np.float32)
+    L.orc_grrad_clw(ctypes.c_int(n), ctypes.c_int(lmk), _fp(tr), ctypes.c_int(ntcw - 1), ctypes.c_int(ncld),
+                    ctypes.c_float(epsq), _fp(out))
+    return out
+
+
+PAYNE_OUT = ("sfcalbedo", "smx", "czmean", "alvsf", "alnsf", "alvwf", "alnwf", "facsf", "facwf")
+
+
+def payne_albedo(salbedo, sm, coszen, tables: dict, which: str = "port") -> dict:
+    """grrad's IALB = 2 surface albedo [n] and the fields it hands setalb (PAYNE_OUT) from salbedo, sm, coszen
+    [n] and the packed tables (woof_nam_b200/data/payne_albedo.npz: trn, za, dza, albd)."""
+    L = lib(which)
+    a, m, c = _f(salbedo), _f(sm), _f(coszen)
+    t = {k: _f(tables[k]) for k in ("trn", "za", "dza", "albd")}
+    n = a.size
+    out = np.zeros((9, n), np.float32)
+    L.orc_payne_albedo(ctypes.c_int(n), _fp(a), _fp(m), _fp(c), _fp(t["trn"]), _fp(t["za"]), _fp(t["dza"]),
+                       _fp(t["albd"]), _fp(out))
+    return {k: out[i] for i, k in enumerate(PAYNE_OUT)}
+
+
 def progcld2(cld: dict, cfg: dict, which: str = "port") -> dict:
     """Ferrier cloud properties of the CLD_FIELDS of cld ([nlay][n], plvl [nlay + 1][n], xlat [n]) under the
     CLD_CFG switches: clouds [9][nlay][n], clds [5][n], mtop, mbot [3][n]."""

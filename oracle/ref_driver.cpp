@@ -130,6 +130,9 @@ namespace r_grs {
 namespace r_grg {
 #include "phys_rrtm_grrad_gases.cu"
 }
+namespace r_grcl {
+#include "phys_rrtm_grrad_clouds.cu"
+}
 namespace r_swcld {
 #include "phys_rrtm_sw_cldprop.cu"
 }
@@ -1331,6 +1334,32 @@ int orc_setaer_volc(int nlay, int ncol, int ivflip, const float* plvl, const flo
     drv::launch(drv::cdiv(ncol, 128), 1, 1, 128, [&] {
         r_seta::phys_rrtm_setaer_volc(aerosw, aerolw, plvl, alat.data(), ivolae, ncol, nlay, ivflip, year1, kmonsav,
                                       add_sw, add_lw, lw1bd);
+    });
+    return 0;
+}
+
+// grrad's condensate from the reference's kernel grrad_clouds_clw (phys_rrtm_grrad_clouds.py:183-193), one row of n
+// columns.  Same signature as the oracle's orc_grrad_clw.
+int orc_grrad_clw(int n, int lmk, const float* tracer, int ntcw0, int ncld, float epsq, float* clw)
+{
+    if (n <= 0) return 0;
+    drv::launch(drv::cdiv(n, 128), 1, lmk, 128, [&] {
+        r_grcl::grrad_clouds_clw(tracer, clw, n, 1, lmk, ntcw0, ncld, epsq);
+    });
+    return 0;
+}
+
+// grrad's IALB = 2 block from the reference's kernel grrad_clouds_albedo (phys_rrtm_grrad_clouds.py:230-245), with
+// its own built-in tables (the table arguments are not read).  Same signature as the oracle's orc_payne_albedo.
+int orc_payne_albedo(int n, const float* salbedo, const float* sm, const float* coszen, const float* trn,
+                     const float* za, const float* dza, const float* albd, float* out)
+{
+    (void)trn; (void)za; (void)dza; (void)albd;
+    if (n <= 0) return 0;
+    float* o[9];
+    for (int f = 0; f < 9; ++f) o[f] = out + (size_t)f * n;
+    drv::launch(drv::cdiv(n, 128), 1, 1, 128, [&] {
+        r_grcl::grrad_clouds_albedo(salbedo, sm, coszen, o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7], o[8], n, 1);
     });
     return 0;
 }

@@ -12,6 +12,10 @@
 //              Fortran's linear searches of the 1-degree emissivity map
 //   progcld2   namgpu/kernels/phys_rrtm_progcld2.cu:92-444 (radiation_clouds_nmmb.f:787-1323 with
 //              rsipath2_tmp :2779-2964 and gethml :2167-2494)
+//   clw        namgpu/kernels/phys_rrtm_grrad_clouds.cu:396-416 (grrad_nmmb.f:1556-1571): the condensate of
+//              the cloud tracers
+//   albedo     namgpu/kernels/phys_rrtm_grrad_clouds.cu:344-393 (grrad_nmmb.f:1722-1794): the IALB = 2 surface
+//              albedo from the zenith angle and the atmospheric transmissivity (the TRN / ZA / DZA / ALBD tables)
 // Layouts: 2-D fields [n] with n = jm * im columns (row-major, point i of row j at j * im + i), 3-D fields
 // [level][n], multi-field outputs [field][level][n].  Never linked into the product.
 #pragma once
@@ -554,6 +558,47 @@ inline void progcld2(int n, int nlay, const CldIn& in, const CldCfg& cfg, float*
             mbot[q * N + c] = mb[q];
         }
     }
+}
+
+// ------------------------------------------------------------------------------------------ clw
+// Total condensate of each layer: the ncld cloud tracers from index ntcw0 (0-based) summed in tracer order, values
+// below epsq set to zero.  tracer [ntrac][lmk][n], clw [lmk][n].
+inline void grrad_clw(int n, int lmk, const float* tracer, int ntcw0, int ncld, float epsq, float* clw)
+{
+    const size_t plane = (size_t)lmk * n;
+    for (size_t p = 0; p < plane; ++p) {
+        float sum = 0.0f;
+        for (int j = 0; j < ncld; ++j) sum += tracer[(size_t)(ntcw0 + j) * plane + p];
+        clw[p] = sum < epsq ? 0.0f : sum;
+    }
+}
+
+// ------------------------------------------------------------------------------------------ IALB = 2 albedo
+// The albedo tables: trn [21], za [20] (degrees, decreasing), dza [19], albd [20][21] ([zenith row][trn column]).
+struct PayneTab {
+    const float *trn, *za, *dza, *albd;
+};
+
+// Surface albedo of one point: salbedo unless the sun is up over land-mask value sm > 0.5, where the table value at
+// the zenith angle and the fixed transmissivity 0.537 (column 11 of the table and its right neighbour) replaces it.
+inline float payne_albedo(float salbedo, float sm, float cz, const PayneTab& t)
+{
+    const float trans = 0.537f;
+    const int iq = (int)(20.0f * trans + 1.0f);                      // transmissivity column (1-based)
+    if (!(cz > 0.0f && sm > 0.5f)) return salbedo;
+    const float deg = 180.0f / 3.14159265f;
+    const float zen = deg * std::acos(std::max(cz, 0.0f));
+    // zenith row: 2-degree rows above 74 degrees, 4-degree rows from 50, 10-degree rows below (1-based)
+    int jx;
+    if (zen >= 74.0f) jx = (int)(0.5f * (90.0f - zen) + 1.0f);
+    else if (zen >= 50.0f) jx = (int)(0.25f * (74.0f - zen) + 9.0f);
+    else jx = (int)(0.1f * (50.0f - zen) + 15.0f);
+    jx = std::min(jx, 19);
+    const float w = -(zen - t.za[jx - 1]) / t.dza[jx - 1];
+    auto A = [&](int row, int col) { return t.albd[(row - 1) * 21 + (col - 1)]; };   // 1-based row, column
+    const float a1 = A(jx, iq) + w * (A(jx + 1, iq) - A(jx, iq));
+    const float a2 = A(jx, iq + 1) + w * (A(jx + 1, iq + 1) - A(jx, iq + 1));
+    return a1 + 20.0f * (a2 - a1) * (trans - t.trn[iq - 1]);
 }
 
 }  // namespace front

@@ -621,6 +621,26 @@ extern "C" int orc_setalb(int n, const float* const* f, int ialbflg, float* sfca
     return 0;
 }
 
+// grrad's condensate: tracer [ntrac][lmk][n] -> clw [lmk][n] (rrtm_front.hpp grrad_clw).
+extern "C" int orc_grrad_clw(int n, int lmk, const float* tracer, int ntcw0, int ncld, float epsq, float* clw)
+{
+    orc::front::grrad_clw(n, lmk, tracer, ntcw0, ncld, epsq, clw);
+    return 0;
+}
+
+// grrad's IALB = 2 block: out [9][n] = sfcalbedo, smx, czmean, alvsf, alnsf, alvwf, alnwf, facsf, facwf.
+extern "C" int orc_payne_albedo(int n, const float* salbedo, const float* sm, const float* coszen, const float* trn,
+                                const float* za, const float* dza, const float* albd, float* out)
+{
+    const orc::front::PayneTab t{trn, za, dza, albd};
+    for (int p = 0; p < n; ++p) {
+        const float a = orc::front::payne_albedo(salbedo[p], sm[p], coszen[p], t);
+        const float v[9] = {a, sm[p], coszen[p], a, a, a, a, 0.0f, 0.0f};
+        for (int f = 0; f < 9; ++f) out[(size_t)f * n + p] = v[f];
+    }
+    return 0;
+}
+
 // f = glon, glat, sm, sice, si, sncovr, z0, stdh, tskin.
 extern "C" int orc_setemis(int n, const float* const* f, const int* idxems, int ialbflg, int iemslw, float* sfcemis)
 {

@@ -1,7 +1,8 @@
 """Generate front_golden.npz, the golden vectors of grrad's front end, from the reference's own kernels
 (oracle/_ref/libref_rrtm.so, built by oracle/build_ref.sh): phys_rrtm_dayparts_cosz / _scatter / _len (with the
 run-start scan), phys_rrtm_getgases, phys_rrtm_getozn, phys_rrtm_setalb, phys_rrtm_setemis and
-phys_rrtm_progcld2_column, on seeded synthetic inputs (columns.front_tables, surface_state, cloud_state; the
+phys_rrtm_progcld2_column, grrad_clouds_clw and grrad_clouds_albedo (the IALB = 2 block, with the reference's own
+tables), on seeded synthetic inputs (columns.front_tables, surface_state, cloud_state; the
 radiation layers of make_columns through grrad's set-up).  Every flag branch of each routine is a case.
 
 Keys: <unit>_in_<name> for the inputs, <unit>_<case>_<output> for the outputs, and the case parameters as
@@ -29,6 +30,7 @@ DP_IM, DP_JM = 131, 7         # DAYPARTS rows
 GAS_CASES = {f"co2_{f}_flip{v}": (f, v) for f in (0, 1, 2) for v in (0, 1)}
 OZN = dict(k1oz=3, k2oz=4, facoz=0.37, blte=-85.0, dlte=10.0)
 EMIS_CASES = {f"alb{a}_lw{lw}": (a, lw) for a in (0, 1) for lw in (0, 1)}
+CLW_CASES = ((2, 1), (2, 3))     # ntcw (1-based), ncld
 CLD_CASES = {   # ivflip, llyr, iovr, lcrick, lcnorm, lnoprec, lsashal, cld_fraction
     "nam": (0, 2, 1, 0, 0, 0, 0, 0),
     "sashal_random": (0, 5, 0, 1, 1, 0, 1, 0),
@@ -101,6 +103,23 @@ def main():
         for k, v in oracle.progcld2(inp, cfg, which="ref").items():
             blob[f"cld_{case}_{k}"] = v
         blob[f"cld_{case}_cfg"] = np.array(c, np.int32)
+    # grrad's condensate (grrad_clouds_clw): four tracers, sums of one and of three from the second
+    r = np.random.default_rng(44)
+    tracer = (r.random((4, 61, N)) * r.choice([0.0, 1e-13, 1e-6, 1e-3], (4, 61, N))).astype(np.float32)
+    blob["clw_in_tracer"] = tracer
+    for ntcw, ncld in CLW_CASES:
+        blob[f"clw_{ntcw}_{ncld}_clw"] = oracle.grrad_clw(tracer, ntcw, ncld, which="ref")
+    # grrad's IALB = 2 albedo (grrad_clouds_albedo, the reference's built-in tables), zenith angles across every
+    # row of the table including the overhead sun
+    deg = np.concatenate([np.linspace(0.0, 95.0, N - 4), [74.0, 50.0, 89.99, 0.0]])
+    pa = {"salbedo": r.uniform(0.05, 0.8, N).astype(np.float32),
+          "sm": r.choice(np.array([0.0, 0.4, 0.6, 1.0], np.float32), N),
+          "coszen": np.cos(np.radians(deg)).astype(np.float32)}
+    for k, v in pa.items():
+        blob[f"payne_in_{k}"] = v
+    tables = dict(np.load(ROOT / "woof_nam_b200" / "data" / "payne_albedo.npz"))
+    for k, v in oracle.payne_albedo(pa["salbedo"], pa["sm"], pa["coszen"], tables, which="ref").items():
+        blob[f"payne_{k}"] = v
     np.savez_compressed(OUT, **blob)
     print(f"wrote {OUT} ({OUT.stat().st_size / 1e3:.0f} kB)")
 

@@ -1,6 +1,8 @@
 """grrad's front end in the oracle, pinned to the reference's kernels: the restatement (oracle/rrtm_front.hpp)
 reproduces the golden vectors of phys_rrtm_dayparts_*, phys_rrtm_getgases, phys_rrtm_getozn, phys_rrtm_setalb,
-phys_rrtm_setemis and phys_rrtm_progcld2_column bit for bit in every flag branch, and the DAYPARTS run table
+phys_rrtm_setemis, phys_rrtm_progcld2_column, grrad's condensate (grrad_clouds_clw) and its IALB = 2 surface
+albedo (grrad_clouds_albedo, whose built-in tables the packed woof_nam_b200/data/payne_albedo.npz reproduces) bit
+for bit in every flag branch, and the DAYPARTS run table
 and gethml's deck indices have the structure the consumers rely on (grrad_nmmb.f:640-653)."""
 from __future__ import annotations
 
@@ -16,6 +18,8 @@ GAS_CASES = {f"co2_{f}_flip{v}": (f, v) for f in (0, 1, 2) for v in (0, 1)}
 OZN = dict(k1oz=3, k2oz=4, facoz=0.37, blte=-85.0, dlte=10.0)
 EMIS_CASES = {f"alb{a}_lw{lw}": (a, lw) for a in (0, 1) for lw in (0, 1)}
 CLD_CASES = ("nam", "sashal_random", "flip", "flip_sashal", "thompson")
+CLW_CASES = ((2, 1), (2, 3))
+PAYNE = Path(__file__).resolve().parents[1] / "woof_nam_b200" / "data" / "payne_albedo.npz"
 
 
 @pytest.fixture(scope="module")
@@ -94,3 +98,23 @@ def test_progcld2(gold, case):
     assert ((r["mtop"] >= 1) & (r["mtop"] <= nlay) & (r["mbot"] >= 1) & (r["mbot"] <= nlay)).all()
     cl = r["clds"]
     assert ((cl >= 0) & (cl <= 1)).all() and (cl[3] >= cl[:3].max(0) - 1e-6).all()   # total >= each deck
+
+
+@pytest.mark.parametrize("ntcw,ncld", CLW_CASES)
+def test_grrad_clw(gold, ntcw, ncld):
+    r = oracle.grrad_clw(gold["clw_in_tracer"], ntcw, ncld)
+    assert np.array_equal(r, gold[f"clw_{ntcw}_{ncld}_clw"])
+    assert (r == 0).any() and (r > 0).any()
+    with pytest.raises(ValueError):
+        oracle.grrad_clw(gold["clw_in_tracer"], 3, 3)
+
+
+def test_payne_albedo(gold):
+    tables = dict(np.load(PAYNE))
+    assert tables["albd"].shape == (20, 21) and tables["za"][0] == 90.0 and tables["za"][-1] == 0.0
+    r = oracle.payne_albedo(gold["payne_in_salbedo"], gold["payne_in_sm"], gold["payne_in_coszen"], tables)
+    for k in oracle.PAYNE_OUT:
+        assert np.array_equal(r[k], gold[f"payne_{k}"]), k
+    changed = r["sfcalbedo"] != gold["payne_in_salbedo"]
+    assert changed.any() and (~changed).any()
+    assert not changed[(gold["payne_in_sm"] <= 0.5) | (gold["payne_in_coszen"] <= 0)].any()
