@@ -308,6 +308,29 @@ typedef struct {
  * stream; needs rad_load_aerosols first. */
 int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faersw, float* faerlw, void* stream);
 
+/* grrad's condensate clw [lmk][ncol] = the sum of the ncld cloud tracers ntcw .. ntcw + ncld - 1 (1-based) of
+ * tracer [ntrac][lmk][ncol], values below epsq set to zero (replaces grrad_clouds_clw,
+ * namgpu/kernels/phys_rrtm_grrad_clouds.cu:396-416, as phys_rrtm_grrad_clouds.py:183-193 launches it; NAM: ncld 1,
+ * epsq 1e-12).  Device pointers; asynchronous on stream. */
+int rad_grrad_clw(RadHandle* h, const float* tracer, int32_t ntrac, int32_t lmk, int64_t ncol, int32_t ntcw,
+                  int32_t ncld, float epsq, float* clw, void* stream);
+
+/* The IALB = 2 albedo tables (grrad_nmmb.f DATA TRN, ZA, DZA, ALBD; woof_nam_b200/data/payne_albedo.npz): host
+ * pointers, copied into each launch. */
+typedef struct {
+    const float* trn;        /* [21] */
+    const float* za;         /* [20] zenith angles, degrees */
+    const float* dza;        /* [19] */
+    const float* albd;       /* [20][21] albedo by zenith row and transmissivity column */
+} RadPayneTables;
+
+/* grrad's IALB = 2 surface albedo of ncol points (replaces grrad_clouds_albedo,
+ * namgpu/kernels/phys_rrtm_grrad_clouds.cu:344-393, phys_rrtm_grrad_clouds.py:230-245): from salbedo, sm and
+ * coszen [ncol] (device) the nine fields out[0..8] [ncol] (device): sfcalbedo, smx, czmean, alvsf, alnsf, alvwf,
+ * alnwf, facsf, facwf, the last six being what rad_setalb (ialbflg 2) reads.  Asynchronous on stream. */
+int rad_payne_albedo(RadHandle* h, const float* salbedo, const float* sm, const float* coszen, int64_t ncol,
+                     const RadPayneTables* t, float* const* out, void* stream);
+
 /* setaer's stratospheric volcanic aerosol term (the lavoflg branch, iaer >= 100; off on NAM): replaces
  * phys_rrtm_setaer_volc (namgpu/kernels/phys_rrtm_setaer.cu:178-330) as phys_rrtm_setaer.py:177-192 calls it
  * after the climatological optics.  Adds, in place, each column's zone optical depth, spread over the layers

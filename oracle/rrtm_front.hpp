@@ -593,7 +593,7 @@ inline float payne_albedo(float salbedo, float sm, float cz, const PayneTab& t)
     if (zen >= 74.0f) jx = (int)(0.5f * (90.0f - zen) + 1.0f);
     else if (zen >= 50.0f) jx = (int)(0.25f * (74.0f - zen) + 9.0f);
     else jx = (int)(0.1f * (50.0f - zen) + 15.0f);
-    jx = std::min(jx, 19);
+    jx = std::max(1, std::min(jx, 19));   // rows 1..19 (a coszen above 1 gives a NaN zenith; the CUDA path clamps)
     const float w = -(zen - t.za[jx - 1]) / t.dza[jx - 1];
     auto A = [&](int row, int col) { return t.albd[(row - 1) * 21 + (col - 1)]; };   // 1-based row, column
     const float a1 = A(jx, iq) + w * (A(jx + 1, iq) - A(jx, iq));

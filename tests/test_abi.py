@@ -41,7 +41,7 @@ def test_struct_layout_matches_header(tmp_path):
     for st in (_lib.RadConfig, _lib.RadColumns, _lib.RadOutputs, _lib.RadProfile, _lib.RadPostIn, _lib.RadPostOut,
                _lib.RadRdtemp, _lib.RadAerClim, _lib.RadAerColumns, _lib.RadSolarIn, _lib.RadSolarState, _lib.RadModelColumns,
                _lib.RadLayerFields, _lib.RadDayparts, _lib.RadGasSetup, _lib.RadOzoneClim, _lib.RadAlbedoIn,
-               _lib.RadEmisIn, _lib.RadCloudIn, _lib.RadCloudCfg, _lib.RadCloudOut):
+               _lib.RadEmisIn, _lib.RadCloudIn, _lib.RadCloudCfg, _lib.RadCloudOut, _lib.RadPayneTables):
         lines.append(f'printf("{st.__name__} size %zu\\n", sizeof({st.__name__}));')
         for f, _ in st._fields_:
             lines.append(f'printf("{st.__name__}.{f} %zu\\n", offsetof({st.__name__}, {f}));')
@@ -54,7 +54,7 @@ def test_struct_layout_matches_header(tmp_path):
     for st in (_lib.RadConfig, _lib.RadColumns, _lib.RadOutputs, _lib.RadProfile, _lib.RadPostIn, _lib.RadPostOut,
                _lib.RadRdtemp, _lib.RadAerClim, _lib.RadAerColumns, _lib.RadSolarIn, _lib.RadSolarState, _lib.RadModelColumns,
                _lib.RadLayerFields, _lib.RadDayparts, _lib.RadGasSetup, _lib.RadOzoneClim, _lib.RadAlbedoIn,
-               _lib.RadEmisIn, _lib.RadCloudIn, _lib.RadCloudCfg, _lib.RadCloudOut):
+               _lib.RadEmisIn, _lib.RadCloudIn, _lib.RadCloudCfg, _lib.RadCloudOut, _lib.RadPayneTables):
         assert int(got[f"{st.__name__} size"]) == ctypes.sizeof(st), st.__name__
         for f, _ in st._fields_:
             assert int(got[f"{st.__name__}.{f}"]) == getattr(st, f).offset, f"{st.__name__}.{f}"

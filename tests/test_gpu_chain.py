@@ -40,7 +40,7 @@ def _sun():
     return solar.sol_update((2026, 7, 1, 14, 30, 0), deltsw=1200.0, deltim=25.0)
 
 
-def _oracle_chain(state, tab, lay, sun, month=None):
+def _oracle_chain(state, tab, lay, sun, month=None, ntcw=None):
     n = IM * JM
     dp = oracle.dayparts(state["glon"], state["sinlat"], state["coslat"], IM, CALL["solhr"], CALL["dtswav"],
                          CALL["nrads"], [sun["sollag"], sun["sindec"], sun["cosdec"]])
@@ -50,9 +50,16 @@ def _oracle_chain(state, tab, lay, sun, month=None):
                           tab["co2vmr_sav"], CALL["ico2flg"], CALL["kmonsav"], 0)
     cin = {k: lay[k] for k in ("plyr", "plvl", "tlyr", "tvly", "qlyr", "qstl", "rhly")}
     cin.update({k: state[k] for k in ("clw", "f_ice", "f_rain", "r_rime", "cldfk1")}, xlat=state["glat"])
+    if ntcw is not None:
+        cin["clw"] = oracle.grrad_clw(state["tracer1"], ntcw, 1)
     cld = oracle.progcld2(cin, dict(ivflip=0, llyr=2, iovr=1, lcrick=0, lcnorm=0, lnoprec=0, lsashal=0,
                                     cld_fraction=0))
-    alb = oracle.setalb(dict(state, coszf=dp["coszen"]), CALL["ialbflg"])
+    sfc = dict(state, coszf=dp["coszen"])
+    if CALL["ialbflg"] == 2 and "sfcalbedo" in state:
+        from woof_nam_b200 import front
+        pa = oracle.payne_albedo(state["sfcalbedo"], state["sm"], dp["coszen"], front.payne_tables())
+        sfc.update({k: pa[k] for k in ("alvsf", "alnsf", "alvwf", "alnwf", "facsf", "facwf")})
+    alb = oracle.setalb(sfc, CALL["ialbflg"])
     ems = oracle.setemis(state, tab["idxems"], CALL["ialbflg"], CALL["iemslw"])
     cols = Columns(plyr=lay["plyr"], plvl=lay["plvl"], tlyr=lay["tlyr"], tlvl=lay["tlvl"], qlyr=lay["qlyr"],
                    olyr=olyr, gasvmr=gas, clouds=cld["clouds"], sfcemis=ems, tsfg=lay["tsfg"], sfcalb=alb,
@@ -120,3 +127,34 @@ def test_chain_with_aerosols():
     assert out["work"]["faer"][0].abs().sum().item() > 0
     ref = _oracle_chain(state, tab, lay, sun, month=1)
     assert_within(got, {k: ref[k] for k in got}, what="radiation call with aerosol")
+
+
+def test_chain_from_tracers_and_ialb2_albedo():
+    """The call started from the cloud tracers (clw = tracer ntcw, grrad's condensate) and, with ialbflg 2, from
+    the surface albedo and land mask through grrad's IALB = 2 block, against the oracle's chain doing the same."""
+    import torch
+    from woof_nam_b200.chain import radiation_call
+    from woof_nam_b200.solver import RadSolver
+    state, tab, lay = _domain(63)
+    r = np.random.default_rng(64)
+    n = IM * JM
+    tracer = r.random((3, lay["plyr"].shape[0], n)).astype(np.float32) * 1e-3
+    tracer[1] = state["clw"]
+    state.update(tracer1=tracer, sfcalbedo=r.uniform(0.05, 0.6, n).astype(np.float32),
+                 clw=np.zeros_like(state["clw"]))
+    sun = _sun()
+    call = dict(CALL, ialbflg=2)
+    s = RadSolver(precision="mixed", nlay=lay["plyr"].shape[0])
+    d, c = _dev(state, tab)
+    out = radiation_call(s, d, c, sun=sun, im=IM, ntcw=2, **call)
+    torch.cuda.synchronize()
+    got = {k: v.cpu().numpy() for k, v in out.items() if k != "work"}
+    saved = dict(CALL)
+    CALL.update(ialbflg=2)
+    try:
+        ref = _oracle_chain(state, tab, lay, sun, ntcw=2)
+    finally:
+        CALL.clear()
+        CALL.update(saved)
+    assert_within(got, {k: ref[k] for k in got}, what="radiation call from tracers, IALB 2")
+    assert out["work"]["clw"].abs().sum().item() > 0 and "albedo" in out["work"]

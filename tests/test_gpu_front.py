@@ -274,3 +274,31 @@ def test_invalid_arguments(solver):
         front.progcld2(solver, cld, ivflip=0, llyr=4, iovr=1)             # llyr outside 1..nlay
     with pytest.raises(ValueError):
         front.dayparts(solver, v, v, v, 0.0, 1.0, 1, _sun([0, 0, 1]), 3)   # 4 points are not rows of 3
+
+
+@pytest.mark.parametrize("ntcw,ncld", [(2, 1), (2, 3)])
+def test_grrad_clw_golden(gold, solver, ntcw, ncld):
+    """grrad's condensate: float sums in tracer order, bit for bit."""
+    import torch
+    from woof_nam_b200 import front
+    clw = front.grrad_clw(solver, _cuda(gold["clw_in_tracer"]), ntcw, ncld)
+    torch.cuda.synchronize()
+    assert np.array_equal(clw.cpu().numpy(), gold[f"clw_{ntcw}_{ncld}_clw"])
+
+
+def test_payne_albedo_golden(gold, solver):
+    """grrad's IALB = 2 albedo with the packed tables against the reference kernel's built-in ones: CUDA's acosf
+    against the host's moves the zenith angle by its last bits, and the table interpolation is continuous across
+    rows, so the albedo agrees to 2e-6; the points the block leaves alone, and the copied fields, bit for bit."""
+    import torch
+    from woof_nam_b200 import front
+    out = front.payne_albedo(solver, _cuda(gold["payne_in_salbedo"]), _cuda(gold["payne_in_sm"]),
+                             _cuda(gold["payne_in_coszen"]))
+    torch.cuda.synchronize()
+    got = {k: v.cpu().numpy() for k, v in out.items()}
+    for k in ("smx", "czmean", "facsf", "facwf"):
+        assert np.array_equal(got[k], gold[f"payne_{k}"]), k
+    keep = gold["payne_sfcalbedo"] == gold["payne_in_salbedo"]
+    for k in ("sfcalbedo", "alvsf", "alnsf", "alvwf", "alnwf"):
+        assert np.array_equal(got[k][keep], gold[f"payne_{k}"][keep]), k
+        assert np.abs(got[k] - gold[f"payne_{k}"]).max() <= 2e-6, k

@@ -148,6 +148,10 @@ class RadEmisIn(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in EMIS_FIELDS]
 
 
+class RadPayneTables(ctypes.Structure):
+    _fields_ = [(k, ctypes.POINTER(ctypes.c_float)) for k in ("trn", "za", "dza", "albd")]
+
+
 class RadCloudIn(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in CLOUD_IN_FIELDS]
 
@@ -201,6 +205,11 @@ SIGNATURES = {
                       ctypes.POINTER(RadCloudCfg), ctypes.POINTER(RadCloudOut), ctypes.c_void_p], ctypes.c_int),
     "rad_setaer": ([ctypes.c_void_p, ctypes.POINTER(RadAerColumns), ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                     ctypes.c_void_p], ctypes.c_int),
+    "rad_grrad_clw": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32,
+                       ctypes.c_int32, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "rad_payne_albedo": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                          ctypes.POINTER(RadPayneTables), ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p],
+                         ctypes.c_int),
     "rad_setaer_volc": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
                          ctypes.POINTER(ctypes.c_int32), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                          ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),

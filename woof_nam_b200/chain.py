@@ -11,7 +11,9 @@ its chain's scratch for the whole domain does not fit its cards and its SW group
     rad_getozn        olyr, climatological ozone on the layers (ntoz 0)
     rad_getgases      gasvmr on the layers
     rad_setaer        faersw, faerlw: the climatological aerosol optics (iaer 11), when an Aerosols is given
+    rad_grrad_clw     clw from the cloud tracers, when ntcw is given
     rad_progcld2      clouds (Ferrier, np3d 3) with gethml's deck fractions
+    rad_payne_albedo  the IALB = 2 albedos from sfcalbedo, sm and the daytime zenith cosine, with ialbflg 2
     rad_setalb        sfcalb (from coszen for ialbflg 0 / 1)
     rad_setemis       sfcemis
     rad_solve         LW and SW: heating rates and fluxes
@@ -38,11 +40,14 @@ CLOUD_NAM = dict(ivflip=0, llyr=2, iovr=1, lcrick=False, lcnorm=False, lnoprec=F
 
 def radiation_call(solver, state: dict, clim: dict, *, sun: dict, solhr: float, dtswav: float, nrads: int, im: int,
                    kmonsav: int, k1oz: int, k2oz: int, facoz: float, ico2flg: int = 1, ialbflg: int = 2,
-                   iemslw: int = 1, cloud: dict | None = None, aerosols=None, work: dict | None = None,
-                   out: dict | None = None, stream=None) -> dict:
+                   iemslw: int = 1, cloud: dict | None = None, aerosols=None, ntcw: int | None = None,
+                   ncld: int = 1, work: dict | None = None, out: dict | None = None, stream=None) -> dict:
     """Run the call; returns the solve's outputs, with the front end's arrays under out["work"] (reused by the
     next call when passed back as `work`).  aerosols: an aerosols.Aerosols with the month's climatology loaded
-    (the state then needs slmsk), or None for no aerosol; state faersw / faerlw are used when given instead."""
+    (the state then needs slmsk), or None for no aerosol; state faersw / faerlw are used when given instead.
+    ntcw (1-based): the condensate clw comes from the tracers state["tracer1"] [ntrac, lmk, n] (grrad's clw);
+    else state["clw"] is read.  With ialbflg 2 and state["sfcalbedo"] (and "sm"), grrad's IALB = 2 block forms
+    the albedos setalb reads from it and the daytime zenith cosine; else state's alvsf ... facwf are read."""
     cloud = {**CLOUD_NAM, **(cloud or {})}
     if cloud["ivflip"] != 0:
         raise ValueError("radiation_call: the layers of grrad's set-up are top first (ivflip 0)")
@@ -79,8 +84,15 @@ def radiation_call(solver, state: dict, clim: dict, *, sun: dict, solhr: float, 
                                     state["glat"], state["slmsk"], out=w.get("faer"), stream=stream)
     cin = {k: lay[k] for k in ("plyr", "plvl", "tlyr", "tvly", "qlyr", "qstl", "rhly")}
     cin.update({k: state.get(k) for k in ("clw", "f_ice", "f_rain", "r_rime", "cldfk1")}, xlat=state["glat"])
+    if ntcw is not None:
+        w["clw"] = front.grrad_clw(solver, state["tracer1"], ntcw, ncld, clw=w.get("clw"), stream=stream)
+        cin["clw"] = w["clw"]
     w["cloud"] = front.progcld2(solver, cin, **cloud, out=w["cloud"], stream=stream)
     sfc = dict(state, coszf=coszen)
+    if ialbflg == 2 and state.get("sfcalbedo") is not None:
+        w["albedo"] = front.payne_albedo(solver, state["sfcalbedo"], state["sm"], coszen, out=w.get("albedo"),
+                                         stream=stream)
+        sfc.update({k: w["albedo"][k] for k in ("alvsf", "alnsf", "alvwf", "alnwf", "facsf", "facwf")})
     front.setalb(solver, sfc, ialbflg, w["sfcalb"], stream=stream)
     front.setemis(solver, state, clim.get("idxems"), ialbflg, iemslw, w["sfcemis"], stream=stream)
     cols = {"plyr": lay["plyr"], "plvl": lay["plvl"], "tlyr": lay["tlyr"], "tlvl": lay["tlvl"], "qlyr": lay["qlyr"],

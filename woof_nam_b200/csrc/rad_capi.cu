@@ -1098,6 +1098,46 @@ int rad_setaer(RadHandle* h, const RadAerColumns* in, int64_t ncol, float* faers
     return RAD_OK;
 }
 
+int rad_grrad_clw(RadHandle* h, const float* tracer, int32_t ntrac, int32_t lmk, int64_t ncol, int32_t ntcw,
+                  int32_t ncld, float epsq, float* clw, void* stream)
+{
+    if (!h) return fail(h, RAD_E_INVALID, "rad_grrad_clw: null argument");
+    if (ncol < 0 || lmk < 1 || ncld < 1 || ntcw < 1 || ntcw - 1 + ncld > ntrac)
+        return fail(h, RAD_E_INVALID, "rad_grrad_clw: sizes or tracer range out of range");
+    if ((int64_t)lmk * ncol > (int64_t)std::numeric_limits<int>::max() * 256)
+        return fail(h, RAD_E_INVALID, "rad_grrad_clw: too many points for one launch");
+    if (ncol == 0) return RAD_OK;
+    if (!tracer || !clw) return fail(h, RAD_E_INVALID, "rad_grrad_clw: a required pointer is null");
+    const front::ClwArgs a{tracer, clw, ncol, lmk, ntcw - 1, ncld, epsq};
+    h->launches += 1;
+    RAD_CUDA(h, front::grrad_clw(a, (cudaStream_t)stream));
+    return RAD_OK;
+}
+
+int rad_payne_albedo(RadHandle* h, const float* salbedo, const float* sm, const float* coszen, int64_t ncol,
+                     const RadPayneTables* t, float* const* out, void* stream)
+{
+    if (!h || !t || !out) return fail(h, RAD_E_INVALID, "rad_payne_albedo: null argument");
+    if (ncol < 0 || ncol > (int64_t)std::numeric_limits<int>::max() * 256)
+        return fail(h, RAD_E_INVALID, "rad_payne_albedo: ncol out of range");
+    if (ncol == 0) return RAD_OK;
+    if (!salbedo || !sm || !coszen || !t->trn || !t->za || !t->dza || !t->albd)
+        return fail(h, RAD_E_INVALID, "rad_payne_albedo: a required pointer is null");
+    front::PayneArgs a{};
+    a.salbedo = salbedo; a.sm = sm; a.coszen = coszen; a.n = ncol;
+    for (int f = 0; f < 9; ++f) {
+        if (!out[f]) return fail(h, RAD_E_INVALID, "rad_payne_albedo: an output pointer is null");
+        a.out[f] = out[f];
+    }
+    std::copy(t->trn, t->trn + 21, a.trn);
+    std::copy(t->za, t->za + 20, a.za);
+    std::copy(t->dza, t->dza + 19, a.dza);
+    std::copy(t->albd, t->albd + 20 * 21, a.albd);
+    h->launches += 1;
+    RAD_CUDA(h, front::payne_albedo(a, (cudaStream_t)stream));
+    return RAD_OK;
+}
+
 int rad_setaer_volc(RadHandle* h, const float* plvl, const float* xlat, int64_t ncol, int32_t ivflip,
                     const int32_t* ivolae, int32_t kyrsav, int32_t kmonsav, int32_t add_sw, int32_t add_lw,
                     int32_t lw1bd, float* faersw, float* faerlw, void* stream)

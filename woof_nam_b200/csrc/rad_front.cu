@@ -25,6 +25,10 @@
 //   k_progcld2   progcld2 with rsipath2_tmp and gethml (radiation_clouds_nmmb.f:787-1323, 2167-2494,
 //                2779-2964; phys_rrtm_progcld2.cu:92-444): one thread per column; the layer cloud fractions
 //                that gethml walks twice are kept in shared memory, [layer][thread].
+//   k_grrad_clw  grrad's condensate (grrad_nmmb.f:1556-1571, phys_rrtm_grrad_clouds.cu:396-416): one thread per
+//                (layer, column), the cloud tracers summed in tracer order.
+//   k_payne_albedo  grrad's IALB = 2 surface albedo (grrad_nmmb.f:1722-1794, phys_rrtm_grrad_clouds.cu:344-393):
+//                one thread per point; the tables travel in the kernel parameters (1.9 KB).
 //   k_setaer_volc  setaer's volcanic stratospheric term (radiation_aerosols.f 2092-2352, the lavoflg branch;
 //                namgpu/kernels/phys_rrtm_setaer.cu:178-330): one thread per column finds the aerosol's top
 //                (5 mb) and bottom (150-250 mb by latitude) layers and adds its zone's optical depth, spread
@@ -594,6 +598,47 @@ __global__ void __launch_bounds__(CLD_THREADS) k_progcld2(const CloudArgs a)
     }
 }
 
+// ------------------------------------------------------------------------------------------ clw
+// Per (layer, column) ncld words read and one written.
+__global__ void __launch_bounds__(256) k_grrad_clw(const ClwArgs a)
+{
+    const int64_t plane = (int64_t)a.lmk * a.n;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= plane) return;
+    float sum = 0.0f;
+    for (int j = 0; j < a.ncld; ++j) sum += __ldg(a.tracer + (int64_t)(a.ntcw0 + j) * plane + p);
+    a.clw[p] = sum < a.epsq ? 0.0f : sum;
+}
+
+// ------------------------------------------------------------------------------------------ IALB = 2 albedo
+// Per point 12 bytes read and 36 written.
+__global__ void __launch_bounds__(256) k_payne_albedo(const __grid_constant__ PayneArgs a)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    const float sm = __ldg(a.sm + p), cz = __ldg(a.coszen + p);
+    float alb = __ldg(a.salbedo + p);
+    const float trans = 0.537f;
+    const int iq = (int)(20.0f * trans + 1.0f);          // transmissivity column (1-based)
+    if (cz > 0.0f && sm > 0.5f) {
+        const float zen = (180.0f / 3.14159265f) * acosf(fmaxf(cz, 0.0f));
+        int jx;                                           // zenith row (1-based)
+        if (zen >= 74.0f) jx = (int)(0.5f * (90.0f - zen) + 1.0f);
+        else if (zen >= 50.0f) jx = (int)(0.25f * (74.0f - zen) + 9.0f);
+        else jx = (int)(0.1f * (50.0f - zen) + 15.0f);
+        jx = max(1, min(jx, 19));                         // rows 1..19 (a coszen above 1 gives a NaN zenith)
+        const float w = -(zen - a.za[jx - 1]) / a.dza[jx - 1];
+        const float* r0 = a.albd + (jx - 1) * 21;
+        const float* r1 = r0 + 21;
+        const float a1 = r0[iq - 1] + w * (r1[iq - 1] - r0[iq - 1]);
+        const float a2 = r0[iq] + w * (r1[iq] - r0[iq]);
+        alb = a1 + 20.0f * (a2 - a1) * (trans - a.trn[iq - 1]);
+    }
+    const float v[9] = {alb, sm, cz, alb, alb, alb, alb, 0.0f, 0.0f};
+#pragma unroll
+    for (int f = 0; f < 9; ++f) a.out[f][p] = v[f];
+}
+
 // ------------------------------------------------------------------------------------------ volcanic term
 // Per column (nlay + 1) * 4 bytes of pressure read, and the extinction of the 30 bands over the aerosol's
 // layers (about 15 of 61 on NAM's levels) read and written.
@@ -711,6 +756,18 @@ cudaError_t progcld2(const CloudArgs& a, cudaStream_t st)
         if (e != cudaSuccess) return e;
     }
     k_progcld2<<<blocks(a.n, CLD_THREADS), CLD_THREADS, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t grrad_clw(const ClwArgs& a, cudaStream_t st)
+{
+    k_grrad_clw<<<blocks((int64_t)a.lmk * a.n, 256), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t payne_albedo(const PayneArgs& a, cudaStream_t st)
+{
+    k_payne_albedo<<<blocks(a.n, 256), 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 

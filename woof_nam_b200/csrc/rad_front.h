@@ -76,6 +76,26 @@ struct CloudArgs {
 constexpr int CLOUD_MAX_LAY = 128;
 cudaError_t progcld2(const CloudArgs& a, cudaStream_t st);
 
+// grrad's condensate: clw [lmk][n] = the ncld tracers from ntcw0 (0-based) of tracer [ntrac][lmk][n], summed,
+// below epsq set to zero.
+struct ClwArgs {
+    const float* tracer;
+    float* clw;
+    int64_t n;
+    int32_t lmk, ntcw0, ncld;
+    float epsq;
+};
+cudaError_t grrad_clw(const ClwArgs& a, cudaStream_t st);
+
+// grrad's IALB = 2 surface albedo of n points, the tables by value.
+struct PayneArgs {
+    const float *salbedo, *sm, *coszen;                 // [n]
+    float* out[9];                                      // sfcalbedo, smx, czmean, alvsf, alnsf, alvwf, alnwf, facsf, facwf
+    int64_t n;
+    float trn[21], za[20], dza[19], albd[20 * 21];      // albd [zenith row][transmissivity column]
+};
+cudaError_t payne_albedo(const PayneArgs& a, cudaStream_t st);
+
 // setaer's volcanic stratospheric term on nlay layers of n columns, added in place to component 0 (extinction).
 struct VolcArgs {
     const float *plvl, *xlat;                           // [nlay + 1][n] mb in the order of ivflip, [n] radians

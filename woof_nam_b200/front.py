@@ -16,6 +16,7 @@ is read back to the host.
 from __future__ import annotations
 
 import ctypes
+import functools
 
 from . import _lib
 
@@ -200,4 +201,63 @@ def progcld2(solver, inputs: dict, *, ivflip: int, llyr: int, iovr: int, lcrick:
                                  _stream(stream))
     _lib.check(solver.lib, solver.handle, rc, "rad_progcld2")
     out["mtopa"], out["mbota"] = out["mtop"], out["mbot"]
+    return out
+
+
+def grrad_clw(solver, tracer, ntcw: int, ncld: int = 1, clw=None, epsq: float = 1.0e-12, stream=None):
+    """grrad's condensate clw [lmk][n] (phys_rrtm_grrad_clouds: grrad_clouds_clw) from the tracers [ntrac][lmk][n]:
+    the ncld tracers from ntcw (1-based; NAM ncld 1) summed, below epsq zero."""
+    torch = _torch()
+    if tracer.dim() != 3:
+        raise ValueError(f"grrad_clw: tracer must be [ntrac, lmk, n], got {tuple(tracer.shape)}")
+    ntrac, lmk, n = tracer.shape
+    _chk(tracer, "tracer", "grrad_clw", (ntrac, lmk, n))
+    if clw is None:
+        clw = torch.empty((lmk, n), dtype=torch.float32, device=tracer.device)
+    _chk(clw, "clw", "grrad_clw", (lmk, n))
+    rc = solver.lib.rad_grrad_clw(solver.handle, _dev(tracer, "tracer", "grrad_clw"), int(ntrac), int(lmk), int(n),
+                                  int(ntcw), int(ncld), float(epsq), _dev(clw, "clw", "grrad_clw"), _stream(stream))
+    _lib.check(solver.lib, solver.handle, rc, "rad_grrad_clw")
+    return clw
+
+
+PAYNE_OUT = ("sfcalbedo", "smx", "czmean", "alvsf", "alnsf", "alvwf", "alnwf", "facsf", "facwf")
+
+
+@functools.lru_cache(maxsize=4)
+def payne_tables(path=None) -> dict:
+    """The IALB = 2 albedo tables (trn, za, dza, albd) as float32 numpy arrays (woof_nam_b200/data/payne_albedo.npz)."""
+    import numpy as np
+    from pathlib import Path
+    p = Path(path) if path is not None else Path(__file__).resolve().parent / "data" / "payne_albedo.npz"
+    with np.load(p) as z:
+        return {k: np.ascontiguousarray(z[k], dtype=np.float32) for k in ("trn", "za", "dza", "albd")}
+
+
+def payne_albedo(solver, salbedo, sm, coszen, tables: dict | None = None, out: dict | None = None, stream=None):
+    """grrad's IALB = 2 surface albedo (phys_rrtm_grrad_clouds: grrad_clouds_albedo) of n points from salbedo, sm,
+    coszen [n]: a dict of PAYNE_OUT [n] CUDA tensors, alvsf / alnsf / alvwf / alnwf / facsf / facwf being what
+    setalb (ialbflg 2) reads."""
+    import numpy as np
+    torch = _torch()
+    n = salbedo.numel()
+    for k, t in (("salbedo", salbedo), ("sm", sm), ("coszen", coszen)):
+        _chk(t, k, "payne_albedo", (n,))
+    t = tables if tables is not None else payne_tables()
+    sizes = {"trn": (21,), "za": (20,), "dza": (19,), "albd": (20, 21)}
+    arr = {k: np.ascontiguousarray(t[k], dtype=np.float32) for k in sizes}
+    for k, shp in sizes.items():
+        if arr[k].shape != shp:
+            raise ValueError(f"payne_albedo: table {k} has shape {arr[k].shape}, expected {shp}")
+    if out is None:
+        out = {k: torch.empty(n, dtype=torch.float32, device=salbedo.device) for k in PAYNE_OUT}
+    for k in PAYNE_OUT:
+        _chk(out[k], k, "payne_albedo", (n,))
+    fp = ctypes.POINTER(ctypes.c_float)
+    tb = _lib.RadPayneTables(*[arr[k].ctypes.data_as(fp) for k in ("trn", "za", "dza", "albd")])
+    ptrs = (ctypes.c_void_p * 9)(*[out[k].data_ptr() for k in PAYNE_OUT])
+    rc = solver.lib.rad_payne_albedo(solver.handle, _dev(salbedo, "salbedo", "payne_albedo"),
+                                     _dev(sm, "sm", "payne_albedo"), _dev(coszen, "coszen", "payne_albedo"), int(n),
+                                     ctypes.byref(tb), ptrs, _stream(stream))
+    _lib.check(solver.lib, solver.handle, rc, "rad_payne_albedo")
     return out
