@@ -342,7 +342,7 @@ def main():
     import torch.distributed as dist
     from oracle import oracle
     from woof_nam_b200.columns import WORKLOADS, workload, make_columns
-    from woof_nam_b200.solver import RadSolver, output_shapes, INPUT_FIELDS
+    from woof_nam_b200.solver import RadSolver, INPUT_FIELDS
 
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
