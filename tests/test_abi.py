@@ -88,4 +88,7 @@ def test_null_arguments(lib):
     assert lib.rad_load_tables(None, None, 0) == _lib.RAD_E_INVALID
     assert lib.rad_load_aerosols(None, None) == _lib.RAD_E_INVALID
     assert lib.rad_setaer(None, None, 0, None, None, None) == _lib.RAD_E_INVALID
+    assert lib.rad_setaer_volc(None, None, None, 0, 0, None, 1, 1, 1, 1, 0, None, None, None) == _lib.RAD_E_INVALID
+    assert lib.rad_grrad_clw(None, None, 1, 61, 0, 1, 1, 1e-12, None, None) == _lib.RAD_E_INVALID
+    assert lib.rad_payne_albedo(None, None, None, None, 0, None, None, None) == _lib.RAD_E_INVALID
     lib.rad_destroy(None)
