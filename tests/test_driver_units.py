@@ -295,3 +295,22 @@ def test_grrad_aerosols_unit_flags_and_volcanic():
     o = grrad_aerosols.run(ctx, lsswr=True, lslwr=True)
     torch.cuda.synchronize()
     assert not o["faersw"].any() and not o["faerlw"].any()
+
+
+def test_aerosol_module_flags():
+    """setaer's module state as the aerosol unit reads it (no GPU): rad_initialize's flag vector, iaer = 11 (NAM),
+    111 (with the volcanic term), 100 (volcanic only) and 0; grrad's aer_state when present; the defaults."""
+    def ctx(**tables):
+        return SimpleNamespace(tables=tables)
+
+    assert driver._aer_flags(ctx()) == {"iaerflg": 11, "laswflg": True, "lalwflg": True, "lavoflg": False,
+                                        "ivflip": 0, "kyrsav": 1, "kmonsav": 1}
+    for iaer, sw, lw, vo in ((11, 1, 1, 0), (111, 1, 1, 1), (100, 0, 0, 1), (0, 0, 0, 0)):
+        p = np.zeros(26, np.int32)
+        p[4:8] = (iaer, sw, lw, vo)
+        p[25] = 1
+        f = driver._aer_flags(ctx(rad_physparam=p, aer_volc=SimpleNamespace(kyrsav=1991, kmonsav=6)))
+        assert (f["iaerflg"], f["laswflg"], f["lalwflg"], f["lavoflg"]) == (iaer, bool(sw), bool(lw), bool(vo))
+        assert (f["ivflip"], f["kyrsav"], f["kmonsav"]) == (1, 1991, 6)
+    st = {"iaerflg": 11, "laswflg": True, "lalwflg": False, "lavoflg": False, "ivflip": 0, "kyrsav": 2, "kmonsav": 3}
+    assert driver._aer_flags(ctx(aer_state=st, rad_physparam=np.zeros(26, np.int32))) is st
