@@ -60,8 +60,13 @@ class RadServer:
     """members[domain] -> list of device-resident column dicts (one per member)."""
 
     def __init__(self, states: dict, solcon: float, slots: int = 4, hbm_budget_gb: float = 120.0,
-                 precision: str = "mixed", keep_outputs: bool = False):
+                 precision: str = "mixed", keep_outputs: bool = False, policy: str = "fifo"):
+        """policy: the order in which queued requests take free slots -- "fifo" (arrival order) or "sjf" (the
+        request with the fewest columns first, arrival order among equals)."""
         import torch
+        if policy not in ("fifo", "sjf"):
+            raise ValueError(f"RadServer: policy must be 'fifo' or 'sjf', got {policy!r}")
+        self.policy = policy
         self.torch = torch
         self.states = states
         self.solcon = solcon
@@ -88,6 +93,9 @@ class RadServer:
         """Device bytes a request adds while it is in flight: its output arrays (the slot's scratch is held
         already and counted at start-up)."""
         return sum(int(np.prod(s)) * 4 for s in output_shapes(solver.cfg.nlay, ncol).values())
+
+    def _ncol(self, req: Request) -> int:
+        return int(self.states[req.domain][req.member]["coszen"].shape[-1])
 
     def _launch(self, slot: _Slot, req: Request, now: float):
         torch = self.torch
@@ -123,11 +131,14 @@ class RadServer:
                     sl.req, sl.out = None, {}
             for sl in self.slots:                      # admissions: a free slot and room in the budget
                 if sl.req is None and queue:
-                    r = queue[0]
-                    need = self.request_bytes(int(self.states[r.domain][r.member]["coszen"].shape[-1]), sl.solver)
+                    qi = 0
+                    if self.policy == "sjf":
+                        qi = min(range(len(queue)), key=lambda i: (self._ncol(queue[i]), queue[i].arrival))
+                    r = queue[qi]
+                    need = self.request_bytes(self._ncol(r), sl.solver)
                     if self.resident + self.held + self.in_use + need > self.budget:
                         break
-                    queue.pop(0)
+                    queue.pop(qi)
                     self.in_use += need
                     self._launch(sl, r, time.perf_counter() - t0)
             if pending and not queue and all(sl.req is None for sl in self.slots):
