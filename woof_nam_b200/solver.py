@@ -7,7 +7,7 @@ layout and returns the LW/SW heating rates and the surface and TOA fluxes under 
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 
@@ -83,6 +83,20 @@ def output_shapes(nlay: int, ncol: int, route: str = "nam", cfg: "SolverConfig |
 MASK_KEYS = ("lw_mask", "sw_mask")
 
 
+def _fits(t, shape: tuple) -> bool:
+    """t holds exactly the elements of `shape` with the columns last (a [3][14][nlay][ncol] array may come as
+    [42][nlay][ncol]: the kernels read contiguous memory by nlay and ncol alone)."""
+    return t.dim() >= 1 and t.shape[-1] == shape[-1] and t.numel() == int(np.prod(shape))
+
+
+def input_shapes(nlay: int, ncol: int) -> dict:
+    """Shapes of a solve's inputs (RadColumns), the optional ones included."""
+    return {"plyr": (nlay, ncol), "plvl": (nlay + 1, ncol), "tlyr": (nlay, ncol), "tlvl": (nlay + 1, ncol),
+            "qlyr": (nlay, ncol), "olyr": (nlay, ncol), "gasvmr": (10, nlay, ncol), "clouds": (9, nlay, ncol),
+            "faerlw": (3, 16, nlay, ncol), "faersw": (3, 14, nlay, ncol), "sfcemis": (ncol,), "tsfg": (ncol,),
+            "sfcalb": (4, ncol), "coszen": (ncol,), "icseed": (2, ncol)}
+
+
 class RadSolver:
     """One library handle on the current CUDA device."""
 
@@ -132,16 +146,22 @@ class RadSolver:
     def _abi_args(self, cols: dict, solcon: float, out: dict | None):
         torch = _torch()
         ncol = int(cols["plyr"].shape[-1])
-        for k in PART_FIELDS[self.cfg.parts]:
-            t = cols.get(k)
-            if t is None:
-                raise KeyError(f"input {k!r} is missing")
-            if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
-                raise TypeError(f"input {k!r} must be a contiguous float32 CUDA tensor")
-            if t.shape[-1] != ncol:
-                raise ValueError(f"input {k!r} has {t.shape[-1]} columns, expected {ncol}")
+        # shapes first (the kernels index by nlay and ncol alone), then devices and types
         if cols["plyr"].shape[0] != self.cfg.nlay:
             raise ValueError(f"plyr has {cols['plyr'].shape[0]} layers, the solver was built for {self.cfg.nlay}")
+        want = input_shapes(self.cfg.nlay, ncol)
+        for k in PART_FIELDS[self.cfg.parts]:
+            if cols.get(k) is None:
+                raise KeyError(f"input {k!r} is missing")
+        for k, shp in want.items():
+            t = cols.get(k)
+            if t is not None and not _fits(t, shp):
+                raise ValueError(f"input {k!r} has shape {tuple(t.shape)}, expected {shp} (or the same elements with "
+                                 "the columns last)")
+        for k in PART_FIELDS[self.cfg.parts]:
+            t = cols[k]
+            if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+                raise TypeError(f"input {k!r} must be a contiguous float32 CUDA tensor")
         if out is None:
             out = self.alloc_outputs(ncol, device=cols["plyr"].device)
         ci = _lib.RadColumns()
@@ -157,8 +177,16 @@ class RadSolver:
             setattr(ci, k, t.data_ptr() if t is not None else None)
         ci.solcon = float(solcon)
         co = _lib.RadOutputs()
+        full = output_shapes(self.cfg.nlay, ncol, "mcica", replace(self.cfg, lhsw0=True, lhswb=True, lhlw0=True,
+                                                                   lhlwb=True, lflxprf=True))
         for k in tuple(output_shapes(1, 1, "mcica")) + OPTIONAL_OUTPUTS:
             t = out.get(k)
+            if t is not None:
+                dt = torch.int32 if k in MASK_KEYS else torch.float32
+                if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == dt and t.is_contiguous()):
+                    raise TypeError(f"output {k!r} must be a contiguous {dt} CUDA tensor")
+                if not _fits(t, full[k]):
+                    raise ValueError(f"output {k!r} has shape {tuple(t.shape)}, expected {full[k]}")
             setattr(co, k, t.data_ptr() if t is not None else None)
         return ci, co, ncol, out
 
